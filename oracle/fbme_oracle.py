@@ -1,0 +1,749 @@
+"""CPU oracle for the FBME plan-replay hot path (numpy restatement).
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference``
+legs of ``bench.py`` may import it.  The product path
+(``fbme_b200`` and the drop-in ``torch_sbl`` / ``torch_sbl_fastest_stable``
+packages) never imports, calls or falls back to it.
+
+It restates, in plain numpy, the algorithm of the reference package
+``torch_sbl`` (FBME-SBL v1.1) for the locked FBME-Fast / FBME-Stable
+profiles (``mode="uamp"``) and the ``mode="cg"`` PCG + Hutchinson path.
+Every function cites the reference ``file:line`` it follows.  Arithmetic
+runs in the dtype of the input (complex64/float32 mirrors the reference's
+complex64 run; complex128 gives the FP64 oracle).
+
+Pinning: the restatement is checked against golden vectors produced by
+executing the reference itself on seeded synthetic scenes
+(``tests/golden/make_golden.py`` writes them; ``tests/test_oracle_golden.py``
+compares).  The reference ships no golden vectors of its own.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from math import ceil, log, prod
+from typing import Any
+
+import numpy as np
+
+try:  # scipy is only used for triangular solves; numpy fallback below.
+    from scipy.linalg import solve_triangular as _solve_triangular
+except Exception:  # pragma: no cover
+    _solve_triangular = None
+
+
+# ---------------------------------------------------------------------------
+# Configuration (the subset of torch_sbl/solver.py:34-176 the hot path reads)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class OracleConfig:
+    """Hot-path fields of ``SBLConfig`` (torch_sbl/solver.py:34-176)."""
+
+    max_iter: int = 200
+    min_iter: int = 3
+    tol: float = 1e-4
+    hyper_shape: float = 1e-8
+    hyper_rate: float = 1e-8
+    noise_shape: float = 1e-8
+    noise_rate: float = 1e-8
+    initial_noise_fraction: float = 1e-2
+    initialization: str = "backprojection"
+    initialization_blend: float = 0.1
+    fixed_noise_variance: float | None = None
+    noise_update: str = "em"
+    damping: float = 0.15
+    min_variance: float = 1e-12
+    max_precision: float = 1e12
+    mode: str = "auto"
+    dense_threshold: int = 2048
+    cg_tolerance: float = 1e-5
+    cg_initial_tolerance: float = 1e-2
+    cg_max_iter: int = 150
+    cg_check_interval: int = 8
+    cg_fixed_iterations: int = 0
+    cg_preconditioner: str = "low_rank"
+    cg_preconditioner_rank: int = 32
+    cg_damping: float = 0.9
+    hutchinson_probes: int = 32
+    max_hutchinson_probes: int = 128
+    initial_hutchinson_probes: int = 16
+    auto_probe_scaling: bool = True
+    adaptive_cg: bool = True
+    adaptive_probes: bool = False
+    cg_warm_start: bool = True
+    cg_min_iter: int = 20
+    convergence_patience: int = 2
+    convergence_check_interval: int = 2
+    cuda_cholesky_jitter_multiplier: float = 8.0
+    uamp_damping: float = 0.1
+    uamp_adaptive_damping: bool = True
+    uamp_max_damping: float = 0.8
+    uamp_min_iter: int = 10
+    uamp_auto_iterations: bool = True
+    uamp_iteration_offset: float = 10.0
+    uamp_iteration_scale: float = 1.1
+    uamp_polish_size: int = 0
+    uamp_polish_iterations: int = 1
+    uamp_polish_prune_tail: bool = False
+    uamp_polish_reinitialize: bool = False
+    uamp_polish_damping: float = 0.0
+    uamp_polish_evidence_gate: bool = False
+    uamp_polish_evidence_margin_factor: float = 0.0
+    uamp_polish_residual_exchange_size: int = 0
+    uamp_polish_fixed_budget_diagnostics: bool = False
+    uamp_support_false_alarm_budget: float | None = None
+    active_set: bool = True
+    active_set_start: int = 30
+    active_set_check_interval: int = 2
+    active_set_min_size: int = 32
+    active_set_max_size: int = 256
+    active_set_tail_fraction: float = 5e-2
+    seed: int = 0
+
+    @classmethod
+    def fast_hybrid_uamp(cls, **overrides: Any) -> "OracleConfig":
+        """torch_sbl/solver.py:197-227."""
+        s: dict[str, Any] = dict(
+            mode="uamp", max_iter=200, min_iter=1, tol=0.0,
+            uamp_auto_iterations=True, uamp_min_iter=3,
+            uamp_iteration_offset=1.0, uamp_iteration_scale=1.0,
+            uamp_polish_size=32, uamp_polish_iterations=2,
+            uamp_polish_prune_tail=True, uamp_polish_reinitialize=True,
+            uamp_polish_damping=0.0, uamp_polish_evidence_gate=True,
+            uamp_polish_residual_exchange_size=0, active_set=False,
+        )
+        s.update(overrides)
+        return cls(**s)
+
+    @classmethod
+    def paper_hybrid_uamp(cls, **overrides: Any) -> "OracleConfig":
+        """torch_sbl/solver.py:229-280 (fields that reach the hot path)."""
+        s: dict[str, Any] = dict(
+            tol=0.0, hyper_shape=0.0, hyper_rate=0.0, noise_shape=0.0,
+            noise_rate=0.0, uamp_iteration_offset=0.0,
+            uamp_iteration_scale=0.8, uamp_damping=0.05,
+            uamp_adaptive_damping=False, uamp_polish_iterations=3,
+            uamp_polish_residual_exchange_size=12,
+            uamp_polish_evidence_margin_factor=64.0,
+            uamp_polish_fixed_budget_diagnostics=True,
+            uamp_support_false_alarm_budget=0.5,
+        )
+        s.update(overrides)
+        return cls.fast_hybrid_uamp(**s)
+
+    @classmethod
+    def stable(cls, polish_size: int = 32) -> "OracleConfig":
+        """FBME-Stable: torch_sbl_fastest_stable/profiles.py:110-115 over
+        torch_sbl/cuda_graph.py:148-154 (realtime = paper preset)."""
+        return cls.paper_hybrid_uamp(
+            uamp_polish_size=polish_size, uamp_polish_iterations=3,
+            uamp_polish_residual_exchange_size=12,
+            uamp_polish_fixed_budget_diagnostics=True,
+        )
+
+    @classmethod
+    def fastest(cls, polish_size: int = 32) -> "OracleConfig":
+        """FBME-Fast: torch_sbl_fastest_stable/profiles.py:63-70."""
+        return cls.paper_hybrid_uamp(
+            uamp_polish_size=polish_size, uamp_polish_iterations=2,
+            uamp_polish_residual_exchange_size=0,
+            uamp_polish_fixed_budget_diagnostics=False,
+        )
+
+
+# ---------------------------------------------------------------------------
+# Prefix Fourier operator (torch_sbl/operators.py)
+# ---------------------------------------------------------------------------
+
+
+def _next_smooth_length(minimum: int) -> int:
+    """operators.py:10-20."""
+    candidate = int(minimum)
+    while True:
+        r = candidate
+        for f in (2, 3, 5, 7):
+            while r % f == 0:
+                r //= f
+        if r == 1:
+            return candidate
+        candidate += 1
+
+
+class PrefixOperator:
+    """Prefix block of the unnormalised 2-D DFT (operators.py:23-160).
+
+    Coefficients are ``[B, N1*N2]`` (row-major), data ``[B, M1*M2]``.
+    """
+
+    def __init__(self, grid, sample, cdtype=np.complex64):
+        self.grid = tuple(int(v) for v in grid)
+        self.sample = tuple(int(v) for v in sample)
+        if len(self.grid) != 2 or len(self.sample) != 2:
+            raise ValueError("the oracle handles 2-D grids")
+        if any(m <= 0 or m > n for m, n in zip(self.sample, self.grid)):
+            raise ValueError("Each sample dimension must satisfy 0 < M <= N.")
+        self.cdtype = np.dtype(cdtype)
+        self.rdtype = np.float64 if self.cdtype == np.complex128 else np.float32
+        self.n_grid = prod(self.grid)
+        self.n_samples = prod(self.sample)
+        # operators.py:103-147 embedding for the BTTB (Toeplitz) matvec
+        self.embedding = tuple(_next_smooth_length(2 * m - 1) for m in self.sample)
+        pos, lag = [], []
+        for m, length, n in zip(self.sample, self.embedding, self.grid):
+            pos.append(np.concatenate([np.arange(m), np.arange(length - m + 1, length)]))
+            lag.append(np.concatenate([np.arange(m), np.arange(-(m - 1), 0)]))
+        p0, p1 = np.meshgrid(pos[0], pos[1], indexing="ij")
+        l0, l1 = np.meshgrid(lag[0], lag[1], indexing="ij")
+        self.embedding_positions = (p0 * self.embedding[1] + p1).reshape(-1)
+        self.embedding_lags = (
+            np.remainder(l0, self.grid[0]) * self.grid[1] + np.remainder(l1, self.grid[1])
+        ).reshape(-1)
+        a0, a1 = np.meshgrid(np.arange(self.sample[0]), np.arange(self.sample[1]), indexing="ij")
+        self.sample_coordinates = np.stack([a0.reshape(-1), a1.reshape(-1)], 1)
+
+    def forward_flat(self, coefficients: np.ndarray) -> np.ndarray:
+        """operators.py:237-253: fft2 then crop."""
+        b = coefficients.shape[0]
+        field = coefficients.reshape(b, *self.grid)
+        spec = np.fft.fft2(field, axes=(1, 2))
+        return spec[:, : self.sample[0], : self.sample[1]].reshape(b, self.n_samples).astype(self.cdtype)
+
+    def adjoint_flat(self, data: np.ndarray) -> np.ndarray:
+        """operators.py:255-280: N * ifft2 with end zero padding."""
+        b = data.shape[0]
+        field = data.reshape(b, *self.sample)
+        coeff = np.fft.ifft2(field, s=self.grid, axes=(1, 2)).astype(self.cdtype)
+        return (coeff * self.rdtype(self.n_grid)).reshape(b, self.n_grid)
+
+    def fourier_columns(self, flat_indices: np.ndarray) -> np.ndarray:
+        """operators.py:444-466: exp(-2*pi*i*<m, n/N>) for selected atoms.
+
+        Follows the reference's real-dtype phase arithmetic (phase formed
+        in the real dtype, then the complex exponential).
+        """
+        rd = self.rdtype
+        n1 = (flat_indices // self.grid[1]).astype(rd)
+        n2 = (flat_indices % self.grid[1]).astype(rd)
+        c = self.sample_coordinates.astype(rd) / np.array(self.grid, dtype=rd)
+        phase = c[None, :, 0:1] * n1[:, None, :] + c[None, :, 1:2] * n2[:, None, :]
+        arg = (rd(-2.0 * np.pi) * phase).astype(rd)
+        return np.exp(1j * arg).astype(self.cdtype)
+
+    def toeplitz_spectrum(self, prior: np.ndarray, noise: np.ndarray) -> np.ndarray:
+        """operators.py:299-326: BTTB embedding spectrum of
+        Q = noise*I + A diag(prior) A^H."""
+        b = prior.shape[0]
+        field = prior.astype(self.cdtype).reshape(b, *self.grid)
+        lags = np.fft.fft2(field, axes=(1, 2)).astype(self.cdtype).reshape(b, self.n_grid)
+        kernel = np.zeros((b, prod(self.embedding)), self.cdtype)
+        kernel[:, self.embedding_positions] = lags[:, self.embedding_lags]
+        kernel[:, 0] += noise
+        return np.fft.fft2(kernel.reshape(b, *self.embedding), axes=(1, 2)).astype(self.cdtype)
+
+    def toeplitz_matvec(self, data: np.ndarray, spectrum: np.ndarray) -> np.ndarray:
+        """operators.py:328-355: data [B, M, R] -> Q data."""
+        b, _, r = data.shape
+        field = data.reshape(b, *self.sample, r)
+        tr = np.fft.fft2(field, s=self.embedding, axes=(1, 2)).astype(self.cdtype)
+        prod_ = np.fft.ifft2(tr * spectrum[..., None], axes=(1, 2)).astype(self.cdtype)
+        return prod_[:, : self.sample[0], : self.sample[1], :].reshape(b, self.n_samples, r)
+
+    def adjoint(self, data: np.ndarray) -> np.ndarray:
+        """operators.py:219-235: [B, M, R] -> [B, N, R]."""
+        b, _, r = data.shape
+        field = data.reshape(b, *self.sample, r)
+        coeff = np.fft.ifft2(field, s=self.grid, axes=(1, 2)).astype(self.cdtype)
+        return (coeff * self.rdtype(self.n_grid)).reshape(b, self.n_grid, r)
+
+    def forward(self, coeff: np.ndarray) -> np.ndarray:
+        """operators.py:208-217: [B, N, R] -> [B, M, R]."""
+        b, _, r = coeff.shape
+        spec = np.fft.fft2(coeff.reshape(b, *self.grid, r), axes=(1, 2)).astype(self.cdtype)
+        return spec[:, : self.sample[0], : self.sample[1], :].reshape(b, self.n_samples, r)
+
+
+# ---------------------------------------------------------------------------
+# Small helpers
+# ---------------------------------------------------------------------------
+
+
+def _finfo(rd):
+    fi = np.finfo(rd)
+    return rd(fi.eps), rd(fi.tiny)
+
+
+def _abs2(z: np.ndarray) -> np.ndarray:
+    """``z.abs().square()`` in the real dtype of ``z``."""
+    return np.square(np.abs(z))
+
+
+def _tri_solve(lower: np.ndarray, rhs: np.ndarray, *, upper: bool = False) -> np.ndarray:
+    """Batched triangular solve (torch.linalg.solve_triangular)."""
+    out = np.empty(np.broadcast_shapes(lower.shape[:-2], rhs.shape[:-2]) + rhs.shape[-2:], rhs.dtype)
+    for i in range(out.shape[0]):
+        a = lower[i]
+        if _solve_triangular is not None:
+            out[i] = _solve_triangular(a, rhs[i], lower=not upper, check_finite=False)
+        else:  # pragma: no cover
+            out[i] = np.linalg.solve(a, rhs[i])
+    return out
+
+
+def _stable_cholesky(matrix: np.ndarray, tiny, eps, *, mode: str, multiplier: float,
+                     fallback=(1.0, 10.0, 1e2, 1e3, 1e4, 1e5)):
+    """solver.py:2898-2931 (_stable_cholesky_raw).
+
+    ``mode="cuda"``: one deterministic loading ``multiplier*eps*scale``
+    (solver.py:2910-2920).  ``mode="cpu"``: the first loading of
+    ``fallback`` that factors (solver.py:2922-2931).
+    """
+    k = matrix.shape[-1]
+    eye = np.eye(k, dtype=matrix.dtype)
+    scale = np.abs(np.real(np.diagonal(matrix, axis1=-2, axis2=-1))).mean(axis=1)
+    scale = np.maximum(scale, tiny).astype(type(eps))
+    base = eps * scale
+    mults = (multiplier,) if mode == "cuda" else fallback
+    for mlt in mults:
+        loaded = matrix + (type(eps)(mlt) * base)[:, None, None] * eye
+        try:
+            return np.linalg.cholesky(loaded)
+        except np.linalg.LinAlgError:
+            if mode == "cuda":
+                raise RuntimeError("CUDA Cholesky failed after deterministic diagonal loading.")
+    return None
+
+
+# ---------------------------------------------------------------------------
+# Reduced exact posterior with evidence (solver.py:3591-3779)
+# ---------------------------------------------------------------------------
+
+
+def active_posterior_with_evidence(y, prior, noise, op: PrefixOperator, active, *, columns,
+                                   gram, column_data, data_energy, chol_mode, chol_multiplier):
+    """solver.py:3591-3779 with tail_loading=0 and no global certificate.
+
+    Returns (mean[B,N], posterior_variance[B,N], data_diagonal[B,N], nle[B]).
+    """
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    b, k = active.shape
+    rows = np.arange(b)[:, None]
+    gamma = prior[rows, active]
+    eff_noise = noise + rd(0.0)
+    system = np.zeros((b, k, k), y.dtype)
+    system[:, np.arange(k), np.arange(k)] = (rd(1.0) / gamma).astype(y.dtype)
+    system = system + gram / eff_noise[:, None, None]
+    system = rd(0.5) * (system + np.conj(np.swapaxes(system, 1, 2)))
+    dscale = np.sqrt(np.maximum(np.real(np.diagonal(system, axis1=1, axis2=2)), tiny))
+    eq = system / dscale[:, :, None] / dscale[:, None, :]
+    eq = rd(0.5) * (eq + np.conj(np.swapaxes(eq, 1, 2)))
+    chol = _stable_cholesky(eq, tiny, eps, mode=chol_mode, multiplier=chol_multiplier)
+    if chol is None:
+        raise RuntimeError("Reduced active-set posterior is not positive definite.")
+    rhs = column_data / eff_noise[:, None, None]
+    srhs = rhs / dscale[:, :, None]
+    fwd = _tri_solve(chol, srhs)
+    eq_mean = _tri_solve(np.conj(np.swapaxes(chol, 1, 2)), fwd, upper=True)
+    inv_factor = _tri_solve(chol, np.broadcast_to(np.eye(k, dtype=y.dtype), (b, k, k)))
+    eq_var = _abs2(inv_factor).sum(axis=1)
+    a_mean = (eq_mean / dscale[:, :, None])[:, :, 0]
+    a_var = np.maximum(np.real(eq_var / np.square(dscale)), rd(0.0)).astype(rd)
+    a_dd = np.maximum((gamma - a_var) / np.square(gamma), rd(0.0))
+    logdet_sys = rd(2.0) * (
+        np.log(np.maximum(np.real(np.diagonal(chol, axis1=1, axis2=2)), tiny)).sum(axis=1)
+        + np.log(dscale).sum(axis=1)
+    )
+    logdet = rd(op.n_samples) * np.log(eff_noise) + np.log(gamma).sum(axis=1) + logdet_sys
+    quad = np.maximum(
+        data_energy / eff_noise - np.real((np.conj(rhs[:, :, 0]) * a_mean).sum(axis=1)), rd(0.0)
+    )
+    nle = (logdet + quad).astype(rd)
+    mean = np.zeros((b, op.n_grid), y.dtype)
+    pv = prior.copy()
+    dd = np.zeros_like(prior)
+    mean[rows, active] = a_mean
+    pv[rows, active] = a_var
+    dd[rows, active] = a_dd
+    return mean, pv, dd, nle
+
+
+def active_evidence_deletion_gain(a_mean, a_pv, a_gamma):
+    """solver.py:3219-3317: the ``deletion_gain`` (current_delta) field."""
+    rd = a_pv.dtype.type
+    _, tiny = _finfo(rd)
+    g = np.maximum(a_gamma, tiny)
+    q = a_mean / g
+    s = np.maximum((g - a_pv) / np.square(g), tiny)
+    down = np.clip(a_pv / g, tiny, rd(1.0))
+    return (-np.log(down) - g * _abs2(q) / down).astype(rd)
+
+
+# ---------------------------------------------------------------------------
+# UAMP sweep (solver.py:2726-2870, torch branch 2808-2850; Triton kernels
+# triton_kernels.py:37-192 compute the same expressions)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class UAMPState:
+    """solver.py:795-804."""
+
+    mean: np.ndarray
+    variance: np.ndarray
+    message: np.ndarray
+    prediction: np.ndarray
+    data_variance: np.ndarray
+
+
+def uamp_sweep(y, prior, noise, op, st: UAMPState, *, damping, initial_backprojection=None,
+               compute_prediction=True, prior_floor=None, prior_damping=0.0,
+               prior_maximum=1e12, hyper_shape=0.0, hyper_rate=0.0):
+    """One UAMP iteration.  Returns (mean, var, dof, new_state, next_prior).
+
+    ``prior_floor`` given: fused ARD update of triton_kernels.py:163-184.
+    """
+    rd = op.rdtype
+    _, tiny = _finfo(rd)
+    d = rd(damping)
+    cv = np.maximum(st.variance, tiny)
+    dv = np.maximum(st.data_variance, tiny)
+    # message (triton_kernels.py:72-89; solver.py:2810-2818)
+    precision = rd(1.0) / (dv + noise)
+    pseudo_data = st.prediction - dv[:, None] * st.message
+    cand = precision[:, None] * (y - pseudo_data)
+    message = d * st.message + (rd(1.0) - d) * cand
+    pv = np.maximum((dv + noise) / rd(op.n_samples), tiny)
+    if initial_backprojection is not None:
+        lifted = initial_backprojection * ((rd(1.0) - d) / (dv + noise))[:, None]
+    else:
+        lifted = op.adjoint_flat(message)
+    # denoise (triton_kernels.py:140-158; solver.py:2832-2850)
+    denom = np.maximum(prior + pv[:, None], tiny)
+    gain = prior / denom
+    pseudo_mean = st.mean + pv[:, None] * lifted
+    cand_mean = gain * pseudo_mean
+    cand_var = prior * pv[:, None] / denom
+    mean = d * st.mean + (rd(1.0) - d) * cand_mean
+    var = np.maximum(d * cv + (rd(1.0) - d) * cand_var, tiny)
+    dof = np.clip(rd(1.0) - var / np.maximum(prior, tiny), 0, 1).sum(axis=1, dtype=rd)
+    next_dv = var.sum(axis=1, dtype=rd)
+    next_prior = None
+    if prior_floor is not None:
+        # triton_kernels.py:163-184 (== solver.py:1630-1648 + 1783-1787)
+        second = _abs2(mean) + var
+        cp = (second + rd(hyper_rate)) / rd(1.0 + hyper_shape)
+        cp = np.maximum(prior_floor[:, None], np.minimum(rd(prior_maximum), cp))
+        nxt = rd(prior_damping) * prior + rd(1.0 - prior_damping) * cp
+        next_prior = np.maximum(nxt, prior_floor[:, None])
+    prediction = op.forward_flat(mean) if compute_prediction else st.prediction
+    return mean, var, dof, UAMPState(mean, var, message, prediction, next_dv), next_prior
+
+
+# ---------------------------------------------------------------------------
+# fast_sbl, mode="uamp" (solver.py:925-2393, plan-relevant branches)
+# ---------------------------------------------------------------------------
+
+
+def _uamp_iteration_limit(cfg: OracleConfig, n_grid: int, n_samples: int) -> int:
+    """solver.py:1287-1309."""
+    minimum = max(cfg.min_iter, cfg.uamp_min_iter)
+    limit = cfg.max_iter
+    if cfg.uamp_auto_iterations:
+        budget = ceil(cfg.uamp_iteration_offset + cfg.uamp_iteration_scale * n_grid / n_samples)
+        limit = min(cfg.max_iter, max(minimum, budget))
+    return limit
+
+
+def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str = "cuda"):
+    """Restatement of ``fast_sbl`` for ``mode="uamp"`` with the polish.
+
+    ``data`` is ``[M1, M2]`` or ``[B, M1, M2]``.  Returns a dict of the
+    ``SBLResult`` fields the FBME plans fill (solver.py:2154-2393).
+    """
+    data = np.asarray(data)
+    cdtype = np.complex128 if data.dtype in (np.complex128, np.float64) else np.complex64
+    single = data.ndim == 2
+    y3 = data[None] if single else data
+    b = y3.shape[0]
+    sample = y3.shape[1:]
+    op = PrefixOperator(grid, sample, cdtype)
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    y = y3.reshape(b, op.n_samples).astype(cdtype)
+    n, m = op.n_grid, op.n_samples
+    if cfg.uamp_support_false_alarm_budget is not None and cfg.uamp_support_false_alarm_budget >= n:
+        raise ValueError("uamp_support_false_alarm_budget must be smaller than the grid size.")
+
+    # initialisation (solver.py:1063-1099, 1151-1182)
+    data_power = np.maximum(_abs2(y).mean(axis=1, dtype=rd), eps).astype(rd)
+    variance_floor = np.maximum(data_power * rd(cfg.min_variance), tiny).astype(rd)
+    uniform = data_power[:, None] / rd(n)
+    initial_bp = None
+    if cfg.initialization == "backprojection":
+        bp = op.adjoint_flat(y)
+        initial_bp = bp
+        e = _abs2(bp)
+        structured = e / np.maximum(e.sum(axis=1, keepdims=True, dtype=rd), eps) * data_power[:, None]
+        prior = rd(cfg.initialization_blend) * structured + rd(1.0 - cfg.initialization_blend) * uniform
+    else:
+        prior = np.broadcast_to(uniform, (b, n)).copy()
+    prior_floor = variance_floor
+    prior = np.maximum(prior, prior_floor[:, None]).astype(rd)
+    if cfg.fixed_noise_variance is None:
+        noise = np.maximum(rd(cfg.initial_noise_fraction) * data_power, variance_floor).astype(rd)
+    else:
+        noise = np.full(b, cfg.fixed_noise_variance, rd)
+    st = UAMPState(np.zeros((b, n), cdtype), prior.copy(), np.zeros((b, m), cdtype),
+                   np.zeros((b, m), cdtype), prior.sum(axis=1, dtype=rd))
+    damping = cfg.uamp_damping
+    if cfg.uamp_adaptive_damping:
+        damping = max(damping, min(cfg.uamp_max_damping, 0.02 * n / m))
+    limit = _uamp_iteration_limit(cfg, n, m)
+    keep = rd(cfg.damping)
+
+    # EM loop (solver.py:1315-1798 for mode="uamp", fused Triton updates)
+    for it in range(1, limit + 1):
+        mean, var, dof_u, st, next_prior = uamp_sweep(
+            y, prior, noise, op, st, damping=damping,
+            initial_backprojection=initial_bp if it == 1 else None,
+            prior_floor=prior_floor, prior_damping=cfg.damping,
+            prior_maximum=cfg.max_precision, hyper_shape=cfg.hyper_shape,
+            hyper_rate=cfg.hyper_rate)
+        dof = np.minimum(dof_u, rd(m * (1.0 - 10.0 * float(eps))))
+        new_prior = next_prior
+        # noise update (triton_kernels.py:298-318; solver.py:1751-1768)
+        if cfg.fixed_noise_variance is None:
+            energy = _abs2(y - st.prediction).sum(axis=1, dtype=rd)
+            if cfg.noise_update == "em":
+                cand = (energy + noise * dof + rd(cfg.noise_rate)) / rd(m + cfg.noise_shape)
+            else:
+                cand = (energy + rd(cfg.noise_rate)) / np.maximum(rd(m) - dof + rd(cfg.noise_shape), eps)
+            cand = np.maximum(cand, variance_floor)
+            new_noise = keep * noise + (rd(1.0) - keep) * cand
+            new_noise = np.maximum(new_noise, variance_floor)
+            noise = new_noise.astype(rd)
+        prior = np.maximum(new_prior, prior_floor[:, None]).astype(rd)
+
+    # final E-step (solver.py:1907-1925)
+    mean, var, dof_u, st, _ = uamp_sweep(y, prior, noise, op, st, damping=damping,
+                                         compute_prediction=False)
+    out: dict[str, Any] = {}
+    if cfg.uamp_polish_size > 0:
+        k = min(cfg.uamp_polish_size, n)
+        score = _abs2(mean) + var
+        active = _topk_indices(score, k)
+        out["uamp_active_indices"] = active.copy()
+        out["uamp_score"] = score
+        pol = uamp_active_em_polish(y, mean, var, prior, noise, op, active, prior_floor, cfg,
+                                    chol_mode=chol_mode)
+        mean, var, dd, prior, noise = pol["mean"], pol["pv"], pol["dd"], pol["prior"], pol["noise"]
+        out.update({kk: v for kk, v in pol.items() if kk not in ("mean", "pv", "dd", "prior", "noise")})
+        if cfg.uamp_polish_fixed_budget_diagnostics:
+            gres, nres = fixed_budget_em_residuals(y, mean, var, prior, noise, pol["active_indices"],
+                                                   prior_floor, op, cfg)
+            trace = pol["evidence_trace"]
+            finite = np.isfinite(trace).all(axis=1)
+            nonincreasing = (trace[:, 1:] <= trace[:, :-1]).all(axis=1)
+            out["fixed_budget_gamma_residual"] = gres
+            out["fixed_budget_noise_residual"] = nres
+            out["fixed_budget_monotone"] = finite & nonincreasing
+            out["fixed_budget_objective_decrease"] = np.maximum(trace[:, 0] - trace[:, -1], rd(0.0))
+        # effective DOF from the exact posterior (solver.py:2081-2092, 3156-3181)
+        rel = np.clip(prior * dd, 0, 1)
+        raw = rel.sum(axis=1, dtype=rd)
+        max_dof = rd(m * (1.0 - 10.0 * float(eps)))
+        scale = np.minimum(rd(1.0), max_dof / np.maximum(raw, eps))
+        dof = (rel * scale[:, None]).sum(axis=1, dtype=rd)
+    else:
+        dof = np.minimum(dof_u, rd(m * (1.0 - 10.0 * float(eps))))
+    precision = (rd(1.0) / prior).astype(rd)
+    # support mask (solver.py:2108-2126)
+    if cfg.uamp_support_false_alarm_budget is not None:
+        thr = rd(log(n / cfg.uamp_support_false_alarm_budget))
+        sscore = _abs2(mean) / np.maximum(var, tiny)
+        out["support_mask"] = (sscore > thr).reshape((-1,) + tuple(grid))
+        out["support_score_threshold"] = np.full(b, thr, rd)
+    shape = tuple(grid)
+    out.update(
+        x=mean.reshape((b,) + shape), posterior_variance=var.reshape((b,) + shape),
+        precision=precision.reshape((b,) + shape), noise_variance=noise, effective_dof=dof,
+        iterations=limit, mode="uamp", arithmetic_dtype=str(np.dtype(cdtype)),
+        active_set_size=(min(cfg.uamp_polish_size, n) if cfg.uamp_polish_size > 0 else 0),
+    )
+    if single:
+        for key, val in list(out.items()):
+            if isinstance(val, np.ndarray) and val.ndim >= 1 and val.shape[0] == 1 and key not in (
+                    "evidence_trace", "penalized_evidence_trace"):
+                out[key] = val[0]
+    return out
+
+
+def _topk_indices(score: np.ndarray, k: int) -> np.ndarray:
+    """``torch.topk(score, k).indices``: descending, ties by lower index."""
+    order = np.argsort(-score, axis=1, kind="stable")
+    return order[:, :k].astype(np.int64)
+
+
+def uamp_active_em_polish(y, uamp_mean, uamp_var, prior, noise, op, active, prior_floor,
+                          cfg: OracleConfig, *, chol_mode="cuda"):
+    """solver.py:3961-4510 (branches reachable from the FBME plans)."""
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    b, k = active.shape
+    rows = np.arange(b)[:, None]
+    m = op.n_samples
+    # prune + reinitialise (4079-4106)
+    working = prior.copy()
+    if cfg.uamp_polish_prune_tail:
+        working = np.broadcast_to(prior_floor[:, None], prior.shape).copy()
+        working[rows, active] = prior[rows, active]
+    if cfg.uamp_polish_reinitialize:
+        second = _abs2(uamp_mean) + uamp_var
+        working[rows, active] = np.maximum(second[rows, active], prior_floor[:, None])
+    columns = op.fourier_columns(active)
+    gram = np.conj(np.swapaxes(columns, 1, 2)) @ columns
+    column_data = np.conj(np.swapaxes(columns, 1, 2)) @ y[:, :, None]
+    data_energy = _abs2(y).sum(axis=1, dtype=rd)
+    active_noise = noise.copy()
+    best = None
+    accepted = []
+    pending = None
+    exch_acc = np.zeros(b, np.int64) if cfg.uamp_polish_residual_exchange_size > 0 else None
+    mean = uamp_mean
+    pv = uamp_var
+    for p in range(cfg.uamp_polish_iterations):
+        c_mean, c_pv, c_dd, c_nle = active_posterior_with_evidence(
+            y, working, active_noise, op, active, columns=columns, gram=gram,
+            column_data=column_data, data_energy=data_energy, chol_mode=chol_mode,
+            chol_multiplier=cfg.cuda_cholesky_jitter_multiplier)
+        cand = dict(mean=c_mean, pv=c_pv, dd=c_dd, prior=working, noise=active_noise, nle=c_nle,
+                    active=active, columns=columns, gram=gram, column_data=column_data)
+        if cfg.uamp_polish_evidence_gate:
+            if best is None:
+                best = {kk: (v.copy() if isinstance(v, np.ndarray) else v) for kk, v in cand.items()}
+            else:
+                margin = rd(cfg.uamp_polish_evidence_margin_factor) * eps * (
+                    rd(1.0) + np.abs(c_nle) + np.abs(best["nle"]))
+                accept = np.isfinite(c_nle) & (~np.isfinite(best["nle"]) | (c_nle <= best["nle"] - margin))
+                for key, val in cand.items():
+                    mask = accept.reshape((b,) + (1,) * (np.ndim(val) - 1))
+                    best[key] = np.where(mask, val, best[key])
+                if pending is not None and exch_acc is not None:
+                    exch_acc = exch_acc + (accept & pending).astype(np.int64)
+                    pending = None
+            cur = best
+        else:
+            cur = cand
+        accepted.append(cur["nle"].copy())
+        mean, pv, base_prior, base_noise = cur["mean"], cur["pv"], cur["prior"], cur["noise"]
+        active, columns, gram, column_data = cur["active"], cur["columns"], cur["gram"], cur["column_data"]
+        if p + 1 == cfg.uamp_polish_iterations:
+            break
+        # EM between evaluations (4320-4391)
+        a_gamma = base_prior[rows, active]
+        a_pv = pv[rows, active]
+        a_mean = mean[rows, active]
+        new_g = np.minimum(np.maximum(_abs2(a_mean) + a_pv, prior_floor[:, None]), rd(cfg.max_precision))
+        keep = rd(cfg.uamp_polish_damping)
+        upd_g = keep * a_gamma + (rd(1.0) - keep) * new_g
+        prediction = (columns @ a_mean[:, :, None])[:, :, 0]
+        residual = y - prediction
+        r_energy = _abs2(residual).sum(axis=1, dtype=rd)
+        eff_noise = base_noise
+        dof = np.clip(rd(1.0) - a_pv / np.maximum(a_gamma, tiny), 0, 1).sum(axis=1, dtype=rd)
+        if cfg.fixed_noise_variance is not None:
+            upd_noise = np.full(b, cfg.fixed_noise_variance, rd)
+        elif cfg.noise_update == "em":
+            upd_noise = (r_energy + eff_noise * dof + rd(cfg.noise_rate)) / rd(m + cfg.noise_shape)
+        else:
+            upd_noise = (r_energy + rd(cfg.noise_rate)) / np.maximum(rd(m) - dof + rd(cfg.noise_shape), eps)
+        upd_noise = np.maximum(upd_noise, prior_floor)
+        if cfg.fixed_noise_variance is None:
+            active_noise = (keep * base_noise + (rd(1.0) - keep) * upd_noise).astype(rd)
+        else:
+            active_noise = upd_noise.astype(rd)
+        working = base_prior.copy()
+        working[rows, active] = upd_g
+        ex = min(cfg.uamp_polish_residual_exchange_size, max(k - 1, 0), op.n_grid - k)
+        if ex > 0 and p == 0:
+            # residual support exchange (4397-4494)
+            rscore = _abs2(op.adjoint_flat(residual))
+            rscore[rows, active] = -np.inf
+            add_idx = _topk_indices(rscore, ex)
+            add_energy = rscore[rows, add_idx]
+            deletion = active_evidence_deletion_gain(a_mean, a_pv, a_gamma)
+            rem_pos = _topk_indices(deletion, ex)
+            rem_idx = active[rows, rem_pos]
+            ce = rd(float(m))
+            ratio = add_energy / np.maximum(base_noise[:, None] * ce, tiny)
+            add_gain = np.where(ratio > 1.0, ratio - rd(1.0) - np.log(np.maximum(ratio, tiny)), rd(0.0))
+            del_gain = deletion[rows, rem_pos]
+            xmask = (add_gain + del_gain) > 0.0
+            repl = np.where(xmask, add_idx, rem_idx)
+            new_active = active.copy()
+            new_active[rows, rem_pos] = repl
+            add_gamma = np.maximum(add_energy - base_noise[:, None] * ce, rd(0.0)) / (ce * ce)
+            add_gamma = np.minimum(np.maximum(add_gamma, prior_floor[:, None]), rd(cfg.max_precision))
+            retained = working[rows, rem_idx]
+            working[rows, rem_idx] = np.where(xmask, prior_floor[:, None], retained)
+            working[rows, repl] = np.where(xmask, add_gamma, retained)
+            active = new_active
+            columns = op.fourier_columns(active)
+            gram = np.conj(np.swapaxes(columns, 1, 2)) @ columns
+            column_data = np.conj(np.swapaxes(columns, 1, 2)) @ y[:, :, None]
+            pending = xmask.any(axis=1)
+            out_ex = dict(add_idx=add_idx, rem_pos=rem_pos, xmask=xmask)
+    fin = best if cfg.uamp_polish_evidence_gate else cand
+    trace = np.stack(accepted, axis=1)
+    res = dict(
+        mean=mean, pv=pv, dd=cur["dd"], prior=fin["prior"], noise=fin["noise"],
+        negative_log_evidence=fin["nle"], evidence_trace=trace,
+        penalized_negative_log_evidence=fin["nle"].copy(), penalized_evidence_trace=trace.copy(),
+        support_log_odds_penalty=np.zeros(b, rd), hard_pruning_accepted=np.zeros(b, bool),
+        truncation_certified=np.zeros(b, bool),
+        active_model_selected=np.full(b, bool(cfg.uamp_polish_prune_tail)),
+        active_indices=fin["active"],
+    )
+    if exch_acc is not None:
+        res["support_repairs_accepted"] = exch_acc
+        res["support_exchanges_accepted"] = exch_acc.copy()
+    return res
+
+
+def fixed_budget_em_residuals(y, mean, pv, prior, noise, active, prior_floor, op, cfg):
+    """solver.py:3408-3496."""
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    b = y.shape[0]
+    rows = np.arange(b)[:, None]
+    ag = np.maximum(prior[rows, active], tiny)
+    ap = pv[rows, active]
+    am = mean[rows, active]
+    gt = (_abs2(am) + ap + rd(cfg.hyper_rate)) / rd(1.0 + cfg.hyper_shape)
+    gt = np.minimum(np.maximum(gt, prior_floor[:, None]), rd(cfg.max_precision))
+    gs = np.maximum(np.maximum(np.abs(ag), np.abs(gt)), tiny)
+    gres = (np.abs(ag - gt) / gs).max(axis=1)
+    if cfg.fixed_noise_variance is not None:
+        return gres, np.zeros_like(noise)
+    dof = np.clip(rd(1.0) - ap / ag, 0, 1).sum(axis=1, dtype=rd)
+    cols = op.fourier_columns(active)
+    pred = (cols @ am[:, :, None])[:, :, 0]
+    energy = _abs2(y - pred).sum(axis=1, dtype=rd)
+    m = op.n_samples
+    if cfg.noise_update == "em":
+        nt = (energy + noise * dof + rd(cfg.noise_rate)) / rd(m + cfg.noise_shape)
+    else:
+        nt = (energy + rd(cfg.noise_rate)) / np.maximum(rd(m) - dof + rd(cfg.noise_shape), eps)
+    nt = np.minimum(np.maximum(nt, prior_floor), rd(cfg.max_precision))
+    ns = np.maximum(np.maximum(np.abs(noise), np.abs(nt)), tiny)
+    return gres.astype(rd), (np.abs(noise - nt) / ns).astype(rd)
+
+
+def fbme_solve(data, grid, profile: str = "stable", *, polish_size: int = 32,
+               chol_mode: str = "cuda"):
+    """The FBME-Fast / FBME-Stable plan replay (profiles.py:35-148)."""
+    cfg = OracleConfig.stable(polish_size) if profile == "stable" else OracleConfig.fastest(polish_size)
+    return fast_sbl_uamp(data, grid, cfg, chol_mode=chol_mode)
