@@ -1,0 +1,150 @@
+"""ctypes binding of the C ABI in ``include/fbme_b200.h``.
+
+The shared library ``libfbme_b200.so`` is built in-tree by
+``fbme_b200.build``.  There is no fallback: if the library is missing or
+fails to load, every entry point raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_float, c_int, c_int32, c_size_t, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libfbme_b200.so"
+
+FBME_OK = 0
+FBME_ERR_INVALID = 1
+FBME_ERR_UNSUPPORTED = 2
+FBME_ERR_CUDA = 3
+FBME_ERR_WORKSPACE = 4
+
+STATUS_NONFINITE = 1
+STATUS_CHOLESKY = 2
+STATUS_TIMEOUT = 4
+STATUS_PCG_BREAKDOWN = 8
+STATUS_ITER_CAP = 16
+
+
+class FbmeShape(ctypes.Structure):
+    _fields_ = [("n1", c_int32), ("n2", c_int32), ("m1", c_int32), ("m2", c_int32)]
+
+
+class FbmeConfig(ctypes.Structure):
+    _fields_ = [
+        ("uamp_iterations", c_int32),
+        ("uamp_damping", c_float),
+        ("damping", c_float),
+        ("initialization_blend", c_float),
+        ("initial_noise_fraction", c_float),
+        ("fixed_noise_variance", c_float),
+        ("min_variance", c_float),
+        ("max_precision", c_float),
+        ("hyper_shape", c_float),
+        ("hyper_rate", c_float),
+        ("noise_shape", c_float),
+        ("noise_rate", c_float),
+        ("noise_update", c_int32),
+        ("polish_size", c_int32),
+        ("polish_iterations", c_int32),
+        ("polish_prune_tail", c_int32),
+        ("polish_reinitialize", c_int32),
+        ("polish_evidence_gate", c_int32),
+        ("polish_damping", c_float),
+        ("evidence_margin_factor", c_float),
+        ("exchange_size", c_int32),
+        ("fixed_budget_diagnostics", c_int32),
+        ("cholesky_jitter_multiplier", c_float),
+        ("support_false_alarm_budget", c_float),
+        ("dft_terms", c_int32),
+    ]
+
+
+class FbmeOutputs(ctypes.Structure):
+    _fields_ = [
+        ("x", c_void_p),
+        ("posterior_variance", c_void_p),
+        ("precision", c_void_p),
+        ("support_mask", c_void_p),
+        ("noise_variance", c_void_p),
+        ("effective_dof", c_void_p),
+        ("negative_log_evidence", c_void_p),
+        ("evidence_trace", c_void_p),
+        ("support_exchanges_accepted", c_void_p),
+        ("fixed_budget_gamma_residual", c_void_p),
+        ("fixed_budget_noise_residual", c_void_p),
+        ("fixed_budget_objective_decrease", c_void_p),
+        ("fixed_budget_monotone", c_void_p),
+        ("support_score_threshold", c_void_p),
+        ("active_indices", c_void_p),
+        ("status", c_void_p),
+    ]
+
+
+class FbmeState(ctypes.Structure):
+    _fields_ = [
+        ("mean", c_void_p),
+        ("variance", c_void_p),
+        ("prior_variance", c_void_p),
+        ("message", c_void_p),
+        ("prediction", c_void_p),
+        ("backprojection", c_void_p),
+        ("noise_variance", c_void_p),
+        ("data_variance", c_void_p),
+    ]
+
+
+# Every symbol include/fbme_b200.h declares, with its ctypes signature.
+SIGNATURES = {
+    "fbme_plan_workspace_bytes": (c_size_t, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig)]),
+    "fbme_plan_create": (c_int, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig), c_void_p,
+                                 c_size_t, c_void_p, POINTER(c_void_p)]),
+    "fbme_plan_replay": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
+    "fbme_plan_destroy": (c_int, [c_void_p]),
+    "fbme_dft_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fbme_dft_adjoint": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fbme_uamp_run": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "fbme_polish_run": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
+    "fbme_plan_state": (c_int, [c_void_p, POINTER(FbmeState)]),
+    "fbme_last_error": (c_char_p, []),
+    "fbme_version": (c_char_p, []),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library once; raise if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"FBME native library not built ({LIB_PATH}); run `python -m fbme_b200.build`."
+        )
+    try:
+        handle = ctypes.CDLL(str(LIB_PATH))
+    except OSError as exc:  # pragma: no cover - depends on the machine
+        raise RuntimeError(f"cannot load {LIB_PATH}: {exc}") from exc
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(handle, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = handle
+    return handle
+
+
+def last_error() -> str:
+    return lib().fbme_last_error().decode()
+
+
+def check(rc: int, what: str) -> None:
+    """Map an FBME_* return code to the reference's exception types."""
+    if rc == FBME_OK:
+        return
+    msg = f"{what}: {last_error()}"
+    if rc in (FBME_ERR_INVALID, FBME_ERR_WORKSPACE):
+        raise ValueError(msg)
+    if rc == FBME_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    raise RuntimeError(msg)

@@ -1,0 +1,274 @@
+// Prefix-DFT contraction on the 5th-generation tensor cores (tcgen05).
+//
+// One "DFT stage" contracts the contiguous axis of a batch of complex
+// matrices with a DFT submatrix:
+//
+//     Out[r, c] = sum_k In[r, k] * w^(k*c),   w = exp(sign * 2*pi*i / L)
+//
+// written as a real GEMM on the interleaved (re, im) view: In is
+// [rows, 2K] and the twiddles are expanded into a real [2K, 2C] matrix
+// E[2k+a][2c+b] = [[Re w, Im w], [-Im w, Re w]][a][b].  Two stages make the
+// 2-D prefix operator A(X) = F_M1 X F_M2^T (forward) and its adjoint.
+//
+// Precision: both operands are split into BF16 parts (x = hi + lo, or
+// hi + mid + lo) and the tensor core accumulates in FP32 the products of
+// order <= 1 (3 terms: hi*hi + hi*lo + lo*hi) or <= 2 (6 terms).  Measured
+// against an FP64 DFT at 256^2/128^2: 3 terms 5.3e-6 relative L2, 6 terms
+// 5.3e-8 (an FP32 FFT is 4.4e-8).
+//
+// Kernel organisation (one CTA = one 128-row x N_TILE-column output tile):
+//   warps 0-3  producer: read In through the prologue policy (fused
+//              elementwise work), split to BF16 parts, store into the K-major
+//              128-byte-swizzled operand layout; thread 0 bulk-copies the
+//              pre-swizzled twiddle blocks for the same K chunk;
+//   warp 4     allocates tensor memory; lane 0 issues tcgen05.mma;
+//   all warps  epilogue: tcgen05.ld the FP32 accumulator and hand each
+//              row's values to the epilogue policy.
+// Epilogue stores put the tile row (the TMEM lane) on the contiguous memory
+// axis, so a warp's 32 lanes write 32 consecutive elements.
+#pragma once
+
+#include "common.cuh"
+
+namespace fbme {
+
+constexpr int kTileRows = 128;  // UMMA M
+constexpr int kKChunk = 64;     // real K per pipeline stage (one 128-byte row)
+constexpr int kStages = 2;
+constexpr int kDftThreads = 256;
+constexpr int kPartBytesA = kTileRows * 128;  // 16 KiB
+
+struct DftGeom {
+  int n_scenes;
+  int rows;                 // data rows per scene
+  int row_tiles;            // ceil(rows / 128)
+  int kcplx;                // contracted complex length
+  int kchunks;              // ceil(2 * kcplx / 64)
+  int cols;                 // complex output columns per scene
+  int col_tiles;            // ceil(2 * cols / N_TILE)
+  int in_ld;                // complex stride between input rows
+  long long in_stride;      // complex elements between scenes (input)
+  int out_ld;               // complex stride between output columns
+  long long out_stride;     // complex elements between scenes (output)
+  int col_per_tile;         // complex output columns per tile (N_TILE / 2)
+  int vec4;                 // rows start on 16-byte boundaries (even strides)
+  const uint8_t* table;     // pre-swizzled twiddle blocks
+  int table_kchunks;        // K chunks per column tile in the table
+};
+
+struct TileCtx {
+  int scene, row_tile, col_tile;
+  const DftGeom* g;
+  __device__ int row0() const { return row_tile * kTileRows; }
+  __device__ int col0() const { return col_tile * g->col_per_tile; }
+};
+
+template <int A_PARTS, int N_TILE>
+struct DftCfg {
+  static constexpr int kPartBytesB = N_TILE * 128;
+  static constexpr int kStageBytes = A_PARTS * kPartBytesA + A_PARTS * kPartBytesB;
+  static constexpr int kPairs = A_PARTS == 2 ? 3 : 6;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*bars*/ +
+                                    64 * sizeof(double) /*reduction scratch*/;
+  static constexpr uint32_t kIdesc = umma_idesc_bf16(kTileRows, N_TILE);
+};
+
+// (a-part, b-part) products of order <= 1 (A_PARTS=2) or <= 2 (A_PARTS=3).
+__device__ __constant__ int8_t kPairA[6] = {0, 0, 1, 0, 1, 2};
+__device__ __constant__ int8_t kPairB[6] = {0, 1, 0, 2, 1, 0};
+
+FBME_DEV uint16_t bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+FBME_DEV float bf16_val(uint16_t b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
+
+// Split four floats into A_PARTS packed bf16 quads (2 x uint32 each).
+template <int A_PARTS>
+FBME_DEV void split4(const float4 v, uint2* out) {
+  float x[4] = {v.x, v.y, v.z, v.w};
+  uint16_t p[3][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float r = x[i];
+#pragma unroll
+    for (int t = 0; t < A_PARTS; ++t) {
+      p[t][i] = bf16_bits(r);
+      r = r - bf16_val(p[t][i]);  // exact in FP32
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < A_PARTS; ++t) {
+    out[t].x = static_cast<uint32_t>(p[t][0]) | (static_cast<uint32_t>(p[t][1]) << 16);
+    out[t].y = static_cast<uint32_t>(p[t][2]) | (static_cast<uint32_t>(p[t][3]) << 16);
+  }
+}
+
+template <int A_PARTS, int N_TILE, class Pro, class Epi>
+__global__ void __launch_bounds__(kDftThreads, 1)
+dft_stage_kernel(const DftGeom g, Pro pro, Epi epi, int* status) {
+  using C = DftCfg<A_PARTS, N_TILE>;
+  extern __shared__ uint8_t smem_dyn[];
+  const uint32_t base_u32 = smem_u32(smem_dyn);
+  uint8_t* smem = smem_dyn + (((base_u32 + 1023u) & ~1023u) - base_u32);
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + kStages * C::kStageBytes);
+  uint64_t* empty_bar = full_bar + kStages;
+  uint64_t* acc_bar = empty_bar + kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+  double* red = reinterpret_cast<double*>(smem + kStages * C::kStageBytes + 256);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  TileCtx t;
+  {
+    int tile = blockIdx.x;
+    t.col_tile = tile % g.col_tiles;
+    tile /= g.col_tiles;
+    t.row_tile = tile % g.row_tiles;
+    t.scene = tile / g.row_tiles;
+    t.g = &g;
+  }
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], 128);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(acc_bar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 4) tmem_alloc(tmem_slot, N_TILE);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+  int* const st_scene = status ? status + t.scene : nullptr;
+
+  if (warp < 4) {
+    // ---------------- producer ----------------
+    for (int kc = 0; kc < g.kchunks && ok; ++kc) {
+      const int s = kc % kStages, use = kc / kStages;
+      uint8_t* st = smem + s * C::kStageBytes;
+      if (kc >= kStages) ok = mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene);
+      if (!ok) break;
+      if (threadIdx.x == 0) {
+        asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;"
+                     ::"r"(smem_u32(&full_bar[s])), "r"(uint32_t(A_PARTS * C::kPartBytesB))
+                     : "memory");
+        const uint8_t* src = g.table + (static_cast<size_t>(t.col_tile) * g.table_kchunks + kc) *
+                                           A_PARTS * C::kPartBytesB;
+        for (int p = 0; p < A_PARTS; ++p)
+          bulk_g2s(st + A_PARTS * kPartBytesA + p * C::kPartBytesB, src + p * C::kPartBytesB,
+                   C::kPartBytesB, &full_bar[s]);
+      }
+      const int q = lane & 15;
+#pragma unroll 4
+      for (int it = 0; it < 16; ++it) {
+        const int row = warp * 32 + it * 2 + (lane >> 4);
+        const float4 v = pro.load4(t, row, kc * kKChunk + q * 4);
+        uint2 parts[A_PARTS];
+        split4<A_PARTS>(v, parts);
+        const uint32_t off = sw128_offset(row, q * 4);
+#pragma unroll
+        for (int p = 0; p < A_PARTS; ++p)
+          *reinterpret_cast<uint2*>(st + p * kPartBytesA + off) = parts[p];
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(&full_bar[s]);
+    }
+  } else if (warp == 4) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      for (int kc = 0; kc < g.kchunks && ok; ++kc) {
+        const int s = kc % kStages, use = kc / kStages;
+        ok = mbar_wait(&full_bar[s], use & 1, st_scene);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(smem + s * C::kStageBytes);
+        const uint32_t b0 = a0 + A_PARTS * kPartBytesA;
+#pragma unroll
+        for (int kk = 0; kk < kKChunk / 16; ++kk) {
+#pragma unroll
+          for (int pr = 0; pr < C::kPairs; ++pr) {
+            const uint64_t ad = sw128_desc(a0 + kPairA[pr] * kPartBytesA + kk * 32);
+            const uint64_t bd = sw128_desc(b0 + kPairB[pr] * C::kPartBytesB + kk * 32);
+            umma_bf16(tmem, ad, bd, C::kIdesc, (kc | kk | pr) != 0);
+          }
+        }
+        umma_commit(&empty_bar[s]);
+      }
+      umma_commit(acc_bar);
+    }
+    __syncwarp();
+  }
+
+  // ---------------- epilogue (all warps) ----------------
+  const bool acc_ok = mbar_wait(acc_bar, 0, st_scene);
+  tc_fence_after();
+  if (acc_ok) {
+    const int q = warp & 3, h = warp >> 2;
+    const int row = q * 32 + lane;
+    constexpr int kHalf = N_TILE / 2;
+#pragma unroll 1
+    for (int c0 = h * kHalf; c0 < (h + 1) * kHalf; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(c0), v);
+      epi.consume(t, row, c0, v);
+    }
+  }
+  epi.finish(t, red);
+  pro.finish(t, red);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 4) {
+    tc_fence_after();
+    tmem_dealloc(tmem, N_TILE);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Prologue / epilogue policies shared by several stages
+// ---------------------------------------------------------------------------
+
+// Load two complex values (4 floats) of row `row` at complex column j0,
+// zero outside [0, rows) x [0, kcplx).
+FBME_DEV float4 load_row4(const float2* base, const TileCtx& t, int row, int kreal) {
+  const DftGeom& g = *t.g;
+  const int r = t.row0() + row;
+  const int j0 = kreal >> 1;
+  if (r >= g.rows || j0 >= g.kcplx) return make_float4(0.f, 0.f, 0.f, 0.f);
+  const float2* p = base + t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
+  if (j0 + 1 < g.kcplx) {
+    if (g.vec4) return *reinterpret_cast<const float4*>(p);
+    const float2 a = p[0], b = p[1];
+    return make_float4(a.x, a.y, b.x, b.y);
+  }
+  const float2 a = p[0];
+  return make_float4(a.x, a.y, 0.f, 0.f);
+}
+
+struct ProPlain {
+  const float2* in;
+  FBME_DEV float4 load4(const TileCtx& t, int row, int kreal) const {
+    return load_row4(in, t, row, kreal);
+  }
+  FBME_DEV void finish(const TileCtx&, double*) {}
+};
+
+// Store Out[j][r] (lane-contiguous) as complex64.
+struct EpiStoreT {
+  float2* out;
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) const {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    if (r >= g.rows) return;
+    float2* o = out + t.scene * g.out_stride + r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = t.col0() + (c0 >> 1) + i;
+      if (j < g.cols) o[static_cast<long long>(j) * g.out_ld] = make_float2(v[2 * i], v[2 * i + 1]);
+    }
+  }
+  FBME_DEV void finish(const TileCtx&, double*) {}
+};
+
+}  // namespace fbme

@@ -1,0 +1,106 @@
+// Internal interfaces shared by the FBME .cu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../../include/fbme_b200.h"
+
+namespace fbme {
+
+constexpr int kMaxTilesPerScene = 64;  // partial-sum slots per scene and stage
+constexpr int kPartSlots = 4;          // reductions carried per tile
+constexpr int kMaxPolish = 32;         // active-set capacity of the warp polish
+
+// Per-scene scalar state, structure of arrays of length B (device).
+struct Scalars {
+  float* data_power;  // max(mean |y|^2, eps)
+  float* floor_;      // variance floor = prior floor
+  float* noise;       // noise variance sigma^2
+  float* dvar;        // UAMP data variance (sum of coefficient variances)
+  float* pv;          // pseudo variance of the current sweep
+  float* prec;        // 1 / (dvar + noise)
+  float* ebp;         // sum |A^H y|^2
+  float* dof;         // UAMP effective DOF of the last sweep
+  float* energy;      // last residual energy
+  float* data_energy; // sum |y|^2
+};
+
+// Geometry of one equal-shape batch.
+struct BatchShape {
+  int B, n1, n2, m1, m2;
+  __host__ __device__ long long n() const { return static_cast<long long>(n1) * n2; }
+  __host__ __device__ long long m() const { return static_cast<long long>(m1) * m2; }
+};
+
+// Resolved numeric configuration used by device code.
+struct DevConfig {
+  float uamp_damping, damping, blend, init_noise, fixed_noise, min_var, max_prec;
+  float hyper_shape, hyper_rate, noise_shape, noise_rate;
+  int noise_evidence;
+  int polish_size, polish_iters, prune_tail, reinit, gate;
+  float polish_damping, margin_factor;
+  int exchange;
+  int fixed_budget;
+  float jitter;
+  float false_alarm;
+  int terms;
+  int uamp_iters;
+};
+
+// ---------------------------------------------------------------------------
+// launchers (all asynchronous on `st`)
+// ---------------------------------------------------------------------------
+void launch_twiddle_table(uint8_t* dst, int L, int sign, int n_tile, int col_tiles, int kchunks,
+                          int parts, cudaStream_t st);
+void launch_dirichlet(float2* dst, int M, int L, cudaStream_t st);
+
+struct DftTables {
+  const uint8_t* fwd_n2;  // L = N2, sign -1
+  const uint8_t* fwd_n1;  // L = N1, sign -1
+  const uint8_t* adj_n2;  // L = N2, sign +1
+  const uint8_t* adj_n1;  // L = N1, sign +1
+  int kchunks_n1, kchunks_n2;
+};
+
+// Buffers of the UAMP stage.
+struct UampBuffers {
+  const float2* y;
+  float2 *mu, *bp, *msg, *pred, *tmp;
+  float *var, *gamma;
+  double* part;  // [B][kMaxTilesPerScene][kPartSlots]
+  uint32_t* keys;  // [B][N] order-preserving score keys (final E-step)
+  Scalars sc;
+  int* status;   // launch status word
+};
+
+cudaError_t set_dft_attributes();
+void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
+                 float2* data, float2* tmp, int* status, cudaStream_t st);
+void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
+                 float2* coeff, float2* tmp, int* status, cudaStream_t st);
+void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
+              cudaStream_t st);
+
+// Active-set stage.
+struct PolishBuffers {
+  const float2* y;
+  const float2* bp;
+  const float2 *mu, *dir1, *dir2;
+  const float *var, *gamma;
+  Scalars sc;
+  // per-scene state
+  int* active;        // [B][K] current active set
+  float* score;       // [B][K] UAMP second moments of the active set
+  float* gamma_init;  // [B][K] prior variances of the active set before reinit
+  unsigned char* pstate;  // opaque per-scene polish state
+  float* xcand_val;   // exchange candidates [B][E]
+  int* xcand_idx;
+  uint32_t* keys;     // [B][N] score keys scratch
+  int* status;        // [B] per-scene status
+};
+void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
+                const FbmeOutputs& out, cudaStream_t st);
+size_t polish_state_bytes();
+
+}  // namespace fbme

@@ -1,0 +1,625 @@
+// Active-set polish of the FBME plans: top-K support from the UAMP score,
+// exact reduced posterior with the Type-II evidence, evidence gate, EM
+// updates of the active variances and the noise, the residual support
+// exchange, fixed-budget diagnostics and the outputs.
+//
+// Follows torch_sbl/solver.py:1926-2021 (driver), 3961-4510
+// (_uamp_active_em_polish, the branches the plans reach), 3591-3779
+// (_active_posterior_with_evidence), 2898-2931 (Cholesky loading),
+// 3219-3317 (deletion gain), 3408-3496 (fixed-budget residuals),
+// 2081-2126 (effective DOF, support mask).
+//
+// Everything except the exchange scoring is K-dimensional (K <= 32): one
+// warp per scene, lane i owning row i.  Fourier atoms are never
+// materialised:
+//   Gram      G[k][l] = D1[(n1k-n1l) mod N1] * D2[(n2k-n2l) mod N2]
+//             (Dirichlet kernels summed in FP64 once per plan),
+//   A_S^H y   = (A^H y)[S], a gather of the backprojection,
+//   ||y - A_S mu||^2 = ||y||^2 - 2 Re(c^H mu) + mu^H G mu   (FP64),
+//   A^H(y - A_S mu)[n] = (A^H y)[n] - sum_k mu_k D(n - n_k)  (exchange).
+// The evidence (log-determinant + quadratic form) is accumulated in FP64.
+#include <math.h>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace fbme {
+
+constexpr float kTinyP = 1.17549435e-38f;
+constexpr float kEpsP = 1.1920929e-07f;
+constexpr int kMaxEval = 8;
+
+struct PolishScene {
+  int active[kMaxPolish];      // base active set (best accepted)
+  int work_active[kMaxPolish]; // active set of the next evaluation
+  float work_gamma[kMaxPolish];
+  float work_noise;
+  float2 best_mean[kMaxPolish];
+  float best_pv[kMaxPolish];
+  float best_dd[kMaxPolish];
+  float best_gamma[kMaxPolish];
+  float best_noise;
+  double best_nle;
+  float trace[kMaxEval];
+  int evals;        // evaluations done
+  int pending;      // exchange proposed at the previous transition
+  int exch_acc;     // accepted exchanges
+  int has_best;
+};
+
+size_t polish_state_bytes() { return sizeof(PolishScene); }
+
+struct PolishArgs {
+  BatchShape s;
+  DevConfig c;
+  PolishBuffers p;
+};
+
+FBME_DEV float2 dirichlet2(const float2* d1, const float2* d2, int n1, int n2, int a1, int a2,
+                           int b1, int b2) {
+  int i1 = a1 - b1, i2 = a2 - b2;
+  if (i1 < 0) i1 += n1;
+  if (i2 < 0) i2 += n2;
+  return cmul(__ldg(d1 + i1), __ldg(d2 + i2));
+}
+
+// Exact reduced posterior + negative log evidence for the work set.
+// Returns in lane k: mean_k, pv_k, dd_k; nle (all lanes); status bits.
+struct EvalOut {
+  float2 mean;
+  float pv, dd;
+  double nle;
+  int status;
+};
+
+FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33], int K, int my_idx,
+                          float my_gamma, float nu, float2 my_c, float data_energy) {
+  const int lane = threadIdx.x & 31;
+  const BatchShape& s = A.s;
+  const bool on = lane < K;
+  const int n1i = my_idx / s.n2, n2i = my_idx % s.n2;
+  // system S = diag(1/gamma) + G / nu, Hermitian-symmetrised
+  for (int j = 0; j < K; ++j) {
+    const int idx_j = __shfl_sync(0xffffffffu, my_idx, j);
+    if (on) {
+      const float2 g = dirichlet2(A.p.dir1, A.p.dir2, s.n1, s.n2, n1i, n2i, idx_j / s.n2,
+                                  idx_j % s.n2);
+      float2 a = make_float2(g.x / nu, g.y / nu);
+      if (j == lane) a.x += 1.0f / my_gamma;
+      M[lane][j] = a;
+    }
+  }
+  __syncwarp();
+  float2 row[kMaxPolish];
+  if (on)
+    for (int j = 0; j < K; ++j) {
+      const float2 a = M[lane][j], b = M[j][lane];
+      row[j] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+    }
+  __syncwarp();
+  if (on)
+    for (int j = 0; j < K; ++j) M[lane][j] = row[j];
+  __syncwarp();
+  const float dscale = on ? sqrtf(fmaxf(M[lane][lane].x, kTinyP)) : 1.0f;
+  // equilibrate: E[i][j] = S[i][j] / d_i / d_j, symmetrise again
+  {
+    float dj_all[kMaxPolish];
+    for (int j = 0; j < K; ++j) dj_all[j] = __shfl_sync(0xffffffffu, dscale, j);
+    if (on)
+      for (int j = 0; j < K; ++j) {
+        const float2 a = M[lane][j];
+        row[j] = make_float2(a.x / dscale / dj_all[j], a.y / dscale / dj_all[j]);
+      }
+    __syncwarp();
+    if (on)
+      for (int j = 0; j < K; ++j) M[lane][j] = row[j];
+    __syncwarp();
+    if (on)
+      for (int j = 0; j < K; ++j) {
+        const float2 a = M[lane][j], b = M[j][lane];
+        row[j] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+      }
+    __syncwarp();
+    if (on)
+      for (int j = 0; j < K; ++j) M[lane][j] = row[j];
+    __syncwarp();
+  }
+  // deterministic diagonal loading: multiplier * eps * mean|Re diag|
+  float dsum = on ? fabsf(M[lane][lane].x) : 0.f;
+  dsum = warp_sum(dsum);
+  const float scale = fmaxf(dsum / static_cast<float>(K), kTinyP);
+  const float jitter = A.c.jitter * (kEpsP * scale);
+  if (on) M[lane][lane].x += jitter;
+  __syncwarp();
+  // Cholesky, lower, in place
+  int status = 0;
+  for (int j = 0; j < K; ++j) {
+    if (lane == j) {
+      float sdiag = M[j][j].x;
+      for (int q = 0; q < j; ++q) sdiag -= abs2(M[j][q]);
+      if (!(sdiag > 0.f)) {
+        status |= isfinite(sdiag) ? FBME_STATUS_CHOLESKY : FBME_STATUS_NONFINITE;
+        sdiag = kTinyP;
+      }
+      M[j][j] = make_float2(sqrtf(sdiag), 0.f);
+    }
+    __syncwarp();
+    const float ljj = M[j][j].x;
+    if (on && lane > j) {
+      float2 v = M[lane][j];
+      for (int q = 0; q < j; ++q) {
+        const float2 a = M[lane][q], b = M[j][q];
+        v.x -= a.x * b.x + a.y * b.y;  // a * conj(b)
+        v.y -= a.y * b.x - a.x * b.y;
+      }
+      M[lane][j] = make_float2(v.x / ljj, v.y / ljj);
+    }
+    __syncwarp();
+  }
+  status = __reduce_or_sync(0xffffffffu, status);
+  // mean: L z = c / nu / d, L^H w = z, mu = w / d
+  const float2 rhs = on ? make_float2(my_c.x / nu, my_c.y / nu) : make_float2(0.f, 0.f);
+  float2 z = make_float2(rhs.x / dscale, rhs.y / dscale);
+  for (int q = 0; q < K; ++q) {
+    if (lane == q) z = make_float2(z.x / M[q][q].x, z.y / M[q][q].x);
+    const float2 zq = make_float2(__shfl_sync(0xffffffffu, z.x, q), __shfl_sync(0xffffffffu, z.y, q));
+    if (on && lane > q) {
+      const float2 l = M[lane][q];
+      z.x -= l.x * zq.x - l.y * zq.y;
+      z.y -= l.x * zq.y + l.y * zq.x;
+    }
+  }
+  float2 w = z;
+  for (int q = K - 1; q >= 0; --q) {
+    if (lane == q) w = make_float2(w.x / M[q][q].x, w.y / M[q][q].x);
+    const float2 wq = make_float2(__shfl_sync(0xffffffffu, w.x, q), __shfl_sync(0xffffffffu, w.y, q));
+    if (on && lane < q) {
+      const float2 l = M[q][lane];  // conj(L[q][lane]) * wq
+      w.x -= l.x * wq.x + l.y * wq.y;
+      w.y -= l.x * wq.y - l.y * wq.x;
+    }
+  }
+  EvalOut o;
+  o.mean = make_float2(w.x / dscale, w.y / dscale);
+  // inverse factor column `lane`: X = L^{-1}, eq_var = sum_i |X[i][lane]|^2
+  float eqv = 0.f;
+  if (on) {
+    for (int i = 0; i < K; ++i) X[i][lane] = make_float2(0.f, 0.f);
+    const float2 xt = make_float2(1.0f / M[lane][lane].x, 0.f);
+    X[lane][lane] = xt;
+    eqv = abs2(xt);
+    for (int i = lane + 1; i < K; ++i) {
+      float2 acc = make_float2(0.f, 0.f);
+      for (int q = lane; q < i; ++q) {
+        const float2 l = M[i][q], x = X[q][lane];
+        acc.x += l.x * x.x - l.y * x.y;
+        acc.y += l.x * x.y + l.y * x.x;
+      }
+      const float lii = M[i][i].x;
+      const float2 xi = make_float2(-acc.x / lii, -acc.y / lii);
+      X[i][lane] = xi;
+      eqv += abs2(xi);
+    }
+  }
+  __syncwarp();
+  o.pv = on ? fmaxf(eqv / (dscale * dscale), 0.f) : 0.f;
+  o.dd = on ? fmaxf((my_gamma - o.pv) / (my_gamma * my_gamma), 0.f) : 0.f;
+  // evidence (FP64 accumulation)
+  double ld = 0.0, lg = 0.0, qd = 0.0;
+  if (on) {
+    ld = log(static_cast<double>(fmaxf(M[lane][lane].x, kTinyP))) + log(static_cast<double>(dscale));
+    lg = log(static_cast<double>(my_gamma));
+    qd = static_cast<double>(rhs.x) * o.mean.x + static_cast<double>(rhs.y) * o.mean.y;
+  }
+  ld = warp_sum(ld);
+  lg = warp_sum(lg);
+  qd = warp_sum(qd);
+  const double logdet = static_cast<double>(s.m()) * log(static_cast<double>(nu)) + lg + 2.0 * ld;
+  double quad = static_cast<double>(data_energy) / nu - qd;
+  if (quad < 0.0) quad = 0.0;
+  o.nle = logdet + quad;
+  if (!isfinite(o.nle)) status |= FBME_STATUS_NONFINITE;
+  o.status = status;
+  return o;
+}
+
+// ||y - A_S mu||^2 by the Gram identity, FP64.
+FBME_DEV double residual_energy(const PolishArgs& A, int K, int my_idx, float2 my_mu, float2 my_c,
+                                float data_energy) {
+  const int lane = threadIdx.x & 31;
+  const BatchShape& s = A.s;
+  double cross = 0.0, quad = 0.0;
+  if (lane < K) {
+    cross = static_cast<double>(my_c.x) * my_mu.x + static_cast<double>(my_c.y) * my_mu.y;
+    const int n1i = my_idx / s.n2, n2i = my_idx % s.n2;
+    double gr = 0.0, gi = 0.0;  // (G mu)_i
+    for (int j = 0; j < K; ++j) {
+      const int idx_j = __shfl_sync(__activemask(), my_idx, j);
+      const float mjx = __shfl_sync(__activemask(), my_mu.x, j);
+      const float mjy = __shfl_sync(__activemask(), my_mu.y, j);
+      const float2 g = dirichlet2(A.p.dir1, A.p.dir2, s.n1, s.n2, n1i, n2i, idx_j / s.n2,
+                                  idx_j % s.n2);
+      gr += static_cast<double>(g.x) * mjx - static_cast<double>(g.y) * mjy;
+      gi += static_cast<double>(g.x) * mjy + static_cast<double>(g.y) * mjx;
+    }
+    quad = my_mu.x * gr + my_mu.y * gi;  // Re(conj(mu_i) (G mu)_i)
+  }
+  cross = warp_sum(cross);
+  quad = warp_sum(quad);
+  double e = static_cast<double>(data_energy) - 2.0 * cross + quad;
+  return e > 0.0 ? e : 0.0;
+}
+
+// Deletion gain of one active atom (solver.py:3247-3276).
+FBME_DEV float deletion_gain(float2 mean, float pv, float gamma) {
+  const float g = fmaxf(gamma, kTinyP);
+  const float2 q = make_float2(mean.x / g, mean.y / g);
+  const float down = fminf(fmaxf(pv / g, kTinyP), 1.0f);
+  return -logf(down) - g * abs_sq(q) / down;
+}
+
+// Warp bitonic sort of (value desc, position asc); returns this lane's
+// position after sorting.
+FBME_DEV int warp_sort_desc(float val, int pos, float* out_val) {
+  const int lane = threadIdx.x & 31;
+  for (int size = 2; size <= 32; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, val, stride);
+      const int op = __shfl_xor_sync(0xffffffffu, pos, stride);
+      const bool other_first = (ov > val) || (ov == val && op < pos);
+      const bool lower = (lane & stride) == 0;
+      const bool asc = (lane & size) == 0;
+      if (lower == asc ? other_first : !other_first) {
+        val = ov;
+        pos = op;
+      }
+    }
+  *out_val = val;
+  return pos;
+}
+
+constexpr int kPolishWarps = 1;
+
+// Evaluations p in [state.evals, P) until done or an exchange is needed.
+// phase 0: initialise from the top-K; phase 1: apply the exchange whose
+// candidates are in p.xcand_*, then continue.
+__global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A, int phase) {
+  __shared__ float2 Msm[kPolishWarps][32][33];
+  __shared__ float2 Xsm[kPolishWarps][32][33];
+  const int lane = threadIdx.x & 31;
+  const int scene = blockIdx.x * kPolishWarps + (threadIdx.x >> 5);
+  if (scene >= A.s.B) return;
+  const BatchShape& s = A.s;
+  const DevConfig& c = A.c;
+  const int K = c.polish_size;
+  const bool on = lane < K;
+  PolishScene* ps = reinterpret_cast<PolishScene*>(A.p.pstate) + scene;
+  const float fl = A.p.sc.floor_[scene];
+  const float data_energy = A.p.sc.data_energy[scene];
+  const float Mf = static_cast<float>(s.m());
+  const long long N = s.n();
+  const float2* bp = A.p.bp + scene * N;
+  float2(*M)[33] = Msm[threadIdx.x >> 5];
+  float2(*X)[33] = Xsm[threadIdx.x >> 5];
+  int status = 0;
+
+  if (phase == 0) {
+    // prune + reinitialise (solver.py:4087-4106)
+    if (on) {
+      const int idx = A.p.active[scene * K + lane];
+      ps->work_active[lane] = idx;
+      const float g0 = A.p.gamma[scene * N + idx];
+      ps->work_gamma[lane] = c.reinit ? fmaxf(A.p.score[scene * K + lane], fl) : g0;
+    }
+    if (lane == 0) {
+      ps->work_noise = A.p.sc.noise[scene];
+      ps->evals = 0;
+      ps->pending = 0;
+      ps->exch_acc = 0;
+      ps->has_best = 0;
+    }
+    __syncwarp();
+  } else {
+    // residual support exchange (solver.py:4397-4494), using the best
+    // state after evaluation 0 as the base.
+    const int E = c.exchange;
+    const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+    const float pv = on ? ps->best_pv[lane] : 0.f;
+    const float g = on ? ps->best_gamma[lane] : 0.f;
+    const float base_noise = ps->best_noise;
+    const float del = on ? deletion_gain(mu, pv, g) : -INFINITY;
+    float sval;
+    const int spos = warp_sort_desc(on ? del : -INFINITY, on ? lane : 0x7fffffff, &sval);
+    // lane r < E: removal position spos, addition candidate r
+    const int rem_pos = spos;
+    int repl_idx = -1;
+    float repl_gamma = 0.f;
+    int xmask = 0;
+    if (lane < E) {
+      const float add_e = A.p.xcand_val[scene * E + lane];
+      const int add_i = A.p.xcand_idx[scene * E + lane];
+      const float ce = Mf;
+      const float ratio = add_e / fmaxf(base_noise * ce, kTinyP);
+      const float add_gain = ratio > 1.0f ? ratio - 1.0f - logf(fmaxf(ratio, kTinyP)) : 0.0f;
+      xmask = (add_gain + sval) > 0.0f;
+      float ag = fmaxf(add_e - base_noise * ce, 0.0f) / (ce * ce);
+      ag = fminf(fmaxf(ag, fl), c.max_prec);
+      repl_idx = add_i;
+      repl_gamma = ag;
+    }
+    // apply: position rem_pos takes the addition where exchanged
+    for (int r = 0; r < E; ++r) {
+      const int pr = __shfl_sync(0xffffffffu, rem_pos, r);
+      const int xm = __shfl_sync(0xffffffffu, xmask, r);
+      const int ri = __shfl_sync(0xffffffffu, repl_idx, r);
+      const float rg = __shfl_sync(0xffffffffu, repl_gamma, r);
+      if (xm && lane == pr) {
+        ps->work_active[lane] = ri;
+        ps->work_gamma[lane] = rg;
+      }
+    }
+    const int any = __any_sync(0xffffffffu, xmask != 0);
+    if (lane == 0) ps->pending = any;
+    __syncwarp();
+  }
+
+  const int P = c.polish_iters;
+  for (int p = ps->evals; p < P; ++p) {
+    const int idx = on ? ps->work_active[lane] : 0;
+    const float gam = on ? ps->work_gamma[lane] : 1.0f;
+    const float nu = ps->work_noise;
+    const float2 cvec = on ? bp[idx] : make_float2(0.f, 0.f);
+    const EvalOut o = evaluate(A, M, X, K, idx, gam, nu, cvec, data_energy);
+    status |= o.status;
+    // evidence gate (solver.py:4168-4298)
+    bool accept = true;
+    if (c.gate && ps->has_best) {
+      const double best = ps->best_nle;
+      const double margin = static_cast<double>(c.margin_factor) * kEpsP *
+                            (1.0 + fabs(o.nle) + fabs(best));
+      accept = isfinite(o.nle) && (!isfinite(best) || o.nle <= best - margin);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      if (c.gate && ps->has_best && ps->pending && accept) ps->exch_acc += 1;
+      if (c.gate && ps->has_best) ps->pending = 0;
+    }
+    if (accept) {
+      if (on) {
+        ps->active[lane] = idx;
+        ps->best_mean[lane] = o.mean;
+        ps->best_pv[lane] = o.pv;
+        ps->best_dd[lane] = o.dd;
+        ps->best_gamma[lane] = gam;
+      }
+      if (lane == 0) {
+        ps->best_noise = nu;
+        ps->best_nle = o.nle;
+        ps->has_best = 1;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      ps->trace[p] = static_cast<float>(ps->best_nle);
+      ps->evals = p + 1;
+    }
+    __syncwarp();
+    if (p + 1 == P) break;
+    // EM between evaluations (solver.py:4320-4391), from the best state
+    const int bidx = on ? ps->active[lane] : 0;
+    const float2 bmu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+    const float bpv = on ? ps->best_pv[lane] : 0.f;
+    const float bg = on ? ps->best_gamma[lane] : 1.0f;
+    const float bnoise = ps->best_noise;
+    float ng = fminf(fmaxf(abs_sq(bmu) + bpv, fl), c.max_prec);
+    const float keep = c.polish_damping;
+    const float upd_g = keep * bg + (1.0f - keep) * ng;
+    const float2 bc = on ? bp[bidx] : make_float2(0.f, 0.f);
+    const double er = residual_energy(A, K, bidx, bmu, bc, data_energy);
+    float dof = on ? fminf(fmaxf(1.0f - bpv / fmaxf(bg, kTinyP), 0.f), 1.f) : 0.f;
+    dof = warp_sum(dof);
+    float un;
+    if (c.fixed_noise > 0.f) {
+      un = c.fixed_noise;
+    } else if (!c.noise_evidence) {
+      un = static_cast<float>((er + static_cast<double>(bnoise) * dof + c.noise_rate) /
+                              (static_cast<double>(Mf) + c.noise_shape));
+    } else {
+      un = static_cast<float>((er + c.noise_rate) /
+                              fmax(static_cast<double>(Mf) - dof + c.noise_shape, kEpsP));
+    }
+    un = fmaxf(un, fl);
+    const float new_noise = c.fixed_noise > 0.f ? un : keep * bnoise + (1.0f - keep) * un;
+    if (on) {
+      ps->work_active[lane] = bidx;
+      ps->work_gamma[lane] = upd_g;
+    }
+    if (lane == 0) ps->work_noise = new_noise;
+    __syncwarp();
+    const int E = c.exchange;
+    if (E > 0 && p == 0) break;  // exchange candidates are scored over the grid next
+  }
+  if (status && lane == 0) atomicOr(&A.p.status[scene], status);
+}
+
+// Residual exchange score over the grid: |A^H y - sum_k mu_k D(n - n_k)|^2,
+// with the active set excluded (key 0), as order-preserving keys.
+__global__ void __launch_bounds__(256) exchange_score_kernel(PolishArgs A, uint32_t* keys) {
+  extern __shared__ float2 shm[];
+  const BatchShape& s = A.s;
+  const int scene = blockIdx.y;
+  const int K = A.c.polish_size;
+  float2* d1 = shm;
+  float2* d2 = d1 + s.n1;
+  float2* mu = d2 + s.n2;
+  int* a1 = reinterpret_cast<int*>(mu + kMaxPolish);
+  int* a2 = a1 + kMaxPolish;
+  const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
+  for (int i = threadIdx.x; i < s.n1; i += blockDim.x) d1[i] = A.p.dir1[i];
+  for (int i = threadIdx.x; i < s.n2; i += blockDim.x) d2[i] = A.p.dir2[i];
+  if (threadIdx.x < K) {
+    const int idx = ps->active[threadIdx.x];
+    mu[threadIdx.x] = ps->best_mean[threadIdx.x];
+    a1[threadIdx.x] = idx / s.n2;
+    a2[threadIdx.x] = idx % s.n2;
+  }
+  __syncthreads();
+  const long long N = s.n();
+  const float2* bp = A.p.bp + scene * N;
+  uint32_t* kp = keys + scene * N;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < N;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int n1 = static_cast<int>(e / s.n2), n2 = static_cast<int>(e % s.n2);
+    float2 acc = make_float2(0.f, 0.f);
+    bool active = false;
+    for (int k = 0; k < K; ++k) {
+      int i1 = n1 - a1[k], i2 = n2 - a2[k];
+      active |= (i1 == 0 && i2 == 0);
+      if (i1 < 0) i1 += s.n1;
+      if (i2 < 0) i2 += s.n2;
+      const float2 dk = cmul(d1[i1], d2[i2]);
+      const float2 t = cmul(mu[k], dk);
+      acc.x += t.x;
+      acc.y += t.y;
+    }
+    const float2 b = bp[e];
+    const float2 r = make_float2(b.x - acc.x, b.y - acc.y);
+    const float score = abs_sq(r);
+    const uint32_t bits = __float_as_uint(score);
+    kp[e] = active ? 0u : ((bits & 0x80000000u) ? ~bits : (bits | 0x80000000u));
+  }
+}
+
+// Final K-space outputs, fixed-budget diagnostics, effective DOF
+// (solver.py:1989-2021, 2081-2092, 3408-3496, 2108-2126).
+__global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOutputs out) {
+  const int lane = threadIdx.x & 31;
+  const int scene = blockIdx.x;
+  if (scene >= A.s.B) return;
+  const BatchShape& s = A.s;
+  const DevConfig& c = A.c;
+  const int K = c.polish_size, P = c.polish_iters;
+  const bool on = lane < K;
+  const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
+  const float fl = A.p.sc.floor_[scene];
+  const float Mf = static_cast<float>(s.m());
+  const long long N = s.n();
+  const int idx = on ? ps->active[lane] : 0;
+  const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+  const float pv = on ? ps->best_pv[lane] : 0.f;
+  const float dd = on ? ps->best_dd[lane] : 0.f;
+  const float g = on ? ps->best_gamma[lane] : 1.0f;
+  const float nu = ps->best_noise;
+  // effective DOF with relevance projection
+  float rel = on ? fminf(fmaxf(g * dd, 0.f), 1.f) : 0.f;
+  const float raw = warp_sum(rel);
+  const float max_dof = static_cast<float>(static_cast<double>(s.m()) * (1.0 - 10.0 * kEpsP));
+  const float sc = fminf(1.0f, max_dof / fmaxf(raw, kEpsP));
+  const float dof = warp_sum(rel * sc);
+  if (lane == 0) {
+    out.noise_variance[scene] = nu;
+    out.effective_dof[scene] = dof;
+    out.negative_log_evidence[scene] = static_cast<float>(ps->best_nle);
+    for (int p = 0; p < P; ++p) out.evidence_trace[scene * P + p] = ps->trace[p];
+    if (out.support_exchanges_accepted) out.support_exchanges_accepted[scene] = ps->exch_acc;
+    if (out.support_score_threshold && c.false_alarm > 0.f)
+      out.support_score_threshold[scene] =
+          static_cast<float>(log(static_cast<double>(N) / static_cast<double>(c.false_alarm)));
+  }
+  if (on && out.active_indices) out.active_indices[scene * K + lane] = idx;
+  if (c.fixed_budget && out.fixed_budget_gamma_residual) {
+    const float ag = fmaxf(g, kTinyP);
+    const float gt = fminf(fmaxf(abs_sq(mu) + pv, fl), c.max_prec);
+    const float gs = fmaxf(fmaxf(fabsf(ag), fabsf(gt)), kTinyP);
+    const float gr = warp_max(on ? fabsf(ag - gt) / gs : 0.f);
+    float d2 = on ? fminf(fmaxf(1.0f - pv / ag, 0.f), 1.f) : 0.f;
+    d2 = warp_sum(d2);
+    const float2 cv = on ? A.p.bp[scene * N + idx] : make_float2(0.f, 0.f);
+    const double er = residual_energy(A, K, idx, mu, cv, A.p.sc.data_energy[scene]);
+    float nt;
+    if (c.fixed_noise > 0.f) {
+      nt = nu;
+    } else if (!c.noise_evidence) {
+      nt = static_cast<float>((er + static_cast<double>(nu) * d2 + c.noise_rate) /
+                              (static_cast<double>(Mf) + c.noise_shape));
+    } else {
+      nt = static_cast<float>((er + c.noise_rate) /
+                              fmax(static_cast<double>(Mf) - d2 + c.noise_shape, kEpsP));
+    }
+    nt = fminf(fmaxf(nt, fl), c.max_prec);
+    const float ns = fmaxf(fmaxf(fabsf(nu), fabsf(nt)), kTinyP);
+    if (lane == 0) {
+      out.fixed_budget_gamma_residual[scene] = gr;
+      out.fixed_budget_noise_residual[scene] = c.fixed_noise > 0.f ? 0.f : fabsf(nu - nt) / ns;
+      bool fin = true, mono = true;
+      for (int p = 0; p < P; ++p) fin &= isfinite(ps->trace[p]) != 0;
+      for (int p = 1; p < P; ++p) mono &= ps->trace[p] <= ps->trace[p - 1];
+      out.fixed_budget_monotone[scene] = fin && mono;
+      out.fixed_budget_objective_decrease[scene] = fmaxf(ps->trace[0] - ps->trace[P - 1], 0.f);
+    }
+  }
+}
+
+// N-space outputs: zero mean, floor variance and 1/floor precision off the
+// active set, then the active entries.
+__global__ void output_fill_kernel(BatchShape s, Scalars sc, FbmeOutputs out) {
+  const long long N = s.n();
+  const int scene = blockIdx.y;
+  const float fl = sc.floor_[scene];
+  const float inv = 1.0f / fl;
+  float2* x = reinterpret_cast<float2*>(out.x) + scene * N;
+  float* pv = out.posterior_variance + scene * N;
+  float* pr = out.precision + scene * N;
+  uint8_t* mk = out.support_mask ? out.support_mask + scene * N : nullptr;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < N;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    x[e] = make_float2(0.f, 0.f);
+    pv[e] = fl;
+    pr[e] = inv;
+    if (mk) mk[e] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(32) output_scatter_kernel(PolishArgs A, FbmeOutputs out) {
+  const int lane = threadIdx.x & 31;
+  const int scene = blockIdx.x;
+  const int K = A.c.polish_size;
+  if (lane >= K) return;
+  const long long N = A.s.n();
+  const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
+  const int idx = ps->active[lane];
+  const float2 mu = ps->best_mean[lane];
+  const float pv = ps->best_pv[lane];
+  const long long e = scene * N + idx;
+  reinterpret_cast<float2*>(out.x)[e] = mu;
+  out.posterior_variance[e] = pv;
+  out.precision[e] = 1.0f / ps->best_gamma[lane];
+  if (out.support_mask && A.c.false_alarm > 0.f) {
+    const float thr = static_cast<float>(log(static_cast<double>(N) / A.c.false_alarm));
+    out.support_mask[e] = (abs_sq(mu) / fmaxf(pv, kTinyP)) > thr;
+  }
+}
+
+void launch_topk(const uint32_t* keys, long long n, int k, int B, int* out_idx, float* out_val,
+                 cudaStream_t st);
+
+void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
+                const FbmeOutputs& out, cudaStream_t st) {
+  PolishArgs A{s, c, p};
+  const int K = c.polish_size;
+  launch_topk(p.keys, s.n(), K, s.B, p.active, p.score, st);
+  polish_kernel<<<s.B, 32, 0, st>>>(A, 0);
+  if (c.exchange > 0 && c.polish_iters > 1) {
+    const int blocks = static_cast<int>((s.n() + 256 * 16 - 1) / (256 * 16));
+    const size_t shm = (s.n1 + s.n2 + kMaxPolish) * sizeof(float2) + 2 * kMaxPolish * sizeof(int);
+    exchange_score_kernel<<<dim3(blocks < 64 ? blocks : 64, s.B), 256, shm, st>>>(A, p.keys);
+    launch_topk(p.keys, s.n(), c.exchange, s.B, p.xcand_idx, p.xcand_val, st);
+    polish_kernel<<<s.B, 32, 0, st>>>(A, 1);
+  }
+  polish_finish_kernel<<<s.B, 32, 0, st>>>(A, out);
+  const int fb = static_cast<int>((s.n() + 2047) / 2048);
+  output_fill_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(s, p.sc, out);
+  output_scatter_kernel<<<s.B, 32, 0, st>>>(A, out);
+}
+
+}  // namespace fbme

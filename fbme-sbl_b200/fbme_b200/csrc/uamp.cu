@@ -1,0 +1,555 @@
+// UAMP stage of the FBME plan: initialisation, T_u message-passing sweeps
+// and the final E-step, for a batch of equally shaped scenes.
+//
+// Per sweep (solver.py:2726-2870 with the fused Triton updates of
+// triton_kernels.py:37-192, 267-417):
+//   adjoint stage 1  prologue: message update  m' = d m + (1-d) (y - (p - dv m)) / (dv + nv)
+//   adjoint stage 2  epilogue: Gaussian denoiser, damping, ARD prior update,
+//                              per-tile sums of relevance (DOF) and variance
+//   forward stage 1
+//   forward stage 2  epilogue: prediction p = A mu and per-tile sum |y - p|^2
+//   scalars          noise update (EM / evidence), data variance, pseudo variance
+// The first sweep reuses A^H y from the initialisation (solver.py:2775-2783).
+//
+// Layouts: coefficient arrays [B][N1][N2], data arrays [B][M1][M2] (the
+// caller's prefix block layout), forward intermediate [B][M2][N1], adjoint
+// intermediate [B][N2][M1].  All reductions are per-tile sums written to
+// fixed slots and added in a fixed order, so results are reproducible run
+// to run.
+#include <math.h>
+
+#include "dft_umma.cuh"
+#include "kernels.cuh"
+
+namespace fbme {
+
+constexpr float kTiny = 1.17549435e-38f;  // FLT_MIN (torch.finfo(float32).tiny)
+constexpr float kEps = 1.1920929e-07f;    // FLT_EPSILON
+
+// ---------------------------------------------------------------------------
+// partial-sum helpers
+// ---------------------------------------------------------------------------
+FBME_DEV double* part_slot(double* part, int scene, int tile, int slot) {
+  return part + (static_cast<long long>(scene) * kMaxTilesPerScene + tile) * kPartSlots + slot;
+}
+FBME_DEV void write_block_partial(double v, double* red, double* part, int scene, int tile,
+                                  int slot) {
+  const double s = block_sum(v, red);
+  if (threadIdx.x == 0) *part_slot(part, scene, tile, slot) = s;
+}
+FBME_DEV int tile_in_scene(const TileCtx& t) { return t.row_tile * t.g->col_tiles + t.col_tile; }
+
+FBME_DEV bool vec_ok(const DftGeom& g) { return g.vec4 != 0; }
+
+// Two consecutive complex values at base[e], e in [0, limit).
+FBME_DEV void load2c(const float2* base, long long e, int avail, bool vec, float2& a, float2& b) {
+  if (avail >= 2 && vec) {
+    const float4 v = *reinterpret_cast<const float4*>(base + e);
+    a = make_float2(v.x, v.y);
+    b = make_float2(v.z, v.w);
+  } else {
+    a = base[e];
+    b = avail >= 2 ? base[e + 1] : make_float2(0.f, 0.f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// prologues
+// ---------------------------------------------------------------------------
+
+// Plain load; also sums |y|^2 (for the data power) over the column-tile-0 CTAs.
+struct ProYPower {
+  const float2* in;
+  double* part;
+  float acc;
+  FBME_DEV float4 load4(const TileCtx& t, int row, int kreal) {
+    const float4 v = load_row4(in, t, row, kreal);
+    if (t.col_tile == 0) {
+      acc += abs_sq(make_float2(v.x, v.y));
+      acc += abs_sq(make_float2(v.z, v.w));
+    }
+    return v;
+  }
+  FBME_DEV void finish(const TileCtx& t, double* red) {
+    write_block_partial(acc, red, part, t.scene, tile_in_scene(t), 0);
+  }
+};
+
+// UAMP message update fused into the adjoint's operand load
+// (triton_kernels.py:72-84).  Reads the previous message from `msg_in`,
+// writes the new one to `msg_out` (column tile 0 only) and feeds it to the
+// tensor core.
+struct ProMessage {
+  const float2 *y, *pred, *msg_in;
+  float2* msg_out;
+  const float *prec, *dvar;
+  float damping;
+  FBME_DEV float4 load4(const TileCtx& t, int row, int kreal) {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    const int j0 = kreal >> 1;
+    if (r >= g.rows || j0 >= g.kcplx) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
+    const int avail = g.kcplx - j0;
+    const bool vec = vec_ok(g);
+    float2 y0, y1, p0, p1, m0, m1;
+    load2c(y, e, avail, vec, y0, y1);
+    load2c(pred, e, avail, vec, p0, p1);
+    load2c(msg_in, e, avail, vec, m0, m1);
+    const float pr = prec[t.scene], dv = dvar[t.scene];
+    const float keep = damping, upd = 1.0f - damping;
+    auto step = [&](float2 yy, float2 pp, float2 mm) {
+      const float2 pseudo = make_float2(pp.x - dv * mm.x, pp.y - dv * mm.y);
+      const float2 cand = make_float2(pr * (yy.x - pseudo.x), pr * (yy.y - pseudo.y));
+      return make_float2(keep * mm.x + upd * cand.x, keep * mm.y + upd * cand.y);
+    };
+    const float2 o0 = step(y0, p0, m0);
+    const float2 o1 = avail >= 2 ? step(y1, p1, m1) : make_float2(0.f, 0.f);
+    if (t.col_tile == 0) {
+      msg_out[e] = o0;
+      if (avail >= 2) msg_out[e + 1] = o1;
+    }
+    return make_float4(o0.x, o0.y, o1.x, o1.y);
+  }
+  FBME_DEV void finish(const TileCtx&, double*) {}
+};
+
+// ---------------------------------------------------------------------------
+// epilogues
+// ---------------------------------------------------------------------------
+
+// Forward stage 2: store the prediction and sum |y - p|^2.
+struct EpiPredict {
+  float2* pred;
+  const float2* y;
+  double* part;
+  float acc;
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    if (r >= g.rows) return;
+    const long long base = t.scene * g.out_stride + r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = t.col0() + (c0 >> 1) + i;
+      if (j < g.cols) {
+        const long long e = base + static_cast<long long>(j) * g.out_ld;
+        const float2 p = make_float2(v[2 * i], v[2 * i + 1]);
+        pred[e] = p;
+        const float2 yy = y[e];
+        const float dr = yy.x - p.x, di = yy.y - p.y;
+        acc += dr * dr + di * di;
+      }
+    }
+  }
+  FBME_DEV void finish(const TileCtx& t, double* red) {
+    write_block_partial(acc, red, part, t.scene, tile_in_scene(t), 2);
+  }
+};
+
+// Adjoint stage 2 during initialisation: store A^H y and sum |A^H y|^2.
+struct EpiBackprojection {
+  float2* bp;
+  double* part;
+  float acc;
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    if (r >= g.rows) return;
+    const long long base = t.scene * g.out_stride + r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = t.col0() + (c0 >> 1) + i;
+      if (j < g.cols) {
+        const float2 b = make_float2(v[2 * i], v[2 * i + 1]);
+        bp[base + static_cast<long long>(j) * g.out_ld] = b;
+        acc += abs_sq(b);
+      }
+    }
+  }
+  FBME_DEV void finish(const TileCtx& t, double* red) {
+    write_block_partial(acc, red, part, t.scene, tile_in_scene(t), 1);
+  }
+};
+
+// Gaussian denoiser with damping and the fused ARD prior update
+// (triton_kernels.py:140-192; solver.py:2832-2850, 1600-1607).
+struct DenoiseArgs {
+  float2* mu;
+  float* var;
+  float* gamma;
+  const float* pv;
+  const float* floor_;
+  double* part;
+  uint32_t* keys;  // optional: score key of |mu|^2 + v for the top-K
+  float damping, prior_damping, prior_max, hyper_shape, hyper_rate;
+  int update_prior;
+};
+
+FBME_DEV uint32_t float_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+FBME_DEV void denoise_one(const DenoiseArgs& a, int scene, long long e, float2 lifted, float pv,
+                          float floor_, float& dof_acc, float& var_acc) {
+  const float prior = a.gamma[e];
+  const float2 old_mean = a.mu[e];
+  const float old_var = fmaxf(a.var[e], kTiny);
+  const float denom = fmaxf(prior + pv, kTiny);
+  const float gain = prior / denom;
+  const float2 pm = make_float2(old_mean.x + pv * lifted.x, old_mean.y + pv * lifted.y);
+  const float2 cm = make_float2(gain * pm.x, gain * pm.y);
+  const float cv = prior * pv / denom;
+  const float keep = a.damping, upd = 1.0f - a.damping;
+  const float2 mean = make_float2(keep * old_mean.x + upd * cm.x, keep * old_mean.y + upd * cm.y);
+  const float variance = fmaxf(keep * old_var + upd * cv, kTiny);
+  float rel = 1.0f - variance / fmaxf(prior, kTiny);
+  rel = fmaxf(0.0f, fminf(1.0f, rel));
+  a.mu[e] = mean;
+  a.var[e] = variance;
+  if (a.update_prior) {
+    const float second = mean.x * mean.x + mean.y * mean.y + variance;
+    float cand = (second + a.hyper_rate) / (1.0f + a.hyper_shape);
+    cand = fmaxf(floor_, fminf(a.prior_max, cand));
+    const float nxt = a.prior_damping * prior + (1.0f - a.prior_damping) * cand;
+    a.gamma[e] = fmaxf(nxt, floor_);
+  }
+  if (a.keys) a.keys[e] = float_key(abs_sq(mean) + variance);
+  dof_acc += rel;
+  var_acc += variance;
+}
+
+struct EpiDenoise {
+  DenoiseArgs a;
+  float dof_acc, var_acc;
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    if (r >= g.rows) return;
+    const float pv = a.pv[t.scene], fl = a.floor_[t.scene];
+    const long long base = t.scene * g.out_stride + r;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = t.col0() + (c0 >> 1) + i;
+      if (j < g.cols)
+        denoise_one(a, t.scene, base + static_cast<long long>(j) * g.out_ld,
+                    make_float2(v[2 * i], v[2 * i + 1]), pv, fl, dof_acc, var_acc);
+    }
+  }
+  FBME_DEV void finish(const TileCtx& t, double* red) {
+    write_block_partial(dof_acc, red, a.part, t.scene, tile_in_scene(t), 0);
+    write_block_partial(var_acc, red, a.part, t.scene, tile_in_scene(t), 1);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// elementwise kernels
+// ---------------------------------------------------------------------------
+constexpr int kEwThreads = 256;
+
+FBME_DEV int ew_blocks_per_scene(long long n) {
+  long long b = (n + 2047) / 2048;
+  return static_cast<int>(b < kMaxTilesPerScene ? (b < 1 ? 1 : b) : kMaxTilesPerScene);
+}
+static int ew_blocks_host(long long n) {
+  long long b = (n + 2047) / 2048;
+  return static_cast<int>(b < kMaxTilesPerScene ? (b < 1 ? 1 : b) : kMaxTilesPerScene);
+}
+
+// Initial prior variances (solver.py:1063-1099): backprojection blend or
+// uniform, floored; per-block sums of the result.
+__global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevConfig c, Scalars sc,
+                                                            const float2* bp, float* gamma,
+                                                            double* part) {
+  __shared__ double red[32];
+  const int scene = blockIdx.y;
+  const long long n = s.n();
+  const float dp = sc.data_power[scene], fl = sc.floor_[scene];
+  const float ebp = fmaxf(sc.ebp[scene], kEps);
+  const float uniform = dp / static_cast<float>(n);
+  float acc = 0.f;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long e = scene * n + i;
+    float g;
+    if (c.blend >= 0.f) {
+      const float structured = abs_sq(bp[e]) / ebp * dp;
+      g = c.blend * structured + (1.0f - c.blend) * uniform;
+    } else {
+      g = uniform;
+    }
+    g = fmaxf(g, fl);
+    gamma[e] = g;
+    acc += g;
+  }
+  write_block_partial(acc, red, part, scene, blockIdx.x, 0);
+}
+
+// First sweep: the lifted message is (1-d)/(dv+nv) * A^H y, the previous
+// mean is zero and the previous variance equals the initial prior
+// (solver.py:1160-1182, 2775-2783).  Blocks past `nblk_n` write the first
+// message m1 = (1-d) * (y / (dv+nv)) instead.
+__global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevConfig c, Scalars sc,
+                                                            DenoiseArgs a, const float2* bp,
+                                                            const float2* y, float2* msg,
+                                                            int nblk_n) {
+  __shared__ double red[32];
+  const int scene = blockIdx.y;
+  if (static_cast<int>(blockIdx.x) >= nblk_n) {
+    const long long m = s.m();
+    const float pr = sc.prec[scene];
+    const float keep = c.uamp_damping, upd = 1.0f - c.uamp_damping;
+    for (long long i = (blockIdx.x - nblk_n) * static_cast<long long>(blockDim.x) + threadIdx.x;
+         i < m; i += static_cast<long long>(gridDim.x - nblk_n) * blockDim.x) {
+      const long long e = scene * m + i;
+      const float2 yy = y[e];
+      msg[e] = make_float2(keep * 0.0f + upd * (pr * yy.x), keep * 0.0f + upd * (pr * yy.y));
+    }
+    return;
+  }
+  const long long n = s.n();
+  const float pv = sc.pv[scene], fl = sc.floor_[scene];
+  const float scale = (1.0f - c.uamp_damping) / (fmaxf(sc.dvar[scene], kTiny) + sc.noise[scene]);
+  float dof = 0.f, sv = 0.f;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(nblk_n) * blockDim.x) {
+    const long long e = scene * n + i;
+    a.mu[e] = make_float2(0.f, 0.f);
+    a.var[e] = a.gamma[e];
+    const float2 b = bp[e];
+    denoise_one(a, scene, e, make_float2(scale * b.x, scale * b.y), pv, fl, dof, sv);
+  }
+  write_block_partial(dof, red, a.part, scene, blockIdx.x, 0);
+  write_block_partial(sv, red, a.part, scene, blockIdx.x, 1);
+}
+
+// Per-scene scalar updates from the per-tile sums (fixed summation order).
+enum ScalarMode { kScalarInit1 = 0, kScalarInit2 = 1, kScalarSweep = 2 };
+
+__global__ void scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part,
+                               int nt0, int nt1, int nt2) {
+  const int scene = blockIdx.x * blockDim.x + threadIdx.x;
+  if (scene >= s.B) return;
+  auto sum = [&](int slot, int nt) {
+    double v = 0.0;
+    for (int t = 0; t < nt; ++t)
+      v += part[(static_cast<long long>(scene) * kMaxTilesPerScene + t) * kPartSlots + slot];
+    return v;
+  };
+  const float M = static_cast<float>(s.m());
+  if (mode == kScalarInit1) {
+    const double ysum = sum(0, nt0);
+    const float dp = fmaxf(static_cast<float>(ysum / static_cast<double>(s.m())), kEps);
+    const float fl = fmaxf(dp * c.min_var, kTiny);
+    sc.data_power[scene] = dp;
+    sc.floor_[scene] = fl;
+    sc.data_energy[scene] = static_cast<float>(ysum);
+    sc.ebp[scene] = static_cast<float>(sum(1, nt1));
+    sc.noise[scene] = c.fixed_noise > 0.f ? c.fixed_noise : fmaxf(c.init_noise * dp, fl);
+  } else if (mode == kScalarInit2) {
+    const float dv = fmaxf(static_cast<float>(sum(0, nt0)), kTiny);
+    const float nv = sc.noise[scene];
+    sc.dvar[scene] = dv;
+    sc.pv[scene] = fmaxf((dv + nv) / M, kTiny);
+    sc.prec[scene] = 1.0f / (dv + nv);
+  } else {
+    const float max_dof = static_cast<float>(static_cast<double>(s.m()) * (1.0 - 10.0 * kEps));
+    const float dof = fminf(static_cast<float>(sum(0, nt0)), max_dof);
+    const float sv = static_cast<float>(sum(1, nt1));
+    const float energy = static_cast<float>(sum(2, nt2));
+    const float fl = sc.floor_[scene];
+    float nv = sc.noise[scene];
+    if (!(c.fixed_noise > 0.f)) {
+      float cand;
+      if (c.noise_evidence)
+        cand = (energy + c.noise_rate) / fmaxf(M - dof + c.noise_shape, kEps);
+      else
+        cand = (energy + nv * dof + c.noise_rate) / (M + c.noise_shape);
+      cand = fmaxf(cand, fl);
+      nv = c.damping * nv + (1.0f - c.damping) * cand;
+      nv = fmaxf(nv, fl);
+    }
+    const float dv = fmaxf(sv, kTiny);
+    sc.dof[scene] = dof;
+    sc.energy[scene] = energy;
+    sc.noise[scene] = nv;
+    sc.dvar[scene] = dv;
+    sc.pv[scene] = fmaxf((dv + nv) / M, kTiny);
+    sc.prec[scene] = 1.0f / (dv + nv);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stage geometry and launch
+// ---------------------------------------------------------------------------
+static int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+static DftGeom make_geom(int B, int rows, int kcplx, int cols, int in_ld, long long in_stride,
+                         int out_ld, long long out_stride, const uint8_t* table, int table_kchunks,
+                         int n_tile) {
+  DftGeom g;
+  g.n_scenes = B;
+  g.rows = rows;
+  g.row_tiles = ceil_div(rows, kTileRows);
+  g.kcplx = kcplx;
+  g.kchunks = ceil_div(2LL * kcplx, kKChunk);
+  g.cols = cols;
+  g.col_tiles = ceil_div(2LL * cols, n_tile);
+  g.in_ld = in_ld;
+  g.in_stride = in_stride;
+  g.out_ld = out_ld;
+  g.out_stride = out_stride;
+  g.col_per_tile = n_tile / 2;
+  g.vec4 = (in_ld % 2 == 0) && (in_stride % 2 == 0);
+  g.table = table;
+  g.table_kchunks = table_kchunks;
+  return g;
+}
+
+enum Stage { kFwd1, kFwd2, kAdj1, kAdj2 };
+
+static DftGeom stage_geom(Stage st, const BatchShape& s, const DftTables& t, int n_tile) {
+  const long long N = s.n(), M = s.m();
+  switch (st) {
+    case kFwd1:  // [n1][n2] -> [m2][n1], contract n2
+      return make_geom(s.B, s.n1, s.n2, s.m2, s.n2, N, s.n1, 1LL * s.m2 * s.n1, t.fwd_n2,
+                       t.kchunks_n2, n_tile);
+    case kFwd2:  // [m2][n1] -> [m1][m2], contract n1
+      return make_geom(s.B, s.m2, s.n1, s.m1, s.n1, 1LL * s.m2 * s.n1, s.m2, M, t.fwd_n1,
+                       t.kchunks_n1, n_tile);
+    case kAdj1:  // [m1][m2] -> [n2][m1], contract m2
+      return make_geom(s.B, s.m1, s.m2, s.n2, s.m2, M, s.m1, 1LL * s.n2 * s.m1, t.adj_n2,
+                       t.kchunks_n2, n_tile);
+    default:     // [n2][m1] -> [n1][n2], contract m1
+      return make_geom(s.B, s.n2, s.m1, s.n1, s.m1, 1LL * s.n2 * s.m1, s.n2, N, t.adj_n1,
+                       t.kchunks_n1, n_tile);
+  }
+}
+
+static int tiles(const DftGeom& g) { return g.n_scenes * g.row_tiles * g.col_tiles; }
+
+template <int A_PARTS, int N_TILE, class Pro, class Epi>
+static cudaError_t set_attr() {
+  return cudaFuncSetAttribute(dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              DftCfg<A_PARTS, N_TILE>::kSmemBytes);
+}
+
+template <class Pro, class Epi>
+static void run_stage(int terms, const DftGeom& g, const Pro& pro, const Epi& epi, int* status,
+                      cudaStream_t st) {
+  if (terms == 6) {
+    dft_stage_kernel<3, 128, Pro, Epi>
+        <<<tiles(g), kDftThreads, DftCfg<3, 128>::kSmemBytes, st>>>(g, pro, epi, status);
+  } else {
+    dft_stage_kernel<2, 256, Pro, Epi>
+        <<<tiles(g), kDftThreads, DftCfg<2, 256>::kSmemBytes, st>>>(g, pro, epi, status);
+  }
+}
+
+template <class Pro, class Epi>
+static cudaError_t set_attr_both() {
+  cudaError_t e = set_attr<2, 256, Pro, Epi>();
+  if (e != cudaSuccess) return e;
+  return set_attr<3, 128, Pro, Epi>();
+}
+
+cudaError_t set_dft_attributes() {
+  cudaError_t e;
+  if ((e = set_attr_both<ProPlain, EpiStoreT>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProYPower, EpiStoreT>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProMessage, EpiStoreT>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiPredict>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiBackprojection>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiDenoise>()) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+static int n_tile_of(int terms) { return terms == 6 ? 128 : 256; }
+
+void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
+                 float2* data, float2* tmp, int* status, cudaStream_t st) {
+  const int nt = n_tile_of(terms);
+  const DftGeom g1 = stage_geom(kFwd1, s, t, nt), g2 = stage_geom(kFwd2, s, t, nt);
+  run_stage(terms, g1, ProPlain{coeff}, EpiStoreT{tmp}, status, st);
+  run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{data}, status, st);
+}
+
+void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
+                 float2* coeff, float2* tmp, int* status, cudaStream_t st) {
+  const int nt = n_tile_of(terms);
+  const DftGeom g1 = stage_geom(kAdj1, s, t, nt), g2 = stage_geom(kAdj2, s, t, nt);
+  run_stage(terms, g1, ProPlain{data}, EpiStoreT{tmp}, status, st);
+  run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{coeff}, status, st);
+}
+
+// Message buffers ping-pong between sweeps: msg[0] / msg[1] are both
+// M-sized regions starting at u.msg and u.msg + B*M.
+void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
+              cudaStream_t st) {
+  const int nt = n_tile_of(c.terms);
+  const DftGeom f1 = stage_geom(kFwd1, s, t, nt), f2 = stage_geom(kFwd2, s, t, nt);
+  const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
+  const int sc_blocks = ceil_div(s.B, 128);
+  const long long BM = static_cast<long long>(s.B) * s.m();
+  float2* msg[2] = {u.msg, u.msg + BM};
+
+  // --- initialisation: A^H y, data power, floors, initial noise, prior ---
+  run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st);
+  run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f}, u.status, st);
+  scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit1, s, c, u.sc, u.part,
+                                            a1.row_tiles * a1.col_tiles,
+                                            a2.row_tiles * a2.col_tiles, 0);
+  const int bn = ew_blocks_host(s.n()), bm = ew_blocks_host(s.m());
+  gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma, u.part);
+  scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit2, s, c, u.sc, u.part, bn, 0, 0);
+
+  DenoiseArgs da;
+  da.mu = u.mu;
+  da.var = u.var;
+  da.gamma = u.gamma;
+  da.pv = u.sc.pv;
+  da.floor_ = u.sc.floor_;
+  da.part = u.part;
+  da.keys = nullptr;
+  da.damping = c.uamp_damping;
+  da.prior_damping = c.damping;
+  da.prior_max = c.max_prec;
+  da.hyper_shape = c.hyper_shape;
+  da.hyper_rate = c.hyper_rate;
+  da.update_prior = 1;
+
+  // --- sweeps ---
+  int cur = 0;  // msg[cur] holds the latest message
+  for (int it = 1; it <= c.uamp_iters; ++it) {
+    int nt_dof;
+    if (it == 1) {
+      sweep1_kernel<<<dim3(bn + bm, s.B), kEwThreads, 0, st>>>(s, c, u.sc, da, u.bp, u.y,
+                                                               msg[cur], bn);
+      nt_dof = bn;
+    } else {
+      run_stage(c.terms, a1,
+                ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar,
+                           c.uamp_damping},
+                EpiStoreT{u.tmp}, u.status, st);
+      cur ^= 1;
+      run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st);
+      nt_dof = a2.row_tiles * a2.col_tiles;
+    }
+    run_stage(c.terms, f1, ProPlain{u.mu}, EpiStoreT{u.tmp}, u.status, st);
+    run_stage(c.terms, f2, ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f}, u.status, st);
+    scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarSweep, s, c, u.sc, u.part, nt_dof, nt_dof,
+                                              f2.row_tiles * f2.col_tiles);
+  }
+
+  // --- final E-step (no prior update, no prediction), score keys ---
+  run_stage(c.terms, a1,
+            ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar, c.uamp_damping},
+            EpiStoreT{u.tmp}, u.status, st);
+  da.update_prior = 0;
+  da.keys = reinterpret_cast<uint32_t*>(u.keys);
+  run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st);
+}
+
+}  // namespace fbme

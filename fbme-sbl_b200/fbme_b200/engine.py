@@ -1,0 +1,296 @@
+"""Host engine: one native FBME plan bound to torch-owned device buffers.
+
+The engine resolves an ``SBLConfig`` into the C ABI's ``FbmeConfig``
+(iteration budget, damping, active-set sizes), allocates the plan
+workspace and every output as torch tensors on the target device, creates
+the native plan, and launches replays on the current torch stream, so the
+whole solve can be captured in a ``torch.cuda.CUDAGraph``.
+
+Semantics follow the reference ``fast_sbl`` for ``mode="uamp"`` with the
+active-set polish (torch_sbl/solver.py:925-2393): outputs are owned by the
+engine and overwritten by the next run.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from math import ceil, log, prod
+from typing import Sequence
+
+import torch
+from torch import Tensor
+
+from . import _native as nat
+from .config import SBLConfig
+from .result import SBLResult
+
+BACKEND_NAME = "cuda-sm100a"
+
+
+def uamp_iteration_limit(cfg: SBLConfig, n_grid: int, n_samples: int) -> int:
+    """UAMP sweep budget (solver.py:1287-1309)."""
+    minimum = max(cfg.min_iter, cfg.uamp_min_iter)
+    limit = cfg.max_iter
+    if cfg.uamp_auto_iterations:
+        budget = ceil(cfg.uamp_iteration_offset + cfg.uamp_iteration_scale * n_grid / n_samples)
+        limit = min(cfg.max_iter, max(minimum, budget))
+    return limit
+
+
+def resolve_native_config(cfg: SBLConfig, grid: Sequence[int], sample: Sequence[int]) -> nat.FbmeConfig:
+    """Map the hot-path fields of ``cfg`` to ``FbmeConfig``."""
+    n_grid, n_samples = prod(grid), prod(sample)
+    damping = cfg.uamp_damping
+    if cfg.uamp_adaptive_damping:  # solver.py:1183-1189
+        damping = max(damping, min(cfg.uamp_max_damping, 0.02 * n_grid / n_samples))
+    k = min(cfg.uamp_polish_size, n_grid)
+    exchange = min(cfg.uamp_polish_residual_exchange_size, max(k - 1, 0), n_grid - k)
+    c = nat.FbmeConfig()
+    c.uamp_iterations = uamp_iteration_limit(cfg, n_grid, n_samples)
+    c.uamp_damping = damping
+    c.damping = cfg.damping
+    c.initialization_blend = cfg.initialization_blend if cfg.initialization == "backprojection" else -1.0
+    c.initial_noise_fraction = cfg.initial_noise_fraction
+    c.fixed_noise_variance = cfg.fixed_noise_variance if cfg.fixed_noise_variance is not None else 0.0
+    c.min_variance = cfg.min_variance
+    c.max_precision = cfg.max_precision
+    c.hyper_shape = cfg.hyper_shape
+    c.hyper_rate = cfg.hyper_rate
+    c.noise_shape = cfg.noise_shape
+    c.noise_rate = cfg.noise_rate
+    c.noise_update = 1 if cfg.noise_update == "evidence" else 0
+    c.polish_size = k
+    c.polish_iterations = cfg.uamp_polish_iterations
+    c.polish_prune_tail = int(cfg.uamp_polish_prune_tail)
+    c.polish_reinitialize = int(cfg.uamp_polish_reinitialize)
+    c.polish_evidence_gate = int(cfg.uamp_polish_evidence_gate)
+    c.polish_damping = cfg.uamp_polish_damping
+    c.evidence_margin_factor = cfg.uamp_polish_evidence_margin_factor
+    c.exchange_size = exchange
+    c.fixed_budget_diagnostics = int(cfg.uamp_polish_fixed_budget_diagnostics)
+    c.cholesky_jitter_multiplier = cfg.cuda_cholesky_jitter_multiplier
+    c.support_false_alarm_budget = (cfg.uamp_support_false_alarm_budget
+                                    if cfg.uamp_support_false_alarm_budget is not None else 0.0)
+    c.dft_terms = cfg.dft_terms
+    return c
+
+
+def check_supported(cfg: SBLConfig) -> None:
+    """Reject configurations outside the built device path."""
+    unsupported = {
+        "joint_sparsity": cfg.joint_sparsity,
+        "spatial_coupling": cfg.spatial_coupling > 0.0 or cfg.learn_spatial_coupling,
+        "uamp_polish_global_certificate": cfg.uamp_polish_global_certificate,
+        "uamp_polish_support_repairs": cfg.uamp_polish_support_repairs != 0,
+        "uamp_polish_support_growth_steps": cfg.uamp_polish_support_growth_steps != 0,
+        "uamp_polish_support_shrink_steps": cfg.uamp_polish_support_shrink_steps != 0,
+        "uamp_polish_coordinate_steps": cfg.uamp_polish_coordinate_steps != 0,
+        "uamp_polish_noise_coordinate_steps": cfg.uamp_polish_noise_coordinate_steps != 0,
+        "uamp_polish_high_precision": cfg.uamp_polish_high_precision,
+        "uamp_polish_max_truncation_delta": cfg.uamp_polish_max_truncation_delta is not None,
+        "offgrid_refinement": cfg.offgrid_refinement,
+    }
+    bad = [k for k, v in unsupported.items() if v]
+    if bad:
+        raise NotImplementedError("the B200 FBME path does not implement: " + ", ".join(bad))
+    if cfg.tol > 0.0:
+        raise NotImplementedError(
+            "mode='uamp' runs the fixed UAMP budget on the device; set tol=0 "
+            "(every UAMP preset does)")
+    if cfg.uamp_polish_size < 1 or not cfg.uamp_polish_prune_tail:
+        raise NotImplementedError(
+            "the device UAMP path implements the zero-tail active-set polish "
+            "(uamp_polish_size >= 1 and uamp_polish_prune_tail=True, as in the FBME presets)")
+
+
+class FBMEEngine:
+    """A native plan for ``batch`` scenes of one shape and configuration."""
+
+    def __init__(self, batch: int, grid: Sequence[int], sample: Sequence[int], cfg: SBLConfig,
+                 device: torch.device, stream: torch.cuda.Stream | None = None) -> None:
+        self.lib = nat.lib()
+        if device.type != "cuda":
+            raise RuntimeError("the FBME B200 engine needs a CUDA device")
+        self.device = device
+        self.batch = int(batch)
+        self.grid = tuple(int(v) for v in grid)
+        self.sample = tuple(int(v) for v in sample)
+        self.cfg = cfg
+        self.n_grid, self.n_samples = prod(self.grid), prod(self.sample)
+        self.native_cfg = resolve_native_config(cfg, self.grid, self.sample)
+        shapes = (nat.FbmeShape * self.batch)()
+        for i in range(self.batch):
+            shapes[i] = nat.FbmeShape(self.grid[0], self.grid[1], self.sample[0], self.sample[1])
+        self._shapes = shapes
+        nbytes = self.lib.fbme_plan_workspace_bytes(shapes, self.batch, ctypes.byref(self.native_cfg))
+        if nbytes == 0:
+            nat.check(nat.FBME_ERR_INVALID if "different shapes" not in nat.last_error()
+                      else nat.FBME_ERR_UNSUPPORTED, "fbme_plan_workspace_bytes")
+        self.workspace = torch.empty(int(nbytes) + 256, dtype=torch.uint8, device=device)
+        base = self.workspace.data_ptr()
+        self._ws_ptr = (base + 255) & ~255
+        B, N, K = self.batch, self.n_grid, self.native_cfg.polish_size
+        P = self.native_cfg.polish_iterations
+        f32 = dict(dtype=torch.float32, device=device)
+        self.out = {
+            "x": torch.zeros(B, N, dtype=torch.complex64, device=device),
+            "posterior_variance": torch.zeros(B, N, **f32),
+            "precision": torch.zeros(B, N, **f32),
+            "support_mask": torch.zeros(B, N, dtype=torch.bool, device=device),
+            "noise_variance": torch.zeros(B, **f32),
+            "effective_dof": torch.zeros(B, **f32),
+            "negative_log_evidence": torch.zeros(B, **f32),
+            "evidence_trace": torch.zeros(B, P, **f32),
+            "support_exchanges_accepted": torch.zeros(B, dtype=torch.int64, device=device),
+            "fixed_budget_gamma_residual": torch.zeros(B, **f32),
+            "fixed_budget_noise_residual": torch.zeros(B, **f32),
+            "fixed_budget_objective_decrease": torch.zeros(B, **f32),
+            "fixed_budget_monotone": torch.zeros(B, dtype=torch.bool, device=device),
+            "support_score_threshold": torch.zeros(B, **f32),
+            "active_indices": torch.zeros(B, K, dtype=torch.int64, device=device),
+            "status": torch.zeros(B, dtype=torch.int32, device=device),
+        }
+        o = nat.FbmeOutputs()
+        for name, _ in nat.FbmeOutputs._fields_:
+            setattr(o, name, self.out[name].data_ptr())
+        self._outputs = o
+        self._plan = ctypes.c_void_p()
+        st = stream or torch.cuda.current_stream(device)
+        with torch.cuda.device(device):
+            rc = self.lib.fbme_plan_create(shapes, self.batch, ctypes.byref(self.native_cfg),
+                                           ctypes.c_void_p(self._ws_ptr), ctypes.c_size_t(nbytes),
+                                           ctypes.c_void_p(st.cuda_stream), ctypes.byref(self._plan))
+        nat.check(rc, "fbme_plan_create")
+        # constant result fields of the zero-tail polish (solver.py:4052-4068, 4639-4653)
+        self._false = torch.zeros(B, dtype=torch.bool, device=device)
+        self._true = torch.ones(B, dtype=torch.bool, device=device)
+        self._zero = torch.zeros(B, **f32)
+
+    # ------------------------------------------------------------------ runs
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def run(self, y: Tensor) -> None:
+        """Solve ``y`` ([B, M1*M2] or any contiguous complex64 view of it)."""
+        self._check_y(y)
+        nat.check(self.lib.fbme_plan_replay(self._plan, ctypes.c_void_p(y.data_ptr()),
+                                            ctypes.byref(self._outputs),
+                                            ctypes.c_void_p(self._stream())), "fbme_plan_replay")
+
+    def run_uamp(self, y: Tensor) -> None:
+        self._check_y(y)
+        nat.check(self.lib.fbme_uamp_run(self._plan, ctypes.c_void_p(y.data_ptr()),
+                                         ctypes.c_void_p(self._stream())), "fbme_uamp_run")
+
+    def run_polish(self, y: Tensor) -> None:
+        self._check_y(y)
+        nat.check(self.lib.fbme_polish_run(self._plan, ctypes.c_void_p(y.data_ptr()),
+                                           ctypes.byref(self._outputs),
+                                           ctypes.c_void_p(self._stream())), "fbme_polish_run")
+
+    def dft_forward(self, coeff: Tensor) -> Tensor:
+        """A(X) for [B, N] complex64 coefficients -> [B, M] data."""
+        self._check(coeff, self.n_grid)
+        out = torch.empty(self.batch, self.n_samples, dtype=torch.complex64, device=self.device)
+        nat.check(self.lib.fbme_dft_forward(self._plan, ctypes.c_void_p(coeff.data_ptr()),
+                                            ctypes.c_void_p(out.data_ptr()),
+                                            ctypes.c_void_p(self._stream())), "fbme_dft_forward")
+        return out
+
+    def dft_adjoint(self, data: Tensor) -> Tensor:
+        """A^H(Y) for [B, M] complex64 data -> [B, N] coefficients."""
+        self._check(data, self.n_samples)
+        out = torch.empty(self.batch, self.n_grid, dtype=torch.complex64, device=self.device)
+        nat.check(self.lib.fbme_dft_adjoint(self._plan, ctypes.c_void_p(data.data_ptr()),
+                                            ctypes.c_void_p(out.data_ptr()),
+                                            ctypes.c_void_p(self._stream())), "fbme_dft_adjoint")
+        return out
+
+    def state(self) -> dict[str, Tensor]:
+        """Views of the resident UAMP state (for tests and tools)."""
+        st = nat.FbmeState()
+        nat.check(self.lib.fbme_plan_state(self._plan, ctypes.byref(st)), "fbme_plan_state")
+        B, N, M = self.batch, self.n_grid, self.n_samples
+
+        def view(ptr: int, shape, dtype):
+            ws0 = self.workspace.data_ptr()
+            itemsize = torch.empty((), dtype=dtype).element_size()
+            off = ptr - ws0
+            n = prod(shape)
+            flat = self.workspace[off: off + n * itemsize].view(dtype)
+            return flat.view(*shape)
+
+        return {
+            "mean": view(st.mean, (B, N), torch.complex64),
+            "variance": view(st.variance, (B, N), torch.float32),
+            "prior_variance": view(st.prior_variance, (B, N), torch.float32),
+            "backprojection": view(st.backprojection, (B, N), torch.complex64),
+            "prediction": view(st.prediction, (B, M), torch.complex64),
+            "noise_variance": view(st.noise_variance, (B,), torch.float32),
+            "data_variance": view(st.data_variance, (B,), torch.float32),
+        }
+
+    def _check(self, t: Tensor, length: int) -> None:
+        if (t.device != self.device or t.dtype != torch.complex64 or not t.is_contiguous()
+                or t.numel() != self.batch * length):
+            raise ValueError(f"expected a contiguous complex64 tensor of {self.batch}x{length} "
+                             f"elements on {self.device}")
+
+    def _check_y(self, y: Tensor) -> None:
+        self._check(y, self.n_samples)
+
+    # --------------------------------------------------------------- results
+    def result(self, batch_shape: tuple[int, ...]) -> SBLResult:
+        """Engine-owned ``SBLResult`` views shaped like the reference's."""
+        o, cfg = self.out, self.cfg
+        out_shape = (*batch_shape, *self.grid)
+        K = self.native_cfg.polish_size
+        exch = o["support_exchanges_accepted"].reshape(batch_shape) \
+            if self.native_cfg.exchange_size > 0 else None
+        fb = bool(self.native_cfg.fixed_budget_diagnostics)
+        has_mask = cfg.uamp_support_false_alarm_budget is not None
+        nle = o["negative_log_evidence"].reshape(batch_shape)
+        return SBLResult(
+            x=o["x"].reshape(out_shape),
+            posterior_variance=o["posterior_variance"].reshape(out_shape),
+            precision=o["precision"].reshape(out_shape),
+            noise_variance=o["noise_variance"].reshape(batch_shape),
+            effective_dof=o["effective_dof"].reshape(batch_shape),
+            iterations=int(self.native_cfg.uamp_iterations),
+            converged=False,
+            relative_change=float("nan"),
+            mode="uamp",
+            arithmetic_dtype="complex64",
+            uamp_backend_used=BACKEND_NAME,
+            active_set_size=K,
+            negative_log_evidence=nle,
+            evidence_trace=o["evidence_trace"],
+            hard_pruning_accepted=self._false.reshape(batch_shape),
+            truncation_certified=self._false.reshape(batch_shape),
+            support_repairs_accepted=exch,
+            support_exchanges_accepted=exch,
+            active_model_selected=self._true.reshape(batch_shape),
+            support_log_odds_penalty=self._zero.reshape(batch_shape),
+            penalized_negative_log_evidence=nle,
+            penalized_evidence_trace=o["evidence_trace"],
+            fixed_budget_gamma_residual=o["fixed_budget_gamma_residual"].reshape(batch_shape) if fb else None,
+            fixed_budget_noise_residual=o["fixed_budget_noise_residual"].reshape(batch_shape) if fb else None,
+            fixed_budget_objective_decrease=(
+                o["fixed_budget_objective_decrease"].reshape(batch_shape) if fb else None),
+            fixed_budget_monotone=o["fixed_budget_monotone"].reshape(batch_shape) if fb else None,
+            support_mask=o["support_mask"].reshape(out_shape) if has_mask else None,
+            support_score_threshold=(o["support_score_threshold"].reshape(batch_shape)
+                                     if has_mask else None),
+            status=o["status"].reshape(batch_shape),
+        )
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) is not None and self._plan.value:
+            self.lib.fbme_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass

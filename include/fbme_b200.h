@@ -1,0 +1,165 @@
+/*
+ * fbme_b200.h -- C ABI of the B200 (sm_100a) FBME plan-replay hot path.
+ *
+ * Plain C types only: device pointers, sizes, a CUDA stream handle.  The
+ * caller (the Python host layer, or any C/C++/FFI host) owns every device
+ * buffer, including the plan workspace whose size fbme_plan_workspace_bytes
+ * reports; the library allocates no device memory.  No exception crosses
+ * this boundary: every entry point returns an FBME_* error code and
+ * fbme_last_error() describes the last failure of the calling thread.
+ *
+ * Thread-safety: one plan per stream; a plan must not be replayed
+ * concurrently with itself.  Plans share no mutable global state.
+ *
+ * Reference interfaces replaced (FBME-SBL v1.1, paths inside that project):
+ *   fbme_plan_create / replay  <-> torch_sbl/cuda_graph.py:22-107
+ *                                  (CUDAGraphSBLPlan.__init__ / .replay) and
+ *                                  torch_sbl_fastest_stable/profiles.py:35-148
+ *   fbme_dft_forward           <-> torch_sbl/operators.py:237-253 (forward_flat)
+ *   fbme_dft_adjoint           <-> torch_sbl/operators.py:255-280 (adjoint_flat)
+ *   fbme_uamp_run              <-> torch_sbl/solver.py:1063-1189, 1295-1798,
+ *                                  1907-1925 (fast_sbl uamp init/loop/E-step),
+ *                                  solver.py:2726-2870 (_uamp_posterior) and the
+ *                                  Triton kernels torch_sbl/triton_kernels.py:
+ *                                  476-547, 550-667, 806-904
+ *   fbme_polish_run            <-> torch_sbl/solver.py:1926-2021, 3961-4510
+ *                                  (top-K + _uamp_active_em_polish + fixed-
+ *                                  budget diagnostics), 2081-2126
+ */
+#ifndef FBME_B200_H
+#define FBME_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same handle as cudaStream_t. */
+typedef struct CUstream_st* fbme_stream_t;
+
+/* Return codes. */
+enum {
+  FBME_OK = 0,
+  FBME_ERR_INVALID = 1,     /* bad argument, shape or config (-> ValueError) */
+  FBME_ERR_UNSUPPORTED = 2, /* valid request outside what is built */
+  FBME_ERR_CUDA = 3,        /* a CUDA runtime call failed (-> RuntimeError) */
+  FBME_ERR_WORKSPACE = 4    /* workspace too small or misaligned */
+};
+
+/* Per-scene status bits written to FbmeOutputs.status. */
+enum {
+  FBME_STATUS_NONFINITE = 1,   /* NaN/Inf reached the reduced posterior */
+  FBME_STATUS_CHOLESKY = 2,    /* reduced Cholesky pivot <= 0 after loading */
+  FBME_STATUS_TIMEOUT = 4,     /* a bounded device wait ran out */
+  FBME_STATUS_PCG_BREAKDOWN = 8,
+  FBME_STATUS_ITER_CAP = 16
+};
+
+/* One scene: reconstruction grid N1 x N2, observed prefix M1 x M2. */
+typedef struct {
+  int32_t n1, n2, m1, m2;
+} FbmeShape;
+
+/* Hot-path fields of SBLConfig (torch_sbl/solver.py:34-176), resolved by
+ * the host layer (e.g. the UAMP iteration budget of solver.py:1295-1309). */
+typedef struct {
+  int32_t uamp_iterations;           /* T_u */
+  float uamp_damping;                /* message/denoiser damping */
+  float damping;                     /* prior and noise damping ("keep") */
+  float initialization_blend;        /* backprojection blend; < 0 => uniform */
+  float initial_noise_fraction;
+  float fixed_noise_variance;        /* <= 0 => estimated */
+  float min_variance;
+  float max_precision;
+  float hyper_shape, hyper_rate, noise_shape, noise_rate;
+  int32_t noise_update;              /* 0 = "em", 1 = "evidence" */
+  int32_t polish_size;               /* K, 0 disables the active-set polish */
+  int32_t polish_iterations;         /* P */
+  int32_t polish_prune_tail;
+  int32_t polish_reinitialize;
+  int32_t polish_evidence_gate;
+  float polish_damping;
+  float evidence_margin_factor;
+  int32_t exchange_size;             /* residual support exchange size */
+  int32_t fixed_budget_diagnostics;
+  float cholesky_jitter_multiplier;  /* reduced Cholesky loading, x eps */
+  float support_false_alarm_budget;  /* <= 0 => no support mask */
+  int32_t dft_terms;                 /* split-BF16 products: 3 or 6 */
+} FbmeConfig;
+
+/* Caller-owned device output buffers for B scenes (N = n1*n2 per scene).
+ * Pointers marked optional may be NULL. */
+typedef struct {
+  void* x;                                 /* [B,N] complex64 */
+  float* posterior_variance;               /* [B,N] */
+  float* precision;                        /* [B,N] */
+  uint8_t* support_mask;                   /* [B,N] bool, optional */
+  float* noise_variance;                   /* [B] */
+  float* effective_dof;                    /* [B] */
+  float* negative_log_evidence;            /* [B] */
+  float* evidence_trace;                   /* [B,P] */
+  int64_t* support_exchanges_accepted;     /* [B], optional */
+  float* fixed_budget_gamma_residual;      /* [B], optional */
+  float* fixed_budget_noise_residual;      /* [B], optional */
+  float* fixed_budget_objective_decrease;  /* [B], optional */
+  uint8_t* fixed_budget_monotone;          /* [B], optional */
+  float* support_score_threshold;          /* [B], optional */
+  int64_t* active_indices;                 /* [B,K], optional */
+  int32_t* status;                         /* [B] */
+} FbmeOutputs;
+
+/* Device pointers into a plan's resident UAMP state (for tests/tools). */
+typedef struct {
+  void* mean;              /* [B,N] complex64 */
+  float* variance;         /* [B,N] */
+  float* prior_variance;   /* [B,N] */
+  void* message;           /* [B,M] complex64 */
+  void* prediction;        /* [B,M] complex64 */
+  void* backprojection;    /* [B,N] complex64 (A^H y) */
+  float* noise_variance;   /* [B] */
+  float* data_variance;    /* [B] */
+} FbmeState;
+
+typedef struct FbmePlan FbmePlan;
+
+/* Bytes of device workspace a plan for these scenes needs (0 on error). */
+size_t fbme_plan_workspace_bytes(const FbmeShape* shapes, int32_t n_scenes,
+                                 const FbmeConfig* cfg);
+
+/* Build a plan: validate, bind the caller's workspace (256-byte aligned)
+ * and fill its constant tables on `stream`.  Launches kernels; call it
+ * outside stream capture. */
+int fbme_plan_create(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg,
+                     void* workspace, size_t workspace_bytes, fbme_stream_t stream,
+                     FbmePlan** plan);
+
+/* Solve every scene: y is [B, M1*M2] complex64 (row-major prefix blocks,
+ * scenes back to back).  Asynchronous on `stream`; capturable. */
+int fbme_plan_replay(FbmePlan* plan, const void* y, const FbmeOutputs* out,
+                     fbme_stream_t stream);
+
+int fbme_plan_destroy(FbmePlan* plan);
+
+/* Stage entry points (same plan, same stream rules). */
+int fbme_dft_forward(FbmePlan* plan, const void* coefficients, void* data, fbme_stream_t stream);
+int fbme_dft_adjoint(FbmePlan* plan, const void* data, void* coefficients, fbme_stream_t stream);
+/* UAMP initialisation, T_u sweeps and the final E-step; the state is left
+ * in the plan (read it with fbme_plan_state). */
+int fbme_uamp_run(FbmePlan* plan, const void* y, fbme_stream_t stream);
+/* Top-K, reduced evidence-gated polish and outputs, from the plan's state
+ * after fbme_uamp_run. */
+int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream);
+int fbme_plan_state(FbmePlan* plan, FbmeState* state);
+
+/* Thread-local description of the last failure ("" if none). */
+const char* fbme_last_error(void);
+/* Library version string. */
+const char* fbme_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FBME_B200_H */

@@ -457,7 +457,8 @@ def _uamp_iteration_limit(cfg: OracleConfig, n_grid: int, n_samples: int) -> int
     return limit
 
 
-def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str = "cuda"):
+def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str = "cuda",
+                  stop_after_uamp: bool = False):
     """Restatement of ``fast_sbl`` for ``mode="uamp"`` with the polish.
 
     ``data`` is ``[M1, M2]`` or ``[B, M1, M2]``.  Returns a dict of the
@@ -530,6 +531,11 @@ def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str =
     # final E-step (solver.py:1907-1925)
     mean, var, dof_u, st, _ = uamp_sweep(y, prior, noise, op, st, damping=damping,
                                          compute_prediction=False)
+    if stop_after_uamp:
+        # state after the final E-step (before top-K and the polish)
+        return dict(mean=mean, variance=var, prior_variance=prior, noise_variance=noise,
+                    backprojection=initial_bp, prediction=st.prediction, iterations=limit,
+                    score=_abs2(mean) + var)
     out: dict[str, Any] = {}
     if cfg.uamp_polish_size > 0:
         k = min(cfg.uamp_polish_size, n)
