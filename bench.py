@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""FBME plan-replay throughput on B200: scenes/s and % of the HBM roofline.
+
+Workload: FBME-Stable replay of 256x256-grid / 128x128-prefix scenes
+(200 Rayleigh point scatterers, 15 dB, polish_size 32), a batch of
+``--batch`` scenes per step solved by one captured plan.  Synthetic scenes
+stand in for recorded data (seeded, shapes and value laws as named).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU (torchrun); every rank solves its own batch
+(weak scaling, no collective on the data path); timing is the max over ranks.
+``--impl reference`` times the CPU restatement of the reference algorithm on
+the host cores (the reference ships no compiled code).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+for _p in (str(REPO), str(REPO / "fbme-sbl_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "scenes/s at equal NMSE: plain vs learned+batched FBME on 1 B200; % roofline"
+UNIT = "scenes/s"
+GRID, PREFIX = (256, 256), (128, 128)
+WORKLOAD = ("FBME-Stable replay, 256x256 grid / 128x128 prefix, 200 Rayleigh points, 15 dB, "
+            "polish_size=32")
+
+
+def _args() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--batch", type=int, default=256, help="scenes per step per GPU")
+    ap.add_argument("--profile", choices=("stable", "fast"), default="stable")
+    ap.add_argument("--cpu-sample", type=int, default=32, help="scenes in the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def _scenes(n: int, seed0: int):
+    from fbme_b200 import scenes
+
+    return [scenes.config_scene("c2", seed0 + i) for i in range(n)]
+
+
+# ---------------------------------------------------------------- CPU side
+def _oracle_solve(args):
+    y, grid, profile = args
+    from oracle import fbme_oracle as O
+
+    return O.fbme_solve(y, grid, profile)["x"]
+
+
+def cpu_baseline(n_scenes: int, profile: str) -> dict:
+    """Oracle port (numpy restatement of the reference) on one core."""
+    import numpy as np  # noqa: F401
+
+    from oracle import fbme_oracle as O
+
+    sc = _scenes(n_scenes, 1_000_000)
+    O.fbme_solve(sc[0].y, sc[0].grid, profile)  # warm
+    t0 = time.perf_counter()
+    for s in sc:
+        O.fbme_solve(s.y, s.grid, profile)
+    dt = time.perf_counter() - t0
+    return {"value": n_scenes / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n_scenes} scenes of the same workload, numpy oracle, one process"}
+
+
+def run_reference(a: argparse.Namespace) -> None:
+    """Reference arm: the CPU restatement with every host core (spawn pool)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    sc = _scenes(cores, 2_000_000)
+    work = [(s.y, s.grid, a.profile) for s in sc]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_limit_threads) as pool:
+        for _ in range(a.warmup):
+            pool.map(_oracle_solve, work)
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            pool.map(_oracle_solve, work)
+        dt = time.perf_counter() - t0
+    value = cores * a.steps / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * dt / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scenes_per_step": cores, "profile": a.profile},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{cores} scenes per step, one per host core (spawn pool)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _limit_threads() -> None:
+    os.environ["OMP_NUM_THREADS"] = "1"
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None) -> None:
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "100"]
+        if gpu_id:
+            cmd += ["-i", gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- roofline
+def _peaks() -> tuple[float, str]:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(group: str, n: int, m: int) -> int:
+    """Algorithmic HBM bytes of one scene for one launch of a kernel group
+    (intermediates of the two-stage DFT are not counted)."""
+    table = {
+        "adjoint_denoise": 32 * n,    # read gamma, mu, v; write mu', v', gamma' (or keys)
+        "adjoint_message": 24 * m,    # read y, m; write m'
+        "forward_1": 8 * n,           # read mu
+        "forward_residual": 16 * m,   # read y; write prediction
+        "sweep1_denoise": 24 * n + 16 * m,
+    }
+    return table.get(group, 0)
+
+
+def scene_bytes(n: int, m: int, t_u: int, p: int) -> int:
+    """Algorithmic bytes of one Stable solve: (T_u+1) sweeps of 32N+24M,
+    8M+8N initialisation, 12N top-K read, P re-reads of y, 17N outputs."""
+    return (t_u + 1) * (32 * n + 24 * m) + 8 * m + 8 * n + 12 * n + p * 8 * m + 17 * n
+
+
+def _traffic(group: str, batch: int):
+    """Measured DRAM bytes per launch for ``group`` from the committed ncu
+    summary (per-scene figure scaled by the batch), or None."""
+    p = REPO / "profiles" / "traffic_per_scene.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    v = d.get(group)
+    return None if v is None else float(v) * batch
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(a: argparse.Namespace) -> None:
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(device)
+
+    from torch_sbl_fastest_stable import make_fastest_plan, make_stable_plan
+
+    B = a.batch
+    sc = _scenes(B, rank * B)
+    y_np = np.stack([s.y for s in sc])
+    x_true = np.stack([s.x for s in sc]).astype(np.complex64)
+    y_host = torch.from_numpy(y_np).pin_memory()
+    y_dev = y_host.to(device)
+    make = make_stable_plan if a.profile == "stable" else make_fastest_plan
+    plan = make(y_dev, GRID, polish_size=32, warmup=1)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+    except Exception:
+        pass
+    clocks = Clocks(gpu_id)
+    stream = torch.cuda.current_stream(device)
+    for _ in range(max(a.warmup, 3)):
+        plan.replay(y_dev)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        plan.replay(y_dev)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = B * a.steps * world / (ms / 1000.0)
+
+    # end to end through the public API: pinned host y -> replay -> host x
+    x_host = torch.empty((B, *GRID), dtype=torch.complex64).pin_memory()
+    nv_host = torch.empty((B,), dtype=torch.float32).pin_memory()
+    res = plan.result
+    for _ in range(2):
+        plan.input_buffer.copy_(y_host, non_blocking=True)
+        r = plan.replay()
+        x_host.copy_(r.x, non_blocking=True)
+        nv_host.copy_(r.noise_variance, non_blocking=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(a.steps):
+        plan.input_buffer.copy_(y_host, non_blocking=True)
+        r = plan.replay()
+        x_host.copy_(r.x, non_blocking=True)
+        nv_host.copy_(r.noise_variance, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e = B * a.steps * world / (e2e_ms / 1000.0)
+
+    # quality of this batch (raw NMSE, no gain alignment)
+    x_hat = x_host.numpy().reshape(B, -1)
+    num = np.sum(np.abs(x_hat - x_true.reshape(B, -1)) ** 2, axis=1)
+    den = np.sum(np.abs(x_true.reshape(B, -1)) ** 2, axis=1)
+    nmse_db = float(10.0 * np.log10(np.mean(num / den)))
+    status_bad = int((res.status != 0).sum().item())
+
+    # live per-kernel timing (one eagerly launched replay with CUDA events)
+    prof = plan._engine.profile(plan.input_buffer.view(B, -1))
+    n, m = GRID[0] * GRID[1], PREFIX[0] * PREFIX[1]
+    launches = sum(c for _, c in prof.values())
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_cnt) = dom
+    per_launch_s = dom_ms / max(dom_cnt, 1) / 1000.0
+    alg = algorithmic_bytes(dom_name, n, m) * B
+    peak, peak_kind = _peaks()
+    achieved = alg / per_launch_s / 1e9 if alg else None
+    t_u = plan._engine.native_cfg.uamp_iterations
+    p_iters = plan._engine.native_cfg.polish_iterations
+    step_bytes = scene_bytes(n, m, t_u, p_iters) * B
+    step_gbs = step_bytes / (ms / a.steps / 1000.0) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = cpu_baseline(a.cpu_sample, a.profile)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {
+                "workload": WORKLOAD, "profile": a.profile, "scenes_per_step_per_gpu": B,
+                "parallelism": f"scene-sharded x{world}", "l2": "inputs larger than L2 "
+                f"(resident state {step_bytes / 1e6:.0f} MB algorithmic traffic per step)",
+                "dft": "tcgen05 split-BF16 3-term, FP32 accumulation",
+                "nmse_db": nmse_db, "scenes_with_status": status_bad,
+            },
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(y_host.numel() * 8),
+                    "d2h_bytes_per_step": int(x_host.numel() * 8 + nv_host.numel() * 4)},
+            "roofline": {
+                "bound": "hbm", "kernel": dom_name,
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": _traffic(dom_name, B),
+                "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_s * 1000.0,
+                "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                "step_algorithmic_gbs": step_gbs, "step_frac": step_gbs / peak,
+            },
+            "kernel_ms_per_replay": {k: round(v[0], 4) for k, v in prof.items()},
+            "gpu_launches": launches * a.steps,
+            "launches_per_step": launches,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    del plan
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

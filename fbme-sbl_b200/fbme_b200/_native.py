@@ -25,6 +25,8 @@ STATUS_TIMEOUT = 4
 STATUS_PCG_BREAKDOWN = 8
 STATUS_ITER_CAP = 16
 
+NUM_GROUPS = 11
+
 
 class FbmeShape(ctypes.Structure):
     _fields_ = [("n1", c_int32), ("n2", c_int32), ("m1", c_int32), ("m2", c_int32)]
@@ -106,6 +108,9 @@ SIGNATURES = {
     "fbme_uamp_run": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fbme_polish_run": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
     "fbme_plan_state": (c_int, [c_void_p, POINTER(FbmeState)]),
+    "fbme_plan_profile": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p,
+                                  POINTER(c_float), POINTER(c_int32), c_int32]),
+    "fbme_profile_group_name": (c_char_p, [c_int32]),
     "fbme_last_error": (c_char_p, []),
     "fbme_version": (c_char_p, []),
 }

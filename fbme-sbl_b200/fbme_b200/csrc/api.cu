@@ -325,6 +325,54 @@ int fbme_plan_replay(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme
   return fbme_polish_run(plan, y, out, stream);
 }
 
+const char* fbme_profile_group_name(int32_t group) {
+  static const char* names[FBME_NUM_GROUPS] = {
+      "init", "adjoint_message", "adjoint_denoise", "forward_1", "forward_residual", "scalars",
+      "sweep1_denoise", "topk", "polish", "exchange_score", "output"};
+  return (group >= 0 && group < FBME_NUM_GROUPS) ? names[group] : "";
+}
+
+int fbme_plan_profile(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream,
+                      float* group_ms, int32_t* group_launches, int32_t n_groups) {
+  if (!plan || !y || !out || !group_ms || !group_launches)
+    return fail(FBME_ERR_INVALID, "NULL argument");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  fbme::Profiler* prof = new (std::nothrow) fbme::Profiler();
+  if (!prof) return fail(FBME_ERR_INVALID, "out of host memory");
+  prof->st = st;
+  for (int i = 0; i < 2 * fbme::Profiler::kMax; ++i) cudaEventCreate(&prof->ev[i]);
+  cudaMemsetAsync(plan->status, 0, plan->s.B * sizeof(int), st);
+  fbme::UampBuffers u = plan->u;
+  u.y = static_cast<const float2*>(y);
+  fbme::uamp_run(plan->s, plan->tables, plan->dc, u, st, prof);
+  fbme::PolishBuffers p = plan->p;
+  p.y = static_cast<const float2*>(y);
+  fbme::polish_run(plan->s, plan->dc, p, *out, st, prof);
+  cudaMemcpyAsync(out->status, plan->status, plan->s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  int rc = FBME_OK;
+  if (e != cudaSuccess) {
+    rc = fail(FBME_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(e));
+  } else {
+    for (int g = 0; g < n_groups; ++g) {
+      group_ms[g] = 0.f;
+      group_launches[g] = 0;
+    }
+    for (int i = 0; i < prof->n; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, prof->ev[2 * i], prof->ev[2 * i + 1]);
+      const int g = prof->group[i];
+      if (g < n_groups) {
+        group_ms[g] += ms;
+        group_launches[g] += 1;
+      }
+    }
+  }
+  for (int i = 0; i < 2 * fbme::Profiler::kMax; ++i) cudaEventDestroy(prof->ev[i]);
+  delete prof;
+  return rc;
+}
+
 int fbme_plan_state(FbmePlan* plan, FbmeState* st) {
   if (!plan || !st) return fail(FBME_ERR_INVALID, "NULL argument");
   st->mean = plan->u.mu;

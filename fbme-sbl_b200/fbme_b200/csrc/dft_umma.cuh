@@ -69,7 +69,7 @@ struct DftCfg {
   static constexpr int kStageBytes = A_PARTS * kPartBytesA + A_PARTS * kPartBytesB;
   static constexpr int kPairs = A_PARTS == 2 ? 3 : 6;
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*bars*/ +
-                                    64 * sizeof(double) /*reduction scratch*/;
+                                    32 * sizeof(double) /*reduction scratch*/;
   static constexpr uint32_t kIdesc = umma_idesc_bf16(kTileRows, N_TILE);
 };
 
@@ -103,125 +103,198 @@ FBME_DEV void split4(const float4 v, uint2* out) {
   }
 }
 
+// Persistent, warp-specialised stage kernel.  Each CTA loops over tiles
+// (static round-robin); two TMEM accumulators let the epilogue of one tile
+// overlap the tensor-core work of the next.
+//   warps 0-3   producer (128 threads): fetch a whole K chunk of operand
+//               values into registers, then wait for the stage to be free,
+//               split to BF16 parts and store; thread 0 also bulk-copies
+//               the twiddle blocks;
+//   warp 4      TMEM allocation; lane 0 issues tcgen05.mma;
+//   warps 5-7   idle;
+//   warps 8-15  epilogue (256 threads): warp w reads TMEM lanes
+//               32*(w%4).. and half (w-8)/4 of the tile's columns.
+// Per-tile sums are reduced per warp (shuffles only) and written to
+// per-warp slots, so no role ever waits on a barrier another role could
+// abandon after a bounded-wait timeout.
+constexpr int kDftPersistThreads = 512;
+constexpr int kEpiWarp0 = 8;
+constexpr int kEpiThreads = 256;
+constexpr int kProThreads = 128;
+
+FBME_DEV TileCtx decode_tile(const DftGeom& g, int tile) {
+  TileCtx t;
+  t.col_tile = tile % g.col_tiles;
+  tile /= g.col_tiles;
+  t.row_tile = tile % g.row_tiles;
+  t.scene = tile / g.row_tiles;
+  t.g = &g;
+  return t;
+}
+
 template <int A_PARTS, int N_TILE, class Pro, class Epi>
-__global__ void __launch_bounds__(kDftThreads, 1)
-dft_stage_kernel(const DftGeom g, Pro pro, Epi epi, int* status) {
+__global__ void __launch_bounds__(kDftPersistThreads, 1)
+dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* status) {
   using C = DftCfg<A_PARTS, N_TILE>;
   extern __shared__ uint8_t smem_dyn[];
   const uint32_t base_u32 = smem_u32(smem_dyn);
   uint8_t* smem = smem_dyn + (((base_u32 + 1023u) & ~1023u) - base_u32);
   uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + kStages * C::kStageBytes);
   uint64_t* empty_bar = full_bar + kStages;
-  uint64_t* acc_bar = empty_bar + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
-  double* red = reinterpret_cast<double*>(smem + kStages * C::kStageBytes + 256);
+  uint64_t* accf_bar = empty_bar + kStages;  // [2]
+  uint64_t* acce_bar = accf_bar + 2;         // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce_bar + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  TileCtx t;
-  {
-    int tile = blockIdx.x;
-    t.col_tile = tile % g.col_tiles;
-    tile /= g.col_tiles;
-    t.row_tile = tile % g.row_tiles;
-    t.scene = tile / g.row_tiles;
-    t.g = &g;
-  }
+  const int ntiles = g.n_scenes * g.row_tiles * g.col_tiles;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full_bar[s], 128);
+      mbar_init(&full_bar[s], kProThreads);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(acc_bar, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&accf_bar[a], 1);
+      mbar_init(&acce_bar[a], kEpiThreads / 32);
+    }
     fence_mbar_init();
   }
-  if (warp == 4) tmem_alloc(tmem_slot, N_TILE);
+  if (warp == 4) tmem_alloc(tmem_slot, 2 * N_TILE);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  bool ok = true;
-  int* const st_scene = status ? status + t.scene : nullptr;
 
   if (warp < 4) {
     // ---------------- producer ----------------
-    for (int kc = 0; kc < g.kchunks && ok; ++kc) {
-      const int s = kc % kStages, use = kc / kStages;
-      uint8_t* st = smem + s * C::kStageBytes;
-      if (kc >= kStages) ok = mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene);
-      if (!ok) break;
-      if (threadIdx.x == 0) {
-        asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;"
-                     ::"r"(smem_u32(&full_bar[s])), "r"(uint32_t(A_PARTS * C::kPartBytesB))
-                     : "memory");
-        const uint8_t* src = g.table + (static_cast<size_t>(t.col_tile) * g.table_kchunks + kc) *
-                                           A_PARTS * C::kPartBytesB;
-        for (int p = 0; p < A_PARTS; ++p)
-          bulk_g2s(st + A_PARTS * kPartBytesA + p * C::kPartBytesB, src + p * C::kPartBytesB,
-                   C::kPartBytesB, &full_bar[s]);
-      }
-      const int q = lane & 15;
-#pragma unroll 4
-      for (int it = 0; it < 16; ++it) {
-        const int row = warp * 32 + it * 2 + (lane >> 4);
-        const float4 v = pro.load4(t, row, kc * kKChunk + q * 4);
-        uint2 parts[A_PARTS];
-        split4<A_PARTS>(v, parts);
-        const uint32_t off = sw128_offset(row, q * 4);
+    const int tid = threadIdx.x;
+    const int q = lane & 15;
+    bool ok = true;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      const TileCtx t = decode_tile(g, tile);
+      int* const st_scene = status ? status + t.scene : nullptr;
+      for (int kc = 0; kc < g.kchunks && ok; ++kc, ++it) {
+        const int s = it % kStages, use = it / kStages;
+        uint8_t* st = smem + s * C::kStageBytes;
+        constexpr int kB = Pro::kBatch;
+        for (int b0 = 0; b0 < 16; b0 += kB) {
+          typename Pro::Frag f[kB];
 #pragma unroll
-        for (int p = 0; p < A_PARTS; ++p)
-          *reinterpret_cast<uint2*>(st + p * kPartBytesA + off) = parts[p];
+          for (int i = 0; i < kB; ++i) {
+            const int row = warp * 32 + (b0 + i) * 2 + (lane >> 4);
+            pro.fetch(t, row, kc * kKChunk + q * 4, f[i]);
+          }
+          if (b0 == 0) {
+            if (it >= kStages) ok = mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene);
+            if (!ok) break;
+            if (tid == 0) {
+              asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;"
+                           ::"r"(smem_u32(&full_bar[s])), "r"(uint32_t(A_PARTS * C::kPartBytesB))
+                           : "memory");
+              const uint8_t* src = g.table + (static_cast<size_t>(t.col_tile) * g.table_kchunks +
+                                              kc) * A_PARTS * C::kPartBytesB;
+              for (int p = 0; p < A_PARTS; ++p)
+                bulk_g2s(st + A_PARTS * kPartBytesA + p * C::kPartBytesB,
+                         src + p * C::kPartBytesB, C::kPartBytesB, &full_bar[s]);
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < kB; ++i) {
+            const int row = warp * 32 + (b0 + i) * 2 + (lane >> 4);
+            const float4 v = pro.make(t, row, kc * kKChunk + q * 4, f[i]);
+            uint2 parts[A_PARTS];
+            split4<A_PARTS>(v, parts);
+            const uint32_t off = sw128_offset(row, q * 4);
+#pragma unroll
+            for (int p = 0; p < A_PARTS; ++p)
+              *reinterpret_cast<uint2*>(st + p * kPartBytesA + off) = parts[p];
+          }
+        }
+        if (!ok) break;
+        fence_proxy_async_smem();
+        mbar_arrive(&full_bar[s]);
       }
-      fence_proxy_async_smem();
-      mbar_arrive(&full_bar[s]);
+      pro.tile_done(t, warp, lane);
     }
   } else if (warp == 4) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      for (int kc = 0; kc < g.kchunks && ok; ++kc) {
-        const int s = kc % kStages, use = kc / kStages;
-        ok = mbar_wait(&full_bar[s], use & 1, st_scene);
+      bool ok = true;
+      int it = 0, lt = 0;
+      for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
+        const TileCtx t = decode_tile(g, tile);
+        int* const st_scene = status ? status + t.scene : nullptr;
+        const int acc = lt & 1, ause = lt >> 1;
+        if (lt >= 2) ok = mbar_wait(&acce_bar[acc], (ause - 1) & 1, st_scene);
         if (!ok) break;
         tc_fence_after();
-        const uint32_t a0 = smem_u32(smem + s * C::kStageBytes);
-        const uint32_t b0 = a0 + A_PARTS * kPartBytesA;
+        const uint32_t dtm = tmem + static_cast<uint32_t>(acc * N_TILE);
+        for (int kc = 0; kc < g.kchunks && ok; ++kc, ++it) {
+          const int s = it % kStages, use = it / kStages;
+          ok = mbar_wait(&full_bar[s], use & 1, st_scene);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + s * C::kStageBytes);
+          const uint32_t b0 = a0 + A_PARTS * kPartBytesA;
 #pragma unroll
-        for (int kk = 0; kk < kKChunk / 16; ++kk) {
+          for (int kk = 0; kk < kKChunk / 16; ++kk) {
 #pragma unroll
-          for (int pr = 0; pr < C::kPairs; ++pr) {
-            const uint64_t ad = sw128_desc(a0 + kPairA[pr] * kPartBytesA + kk * 32);
-            const uint64_t bd = sw128_desc(b0 + kPairB[pr] * C::kPartBytesB + kk * 32);
-            umma_bf16(tmem, ad, bd, C::kIdesc, (kc | kk | pr) != 0);
+            for (int pr = 0; pr < C::kPairs; ++pr) {
+              const uint64_t ad = sw128_desc(a0 + kPairA[pr] * kPartBytesA + kk * 32);
+              const uint64_t bd = sw128_desc(b0 + kPairB[pr] * C::kPartBytesB + kk * 32);
+              umma_bf16(dtm, ad, bd, C::kIdesc, (kc | kk | pr) != 0);
+            }
           }
+          umma_commit(&empty_bar[s]);
         }
-        umma_commit(&empty_bar[s]);
+        umma_commit(&accf_bar[acc]);
       }
-      umma_commit(acc_bar);
     }
     __syncwarp();
-  }
-
-  // ---------------- epilogue (all warps) ----------------
-  const bool acc_ok = mbar_wait(acc_bar, 0, st_scene);
-  tc_fence_after();
-  if (acc_ok) {
-    const int q = warp & 3, h = warp >> 2;
+  } else if (warp >= kEpiWarp0) {
+    // ---------------- epilogue ----------------
+    const int q = warp & 3, h = (warp - kEpiWarp0) >> 2;
     const int row = q * 32 + lane;
     constexpr int kHalf = N_TILE / 2;
+    bool ok = true;
+    int lt = 0;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
+      const TileCtx t = decode_tile(g, tile);
+      int* const st_scene = status ? status + t.scene : nullptr;
+      const int acc = lt & 1;
+      ok = mbar_wait(&accf_bar[acc], (lt >> 1) & 1, st_scene);
+      tc_fence_after();
+      if (ok) {
+        const uint32_t base = tmem + static_cast<uint32_t>(acc * N_TILE) +
+                              (static_cast<uint32_t>(q * 32) << 16);
+        float va[16], vb[16];
+        tmem_ld16(base + static_cast<uint32_t>(h * kHalf), va);
 #pragma unroll 1
-    for (int c0 = h * kHalf; c0 < (h + 1) * kHalf; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(c0), v);
-      epi.consume(t, row, c0, v);
+        for (int c0 = h * kHalf; c0 < (h + 1) * kHalf; c0 += 32) {
+          const bool more = c0 + 16 < (h + 1) * kHalf;
+          if (more) tmem_ld16_async(base + static_cast<uint32_t>(c0 + 16), vb);
+          epi.consume(t, row, c0, va);
+          if (more) {
+            tmem_wait_ld(vb);
+            const bool more2 = c0 + 32 < (h + 1) * kHalf;
+            if (more2) tmem_ld16_async(base + static_cast<uint32_t>(c0 + 32), va);
+            epi.consume(t, row, c0 + 16, vb);
+            if (more2) tmem_wait_ld(va);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce_bar[acc]);
+      epi.tile_done(t, warp - kEpiWarp0, lane);
     }
   }
-  epi.finish(t, red);
-  pro.finish(t, red);
   tc_fence_before();
   __syncthreads();
   if (warp == 4) {
     tc_fence_after();
-    tmem_dealloc(tmem, N_TILE);
+    tmem_dealloc(tmem, 2 * N_TILE);
   }
 }
 
@@ -238,20 +311,23 @@ FBME_DEV float4 load_row4(const float2* base, const TileCtx& t, int row, int kre
   if (r >= g.rows || j0 >= g.kcplx) return make_float4(0.f, 0.f, 0.f, 0.f);
   const float2* p = base + t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
   if (j0 + 1 < g.kcplx) {
-    if (g.vec4) return *reinterpret_cast<const float4*>(p);
-    const float2 a = p[0], b = p[1];
+    if (g.vec4) return __ldg(reinterpret_cast<const float4*>(p));
+    const float2 a = __ldg(p), b = __ldg(p + 1);
     return make_float4(a.x, a.y, b.x, b.y);
   }
-  const float2 a = p[0];
+  const float2 a = __ldg(p);
   return make_float4(a.x, a.y, 0.f, 0.f);
 }
 
 struct ProPlain {
+  static constexpr int kBatch = 16;
+  using Frag = float4;
   const float2* in;
-  FBME_DEV float4 load4(const TileCtx& t, int row, int kreal) const {
-    return load_row4(in, t, row, kreal);
+  FBME_DEV void fetch(const TileCtx& t, int row, int kreal, Frag& f) const {
+    f = load_row4(in, t, row, kreal);
   }
-  FBME_DEV void finish(const TileCtx&, double*) {}
+  FBME_DEV float4 make(const TileCtx&, int, int, const Frag& f) const { return f; }
+  FBME_DEV void tile_done(const TileCtx&, int, int) {}
 };
 
 // Store Out[j][r] (lane-contiguous) as complex64.
@@ -268,7 +344,7 @@ struct EpiStoreT {
       if (j < g.cols) o[static_cast<long long>(j) * g.out_ld] = make_float2(v[2 * i], v[2 * i + 1]);
     }
   }
-  FBME_DEV void finish(const TileCtx&, double*) {}
+  FBME_DEV void tile_done(const TileCtx&, int, int) {}
 };
 
 }  // namespace fbme

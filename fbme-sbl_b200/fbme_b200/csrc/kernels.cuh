@@ -8,8 +8,16 @@
 
 namespace fbme {
 
+#define FBME_TIMED(prof, g, launch) \
+  do {                              \
+    if (prof) (prof)->begin(g);     \
+    launch;                         \
+    if (prof) (prof)->end();        \
+  } while (0)
+
 constexpr int kMaxTilesPerScene = 64;  // partial-sum slots per scene and stage
-constexpr int kPartSlots = 4;          // reductions carried per tile
+constexpr int kPartWarps = 8;          // per-warp partial sums kept per tile and reduction
+constexpr int kPartSlots = 4 * kPartWarps;  // 4 reductions x 8 warps per tile
 constexpr int kMaxPolish = 32;         // active-set capacity of the warp polish
 
 // Per-scene scalar state, structure of arrays of length B (device).
@@ -48,6 +56,27 @@ struct DevConfig {
   int uamp_iters;
 };
 
+// Optional per-launch event timing (fbme_plan_profile); nullptr otherwise.
+struct Profiler {
+  static constexpr int kMax = 512;
+  cudaEvent_t ev[2 * kMax];
+  int group[kMax];
+  int n = 0;
+  cudaStream_t st = nullptr;
+  void begin(int g) {
+    if (n < kMax) {
+      group[n] = g;
+      cudaEventRecord(ev[2 * n], st);
+    }
+  }
+  void end() {
+    if (n < kMax) {
+      cudaEventRecord(ev[2 * n + 1], st);
+      ++n;
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // launchers (all asynchronous on `st`)
 // ---------------------------------------------------------------------------
@@ -80,7 +109,7 @@ void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float
 void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
                  float2* coeff, float2* tmp, int* status, cudaStream_t st);
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
-              cudaStream_t st);
+              cudaStream_t st, Profiler* prof = nullptr);
 
 // Active-set stage.
 struct PolishBuffers {
@@ -100,7 +129,7 @@ struct PolishBuffers {
   int* status;        // [B] per-scene status
 };
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
-                const FbmeOutputs& out, cudaStream_t st);
+                const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
 size_t polish_state_bytes();
 
 }  // namespace fbme

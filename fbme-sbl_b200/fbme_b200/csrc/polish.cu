@@ -604,22 +604,26 @@ void launch_topk(const uint32_t* keys, long long n, int k, int B, int* out_idx, 
                  cudaStream_t st);
 
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
-                const FbmeOutputs& out, cudaStream_t st) {
+                const FbmeOutputs& out, cudaStream_t st, Profiler* prof) {
   PolishArgs A{s, c, p};
   const int K = c.polish_size;
-  launch_topk(p.keys, s.n(), K, s.B, p.active, p.score, st);
-  polish_kernel<<<s.B, 32, 0, st>>>(A, 0);
+  FBME_TIMED(prof, FBME_GROUP_TOPK, launch_topk(p.keys, s.n(), K, s.B, p.active, p.score, st));
+  FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, 0, st>>>(A, 0)));
   if (c.exchange > 0 && c.polish_iters > 1) {
     const int blocks = static_cast<int>((s.n() + 256 * 16 - 1) / (256 * 16));
     const size_t shm = (s.n1 + s.n2 + kMaxPolish) * sizeof(float2) + 2 * kMaxPolish * sizeof(int);
-    exchange_score_kernel<<<dim3(blocks < 64 ? blocks : 64, s.B), 256, shm, st>>>(A, p.keys);
-    launch_topk(p.keys, s.n(), c.exchange, s.B, p.xcand_idx, p.xcand_val, st);
-    polish_kernel<<<s.B, 32, 0, st>>>(A, 1);
+    FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
+               (exchange_score_kernel<<<dim3(blocks < 64 ? blocks : 64, s.B), 256, shm, st>>>(
+                   A, p.keys)));
+    FBME_TIMED(prof, FBME_GROUP_TOPK,
+               launch_topk(p.keys, s.n(), c.exchange, s.B, p.xcand_idx, p.xcand_val, st));
+    FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, 0, st>>>(A, 1)));
   }
-  polish_finish_kernel<<<s.B, 32, 0, st>>>(A, out);
+  FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, 0, st>>>(A, out)));
   const int fb = static_cast<int>((s.n() + 2047) / 2048);
-  output_fill_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(s, p.sc, out);
-  output_scatter_kernel<<<s.B, 32, 0, st>>>(A, out);
+  FBME_TIMED(prof, FBME_GROUP_OUTPUT,
+             (output_fill_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(s, p.sc, out)));
+  FBME_TIMED(prof, FBME_GROUP_OUTPUT, (output_scatter_kernel<<<s.B, 32, 0, st>>>(A, out)));
 }
 
 }  // namespace fbme

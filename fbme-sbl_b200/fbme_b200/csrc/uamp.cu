@@ -37,19 +37,25 @@ FBME_DEV void write_block_partial(double v, double* red, double* part, int scene
   const double s = block_sum(v, red);
   if (threadIdx.x == 0) *part_slot(part, scene, tile, slot) = s;
 }
-FBME_DEV int tile_in_scene(const TileCtx& t) { return t.row_tile * t.g->col_tiles + t.col_tile; }
+// Reduction `sum` of one tile: warp `w` (of the stage's producer or
+// epilogue group) writes its warp total to slot sum*kPartWarps + w.
+FBME_DEV void warp_partial(double v, double* part, const TileCtx& t, int sum, int w, int lane) {
+  v = warp_sum(v);
+  if (lane == 0)
+    *part_slot(part, t.scene, t.row_tile * t.g->col_tiles + t.col_tile, sum * kPartWarps + w) = v;
+}
 
 FBME_DEV bool vec_ok(const DftGeom& g) { return g.vec4 != 0; }
 
-// Two consecutive complex values at base[e], e in [0, limit).
+// Two consecutive complex values at base[e] through the read-only path.
 FBME_DEV void load2c(const float2* base, long long e, int avail, bool vec, float2& a, float2& b) {
   if (avail >= 2 && vec) {
-    const float4 v = *reinterpret_cast<const float4*>(base + e);
+    const float4 v = __ldg(reinterpret_cast<const float4*>(base + e));
     a = make_float2(v.x, v.y);
     b = make_float2(v.z, v.w);
   } else {
-    a = base[e];
-    b = avail >= 2 ? base[e + 1] : make_float2(0.f, 0.f);
+    a = __ldg(base + e);
+    b = avail >= 2 ? __ldg(base + e + 1) : make_float2(0.f, 0.f);
   }
 }
 
@@ -57,21 +63,26 @@ FBME_DEV void load2c(const float2* base, long long e, int avail, bool vec, float
 // prologues
 // ---------------------------------------------------------------------------
 
-// Plain load; also sums |y|^2 (for the data power) over the column-tile-0 CTAs.
+// Plain load; also sums |y|^2 (for the data power) over the column-tile-0 tiles.
 struct ProYPower {
+  static constexpr int kBatch = 16;
+  using Frag = float4;
   const float2* in;
   double* part;
   float acc;
-  FBME_DEV float4 load4(const TileCtx& t, int row, int kreal) {
-    const float4 v = load_row4(in, t, row, kreal);
+  FBME_DEV void fetch(const TileCtx& t, int row, int kreal, Frag& f) const {
+    f = load_row4(in, t, row, kreal);
+  }
+  FBME_DEV float4 make(const TileCtx& t, int, int, const Frag& v) {
     if (t.col_tile == 0) {
       acc += abs_sq(make_float2(v.x, v.y));
       acc += abs_sq(make_float2(v.z, v.w));
     }
     return v;
   }
-  FBME_DEV void finish(const TileCtx& t, double* red) {
-    write_block_partial(acc, red, part, t.scene, tile_in_scene(t), 0);
+  FBME_DEV void tile_done(const TileCtx& t, int w, int lane) {
+    warp_partial(acc, part, t, 3, w, lane);
+    acc = 0.f;
   }
 };
 
@@ -80,22 +91,35 @@ struct ProYPower {
 // writes the new one to `msg_out` (column tile 0 only) and feeds it to the
 // tensor core.
 struct ProMessage {
+  static constexpr int kBatch = 8;
+  struct Frag {
+    float2 y0, y1, p0, p1, m0, m1;
+  };
   const float2 *y, *pred, *msg_in;
   float2* msg_out;
   const float *prec, *dvar;
   float damping;
-  FBME_DEV float4 load4(const TileCtx& t, int row, int kreal) {
+  FBME_DEV void fetch(const TileCtx& t, int row, int kreal, Frag& f) const {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    const int j0 = kreal >> 1;
+    if (r >= g.rows || j0 >= g.kcplx) {
+      f.y0 = f.y1 = f.p0 = f.p1 = f.m0 = f.m1 = make_float2(0.f, 0.f);
+      return;
+    }
+    const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
+    const int avail = g.kcplx - j0;
+    const bool vec = vec_ok(g);
+    load2c(y, e, avail, vec, f.y0, f.y1);
+    load2c(pred, e, avail, vec, f.p0, f.p1);
+    load2c(msg_in, e, avail, vec, f.m0, f.m1);
+  }
+  FBME_DEV float4 make(const TileCtx& t, int row, int kreal, const Frag& f) const {
     const DftGeom& g = *t.g;
     const int r = t.row0() + row;
     const int j0 = kreal >> 1;
     if (r >= g.rows || j0 >= g.kcplx) return make_float4(0.f, 0.f, 0.f, 0.f);
-    const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
     const int avail = g.kcplx - j0;
-    const bool vec = vec_ok(g);
-    float2 y0, y1, p0, p1, m0, m1;
-    load2c(y, e, avail, vec, y0, y1);
-    load2c(pred, e, avail, vec, p0, p1);
-    load2c(msg_in, e, avail, vec, m0, m1);
     const float pr = prec[t.scene], dv = dvar[t.scene];
     const float keep = damping, upd = 1.0f - damping;
     auto step = [&](float2 yy, float2 pp, float2 mm) {
@@ -103,15 +127,20 @@ struct ProMessage {
       const float2 cand = make_float2(pr * (yy.x - pseudo.x), pr * (yy.y - pseudo.y));
       return make_float2(keep * mm.x + upd * cand.x, keep * mm.y + upd * cand.y);
     };
-    const float2 o0 = step(y0, p0, m0);
-    const float2 o1 = avail >= 2 ? step(y1, p1, m1) : make_float2(0.f, 0.f);
+    const float2 o0 = step(f.y0, f.p0, f.m0);
+    const float2 o1 = avail >= 2 ? step(f.y1, f.p1, f.m1) : make_float2(0.f, 0.f);
     if (t.col_tile == 0) {
-      msg_out[e] = o0;
-      if (avail >= 2) msg_out[e + 1] = o1;
+      const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
+      if (avail >= 2 && vec_ok(g)) {
+        *reinterpret_cast<float4*>(msg_out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
+      } else {
+        msg_out[e] = o0;
+        if (avail >= 2) msg_out[e + 1] = o1;
+      }
     }
     return make_float4(o0.x, o0.y, o1.x, o1.y);
   }
-  FBME_DEV void finish(const TileCtx&, double*) {}
+  FBME_DEV void tile_done(const TileCtx&, int, int) {}
 };
 
 // ---------------------------------------------------------------------------
@@ -129,21 +158,26 @@ struct EpiPredict {
     const int r = t.row0() + row;
     if (r >= g.rows) return;
     const long long base = t.scene * g.out_stride + r;
+    float2 yy[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = t.col0() + (c0 >> 1) + i;
+      yy[i] = j < g.cols ? __ldg(y + base + static_cast<long long>(j) * g.out_ld) : make_float2(0.f, 0.f);
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int j = t.col0() + (c0 >> 1) + i;
       if (j < g.cols) {
-        const long long e = base + static_cast<long long>(j) * g.out_ld;
         const float2 p = make_float2(v[2 * i], v[2 * i + 1]);
-        pred[e] = p;
-        const float2 yy = y[e];
-        const float dr = yy.x - p.x, di = yy.y - p.y;
+        pred[base + static_cast<long long>(j) * g.out_ld] = p;
+        const float dr = yy[i].x - p.x, di = yy[i].y - p.y;
         acc += dr * dr + di * di;
       }
     }
   }
-  FBME_DEV void finish(const TileCtx& t, double* red) {
-    write_block_partial(acc, red, part, t.scene, tile_in_scene(t), 2);
+  FBME_DEV void tile_done(const TileCtx& t, int w, int lane) {
+    warp_partial(acc, part, t, 2, w, lane);
+    acc = 0.f;
   }
 };
 
@@ -167,8 +201,9 @@ struct EpiBackprojection {
       }
     }
   }
-  FBME_DEV void finish(const TileCtx& t, double* red) {
-    write_block_partial(acc, red, part, t.scene, tile_in_scene(t), 1);
+  FBME_DEV void tile_done(const TileCtx& t, int w, int lane) {
+    warp_partial(acc, part, t, 1, w, lane);
+    acc = 0.f;
   }
 };
 
@@ -191,11 +226,11 @@ FBME_DEV uint32_t float_key(float f) {
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
-FBME_DEV void denoise_one(const DenoiseArgs& a, int scene, long long e, float2 lifted, float pv,
-                          float floor_, float& dof_acc, float& var_acc) {
-  const float prior = a.gamma[e];
-  const float2 old_mean = a.mu[e];
-  const float old_var = fmaxf(a.var[e], kTiny);
+// One coefficient of the denoiser; writes mu, v (and gamma / key) at e.
+FBME_DEV void denoise_core(const DenoiseArgs& a, long long e, float prior, float2 old_mean,
+                           float old_var_raw, float2 lifted, float pv, float floor_,
+                           float& dof_acc, float& var_acc) {
+  const float old_var = fmaxf(old_var_raw, kTiny);
   const float denom = fmaxf(prior + pv, kTiny);
   const float gain = prior / denom;
   const float2 pm = make_float2(old_mean.x + pv * lifted.x, old_mean.y + pv * lifted.y);
@@ -229,17 +264,32 @@ struct EpiDenoise {
     if (r >= g.rows) return;
     const float pv = a.pv[t.scene], fl = a.floor_[t.scene];
     const long long base = t.scene * g.out_stride + r;
+    // all loads of the chunk first (independent addresses, in flight together)
+    float pri[8], ov[8];
+    float2 om[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = t.col0() + (c0 >> 1) + i;
+      if (j < g.cols) {
+        const long long e = base + static_cast<long long>(j) * g.out_ld;
+        pri[i] = a.gamma[e];
+        om[i] = a.mu[e];
+        ov[i] = a.var[e];
+      }
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int j = t.col0() + (c0 >> 1) + i;
       if (j < g.cols)
-        denoise_one(a, t.scene, base + static_cast<long long>(j) * g.out_ld,
-                    make_float2(v[2 * i], v[2 * i + 1]), pv, fl, dof_acc, var_acc);
+        denoise_core(a, base + static_cast<long long>(j) * g.out_ld, pri[i], om[i], ov[i],
+                     make_float2(v[2 * i], v[2 * i + 1]), pv, fl, dof_acc, var_acc);
     }
   }
-  FBME_DEV void finish(const TileCtx& t, double* red) {
-    write_block_partial(dof_acc, red, a.part, t.scene, tile_in_scene(t), 0);
-    write_block_partial(var_acc, red, a.part, t.scene, tile_in_scene(t), 1);
+  FBME_DEV void tile_done(const TileCtx& t, int w, int lane) {
+    warp_partial(dof_acc, a.part, t, 0, w, lane);
+    warp_partial(var_acc, a.part, t, 1, w, lane);
+    dof_acc = 0.f;
+    var_acc = 0.f;
   }
 };
 
@@ -283,7 +333,7 @@ __global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevCon
     gamma[e] = g;
     acc += g;
   }
-  write_block_partial(acc, red, part, scene, blockIdx.x, 0);
+  write_block_partial(acc, red, part, scene, blockIdx.x, 0 * kPartWarps);
 }
 
 // First sweep: the lifted message is (1-d)/(dv+nv) * A^H y, the previous
@@ -315,49 +365,56 @@ __global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevCon
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<long long>(nblk_n) * blockDim.x) {
     const long long e = scene * n + i;
-    a.mu[e] = make_float2(0.f, 0.f);
-    a.var[e] = a.gamma[e];
+    const float g0 = a.gamma[e];
     const float2 b = bp[e];
-    denoise_one(a, scene, e, make_float2(scale * b.x, scale * b.y), pv, fl, dof, sv);
+    denoise_core(a, e, g0, make_float2(0.f, 0.f), g0, make_float2(scale * b.x, scale * b.y), pv, fl,
+                 dof, sv);
   }
-  write_block_partial(dof, red, a.part, scene, blockIdx.x, 0);
-  write_block_partial(sv, red, a.part, scene, blockIdx.x, 1);
+  write_block_partial(dof, red, a.part, scene, blockIdx.x, 0 * kPartWarps);
+  write_block_partial(sv, red, a.part, scene, blockIdx.x, 1 * kPartWarps);
 }
 
 // Per-scene scalar updates from the per-tile sums (fixed summation order).
 enum ScalarMode { kScalarInit1 = 0, kScalarInit2 = 1, kScalarSweep = 2 };
 
+// Partial-sum source of one reduction: tiles x warps per tile.
+struct PartSrc {
+  int tiles, warps;
+};
+
 __global__ void scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part,
-                               int nt0, int nt1, int nt2) {
+                               PartSrc p0, PartSrc p1, PartSrc p2) {
   const int scene = blockIdx.x * blockDim.x + threadIdx.x;
   if (scene >= s.B) return;
-  auto sum = [&](int slot, int nt) {
+  auto sum = [&](int id, PartSrc src) {
     double v = 0.0;
-    for (int t = 0; t < nt; ++t)
-      v += part[(static_cast<long long>(scene) * kMaxTilesPerScene + t) * kPartSlots + slot];
+    for (int t = 0; t < src.tiles; ++t)
+      for (int w = 0; w < src.warps; ++w)
+        v += part[(static_cast<long long>(scene) * kMaxTilesPerScene + t) * kPartSlots +
+                  id * kPartWarps + w];
     return v;
   };
   const float M = static_cast<float>(s.m());
   if (mode == kScalarInit1) {
-    const double ysum = sum(0, nt0);
+    const double ysum = sum(3, p0);
     const float dp = fmaxf(static_cast<float>(ysum / static_cast<double>(s.m())), kEps);
     const float fl = fmaxf(dp * c.min_var, kTiny);
     sc.data_power[scene] = dp;
     sc.floor_[scene] = fl;
     sc.data_energy[scene] = static_cast<float>(ysum);
-    sc.ebp[scene] = static_cast<float>(sum(1, nt1));
+    sc.ebp[scene] = static_cast<float>(sum(1, p1));
     sc.noise[scene] = c.fixed_noise > 0.f ? c.fixed_noise : fmaxf(c.init_noise * dp, fl);
   } else if (mode == kScalarInit2) {
-    const float dv = fmaxf(static_cast<float>(sum(0, nt0)), kTiny);
+    const float dv = fmaxf(static_cast<float>(sum(0, p0)), kTiny);
     const float nv = sc.noise[scene];
     sc.dvar[scene] = dv;
     sc.pv[scene] = fmaxf((dv + nv) / M, kTiny);
     sc.prec[scene] = 1.0f / (dv + nv);
   } else {
     const float max_dof = static_cast<float>(static_cast<double>(s.m()) * (1.0 - 10.0 * kEps));
-    const float dof = fminf(static_cast<float>(sum(0, nt0)), max_dof);
-    const float sv = static_cast<float>(sum(1, nt1));
-    const float energy = static_cast<float>(sum(2, nt2));
+    const float dof = fminf(static_cast<float>(sum(0, p0)), max_dof);
+    const float sv = static_cast<float>(sum(1, p1));
+    const float energy = static_cast<float>(sum(2, p2));
     const float fl = sc.floor_[scene];
     float nv = sc.noise[scene];
     if (!(c.fixed_noise > 0.f)) {
@@ -429,6 +486,22 @@ static DftGeom stage_geom(Stage st, const BatchShape& s, const DftTables& t, int
 
 static int tiles(const DftGeom& g) { return g.n_scenes * g.row_tiles * g.col_tiles; }
 
+static int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+      n = 148;
+  }
+  return n;
+}
+
+static int persistent_grid(const DftGeom& g) {
+  const int t = tiles(g), s = sm_count();
+  return t < s ? t : s;
+}
+
 template <int A_PARTS, int N_TILE, class Pro, class Epi>
 static cudaError_t set_attr() {
   return cudaFuncSetAttribute(dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>,
@@ -441,10 +514,12 @@ static void run_stage(int terms, const DftGeom& g, const Pro& pro, const Epi& ep
                       cudaStream_t st) {
   if (terms == 6) {
     dft_stage_kernel<3, 128, Pro, Epi>
-        <<<tiles(g), kDftThreads, DftCfg<3, 128>::kSmemBytes, st>>>(g, pro, epi, status);
+        <<<persistent_grid(g), kDftPersistThreads, DftCfg<3, 128>::kSmemBytes, st>>>(g, pro, epi,
+                                                                                     status);
   } else {
     dft_stage_kernel<2, 256, Pro, Epi>
-        <<<tiles(g), kDftThreads, DftCfg<2, 256>::kSmemBytes, st>>>(g, pro, epi, status);
+        <<<persistent_grid(g), kDftPersistThreads, DftCfg<2, 256>::kSmemBytes, st>>>(g, pro, epi,
+                                                                                     status);
   }
 }
 
@@ -487,7 +562,7 @@ void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float
 // Message buffers ping-pong between sweeps: msg[0] / msg[1] are both
 // M-sized regions starting at u.msg and u.msg + B*M.
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
-              cudaStream_t st) {
+              cudaStream_t st, Profiler* prof) {
   const int nt = n_tile_of(c.terms);
   const DftGeom f1 = stage_geom(kFwd1, s, t, nt), f2 = stage_geom(kFwd2, s, t, nt);
   const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
@@ -496,14 +571,23 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   float2* msg[2] = {u.msg, u.msg + BM};
 
   // --- initialisation: A^H y, data power, floors, initial noise, prior ---
-  run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st);
-  run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f}, u.status, st);
-  scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit1, s, c, u.sc, u.part,
-                                            a1.row_tiles * a1.col_tiles,
-                                            a2.row_tiles * a2.col_tiles, 0);
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f},
+                       u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(
+                 kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, 4},
+                 PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
   const int bn = ew_blocks_host(s.n()), bm = ew_blocks_host(s.m());
-  gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma, u.part);
-  scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit2, s, c, u.sc, u.part, bn, 0, 0);
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             (gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma,
+                                                                  u.part)));
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit2, s, c, u.sc, u.part,
+                                                        PartSrc{bn, 1}, PartSrc{0, 0},
+                                                        PartSrc{0, 0})));
 
   DenoiseArgs da;
   da.mu = u.mu;
@@ -523,33 +607,44 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   // --- sweeps ---
   int cur = 0;  // msg[cur] holds the latest message
   for (int it = 1; it <= c.uamp_iters; ++it) {
-    int nt_dof;
+    PartSrc src_dof;
     if (it == 1) {
-      sweep1_kernel<<<dim3(bn + bm, s.B), kEwThreads, 0, st>>>(s, c, u.sc, da, u.bp, u.y,
-                                                               msg[cur], bn);
-      nt_dof = bn;
+      FBME_TIMED(prof, FBME_GROUP_SWEEP1,
+                 (sweep1_kernel<<<dim3(bn + bm, s.B), kEwThreads, 0, st>>>(s, c, u.sc, da, u.bp,
+                                                                           u.y, msg[cur], bn)));
+      src_dof = PartSrc{bn, 1};
     } else {
-      run_stage(c.terms, a1,
-                ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar,
-                           c.uamp_damping},
-                EpiStoreT{u.tmp}, u.status, st);
+      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+                 run_stage(c.terms, a1,
+                           ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar,
+                                      c.uamp_damping},
+                           EpiStoreT{u.tmp}, u.status, st));
       cur ^= 1;
-      run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st);
-      nt_dof = a2.row_tiles * a2.col_tiles;
+      FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
+                 run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st));
+      src_dof = PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps};
     }
-    run_stage(c.terms, f1, ProPlain{u.mu}, EpiStoreT{u.tmp}, u.status, st);
-    run_stage(c.terms, f2, ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f}, u.status, st);
-    scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarSweep, s, c, u.sc, u.part, nt_dof, nt_dof,
-                                              f2.row_tiles * f2.col_tiles);
+    FBME_TIMED(prof, FBME_GROUP_FWD_1,
+               run_stage(c.terms, f1, ProPlain{u.mu}, EpiStoreT{u.tmp}, u.status, st));
+    FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL,
+               run_stage(c.terms, f2, ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f},
+                         u.status, st));
+    FBME_TIMED(prof, FBME_GROUP_SCALARS,
+               (scalars_kernel<<<sc_blocks, 128, 0, st>>>(
+                   kScalarSweep, s, c, u.sc, u.part, src_dof, src_dof,
+                   PartSrc{f2.row_tiles * f2.col_tiles, kPartWarps})));
   }
 
   // --- final E-step (no prior update, no prediction), score keys ---
-  run_stage(c.terms, a1,
-            ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar, c.uamp_damping},
-            EpiStoreT{u.tmp}, u.status, st);
+  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+             run_stage(c.terms, a1,
+                       ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar,
+                                  c.uamp_damping},
+                       EpiStoreT{u.tmp}, u.status, st));
   da.update_prior = 0;
   da.keys = reinterpret_cast<uint32_t*>(u.keys);
-  run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st);
+  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
+             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st));
 }
 
 }  // namespace fbme

@@ -188,6 +188,20 @@ class FBMEEngine:
                                            ctypes.byref(self._outputs),
                                            ctypes.c_void_p(self._stream())), "fbme_polish_run")
 
+    def profile(self, y: Tensor) -> dict[str, tuple[float, int]]:
+        """One eagerly launched replay with CUDA events around every kernel:
+        {group name: (device ms summed over launches, launches)}."""
+        self._check_y(y)
+        n = nat.NUM_GROUPS
+        ms = (ctypes.c_float * n)()
+        cnt = (ctypes.c_int32 * n)()
+        nat.check(self.lib.fbme_plan_profile(self._plan, ctypes.c_void_p(y.data_ptr()),
+                                             ctypes.byref(self._outputs),
+                                             ctypes.c_void_p(self._stream()), ms, cnt, n),
+                  "fbme_plan_profile")
+        return {self.lib.fbme_profile_group_name(g).decode(): (float(ms[g]), int(cnt[g]))
+                for g in range(n)}
+
     def dft_forward(self, coeff: Tensor) -> Tensor:
         """A(X) for [B, N] complex64 coefficients -> [B, M] data."""
         self._check(coeff, self.n_grid)

@@ -153,6 +153,29 @@ int fbme_uamp_run(FbmePlan* plan, const void* y, fbme_stream_t stream);
 int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream);
 int fbme_plan_state(FbmePlan* plan, FbmeState* state);
 
+/* Kernel groups timed by fbme_plan_profile. */
+enum {
+  FBME_GROUP_INIT = 0,        /* A^H y, data power, prior/noise initialisation */
+  FBME_GROUP_ADJ_MESSAGE = 1, /* adjoint stage 1 with the fused message update */
+  FBME_GROUP_ADJ_DENOISE = 2, /* adjoint stage 2 with the fused denoiser / ARD update */
+  FBME_GROUP_FWD_1 = 3,       /* forward stage 1 */
+  FBME_GROUP_FWD_RESIDUAL = 4,/* forward stage 2 with the fused residual energy */
+  FBME_GROUP_SCALARS = 5,     /* per-scene noise / variance updates */
+  FBME_GROUP_SWEEP1 = 6,      /* first-sweep denoiser (reuses A^H y) */
+  FBME_GROUP_TOPK = 7,        /* top-K selections */
+  FBME_GROUP_POLISH = 8,      /* reduced posterior, gate, EM, diagnostics */
+  FBME_GROUP_EXCHANGE = 9,    /* residual exchange scoring over the grid */
+  FBME_GROUP_OUTPUT = 10,     /* dense outputs */
+  FBME_NUM_GROUPS = 11
+};
+
+/* One replay with CUDA events around every kernel launch (not capturable;
+ * synchronises `stream`).  group_ms[g] receives the summed device time of
+ * group g and group_launches[g] its launch count, for g < n_groups. */
+int fbme_plan_profile(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream,
+                      float* group_ms, int32_t* group_launches, int32_t n_groups);
+const char* fbme_profile_group_name(int32_t group);
+
 /* Thread-local description of the last failure ("" if none). */
 const char* fbme_last_error(void);
 /* Library version string. */

@@ -1,0 +1,72 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares;
+host-side validation returns the documented codes without touching a GPU."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from fbme_b200 import _native as nat
+
+HEADERS = sorted((Path(__file__).resolve().parents[1] / "include").glob("*.h"))
+
+
+def _declared():
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(fbme_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_every_declared_symbol_is_exported_and_bound():
+    lib = nat.lib()
+    declared = _declared()
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared <= set(nat.SIGNATURES), declared - set(nat.SIGNATURES)
+
+
+def test_version_and_group_names():
+    lib = nat.lib()
+    assert b"sm_100a" in lib.fbme_version()
+    names = [lib.fbme_profile_group_name(g).decode() for g in range(nat.NUM_GROUPS)]
+    assert names[2] == "adjoint_denoise" and all(names)
+
+
+def _cfg(**kw):
+    from fbme_b200.config import SBLConfig
+    from fbme_b200.engine import resolve_native_config
+
+    cfg = SBLConfig.paper_hybrid_uamp(uamp_polish_size=32, **kw)
+    return resolve_native_config(cfg, (256, 256), (128, 128))
+
+
+def test_workspace_bytes_and_validation_codes():
+    lib = nat.lib()
+    c = _cfg()
+    shapes = (nat.FbmeShape * 2)(nat.FbmeShape(256, 256, 128, 128), nat.FbmeShape(256, 256, 128, 128))
+    nbytes = lib.fbme_plan_workspace_bytes(shapes, 2, ctypes.byref(c))
+    assert nbytes > 2 * 256 * 256 * 8
+    bad = (nat.FbmeShape * 1)(nat.FbmeShape(64, 64, 128, 32))
+    assert lib.fbme_plan_workspace_bytes(bad, 1, ctypes.byref(c)) == 0
+    plan = ctypes.c_void_p()
+    rc = lib.fbme_plan_create(bad, 1, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
+    assert rc == nat.FBME_ERR_INVALID and "0 < M <= N" in nat.last_error()
+    uneven = (nat.FbmeShape * 2)(nat.FbmeShape(64, 64, 32, 32), nat.FbmeShape(128, 64, 32, 32))
+    rc = lib.fbme_plan_create(uneven, 2, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
+    assert rc == nat.FBME_ERR_UNSUPPORTED
+    rc = lib.fbme_plan_create(shapes, 2, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
+    assert rc == nat.FBME_ERR_WORKSPACE
+    big = _cfg()
+    big.polish_size = 64
+    rc = lib.fbme_plan_create(shapes, 2, ctypes.byref(big), None, 0, None, ctypes.byref(plan))
+    assert rc == nat.FBME_ERR_UNSUPPORTED
+    with pytest.raises(ValueError):
+        nat.check(nat.FBME_ERR_INVALID, "x")
+    with pytest.raises(NotImplementedError):
+        nat.check(nat.FBME_ERR_UNSUPPORTED, "x")
+    with pytest.raises(RuntimeError):
+        nat.check(nat.FBME_ERR_CUDA, "x")
