@@ -30,7 +30,7 @@ size_t table_bytes(int L, int terms) {
 struct Layout {
   size_t tab_f2, tab_f1, tab_a2, tab_a1, dir1, dir2;
   size_t mu, bp, var, gamma, msg, pred, tmp, keys, part, scal;
-  size_t active, score, pstate, xval, xidx, status;
+  size_t active, score, pstate, xval, xidx, status, ckey, cidx;
   size_t total;
 };
 
@@ -73,6 +73,11 @@ Layout make_layout(const fbme::BatchShape& s, const FbmeConfig& c) {
   L.xval = take(B * E * sizeof(float));
   L.xidx = take(B * E * sizeof(int));
   L.status = take(B * sizeof(int));
+  const size_t c1 = static_cast<size_t>(fbme::topk_slices(s.n())) * K;
+  const size_t c2 = static_cast<size_t>(fbme::exchange_blocks(s)) * E;
+  const size_t nc = c1 > c2 ? c1 : c2;
+  L.ckey = take(B * nc * sizeof(uint32_t));
+  L.cidx = take(B * nc * sizeof(int));
   L.total = off;
   return L;
 }
@@ -112,6 +117,10 @@ int validate(const FbmeShape* shapes, int n, const FbmeConfig* c, fbme::BatchSha
   if (!(c->uamp_damping >= 0.f && c->uamp_damping < 1.f) || !(c->damping >= 0.f && c->damping < 1.f))
     return fail(FBME_ERR_INVALID, "damping values must be in [0, 1)");
   if (1LL * s0.n1 * s0.n2 * n > (1LL << 40)) return fail(FBME_ERR_INVALID, "batch too large");
+  if (N > 524288 || s0.n2 > 512)
+    return fail(FBME_ERR_UNSUPPORTED, "grids above 524288 points or N2 > 512 are not built");
+  if (static_cast<long long>((s0.n1 + 15) / 16) * c->exchange_size > 2048)
+    return fail(FBME_ERR_UNSUPPORTED, "exchange candidate count above 2048");
   out->B = n;
   out->n1 = s0.n1;
   out->n2 = s0.n2;
@@ -254,6 +263,8 @@ int fbme_plan_create(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig
   p.xcand_val = reinterpret_cast<float*>(w + L.xval);
   p.xcand_idx = reinterpret_cast<int*>(w + L.xidx);
   p.keys = u.keys;
+  p.cand_key = reinterpret_cast<uint32_t*>(w + L.ckey);
+  p.cand_idx = reinterpret_cast<int*>(w + L.cidx);
   p.status = P->status;
 
   e = cudaGetLastError();

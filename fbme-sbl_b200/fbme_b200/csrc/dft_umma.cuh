@@ -82,24 +82,21 @@ FBME_DEV uint16_t bf16_bits(float x) {
 }
 FBME_DEV float bf16_val(uint16_t b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
 
-// Split four floats into A_PARTS packed bf16 quads (2 x uint32 each).
+// Split four floats into A_PARTS packed bf16 quads (2 x uint32 each):
+// part t holds bf16(x - sum of earlier parts); the subtraction is exact.
 template <int A_PARTS>
 FBME_DEV void split4(const float4 v, uint2* out) {
-  float x[4] = {v.x, v.y, v.z, v.w};
-  uint16_t p[3][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    float r = x[i];
-#pragma unroll
-    for (int t = 0; t < A_PARTS; ++t) {
-      p[t][i] = bf16_bits(r);
-      r = r - bf16_val(p[t][i]);  // exact in FP32
-    }
-  }
+  float2 a = make_float2(v.x, v.y), b = make_float2(v.z, v.w);
 #pragma unroll
   for (int t = 0; t < A_PARTS; ++t) {
-    out[t].x = static_cast<uint32_t>(p[t][0]) | (static_cast<uint32_t>(p[t][1]) << 16);
-    out[t].y = static_cast<uint32_t>(p[t][2]) | (static_cast<uint32_t>(p[t][3]) << 16);
+    const __nv_bfloat162 ha = __float22bfloat162_rn(a), hb = __float22bfloat162_rn(b);
+    out[t].x = *reinterpret_cast<const uint32_t*>(&ha);
+    out[t].y = *reinterpret_cast<const uint32_t*>(&hb);
+    if (t + 1 < A_PARTS) {
+      const float2 fa = __bfloat1622float2(ha), fb = __bfloat1622float2(hb);
+      a = make_float2(a.x - fa.x, a.y - fa.y);
+      b = make_float2(b.x - fb.x, b.y - fb.y);
+    }
   }
 }
 
@@ -268,18 +265,27 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
       if (ok) {
         const uint32_t base = tmem + static_cast<uint32_t>(acc * N_TILE) +
                               (static_cast<uint32_t>(q * 32) << 16);
+        const int c_begin = h * kHalf, c_end = (h + 1) * kHalf;
         float va[16], vb[16];
-        tmem_ld16(base + static_cast<uint32_t>(h * kHalf), va);
+        typename Epi::Pre pa, pb;
+        epi.prefetch(t, row, c_begin, pa);
+        tmem_ld16(base + static_cast<uint32_t>(c_begin), va);
 #pragma unroll 1
-        for (int c0 = h * kHalf; c0 < (h + 1) * kHalf; c0 += 32) {
-          const bool more = c0 + 16 < (h + 1) * kHalf;
-          if (more) tmem_ld16_async(base + static_cast<uint32_t>(c0 + 16), vb);
-          epi.consume(t, row, c0, va);
+        for (int c0 = c_begin; c0 < c_end; c0 += 32) {
+          const bool more = c0 + 16 < c_end;
+          if (more) {
+            tmem_ld16_async(base + static_cast<uint32_t>(c0 + 16), vb);
+            epi.prefetch(t, row, c0 + 16, pb);
+          }
+          epi.consume(t, row, c0, va, pa);
           if (more) {
             tmem_wait_ld(vb);
-            const bool more2 = c0 + 32 < (h + 1) * kHalf;
-            if (more2) tmem_ld16_async(base + static_cast<uint32_t>(c0 + 32), va);
-            epi.consume(t, row, c0 + 16, vb);
+            const bool more2 = c0 + 32 < c_end;
+            if (more2) {
+              tmem_ld16_async(base + static_cast<uint32_t>(c0 + 32), va);
+              epi.prefetch(t, row, c0 + 32, pa);
+            }
+            epi.consume(t, row, c0 + 16, vb, pb);
             if (more2) tmem_wait_ld(va);
           }
         }
@@ -330,18 +336,25 @@ struct ProPlain {
   FBME_DEV void tile_done(const TileCtx&, int, int) {}
 };
 
+// Epilogue policies: prefetch(t, row, c0, pre) issues the global loads a
+// 16-column chunk needs one chunk ahead; consume(t, row, c0, v, pre) gets
+// the chunk's 16 accumulator values (8 complex) and the prefetched data.
+struct NoPre {};
+
 // Store Out[j][r] (lane-contiguous) as complex64.
 struct EpiStoreT {
+  using Pre = NoPre;
   float2* out;
-  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) const {
+  FBME_DEV void prefetch(const TileCtx&, int, int, Pre&) const {}
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v, const Pre&) const {
     const DftGeom& g = *t.g;
     const int r = t.row0() + row;
     if (r >= g.rows) return;
     float2* o = out + t.scene * g.out_stride + r;
+    const int jb = t.col0() + (c0 >> 1);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int j = t.col0() + (c0 >> 1) + i;
-      if (j < g.cols) o[static_cast<long long>(j) * g.out_ld] = make_float2(v[2 * i], v[2 * i + 1]);
+      if (jb + i < g.cols) o[(jb + i) * g.out_ld] = make_float2(v[2 * i], v[2 * i + 1]);
     }
   }
   FBME_DEV void tile_done(const TileCtx&, int, int) {}

@@ -126,10 +126,14 @@ struct PolishBuffers {
   float* xcand_val;   // exchange candidates [B][E]
   int* xcand_idx;
   uint32_t* keys;     // [B][N] score keys scratch
+  uint32_t* cand_key; // [B][max candidates] top-k candidate keys
+  int* cand_idx;      // [B][max candidates] their grid indices
   int* status;        // [B] per-scene status
 };
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
 size_t polish_state_bytes();
+int topk_slices(long long n);
+int exchange_blocks(const BatchShape& s);
 
 }  // namespace fbme

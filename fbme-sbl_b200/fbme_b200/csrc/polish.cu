@@ -22,6 +22,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "topk.cuh"
 
 namespace fbme {
 
@@ -60,7 +61,14 @@ FBME_DEV float2 dirichlet2(const float2* d1, const float2* d2, int n1, int n2, i
   int i1 = a1 - b1, i2 = a2 - b2;
   if (i1 < 0) i1 += n1;
   if (i2 < 0) i2 += n2;
-  return cmul(__ldg(d1 + i1), __ldg(d2 + i2));
+  return cmul(d1[i1], d2[i2]);
+}
+
+// Copy the Dirichlet tables of a scene shape into shared memory.
+FBME_DEV void load_dirichlet(const PolishArgs& A, float2* d1, float2* d2) {
+  for (int i = threadIdx.x; i < A.s.n1; i += blockDim.x) d1[i] = __ldg(A.p.dir1 + i);
+  for (int i = threadIdx.x; i < A.s.n2; i += blockDim.x) d2[i] = __ldg(A.p.dir2 + i);
+  __syncwarp();
 }
 
 // Exact reduced posterior + negative log evidence for the work set.
@@ -72,18 +80,19 @@ struct EvalOut {
   int status;
 };
 
-FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33], int K, int my_idx,
-                          float my_gamma, float nu, float2 my_c, float data_energy) {
+FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33], const float2* d1,
+                          const float2* d2, int K, int my_idx, float my_gamma, float nu, float2 my_c,
+                          float data_energy) {
   const int lane = threadIdx.x & 31;
   const BatchShape& s = A.s;
   const bool on = lane < K;
   const int n1i = my_idx / s.n2, n2i = my_idx % s.n2;
   // system S = diag(1/gamma) + G / nu, Hermitian-symmetrised
-  for (int j = 0; j < K; ++j) {
+#pragma unroll
+  for (int j = 0; j < kMaxPolish; ++j) {
     const int idx_j = __shfl_sync(0xffffffffu, my_idx, j);
-    if (on) {
-      const float2 g = dirichlet2(A.p.dir1, A.p.dir2, s.n1, s.n2, n1i, n2i, idx_j / s.n2,
-                                  idx_j % s.n2);
+    if (on && j < K) {
+      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, idx_j / s.n2, idx_j % s.n2);
       float2 a = make_float2(g.x / nu, g.y / nu);
       if (j == lane) a.x += 1.0f / my_gamma;
       M[lane][j] = a;
@@ -91,37 +100,43 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   }
   __syncwarp();
   float2 row[kMaxPolish];
-  if (on)
-    for (int j = 0; j < K; ++j) {
+#pragma unroll
+  for (int j = 0; j < kMaxPolish; ++j)
+    if (on && j < K) {
       const float2 a = M[lane][j], b = M[j][lane];
       row[j] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
     }
   __syncwarp();
-  if (on)
-    for (int j = 0; j < K; ++j) M[lane][j] = row[j];
+#pragma unroll
+  for (int j = 0; j < kMaxPolish; ++j)
+    if (on && j < K) M[lane][j] = row[j];
   __syncwarp();
   const float dscale = on ? sqrtf(fmaxf(M[lane][lane].x, kTinyP)) : 1.0f;
   // equilibrate: E[i][j] = S[i][j] / d_i / d_j, symmetrise again
   {
-    float dj_all[kMaxPolish];
-    for (int j = 0; j < K; ++j) dj_all[j] = __shfl_sync(0xffffffffu, dscale, j);
-    if (on)
-      for (int j = 0; j < K; ++j) {
+#pragma unroll
+    for (int j = 0; j < kMaxPolish; ++j) {
+      const float dj = __shfl_sync(0xffffffffu, dscale, j);
+      if (on && j < K) {
         const float2 a = M[lane][j];
-        row[j] = make_float2(a.x / dscale / dj_all[j], a.y / dscale / dj_all[j]);
+        row[j] = make_float2(a.x / dscale / dj, a.y / dscale / dj);
       }
+    }
     __syncwarp();
-    if (on)
-      for (int j = 0; j < K; ++j) M[lane][j] = row[j];
+#pragma unroll
+    for (int j = 0; j < kMaxPolish; ++j)
+      if (on && j < K) M[lane][j] = row[j];
     __syncwarp();
-    if (on)
-      for (int j = 0; j < K; ++j) {
+#pragma unroll
+    for (int j = 0; j < kMaxPolish; ++j)
+      if (on && j < K) {
         const float2 a = M[lane][j], b = M[j][lane];
         row[j] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
       }
     __syncwarp();
-    if (on)
-      for (int j = 0; j < K; ++j) M[lane][j] = row[j];
+#pragma unroll
+    for (int j = 0; j < kMaxPolish; ++j)
+      if (on && j < K) M[lane][j] = row[j];
     __syncwarp();
   }
   // deterministic diagonal loading: multiplier * eps * mean|Re diag|
@@ -224,8 +239,8 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
 }
 
 // ||y - A_S mu||^2 by the Gram identity, FP64.
-FBME_DEV double residual_energy(const PolishArgs& A, int K, int my_idx, float2 my_mu, float2 my_c,
-                                float data_energy) {
+FBME_DEV double residual_energy(const PolishArgs& A, const float2* d1, const float2* d2, int K,
+                                int my_idx, float2 my_mu, float2 my_c, float data_energy) {
   const int lane = threadIdx.x & 31;
   const BatchShape& s = A.s;
   double cross = 0.0, quad = 0.0;
@@ -237,8 +252,7 @@ FBME_DEV double residual_energy(const PolishArgs& A, int K, int my_idx, float2 m
       const int idx_j = __shfl_sync(__activemask(), my_idx, j);
       const float mjx = __shfl_sync(__activemask(), my_mu.x, j);
       const float mjy = __shfl_sync(__activemask(), my_mu.y, j);
-      const float2 g = dirichlet2(A.p.dir1, A.p.dir2, s.n1, s.n2, n1i, n2i, idx_j / s.n2,
-                                  idx_j % s.n2);
+      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, idx_j / s.n2, idx_j % s.n2);
       gr += static_cast<double>(g.x) * mjx - static_cast<double>(g.y) * mjy;
       gi += static_cast<double>(g.x) * mjy + static_cast<double>(g.y) * mjx;
     }
@@ -286,6 +300,7 @@ constexpr int kPolishWarps = 1;
 __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A, int phase) {
   __shared__ float2 Msm[kPolishWarps][32][33];
   __shared__ float2 Xsm[kPolishWarps][32][33];
+  extern __shared__ float2 dtab[];  // D1 (n1) then D2 (n2)
   const int lane = threadIdx.x & 31;
   const int scene = blockIdx.x * kPolishWarps + (threadIdx.x >> 5);
   if (scene >= A.s.B) return;
@@ -301,6 +316,9 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
   const float2* bp = A.p.bp + scene * N;
   float2(*M)[33] = Msm[threadIdx.x >> 5];
   float2(*X)[33] = Xsm[threadIdx.x >> 5];
+  float2* d1 = dtab;
+  float2* d2 = dtab + s.n1;
+  load_dirichlet(A, d1, d2);
   int status = 0;
 
   if (phase == 0) {
@@ -369,7 +387,7 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
     const float gam = on ? ps->work_gamma[lane] : 1.0f;
     const float nu = ps->work_noise;
     const float2 cvec = on ? bp[idx] : make_float2(0.f, 0.f);
-    const EvalOut o = evaluate(A, M, X, K, idx, gam, nu, cvec, data_energy);
+    const EvalOut o = evaluate(A, M, X, d1, d2, K, idx, gam, nu, cvec, data_energy);
     status |= o.status;
     // evidence gate (solver.py:4168-4298)
     bool accept = true;
@@ -415,7 +433,7 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
     const float keep = c.polish_damping;
     const float upd_g = keep * bg + (1.0f - keep) * ng;
     const float2 bc = on ? bp[bidx] : make_float2(0.f, 0.f);
-    const double er = residual_energy(A, K, bidx, bmu, bc, data_energy);
+    const double er = residual_energy(A, d1, d2, K, bidx, bmu, bc, data_energy);
     float dof = on ? fminf(fmaxf(1.0f - bpv / fmaxf(bg, kTinyP), 0.f), 1.f) : 0.f;
     dof = warp_sum(dof);
     float un;
@@ -442,57 +460,106 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
   if (status && lane == 0) atomicOr(&A.p.status[scene], status);
 }
 
-// Residual exchange score over the grid: |A^H y - sum_k mu_k D(n - n_k)|^2,
-// with the active set excluded (key 0), as order-preserving keys.
-__global__ void __launch_bounds__(256) exchange_score_kernel(PolishArgs A, uint32_t* keys) {
-  extern __shared__ float2 shm[];
+// Residual exchange scoring (solver.py:4398-4412) without the M-space
+// residual: score[n] = |A^H y[n] - sum_k mu_k D1[n1-a_k] D2[n2-b_k]|^2 over
+// the grid, active atoms excluded.  A CTA covers kExRows grid rows; thread
+// (tx, ty) accumulates a 4-row x CT-column block (columns tx + 64 c), so
+// each u_k(n1) = mu_k D1[n1-a_k] and each D2 value loaded is reused 4 and
+// CT times; complex MACs use the paired FP32 FMA.  Each CTA emits its E best
+// (key, index) candidates.
+constexpr int kExRows = 16;
+constexpr int kExThreads = 256;
+
+template <int CT>
+__global__ void __launch_bounds__(kExThreads)
+exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
+  extern __shared__ float2 ex_shm[];
+  __shared__ TopkShared S;
+  __shared__ float4 u4[kMaxPolish][kExRows];  // {u.x, u.x, -u.y, u.y}
+  __shared__ int bk[kMaxPolish];
+  __shared__ uint32_t excl[kExRows][16];      // active-atom bitmap per row (N2 <= 512)
   const BatchShape& s = A.s;
-  const int scene = blockIdx.y;
-  const int K = A.c.polish_size;
-  float2* d1 = shm;
-  float2* d2 = d1 + s.n1;
-  float2* mu = d2 + s.n2;
-  int* a1 = reinterpret_cast<int*>(mu + kMaxPolish);
-  int* a2 = a1 + kMaxPolish;
+  const int scene = blockIdx.y, r0 = blockIdx.x * kExRows;
+  const int K = A.c.polish_size, E = A.c.exchange;
+  const int N1 = s.n1, N2 = s.n2;
+  const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
+  float2* d2 = ex_shm;
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
-  for (int i = threadIdx.x; i < s.n1; i += blockDim.x) d1[i] = A.p.dir1[i];
-  for (int i = threadIdx.x; i < s.n2; i += blockDim.x) d2[i] = A.p.dir2[i];
-  if (threadIdx.x < K) {
-    const int idx = ps->active[threadIdx.x];
-    mu[threadIdx.x] = ps->best_mean[threadIdx.x];
-    a1[threadIdx.x] = idx / s.n2;
-    a2[threadIdx.x] = idx % s.n2;
+  for (int i = threadIdx.x; i < N2; i += blockDim.x) d2[i] = A.p.dir2[i];
+  for (int i = threadIdx.x; i < kExRows * 16; i += blockDim.x) (&excl[0][0])[i] = 0u;
+  __syncthreads();
+  for (int i = threadIdx.x; i < K * kExRows; i += blockDim.x) {
+    const int k = i / kExRows, ri = i % kExRows;
+    const int idx = ps->active[k];
+    const int a = idx / N2;
+    int dd = r0 + ri - a;
+    dd %= N1;
+    if (dd < 0) dd += N1;
+    const float2 uv = (r0 + ri < N1) ? cmul(ps->best_mean[k], A.p.dir1[dd]) : make_float2(0.f, 0.f);
+    u4[k][ri] = make_float4(uv.x, uv.x, -uv.y, uv.y);
+    if (ri == 0) {
+      bk[k] = idx % N2;
+      const int ra = a - r0;
+      if (ra >= 0 && ra < kExRows) atomicOr(&excl[ra][(idx % N2) >> 5], 1u << ((idx % N2) & 31));
+    }
   }
   __syncthreads();
-  const long long N = s.n();
-  const float2* bp = A.p.bp + scene * N;
-  uint32_t* kp = keys + scene * N;
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < N;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int n1 = static_cast<int>(e / s.n2), n2 = static_cast<int>(e % s.n2);
-    float2 acc = make_float2(0.f, 0.f);
-    bool active = false;
-    for (int k = 0; k < K; ++k) {
-      int i1 = n1 - a1[k], i2 = n2 - a2[k];
-      active |= (i1 == 0 && i2 == 0);
-      if (i1 < 0) i1 += s.n1;
-      if (i2 < 0) i2 += s.n2;
-      const float2 dk = cmul(d1[i1], d2[i2]);
-      const float2 t = cmul(mu[k], dk);
-      acc.x += t.x;
-      acc.y += t.y;
+  float2 acc[4][CT];
+#pragma unroll
+  for (int ri = 0; ri < 4; ++ri)
+#pragma unroll
+    for (int c = 0; c < CT; ++c) acc[ri][c] = make_float2(0.f, 0.f);
+  for (int k = 0; k < K; ++k) {
+    const int b = bk[k];
+    float2 d[CT], ds[CT];
+#pragma unroll
+    for (int c = 0; c < CT; ++c) {
+      const int n2 = tx + 64 * c;
+      int i2 = n2 - b;
+      i2 += i2 < 0 ? N2 : 0;
+      d[c] = n2 < N2 ? d2[i2] : make_float2(0.f, 0.f);
+      ds[c] = make_float2(d[c].y, d[c].x);
     }
-    const float2 b = bp[e];
-    const float2 r = make_float2(b.x - acc.x, b.y - acc.y);
-    const float score = abs_sq(r);
-    const uint32_t bits = __float_as_uint(score);
-    kp[e] = active ? 0u : ((bits & 0x80000000u) ? ~bits : (bits | 0x80000000u));
+#pragma unroll
+    for (int ri = 0; ri < 4; ++ri) {
+      const float4 uu = u4[k][4 * ty + ri];
+      const float2 ux = make_float2(uu.x, uu.y), uy = make_float2(uu.z, uu.w);
+#pragma unroll
+      for (int c = 0; c < CT; ++c) {
+        acc[ri][c] = __ffma2_rn(ux, d[c], acc[ri][c]);
+        acc[ri][c] = __ffma2_rn(uy, ds[c], acc[ri][c]);
+      }
+    }
   }
+  const float2* bp = A.p.bp + scene * s.n();
+  uint32_t key[4 * CT];
+  int gidx[4 * CT];
+  bool valid[4 * CT];
+#pragma unroll
+  for (int ri = 0; ri < 4; ++ri)
+#pragma unroll
+    for (int c = 0; c < CT; ++c) {
+      const int i = ri * CT + c;
+      const int lr = 4 * ty + ri;
+      const int n1 = r0 + lr, n2 = tx + 64 * c;
+      valid[i] = n1 < N1 && n2 < N2;
+      gidx[i] = n1 * N2 + n2;
+      key[i] = 0u;
+      if (valid[i]) {
+        const float2 bv = bp[gidx[i]];
+        const float2 r = make_float2(bv.x - acc[ri][c].x, bv.y - acc[ri][c].y);
+        const bool act = (excl[lr][n2 >> 5] >> (n2 & 31)) & 1u;
+        key[i] = act ? 0u : float_key_t(abs_sq(r));
+      }
+    }
+  const size_t off = (static_cast<size_t>(scene) * gridDim.x + blockIdx.x) * E;
+  block_topk(key, gidx, valid, E, S, cand_key + off, cand_idx + off);
 }
 
 // Final K-space outputs, fixed-budget diagnostics, effective DOF
 // (solver.py:1989-2021, 2081-2092, 3408-3496, 2108-2126).
 __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOutputs out) {
+  extern __shared__ float2 dtab[];
   const int lane = threadIdx.x & 31;
   const int scene = blockIdx.x;
   if (scene >= A.s.B) return;
@@ -504,6 +571,9 @@ __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOut
   const float fl = A.p.sc.floor_[scene];
   const float Mf = static_cast<float>(s.m());
   const long long N = s.n();
+  float2* d1 = dtab;
+  float2* d2 = dtab + s.n1;
+  load_dirichlet(A, d1, d2);
   const int idx = on ? ps->active[lane] : 0;
   const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
   const float pv = on ? ps->best_pv[lane] : 0.f;
@@ -532,19 +602,19 @@ __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOut
     const float gt = fminf(fmaxf(abs_sq(mu) + pv, fl), c.max_prec);
     const float gs = fmaxf(fmaxf(fabsf(ag), fabsf(gt)), kTinyP);
     const float gr = warp_max(on ? fabsf(ag - gt) / gs : 0.f);
-    float d2 = on ? fminf(fmaxf(1.0f - pv / ag, 0.f), 1.f) : 0.f;
-    d2 = warp_sum(d2);
+    float dofd = on ? fminf(fmaxf(1.0f - pv / ag, 0.f), 1.f) : 0.f;
+    dofd = warp_sum(dofd);
     const float2 cv = on ? A.p.bp[scene * N + idx] : make_float2(0.f, 0.f);
-    const double er = residual_energy(A, K, idx, mu, cv, A.p.sc.data_energy[scene]);
+    const double er = residual_energy(A, d1, d2, K, idx, mu, cv, A.p.sc.data_energy[scene]);
     float nt;
     if (c.fixed_noise > 0.f) {
       nt = nu;
     } else if (!c.noise_evidence) {
-      nt = static_cast<float>((er + static_cast<double>(nu) * d2 + c.noise_rate) /
+      nt = static_cast<float>((er + static_cast<double>(nu) * dofd + c.noise_rate) /
                               (static_cast<double>(Mf) + c.noise_shape));
     } else {
       nt = static_cast<float>((er + c.noise_rate) /
-                              fmax(static_cast<double>(Mf) - d2 + c.noise_shape, kEpsP));
+                              fmax(static_cast<double>(Mf) - dofd + c.noise_shape, kEpsP));
     }
     nt = fminf(fmaxf(nt, fl), c.max_prec);
     const float ns = fmaxf(fmaxf(fabsf(nu), fabsf(nt)), kTinyP);
@@ -600,26 +670,37 @@ __global__ void __launch_bounds__(32) output_scatter_kernel(PolishArgs A, FbmeOu
   }
 }
 
-void launch_topk(const uint32_t* keys, long long n, int k, int B, int* out_idx, float* out_val,
-                 cudaStream_t st);
+void launch_topk(const uint32_t* keys, long long n, int k, int B, uint32_t* cand_key, int* cand_idx,
+                 int* out_idx, float* out_val, cudaStream_t st);
+void launch_topk_merge(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, int B,
+                       int* out_idx, float* out_val, cudaStream_t st);
+
+int exchange_blocks(const BatchShape& s) { return (s.n1 + kExRows - 1) / kExRows; }
 
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof) {
   PolishArgs A{s, c, p};
   const int K = c.polish_size;
-  FBME_TIMED(prof, FBME_GROUP_TOPK, launch_topk(p.keys, s.n(), K, s.B, p.active, p.score, st));
-  FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, 0, st>>>(A, 0)));
+  FBME_TIMED(prof, FBME_GROUP_TOPK,
+             launch_topk(p.keys, s.n(), K, s.B, p.cand_key, p.cand_idx, p.active, p.score, st));
+  const size_t dsm = (s.n1 + s.n2) * sizeof(float2);
+  FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 0)));
   if (c.exchange > 0 && c.polish_iters > 1) {
-    const int blocks = static_cast<int>((s.n() + 256 * 16 - 1) / (256 * 16));
-    const size_t shm = (s.n1 + s.n2 + kMaxPolish) * sizeof(float2) + 2 * kMaxPolish * sizeof(int);
-    FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
-               (exchange_score_kernel<<<dim3(blocks < 64 ? blocks : 64, s.B), 256, shm, st>>>(
-                   A, p.keys)));
+    const int nb = exchange_blocks(s);
+    const size_t shm = s.n2 * sizeof(float2);
+    const dim3 grid(nb, s.B);
+    if (s.n2 <= 256)
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
+                 (exchange_kernel<4><<<grid, kExThreads, shm, st>>>(A, p.cand_key, p.cand_idx)));
+    else
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
+                 (exchange_kernel<8><<<grid, kExThreads, shm, st>>>(A, p.cand_key, p.cand_idx)));
     FBME_TIMED(prof, FBME_GROUP_TOPK,
-               launch_topk(p.keys, s.n(), c.exchange, s.B, p.xcand_idx, p.xcand_val, st));
-    FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, 0, st>>>(A, 1)));
+               launch_topk_merge(p.cand_key, p.cand_idx, nb * c.exchange, c.exchange, s.B,
+                                 p.xcand_idx, p.xcand_val, st));
+    FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 1)));
   }
-  FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, 0, st>>>(A, out)));
+  FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, dsm, st>>>(A, out)));
   const int fb = static_cast<int>((s.n() + 2047) / 2048);
   FBME_TIMED(prof, FBME_GROUP_OUTPUT,
              (output_fill_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(s, p.sc, out)));

@@ -1,0 +1,184 @@
+// Block-wide top-k (k <= 32) over order-preserving 32-bit keys held in
+// registers, with the index-order tie break of a stable descending sort.
+//
+// Used twice per selection: many CTAs per scene each reduce a slice of the
+// grid to k candidates, then one CTA per scene merges the candidates; the
+// result is exactly the k largest keys of the scene (largest first, ties by
+// lower index), which is what torch.topk returns at solver.py:1931/4410.
+#pragma once
+
+#include "common.cuh"
+
+namespace fbme {
+
+FBME_DEV uint32_t float_key_t(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+FBME_DEV float key_to_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+struct TopkShared {
+  uint32_t hist[256];
+  uint32_t prefix, mask;
+  int remaining, ngt, neq, filled, nvalid;
+  int red_idx[32];
+  uint32_t sel_key[32];
+  int sel_idx[32];
+};
+
+// Block-wide top-k (k <= 32) of the valid (key, gidx) pairs held KPT per
+// thread.  Radix select with 8-bit digits finds the k-th largest key T;
+// keys above T are all taken; among keys equal to T the lowest indices are
+// taken.  Writes k winners, sorted (key desc, index asc), to out_key/out_idx.
+template <int KPT>
+FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], const bool (&valid)[KPT],
+                         int k, TopkShared& S, uint32_t* out_key, int* out_idx) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = (blockDim.x + 31) >> 5;
+  if (tid == 0) {
+    S.prefix = 0;
+    S.mask = 0;
+    S.ngt = 0;
+    S.neq = 0;
+    S.filled = 0;
+    S.nvalid = 0;
+  }
+  __syncthreads();
+  {
+    int nv = 0;
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) nv += valid[i] ? 1 : 0;
+    nv = warp_sum(nv);
+    if (lane == 0 && nv) atomicAdd(&S.nvalid, nv);
+  }
+  __syncthreads();
+  const int k_out = k;
+  k = min(k, S.nvalid);  // fewer valid entries than k: pad the output
+  if (tid == 0) S.remaining = k;
+  if (k == 0) {
+    if (tid < k_out) {
+      out_key[tid] = 0u;
+      out_idx[tid] = 0x7fffffff;
+    }
+    __syncthreads();
+    return;
+  }
+#pragma unroll 1
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+    for (int b = tid; b < 256; b += blockDim.x) S.hist[b] = 0;
+    __syncthreads();
+    const uint32_t prefix = S.prefix, mask = S.mask;
+#pragma unroll
+    for (int i = 0; i < KPT; ++i)
+      if (valid[i] && (key[i] & mask) == prefix) atomicAdd(&S.hist[(key[i] >> shift) & 255u], 1u);
+    __syncthreads();
+    if (warp == 0) {
+      const int hi = 256 - 8 * lane;  // lane owns bins [hi-8, hi), counted from the top
+      uint32_t local = 0;
+#pragma unroll
+      for (int b = 1; b <= 8; ++b) local += S.hist[hi - b];
+      uint32_t incl = local;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t excl = incl - local;
+      const int rem = S.remaining;
+      const bool here = excl < static_cast<uint32_t>(rem) && incl >= static_cast<uint32_t>(rem);
+      const unsigned ball = __ballot_sync(0xffffffffu, here);
+      const int owner = ball ? __ffs(ball) - 1 : 31;
+      if (lane == owner) {
+        uint32_t cum = excl;
+        int sel = hi - 8;
+        for (int b = hi - 1; b >= hi - 8; --b) {
+          if (cum + S.hist[b] >= static_cast<uint32_t>(rem)) {
+            sel = b;
+            break;
+          }
+          cum += S.hist[b];
+        }
+        S.remaining = rem - static_cast<int>(cum);
+        S.prefix = prefix | (static_cast<uint32_t>(sel) << shift);
+        S.mask = mask | (255u << shift);
+      }
+    }
+    __syncthreads();
+  }
+  const uint32_t T = S.prefix;
+  const int need_eq = S.remaining;  // >= 1
+  int my_eq = 0;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    if (valid[i] && key[i] > T) {
+      const int pos = atomicAdd(&S.ngt, 1);
+      if (pos < 32) {
+        S.sel_key[pos] = key[i];
+        S.sel_idx[pos] = gidx[i];
+      }
+    }
+    my_eq += (valid[i] && key[i] == T) ? 1 : 0;
+  }
+  my_eq = warp_sum(my_eq);
+  if (lane == 0 && my_eq) atomicAdd(&S.neq, my_eq);
+  __syncthreads();
+  const int base = k - need_eq;
+  if (S.neq == need_eq) {
+    // every tie is a winner
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) {
+      if (valid[i] && key[i] == T) {
+        const int pos = atomicAdd(&S.filled, 1);
+        S.sel_key[base + pos] = T;
+        S.sel_idx[base + pos] = gidx[i];
+      }
+    }
+  } else {
+    // more ties than places: take the lowest indices, one per round
+    int taken_below = -1;  // indices <= taken_below are already taken
+    for (int r = 0; r < need_eq; ++r) {
+      int best = 0x7fffffff;
+#pragma unroll
+      for (int i = 0; i < KPT; ++i)
+        if (valid[i] && key[i] == T && gidx[i] > taken_below && gidx[i] < best) best = gidx[i];
+      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+      if (lane == 0) S.red_idx[warp] = best;
+      __syncthreads();
+      int b2 = 0x7fffffff;
+      for (int w = 0; w < nwarps; ++w) b2 = min(b2, S.red_idx[w]);
+      if (tid == 0) {
+        S.sel_key[base + r] = T;
+        S.sel_idx[base + r] = b2;
+      }
+      taken_below = b2;
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t kk = lane < k ? S.sel_key[lane] : 0u;
+    int ii = lane < k ? S.sel_idx[lane] : 0x7fffffff;
+    for (int size = 2; size <= 32; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const uint32_t ok = __shfl_xor_sync(0xffffffffu, kk, stride);
+        const int oi = __shfl_xor_sync(0xffffffffu, ii, stride);
+        const bool other_first = (ok > kk) || (ok == kk && oi < ii);
+        const bool lower = (lane & stride) == 0;
+        const bool asc = (lane & size) == 0;
+        if (lower == asc ? other_first : !other_first) {
+          kk = ok;
+          ii = oi;
+        }
+      }
+    if (lane < k_out) {
+      out_key[lane] = lane < k ? kk : 0u;
+      out_idx[lane] = lane < k ? ii : 0x7fffffff;
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace fbme

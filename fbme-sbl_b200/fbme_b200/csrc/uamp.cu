@@ -149,28 +149,35 @@ struct ProMessage {
 
 // Forward stage 2: store the prediction and sum |y - p|^2.
 struct EpiPredict {
+  struct Pre {
+    float2 y[8];
+  };
   float2* pred;
   const float2* y;
   double* part;
   float acc;
-  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) {
+  FBME_DEV void prefetch(const TileCtx& t, int row, int c0, Pre& p) const {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    const float2* ys = y + t.scene * g.out_stride;
+    const int jb = t.col0() + (c0 >> 1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      p.y[i] = (r < g.rows && jb + i < g.cols) ? __ldg(ys + (jb + i) * g.out_ld + r)
+                                               : make_float2(0.f, 0.f);
+  }
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v, const Pre& pre) {
     const DftGeom& g = *t.g;
     const int r = t.row0() + row;
     if (r >= g.rows) return;
-    const long long base = t.scene * g.out_stride + r;
-    float2 yy[8];
+    float2* ps = pred + t.scene * g.out_stride;
+    const int jb = t.col0() + (c0 >> 1);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int j = t.col0() + (c0 >> 1) + i;
-      yy[i] = j < g.cols ? __ldg(y + base + static_cast<long long>(j) * g.out_ld) : make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int j = t.col0() + (c0 >> 1) + i;
-      if (j < g.cols) {
+      if (jb + i < g.cols) {
         const float2 p = make_float2(v[2 * i], v[2 * i + 1]);
-        pred[base + static_cast<long long>(j) * g.out_ld] = p;
-        const float dr = yy[i].x - p.x, di = yy[i].y - p.y;
+        ps[(jb + i) * g.out_ld + r] = p;
+        const float dr = pre.y[i].x - p.x, di = pre.y[i].y - p.y;
         acc += dr * dr + di * di;
       }
     }
@@ -183,20 +190,22 @@ struct EpiPredict {
 
 // Adjoint stage 2 during initialisation: store A^H y and sum |A^H y|^2.
 struct EpiBackprojection {
+  using Pre = NoPre;
   float2* bp;
   double* part;
   float acc;
-  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) {
+  FBME_DEV void prefetch(const TileCtx&, int, int, Pre&) const {}
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v, const Pre&) {
     const DftGeom& g = *t.g;
     const int r = t.row0() + row;
     if (r >= g.rows) return;
-    const long long base = t.scene * g.out_stride + r;
+    float2* bs = bp + t.scene * g.out_stride + r;
+    const int jb = t.col0() + (c0 >> 1);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int j = t.col0() + (c0 >> 1) + i;
-      if (j < g.cols) {
+      if (jb + i < g.cols) {
         const float2 b = make_float2(v[2 * i], v[2 * i + 1]);
-        bp[base + static_cast<long long>(j) * g.out_ld] = b;
+        bs[(jb + i) * g.out_ld] = b;
         acc += abs_sq(b);
       }
     }
@@ -218,6 +227,7 @@ struct DenoiseArgs {
   double* part;
   uint32_t* keys;  // optional: score key of |mu|^2 + v for the top-K
   float damping, prior_damping, prior_max, hyper_shape, hyper_rate;
+  float inv_hyper;  // 1 / (1 + hyper_shape)
   int update_prior;
 };
 
@@ -226,63 +236,74 @@ FBME_DEV uint32_t float_key(float f) {
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
-// One coefficient of the denoiser; writes mu, v (and gamma / key) at e.
-FBME_DEV void denoise_core(const DenoiseArgs& a, long long e, float prior, float2 old_mean,
-                           float old_var_raw, float2 lifted, float pv, float floor_,
-                           float& dof_acc, float& var_acc) {
-  const float old_var = fmaxf(old_var_raw, kTiny);
-  const float denom = fmaxf(prior + pv, kTiny);
-  const float gain = prior / denom;
-  const float2 pm = make_float2(old_mean.x + pv * lifted.x, old_mean.y + pv * lifted.y);
-  const float2 cm = make_float2(gain * pm.x, gain * pm.y);
-  const float cv = prior * pv / denom;
+// One coefficient of the denoiser (triton_kernels.py:140-184): new mean,
+// variance, relevance and (optionally) prior variance.  Divisions use the
+// fast reciprocal path (<= 2 ulp), as the fused Triton kernel's `/` does.
+struct DenoiseOut {
+  float2 mean;
+  float variance, rel, gamma;
+};
+
+FBME_DEV DenoiseOut denoise_math(const DenoiseArgs& a, float prior, float2 om, float ov_raw,
+                                 float2 L, float pv, float fl) {
+  DenoiseOut o;
+  const float ov = fmaxf(ov_raw, kTiny);
+  const float den = fmaxf(prior + pv, kTiny);
+  const float gain = __fdividef(prior, den);
+  const float2 pm = make_float2(om.x + pv * L.x, om.y + pv * L.y);
   const float keep = a.damping, upd = 1.0f - a.damping;
-  const float2 mean = make_float2(keep * old_mean.x + upd * cm.x, keep * old_mean.y + upd * cm.y);
-  const float variance = fmaxf(keep * old_var + upd * cv, kTiny);
-  float rel = 1.0f - variance / fmaxf(prior, kTiny);
-  rel = fmaxf(0.0f, fminf(1.0f, rel));
-  a.mu[e] = mean;
-  a.var[e] = variance;
-  if (a.update_prior) {
-    const float second = mean.x * mean.x + mean.y * mean.y + variance;
-    float cand = (second + a.hyper_rate) / (1.0f + a.hyper_shape);
-    cand = fmaxf(floor_, fminf(a.prior_max, cand));
-    const float nxt = a.prior_damping * prior + (1.0f - a.prior_damping) * cand;
-    a.gamma[e] = fmaxf(nxt, floor_);
-  }
-  if (a.keys) a.keys[e] = float_key(abs_sq(mean) + variance);
-  dof_acc += rel;
-  var_acc += variance;
+  o.mean = make_float2(keep * om.x + upd * (gain * pm.x), keep * om.y + upd * (gain * pm.y));
+  const float cv = __fdividef(prior * pv, den);
+  o.variance = fmaxf(keep * ov + upd * cv, kTiny);
+  o.rel = fmaxf(0.0f, fminf(1.0f, 1.0f - __fdividef(o.variance, fmaxf(prior, kTiny))));
+  const float second = o.mean.x * o.mean.x + o.mean.y * o.mean.y + o.variance;
+  float cand = (second + a.hyper_rate) * a.inv_hyper;
+  cand = fmaxf(fl, fminf(a.prior_max, cand));
+  o.gamma = fmaxf(a.prior_damping * prior + (1.0f - a.prior_damping) * cand, fl);
+  return o;
 }
 
 struct EpiDenoise {
+  using Pre = NoPre;  // loads are issued inside consume (measured faster than prefetching)
   DenoiseArgs a;
   float dof_acc, var_acc;
-  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v) {
+  FBME_DEV void prefetch(const TileCtx&, int, int, Pre&) const {}
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v, const Pre&) {
     const DftGeom& g = *t.g;
     const int r = t.row0() + row;
     if (r >= g.rows) return;
     const float pv = a.pv[t.scene], fl = a.floor_[t.scene];
-    const long long base = t.scene * g.out_stride + r;
+    const long long sb = t.scene * g.out_stride;
+    float2* mu = a.mu + sb;
+    float* var = a.var + sb;
+    float* gam = a.gamma + sb;
+    const int jb = t.col0() + (c0 >> 1);
+    const int ld = g.out_ld;
     // all loads of the chunk first (independent addresses, in flight together)
     float pri[8], ov[8];
     float2 om[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int j = t.col0() + (c0 >> 1) + i;
-      if (j < g.cols) {
-        const long long e = base + static_cast<long long>(j) * g.out_ld;
-        pri[i] = a.gamma[e];
-        om[i] = a.mu[e];
-        ov[i] = a.var[e];
+      if (jb + i < g.cols) {
+        const int e = (jb + i) * ld + r;
+        pri[i] = gam[e];
+        om[i] = mu[e];
+        ov[i] = var[e];
       }
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int j = t.col0() + (c0 >> 1) + i;
-      if (j < g.cols)
-        denoise_core(a, base + static_cast<long long>(j) * g.out_ld, pri[i], om[i], ov[i],
-                     make_float2(v[2 * i], v[2 * i + 1]), pv, fl, dof_acc, var_acc);
+      if (jb + i < g.cols) {
+        const int e = (jb + i) * ld + r;
+        const DenoiseOut o =
+            denoise_math(a, pri[i], om[i], ov[i], make_float2(v[2 * i], v[2 * i + 1]), pv, fl);
+        mu[e] = o.mean;
+        var[e] = o.variance;
+        if (a.update_prior) gam[e] = o.gamma;
+        if (a.keys) a.keys[sb + e] = float_key(abs_sq(o.mean) + o.variance);
+        dof_acc += o.rel;
+        var_acc += o.variance;
+      }
     }
   }
   FBME_DEV void tile_done(const TileCtx& t, int w, int lane) {
@@ -367,8 +388,13 @@ __global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevCon
     const long long e = scene * n + i;
     const float g0 = a.gamma[e];
     const float2 b = bp[e];
-    denoise_core(a, e, g0, make_float2(0.f, 0.f), g0, make_float2(scale * b.x, scale * b.y), pv, fl,
-                 dof, sv);
+    const DenoiseOut o =
+        denoise_math(a, g0, make_float2(0.f, 0.f), g0, make_float2(scale * b.x, scale * b.y), pv, fl);
+    a.mu[e] = o.mean;
+    a.var[e] = o.variance;
+    if (a.update_prior) a.gamma[e] = o.gamma;
+    dof += o.rel;
+    sv += o.variance;
   }
   write_block_partial(dof, red, a.part, scene, blockIdx.x, 0 * kPartWarps);
   write_block_partial(sv, red, a.part, scene, blockIdx.x, 1 * kPartWarps);
@@ -602,6 +628,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   da.prior_max = c.max_prec;
   da.hyper_shape = c.hyper_shape;
   da.hyper_rate = c.hyper_rate;
+  da.inv_hyper = 1.0f / (1.0f + c.hyper_shape);
   da.update_prior = 1;
 
   // --- sweeps ---
