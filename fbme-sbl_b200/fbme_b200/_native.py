@@ -8,7 +8,7 @@ fails to load, every entry point raises ``RuntimeError``.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_float, c_int, c_int32, c_size_t, c_void_p
+from ctypes import POINTER, c_char_p, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libfbme_b200.so"
@@ -111,6 +111,9 @@ SIGNATURES = {
     "fbme_plan_profile": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p,
                                   POINTER(c_float), POINTER(c_int32), c_int32]),
     "fbme_profile_group_name": (c_char_p, [c_int32]),
+    "fbme_topk_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32]),
+    "fbme_topk": (c_int, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_size_t, c_void_p,
+                          c_void_p, c_void_p]),
     "fbme_last_error": (c_char_p, []),
     "fbme_version": (c_char_p, []),
 }

@@ -384,6 +384,23 @@ int fbme_plan_profile(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbm
   return rc;
 }
 
+size_t fbme_topk_workspace_bytes(int64_t n, int32_t k, int32_t batch) {
+  if (fbme::topk_check(n, k, batch)) return 0;
+  return fbme::topk_scratch_bytes(n, k, batch);
+}
+
+int fbme_topk(const float* scores, int64_t n, int32_t k, int32_t batch, void* workspace,
+              size_t workspace_bytes, int64_t* indices, float* values, fbme_stream_t stream) {
+  if (!scores || !indices || !values) return fail(FBME_ERR_INVALID, "NULL argument");
+  if (const char* why = fbme::topk_check(n, k, batch)) return fail(FBME_ERR_INVALID, why);
+  if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 15u) != 0 ||
+      workspace_bytes < fbme::topk_scratch_bytes(n, k, batch))
+    return fail(FBME_ERR_WORKSPACE, "workspace smaller than fbme_topk_workspace_bytes() or unaligned");
+  fbme::topk_scores(scores, n, k, batch, workspace, indices, values,
+                    reinterpret_cast<cudaStream_t>(stream));
+  return check_launch("fbme_topk");
+}
+
 int fbme_plan_state(FbmePlan* plan, FbmeState* st) {
   if (!plan || !st) return fail(FBME_ERR_INVALID, "NULL argument");
   st->mean = plan->u.mu;

@@ -134,6 +134,10 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
 size_t polish_state_bytes();
 int topk_slices(long long n);
+size_t topk_scratch_bytes(long long n, int k, int batch);
+const char* topk_check(long long n, int k, int batch);
+void topk_scores(const float* scores, long long n, int k, int batch, void* scratch,
+                 int64_t* indices, float* values, cudaStream_t st);
 int exchange_blocks(const BatchShape& s);
 
 }  // namespace fbme

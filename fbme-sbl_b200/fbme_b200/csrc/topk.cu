@@ -18,11 +18,14 @@ constexpr int kTopkKpt = 32;
 constexpr int kTopkSlice = kTopkBlockThreads * kTopkKpt;  // 8192 keys per CTA
 constexpr int kMergeMax = 2048;
 
+// FROM_SCORES: `in` holds float scores (converted to keys); else keys.
+template <bool FROM_SCORES>
 __global__ void __launch_bounds__(kTopkBlockThreads)
-topk_blocks_kernel(const uint32_t* keys, long long n, int k, uint32_t* cand_key, int* cand_idx) {
+topk_blocks_kernel(const void* in, long long n, int k, uint32_t* cand_key, int* cand_idx) {
   __shared__ TopkShared S;
   const int scene = blockIdx.y, blk = blockIdx.x;
-  const uint32_t* kp = keys + scene * n;
+  const uint32_t* kp = static_cast<const uint32_t*>(in) + scene * n;
+  const float* sp = static_cast<const float*>(in) + scene * n;
   const long long base = static_cast<long long>(blk) * kTopkSlice;
   uint32_t key[kTopkKpt];
   int gidx[kTopkKpt];
@@ -31,15 +34,16 @@ topk_blocks_kernel(const uint32_t* keys, long long n, int k, uint32_t* cand_key,
   for (int i = 0; i < kTopkKpt; ++i) {
     const long long e = base + static_cast<long long>(i) * kTopkBlockThreads + threadIdx.x;
     valid[i] = e < n;
-    key[i] = valid[i] ? kp[e] : 0u;
+    key[i] = valid[i] ? (FROM_SCORES ? float_key_t(sp[e]) : kp[e]) : 0u;
     gidx[i] = static_cast<int>(e);
   }
   const size_t off = (static_cast<size_t>(scene) * gridDim.x + blk) * k;
   block_topk(key, gidx, valid, k, S, cand_key + off, cand_idx + off);
 }
 
+template <typename Idx>
 __global__ void __launch_bounds__(1024)
-topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, int* out_idx,
+topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, Idx* out_idx,
                   float* out_val) {
   __shared__ unsigned long long s[kMergeMax];
   const int scene = blockIdx.x;
@@ -73,7 +77,7 @@ topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int 
     }
   if (threadIdx.x < k) {
     const unsigned long long w = s[threadIdx.x];
-    out_idx[scene * k + threadIdx.x] = static_cast<int>(0xFFFFFFFFu - static_cast<uint32_t>(w));
+    out_idx[scene * k + threadIdx.x] = static_cast<Idx>(0xFFFFFFFFu - static_cast<uint32_t>(w));
     out_val[scene * k + threadIdx.x] = key_to_float(static_cast<uint32_t>(w >> 32));
   }
 }
@@ -83,13 +87,40 @@ int topk_slices(long long n) { return static_cast<int>((n + kTopkSlice - 1) / kT
 void launch_topk(const uint32_t* keys, long long n, int k, int B, uint32_t* cand_key, int* cand_idx,
                  int* out_idx, float* out_val, cudaStream_t st) {
   const int nblk = topk_slices(n);
-  topk_blocks_kernel<<<dim3(nblk, B), kTopkBlockThreads, 0, st>>>(keys, n, k, cand_key, cand_idx);
-  topk_merge_kernel<<<B, 1024, 0, st>>>(cand_key, cand_idx, nblk * k, k, out_idx, out_val);
+  topk_blocks_kernel<false>
+      <<<dim3(nblk, B), kTopkBlockThreads, 0, st>>>(keys, n, k, cand_key, cand_idx);
+  topk_merge_kernel<int><<<B, 1024, 0, st>>>(cand_key, cand_idx, nblk * k, k, out_idx, out_val);
 }
 
 void launch_topk_merge(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, int B,
                        int* out_idx, float* out_val, cudaStream_t st) {
-  topk_merge_kernel<<<B, 1024, 0, st>>>(cand_key, cand_idx, ncand, k, out_idx, out_val);
+  topk_merge_kernel<int><<<B, 1024, 0, st>>>(cand_key, cand_idx, ncand, k, out_idx, out_val);
+}
+
+// Candidate scratch of the score top-k: per row, one k-list per 8192-score slice.
+size_t topk_scratch_bytes(long long n, int k, int batch) {
+  return static_cast<size_t>(batch) * topk_slices(n) * k * (sizeof(uint32_t) + sizeof(int));
+}
+
+const char* topk_check(long long n, int k, int batch) {
+  if (n < 1 || batch < 1) return "n and batch must be positive";
+  if (k < 1 || k > 32) return "k must be in [1, 32]";
+  if (k > n) return "k exceeds n";
+  if (n > (1LL << 31) - 1) return "n above 2^31 - 1";
+  if (static_cast<long long>(topk_slices(n)) * k > kMergeMax)
+    return "n too large for the candidate merge (ceil(n/8192)*k must be <= 2048)";
+  return nullptr;
+}
+
+// Top-k of float scores with candidates in `scratch` (topk_scratch_bytes).
+void topk_scores(const float* scores, long long n, int k, int batch, void* scratch,
+                 int64_t* indices, float* values, cudaStream_t st) {
+  const int nblk = topk_slices(n);
+  uint32_t* ck = static_cast<uint32_t*>(scratch);
+  int* ci = reinterpret_cast<int*>(ck + static_cast<size_t>(batch) * nblk * k);
+  topk_blocks_kernel<true><<<dim3(nblk, batch), kTopkBlockThreads, 0, st>>>(scores, n, k, ck, ci);
+  topk_merge_kernel<int64_t><<<batch, 1024, 0, st>>>(ck, ci, nblk * k, k, indices, values);
 }
 
 }  // namespace fbme
+

@@ -153,6 +153,15 @@ int fbme_uamp_run(FbmePlan* plan, const void* y, fbme_stream_t stream);
 int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream);
 int fbme_plan_state(FbmePlan* plan, FbmeState* state);
 
+/* Top-k (k <= 32) of each of `batch` rows of `n` float scores: values
+ * largest first, ties by lower index, as torch.topk(scores, k) at
+ * torch_sbl/solver.py:1931 and 4410.  `indices` / `values` are [batch, k].
+ * The caller provides fbme_topk_workspace_bytes(n, k, batch) bytes of
+ * 16-byte aligned device workspace for the per-slice candidates. */
+size_t fbme_topk_workspace_bytes(int64_t n, int32_t k, int32_t batch);
+int fbme_topk(const float* scores, int64_t n, int32_t k, int32_t batch, void* workspace,
+              size_t workspace_bytes, int64_t* indices, float* values, fbme_stream_t stream);
+
 /* Kernel groups timed by fbme_plan_profile. */
 enum {
   FBME_GROUP_INIT = 0,        /* A^H y, data power, prior/noise initialisation */
