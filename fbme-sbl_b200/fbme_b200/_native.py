@@ -114,6 +114,9 @@ SIGNATURES = {
     "fbme_topk_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32]),
     "fbme_topk": (c_int, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_size_t, c_void_p,
                           c_void_p, c_void_p]),
+    "fbme_topk_static": (c_int, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p,
+                                 c_void_p]),
+    "fbme_topk_static_error": (c_char_p, []),
     "fbme_last_error": (c_char_p, []),
     "fbme_version": (c_char_p, []),
 }

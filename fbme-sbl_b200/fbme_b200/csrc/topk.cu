@@ -124,3 +124,89 @@ void topk_scores(const float* scores, long long n, int k, int batch, void* scrat
 
 }  // namespace fbme
 
+// ---------------------------------------------------------------------------
+// Allocation-free top-k (C ABI fbme_topk_static).
+//
+// For callers that cannot allocate device memory when they need a top-k:
+// code that runs while another component captures a CUDA graph (allocation
+// is not allowed during global-mode stream capture), real-time hosts that
+// freeze their memory budget after start-up, and FFI hosts that only receive
+// device pointers from another framework.  The candidate scratch lives in a
+// library-owned, file-scope device array instead of a caller workspace.
+// ---------------------------------------------------------------------------
+#include <mutex>
+#include <string>
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = FBME_TOPK_STATIC_SCRATCH_BYTES;
+// Held by every GPU that loads this library until the process exits.  All
+// calls share it; its contents persist from the last call.
+__device__ __align__(256) unsigned char g_topk_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void* g_scratch_ptr[kMaxDevices] = {};
+thread_local std::string g_static_error;
+
+// Device address of g_topk_scratch on the current device, looked up once per
+// device (with that device current).  In host code the array's name is only
+// a host-side stand-in, never a device address.
+int static_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    g_static_error = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+    return FBME_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    g_static_error = "device ordinal outside the static scratch table";
+    return FBME_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_topk_scratch);
+    if (e != cudaSuccess || !p) {
+      g_static_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      return FBME_ERR_CUDA;
+    }
+    g_scratch_ptr[dev] = p;
+  }
+  *out = g_scratch_ptr[dev];
+  return FBME_OK;
+}
+
+}  // namespace
+
+extern "C" int fbme_topk_static(const float* scores, int64_t n, int32_t k, int32_t batch,
+                                int64_t* indices, float* values, fbme_stream_t stream) {
+  if (!scores || !indices || !values) {
+    g_static_error = "NULL argument";
+    return FBME_ERR_INVALID;
+  }
+  if (const char* why = fbme::topk_check(n, k, batch)) {
+    g_static_error = why;
+    return FBME_ERR_INVALID;
+  }
+  const size_t need = fbme::topk_scratch_bytes(n, k, batch);
+  if (need > kStaticScratchBytes) {
+    g_static_error = "fbme_topk_static: batch * ceil(n/8192) * k * 8 bytes exceeds the " +
+                     std::to_string(kStaticScratchBytes) + "-byte static scratch";
+    return FBME_ERR_INVALID;
+  }
+  void* scratch = nullptr;
+  const int rc = static_scratch(&scratch);
+  if (rc != FBME_OK) return rc;
+  // Every candidate slot is written before it is read: nothing to clear.
+  fbme::topk_scores(scores, n, k, batch, scratch, indices, values,
+                    reinterpret_cast<cudaStream_t>(stream));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_static_error = std::string("fbme_topk_static: ") + cudaGetErrorString(e);
+    return FBME_ERR_CUDA;
+  }
+  return FBME_OK;
+}
+
+extern "C" const char* fbme_topk_static_error(void) { return g_static_error.c_str(); }

@@ -162,6 +162,25 @@ size_t fbme_topk_workspace_bytes(int64_t n, int32_t k, int32_t batch);
 int fbme_topk(const float* scores, int64_t n, int32_t k, int32_t batch, void* workspace,
               size_t workspace_bytes, int64_t* indices, float* values, fbme_stream_t stream);
 
+/* Allocation-free top-k; no counterpart in the reference.  Same result as
+ * fbme_topk, for callers that cannot allocate device memory when they need
+ * it: code running while another component captures a CUDA graph (no
+ * allocation during global-mode capture), real-time hosts that freeze their
+ * memory budget after start-up, FFI hosts that only receive device pointers.
+ * The candidate scratch is a library-owned static device array of
+ * FBME_TOPK_STATIC_SCRATCH_BYTES (1 MiB), held by every GPU that loads the
+ * library until the process exits.  Requests needing more than that
+ * (batch * ceil(n/8192) * k * 8 bytes) return FBME_ERR_INVALID.  The first
+ * call on a device looks up the array's device address with that device
+ * current: make it before any stream capture.  All calls share the array
+ * (nothing in it needs to start at zero); calls that overlap on the GPU race
+ * on it, so the caller must order them.  Allocates nothing.  Error text:
+ * fbme_topk_static_error(). */
+#define FBME_TOPK_STATIC_SCRATCH_BYTES (1u << 20)
+int fbme_topk_static(const float* scores, int64_t n, int32_t k, int32_t batch, int64_t* indices,
+                     float* values, fbme_stream_t stream);
+const char* fbme_topk_static_error(void);
+
 /* Kernel groups timed by fbme_plan_profile. */
 enum {
   FBME_GROUP_INIT = 0,        /* A^H y, data power, prior/noise initialisation */
