@@ -96,6 +96,68 @@ class FbmeState(ctypes.Structure):
     ]
 
 
+class FbmeCgConfig(ctypes.Structure):
+    _fields_ = [
+        ("max_iter", c_int32),
+        ("min_iter", c_int32),
+        ("cg_min_iter", c_int32),
+        ("tol", c_float),
+        ("convergence_patience", c_int32),
+        ("convergence_check_interval", c_int32),
+        ("hyper_shape", c_float),
+        ("hyper_rate", c_float),
+        ("noise_shape", c_float),
+        ("noise_rate", c_float),
+        ("initial_noise_fraction", c_float),
+        ("initialization_blend", c_float),
+        ("fixed_noise_variance", c_float),
+        ("noise_update", c_int32),
+        ("damping", c_float),
+        ("cg_damping", c_float),
+        ("min_variance", c_float),
+        ("max_precision", c_float),
+        ("cg_tolerance", c_float),
+        ("cg_initial_tolerance", c_float),
+        ("cg_max_iter", c_int32),
+        ("cg_check_interval", c_int32),
+        ("cg_fixed_iterations", c_int32),
+        ("preconditioner_rank", c_int32),
+        ("probes", c_int32),
+        ("initial_probes", c_int32),
+        ("adaptive_cg", c_int32),
+        ("adaptive_probes", c_int32),
+        ("warm_start", c_int32),
+        ("jitter_multiplier", c_float),
+        ("dft_terms", c_int32),
+    ]
+
+
+class FbmeCgOutputs(ctypes.Structure):
+    _fields_ = [
+        ("x", c_void_p),
+        ("posterior_variance", c_void_p),
+        ("precision", c_void_p),
+        ("noise_variance", c_void_p),
+        ("effective_dof", c_void_p),
+        ("support_mask", c_void_p),
+        ("support_threshold", c_float),
+        ("status", c_void_p),
+    ]
+
+
+class FbmeCgInfo(ctypes.Structure):
+    _fields_ = [
+        ("iterations", c_int32),
+        ("converged", c_int32),
+        ("relative_change", c_float),
+        ("last_cg_iterations", c_int32),
+        ("history", POINTER(c_float)),
+    ]
+
+
+CG_HISTORY_COLUMNS = ("relative_change", "noise_variance", "effective_dof", "cg_iterations",
+                      "hutchinson_probes", "cg_tolerance")
+
 # Every symbol include/fbme_b200.h declares, with its ctypes signature.
 SIGNATURES = {
     "fbme_plan_workspace_bytes": (c_size_t, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig)]),
@@ -117,6 +179,16 @@ SIGNATURES = {
     "fbme_topk_static": (c_int, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p,
                                  c_void_p]),
     "fbme_topk_static_error": (c_char_p, []),
+    "fbme_cg_workspace_bytes": (c_size_t, [POINTER(FbmeShape), c_int32, POINTER(FbmeCgConfig)]),
+    "fbme_cg_create": (c_int, [POINTER(FbmeShape), c_int32, POINTER(FbmeCgConfig), c_void_p,
+                               c_size_t, c_void_p, POINTER(c_void_p)]),
+    "fbme_cg_solve": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(FbmeCgOutputs),
+                              POINTER(FbmeCgInfo), c_void_p]),
+    "fbme_cg_destroy": (c_int, [c_void_p]),
+    "fbme_cg_matvec": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                               c_void_p]),
+    "fbme_pcg_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                               c_float, c_void_p, POINTER(c_int32), c_void_p]),
     "fbme_last_error": (c_char_p, []),
     "fbme_version": (c_char_p, []),
 }

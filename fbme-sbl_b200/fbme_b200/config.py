@@ -159,8 +159,11 @@ class SBLConfig:
     device: str | torch.device = "auto"
     return_history: bool = True
     verbose: bool = False
-    # B200 extension: split-BF16 products of the tensor-core DFT (3 or 6).
+    # B200 extension: split-BF16 products of the tensor-core DFT (3 or 6)
+    # for mode="uamp" and mode="cg".  Both stay within 1e-5 relative of the
+    # exact operator (FP32 tensor-core accumulation bounds the error).
     dft_terms: int = 3
+    cg_dft_terms: int = 3
 
     # ------------------------------------------------------------------ presets
     @classmethod
@@ -393,3 +396,4 @@ def _rules(c: SBLConfig):
            c.offgrid_max_iter < 1 or c.offgrid_tolerance <= 0.0 or c.offgrid_max_step <= 0.0
            or c.offgrid_damping <= 0.0 or c.offgrid_ridge < 0.0)
     yield "dft_terms must be 3 or 6.", c.dft_terms not in (3, 6)
+    yield "cg_dft_terms must be 3 or 6.", c.cg_dft_terms not in (3, 6)

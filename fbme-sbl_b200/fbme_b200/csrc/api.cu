@@ -161,6 +161,12 @@ fbme::DevConfig dev_config(const FbmeConfig& c) {
 
 }  // namespace
 
+namespace fbme {
+// Error reporting and table sizing shared with the cg translation unit.
+int api_fail(int code, const std::string& msg) { return fail(code, msg); }
+size_t dft_table_bytes(int L, int terms) { return table_bytes(L, terms); }
+}  // namespace fbme
+
 struct FbmePlan {
   fbme::BatchShape s;
   FbmeConfig cfg;

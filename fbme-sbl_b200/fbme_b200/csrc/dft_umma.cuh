@@ -12,9 +12,11 @@
 //
 // Precision: both operands are split into BF16 parts (x = hi + lo, or
 // hi + mid + lo) and the tensor core accumulates in FP32 the products of
-// order <= 1 (3 terms: hi*hi + hi*lo + lo*hi) or <= 2 (6 terms).  Measured
-// against an FP64 DFT at 256^2/128^2: 3 terms 5.3e-6 relative L2, 6 terms
-// 5.3e-8 (an FP32 FFT is 4.4e-8).
+// order <= 1 (3 terms: hi*hi + hi*lo + lo*hi) or <= 2 (6 terms).  The FP32
+// accumulation over the contracted axis, not the split, sets the error:
+// measured against an FP64 DFT on B200, one 2-D transform is 5-6e-6
+// relative L2 with 3 terms at 64^2/32^2 and 256^2/128^2, and 1-6e-6 with
+// 6 terms (an FP32 FFT is ~5e-8).
 //
 // Kernel organisation (one CTA = one 128-row x N_TILE-column output tile):
 //   warps 0-3  producer: read In through the prologue policy (fused
@@ -54,6 +56,7 @@ struct DftGeom {
   int vec4;                 // rows start on 16-byte boundaries (even strides)
   const uint8_t* table;     // pre-swizzled twiddle blocks
   int table_kchunks;        // K chunks per column tile in the table
+  int status_div;           // status word of a unit: status[unit / status_div]
 };
 
 struct TileCtx {
@@ -170,7 +173,7 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
       const TileCtx t = decode_tile(g, tile);
-      int* const st_scene = status ? status + t.scene : nullptr;
+      int* const st_scene = status ? status + t.scene / g.status_div : nullptr;
       for (int kc = 0; kc < g.kchunks && ok; ++kc, ++it) {
         const int s = it % kStages, use = it / kStages;
         uint8_t* st = smem + s * C::kStageBytes;
@@ -221,7 +224,7 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
       int it = 0, lt = 0;
       for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
         const TileCtx t = decode_tile(g, tile);
-        int* const st_scene = status ? status + t.scene : nullptr;
+        int* const st_scene = status ? status + t.scene / g.status_div : nullptr;
         const int acc = lt & 1, ause = lt >> 1;
         if (lt >= 2) ok = mbar_wait(&acce_bar[acc], (ause - 1) & 1, st_scene);
         if (!ok) break;
@@ -258,7 +261,7 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
     int lt = 0;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
       const TileCtx t = decode_tile(g, tile);
-      int* const st_scene = status ? status + t.scene : nullptr;
+      int* const st_scene = status ? status + t.scene / g.status_div : nullptr;
       const int acc = lt & 1;
       ok = mbar_wait(&accf_bar[acc], (lt >> 1) & 1, st_scene);
       tc_fence_after();

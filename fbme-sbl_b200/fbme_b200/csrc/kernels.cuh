@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "../../../include/fbme_b200.h"
 
 namespace fbme {
@@ -108,6 +110,8 @@ void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float
                  float2* data, float2* tmp, int* status, cudaStream_t st);
 void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
                  float2* coeff, float2* tmp, int* status, cudaStream_t st);
+void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
+              cudaStream_t st, Profiler* prof = nullptr);
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
               cudaStream_t st, Profiler* prof = nullptr);
 
@@ -139,5 +143,10 @@ const char* topk_check(long long n, int k, int batch);
 void topk_scores(const float* scores, long long n, int k, int batch, void* scratch,
                  int64_t* indices, float* values, cudaStream_t st);
 int exchange_blocks(const BatchShape& s);
+
+// Shared by the C ABI translation units.
+int api_fail(int code, const std::string& msg);
+size_t dft_table_bytes(int L, int terms);
+cudaError_t set_cg_attributes();
 
 }  // namespace fbme

@@ -1,0 +1,183 @@
+// Host-side geometry and launch helpers of the tcgen05 DFT stage kernel,
+// plus the partial-sum and load helpers shared by the UAMP and PCG
+// translation units.
+//
+// A "unit" is one independent 2-D transform: a scene for the UAMP sweeps,
+// a (scene, right-hand side) pair for the PCG matvecs.  Units are laid out
+// back to back, so every stage is described by its per-unit strides.
+#pragma once
+
+#include "dft_umma.cuh"
+#include "kernels.cuh"
+
+namespace fbme {
+
+constexpr float kTiny = 1.17549435e-38f;  // FLT_MIN (torch.finfo(float32).tiny)
+constexpr float kEps = 1.1920929e-07f;    // FLT_EPSILON
+
+// ---------------------------------------------------------------------------
+// partial-sum helpers
+// ---------------------------------------------------------------------------
+FBME_DEV double* part_slot(double* part, int unit, int tile, int slot) {
+  return part + (static_cast<long long>(unit) * kMaxTilesPerScene + tile) * kPartSlots + slot;
+}
+FBME_DEV void write_block_partial(double v, double* red, double* part, int unit, int tile,
+                                  int slot) {
+  const double s = block_sum(v, red);
+  if (threadIdx.x == 0) *part_slot(part, unit, tile, slot) = s;
+}
+// Reduction `sum` of one tile: warp `w` (of the stage's producer or
+// epilogue group) writes its warp total to slot sum*kPartWarps + w.
+FBME_DEV void warp_partial(double v, double* part, const TileCtx& t, int sum, int w, int lane) {
+  v = warp_sum(v);
+  if (lane == 0)
+    *part_slot(part, t.scene, t.row_tile * t.g->col_tiles + t.col_tile, sum * kPartWarps + w) = v;
+}
+// Sum of reduction `sum` of one unit over `tiles` tiles x `warps` slots,
+// in a fixed order.
+FBME_DEV double unit_sum(const double* part, int unit, int sum, int tiles, int warps) {
+  double v = 0.0;
+  for (int t = 0; t < tiles; ++t)
+    for (int w = 0; w < warps; ++w)
+      v += part[(static_cast<long long>(unit) * kMaxTilesPerScene + t) * kPartSlots +
+                sum * kPartWarps + w];
+  return v;
+}
+
+FBME_DEV bool vec_ok(const DftGeom& g) { return g.vec4 != 0; }
+
+// Two consecutive complex values at base[e] through the read-only path.
+FBME_DEV void load2c(const float2* base, long long e, int avail, bool vec, float2& a, float2& b) {
+  if (avail >= 2 && vec) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(base + e));
+    a = make_float2(v.x, v.y);
+    b = make_float2(v.z, v.w);
+  } else {
+    a = __ldg(base + e);
+    b = avail >= 2 ? __ldg(base + e + 1) : make_float2(0.f, 0.f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// elementwise launch shape
+// ---------------------------------------------------------------------------
+constexpr int kEwThreads = 256;
+
+FBME_DEV int ew_blocks_per_scene(long long n) {
+  long long b = (n + 2047) / 2048;
+  return static_cast<int>(b < kMaxTilesPerScene ? (b < 1 ? 1 : b) : kMaxTilesPerScene);
+}
+static inline int ew_blocks_host(long long n) {
+  long long b = (n + 2047) / 2048;
+  return static_cast<int>(b < kMaxTilesPerScene ? (b < 1 ? 1 : b) : kMaxTilesPerScene);
+}
+
+// Partial-sum source of one reduction: tiles x warps per tile.
+struct PartSrc {
+  int tiles, warps;
+};
+
+// ---------------------------------------------------------------------------
+// stage geometry
+// ---------------------------------------------------------------------------
+static inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+static inline DftGeom make_geom(int units, int rows, int kcplx, int cols, int in_ld,
+                                long long in_stride, int out_ld, long long out_stride,
+                                const uint8_t* table, int table_kchunks, int n_tile,
+                                int status_div = 1) {
+  DftGeom g;
+  g.n_scenes = units;
+  g.rows = rows;
+  g.row_tiles = ceil_div(rows, kTileRows);
+  g.kcplx = kcplx;
+  g.kchunks = ceil_div(2LL * kcplx, kKChunk);
+  g.cols = cols;
+  g.col_tiles = ceil_div(2LL * cols, n_tile);
+  g.in_ld = in_ld;
+  g.in_stride = in_stride;
+  g.out_ld = out_ld;
+  g.out_stride = out_stride;
+  g.col_per_tile = n_tile / 2;
+  g.vec4 = (in_ld % 2 == 0) && (in_stride % 2 == 0);
+  g.table = table;
+  g.table_kchunks = table_kchunks;
+  g.status_div = status_div;
+  return g;
+}
+
+enum Stage { kFwd1, kFwd2, kAdj1, kAdj2 };
+
+// The four stages of the prefix operator for `units` transforms of shape s
+// (s.B is ignored); status words are indexed by unit / status_div.
+static inline DftGeom stage_geom_units(Stage st, const BatchShape& s, const DftTables& t,
+                                       int n_tile, int units, int status_div) {
+  const long long N = s.n(), M = s.m();
+  switch (st) {
+    case kFwd1:  // [n1][n2] -> [m2][n1], contract n2
+      return make_geom(units, s.n1, s.n2, s.m2, s.n2, N, s.n1, 1LL * s.m2 * s.n1, t.fwd_n2,
+                       t.kchunks_n2, n_tile, status_div);
+    case kFwd2:  // [m2][n1] -> [m1][m2], contract n1
+      return make_geom(units, s.m2, s.n1, s.m1, s.n1, 1LL * s.m2 * s.n1, s.m2, M, t.fwd_n1,
+                       t.kchunks_n1, n_tile, status_div);
+    case kAdj1:  // [m1][m2] -> [n2][m1], contract m2
+      return make_geom(units, s.m1, s.m2, s.n2, s.m2, M, s.m1, 1LL * s.n2 * s.m1, t.adj_n2,
+                       t.kchunks_n2, n_tile, status_div);
+    default:     // [n2][m1] -> [n1][n2], contract m1
+      return make_geom(units, s.n2, s.m1, s.n1, s.m1, 1LL * s.n2 * s.m1, s.n2, N, t.adj_n1,
+                       t.kchunks_n1, n_tile, status_div);
+  }
+}
+static inline DftGeom stage_geom(Stage st, const BatchShape& s, const DftTables& t, int n_tile) {
+  return stage_geom_units(st, s, t, n_tile, s.B, 1);
+}
+
+static inline int tiles(const DftGeom& g) { return g.n_scenes * g.row_tiles * g.col_tiles; }
+
+static inline int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+      n = 148;
+  }
+  return n;
+}
+
+static inline int persistent_grid(const DftGeom& g) {
+  const int t = tiles(g), s = sm_count();
+  return t < s ? t : s;
+}
+
+static inline int n_tile_of(int terms) { return terms == 6 ? 128 : 256; }
+
+template <int A_PARTS, int N_TILE, class Pro, class Epi>
+static cudaError_t set_attr() {
+  return cudaFuncSetAttribute(dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              DftCfg<A_PARTS, N_TILE>::kSmemBytes);
+}
+
+template <class Pro, class Epi>
+static void run_stage(int terms, const DftGeom& g, const Pro& pro, const Epi& epi, int* status,
+                      cudaStream_t st) {
+  if (terms == 6) {
+    dft_stage_kernel<3, 128, Pro, Epi>
+        <<<persistent_grid(g), kDftPersistThreads, DftCfg<3, 128>::kSmemBytes, st>>>(g, pro, epi,
+                                                                                     status);
+  } else {
+    dft_stage_kernel<2, 256, Pro, Epi>
+        <<<persistent_grid(g), kDftPersistThreads, DftCfg<2, 256>::kSmemBytes, st>>>(g, pro, epi,
+                                                                                     status);
+  }
+}
+
+template <class Pro, class Epi>
+static cudaError_t set_attr_both() {
+  cudaError_t e = set_attr<2, 256, Pro, Epi>();
+  if (e != cudaSuccess) return e;
+  return set_attr<3, 128, Pro, Epi>();
+}
+
+}  // namespace fbme

@@ -20,44 +20,9 @@
 
 #include "dft_umma.cuh"
 #include "kernels.cuh"
+#include "stage.cuh"
 
 namespace fbme {
-
-constexpr float kTiny = 1.17549435e-38f;  // FLT_MIN (torch.finfo(float32).tiny)
-constexpr float kEps = 1.1920929e-07f;    // FLT_EPSILON
-
-// ---------------------------------------------------------------------------
-// partial-sum helpers
-// ---------------------------------------------------------------------------
-FBME_DEV double* part_slot(double* part, int scene, int tile, int slot) {
-  return part + (static_cast<long long>(scene) * kMaxTilesPerScene + tile) * kPartSlots + slot;
-}
-FBME_DEV void write_block_partial(double v, double* red, double* part, int scene, int tile,
-                                  int slot) {
-  const double s = block_sum(v, red);
-  if (threadIdx.x == 0) *part_slot(part, scene, tile, slot) = s;
-}
-// Reduction `sum` of one tile: warp `w` (of the stage's producer or
-// epilogue group) writes its warp total to slot sum*kPartWarps + w.
-FBME_DEV void warp_partial(double v, double* part, const TileCtx& t, int sum, int w, int lane) {
-  v = warp_sum(v);
-  if (lane == 0)
-    *part_slot(part, t.scene, t.row_tile * t.g->col_tiles + t.col_tile, sum * kPartWarps + w) = v;
-}
-
-FBME_DEV bool vec_ok(const DftGeom& g) { return g.vec4 != 0; }
-
-// Two consecutive complex values at base[e] through the read-only path.
-FBME_DEV void load2c(const float2* base, long long e, int avail, bool vec, float2& a, float2& b) {
-  if (avail >= 2 && vec) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(base + e));
-    a = make_float2(v.x, v.y);
-    b = make_float2(v.z, v.w);
-  } else {
-    a = __ldg(base + e);
-    b = avail >= 2 ? __ldg(base + e + 1) : make_float2(0.f, 0.f);
-  }
-}
 
 // ---------------------------------------------------------------------------
 // prologues
@@ -317,17 +282,6 @@ struct EpiDenoise {
 // ---------------------------------------------------------------------------
 // elementwise kernels
 // ---------------------------------------------------------------------------
-constexpr int kEwThreads = 256;
-
-FBME_DEV int ew_blocks_per_scene(long long n) {
-  long long b = (n + 2047) / 2048;
-  return static_cast<int>(b < kMaxTilesPerScene ? (b < 1 ? 1 : b) : kMaxTilesPerScene);
-}
-static int ew_blocks_host(long long n) {
-  long long b = (n + 2047) / 2048;
-  return static_cast<int>(b < kMaxTilesPerScene ? (b < 1 ? 1 : b) : kMaxTilesPerScene);
-}
-
 // Initial prior variances (solver.py:1063-1099): backprojection blend or
 // uniform, floored; per-block sums of the result.
 __global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevConfig c, Scalars sc,
@@ -403,11 +357,6 @@ __global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevCon
 // Per-scene scalar updates from the per-tile sums (fixed summation order).
 enum ScalarMode { kScalarInit1 = 0, kScalarInit2 = 1, kScalarSweep = 2 };
 
-// Partial-sum source of one reduction: tiles x warps per tile.
-struct PartSrc {
-  int tiles, warps;
-};
-
 __global__ void scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part,
                                PartSrc p0, PartSrc p1, PartSrc p2) {
   const int scene = blockIdx.x * blockDim.x + threadIdx.x;
@@ -466,96 +415,6 @@ __global__ void scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, 
 // ---------------------------------------------------------------------------
 // stage geometry and launch
 // ---------------------------------------------------------------------------
-static int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
-
-static DftGeom make_geom(int B, int rows, int kcplx, int cols, int in_ld, long long in_stride,
-                         int out_ld, long long out_stride, const uint8_t* table, int table_kchunks,
-                         int n_tile) {
-  DftGeom g;
-  g.n_scenes = B;
-  g.rows = rows;
-  g.row_tiles = ceil_div(rows, kTileRows);
-  g.kcplx = kcplx;
-  g.kchunks = ceil_div(2LL * kcplx, kKChunk);
-  g.cols = cols;
-  g.col_tiles = ceil_div(2LL * cols, n_tile);
-  g.in_ld = in_ld;
-  g.in_stride = in_stride;
-  g.out_ld = out_ld;
-  g.out_stride = out_stride;
-  g.col_per_tile = n_tile / 2;
-  g.vec4 = (in_ld % 2 == 0) && (in_stride % 2 == 0);
-  g.table = table;
-  g.table_kchunks = table_kchunks;
-  return g;
-}
-
-enum Stage { kFwd1, kFwd2, kAdj1, kAdj2 };
-
-static DftGeom stage_geom(Stage st, const BatchShape& s, const DftTables& t, int n_tile) {
-  const long long N = s.n(), M = s.m();
-  switch (st) {
-    case kFwd1:  // [n1][n2] -> [m2][n1], contract n2
-      return make_geom(s.B, s.n1, s.n2, s.m2, s.n2, N, s.n1, 1LL * s.m2 * s.n1, t.fwd_n2,
-                       t.kchunks_n2, n_tile);
-    case kFwd2:  // [m2][n1] -> [m1][m2], contract n1
-      return make_geom(s.B, s.m2, s.n1, s.m1, s.n1, 1LL * s.m2 * s.n1, s.m2, M, t.fwd_n1,
-                       t.kchunks_n1, n_tile);
-    case kAdj1:  // [m1][m2] -> [n2][m1], contract m2
-      return make_geom(s.B, s.m1, s.m2, s.n2, s.m2, M, s.m1, 1LL * s.n2 * s.m1, t.adj_n2,
-                       t.kchunks_n2, n_tile);
-    default:     // [n2][m1] -> [n1][n2], contract m1
-      return make_geom(s.B, s.n2, s.m1, s.n1, s.m1, 1LL * s.n2 * s.m1, s.n2, N, t.adj_n1,
-                       t.kchunks_n1, n_tile);
-  }
-}
-
-static int tiles(const DftGeom& g) { return g.n_scenes * g.row_tiles * g.col_tiles; }
-
-static int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
-      n = 148;
-  }
-  return n;
-}
-
-static int persistent_grid(const DftGeom& g) {
-  const int t = tiles(g), s = sm_count();
-  return t < s ? t : s;
-}
-
-template <int A_PARTS, int N_TILE, class Pro, class Epi>
-static cudaError_t set_attr() {
-  return cudaFuncSetAttribute(dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              DftCfg<A_PARTS, N_TILE>::kSmemBytes);
-}
-
-template <class Pro, class Epi>
-static void run_stage(int terms, const DftGeom& g, const Pro& pro, const Epi& epi, int* status,
-                      cudaStream_t st) {
-  if (terms == 6) {
-    dft_stage_kernel<3, 128, Pro, Epi>
-        <<<persistent_grid(g), kDftPersistThreads, DftCfg<3, 128>::kSmemBytes, st>>>(g, pro, epi,
-                                                                                     status);
-  } else {
-    dft_stage_kernel<2, 256, Pro, Epi>
-        <<<persistent_grid(g), kDftPersistThreads, DftCfg<2, 256>::kSmemBytes, st>>>(g, pro, epi,
-                                                                                     status);
-  }
-}
-
-template <class Pro, class Epi>
-static cudaError_t set_attr_both() {
-  cudaError_t e = set_attr<2, 256, Pro, Epi>();
-  if (e != cudaSuccess) return e;
-  return set_attr<3, 128, Pro, Epi>();
-}
-
 cudaError_t set_dft_attributes() {
   cudaError_t e;
   if ((e = set_attr_both<ProPlain, EpiStoreT>()) != cudaSuccess) return e;
@@ -566,8 +425,6 @@ cudaError_t set_dft_attributes() {
   if ((e = set_attr_both<ProPlain, EpiDenoise>()) != cudaSuccess) return e;
   return cudaSuccess;
 }
-
-static int n_tile_of(int terms) { return terms == 6 ? 128 : 256; }
 
 void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
                  float2* data, float2* tmp, int* status, cudaStream_t st) {
@@ -585,6 +442,33 @@ void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float
   run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{coeff}, status, st);
 }
 
+// Initialisation shared by the UAMP and PCG paths (solver.py:1063-1159):
+// A^H y, data power, variance floor, initial noise and the initial prior
+// variances (backprojection blend or uniform).
+void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
+              cudaStream_t st, Profiler* prof) {
+  const int nt = n_tile_of(c.terms);
+  const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
+  const int sc_blocks = ceil_div(s.B, 128);
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f},
+                       u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(
+                 kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, 4},
+                 PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
+  const int bn = ew_blocks_host(s.n());
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             (gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma,
+                                                                  u.part)));
+  FBME_TIMED(prof, FBME_GROUP_INIT,
+             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit2, s, c, u.sc, u.part,
+                                                        PartSrc{bn, 1}, PartSrc{0, 0},
+                                                        PartSrc{0, 0})));
+}
+
 // Message buffers ping-pong between sweeps: msg[0] / msg[1] are both
 // M-sized regions starting at u.msg and u.msg + B*M.
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
@@ -596,25 +480,8 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   const long long BM = static_cast<long long>(s.B) * s.m();
   float2* msg[2] = {u.msg, u.msg + BM};
 
-  // --- initialisation: A^H y, data power, floors, initial noise, prior ---
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st));
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f},
-                       u.status, st));
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(
-                 kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, 4},
-                 PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
+  sbl_init(s, t, c, u, st, prof);
   const int bn = ew_blocks_host(s.n()), bm = ew_blocks_host(s.m());
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             (gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma,
-                                                                  u.part)));
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit2, s, c, u.sc, u.part,
-                                                        PartSrc{bn, 1}, PartSrc{0, 0},
-                                                        PartSrc{0, 0})));
-
   DenoiseArgs da;
   da.mu = u.mu;
   da.var = u.var;

@@ -111,6 +111,8 @@ class FBMEEngine:
         self.lib = nat.lib()
         if device.type != "cuda":
             raise RuntimeError("the FBME B200 engine needs a CUDA device")
+        if device.index is None:
+            device = torch.device("cuda", torch.cuda.current_device())
         self.device = device
         self.batch = int(batch)
         self.grid = tuple(int(v) for v in grid)

@@ -181,6 +181,93 @@ int fbme_topk_static(const float* scores, int64_t n, int32_t k, int32_t batch, i
                      float* values, fbme_stream_t stream);
 const char* fbme_topk_static_error(void);
 
+/* ------------------------------------------------------------------------
+ * mode="cg": PCG + Hutchinson SBL for a batch of equally shaped scenes.
+ *
+ * Replaces (FBME-SBL v1.1):
+ *   fbme_cg_solve     <-> torch_sbl/solver.py:925-2393 (fast_sbl) with
+ *                         mode="cg": initialisation 1063-1159, probe setup
+ *                         1191-1221, EM loop 1315-1904 (_posterior cg
+ *                         branch 2991-3036, relevance 3156-3181, MacKay
+ *                         update 1669-1677, noise update 1737-1791,
+ *                         convergence 1800-1904), final posterior 2023-2080
+ *   fbme_pcg_solve    <-> torch_sbl/solver.py:5582-5723 (_pcg) with the
+ *                         low-rank preconditioner 5786-5848
+ *   fbme_cg_matvec    <-> torch_sbl/operators.py:299-371 (Q = noise I +
+ *                         A diag(prior) A^H; toeplitz_matvec / matvec)
+ * The active-set switch of single-scene runs (solver.py:1316-1341) is not
+ * part of this entry point: the host runs it with active_set off.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int32_t max_iter, min_iter;           /* outer EM iterations */
+  int32_t cg_min_iter;
+  float tol;                            /* relative change tolerance (0: off) */
+  int32_t convergence_patience, convergence_check_interval;
+  float hyper_shape, hyper_rate, noise_shape, noise_rate;
+  float initial_noise_fraction;
+  float initialization_blend;           /* < 0: uniform initialisation */
+  float fixed_noise_variance;           /* > 0: fixed noise variance */
+  int32_t noise_update;                 /* 0 = EM, 1 = evidence */
+  float damping, cg_damping;            /* keep = max(damping, cg_damping) */
+  float min_variance, max_precision;
+  float cg_tolerance, cg_initial_tolerance;
+  int32_t cg_max_iter, cg_check_interval, cg_fixed_iterations;
+  int32_t preconditioner_rank;          /* low-rank preconditioner atoms (<= 32) */
+  int32_t probes;                       /* maximum Hutchinson probes P */
+  int32_t initial_probes;               /* adaptive schedule: probes of iterations 1-5 */
+  int32_t adaptive_cg, adaptive_probes, warm_start;
+  float jitter_multiplier;              /* Cholesky loading: max(10, m) * eps * mean|diag| */
+  int32_t dft_terms;                    /* 3 or 6 split-BF16 products */
+} FbmeCgConfig;
+
+/* Device outputs of fbme_cg_solve (shapes [B][N1][N2] / [B]). */
+typedef struct {
+  void* x;                       /* complex64 posterior mean */
+  float* posterior_variance;
+  float* precision;              /* 1 / prior variance */
+  float* noise_variance;
+  float* effective_dof;
+  uint8_t* support_mask;         /* optional: |x|^2 / max(v, tiny) > support_threshold */
+  float support_threshold;       /* used when support_mask is set (solver.py:2108-2126) */
+  int32_t* status;               /* FBME_STATUS_* bits per scene */
+} FbmeCgOutputs;
+
+/* Host-side run summary.  `history`, if not NULL, receives max_iter rows of
+ * {relative change (max over scenes), mean noise variance, mean effective
+ * DOF, PCG iterations, probes, PCG tolerance} for the iterations run. */
+typedef struct {
+  int32_t iterations;
+  int32_t converged;
+  float relative_change;
+  int32_t last_cg_iterations;
+  float* history;
+} FbmeCgInfo;
+
+typedef struct FbmeCgPlan FbmeCgPlan;
+
+size_t fbme_cg_workspace_bytes(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig* cfg);
+int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig* cfg,
+                   void* workspace, size_t workspace_bytes, fbme_stream_t stream,
+                   FbmeCgPlan** plan);
+/* y: complex64 [B][M1][M2]; probes: float32 +-1 [B][P][M1][M2] (probe p of
+ * scene b over the observed samples, the reference's probes[b, :, p]).
+ * Synchronises `stream` at PCG restart checks and convergence checks, as
+ * the reference reads those flags on the host. */
+int fbme_cg_solve(FbmeCgPlan* plan, const void* y, const float* probes, const FbmeCgOutputs* out,
+                  FbmeCgInfo* info, fbme_stream_t stream);
+int fbme_cg_destroy(FbmeCgPlan* plan);
+/* out = Q v for `rhs` vectors per scene: v, out complex64 [B][rhs][M1][M2];
+ * prior float [B][N1][N2]; noise float [B]; rhs <= 1 + P. */
+int fbme_cg_matvec(FbmeCgPlan* plan, const float* prior, const float* noise, const void* v,
+                   int32_t rhs, void* out, fbme_stream_t stream);
+/* One preconditioned solve Q X = RHS (rhs columns per scene, layout as
+ * fbme_cg_matvec), initial guess `initial` (NULL: zero), with the plan's
+ * cg_max_iter / cg_check_interval / cg_fixed_iterations / rank.  Writes the
+ * solution and the iteration count of the last loop. */
+int fbme_pcg_solve(FbmeCgPlan* plan, const float* prior, const float* noise, const void* rhs,
+                   int32_t rhs_count, const void* initial, float tolerance, void* solution,
+                   int32_t* iterations, fbme_stream_t stream);
+
 /* Kernel groups timed by fbme_plan_profile. */
 enum {
   FBME_GROUP_INIT = 0,        /* A^H y, data power, prior/noise initialisation */

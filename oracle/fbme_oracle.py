@@ -78,6 +78,7 @@ class OracleConfig:
     convergence_patience: int = 2
     convergence_check_interval: int = 2
     cuda_cholesky_jitter_multiplier: float = 8.0
+    cg_matvec: str = "tbt"
     uamp_damping: float = 0.1
     uamp_adaptive_damping: bool = True
     uamp_max_damping: float = 0.8
@@ -753,3 +754,286 @@ def fbme_solve(data, grid, profile: str = "stable", *, polish_size: int = 32,
     """The FBME-Fast / FBME-Stable plan replay (profiles.py:35-148)."""
     cfg = OracleConfig.stable(polish_size) if profile == "stable" else OracleConfig.fastest(polish_size)
     return fast_sbl_uamp(data, grid, cfg, chol_mode=chol_mode)
+
+
+# ---------------------------------------------------------------------------
+# mode="cg": PCG + Hutchinson posterior (solver.py:1194-1221, 1314-1904,
+# 2991-3036, 3156-3181, 5582-5848, 6086-6138)
+# ---------------------------------------------------------------------------
+
+
+def cg_probe_count(cfg: OracleConfig, n_grid: int, n_samples: int) -> int:
+    """solver.py:1193-1208."""
+    maximum = cfg.hutchinson_probes
+    if cfg.auto_probe_scaling:
+        under = n_grid / n_samples
+        rec = 8.0 * under ** 0.5
+        if under > 16.0:
+            rec = max(rec, 2.0 * under)
+        maximum = min(cfg.max_hutchinson_probes, max(cfg.hutchinson_probes, int(rec + 0.999999)))
+    return maximum
+
+
+def cg_schedule(iteration: int, cfg: OracleConfig, maximum_probes: int):
+    """solver.py:6086-6118 (probe count, tolerance)."""
+    if not cfg.adaptive_cg:
+        return maximum_probes, cfg.cg_tolerance
+    initial = min(cfg.initial_hutchinson_probes, maximum_probes) if cfg.adaptive_probes else maximum_probes
+    if iteration <= 5:
+        return initial, max(cfg.cg_initial_tolerance, cfg.cg_tolerance)
+    if iteration <= 15:
+        mid = (min(maximum_probes, max(initial, min(24, maximum_probes))) if cfg.adaptive_probes
+               else maximum_probes)
+        return mid, max(cfg.cg_tolerance, (cfg.cg_initial_tolerance * cfg.cg_tolerance) ** 0.5)
+    return maximum_probes, cfg.cg_tolerance
+
+
+def rademacher_probes(batch: int, n_samples: int, count: int, seed: int):
+    """solver.py:5979-6000 with torch's CPU generator (the reference's
+    stream on CPU).  Returns [B, M, P] complex."""
+    import torch
+
+    g = torch.Generator(device="cpu")
+    g.manual_seed(seed)
+    r = 2 * torch.randint(0, 2, (batch, n_samples, count), generator=g) - 1
+    return r.numpy().astype(np.float64)
+
+
+def low_rank_preconditioner(prior, noise, op: PrefixOperator, rank: int, chol_mode: str,
+                            jitter_multiplier: float):
+    """solver.py:5786-5833."""
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    rank = min(rank, op.n_samples, op.n_grid)
+    total = prior.sum(axis=1, dtype=rd)
+    if rank == 0:
+        return (noise + total).astype(rd), None, None
+    idx = _topk_indices(prior, rank)
+    vals = np.take_along_axis(prior, idx, axis=1)
+    cols = op.fourier_columns(idx)
+    factors = (cols * np.sqrt(vals)[:, None, :]).astype(op.cdtype)
+    omitted = np.maximum(total - vals.sum(axis=1, dtype=rd), rd(0.0))
+    background = np.maximum(noise + omitted, eps * total).astype(rd)
+    gram = np.conj(np.swapaxes(factors, 1, 2)) @ factors
+    eye = np.eye(rank, dtype=op.cdtype)
+    small = eye + gram / background[:, None, None]
+    small = rd(0.5) * (small + np.conj(np.swapaxes(small, 1, 2)))
+    chol = _stable_cholesky(small, tiny, eps, mode=chol_mode, multiplier=max(10.0, jitter_multiplier),
+                            fallback=(10.0, 1e2, 1e3, 1e4, 1e5))
+    if chol is None:
+        return (noise + total).astype(rd), None, None
+    inv = np.linalg.inv(chol)
+    small_inv = np.conj(np.swapaxes(inv, 1, 2)) @ inv
+    return background, factors, small_inv
+
+
+def apply_low_rank(value, pre):
+    """solver.py:5836-5848."""
+    background, factors, small_inv = pre
+    base = value / background[:, None, None]
+    if factors is None:
+        return base
+    projected = np.conj(np.swapaxes(factors, 1, 2)) @ value
+    w = small_inv @ (projected / background[:, None, None])
+    return base - (factors @ w) / background[:, None, None]
+
+
+def pcg(rhs, prior, noise, op: PrefixOperator, cfg: OracleConfig, *, initial, tolerance,
+        chol_mode="cuda", matvec_mode="tbt"):
+    """solver.py:5582-5723 with the low-rank preconditioner.  ``matvec``
+    "tbt" (the default, solver.py:2995-2999) applies Q through its BTTB
+    embedding spectrum (operators.py:299-355); "fourier" applies
+    Q v = noise v + A(prior * A^H v) (operators.py:357-371).
+    ``fixed_iterations > 0`` keeps the best checkpoint (solver.py:5631-5694)."""
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    fixed_iterations = cfg.cg_fixed_iterations
+    if matvec_mode == "tbt":
+        spectrum = op.toeplitz_spectrum(prior, noise)
+
+        def matvec(v):
+            return op.toeplitz_matvec(v, spectrum)
+    else:
+        def matvec(v):
+            return noise[:, None, None] * v + op.forward(prior[:, :, None] * op.adjoint(v))
+
+    if initial is None:
+        x = np.zeros_like(rhs)
+        r = rhs.copy()
+    else:
+        x = initial.copy()
+        r = rhs - matvec(x)
+    pre = low_rank_preconditioner(prior, noise, op, cfg.cg_preconditioner_rank, chol_mode,
+                                  cfg.cuda_cholesky_jitter_multiplier)
+    z = apply_low_rank(r, pre)
+    d = z.copy()
+    rho = np.real((np.conj(r) * z).sum(axis=1))
+    init_norm = np.maximum(np.linalg.norm(rhs, axis=1), eps)
+    best_x = x.copy() if fixed_iterations > 0 else None
+    best_rel = np.linalg.norm(r, axis=1) / init_norm if fixed_iterations > 0 else None
+    active = np.linalg.norm(r, axis=1) > tolerance * init_norm
+    d = np.where(active[:, None, :], d, 0)
+    it = 0
+    limit = fixed_iterations if fixed_iterations > 0 else cfg.cg_max_iter
+    for it in range(1, limit + 1):
+        qd = matvec(d)
+        curv = np.real((np.conj(d) * qd).sum(axis=1))
+        valid = active & np.isfinite(curv) & np.isfinite(rho) & (curv > tiny) & (rho > tiny)
+        alpha = np.where(valid, rho / np.maximum(curv, tiny), 0.0)
+        x = x + alpha[:, None, :] * d
+        r = r - alpha[:, None, :] * qd
+        active = valid
+        if it % cfg.cg_check_interval == 0 or it == limit:
+            r = rhs - matvec(x)
+            rel = np.linalg.norm(r, axis=1) / init_norm
+            if fixed_iterations > 0:
+                improved = rel < best_rel
+                best_x = np.where(improved[:, None, :], x, best_x)
+                best_rel = np.minimum(best_rel, rel)
+            res_active = np.isfinite(rel) & (rel > tolerance)
+            active = active & res_active if fixed_iterations > 0 else res_active
+            z = apply_low_rank(r, pre)
+            rr = np.real((np.conj(r) * z).sum(axis=1))
+            active = active & np.isfinite(rr) & (rr > tiny)
+            d = np.where(active[:, None, :], z, 0)
+            rho = np.where(active, rr, rho)
+            if fixed_iterations == 0 and not active.any():
+                break
+            continue
+        z = apply_low_rank(r, pre)
+        new_rho = np.real((np.conj(r) * z).sum(axis=1))
+        upd = active & np.isfinite(new_rho) & (new_rho > tiny)
+        beta = np.where(upd, new_rho / np.maximum(rho, tiny), 0.0)
+        d = z + beta[:, None, :] * d
+        d = np.where(upd[:, None, :], d, 0)
+        rho = np.where(upd, new_rho, rho)
+        active = upd
+    out = best_x if best_x is not None else x
+    return out.astype(op.cdtype), it
+
+
+def project_relevance(prior, dd, n_samples, eps):
+    """solver.py:3156-3181."""
+    rel = np.clip(prior * dd, 0, 1)
+    raw = rel.sum(axis=1)
+    scale = np.minimum(1.0, n_samples * (1.0 - 10.0 * eps) / np.maximum(raw, eps))
+    return rel * scale[:, None]
+
+
+def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda"):
+    """``fast_sbl`` with ``mode="cg"`` and ``active_set=False`` (or batch >
+    1, where the reference never switches).  ``probes``: [B, M, Pmax]
+    (default: the reference's CPU Rademacher stream)."""
+    data = np.asarray(data)
+    cdtype = np.complex128 if data.dtype in (np.complex128, np.float64) else np.complex64
+    single = data.ndim == 2
+    y3 = data[None] if single else data
+    b = y3.shape[0]
+    op = PrefixOperator(grid, y3.shape[1:], cdtype)
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    n, m = op.n_grid, op.n_samples
+    y = y3.reshape(b, m).astype(cdtype)
+    # initialisation: identical to the uamp branch (solver.py:1063-1159)
+    dp = np.maximum(_abs2(y).mean(axis=1, dtype=rd), eps).astype(rd)
+    floor = np.maximum(dp * rd(cfg.min_variance), tiny).astype(rd)
+    uniform = dp[:, None] / rd(n)
+    if cfg.initialization == "backprojection":
+        bp = op.adjoint_flat(y)
+        e = _abs2(bp)
+        structured = e / np.maximum(e.sum(axis=1, keepdims=True, dtype=rd), eps) * dp[:, None]
+        prior = rd(cfg.initialization_blend) * structured + rd(1 - cfg.initialization_blend) * uniform
+    else:
+        prior = np.broadcast_to(uniform, (b, n)).copy()
+    prior = np.maximum(prior, floor[:, None]).astype(rd)
+    noise = (np.full(b, cfg.fixed_noise_variance, rd) if cfg.fixed_noise_variance is not None
+             else np.maximum(rd(cfg.initial_noise_fraction) * dp, floor).astype(rd))
+    pmax = cg_probe_count(cfg, n, m)
+    if probes is None:
+        probes = rademacher_probes(b, m, pmax, cfg.seed)
+    probes = np.asarray(probes).astype(cdtype)
+    lifted_probes = op.adjoint(probes)
+    minimum = max(cfg.min_iter, cfg.cg_min_iter)
+    limit = cfg.max_iter
+    conv = cfg.tol > 0.0 and minimum < limit
+    keep = rd(max(cfg.damping, cfg.cg_damping))
+    prev_mean = np.zeros((b, n), cdtype)
+    solution = None
+    streak = 0
+    converged = False
+    hist = {"relative_change": [], "noise_variance": [], "effective_dof": [], "cg_iterations": []}
+    it = 0
+    for it in range(1, limit + 1):
+        count, tol_cg = cg_schedule(it, cfg, pmax)
+        tol_cg = max(tol_cg, 3.0 * float(eps) ** 0.5)
+        rhs = np.concatenate([y[:, :, None], probes[:, :, :count]], axis=2)
+        if cfg.cg_warm_start and solution is not None and solution.shape[2] != 1 + count:
+            rs = np.zeros((b, m, 1 + count), cdtype)
+            sh = min(1 + count, solution.shape[2])
+            rs[:, :, :sh] = solution[:, :, :sh]
+            solution = rs
+        sol, cg_it = pcg(rhs, prior, noise, op, cfg, initial=solution if cfg.cg_warm_start else None,
+                         tolerance=tol_cg, chol_mode=chol_mode, matvec_mode=cfg.cg_matvec)
+        lifted = op.adjoint(sol)
+        dd = np.maximum(np.real(lifted[:, :, 1:] * np.conj(lifted_probes[:, :, :count])).mean(axis=2),
+                        0.0).astype(rd)
+        mean = (prior * lifted[:, :, 0]).astype(cdtype)
+        pv = np.maximum(prior - np.square(prior) * dd, 0.0).astype(rd)
+        solution = sol if cfg.cg_warm_start else None
+        rel = project_relevance(prior, dd, m, eps).astype(rd)
+        dof = rel.sum(axis=1, dtype=rd)
+        # MacKay precision update (solver.py:1669-1677)
+        prec = (rel + rd(cfg.hyper_shape)) / (_abs2(mean) + rd(cfg.hyper_rate))
+        prec = np.clip(prec, rd(1.0 / cfg.max_precision), rd(cfg.max_precision))
+        new_prior = (rd(1.0) / prec).astype(rd)
+        # noise update (solver.py:1737-1768)
+        residual = y - op.forward_flat(mean)
+        energy = _abs2(residual).sum(axis=1, dtype=rd)
+        if cfg.fixed_noise_variance is not None:
+            new_noise = np.full(b, cfg.fixed_noise_variance, rd)
+        elif cfg.noise_update == "em":
+            new_noise = (energy + noise * dof + rd(cfg.noise_rate)) / rd(m + cfg.noise_shape)
+        else:
+            new_noise = (energy + rd(cfg.noise_rate)) / np.maximum(rd(m) - dof + rd(cfg.noise_shape), eps)
+        new_noise = np.maximum(new_noise, floor)
+        prior = np.maximum(keep * prior + (rd(1.0) - keep) * new_prior, floor[:, None]).astype(rd)
+        noise = (new_noise if cfg.fixed_noise_variance is not None
+                 else keep * noise + (rd(1.0) - keep) * new_noise).astype(rd)
+        should_check = conv and it >= minimum and ((it - minimum) % cfg.convergence_check_interval == 0
+                                                   or it == limit)
+        den = np.maximum(np.linalg.norm(mean, axis=1), eps)
+        change = float((np.linalg.norm(mean - prev_mean, axis=1) / den).max())
+        prev_mean = mean
+        hist["relative_change"].append(change)
+        hist["noise_variance"].append(float(noise.mean()))
+        hist["effective_dof"].append(float(dof.mean()))
+        hist["cg_iterations"].append(cg_it)
+        if should_check:
+            streak = streak + 1 if change <= cfg.tol else 0
+            if streak >= cfg.convergence_patience:
+                converged = True
+                break
+    # final posterior with all probes (solver.py:2023-2080)
+    rhs = np.concatenate([y[:, :, None], probes], axis=2)
+    if cfg.cg_warm_start and solution is not None and solution.shape[2] != rhs.shape[2]:
+        rs = np.zeros_like(rhs)
+        sh = min(rhs.shape[2], solution.shape[2])
+        rs[:, :, :sh] = solution[:, :, :sh]
+        solution = rs
+    sol, _ = pcg(rhs, prior, noise, op, cfg, initial=solution if cfg.cg_warm_start else None,
+                 tolerance=max(cfg.cg_tolerance, 3.0 * float(eps) ** 0.5), chol_mode=chol_mode,
+                 matvec_mode=cfg.cg_matvec)
+    lifted = op.adjoint(sol)
+    dd = np.maximum(np.real(lifted[:, :, 1:] * np.conj(lifted_probes)).mean(axis=2), 0.0).astype(rd)
+    mean = (prior * lifted[:, :, 0]).astype(cdtype)
+    pv = np.maximum(prior - np.square(prior) * dd, 0.0).astype(rd)
+    dof = project_relevance(prior, dd, m, eps).sum(axis=1, dtype=rd)
+    shape = tuple(grid)
+    out = dict(x=mean.reshape((b,) + shape), posterior_variance=pv.reshape((b,) + shape),
+               precision=(rd(1.0) / prior).reshape((b,) + shape), noise_variance=noise,
+               effective_dof=dof.astype(rd), iterations=it, converged=converged, mode="cg",
+               history=hist, relative_change=hist["relative_change"][-1])
+    if single:
+        for key in ("x", "posterior_variance", "precision", "noise_variance", "effective_dof"):
+            out[key] = out[key][0]
+    return out
