@@ -357,39 +357,52 @@ __global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevCon
 // Per-scene scalar updates from the per-tile sums (fixed summation order).
 enum ScalarMode { kScalarInit1 = 0, kScalarInit2 = 1, kScalarSweep = 2 };
 
-__global__ void scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part,
-                               PartSrc p0, PartSrc p1, PartSrc p2) {
-  const int scene = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per scene: lanes stride the partial slots, a fixed shuffle tree
+// adds them, lane 0 applies the update.
+constexpr int kScalarScenesPerBlock = 4;
+
+__global__ void __launch_bounds__(32 * kScalarScenesPerBlock)
+scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part, PartSrc p0,
+               PartSrc p1, PartSrc p2) {
+  const int lane = threadIdx.x & 31;
+  const int scene = blockIdx.x * kScalarScenesPerBlock + (threadIdx.x >> 5);
   if (scene >= s.B) return;
   auto sum = [&](int id, PartSrc src) {
     double v = 0.0;
-    for (int t = 0; t < src.tiles; ++t)
-      for (int w = 0; w < src.warps; ++w)
-        v += part[(static_cast<long long>(scene) * kMaxTilesPerScene + t) * kPartSlots +
-                  id * kPartWarps + w];
-    return v;
+    const int n = src.tiles * src.warps;
+    for (int i = lane; i < n; i += 32) {
+      const int t = i / src.warps, w = i % src.warps;
+      v += part[(static_cast<long long>(scene) * kMaxTilesPerScene + t) * kPartSlots +
+                id * kPartWarps + w];
+    }
+    return warp_sum(v);
   };
   const float M = static_cast<float>(s.m());
+  // all reductions first (collective over the warp), then lane 0 alone
+  const double r0 = mode == kScalarInit1 ? sum(3, p0) : sum(0, p0);
+  const double r1 = mode == kScalarInit2 ? 0.0 : sum(1, p1);
+  const double r2 = mode == kScalarSweep ? sum(2, p2) : 0.0;
+  if (lane != 0) return;
   if (mode == kScalarInit1) {
-    const double ysum = sum(3, p0);
+    const double ysum = r0;
     const float dp = fmaxf(static_cast<float>(ysum / static_cast<double>(s.m())), kEps);
     const float fl = fmaxf(dp * c.min_var, kTiny);
     sc.data_power[scene] = dp;
     sc.floor_[scene] = fl;
     sc.data_energy[scene] = static_cast<float>(ysum);
-    sc.ebp[scene] = static_cast<float>(sum(1, p1));
+    sc.ebp[scene] = static_cast<float>(r1);
     sc.noise[scene] = c.fixed_noise > 0.f ? c.fixed_noise : fmaxf(c.init_noise * dp, fl);
   } else if (mode == kScalarInit2) {
-    const float dv = fmaxf(static_cast<float>(sum(0, p0)), kTiny);
+    const float dv = fmaxf(static_cast<float>(r0), kTiny);
     const float nv = sc.noise[scene];
     sc.dvar[scene] = dv;
     sc.pv[scene] = fmaxf((dv + nv) / M, kTiny);
     sc.prec[scene] = 1.0f / (dv + nv);
   } else {
     const float max_dof = static_cast<float>(static_cast<double>(s.m()) * (1.0 - 10.0 * kEps));
-    const float dof = fminf(static_cast<float>(sum(0, p0)), max_dof);
-    const float sv = static_cast<float>(sum(1, p1));
-    const float energy = static_cast<float>(sum(2, p2));
+    const float dof = fminf(static_cast<float>(r0), max_dof);
+    const float sv = static_cast<float>(r1);
+    const float energy = static_cast<float>(r2);
     const float fl = sc.floor_[scene];
     float nv = sc.noise[scene];
     if (!(c.fixed_noise > 0.f)) {
@@ -449,14 +462,14 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
               cudaStream_t st, Profiler* prof) {
   const int nt = n_tile_of(c.terms);
   const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
-  const int sc_blocks = ceil_div(s.B, 128);
+  const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   FBME_TIMED(prof, FBME_GROUP_INIT,
              run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st));
   FBME_TIMED(prof, FBME_GROUP_INIT,
              run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f},
                        u.status, st));
   FBME_TIMED(prof, FBME_GROUP_INIT,
-             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(
+             (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                  kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, 4},
                  PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
   const int bn = ew_blocks_host(s.n());
@@ -464,7 +477,7 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
              (gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma,
                                                                   u.part)));
   FBME_TIMED(prof, FBME_GROUP_INIT,
-             (scalars_kernel<<<sc_blocks, 128, 0, st>>>(kScalarInit2, s, c, u.sc, u.part,
+             (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(kScalarInit2, s, c, u.sc, u.part,
                                                         PartSrc{bn, 1}, PartSrc{0, 0},
                                                         PartSrc{0, 0})));
 }
@@ -476,7 +489,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   const int nt = n_tile_of(c.terms);
   const DftGeom f1 = stage_geom(kFwd1, s, t, nt), f2 = stage_geom(kFwd2, s, t, nt);
   const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
-  const int sc_blocks = ceil_div(s.B, 128);
+  const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   const long long BM = static_cast<long long>(s.B) * s.m();
   float2* msg[2] = {u.msg, u.msg + BM};
 
@@ -524,7 +537,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                run_stage(c.terms, f2, ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f},
                          u.status, st));
     FBME_TIMED(prof, FBME_GROUP_SCALARS,
-               (scalars_kernel<<<sc_blocks, 128, 0, st>>>(
+               (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                    kScalarSweep, s, c, u.sc, u.part, src_dof, src_dof,
                    PartSrc{f2.row_tiles * f2.col_tiles, kPartWarps})));
   }
