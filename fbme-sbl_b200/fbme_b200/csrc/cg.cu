@@ -130,26 +130,17 @@ struct ProDirection {
   float2* d_out;
   const float* beta;
   const int* dmask;
-  FBME_DEV void fetch(const TileCtx& t, int row, int kreal, Frag& f) const {
-    const DftGeom& g = *t.g;
-    const int r = t.row0() + row;
-    const int j0 = kreal >> 1;
-    if (r >= g.rows || j0 >= g.kcplx) {
+  FBME_DEV void fetch(const TileCtx& t, long long e, int avail, Frag& f) const {
+    if (avail <= 0) {
       f.z0 = f.z1 = f.d0 = f.d1 = make_float2(0.f, 0.f);
       return;
     }
-    const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
-    const int avail = g.kcplx - j0;
-    const bool vec = vec_ok(g);
+    const bool vec = vec_ok(*t.g);
     load2c(z, e, avail, vec, f.z0, f.z1);
     load2c(d_in, e, avail, vec, f.d0, f.d1);
   }
-  FBME_DEV float4 make(const TileCtx& t, int row, int kreal, const Frag& f) const {
-    const DftGeom& g = *t.g;
-    const int r = t.row0() + row;
-    const int j0 = kreal >> 1;
-    if (r >= g.rows || j0 >= g.kcplx) return make_float4(0.f, 0.f, 0.f, 0.f);
-    const int avail = g.kcplx - j0;
+  FBME_DEV float4 make(const TileCtx& t, long long e, int avail, const Frag& f) const {
+    if (avail <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
     const int mk = dmask[t.scene];
     const float bt = beta[t.scene];
     auto dir = [&](float2 zz, float2 dd) {
@@ -160,8 +151,7 @@ struct ProDirection {
     const float2 o0 = dir(f.z0, f.d0);
     const float2 o1 = avail >= 2 ? dir(f.z1, f.d1) : make_float2(0.f, 0.f);
     if (t.col_tile == 0) {
-      const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
-      if (avail >= 2 && vec_ok(g)) {
+      if (avail >= 2 && vec_ok(*t.g)) {
         *reinterpret_cast<float4*>(d_out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
       } else {
         d_out[e] = o0;

@@ -35,10 +35,10 @@ struct ProYPower {
   const float2* in;
   double* part;
   float acc;
-  FBME_DEV void fetch(const TileCtx& t, int row, int kreal, Frag& f) const {
-    f = load_row4(in, t, row, kreal);
+  FBME_DEV void fetch(const TileCtx& t, long long e, int avail, Frag& f) const {
+    f = load_pair(in, e, avail, t.g->vec4 != 0);
   }
-  FBME_DEV float4 make(const TileCtx& t, int, int, const Frag& v) {
+  FBME_DEV float4 make(const TileCtx& t, long long, int, const Frag& v) {
     if (t.col_tile == 0) {
       acc += abs_sq(make_float2(v.x, v.y));
       acc += abs_sq(make_float2(v.z, v.w));
@@ -64,27 +64,18 @@ struct ProMessage {
   float2* msg_out;
   const float *prec, *dvar;
   float damping;
-  FBME_DEV void fetch(const TileCtx& t, int row, int kreal, Frag& f) const {
-    const DftGeom& g = *t.g;
-    const int r = t.row0() + row;
-    const int j0 = kreal >> 1;
-    if (r >= g.rows || j0 >= g.kcplx) {
+  FBME_DEV void fetch(const TileCtx& t, long long e, int avail, Frag& f) const {
+    if (avail <= 0) {
       f.y0 = f.y1 = f.p0 = f.p1 = f.m0 = f.m1 = make_float2(0.f, 0.f);
       return;
     }
-    const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
-    const int avail = g.kcplx - j0;
-    const bool vec = vec_ok(g);
+    const bool vec = vec_ok(*t.g);
     load2c(y, e, avail, vec, f.y0, f.y1);
     load2c(pred, e, avail, vec, f.p0, f.p1);
     load2c(msg_in, e, avail, vec, f.m0, f.m1);
   }
-  FBME_DEV float4 make(const TileCtx& t, int row, int kreal, const Frag& f) const {
-    const DftGeom& g = *t.g;
-    const int r = t.row0() + row;
-    const int j0 = kreal >> 1;
-    if (r >= g.rows || j0 >= g.kcplx) return make_float4(0.f, 0.f, 0.f, 0.f);
-    const int avail = g.kcplx - j0;
+  FBME_DEV float4 make(const TileCtx& t, long long e, int avail, const Frag& f) const {
+    if (avail <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
     const float pr = prec[t.scene], dv = dvar[t.scene];
     const float keep = damping, upd = 1.0f - damping;
     auto step = [&](float2 yy, float2 pp, float2 mm) {
@@ -95,8 +86,7 @@ struct ProMessage {
     const float2 o0 = step(f.y0, f.p0, f.m0);
     const float2 o1 = avail >= 2 ? step(f.y1, f.p1, f.m1) : make_float2(0.f, 0.f);
     if (t.col_tile == 0) {
-      const long long e = t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld + j0;
-      if (avail >= 2 && vec_ok(g)) {
+      if (avail >= 2 && vec_ok(*t.g)) {
         *reinterpret_cast<float4*>(msg_out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
       } else {
         msg_out[e] = o0;
@@ -470,7 +460,7 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                        u.status, st));
   FBME_TIMED(prof, FBME_GROUP_INIT,
              (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
-                 kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, 4},
+                 kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, kProWarps},
                  PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
   const int bn = ew_blocks_host(s.n());
   FBME_TIMED(prof, FBME_GROUP_INIT,
