@@ -122,6 +122,7 @@ FBME_DEV float2 atom_value(const BatchShape& s, int m1, int m2, long long idx, f
 // d_out by the column-tile-0 tiles and fed to the tensor core.
 struct ProDirection {
   static constexpr int kBatch = 8;
+  static constexpr bool kPipelined = false;
   struct Frag {
     float2 z0, z1, d0, d1;
   };

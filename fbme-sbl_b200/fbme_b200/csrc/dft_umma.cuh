@@ -201,6 +201,58 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
                       ? t.scene * g.in_stride + static_cast<long long>(r) * g.in_ld
                       : -1;
       }
+      if constexpr (Pro::kPipelined) {
+        // Two register buffers, used in turn: the loads of chunk kc+1 are in
+        // flight while chunk kc is converted and stored.
+        typename Pro::Frag fa[kProIters], fb[kProIters];
+        auto fetch_all = [&](int kcc, typename Pro::Frag(&f)[kProIters]) {
+          const int j0 = kcc * (kKChunk / 2) + q * 2;
+          const int avail = g.kcplx - j0;
+#pragma unroll
+          for (int i = 0; i < kProIters; ++i) pro.fetch(t, erow[i] + j0, erow[i] >= 0 ? avail : 0, f[i]);
+        };
+        auto store_all = [&](int kcc, const typename Pro::Frag(&f)[kProIters]) -> bool {
+          const int s = it % kStages, use = it / kStages;
+          uint8_t* st = smem + s * C::kStageBytes;
+          if (it >= kStages && !mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene)) return false;
+          if (tid == 0) {
+            asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;"
+                         ::"r"(smem_u32(&full_bar[s])), "r"(uint32_t(A_PARTS * C::kPartBytesB))
+                         : "memory");
+            const uint8_t* src = g.table + (static_cast<size_t>(t.col_tile) * g.table_kchunks + kcc) *
+                                               A_PARTS * C::kPartBytesB;
+            for (int p = 0; p < A_PARTS; ++p)
+              bulk_g2s(st + A_PARTS * kPartBytesA + p * C::kPartBytesB, src + p * C::kPartBytesB,
+                       C::kPartBytesB, &full_bar[s]);
+          }
+          const int j0 = kcc * (kKChunk / 2) + q * 2;
+          const int avail = g.kcplx - j0;
+#pragma unroll
+          for (int i = 0; i < kProIters; ++i) {
+            if (pw + kProWarps * i >= kRowPairs) continue;
+            const float4 v = pro.make(t, erow[i] + j0, erow[i] >= 0 ? avail : 0, f[i]);
+            uint2 parts[A_PARTS];
+            split4<A_PARTS>(v, parts);
+#pragma unroll
+            for (int p = 0; p < A_PARTS; ++p)
+              *reinterpret_cast<uint2*>(st + p * kPartBytesA + soff[i]) = parts[p];
+          }
+          fence_proxy_async_smem();
+          mbar_arrive(&full_bar[s]);
+          ++it;
+          return true;
+        };
+        fetch_all(0, fa);
+        for (int kc = 0; kc < g.kchunks && ok; kc += 2) {
+          if (kc + 1 < g.kchunks) fetch_all(kc + 1, fb);
+          ok = store_all(kc, fa);
+          if (!ok || kc + 1 >= g.kchunks) break;
+          if (kc + 2 < g.kchunks) fetch_all(kc + 2, fa);
+          ok = store_all(kc + 1, fb);
+        }
+        pro.tile_done(t, pw, lane);
+        continue;
+      }
       for (int kc = 0; kc < g.kchunks && ok; ++kc, ++it) {
         const int s = it % kStages, use = it / kStages;
         uint8_t* st = smem + s * C::kStageBytes;
@@ -367,6 +419,7 @@ FBME_DEV float4 load_pair(const float2* base, long long e, int avail, bool vec) 
 
 struct ProPlain {
   static constexpr int kBatch = 16;
+  static constexpr bool kPipelined = true;
   using Frag = float4;
   const float2* in;
   FBME_DEV void fetch(const TileCtx& t, long long e, int avail, Frag& f) const {

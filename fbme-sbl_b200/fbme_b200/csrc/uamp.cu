@@ -31,6 +31,7 @@ namespace fbme {
 // Plain load; also sums |y|^2 (for the data power) over the column-tile-0 tiles.
 struct ProYPower {
   static constexpr int kBatch = 16;
+  static constexpr bool kPipelined = true;
   using Frag = float4;
   const float2* in;
   double* part;
@@ -57,6 +58,7 @@ struct ProYPower {
 // tensor core.
 struct ProMessage {
   static constexpr int kBatch = 8;
+  static constexpr bool kPipelined = false;
   struct Frag {
     float2 y0, y1, p0, p1, m0, m1;
   };
