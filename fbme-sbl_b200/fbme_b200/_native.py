@@ -189,6 +189,15 @@ SIGNATURES = {
                                c_void_p]),
     "fbme_pcg_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                c_float, c_void_p, POINTER(c_int32), c_void_p]),
+    "fbme_cnn_param_count": (c_int32, []),
+    "fbme_cnn_workspace_bytes": (c_size_t, [c_int32, c_int32, c_int32]),
+    "fbme_cnn_features": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
+    "fbme_cnn_forward": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
+    "fbme_cnn_backward": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
+                                  c_void_p]),
+    "fbme_cnn_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_void_p]),
+    "fbme_plan_warm_workspace_bytes": (c_size_t, [POINTER(FbmeShape), c_int32]),
+    "fbme_plan_set_warm_start": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "fbme_last_error": (c_char_p, []),
     "fbme_version": (c_char_p, []),
 }

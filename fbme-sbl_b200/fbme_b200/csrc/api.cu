@@ -282,6 +282,31 @@ int fbme_plan_create(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig
   return FBME_OK;
 }
 
+size_t fbme_plan_warm_workspace_bytes(const FbmeShape* shapes, int32_t n_scenes) {
+  if (!shapes || n_scenes < 1) return 0;
+  if (fbme::cnn_check(n_scenes, shapes[0].n1, shapes[0].n2)) return 0;
+  return fbme::cnn_workspace_bytes(n_scenes, shapes[0].n1, shapes[0].n2);
+}
+
+int fbme_plan_set_warm_start(FbmePlan* plan, const float* params, void* workspace,
+                             size_t workspace_bytes) {
+  if (!plan) return fail(FBME_ERR_INVALID, "plan is NULL");
+  if (!params) {
+    plan->u.warm_params = nullptr;
+    plan->u.warm_ws = nullptr;
+    return FBME_OK;
+  }
+  if (const char* why = fbme::cnn_check(plan->s.B, plan->s.n1, plan->s.n2))
+    return fail(FBME_ERR_UNSUPPORTED, why);
+  const size_t need = fbme::cnn_workspace_bytes(plan->s.B, plan->s.n1, plan->s.n2);
+  if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0 || workspace_bytes < need)
+    return fail(FBME_ERR_WORKSPACE, "warm-start workspace smaller than fbme_plan_warm_workspace_bytes() "
+                                    "or not 256-byte aligned");
+  plan->u.warm_params = params;
+  plan->u.warm_ws = workspace;
+  return FBME_OK;
+}
+
 int fbme_plan_destroy(FbmePlan* plan) {
   delete plan;
   return FBME_OK;

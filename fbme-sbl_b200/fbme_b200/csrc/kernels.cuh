@@ -103,6 +103,9 @@ struct UampBuffers {
   uint32_t* keys;  // [B][N] order-preserving score keys (final E-step)
   Scalars sc;
   int* status;   // launch status word
+  // learned warm start (optional): FP32 network parameters and its workspace
+  const float* warm_params;
+  void* warm_ws;
 };
 
 cudaError_t set_dft_attributes();
@@ -143,6 +146,19 @@ const char* topk_check(long long n, int k, int batch);
 void topk_scores(const float* scores, long long n, int k, int batch, void* scratch,
                  int64_t* indices, float* values, cudaStream_t st);
 int exchange_blocks(const BatchShape& s);
+
+// Learned warm start (csrc/cnn.cu).
+int cnn_param_count();
+size_t cnn_workspace_bytes(long long B, long long H, long long W);
+const char* cnn_check(long long B, long long H, long long W);
+void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t st);
+void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st);
+void cnn_backward(const float* target, int B, int H, int W, void* ws, float* grad, double* loss_out,
+                  cudaStream_t st);
+void cnn_adam(float* params, const float* grad, float* m, float* v, int step, float lr, cudaStream_t st);
+void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, void* ws,
+                    const float* data_power, const float* floor_, float* gamma, double* upart,
+                    int nblocks, cudaStream_t st);
 
 // Shared by the C ABI translation units.
 int api_fail(int code, const std::string& msg);

@@ -487,6 +487,16 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
 
   sbl_init(s, t, c, u, st, prof);
   const int bn = ew_blocks_host(s.n()), bm = ew_blocks_host(s.m());
+  if (u.warm_params) {
+    // learned warm start: the network's prior replaces the initial prior,
+    // then the scalar initialisation is redone from its sums
+    FBME_TIMED(prof, FBME_GROUP_INIT,
+               cnn_warm_prior(u.warm_params, u.bp, s.B, s.n1, s.n2, u.warm_ws, u.sc.data_power,
+                              u.sc.floor_, u.gamma, u.part, bn, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT,
+               (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
+                   kScalarInit2, s, c, u.sc, u.part, PartSrc{bn, 1}, PartSrc{0, 0}, PartSrc{0, 0})));
+  }
   DenoiseArgs da;
   da.mu = u.mu;
   da.var = u.var;

@@ -1,0 +1,257 @@
+"""Learned warm start of the FBME plans (no counterpart in the reference).
+
+A 3-layer 3x3 convolutional network (16 hidden channels, 2,769 parameters;
+BF16 operands on the tensor cores, FP32 accumulation; csrc/cnn.cu) maps the
+features of the backprojection A^H y to the log of the initial prior
+variance relative to the uniform level P/N (P the data power).  It replaces
+the backprojection-blend initialisation of torch_sbl/solver.py:1072-1099;
+with it the plan runs fewer UAMP sweeps.
+
+Training pairs come from the plain solver itself: the network's target is
+log(prior / (P/N)) after ``target_sweeps`` plain UAMP sweeps (the
+converged posterior of the plain path), clamped to [-20, 20].  Training
+runs on the GPU with the library's own forward, backward and Adam kernels.
+
+``LearnedPlan`` runs the warm-started replay and keeps plain FBME as the
+fallback: a scene whose warm-started solve fails the evidence / residual
+check (finite, monotone evidence trace; fixed-point residuals of the prior
+and noise below the plain solver's calibrated bounds) is solved again by
+the plain plan, whose result is returned for it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import fields
+from math import prod
+from pathlib import Path
+from typing import Sequence
+
+import numpy as np
+import torch
+from torch import Tensor
+
+from . import _native as nat
+from . import scenes
+from .config import SBLConfig
+from .engine import FBMEEngine
+
+HIDDEN = 16
+TARGET_CLAMP = 20.0
+WEIGHTS_DIR = Path(__file__).resolve().parent / "weights"
+DEFAULT_WEIGHTS = WEIGHTS_DIR / "warm_start_256x256_128x128.npz"
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-normal initial parameters in the flat layout of the C ABI."""
+    rng = np.random.default_rng(seed)
+    parts = [
+        rng.normal(0.0, np.sqrt(2.0 / 18.0), 9 * 2 * HIDDEN), np.zeros(HIDDEN),
+        rng.normal(0.0, np.sqrt(2.0 / (9.0 * HIDDEN)), 9 * HIDDEN * HIDDEN), np.zeros(HIDDEN),
+        0.1 * rng.normal(0.0, np.sqrt(2.0 / (9.0 * HIDDEN)), 9 * HIDDEN), np.zeros(1),
+    ]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def _ptr(t: Tensor | None) -> ctypes.c_void_p | None:
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class WarmStartNet:
+    """Network parameters on a device plus the training / inference calls."""
+
+    def __init__(self, device: torch.device, params: np.ndarray | Tensor | None = None, seed: int = 0):
+        self.lib = nat.lib()
+        if device.type != "cuda":
+            raise RuntimeError("the warm-start network runs on CUDA devices only")
+        self.device = device if device.index is not None else torch.device("cuda", torch.cuda.current_device())
+        self.n_params = int(self.lib.fbme_cnn_param_count())
+        p = init_params(seed) if params is None else params
+        p = torch.as_tensor(p, dtype=torch.float32).to(self.device).contiguous()
+        if p.numel() != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {p.numel()}")
+        self.params = p
+        self._ws: dict[tuple, tuple[Tensor, int, int]] = {}
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grad = torch.zeros_like(self.params)
+        self.step = 0
+
+    # ---------------------------------------------------------------- io
+    def save(self, path: str | Path, **meta) -> None:
+        Path(path).parent.mkdir(parents=True, exist_ok=True)
+        np.savez(path, params=self.params.cpu().numpy(), **{k: np.asarray(v) for k, v in meta.items()})
+
+    @classmethod
+    def load(cls, path: str | Path, device: torch.device) -> "WarmStartNet":
+        d = np.load(path)
+        return cls(device, d["params"])
+
+    # ------------------------------------------------------------- stages
+    def workspace(self, batch: int, n1: int, n2: int) -> tuple[int, int]:
+        key = (batch, n1, n2)
+        if key not in self._ws:
+            nbytes = int(self.lib.fbme_cnn_workspace_bytes(batch, n1, n2))
+            if nbytes == 0:
+                raise ValueError("the warm-start network needs N1 % 8 == 0 and N2 % 16 == 0")
+            buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.device)
+            self._ws[key] = (buf, (buf.data_ptr() + 255) & ~255, nbytes)
+        _, ptr, nbytes = self._ws[key]
+        return ptr, nbytes
+
+    def _stream(self) -> ctypes.c_void_p:
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def features(self, bp: Tensor, n1: int, n2: int) -> None:
+        """Features of the backprojection ``bp`` (complex64 [B, N1*N2])."""
+        b = bp.shape[0]
+        bp = bp.contiguous()
+        ws, _ = self.workspace(b, n1, n2)
+        nat.check(self.lib.fbme_cnn_features(_ptr(bp), b, n1, n2, ctypes.c_void_p(ws), self._stream()),
+                  "fbme_cnn_features")
+
+    def forward(self, batch: int, n1: int, n2: int) -> Tensor:
+        out = torch.empty(batch, n1 * n2, dtype=torch.float32, device=self.device)
+        ws, _ = self.workspace(batch, n1, n2)
+        nat.check(self.lib.fbme_cnn_forward(_ptr(self.params), batch, n1, n2, ctypes.c_void_p(ws), _ptr(out),
+                                            self._stream()), "fbme_cnn_forward")
+        return out
+
+    def backward(self, target: Tensor, batch: int, n1: int, n2: int) -> Tensor:
+        """Gradient into self.grad; returns the loss as a 0-d device tensor."""
+        loss = torch.zeros(1, dtype=torch.float64, device=self.device)
+        ws, _ = self.workspace(batch, n1, n2)
+        target = target.to(torch.float32).contiguous()
+        nat.check(self.lib.fbme_cnn_backward(_ptr(target), batch, n1, n2, ctypes.c_void_p(ws), _ptr(self.grad),
+                                             _ptr(loss), self._stream()), "fbme_cnn_backward")
+        return loss[0]
+
+    def adam(self, lr: float) -> None:
+        self.step += 1
+        nat.check(self.lib.fbme_cnn_adam(_ptr(self.params), _ptr(self.grad), _ptr(self.m), _ptr(self.v),
+                                         self.step, float(lr), self._stream()), "fbme_cnn_adam")
+
+    def predict(self, bp: Tensor, n1: int, n2: int) -> Tensor:
+        self.features(bp, n1, n2)
+        return self.forward(bp.shape[0], n1, n2)
+
+
+# ---------------------------------------------------------------- training
+def plain_config(sweeps: int | None = None, profile: str = "stable") -> SBLConfig:
+    """The FBME plan configuration (profiles.py:63-70, 110-115), optionally
+    with a fixed sweep budget instead of the auto rule."""
+    over = dict(uamp_polish_size=32, uamp_polish_compute_truncation_diagnostic=False)
+    if profile == "stable":
+        over.update(uamp_polish_iterations=3, uamp_polish_residual_exchange_size=12,
+                    uamp_polish_fixed_budget_diagnostics=True)
+    else:
+        over.update(uamp_polish_iterations=2, uamp_polish_residual_exchange_size=0,
+                    uamp_polish_fixed_budget_diagnostics=False)
+    if sweeps is not None:
+        over.update(uamp_auto_iterations=False, max_iter=int(sweeps), min_iter=1, uamp_min_iter=1)
+    return SBLConfig.paper_hybrid_uamp(**over)
+
+
+def training_pairs(seeds: Sequence[int], device: torch.device, *, batch: int = 64,
+                   target_sweeps: int = 12) -> tuple[Tensor, Tensor]:
+    """(backprojections [S, N] complex64, targets [S, N] float32) on the
+    device, from plain solves with ``target_sweeps`` UAMP sweeps."""
+    sc0 = scenes.learned_scene(int(seeds[0]))
+    grid, prefix = sc0.grid, sc0.y.shape
+    n = prod(grid)
+    eng = FBMEEngine(batch, grid, prefix, plain_config(target_sweeps), device)
+    bps, tgts = [], []
+    seeds = list(seeds)
+    for s0 in range(0, len(seeds), batch):
+        chunk = seeds[s0:s0 + batch]
+        ys = np.zeros((batch, prefix[0] * prefix[1]), np.complex64)
+        for i, sd in enumerate(chunk):
+            ys[i] = scenes.learned_scene(int(sd)).y.reshape(-1)
+        y = torch.from_numpy(ys).to(device)
+        eng.run_uamp(y)
+        st = eng.state()
+        dp = (y.abs() ** 2).mean(dim=1).clamp_min(float(np.finfo(np.float32).eps))
+        tgt = torch.log(st["prior_variance"] / (dp[:, None] / n)).clamp(-TARGET_CLAMP, TARGET_CLAMP)
+        bps.append(st["backprojection"][: len(chunk)].clone())
+        tgts.append(tgt[: len(chunk)].clone())
+    eng.close()
+    return torch.cat(bps), torch.cat(tgts)
+
+
+def train(net: WarmStartNet, bp: Tensor, target: Tensor, grid: Sequence[int], *, epochs: int = 3,
+          batch: int = 16, lr: float = 2e-3, seed: int = 0, log_every: int = 200) -> list[float]:
+    """Minibatch Adam on (bp, target); returns the per-step losses."""
+    n1, n2 = grid
+    s = bp.shape[0]
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    losses: list[float] = []
+    total = epochs * (s // batch)
+    step = 0
+    for _ in range(epochs):
+        order = torch.randperm(s, generator=gen)
+        for b0 in range(0, s - batch + 1, batch):
+            idx = order[b0:b0 + batch].to(bp.device)
+            net.features(bp[idx], n1, n2)
+            net.forward(batch, n1, n2)
+            loss = net.backward(target[idx], batch, n1, n2)
+            rate = lr * 0.5 * (1.0 + np.cos(np.pi * step / max(total, 1)))  # cosine decay
+            net.adam(rate)
+            step += 1
+            if step % log_every == 0 or step == total:
+                losses.append(float(loss))
+    return losses
+
+
+# ------------------------------------------------------------ warm plans
+class LearnedPlan:
+    """Warm-started FBME plan for ``batch`` scenes with plain-FBME fallback.
+
+    ``run(y)`` solves [B, M] complex64 observations: the warm-started plan
+    (``sweeps`` UAMP sweeps after the network's prior) first; scenes that
+    fail the evidence / residual check are solved again by the plain plan.
+    """
+
+    def __init__(self, net: WarmStartNet, batch: int, grid: Sequence[int], prefix: Sequence[int], *,
+                 sweeps: int = 1, profile: str = "stable", gamma_residual_max: float = 0.5,
+                 noise_residual_max: float = 0.5):
+        self.net = net
+        self.device = net.device
+        self.grid, self.prefix, self.batch = tuple(grid), tuple(prefix), int(batch)
+        self.warm = FBMEEngine(self.batch, self.grid, self.prefix, plain_config(sweeps, profile), self.device)
+        self.plain = FBMEEngine(self.batch, self.grid, self.prefix, plain_config(None, profile), self.device)
+        shape = (nat.FbmeShape * self.batch)(*[nat.FbmeShape(*self.grid, *self.prefix)] * self.batch)
+        nbytes = int(net.lib.fbme_plan_warm_workspace_bytes(shape, self.batch))
+        if nbytes == 0:
+            raise ValueError("the warm-start network needs N1 % 8 == 0 and N2 % 16 == 0")
+        self._ws = torch.empty(nbytes + 256, dtype=torch.uint8, device=self.device)
+        ptr = (self._ws.data_ptr() + 255) & ~255
+        nat.check(net.lib.fbme_plan_set_warm_start(self.warm._plan, _ptr(net.params), ctypes.c_void_p(ptr),
+                                                   ctypes.c_size_t(nbytes)), "fbme_plan_set_warm_start")
+        self.gamma_residual_max = gamma_residual_max
+        self.noise_residual_max = noise_residual_max
+        self.fallbacks = 0
+
+    def check(self) -> Tensor:
+        """Per-scene pass flags of the warm-started solve (device bool)."""
+        o = self.warm.out
+        ok = torch.isfinite(o["negative_log_evidence"]) & (o["status"] == 0)
+        ok &= o["fixed_budget_monotone"]
+        ok &= o["fixed_budget_gamma_residual"] <= self.gamma_residual_max
+        ok &= o["fixed_budget_noise_residual"] <= self.noise_residual_max
+        return ok
+
+    def run(self, y: Tensor):
+        y = y.to(self.device, torch.complex64).reshape(self.batch, -1).contiguous()
+        self.warm.run(y)
+        res = self.warm.result(())
+        ok = self.check()
+        bad = (~ok).nonzero().flatten()
+        self.fallbacks = int(bad.numel())
+        if self.fallbacks:
+            self.plain.run(y)
+            plain = self.plain.result(())
+            for f in fields(res):
+                v, pv = getattr(res, f.name), getattr(plain, f.name)
+                if isinstance(v, Tensor) and v.ndim >= 1 and v.shape[0] == self.batch:
+                    v[bad] = pv[bad]
+        return res, ok

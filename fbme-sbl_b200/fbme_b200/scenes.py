@@ -109,6 +109,15 @@ def uneven_batch(batch_seed: int, n_scenes: int = 64) -> list[Scene]:
     return out
 
 
+def learned_scene(seed: int) -> Scene:
+    """Training / evaluation scenes of the learned warm start: 256x256 grid,
+    128x128 prefix, K ~ U{100..400} Rayleigh points, SNR ~ U[5, 25] dB."""
+    rng = np.random.default_rng(7_000_000 + seed)
+    k = int(rng.integers(100, 401))
+    snr = float(rng.uniform(5.0, 25.0))
+    return point_scene((256, 256), (128, 128), k, snr, seed, "rayleigh")
+
+
 def config_scene(name: str, seed: int) -> Scene:
     """The named single-scene workloads.
 

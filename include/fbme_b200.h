@@ -268,6 +268,41 @@ int fbme_pcg_solve(FbmeCgPlan* plan, const float* prior, const float* noise, con
                    int32_t rhs_count, const void* initial, float tolerance, void* solution,
                    int32_t* iterations, fbme_stream_t stream);
 
+/* ------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference: it is the learned
+ * part of this implementation).  A 3-layer 3x3 convolutional network
+ * (16 hidden channels, BF16 operands, FP32 accumulation) maps the features
+ * of A^H y to the initial log prior variance that replaces the
+ * backprojection initialisation of torch_sbl/solver.py:1072-1099.
+ * Parameters are an FP32 vector of fbme_cnn_param_count() values; the
+ * layout is W1[3][3][2][16], b1[16], W2[3][3][16][16], b2[16],
+ * W3[3][3][16][1], b3[1].  Grids need N1 % 8 == 0 and N2 % 16 == 0.
+ * ---------------------------------------------------------------------- */
+int32_t fbme_cnn_param_count(void);
+size_t fbme_cnn_workspace_bytes(int32_t batch, int32_t n1, int32_t n2);
+/* Features of the backprojection (complex64 [batch][n1][n2]) into the
+ * workspace; forward / backward then read them from there. */
+int fbme_cnn_features(const void* backprojection, int32_t batch, int32_t n1, int32_t n2, void* workspace,
+                      fbme_stream_t stream);
+/* out [batch][n1][n2] FP32 = network output (predicted log(prior / (P/N)),
+ * P the data power).  Keeps the activations for fbme_cnn_backward. */
+int fbme_cnn_forward(const float* params, int32_t batch, int32_t n1, int32_t n2, void* workspace, float* out,
+                     fbme_stream_t stream);
+/* Gradient of mean((out - target)^2) after fbme_cnn_forward on the same
+ * workspace; writes grad[param_count] and the loss to *loss (device FP64,
+ * may be NULL). */
+int fbme_cnn_backward(const float* target, int32_t batch, int32_t n1, int32_t n2, void* workspace, float* grad,
+                      double* loss, fbme_stream_t stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the FP32 parameters. */
+int fbme_cnn_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
+                  fbme_stream_t stream);
+/* Warm-started replays: from the next replay on, the plan's initial prior
+ * is max(P/N * exp(network output), floor) instead of the backprojection
+ * blend.  `params` (device, FP32) and `workspace` stay caller-owned and
+ * must outlive the replays; params == NULL turns the warm start off. */
+size_t fbme_plan_warm_workspace_bytes(const FbmeShape* shapes, int32_t n_scenes);
+int fbme_plan_set_warm_start(FbmePlan* plan, const float* params, void* workspace, size_t workspace_bytes);
+
 /* Kernel groups timed by fbme_plan_profile. */
 enum {
   FBME_GROUP_INIT = 0,        /* A^H y, data power, prior/noise initialisation */

@@ -459,11 +459,14 @@ def _uamp_iteration_limit(cfg: OracleConfig, n_grid: int, n_samples: int) -> int
 
 
 def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str = "cuda",
-                  stop_after_uamp: bool = False):
+                  stop_after_uamp: bool = False, initial_prior: np.ndarray | None = None):
     """Restatement of ``fast_sbl`` for ``mode="uamp"`` with the polish.
 
     ``data`` is ``[M1, M2]`` or ``[B, M1, M2]``.  Returns a dict of the
     ``SBLResult`` fields the FBME plans fill (solver.py:2154-2393).
+    ``initial_prior`` ([B, N], optional) replaces the initial prior variances
+    of solver.py:1072-1099 (floored as there): the warm start of the learned
+    path; everything else is unchanged.
     """
     data = np.asarray(data)
     cdtype = np.complex128 if data.dtype in (np.complex128, np.float64) else np.complex64
@@ -493,6 +496,8 @@ def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str =
     else:
         prior = np.broadcast_to(uniform, (b, n)).copy()
     prior_floor = variance_floor
+    if initial_prior is not None:
+        prior = np.asarray(initial_prior, dtype=rd).reshape(b, n)
     prior = np.maximum(prior, prior_floor[:, None]).astype(rd)
     if cfg.fixed_noise_variance is None:
         noise = np.maximum(rd(cfg.initial_noise_fraction) * data_power, variance_floor).astype(rd)
