@@ -12,7 +12,7 @@ from __future__ import annotations
 
 from copy import deepcopy
 from math import prod
-from typing import Any, Sequence
+from typing import Any, Callable, Sequence
 
 import torch
 from torch import Tensor
@@ -31,7 +31,7 @@ class CUDAGraphSBLPlan:
     """
 
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, config: SBLConfig,
-                 warmup: int = 3) -> None:
+                 warmup: int = 3, engine_hook: Callable[[FBMEEngine], None] | None = None) -> None:
         if not torch.cuda.is_available():
             raise RuntimeError("CUDA Graph execution requires CUDA.")
         if not isinstance(example_data, Tensor) or not example_data.is_cuda:
@@ -74,6 +74,8 @@ class CUDAGraphSBLPlan:
         self.input_buffer = torch.empty(self.shape, dtype=self.dtype, device=self.device)
         self.input_buffer.copy_(example_data)
         self._engine = FBMEEngine(batch, self.grid_shape, sample, self.config, self.device)
+        if engine_hook is not None:  # e.g. the learned warm start, before warm-up and capture
+            engine_hook(self._engine)
         flat = self.input_buffer.view(batch, -1)
 
         warmup_stream = torch.cuda.Stream(device=self.device)

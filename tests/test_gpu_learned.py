@@ -1,0 +1,110 @@
+"""Learned warm start on the B200: what the trained network gains, the plain
+fallback, and parity of the warm-started solve with the oracle.
+
+Held-out scenes come from the learned-training distribution (256x256 grid,
+128x128 prefix, K ~ U{100..400}, SNR ~ U[5, 25] dB) with seeds 2*10^6 ...,
+which training never saw (training seeds are 10^6 ... 10^6 + 19999).
+"""
+
+import numpy as np
+import pytest
+
+from gpu_util import X_TOL, need_gpu, rel_l2
+
+torch = pytest.importorskip("torch")
+
+GRID, PREFIX = (256, 256), (128, 128)
+
+
+def _batch(n, seed0=2_000_000):
+    from fbme_b200 import scenes
+
+    sc = [scenes.learned_scene(seed0 + i) for i in range(n)]
+    y = np.stack([c.y for c in sc]).astype(np.complex64)
+    x = np.stack([c.x.reshape(-1) for c in sc])
+    return y, x
+
+
+def _nmse(xh, x):
+    xh = xh.reshape(x.shape[0], -1)
+    return 10 * np.log10(np.sum(np.abs(xh - x) ** 2, 1) / np.sum(np.abs(x) ** 2, 1))
+
+
+@pytest.mark.gpu
+def test_trained_network_gains_over_plain_start():
+    """At the warm plan's budget (1 UAMP sweep) the network's prior beats the
+    backprojection start by > 0.1 dB, and the warm plan is at least as good
+    as plain FBME-Stable with its own budget (within 0.1 dB)."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.learned import make_learned_plan, plain_config
+    from torch_sbl_fastest_stable import make_stable_plan
+
+    y, x = _batch(64)
+    yt = torch.from_numpy(y).cuda()
+    stable = make_stable_plan(yt, GRID, warmup=1)
+    n_stable = _nmse(stable.replay(yt, synchronize=True).x.cpu().numpy(), x).mean()
+    e1 = FBMEEngine(64, GRID, PREFIX, plain_config(1), torch.device("cuda", 0))
+    e1.run(yt.view(64, -1))
+    n_plain1 = _nmse(e1.result((64,)).x.cpu().numpy(), x).mean()
+    learned = make_learned_plan(yt, GRID, warmup=1)
+    n_learned = _nmse(learned.replay(yt, synchronize=True).x.cpu().numpy(), x).mean()
+    print(f"NMSE dB: stable {n_stable:.3f}, plain 1 sweep {n_plain1:.3f}, learned 1 sweep {n_learned:.3f}, "
+          f"fallbacks {learned.fallbacks}")
+    assert n_learned < n_plain1 - 0.1
+    assert n_learned < n_stable + 0.1
+    assert learned.fallbacks < 16
+
+
+@pytest.mark.gpu
+def test_fallback_returns_the_plain_plan_result():
+    need_gpu()
+    from fbme_b200.learned import make_learned_plan
+    from torch_sbl_fastest_stable import make_stable_plan
+
+    y, _ = _batch(8, 2_100_000)
+    yt = torch.from_numpy(y).cuda()
+    learned = make_learned_plan(yt, GRID, warmup=1)
+    learned.gamma_residual_max = -1.0  # every scene fails the check
+    r = learned.replay(yt, synchronize=True)
+    assert learned.fallbacks == 8
+    p = make_stable_plan(yt, GRID, warmup=1).replay(yt, synchronize=True)
+    assert torch.equal(r.x, p.x)
+    assert torch.equal(r.posterior_variance, p.posterior_variance)
+    assert torch.equal(r.negative_log_evidence, p.negative_log_evidence)
+
+
+@pytest.mark.gpu
+def test_warm_started_solve_matches_oracle_from_the_network_prior():
+    """The warm plan is the plain algorithm started from the network's prior:
+    the oracle restatement given the same prior agrees (x within 1e-4
+    relative L2, identical support)."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.learned import DEFAULT_WEIGHTS, WarmStartNet, attach_warm_start, plain_config
+    from oracle import fbme_oracle as O
+
+    y, _ = _batch(2, 2_200_000)
+    dev = torch.device("cuda", 0)
+    yt = torch.from_numpy(y).cuda().view(2, -1)
+    net = WarmStartNet.load(DEFAULT_WEIGHTS, dev)
+    eng = FBMEEngine(2, GRID, PREFIX, plain_config(1), dev)
+    ws = attach_warm_start(eng, net)
+    eng.run(yt)
+    x = eng.result((2,)).x.cpu().numpy().reshape(2, -1)
+    bp = eng.state()["backprojection"].clone()
+    out = net.predict(bp, *GRID).cpu().numpy().astype(np.float32)
+    n = GRID[0] * GRID[1]
+    dp = np.maximum(np.mean(np.abs(y.reshape(2, -1)) ** 2, axis=1), np.finfo(np.float32).eps).astype(np.float32)
+    fl = np.maximum(dp * np.float32(1e-12), np.finfo(np.float32).tiny)
+    prior0 = np.maximum((dp / np.float32(n))[:, None] * np.exp(np.clip(out, -40, 40)), fl[:, None])
+    cfg = O.OracleConfig.stable(32)
+    cfg.uamp_auto_iterations = False
+    cfg.max_iter = 1
+    cfg.uamp_min_iter = 1
+    r = O.fast_sbl_uamp(y, GRID, cfg, initial_prior=prior0.astype(np.float32))
+    xo = r["x"].reshape(2, -1)
+    for b in range(2):
+        assert set(np.flatnonzero(x[b])) == set(np.flatnonzero(xo[b]))
+    assert rel_l2(x, xo) < X_TOL
+    del ws
