@@ -48,6 +48,7 @@ def _args() -> argparse.Namespace:
     ap.add_argument("--profile", choices=("stable", "fast"), default="stable")
     ap.add_argument("--cpu-sample", type=int, default=32, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain section")
     return ap.parse_args()
 
 
@@ -55,6 +56,63 @@ def _scenes(n: int, seed0: int):
     from fbme_b200 import scenes
 
     return [scenes.config_scene("c2", seed0 + i) for i in range(n)]
+
+
+def learned_section(device, steps: int, batch: int = 256) -> dict:
+    """Plain vs learned+batched FBME on held-out scenes of the learned
+    distribution (256x256 / 128x128, K ~ U{100..400}, SNR ~ U[5, 25] dB,
+    seeds 2*10^6 ...): scenes/s of the warm-started plan (1 UAMP sweep,
+    plain fallback on, which reads the fallback count on the host every
+    replay), of the plain Stable plan on the same batch, and of the plain
+    plan solving one scene per replay; raw NMSE of each."""
+    import numpy as np
+    import torch
+
+    from fbme_b200 import scenes
+    from fbme_b200.learned import make_learned_plan
+    from torch_sbl_fastest_stable import make_stable_plan
+
+    sc = [scenes.learned_scene(2_000_000 + i) for i in range(batch)]
+    y = torch.from_numpy(np.stack([s.y for s in sc])).to(device)
+    x_true = np.stack([s.x.reshape(-1) for s in sc])
+
+    def nmse(xh):
+        xh = xh.reshape(len(sc), -1)
+        return float(np.mean(10 * np.log10(np.sum(np.abs(xh - x_true) ** 2, 1) / np.sum(np.abs(x_true) ** 2, 1))))
+
+    def rate(fn, n_scenes, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(device)
+        return n_scenes * reps / (e0.elapsed_time(e1) / 1000.0)
+
+    learned = make_learned_plan(y, GRID, warmup=1)
+    plain = make_stable_plan(y, GRID, warmup=1)
+    r_learned = rate(lambda: learned.replay(y), batch, steps)
+    fallbacks = learned.fallbacks
+    n_learned = nmse(learned.replay(y, synchronize=True).x.cpu().numpy())
+    r_plain = rate(lambda: plain.replay(y), batch, steps)
+    n_plain = nmse(plain.replay(y, synchronize=True).x.cpu().numpy())
+    single = make_stable_plan(y[:1], GRID, warmup=1)
+    r_single = rate(lambda: single.replay(y[:1]), 1, max(steps, 50))
+    return {
+        "workload": "held-out learned-distribution scenes, 256x256 / 128x128, K~U{100..400}, "
+                    f"SNR~U[5,25] dB, batch {batch}",
+        "learned_batched_scenes_per_s": r_learned,
+        "plain_batched_scenes_per_s": r_plain,
+        "plain_single_scene_scenes_per_s": r_single,
+        "learned_batched_vs_plain_single": r_learned / r_single,
+        "learned_vs_plain_batched": r_learned / r_plain,
+        "nmse_db": {"plain": n_plain, "learned": n_learned},
+        "fallbacks_per_replay": fallbacks,
+        "learned_sweeps": 1, "plain_sweeps": 4,
+    }
 
 
 # ---------------------------------------------------------------- CPU side
@@ -312,6 +370,9 @@ def run_ours(a: argparse.Namespace) -> None:
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_baseline(a.cpu_sample, a.profile)
+    learned = None
+    if world == 1 and not a.no_learned:
+        learned = learned_section(device, min(a.steps, 20))
 
     if rank == 0:
         line = {
@@ -343,6 +404,8 @@ def run_ours(a: argparse.Namespace) -> None:
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if learned is not None:
+            line["learned"] = learned
         print(json.dumps(line), flush=True)
     del plan
     if dist is not None:

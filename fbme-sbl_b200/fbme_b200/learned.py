@@ -237,14 +237,15 @@ def attach_warm_start(engine: FBMEEngine, net: WarmStartNet) -> Tensor:
 class LearnedSBLPlan:
     """Warm-started FBME plan with the plain plan as fallback.
 
-    Two CUDA graphs over one input buffer: the warm-started solve (the
+    Two CUDA graphs: the warm-started solve of the whole batch (the
     network's prior, ``sweeps`` UAMP sweeps, the profile's polish) and the
-    plain locked plan of the same profile.  ``replay`` launches the warm
-    graph, applies the evidence / residual check per scene and, when a scene
-    fails it, launches the plain graph and returns its result for those
-    scenes (this reads the failure count on the host, so a replay with
-    fallback synchronises the stream).  Results are graph-owned, as for the
-    plain plans.
+    plain locked plan of the same profile for ``fallback_batch`` scenes.
+    ``replay`` launches the warm graph, applies the evidence / residual
+    check per scene, solves the scenes that fail it with the plain plan (in
+    groups of ``fallback_batch``) and returns the plain results for them
+    (this reads the failure count on the host, so a replay with fallback
+    synchronises the stream).  Results are graph-owned, as for the plain
+    plans.
 
     Check (per scene): finite negative log evidence, status 0, monotone
     evidence trace, and fixed-point residuals of the prior and the noise no
@@ -258,7 +259,7 @@ class LearnedSBLPlan:
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, net: WarmStartNet | None = None,
                  weights: str | Path = DEFAULT_WEIGHTS, sweeps: int = 1, polish_size: int = 32,
                  warmup: int = 3, profile: str = "stable", gamma_residual_max: float = 0.75,
-                 noise_residual_max: float = 0.05) -> None:
+                 noise_residual_max: float = 0.05, fallback_batch: int = 16) -> None:
         from torch_sbl_fastest_stable import make_fastest_plan, make_stable_plan
 
         from .plans import CUDAGraphSBLPlan
@@ -273,9 +274,11 @@ class LearnedSBLPlan:
             example_data, grid_shape, config=cfg, warmup=warmup,
             engine_hook=lambda eng: self._ws.append(attach_warm_start(eng, self.net)))
         make = make_stable_plan if profile == "stable" else make_fastest_plan
-        self._plain = make(example_data, grid_shape, polish_size=polish_size, warmup=warmup)
         self.input_buffer = self._warm.input_buffer
         self.batch = self._warm._engine.batch
+        flat = self.input_buffer.reshape(self.batch, *self.input_buffer.shape[-2:])
+        self._fb = min(int(fallback_batch), self.batch)
+        self._plain = make(flat[: self._fb].clone(), grid_shape, polish_size=polish_size, warmup=warmup)
         self.gamma_residual_max = gamma_residual_max
         self.noise_residual_max = noise_residual_max
         self.fallbacks = 0
@@ -302,12 +305,19 @@ class LearnedSBLPlan:
         if fallback:
             bad = (~self.passed).nonzero().flatten()
             self.fallbacks = int(bad.numel())
-            if self.fallbacks:
-                plain = self._plain.replay(self.input_buffer)
+            flat = self.input_buffer.reshape(self.batch, *self.input_buffer.shape[-2:])
+            for c0 in range(0, self.fallbacks, self._fb):
+                # the failed scenes, in groups of the fallback plan's batch (the
+                # last group padded with its first scene)
+                idx = bad[c0:c0 + self._fb]
+                take = torch.cat([idx, idx[:1].expand(self._fb - idx.numel())])
+                plain = self._plain.replay(flat[take])
                 for f in fields(res):
                     v, pv = getattr(res, f.name), getattr(plain, f.name)
-                    if isinstance(v, Tensor) and isinstance(pv, Tensor) and v.shape == pv.shape:
-                        v.view(self.batch, -1)[bad] = pv.view(self.batch, -1)[bad]
+                    if (isinstance(v, Tensor) and isinstance(pv, Tensor) and v.ndim >= 1
+                            and v.shape[1:] == pv.shape[1:] and v.shape[0] == self.batch
+                            and pv.shape[0] == self._fb):
+                        v[idx] = pv[: idx.numel()]
         if synchronize:
             torch.cuda.synchronize(self.input_buffer.device)
         return res
