@@ -4,21 +4,24 @@
 // replaces the initial prior of torch_sbl/solver.py:1072-1099).
 //
 //   x   = features(A^H y)                       [B][H][W][8]  BF16 (2 used)
-//   h1  = relu(conv(x, W1) + b1)                [B][H][W][16] BF16
-//   h2  = relu(conv(h1, W2) + b2)               [B][H][W][16] BF16
+//   h1  = relu(conv(x, W1) + b1)                [B][H][W][8]  BF16
+//   h2  = relu(conv(h1, W2) + b2)               [B][H][W][8]  BF16
 //   out = conv(h2, W3) + b3                     [B][H][W]     FP32
 //   prior0 = max(data_power / N * exp(out), floor)
 //
-// Convolutions run as implicit GEMMs on the tensor cores
-// (mma.sync m16n8k16, BF16 operands, FP32 accumulation): M = 16 pixels of
-// one tile row, N = 8 output channels, K = (tap, input channel) with the
-// channel fastest, so an operand pair is one 32-bit load from the NHWC tile
-// in shared memory.  The gradient with respect to a layer input is the same
+// The 8-to-8-channel convolutions (layer 2 forward, the input gradients)
+// run as implicit GEMMs on the tensor cores (mma.sync m16n8k16, BF16
+// operands, FP32 accumulation): M = 16 pixels of one tile row, N = 8 output
+// channels, K = (tap, input channel) with the channel fastest, so an operand
+// pair is one 32-bit load from the NHWC tile in shared memory.  Layers 1
+// (2 inputs) and 3 (1 output) run on the CUDA cores: padded to MMA shapes
+// they would waste most of the work.  The gradient with respect to a layer input is the same
 // convolution with flipped, transposed weights; the weight gradient is a
 // reduction over pixels on the CUDA cores with fixed-order block partials.
 // Parameters are an FP32 master vector; every use packs them into the BF16
 // matrices the kernels read.
 #include <cuda_bf16.h>
+#include <type_traits>
 #include <math.h>
 
 #include <algorithm>
@@ -29,7 +32,7 @@
 namespace fbme {
 namespace cnn {
 
-constexpr int kHid = 16;   // hidden channels
+constexpr int kHid = 8;    // hidden channels
 constexpr int kInP = 8;    // input feature channels, padded (2 used)
 constexpr int kIn = 2;
 constexpr int kTileH = 8, kTileW = 16;
@@ -57,7 +60,9 @@ struct Packed {
   __nv_bfloat16* wt3;  // [8][144]
   __nv_bfloat16* wb3;  // [16][80]   d h2 = conv(d out, W3 flipped)
   __nv_bfloat16* wb2;  // [16][144]  d h1 = conv(d a2, W2 flipped)
-  float *b1, *b2, *b3;  // [16], [16], [8]
+  float *b1, *b2, *b3;  // [kHid], [kHid], [8]
+  float* w1f;  // [9][2][kHid]  layer 1, BF16-rounded, for the CUDA-core forward
+  float* w3f;  // [9][kHid]     layer 3, BF16-rounded
 };
 
 __global__ void pack_kernel(const float* p, Packed P) {
@@ -88,6 +93,8 @@ __global__ void pack_kernel(const float* p, Packed P) {
     P.b1[i] = p[kOffB1 + i];
     P.b2[i] = p[kOffB2 + i];
   }
+  if (i < 9 * kIn * kHid) P.w1f[i] = __bfloat162float(__float2bfloat16_rn(p[kOffW1 + i]));
+  if (i < 9 * kHid) P.w3f[i] = __bfloat162float(__float2bfloat16_rn(p[kOffW3 + i]));
   if (i < 8) P.b3[i] = i == 0 ? p[kOffB3] : 0.f;
 }
 
@@ -132,6 +139,25 @@ conv3x3_kernel(const TIn* x, const __nv_bfloat16* mask, const __nv_bfloat16* wt,
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH, b = blockIdx.z;
   const long long img = static_cast<long long>(b) * H * W;
+  if (std::is_same<TIn, __nv_bfloat16>::value && CIN % 8 == 0 && !mask) {
+    // BF16 input without a mask: 16-byte loads, all of a thread's issued
+    // before any is stored.
+    constexpr int V = CIN / 8, NV = HW * WW * V, IT = (NV + kConvThreads - 1) / kConvThreads;
+    uint4 v[IT];
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+      const int i = tid + j * kConvThreads, pix = i / V;
+      const int gy = y0 - 1 + pix / WW, gx = x0 - 1 + pix % WW;
+      v[j] = make_uint4(0u, 0u, 0u, 0u);
+      if (i < NV && gy >= 0 && gy < H && gx >= 0 && gx < W)
+        v[j] = *reinterpret_cast<const uint4*>(x + (img + static_cast<long long>(gy) * W + gx) * CIN + 8 * (i % V));
+    }
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+      const int i = tid + j * kConvThreads;
+      if (i < NV) reinterpret_cast<uint4*>(xs)[i] = v[j];
+    }
+  } else
   for (int i = tid; i < HW * WW * WPP; i += kConvThreads) {
     const int pix = i / WPP, w2 = i % WPP;
     const int gy = y0 - 1 + pix / WW, gx = x0 - 1 + pix % WW;
@@ -223,6 +249,120 @@ conv3x3_kernel(const TIn* x, const __nv_bfloat16* mask, const __nv_bfloat16* wt,
           *reinterpret_cast<float2*>(static_cast<float*>(out) + pix * COUTP + co) = make_float2(v0, v1);
         }
       }
+    }
+  }
+}
+
+// Layers with few channels on the CUDA cores: 3x3 convolution, zero
+// padding 1, from CIN channels of an NHWC BF16 input (stride CSTR) to COUT
+// outputs over a 16 x 32 tile; each of the 128 threads computes 4 pixels
+// of one column, so every input value loaded from shared memory serves up
+// to 3 taps of 4 pixels and every weight vector 4 pixels.  BF16-rounded
+// weights w[tap][ci][co], FP32 accumulation.  RELU_BF16: relu, BF16 NHWC
+// output with COUT channels; else FP32 channel 0.  With f1part (layer 1),
+// input channel 1 is not read: it is the scene constant BF16(sum of the
+// nparts feature partials f1part[b * 128 + 64 + k] / N), the value the
+// third feature pass stores.
+constexpr int kSmallTW = 16, kSmallTH = 32, kSmallThreads = 128, kSmallRows = 4;
+template <int CIN, int CSTR, int COUT, bool RELU_BF16>
+__global__ void __launch_bounds__(kSmallThreads)
+conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, void* out, int H, int W,
+                  const double* f1part = nullptr, int nparts = 0) {
+  static_assert(CIN == 2 || CIN == 8, "input channels: one 32-bit or 128-bit load");
+  static_assert(COUT == 8 || COUT == 1, "output channels");
+  constexpr int TW = kSmallTW + 2, TH = kSmallTH + 2, NP = TW * TH, R = kSmallRows;
+  constexpr int NW = 9 * CIN * COUT;
+  __shared__ float xs[CIN * NP];  // channel-major: lanes read consecutive words
+  __shared__ __align__(16) float ws[NW + 8];
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * kSmallTW, y0 = blockIdx.y * kSmallTH, b = blockIdx.z;
+  const long long img = static_cast<long long>(b) * H * W;
+  float c1 = 0.f;
+  if (CIN == 2 && f1part) {
+    double f1 = 0.0;
+    for (int k = 0; k < nparts; ++k) f1 += f1part[b * 128 + 64 + k];
+    c1 = __bfloat162float(__float2bfloat16_rn(static_cast<float>(f1 / (static_cast<double>(H) * W))));
+  }
+  // All of a thread's global loads are issued before any is stored.
+  constexpr int IT = (NP + kSmallThreads - 1) / kSmallThreads;
+  using LoadT = typename std::conditional<CIN == 8, uint4, uint32_t>::type;
+  LoadT v[IT];
+  bool in[IT];
+#pragma unroll
+  for (int j = 0; j < IT; ++j) {
+    const int pix = tid + j * kSmallThreads;
+    const int gy = y0 - 1 + pix / TW, gx = x0 - 1 + pix % TW;
+    in[j] = pix < NP && gy >= 0 && gy < H && gx >= 0 && gx < W;
+    v[j] = LoadT{};
+    if (in[j]) v[j] = *reinterpret_cast<const LoadT*>(x + (img + static_cast<long long>(gy) * W + gx) * CSTR);
+  }
+#pragma unroll
+  for (int j = 0; j < IT; ++j) {
+    const int pix = tid + j * kSmallThreads;
+    if (pix >= NP) break;
+    if constexpr (CIN == 8) {
+      const uint32_t u[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[k]));
+        xs[(2 * k) * NP + pix] = f.x;
+        xs[(2 * k + 1) * NP + pix] = f.y;
+      }
+    } else {
+      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v[j]));
+      xs[pix] = f.x;
+      xs[NP + pix] = f1part ? (in[j] ? c1 : 0.f) : f.y;
+    }
+  }
+  for (int i = tid; i < NW; i += kSmallThreads) ws[i] = w[i];
+  if (tid < COUT) ws[NW + tid] = bias[tid];
+  __syncthreads();
+  const int px = tid % kSmallTW, r0 = (tid / kSmallTW) * R;
+  float acc[R][COUT];
+#pragma unroll
+  for (int p = 0; p < R; ++p)
+#pragma unroll
+    for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
+#pragma unroll
+  for (int ci = 0; ci < CIN; ++ci) {
+    float xw[R + 2][3];
+#pragma unroll
+    for (int r = 0; r < R + 2; ++r)
+#pragma unroll
+      for (int dx = 0; dx < 3; ++dx) xw[r][dx] = xs[ci * NP + (r0 + r) * TW + px + dx];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      float wv[COUT];
+      if constexpr (COUT == 8) {
+        const float4 a = *reinterpret_cast<const float4*>(ws + (tap * CIN + ci) * 8);
+        const float4 c = *reinterpret_cast<const float4*>(ws + (tap * CIN + ci) * 8 + 4);
+        wv[0] = a.x; wv[1] = a.y; wv[2] = a.z; wv[3] = a.w;
+        wv[4] = c.x; wv[5] = c.y; wv[6] = c.z; wv[7] = c.w;
+      } else {
+        wv[0] = ws[tap * CIN + ci];
+      }
+#pragma unroll
+      for (int p = 0; p < R; ++p)
+#pragma unroll
+        for (int co = 0; co < COUT; ++co) acc[p][co] += xw[p + tap / 3][tap % 3] * wv[co];
+    }
+  }
+  const int gx = x0 + px;
+  if (gx >= W) return;
+#pragma unroll
+  for (int p = 0; p < R; ++p) {
+    const int gy = y0 + r0 + p;
+    if (gy >= H) break;
+    const long long pix = img + static_cast<long long>(gy) * W + gx;
+    if constexpr (RELU_BF16) {
+      static_assert(!RELU_BF16 || COUT == 8, "one 128-bit store per pixel");
+      uint32_t o[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        o[k] = pack_bf16x2(fmaxf(acc[p][2 * k] + ws[NW + 2 * k], 0.f), fmaxf(acc[p][2 * k + 1] + ws[NW + 2 * k + 1], 0.f));
+      *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * COUT) = make_uint4(o[0], o[1], o[2], o[3]);
+    } else {
+      static_cast<float*>(out)[pix] = acc[p][0] + ws[NW];
     }
   }
 }
@@ -378,7 +518,7 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
     if (pass == 0) {
       acc += e;
     } else if (pass == 1) {
-      const float f0 = static_cast<float>(log(e / mean + 1e-3));
+      const float f0 = logf(static_cast<float>(e / mean) + 1e-3f);
       acc += f0;
       uint4 w;
       w.x = pack_bf16x2(f0, 0.f);
@@ -476,6 +616,8 @@ cnn::Packed packed_at(uint8_t* w) {
   P.b1 = reinterpret_cast<float*>(take(kHid * 4));
   P.b2 = reinterpret_cast<float*>(take(kHid * 4));
   P.b3 = reinterpret_cast<float*>(take(8 * 4));
+  P.w1f = reinterpret_cast<float*>(take(9 * kIn * kHid * 4));
+  P.w3f = reinterpret_cast<float*>(take(9 * kHid * 4));
   return P;
 }
 
@@ -494,16 +636,26 @@ const char* cnn_check(long long B, long long H, long long W) {
   return nullptr;
 }
 
-void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t st) {
+namespace {
+int feature_parts(int H, int W) {
+  return static_cast<int>(std::min<long long>(64, (static_cast<long long>(H) * W + 255) / 256));
+}
+// Passes 0 and 1 (the energy mean, f0 and its partial sums); pass 2 stores
+// the f1 channel, which only the backward pass reads from the workspace.
+void features_passes(const float2* bp, int B, int H, int W, void* ws, int passes, cudaStream_t st) {
   using namespace cnn;
   const CnnLayout L = cnn_layout(B, H, W);
   uint8_t* w = static_cast<uint8_t*>(ws);
-  const long long N = static_cast<long long>(H) * W;
   auto* x8 = reinterpret_cast<__nv_bfloat16*>(w + L.x8);
   auto* fpart = reinterpret_cast<double*>(w + L.fpart);
-  const int nb = static_cast<int>(std::min<long long>(64, (N + 255) / 256));
-  for (int pass = 0; pass < 3; ++pass)
-    features_kernel<<<dim3(nb, B), 256, 0, st>>>(pass, bp, B, N, x8, fpart);
+  for (int pass = 0; pass < passes; ++pass)
+    features_kernel<<<dim3(feature_parts(H, W), B), 256, 0, st>>>(pass, bp, B, static_cast<long long>(H) * W,
+                                                                  x8, fpart);
+}
+}  // namespace
+
+void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t st) {
+  features_passes(bp, B, H, W, ws, 3, st);
 }
 
 // Forward pass from the features in the workspace; the output [B][H][W]
@@ -518,13 +670,13 @@ void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out,
   auto* x8 = reinterpret_cast<const __nv_bfloat16*>(w + L.x8);
   auto* h1 = reinterpret_cast<__nv_bfloat16*>(w + L.h1);
   auto* h2 = reinterpret_cast<__nv_bfloat16*>(w + L.h2);
-  conv3x3_kernel<__nv_bfloat16, kInP, kHid, kOutReluBf16><<<grid, kConvThreads, 0, st>>>(
-      x8, nullptr, P.wt1, P.b1, h1, H, W);
+  const dim3 grid_small((W + kSmallTW - 1) / kSmallTW, (H + kSmallTH - 1) / kSmallTH, B);
+  conv_small_kernel<kIn, kInP, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
+      x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
   conv3x3_kernel<__nv_bfloat16, kHid, kHid, kOutReluBf16><<<grid, kConvThreads, 0, st>>>(
       h1, nullptr, P.wt2, P.b2, h2, H, W);
   float* wout = reinterpret_cast<float*>(w + L.out);  // kept for cnn_backward
-  conv3x3_kernel<__nv_bfloat16, kHid, 8, kOutF32Ch0><<<grid, kConvThreads, 0, st>>>(
-      h2, nullptr, P.wt3, P.b3, wout, H, W);
+  conv_small_kernel<kHid, kHid, 1, false><<<grid_small, kSmallThreads, 0, st>>>(h2, P.w3f, P.b3, wout, H, W);
   if (out && out != wout)
     cudaMemcpyAsync(out, wout, static_cast<size_t>(B) * H * W * sizeof(float), cudaMemcpyDeviceToDevice, st);
 }
@@ -582,7 +734,7 @@ void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, 
                     const float* data_power, const float* floor_, float* gamma, double* upart,
                     int nblocks, cudaStream_t st) {
   using namespace cnn;
-  cnn_features(bp, B, H, W, ws, st);
+  features_passes(bp, B, H, W, ws, 2, st);
   const CnnLayout L = cnn_layout(B, H, W);
   float* out = reinterpret_cast<float*>(static_cast<uint8_t*>(ws) + L.out);
   cnn_forward(params, B, H, W, ws, out, st);

@@ -1,7 +1,7 @@
 """Learned warm start of the FBME plans (no counterpart in the reference).
 
-A 3-layer 3x3 convolutional network (16 hidden channels, 2,769 parameters;
-BF16 operands on the tensor cores, FP32 accumulation; csrc/cnn.cu) maps the
+A 3-layer 3x3 convolutional network (8 hidden channels, 809 parameters;
+BF16 operands, FP32 accumulation; csrc/cnn.cu) maps the
 features of the backprojection A^H y to the log of the initial prior
 variance relative to the uniform level P/N (P the data power).  It replaces
 the backprojection-blend initialisation of torch_sbl/solver.py:1072-1099;
@@ -38,7 +38,7 @@ from . import scenes
 from .config import SBLConfig
 from .engine import FBMEEngine
 
-HIDDEN = 16
+HIDDEN = 8
 TARGET_CLAMP = 20.0
 WEIGHTS_DIR = Path(__file__).resolve().parent / "weights"
 DEFAULT_WEIGHTS = WEIGHTS_DIR / "warm_start_256x256_128x128.npz"

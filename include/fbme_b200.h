@@ -271,12 +271,12 @@ int fbme_pcg_solve(FbmeCgPlan* plan, const float* prior, const float* noise, con
 /* ------------------------------------------------------------------------
  * Learned warm start (no counterpart in the reference: it is the learned
  * part of this implementation).  A 3-layer 3x3 convolutional network
- * (16 hidden channels, BF16 operands, FP32 accumulation) maps the features
+ * (8 hidden channels, BF16 operands, FP32 accumulation) maps the features
  * of A^H y to the initial log prior variance that replaces the
  * backprojection initialisation of torch_sbl/solver.py:1072-1099.
  * Parameters are an FP32 vector of fbme_cnn_param_count() values; the
- * layout is W1[3][3][2][16], b1[16], W2[3][3][16][16], b2[16],
- * W3[3][3][16][1], b3[1].  Grids need N1 % 8 == 0 and N2 % 16 == 0.
+ * layout is W1[3][3][2][8], b1[8], W2[3][3][8][8], b2[8], W3[3][3][8][1],
+ * b3[1] (809 values).  Grids need N1 % 8 == 0 and N2 % 16 == 0.
  * ---------------------------------------------------------------------- */
 int32_t fbme_cnn_param_count(void);
 size_t fbme_cnn_workspace_bytes(int32_t batch, int32_t n1, int32_t n2);

@@ -98,7 +98,7 @@ def loss_and_grads(params, x, target, mask=None):
     return loss, out, {"W1": dW1, "b1": db1, "W2": dW2, "b2": db2, "W3": dW3, "b3": db3}
 
 
-def init_params(hidden: int = 16, seed: int = 0):
+def init_params(hidden: int = 8, seed: int = 0):
     """He-style initial weights (FP64)."""
     rng = np.random.default_rng(seed)
     def w(ci, co):

@@ -21,7 +21,9 @@ GRID = (32, 48)
 
 
 def _flat_to_dict(p):
-    h = 16
+    from fbme_b200.learned import HIDDEN
+
+    h = HIDDEN
     o, d = 0, {}
     for name, shape in (("W1", (3, 3, 2, h)), ("b1", (h,)), ("W2", (3, 3, h, h)), ("b2", (h,)),
                         ("W3", (3, 3, h, 1)), ("b3", (1,))):
