@@ -32,6 +32,12 @@ class FbmeShape(ctypes.Structure):
     _fields_ = [("n1", c_int32), ("n2", c_int32), ("m1", c_int32), ("m2", c_int32)]
 
 
+class FbmeShapeParams(ctypes.Structure):
+    """Per-shape settings of a plan (uneven batches, tuned tile width)."""
+    _fields_ = [("shape", FbmeShape), ("uamp_iterations", c_int32), ("uamp_damping", c_float),
+                ("exchange_size", c_int32), ("dft_n_tile", c_int32)]
+
+
 class FbmeConfig(ctypes.Structure):
     _fields_ = [
         ("uamp_iterations", c_int32),
@@ -163,6 +169,13 @@ SIGNATURES = {
     "fbme_plan_workspace_bytes": (c_size_t, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig)]),
     "fbme_plan_create": (c_int, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig), c_void_p,
                                  c_size_t, c_void_p, POINTER(c_void_p)]),
+    "fbme_plan_workspace_bytes_ex": (c_size_t, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig),
+                                                POINTER(FbmeShapeParams), c_int32]),
+    "fbme_plan_create_ex": (c_int, [POINTER(FbmeShape), c_int32, POINTER(FbmeConfig),
+                                    POINTER(FbmeShapeParams), c_int32, c_void_p, c_size_t, c_void_p,
+                                    POINTER(c_void_p)]),
+    "fbme_plan_bucket_count": (c_int32, [c_void_p]),
+    "fbme_plan_bucket": (c_int, [c_void_p, c_int32, POINTER(FbmeShapeParams), POINTER(c_int32)]),
     "fbme_plan_replay": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
     "fbme_plan_destroy": (c_int, [c_void_p]),
     "fbme_dft_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -397,3 +397,23 @@ def _rules(c: SBLConfig):
            or c.offgrid_damping <= 0.0 or c.offgrid_ridge < 0.0)
     yield "dft_terms must be 3 or 6.", c.dft_terms not in (3, 6)
     yield "cg_dft_terms must be 3 or 6.", c.cg_dft_terms not in (3, 6)
+
+
+def fbme_profile_config(profile: str = "stable", polish_size: int = 32,
+                        sweeps: int | None = None) -> SBLConfig:
+    """The configuration of the FBME plans (torch_sbl_fastest_stable/
+    profiles.py:63-70 for "fast", 110-115 for "stable"), optionally with a
+    fixed UAMP sweep budget instead of the auto rule."""
+    if profile not in ("stable", "fast"):
+        raise ValueError("profile must be 'stable' or 'fast'")
+    over: dict[str, Any] = dict(uamp_polish_size=polish_size,
+                                uamp_polish_compute_truncation_diagnostic=False)
+    if profile == "stable":
+        over.update(uamp_polish_iterations=3, uamp_polish_residual_exchange_size=12,
+                    uamp_polish_fixed_budget_diagnostics=True)
+    else:
+        over.update(uamp_polish_iterations=2, uamp_polish_residual_exchange_size=0,
+                    uamp_polish_fixed_budget_diagnostics=False)
+    if sweeps is not None:
+        over.update(uamp_auto_iterations=False, max_iter=int(sweeps), min_iter=1, uamp_min_iter=1)
+    return SBLConfig.paper_hybrid_uamp(**over)

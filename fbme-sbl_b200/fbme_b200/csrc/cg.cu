@@ -1666,6 +1666,7 @@ int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig*
   P->tables.adj_n1 = w + L.tab_a1;
   P->tables.kchunks_n1 = cdiv(2LL * s.n1, 64);
   P->tables.kchunks_n2 = cdiv(2LL * s.n2, 64);
+  P->tables.n_tile = nt;
   P->dir1 = reinterpret_cast<float2*>(w + L.dir1);
   P->dir2 = reinterpret_cast<float2*>(w + L.dir2);
   fbme::launch_dirichlet(P->dir1, s.m1, s.n1, st);

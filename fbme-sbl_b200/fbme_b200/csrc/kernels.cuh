@@ -92,6 +92,7 @@ struct DftTables {
   const uint8_t* adj_n2;  // L = N2, sign +1
   const uint8_t* adj_n1;  // L = N1, sign +1
   int kchunks_n1, kchunks_n2;
+  int n_tile;  // real output columns per stage tile the tables are laid out for
 };
 
 // Buffers of the UAMP stage.

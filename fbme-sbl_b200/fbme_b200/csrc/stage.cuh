@@ -150,7 +150,22 @@ static inline int persistent_grid(const DftGeom& g) {
   return t < s ? t : s;
 }
 
+// Default stage tile width (real output columns): 256 for 3-term
+// products, 128 for 6 (the 6-term operands fill shared memory sooner).
+// Plans may lay their tables out for 64 or 128 columns with 3 terms
+// instead (dft_n_tile_ok), which wastes less of a tile on short axes.
 static inline int n_tile_of(int terms) { return terms == 6 ? 128 : 256; }
+
+// A tile width a plan of this shape may use: 64, 128 or 256 with 3 terms,
+// 128 with 6, and at most kMaxTilesPerScene tiles per scene in every stage.
+static inline bool dft_n_tile_ok(int terms, int n_tile, const BatchShape& s) {
+  if (terms == 6 ? n_tile != 128 : (n_tile != 64 && n_tile != 128 && n_tile != 256)) return false;
+  const long long r[4][2] = {{s.n1, s.m2}, {s.m2, s.m1}, {s.m1, s.n2}, {s.n2, s.n1}};  // rows, cols
+  for (const auto& rc : r)
+    if (static_cast<long long>(ceil_div(rc[0], kTileRows)) * ceil_div(2 * rc[1], n_tile) > kMaxTilesPerScene)
+      return false;
+  return true;
+}
 
 template <int A_PARTS, int N_TILE, class Pro, class Epi>
 static cudaError_t set_attr() {
@@ -159,24 +174,33 @@ static cudaError_t set_attr() {
                               DftCfg<A_PARTS, N_TILE>::kSmemBytes);
 }
 
+template <int A_PARTS, int N_TILE, class Pro, class Epi>
+static void launch_stage(const DftGeom& g, const Pro& pro, const Epi& epi, int* status, cudaStream_t st) {
+  dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>
+      <<<persistent_grid(g), kDftPersistThreads, DftCfg<A_PARTS, N_TILE>::kSmemBytes, st>>>(g, pro, epi, status);
+}
+
+// One stage launch; the tile width is the one the geometry was built for.
 template <class Pro, class Epi>
 static void run_stage(int terms, const DftGeom& g, const Pro& pro, const Epi& epi, int* status,
                       cudaStream_t st) {
   if (terms == 6) {
-    dft_stage_kernel<3, 128, Pro, Epi>
-        <<<persistent_grid(g), kDftPersistThreads, DftCfg<3, 128>::kSmemBytes, st>>>(g, pro, epi,
-                                                                                     status);
+    launch_stage<3, 128>(g, pro, epi, status, st);
+  } else if (g.col_per_tile == 32) {
+    launch_stage<2, 64>(g, pro, epi, status, st);
+  } else if (g.col_per_tile == 64) {
+    launch_stage<2, 128>(g, pro, epi, status, st);
   } else {
-    dft_stage_kernel<2, 256, Pro, Epi>
-        <<<persistent_grid(g), kDftPersistThreads, DftCfg<2, 256>::kSmemBytes, st>>>(g, pro, epi,
-                                                                                     status);
+    launch_stage<2, 256>(g, pro, epi, status, st);
   }
 }
 
 template <class Pro, class Epi>
 static cudaError_t set_attr_both() {
-  cudaError_t e = set_attr<2, 256, Pro, Epi>();
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  if ((e = set_attr<2, 256, Pro, Epi>()) != cudaSuccess) return e;
+  if ((e = set_attr<2, 128, Pro, Epi>()) != cudaSuccess) return e;
+  if ((e = set_attr<2, 64, Pro, Epi>()) != cudaSuccess) return e;
   return set_attr<3, 128, Pro, Epi>();
 }
 

@@ -433,7 +433,7 @@ cudaError_t set_dft_attributes() {
 
 void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
                  float2* data, float2* tmp, int* status, cudaStream_t st) {
-  const int nt = n_tile_of(terms);
+  const int nt = t.n_tile;
   const DftGeom g1 = stage_geom(kFwd1, s, t, nt), g2 = stage_geom(kFwd2, s, t, nt);
   run_stage(terms, g1, ProPlain{coeff}, EpiStoreT{tmp}, status, st);
   run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{data}, status, st);
@@ -441,7 +441,7 @@ void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float
 
 void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
                  float2* coeff, float2* tmp, int* status, cudaStream_t st) {
-  const int nt = n_tile_of(terms);
+  const int nt = t.n_tile;
   const DftGeom g1 = stage_geom(kAdj1, s, t, nt), g2 = stage_geom(kAdj2, s, t, nt);
   run_stage(terms, g1, ProPlain{data}, EpiStoreT{tmp}, status, st);
   run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{coeff}, status, st);
@@ -452,7 +452,7 @@ void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float
 // variances (backprojection blend or uniform).
 void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
               cudaStream_t st, Profiler* prof) {
-  const int nt = n_tile_of(c.terms);
+  const int nt = t.n_tile;
   const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   FBME_TIMED(prof, FBME_GROUP_INIT,
@@ -478,7 +478,7 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
 // M-sized regions starting at u.msg and u.msg + B*M.
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
               cudaStream_t st, Profiler* prof) {
-  const int nt = n_tile_of(c.terms);
+  const int nt = t.n_tile;
   const DftGeom f1 = stage_geom(kFwd1, s, t, nt), f2 = stage_geom(kFwd2, s, t, nt);
   const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);

@@ -107,7 +107,8 @@ class FBMEEngine:
     """A native plan for ``batch`` scenes of one shape and configuration."""
 
     def __init__(self, batch: int, grid: Sequence[int], sample: Sequence[int], cfg: SBLConfig,
-                 device: torch.device, stream: torch.cuda.Stream | None = None) -> None:
+                 device: torch.device, stream: torch.cuda.Stream | None = None,
+                 n_tile: int | None = None) -> None:
         self.lib = nat.lib()
         if device.type != "cuda":
             raise RuntimeError("the FBME B200 engine needs a CUDA device")
@@ -124,10 +125,13 @@ class FBMEEngine:
         for i in range(self.batch):
             shapes[i] = nat.FbmeShape(self.grid[0], self.grid[1], self.sample[0], self.sample[1])
         self._shapes = shapes
-        nbytes = self.lib.fbme_plan_workspace_bytes(shapes, self.batch, ctypes.byref(self.native_cfg))
+        # the DFT stage tile width (None: the library default)
+        self.n_tile = n_tile
+        self._params = nat.FbmeShapeParams(shapes[0], 0, -1.0, -1, int(n_tile or 0))
+        nbytes = self.lib.fbme_plan_workspace_bytes_ex(shapes, self.batch, ctypes.byref(self.native_cfg),
+                                                       ctypes.byref(self._params), 1)
         if nbytes == 0:
-            nat.check(nat.FBME_ERR_INVALID if "different shapes" not in nat.last_error()
-                      else nat.FBME_ERR_UNSUPPORTED, "fbme_plan_workspace_bytes")
+            nat.check(nat.FBME_ERR_INVALID, "fbme_plan_workspace_bytes")
         self.workspace = torch.empty(int(nbytes) + 256, dtype=torch.uint8, device=device)
         base = self.workspace.data_ptr()
         self._ws_ptr = (base + 255) & ~255
@@ -159,9 +163,10 @@ class FBMEEngine:
         self._plan = ctypes.c_void_p()
         st = stream or torch.cuda.current_stream(device)
         with torch.cuda.device(device):
-            rc = self.lib.fbme_plan_create(shapes, self.batch, ctypes.byref(self.native_cfg),
-                                           ctypes.c_void_p(self._ws_ptr), ctypes.c_size_t(nbytes),
-                                           ctypes.c_void_p(st.cuda_stream), ctypes.byref(self._plan))
+            rc = self.lib.fbme_plan_create_ex(shapes, self.batch, ctypes.byref(self.native_cfg),
+                                              ctypes.byref(self._params), 1, ctypes.c_void_p(self._ws_ptr),
+                                              ctypes.c_size_t(nbytes), ctypes.c_void_p(st.cuda_stream),
+                                              ctypes.byref(self._plan))
         nat.check(rc, "fbme_plan_create")
         # constant result fields of the zero-tail polish (solver.py:4052-4068, 4639-4653)
         self._false = torch.zeros(B, dtype=torch.bool, device=device)

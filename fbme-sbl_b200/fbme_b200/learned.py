@@ -35,7 +35,7 @@ from torch import Tensor
 
 from . import _native as nat
 from . import scenes
-from .config import SBLConfig
+from .config import SBLConfig, fbme_profile_config
 from .engine import FBMEEngine
 
 HIDDEN = 8
@@ -142,16 +142,7 @@ class WarmStartNet:
 def plain_config(sweeps: int | None = None, profile: str = "stable") -> SBLConfig:
     """The FBME plan configuration (profiles.py:63-70, 110-115), optionally
     with a fixed sweep budget instead of the auto rule."""
-    over = dict(uamp_polish_size=32, uamp_polish_compute_truncation_diagnostic=False)
-    if profile == "stable":
-        over.update(uamp_polish_iterations=3, uamp_polish_residual_exchange_size=12,
-                    uamp_polish_fixed_budget_diagnostics=True)
-    else:
-        over.update(uamp_polish_iterations=2, uamp_polish_residual_exchange_size=0,
-                    uamp_polish_fixed_budget_diagnostics=False)
-    if sweeps is not None:
-        over.update(uamp_auto_iterations=False, max_iter=int(sweeps), min_iter=1, uamp_min_iter=1)
-    return SBLConfig.paper_hybrid_uamp(**over)
+    return fbme_profile_config(profile, 32, sweeps)
 
 
 def training_pairs(seeds: Sequence[int], device: torch.device, *, batch: int = 64,

@@ -129,20 +129,58 @@ size_t fbme_plan_workspace_bytes(const FbmeShape* shapes, int32_t n_scenes,
                                  const FbmeConfig* cfg);
 
 /* Build a plan: validate, bind the caller's workspace (256-byte aligned)
- * and fill its constant tables on `stream`.  Launches kernels; call it
- * outside stream capture. */
+ * and fill its constant tables on `stream`.  Launches kernels and waits
+ * for them; call it outside stream capture. */
 int fbme_plan_create(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg,
                      void* workspace, size_t workspace_bytes, fbme_stream_t stream,
                      FbmePlan** plan);
 
-/* Solve every scene: y is [B, M1*M2] complex64 (row-major prefix blocks,
- * scenes back to back).  Asynchronous on `stream`; capturable. */
+/* Solve every scene.  Equal shapes: y is [B, M1*M2] complex64 (row-major
+ * prefix blocks, scenes back to back) and the outputs are as FbmeOutputs
+ * lists them.  Scenes of different shapes (an uneven plan): y holds each
+ * scene's M1*M2 samples back to back in scene order, and the per-pixel
+ * outputs (x, posterior_variance, precision, support_mask) each scene's
+ * N1*N2 values back to back; per-scene outputs stay [B], [B,P], [B,K].
+ * Asynchronous on `stream`; capturable (an uneven plan forks its shape
+ * buckets onto plan-owned streams and joins them back on `stream`). */
 int fbme_plan_replay(FbmePlan* plan, const void* y, const FbmeOutputs* out,
                      fbme_stream_t stream);
 
 int fbme_plan_destroy(FbmePlan* plan);
 
-/* Stage entry points (same plan, same stream rules). */
+/* ------------------------------------------------------------------------
+ * Uneven batches (no counterpart in the reference, which batches only
+ * equal shapes through leading dimensions, torch_sbl/solver.py:966-1001).
+ * A plan may hold scenes of different shapes: it groups them into one
+ * bucket per shape, in order of first appearance; each bucket is solved
+ * as an equal-shape batch with its own tables and state, the buckets run
+ * concurrently, and a gather / scatter kernel pair maps the scene-order
+ * buffers to bucket order and back.  Values that depend on the shape are
+ * set per bucket by FbmeShapeParams (the host resolves them from N and M
+ * as torch_sbl/solver.py:1183-1189 and 1295-1309 do); the solve of a
+ * scene stops after its own bucket's T_u sweeps.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  FbmeShape shape;            /* scenes of this shape use the values below */
+  int32_t uamp_iterations;    /* T_u; <= 0 keeps FbmeConfig.uamp_iterations */
+  float uamp_damping;         /* < 0 keeps FbmeConfig.uamp_damping */
+  int32_t exchange_size;      /* < 0 keeps FbmeConfig.exchange_size */
+  int32_t dft_n_tile;         /* DFT stage tile width in real columns: 64,
+                                 128 or 256 with 3 terms (128 with 6); 0 =
+                                 default (256, or 128 with 6 terms) */
+} FbmeShapeParams;
+
+size_t fbme_plan_workspace_bytes_ex(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg,
+                                    const FbmeShapeParams* params, int32_t n_params);
+int fbme_plan_create_ex(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg,
+                        const FbmeShapeParams* params, int32_t n_params, void* workspace,
+                        size_t workspace_bytes, fbme_stream_t stream, FbmePlan** plan);
+/* Buckets of a plan (1 for equal shapes) and the resolved values of one. */
+int32_t fbme_plan_bucket_count(const FbmePlan* plan);
+int fbme_plan_bucket(const FbmePlan* plan, int32_t bucket, FbmeShapeParams* resolved, int32_t* n_scenes);
+
+/* Stage entry points (same plan, same stream rules; equal-shape plans
+ * only: an uneven plan returns FBME_ERR_UNSUPPORTED). */
 int fbme_dft_forward(FbmePlan* plan, const void* coefficients, void* data, fbme_stream_t stream);
 int fbme_dft_adjoint(FbmePlan* plan, const void* data, void* coefficients, fbme_stream_t stream);
 /* UAMP initialisation, T_u sweeps and the final E-step; the state is left

@@ -1,0 +1,188 @@
+"""Uneven batches and tuned tile widths on the B200.
+
+An uneven plan groups its scenes into one bucket per shape and solves each
+bucket as an equal-shape batch; scenes are independent, so every scene's
+result must equal, bit for bit, the result of an equal-shape plan holding
+that shape's scenes in the same order.  Odd shapes (non-square grids,
+prefix lengths that are not multiples of the tile sizes) are checked
+against the oracle at the parity bar: identical support, x within 1e-4
+relative L2, posterior variance within 1e-3 on the support.  The tile
+width changes only the grouping of the per-tile partial sums, so plans
+with 64-, 128- and 256-column tiles agree to rounding and all meet the bar.
+"""
+
+import numpy as np
+import pytest
+
+from gpu_util import PV_TOL, X_TOL, need_gpu, rel_l2
+
+torch = pytest.importorskip("torch")
+
+A = ((64, 64), (32, 32))
+B = ((128, 64), (48, 40))
+C = ((96, 128), (24, 64))
+ORDER = [A, B, A, C, B, A]
+
+
+def _scenes(shapes, seed0=500):
+    from fbme_b200 import scenes
+
+    out = []
+    for i, (g, s) in enumerate(shapes):
+        k = max(8, int(0.02 * g[0] * g[1]))
+        out.append(scenes.point_scene(g, s, k, 15.0, seed0 + i, "cn"))
+    return out
+
+
+def _cfg(profile="stable"):
+    from fbme_b200.config import fbme_profile_config
+
+    return fbme_profile_config(profile)
+
+
+FIELDS_PIX = ("x", "posterior_variance", "precision", "support_mask")
+FIELDS_SCENE = ("noise_variance", "effective_dof", "negative_log_evidence", "evidence_trace",
+                "support_exchanges_accepted", "fixed_budget_gamma_residual", "fixed_budget_noise_residual",
+                "fixed_budget_objective_decrease", "fixed_budget_monotone", "support_score_threshold",
+                "active_indices", "status")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+def test_uneven_plan_equals_per_shape_plans(profile):
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine, uamp_iteration_limit
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    cfg = _cfg(profile)
+    sc = _scenes(ORDER)
+    eng = UnevenEngine(ORDER, cfg, dev)
+    y = eng.pack([torch.from_numpy(s.y).to(dev) for s in sc])
+    eng.run(y)
+    torch.cuda.synchronize()
+    # buckets in order of first appearance, with the shape's own T_u
+    bk = eng.buckets()
+    assert [(b["grid"], b["sample"], b["scenes"]) for b in bk] == [(A[0], A[1], 3), (B[0], B[1], 2),
+                                                                 (C[0], C[1], 1)]
+    for b in bk:
+        assert b["uamp_iterations"] == uamp_iteration_limit(cfg, b["grid"][0] * b["grid"][1],
+                                                             b["sample"][0] * b["sample"][1])
+    assert len({b["uamp_iterations"] for b in bk}) > 1  # the scenes stop at different sweeps
+    for shape in (A, B, C):
+        idx = [i for i, s in enumerate(ORDER) if s == shape]
+        ref = FBMEEngine(len(idx), shape[0], shape[1], cfg, dev)
+        ys = torch.stack([torch.from_numpy(sc[i].y).to(dev) for i in idx]).reshape(len(idx), -1)
+        ref.run(ys.contiguous())
+        torch.cuda.synchronize()
+        n = shape[0][0] * shape[0][1]
+        for j, i in enumerate(idx):
+            p0 = eng.pix_off[i]
+            for f in FIELDS_PIX:
+                assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][j]), (f, i)
+            for f in FIELDS_SCENE:
+                assert torch.equal(eng.out[f][i], ref.out[f][j]), (f, i)
+        ref.close()
+    assert int(eng.out["status"].abs().sum()) == 0
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_uneven_graph_replay_and_results():
+    need_gpu()
+    from fbme_b200.uneven import UnevenEngine, make_uneven_plan
+
+    dev = torch.device("cuda", 0)
+    sc = _scenes(ORDER, 900)
+    ys = [torch.from_numpy(s.y).to(dev) for s in sc]
+    plan = make_uneven_plan(ys, [s[0] for s in ORDER], warmup=1)
+    res = plan.replay(ys, synchronize=True)
+    assert len(res) == len(ORDER)
+    for r, (g, _) in zip(res, ORDER):
+        assert tuple(r.x.shape) == g and r.x.dtype == torch.complex64
+    eager = UnevenEngine(ORDER, plan.config, dev)
+    eager.run(eager.pack(ys))
+    torch.cuda.synchronize()
+    for f in FIELDS_PIX + FIELDS_SCENE:
+        assert torch.equal(plan.engine.out[f], eager.out[f]), f
+    # new data through the packed entry point, then the first data again
+    other = [torch.from_numpy(s.y).to(dev) for s in _scenes(ORDER, 950)]
+    x0 = res[3].x.clone()
+    plan.replay(torch.cat([o.reshape(-1) for o in other]), synchronize=True)
+    assert not torch.equal(plan.result[3].x, x0)
+    plan.replay(ys, synchronize=True)
+    assert torch.equal(plan.result[3].x, x0)
+    eager.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [B, C], ids=["128x64_48x40", "96x128_24x64"])
+def test_uneven_scene_matches_oracle(shape):
+    need_gpu()
+    from fbme_b200.uneven import UnevenEngine
+    from oracle import fbme_oracle as O
+
+    dev = torch.device("cuda", 0)
+    order = [A, shape, A]
+    sc = _scenes(order, 1300)
+    eng = UnevenEngine(order, _cfg(), dev)
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    res = eng.results()
+    for i in (0, 1):
+        g = order[i][0]
+        ref = O.fbme_solve(sc[i].y[None], g, "stable")
+        x = res[i].x.cpu().numpy().reshape(-1)
+        xr = ref["x"].reshape(-1)
+        assert set(np.flatnonzero(x)) == set(np.flatnonzero(xr))
+        assert rel_l2(x, xr) < X_TOL
+        pv = res[i].posterior_variance.cpu().numpy().reshape(-1)
+        pvr = ref["posterior_variance"].reshape(-1)
+        sup = xr != 0
+        assert np.max(np.abs(pv[sup] - pvr[sup]) / pvr[sup]) < PV_TOL
+        assert res[i].iterations == int(ref["iterations"])
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_tile_widths_agree_and_meet_the_bar():
+    need_gpu()
+    from fbme_b200.autotune import candidates
+    from fbme_b200.engine import FBMEEngine
+    from oracle import fbme_oracle as O
+
+    dev = torch.device("cuda", 0)
+    shape = B
+    sc = _scenes([shape] * 3, 1700)
+    y_np = np.stack([s.y for s in sc])
+    y = torch.from_numpy(y_np).to(dev).reshape(3, -1).contiguous()
+    xs = {}
+    for w in candidates(*shape):
+        e = FBMEEngine(3, shape[0], shape[1], _cfg(), dev, n_tile=w)
+        e.run(y)
+        torch.cuda.synchronize()
+        xs[w] = e.out["x"].cpu().numpy()
+        assert int(e.out["status"].abs().sum()) == 0
+        e.close()
+    assert set(xs) == {64, 128, 256}
+    ref = O.fbme_solve(y_np, shape[0], "stable")["x"].reshape(3, -1)
+    for w, x in xs.items():
+        for i in range(3):
+            assert set(np.flatnonzero(x[i])) == set(np.flatnonzero(ref[i])), w
+            assert rel_l2(x[i], ref[i]) < X_TOL, w
+            assert rel_l2(x[i], xs[256][i]) < 1e-5, w
+
+
+@pytest.mark.gpu
+def test_autotuner_times_every_width_and_caches(tmp_path):
+    need_gpu()
+    from fbme_b200.autotune import TileCache, candidates, tune_shape
+
+    dev = torch.device("cuda", 0)
+    cache = TileCache(tmp_path / "tune.json")
+    best = tune_shape(A[0], A[1], _cfg(), dev, 8, cache=cache)
+    assert best in candidates(*A)
+    (entry,) = cache.entries.values()
+    assert set(entry["ms"]) == {str(w) for w in candidates(*A)}
+    assert all(t > 0 for t in entry["ms"].values())
+    assert entry["ms"][str(best)] == min(entry["ms"].values())
