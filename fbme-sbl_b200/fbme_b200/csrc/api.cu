@@ -296,6 +296,9 @@ int plan_spec(const FbmeShape* shapes, int n, const FbmeConfig* c, const FbmeSha
     k.L = make_layout(k.s, k.cfg, nt);
     k.base = off;
     off = align256(off + k.L.total);
+    // each bucket's staging starts on a 256-byte boundary
+    pix = (pix + 255) & ~255LL;
+    smp = (smp + 31) & ~31LL;
     k.first = first;
     k.pix0 = pix;
     k.smp0 = smp;

@@ -450,10 +450,18 @@ void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float
 // Initialisation shared by the UAMP and PCG paths (solver.py:1063-1159):
 // A^H y, data power, variance floor, initial noise and the initial prior
 // variances (backprojection blend or uniform).
+// Geometry of a stage whose prologue reads the caller's observations y:
+// vector (16-byte) accesses need y itself 16-byte aligned, which a caller's
+// pointer need not be (complex64 is 8-byte aligned).
+static DftGeom with_y(DftGeom g, const float2* y) {
+  if (reinterpret_cast<uintptr_t>(y) & 15u) g.vec4 = 0;
+  return g;
+}
+
 void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
               cudaStream_t st, Profiler* prof) {
   const int nt = t.n_tile;
-  const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
+  const DftGeom a1 = with_y(stage_geom(kAdj1, s, t, nt), u.y), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   FBME_TIMED(prof, FBME_GROUP_INIT,
              run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st));
@@ -480,7 +488,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
               cudaStream_t st, Profiler* prof) {
   const int nt = t.n_tile;
   const DftGeom f1 = stage_geom(kFwd1, s, t, nt), f2 = stage_geom(kFwd2, s, t, nt);
-  const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
+  const DftGeom a1 = with_y(stage_geom(kAdj1, s, t, nt), u.y), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   const long long BM = static_cast<long long>(s.B) * s.m();
   float2* msg[2] = {u.msg, u.msg + BM};

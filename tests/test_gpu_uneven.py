@@ -186,3 +186,59 @@ def test_autotuner_times_every_width_and_caches(tmp_path):
     assert set(entry["ms"]) == {str(w) for w in candidates(*A)}
     assert all(t > 0 for t in entry["ms"].values())
     assert entry["ms"][str(best)] == min(entry["ms"].values())
+
+
+D = ((64, 64), (31, 33))
+E = ((128, 64), (45, 37))
+
+
+@pytest.mark.gpu
+def test_odd_sample_counts_in_an_uneven_plan():
+    """Odd M puts scenes at 8-byte (not 16-byte) offsets of the packed
+    samples; each bucket's copy starts aligned, and scene rows with odd
+    strides take the scalar path."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    order = [D, E, D, A]
+    sc = _scenes(order, 2100)
+    eng = UnevenEngine(order, _cfg(), dev)
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    for shape in (D, E):
+        idx = [i for i, s in enumerate(order) if s == shape]
+        ref = FBMEEngine(len(idx), shape[0], shape[1], _cfg(), dev)
+        ref.run(torch.stack([torch.from_numpy(sc[i].y).to(dev) for i in idx]).reshape(len(idx), -1).contiguous())
+        torch.cuda.synchronize()
+        n = shape[0][0] * shape[0][1]
+        for j, i in enumerate(idx):
+            assert torch.equal(eng.out["x"][eng.pix_off[i]:eng.pix_off[i] + n], ref.out["x"][j])
+            assert torch.equal(eng.out["negative_log_evidence"][i], ref.out["negative_log_evidence"][j])
+        ref.close()
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_samples_at_an_8_byte_offset():
+    """A caller's complex64 pointer need only be 8-byte aligned: stages
+    that read y fall back to 8-byte accesses and give the same result."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+
+    dev = torch.device("cuda", 0)
+    sc = _scenes([A, A], 2200)
+    y = torch.stack([torch.from_numpy(s.y).to(dev) for s in sc]).reshape(2, -1).contiguous()
+    buf = torch.zeros(y.numel() + 1, dtype=torch.complex64, device=dev)
+    buf[1:].copy_(y.reshape(-1))
+    view = buf[1:].view(2, -1)
+    assert view.data_ptr() % 16 == 8
+    eng = FBMEEngine(2, A[0], A[1], _cfg(), dev)
+    eng.run(y)
+    torch.cuda.synchronize()
+    x0 = eng.out["x"].clone()
+    eng.run(view)
+    torch.cuda.synchronize()
+    assert torch.equal(eng.out["x"], x0)
+    eng.close()
