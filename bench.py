@@ -49,6 +49,7 @@ def _args() -> argparse.Namespace:
     ap.add_argument("--cpu-sample", type=int, default=32, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain section")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the batched-uneven section")
     return ap.parse_args()
 
 
@@ -112,6 +113,54 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
         "nmse_db": {"plain": n_plain, "learned": n_learned},
         "fallbacks_per_replay": fallbacks,
         "learned_sweeps": 1, "plain_sweeps": 4,
+    }
+
+
+def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
+    """The batched-uneven workload: 64 scenes with grids from {128x128,
+    192x256, 256x256, 384x256}, prefix ratio per axis U[0.3, 0.7],
+    sparsity 1-3 %, SNR U[5, 25] dB (every scene its own shape).  Scenes/s
+    of one captured uneven plan, and of one single-scene plan per scene
+    replayed in turn (the only way to solve such a batch with equal-shape
+    plans); the two give bit-identical results."""
+    import torch
+
+    from fbme_b200 import scenes
+    from fbme_b200.uneven import make_uneven_plan
+    from torch_sbl_fastest_stable import make_stable_plan
+
+    sc = scenes.uneven_batch(0, n_scenes)
+    ys = [torch.from_numpy(s.y).to(device) for s in sc]
+    grids = [s.grid for s in sc]
+
+    def rate(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(device)
+        return n_scenes * reps / (e0.elapsed_time(e1) / 1000.0)
+
+    plan = make_uneven_plan(ys, grids, warmup=1)
+    r_uneven = rate(lambda: plan.replay(), steps)
+    singles = [make_stable_plan(y, g, warmup=1) for y, g in zip(ys, grids)]
+
+    def one_by_one():
+        for q in singles:
+            q.replay()
+
+    r_single = rate(one_by_one, max(2, steps // 10))
+    return {
+        "workload": f"{n_scenes} uneven scenes, grids from {{128x128, 192x256, 256x256, 384x256}}, "
+                    "prefix ratio U[0.3,0.7] per axis, 1-3 % CN(0,1) points, SNR U[5,25] dB",
+        "distinct_shapes": len({(s.grid, s.y.shape) for s in sc}),
+        "uneven_plan_scenes_per_s": r_uneven,
+        "single_scene_plans_scenes_per_s": r_single,
+        "uneven_vs_single_scene_plans": r_uneven / r_single,
     }
 
 
@@ -324,29 +373,42 @@ def run_ours(a: argparse.Namespace) -> None:
     ms = max_over_ranks(e0.elapsed_time(e1))
     value = B * a.steps * world / (ms / 1000.0)
 
-    # end to end through the public API: pinned host y -> replay -> host x
-    x_host = torch.empty((B, *GRID), dtype=torch.complex64).pin_memory()
-    nv_host = torch.empty((B,), dtype=torch.float32).pin_memory()
-    res = plan.result
-    for _ in range(2):
-        plan.input_buffer.copy_(y_host, non_blocking=True)
-        r = plan.replay()
-        x_host.copy_(r.x, non_blocking=True)
-        nv_host.copy_(r.noise_variance, non_blocking=True)
-    barrier()
-    e0.record(stream)
-    for _ in range(a.steps):
-        plan.input_buffer.copy_(y_host, non_blocking=True)
-        r = plan.replay()
-        x_host.copy_(r.x, non_blocking=True)
-        nv_host.copy_(r.noise_variance, non_blocking=True)
-    e1.record(stream)
-    barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e = B * a.steps * world / (e2e_ms / 1000.0)
+    # end to end through the public API (fbme_b200.streaming.HostPipeline):
+    # every step copies its observations from pinned host memory and its
+    # result back to pinned host memory, overlapped with the neighbouring
+    # steps' solves.  Headline: the compact result (active indices and x
+    # values -- x is zero elsewhere -- noise variance, evidence, status);
+    # e2e_dense reads the dense x back instead.
+    from fbme_b200.streaming import HostPipeline
 
-    # quality of this batch (raw NMSE, no gain alignment)
-    x_hat = x_host.numpy().reshape(B, -1)
+    res = plan.result
+
+    def run_pipeline(dense: bool):
+        pipe = HostPipeline(plan, dense=dense)
+        outs = [pipe.host_result(), pipe.host_result()]
+        for i in range(2):
+            pipe.submit(y_host, outs[i % 2])
+        pipe.synchronize()
+        barrier()
+        e0.record(stream)
+        for i in range(a.steps):
+            pipe.submit(y_host, outs[i % 2])
+        pipe.join()
+        e1.record(stream)
+        barrier()
+        t = max_over_ranks(e0.elapsed_time(e1))
+        last = outs[(a.steps - 1) % 2]
+        d2h = sum(getattr(last, f).numel() * getattr(last, f).element_size()
+                  for f in ("noise_variance", "negative_log_evidence", "status", "active_indices",
+                            "active_values", "x") if getattr(last, f) is not None)
+        return B * a.steps * world / (t / 1000.0), last, d2h
+
+    e2e, host_res, e2e_d2h = run_pipeline(False)
+    e2e_dense, _, e2e_dense_d2h = run_pipeline(True)
+
+    # quality of this batch (raw NMSE, no gain alignment), from the host result
+    x_hat = host_res.dense_x(GRID).numpy().reshape(B, -1)
+    assert np.array_equal(x_hat, res.x.cpu().numpy().reshape(B, -1))
     num = np.sum(np.abs(x_hat - x_true.reshape(B, -1)) ** 2, axis=1)
     den = np.sum(np.abs(x_true.reshape(B, -1)) ** 2, axis=1)
     nmse_db = float(10.0 * np.log10(np.mean(num / den)))
@@ -373,6 +435,9 @@ def run_ours(a: argparse.Namespace) -> None:
     learned = None
     if world == 1 and not a.no_learned:
         learned = learned_section(device, min(a.steps, 20))
+    uneven = None
+    if world == 1 and not a.no_uneven:
+        uneven = uneven_section(device, min(a.steps, 20))
 
     if rank == 0:
         line = {
@@ -387,7 +452,11 @@ def run_ours(a: argparse.Namespace) -> None:
                 "nmse_db": nmse_db, "scenes_with_status": status_bad,
             },
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(y_host.numel() * 8),
-                    "d2h_bytes_per_step": int(x_host.numel() * 8 + nv_host.numel() * 4)},
+                    "d2h_bytes_per_step": int(e2e_d2h),
+                    "api": "fbme_b200.streaming.HostPipeline (pinned host batches, copies overlapped with "
+                           "the neighbouring solves); result: active indices + x values (x is zero "
+                           "elsewhere), noise variance, evidence, status",
+                    "dense": {"value": e2e_dense, "d2h_bytes_per_step": int(e2e_dense_d2h)}},
             "roofline": {
                 "bound": "hbm", "kernel": dom_name,
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -406,6 +475,8 @@ def run_ours(a: argparse.Namespace) -> None:
             line["cpu_baseline"] = cpu
         if learned is not None:
             line["learned"] = learned
+        if uneven is not None:
+            line["uneven"] = uneven
         print(json.dumps(line), flush=True)
     del plan
     if dist is not None:

@@ -85,6 +85,7 @@ class FbmeOutputs(ctypes.Structure):
         ("fixed_budget_monotone", c_void_p),
         ("support_score_threshold", c_void_p),
         ("active_indices", c_void_p),
+        ("active_values", c_void_p),
         ("status", c_void_p),
     ]
 

@@ -193,7 +193,7 @@ struct SceneMap {
 
 // Bucket-order staging of an uneven plan (workspace offsets).
 struct Staging {
-  size_t map, y, x, var, prec, mask, noise, dof, nle, trace, exch, fbg, fbn, fbd, fbm, thr, active, status;
+  size_t map, y, x, var, prec, mask, noise, dof, nle, trace, exch, fbg, fbn, fbd, fbm, thr, active, aval, status;
   size_t total;
 };
 
@@ -333,6 +333,7 @@ int plan_spec(const FbmeShape* shapes, int n, const FbmeConfig* c, const FbmeSha
     S.fbm = take(B);
     S.thr = take(B * 4);
     S.active = take(B * K * 8);
+    S.aval = take(B * K * 8);
     S.status = take(B * 4);
     S.total = off;
   }
@@ -420,7 +421,7 @@ struct ScatterField {
   int elem_bytes;  // 1, 4 or 8
   int count;       // 0 = one element per pixel
 };
-constexpr int kScatterFields = 16;
+constexpr int kScatterFields = 20;
 struct ScatterArgs {
   ScatterField f[kScatterFields];
   int n;
@@ -500,6 +501,7 @@ FbmeOutputs bucket_outputs(const FbmePlan* P, const Bucket& k, const FbmeOutputs
   o.support_score_threshold =
       caller.support_score_threshold ? reinterpret_cast<float*>(at(S.thr, f, 4)) : nullptr;
   o.active_indices = caller.active_indices ? reinterpret_cast<int64_t*>(at(S.active, f * K, 8)) : nullptr;
+  o.active_values = caller.active_values ? at(S.aval, f * K, 8) : nullptr;
   o.status = reinterpret_cast<int32_t*>(at(S.status, f, 4));
   return o;
 }
@@ -532,6 +534,7 @@ ScatterArgs scatter_args(const FbmePlan* P, const FbmeOutputs& c) {
   add(S.fbm, c.fixed_budget_monotone, 1, 1, fb);
   add(S.thr, c.support_score_threshold, 4, 1, mask);
   add(S.active, c.active_indices, 8, K);
+  add(S.aval, c.active_values, 8, K);
   add(S.status, c.status, 4, 1);
   return a;
 }

@@ -662,6 +662,7 @@ __global__ void __launch_bounds__(32) output_scatter_kernel(PolishArgs A, FbmeOu
   const float pv = ps->best_pv[lane];
   const long long e = scene * N + idx;
   reinterpret_cast<float2*>(out.x)[e] = mu;
+  if (out.active_values) reinterpret_cast<float2*>(out.active_values)[scene * K + lane] = mu;
   out.posterior_variance[e] = pv;
   out.precision[e] = 1.0f / ps->best_gamma[lane];
   if (out.support_mask && A.c.false_alarm > 0.f) {

@@ -120,6 +120,7 @@ class UnevenEngine:
             "fixed_budget_monotone": torch.zeros(B, dtype=torch.bool, device=device),
             "support_score_threshold": torch.zeros(B, **f32),
             "active_indices": torch.zeros(B, K, dtype=torch.int64, device=device),
+            "active_values": torch.zeros(B, K, dtype=torch.complex64, device=device),
             "status": torch.zeros(B, dtype=torch.int32, device=device),
         }
         o = nat.FbmeOutputs()

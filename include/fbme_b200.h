@@ -107,6 +107,10 @@ typedef struct {
   uint8_t* fixed_budget_monotone;          /* [B], optional */
   float* support_score_threshold;          /* [B], optional */
   int64_t* active_indices;                 /* [B,K], optional */
+  void* active_values;                     /* [B,K] complex64, optional: x at
+                                              active_indices (x is zero
+                                              elsewhere, so the pair is the
+                                              whole reconstruction) */
   int32_t* status;                         /* [B] */
 } FbmeOutputs;
 
