@@ -116,6 +116,44 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
     }
 
 
+# Published single-scene replay latencies of the reference (RTX 4090, 40x32
+# grid, 20x16 prefix, 21 targets, 10 dB; device P50 over 20 repeats of
+# resident input copy + warm solve): FBME-Fast 0.6415 ms, FBME-Stable
+# 1.0988 ms.
+PUBLISHED_MS = {"fast": 0.6415, "stable": 1.0988}
+
+
+def published_shape_section(device, repeats: int = 20) -> dict:
+    """The same protocol on the B200 with a seeded synthetic scene of the
+    archived shape (its generator and arrays were not released): device
+    P50 and max over `repeats` replays, each timed with CUDA events around
+    the resident input copy and the replay."""
+    import torch
+
+    from fbme_b200 import scenes
+    from torch_sbl_fastest_stable import make_fastest_plan, make_stable_plan
+
+    sc = scenes.point_scene((40, 32), (20, 16), 21, 10.0, 200, "cn")
+    y = torch.from_numpy(sc.y).to(device)
+    out = {"workload": "one 40x32 / 20x16 scene, 21 CN(0,1) points, 10 dB, seed 200"}
+    for name, make in (("fast", make_fastest_plan), ("stable", make_stable_plan)):
+        plan = make(y, (40, 32), warmup=3)
+        times = []
+        for _ in range(repeats + 3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan.replay(y)
+            e1.record()
+            torch.cuda.synchronize(device)
+            times.append(e0.elapsed_time(e1))
+        t = sorted(times[3:])
+        p50 = 0.5 * (t[len(t) // 2 - 1] + t[len(t) // 2])
+        out[name] = {"device_p50_ms": p50, "device_max_ms": t[-1],
+                     "published_rtx4090_p50_ms": PUBLISHED_MS[name],
+                     "speedup_vs_published": PUBLISHED_MS[name] / p50}
+    return out
+
+
 def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
     """The batched-uneven workload: 64 scenes with grids from {128x128,
     192x256, 256x256, 384x256}, prefix ratio per axis U[0.3, 0.7],
@@ -299,15 +337,18 @@ def scene_bytes(n: int, m: int, t_u: int, p: int) -> int:
     return (t_u + 1) * (32 * n + 24 * m) + 8 * m + 8 * n + 12 * n + p * 8 * m + 17 * n
 
 
+# DRAM bytes per scene of one launch, from one ncu capture (128 scenes of
+# 256x256 / 128x128; profiles/adjoint2_denoise_256x256_b128.md):
+# dram__bytes_read.sum + dram__bytes_write.sum = 168.4 + 78.2 MB.  Traffic
+# grows in proportion to the scenes of a launch.
+TRAFFIC_PER_SCENE = {"adjoint_denoise": (168.4e6 + 78.2e6) / 128}
+
+
 def _traffic(group: str, batch: int):
-    """Measured DRAM bytes per launch for ``group`` from the committed ncu
-    summary (per-scene figure scaled by the batch), or None."""
-    p = REPO / "profiles" / "traffic_per_scene.json"
-    if not p.exists():
-        return None
-    d = json.loads(p.read_text())
-    v = d.get(group)
-    return None if v is None else float(v) * batch
+    """Measured DRAM bytes per launch for ``group`` (per-scene figure of the
+    capture scaled by the batch), or None where no capture exists."""
+    v = TRAFFIC_PER_SCENE.get(group)
+    return None if v is None else v * batch
 
 
 # ---------------------------------------------------------------- our arm
@@ -438,6 +479,7 @@ def run_ours(a: argparse.Namespace) -> None:
     uneven = None
     if world == 1 and not a.no_uneven:
         uneven = uneven_section(device, min(a.steps, 20))
+    published = published_shape_section(device) if world == 1 and not a.no_uneven else None
 
     if rank == 0:
         line = {
@@ -477,6 +519,8 @@ def run_ours(a: argparse.Namespace) -> None:
             line["learned"] = learned
         if uneven is not None:
             line["uneven"] = uneven
+        if published is not None:
+            line["published_shape"] = published
         print(json.dumps(line), flush=True)
     del plan
     if dist is not None:
