@@ -87,14 +87,18 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   const BatchShape& s = A.s;
   const bool on = lane < K;
   const int n1i = my_idx / s.n2, n2i = my_idx % s.n2;
+  // One reciprocal per scale, reused by multiplication: a division here is
+  // a full IEEE sequence with a slow-path branch, on the critical path of
+  // a single warp.
+  const float inv_nu = 1.0f / nu, inv_g = 1.0f / my_gamma;
   // system S = diag(1/gamma) + G / nu, Hermitian-symmetrised
 #pragma unroll
   for (int j = 0; j < kMaxPolish; ++j) {
-    const int idx_j = __shfl_sync(0xffffffffu, my_idx, j);
+    const int n1j = __shfl_sync(0xffffffffu, n1i, j), n2j = __shfl_sync(0xffffffffu, n2i, j);
     if (on && j < K) {
-      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, idx_j / s.n2, idx_j % s.n2);
-      float2 a = make_float2(g.x / nu, g.y / nu);
-      if (j == lane) a.x += 1.0f / my_gamma;
+      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, n1j, n2j);
+      float2 a = make_float2(g.x * inv_nu, g.y * inv_nu);
+      if (j == lane) a.x += inv_g;
       M[lane][j] = a;
     }
   }
@@ -112,14 +116,16 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
     if (on && j < K) M[lane][j] = row[j];
   __syncwarp();
   const float dscale = on ? sqrtf(fmaxf(M[lane][lane].x, kTinyP)) : 1.0f;
-  // equilibrate: E[i][j] = S[i][j] / d_i / d_j, symmetrise again
+  const float inv_d = 1.0f / dscale;
+  // equilibrate: E[i][j] = S[i][j] / (d_i d_j), symmetrise again
   {
 #pragma unroll
     for (int j = 0; j < kMaxPolish; ++j) {
-      const float dj = __shfl_sync(0xffffffffu, dscale, j);
+      const float idj = __shfl_sync(0xffffffffu, inv_d, j);
       if (on && j < K) {
         const float2 a = M[lane][j];
-        row[j] = make_float2(a.x / dscale / dj, a.y / dscale / dj);
+        const float f = inv_d * idj;
+        row[j] = make_float2(a.x * f, a.y * f);
       }
     }
     __syncwarp();
@@ -146,37 +152,53 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   const float jitter = A.c.jitter * (kEpsP * scale);
   if (on) M[lane][lane].x += jitter;
   __syncwarp();
-  // Cholesky, lower, in place
+  // Cholesky, lower, in place, right-looking: once column q is final,
+  // lane i > q subtracts L[i][q] conj(L[k][q]) from its row entries k in
+  // (q, i] -- independent updates instead of one dot-product chain per
+  // entry.  Every entry receives its terms in the same order q = 0, 1, ...
+  // as the dot-product form.
+  // Each lane touches only its own row inside the loop; the pivot and the
+  // column entries L[k][q] reach the other lanes by shuffles.
   int status = 0;
-  for (int j = 0; j < K; ++j) {
-    if (lane == j) {
-      float sdiag = M[j][j].x;
-      for (int q = 0; q < j; ++q) sdiag -= abs2(M[j][q]);
+  __syncwarp();
+  for (int q = 0; q < K; ++q) {
+    float piv = 0.f;
+    if (lane == q) {
+      float sdiag = M[q][q].x;
       if (!(sdiag > 0.f)) {
         status |= isfinite(sdiag) ? FBME_STATUS_CHOLESKY : FBME_STATUS_NONFINITE;
         sdiag = kTinyP;
       }
-      M[j][j] = make_float2(sqrtf(sdiag), 0.f);
+      piv = sqrtf(sdiag);
+      M[q][q] = make_float2(piv, 0.f);
     }
-    __syncwarp();
-    const float ljj = M[j][j].x;
-    if (on && lane > j) {
-      float2 v = M[lane][j];
-      for (int q = 0; q < j; ++q) {
-        const float2 a = M[lane][q], b = M[j][q];
-        v.x -= a.x * b.x + a.y * b.y;  // a * conj(b)
-        v.y -= a.y * b.x - a.x * b.y;
+    const float rq = 1.0f / __shfl_sync(0xffffffffu, piv, q);
+    float2 a = make_float2(0.f, 0.f);
+    if (on && lane > q) {
+      const float2 v = M[lane][q];
+      a = make_float2(v.x * rq, v.y * rq);
+      M[lane][q] = a;
+    }
+#pragma unroll 4
+    for (int k = q + 1; k < K; ++k) {
+      const float bx = __shfl_sync(0xffffffffu, a.x, k), by = __shfl_sync(0xffffffffu, a.y, k);
+      if (on && k < lane) {
+        float2 v = M[lane][k];
+        v.x -= a.x * bx + a.y * by;  // a * conj(b)
+        v.y -= a.y * bx - a.x * by;
+        M[lane][k] = v;
       }
-      M[lane][j] = make_float2(v.x / ljj, v.y / ljj);
     }
-    __syncwarp();
+    if (on && lane > q) M[lane][lane].x -= abs2(a);
   }
+  __syncwarp();
   status = __reduce_or_sync(0xffffffffu, status);
   // mean: L z = c / nu / d, L^H w = z, mu = w / d
-  const float2 rhs = on ? make_float2(my_c.x / nu, my_c.y / nu) : make_float2(0.f, 0.f);
-  float2 z = make_float2(rhs.x / dscale, rhs.y / dscale);
+  const float rl = on ? 1.0f / M[lane][lane].x : 1.0f;  // 1 / L[lane][lane]
+  const float2 rhs = on ? make_float2(my_c.x * inv_nu, my_c.y * inv_nu) : make_float2(0.f, 0.f);
+  float2 z = make_float2(rhs.x * inv_d, rhs.y * inv_d);
   for (int q = 0; q < K; ++q) {
-    if (lane == q) z = make_float2(z.x / M[q][q].x, z.y / M[q][q].x);
+    if (lane == q) z = make_float2(z.x * rl, z.y * rl);
     const float2 zq = make_float2(__shfl_sync(0xffffffffu, z.x, q), __shfl_sync(0xffffffffu, z.y, q));
     if (on && lane > q) {
       const float2 l = M[lane][q];
@@ -186,7 +208,7 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   }
   float2 w = z;
   for (int q = K - 1; q >= 0; --q) {
-    if (lane == q) w = make_float2(w.x / M[q][q].x, w.y / M[q][q].x);
+    if (lane == q) w = make_float2(w.x * rl, w.y * rl);
     const float2 wq = make_float2(__shfl_sync(0xffffffffu, w.x, q), __shfl_sync(0xffffffffu, w.y, q));
     if (on && lane < q) {
       const float2 l = M[q][lane];  // conj(L[q][lane]) * wq
@@ -195,30 +217,44 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
     }
   }
   EvalOut o;
-  o.mean = make_float2(w.x / dscale, w.y / dscale);
-  // inverse factor column `lane`: X = L^{-1}, eq_var = sum_i |X[i][lane]|^2
+  o.mean = make_float2(w.x * inv_d, w.y * inv_d);
+  // inverse factor column `lane`: X = L^{-1}, eq_var = sum_i |X[i][lane]|^2.
+  // Right-looking: when X[q][lane] is final, its contribution L[i][q] X[q]
+  // is added to the accumulators of every row i > q (held in X until row
+  // i is final) -- the same terms in the same order as the dot-product
+  // form, without its dependency chain.
   float eqv = 0.f;
-  if (on) {
-    for (int i = 0; i < K; ++i) X[i][lane] = make_float2(0.f, 0.f);
-    const float2 xt = make_float2(1.0f / M[lane][lane].x, 0.f);
-    X[lane][lane] = xt;
-    eqv = abs2(xt);
-    for (int i = lane + 1; i < K; ++i) {
-      float2 acc = make_float2(0.f, 0.f);
-      for (int q = lane; q < i; ++q) {
-        const float2 l = M[i][q], x = X[q][lane];
-        acc.x += l.x * x.x - l.y * x.y;
-        acc.y += l.x * x.y + l.y * x.x;
+  {
+    const float2(*__restrict__ L)[33] = M;
+    float2(*__restrict__ Xc)[33] = X;
+    if (on)
+      for (int i = 0; i < K; ++i) Xc[i][lane] = make_float2(0.f, 0.f);
+    for (int q = 0; q < K; ++q) {
+      const float rlq = __shfl_sync(0xffffffffu, rl, q);
+      if (on && lane <= q) {
+        float2 xq;
+        if (lane == q) {
+          xq = make_float2(rlq, 0.f);
+        } else {
+          const float2 acc = Xc[q][lane];
+          xq = make_float2(-acc.x * rlq, -acc.y * rlq);
+        }
+        Xc[q][lane] = xq;
+        eqv += abs2(xq);
+#pragma unroll 4
+        for (int i = q + 1; i < K; ++i) {
+          const float2 l = L[i][q];
+          float2 acc = Xc[i][lane];
+          acc.x += l.x * xq.x - l.y * xq.y;
+          acc.y += l.x * xq.y + l.y * xq.x;
+          Xc[i][lane] = acc;
+        }
       }
-      const float lii = M[i][i].x;
-      const float2 xi = make_float2(-acc.x / lii, -acc.y / lii);
-      X[i][lane] = xi;
-      eqv += abs2(xi);
     }
   }
   __syncwarp();
-  o.pv = on ? fmaxf(eqv / (dscale * dscale), 0.f) : 0.f;
-  o.dd = on ? fmaxf((my_gamma - o.pv) / (my_gamma * my_gamma), 0.f) : 0.f;
+  o.pv = on ? fmaxf(eqv * (inv_d * inv_d), 0.f) : 0.f;
+  o.dd = on ? fmaxf((my_gamma - o.pv) * (inv_g * inv_g), 0.f) : 0.f;
   // evidence (FP64 accumulation)
   double ld = 0.0, lg = 0.0, qd = 0.0;
   if (on) {
@@ -249,10 +285,10 @@ FBME_DEV double residual_energy(const PolishArgs& A, const float2* d1, const flo
     const int n1i = my_idx / s.n2, n2i = my_idx % s.n2;
     double gr = 0.0, gi = 0.0;  // (G mu)_i
     for (int j = 0; j < K; ++j) {
-      const int idx_j = __shfl_sync(__activemask(), my_idx, j);
+      const int n1j = __shfl_sync(__activemask(), n1i, j), n2j = __shfl_sync(__activemask(), n2i, j);
       const float mjx = __shfl_sync(__activemask(), my_mu.x, j);
       const float mjy = __shfl_sync(__activemask(), my_mu.y, j);
-      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, idx_j / s.n2, idx_j % s.n2);
+      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, n1j, n2j);
       gr += static_cast<double>(g.x) * mjx - static_cast<double>(g.y) * mjy;
       gi += static_cast<double>(g.x) * mjy + static_cast<double>(g.y) * mjx;
     }
