@@ -355,11 +355,11 @@ def scene_bytes(n: int, m: int, t_u: int, p: int) -> int:
     return (t_u + 1) * (32 * n + 24 * m) + 8 * m + 8 * n + 12 * n + p * 8 * m + 17 * n
 
 
-# DRAM bytes per scene of one launch, from one ncu capture (128 scenes of
-# 256x256 / 128x128; profiles/adjoint2_denoise_256x256_b128.md):
-# dram__bytes_read.sum + dram__bytes_write.sum = 168.4 + 78.2 MB.  Traffic
-# grows in proportion to the scenes of a launch.
-TRAFFIC_PER_SCENE = {"adjoint_denoise": (168.4e6 + 78.2e6) / 128}
+# DRAM bytes per scene of one launch, from one ncu capture of 128 scenes of
+# 256x256 / 128x128 (dram__bytes_read.sum + dram__bytes_write.sum, in
+# the profiles/ summary of the kernel).  Traffic grows in proportion to
+# the scenes of a launch.
+TRAFFIC_PER_SCENE = {"adjoint_denoise": (201.48e6 + 85.42e6) / 128}
 
 
 def _traffic(group: str, batch: int):

@@ -33,7 +33,7 @@ int default_n_tile(int terms) { return terms == 6 ? 128 : 256; }
 
 struct Layout {
   size_t tab_f2, tab_f1, tab_a2, tab_a1, dir1, dir2;
-  size_t mu, bp, var, gamma, msg, pred, tmp, keys, part, scal;
+  size_t mu, bp, var, gamma, msg, pred, tmp, lift, keys, part, scal;
   size_t active, score, pstate, xval, xidx, status, ckey, cidx;
   size_t total;
 };
@@ -68,6 +68,7 @@ Layout make_layout(const fbme::BatchShape& s, const FbmeConfig& c, int nt) {
   L.pred = take(B * M * sizeof(float2));
   const size_t tmp1 = static_cast<size_t>(s.m2) * s.n1, tmp2 = static_cast<size_t>(s.n2) * s.m1;
   L.tmp = take(B * (tmp1 > tmp2 ? tmp1 : tmp2) * sizeof(float2));
+  L.lift = take(B * N * sizeof(float2));
   L.keys = take(B * N * sizeof(uint32_t));
   L.part = take(B * fbme::kMaxTilesPerScene * fbme::kPartSlots * sizeof(double));
   L.scal = take(10 * B * sizeof(float));
@@ -375,6 +376,7 @@ void bind_bucket(Bucket& k, uint8_t* ws, cudaStream_t st) {
   u.msg = reinterpret_cast<float2*>(w + L.msg);
   u.pred = reinterpret_cast<float2*>(w + L.pred);
   u.tmp = reinterpret_cast<float2*>(w + L.tmp);
+  u.lift = reinterpret_cast<float2*>(w + L.lift);
   u.var = reinterpret_cast<float*>(w + L.var);
   u.gamma = reinterpret_cast<float*>(w + L.gamma);
   u.part = reinterpret_cast<double*>(w + L.part);
@@ -809,7 +811,7 @@ int fbme_plan_replay(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme
 const char* fbme_profile_group_name(int32_t group) {
   static const char* names[FBME_NUM_GROUPS] = {
       "init", "adjoint_message", "adjoint_denoise", "forward_1", "forward_residual", "scalars",
-      "sweep1_denoise", "topk", "polish", "exchange_score", "output"};
+      "sweep1_denoise", "topk", "polish", "exchange_score", "output", "adjoint_2"};
   return (group >= 0 && group < FBME_NUM_GROUPS) ? names[group] : "";
 }
 

@@ -99,6 +99,7 @@ struct DftTables {
 struct UampBuffers {
   const float2* y;
   float2 *mu, *bp, *msg, *pred, *tmp;
+  float2* lift;  // [B][N] adjoint output A^H m (the denoiser's input)
   float *var, *gamma;
   double* part;  // [B][kMaxTilesPerScene][kPartSlots]
   uint32_t* keys;  // [B][N] order-preserving score keys (final E-step)

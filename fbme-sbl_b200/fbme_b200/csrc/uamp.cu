@@ -220,57 +220,6 @@ FBME_DEV DenoiseOut denoise_math(const DenoiseArgs& a, float prior, float2 om, f
   return o;
 }
 
-struct EpiDenoise {
-  using Pre = NoPre;  // loads are issued inside consume (measured faster than prefetching)
-  DenoiseArgs a;
-  float dof_acc, var_acc;
-  FBME_DEV void prefetch(const TileCtx&, int, int, Pre&) const {}
-  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v, const Pre&) {
-    const DftGeom& g = *t.g;
-    const int r = t.row0() + row;
-    if (r >= g.rows) return;
-    const float pv = a.pv[t.scene], fl = a.floor_[t.scene];
-    const long long sb = t.scene * g.out_stride;
-    float2* mu = a.mu + sb;
-    float* var = a.var + sb;
-    float* gam = a.gamma + sb;
-    const int jb = t.col0() + (c0 >> 1);
-    const int ld = g.out_ld;
-    // all loads of the chunk first (independent addresses, in flight together)
-    float pri[8], ov[8];
-    float2 om[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      if (jb + i < g.cols) {
-        const int e = (jb + i) * ld + r;
-        pri[i] = gam[e];
-        om[i] = mu[e];
-        ov[i] = var[e];
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      if (jb + i < g.cols) {
-        const int e = (jb + i) * ld + r;
-        const DenoiseOut o =
-            denoise_math(a, pri[i], om[i], ov[i], make_float2(v[2 * i], v[2 * i + 1]), pv, fl);
-        mu[e] = o.mean;
-        var[e] = o.variance;
-        if (a.update_prior) gam[e] = o.gamma;
-        if (a.keys) a.keys[sb + e] = float_key(abs_sq(o.mean) + o.variance);
-        dof_acc += o.rel;
-        var_acc += o.variance;
-      }
-    }
-  }
-  FBME_DEV void tile_done(const TileCtx& t, int w, int lane) {
-    warp_partial(dof_acc, a.part, t, 0, w, lane);
-    warp_partial(var_acc, a.part, t, 1, w, lane);
-    dof_acc = 0.f;
-    var_acc = 0.f;
-  }
-};
-
 // ---------------------------------------------------------------------------
 // elementwise kernels
 // ---------------------------------------------------------------------------
@@ -301,6 +250,58 @@ __global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevCon
     acc += g;
   }
   write_block_partial(acc, red, part, scene, blockIdx.x, 0 * kPartWarps);
+}
+
+// Denoiser of sweeps 2..T_u and of the final E-step, on the adjoint output
+// A^H m that adjoint stage 2 stored (`lift`): the epilogue of that stage
+// runs one CTA per SM, too few warps to keep the denoiser's loads in
+// flight, while this kernel runs at full occupancy.  Per-block DOF and
+// variance sums go to partial slots 0 and 1, as sweep1_kernel's.
+__global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, DenoiseArgs a, const float2* lift) {
+  __shared__ double red[32];
+  const int scene = blockIdx.y;
+  const long long n = s.n();
+  const float pv = a.pv[scene], fl = a.floor_[scene];
+  float dof = 0.f, sv = 0.f;
+  auto one = [&](long long e, float g, float2 m, float v, float2 l) {
+    const DenoiseOut o = denoise_math(a, g, m, v, l, pv, fl);
+    dof += o.rel;
+    sv += o.variance;
+    return o;
+  };
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long first = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if ((n & 1) == 0) {
+    // two coefficients per step: 16-byte accesses to mu and the lift, 8-byte
+    // to the variances (scene offsets are even, so every access is aligned)
+    const long long base = scene * n;
+    for (long long j = first; j < n / 2; j += stride) {
+      const long long e = base + 2 * j;
+      const float4 m = *reinterpret_cast<const float4*>(a.mu + e);
+      const float4 l = __ldg(reinterpret_cast<const float4*>(lift + e));
+      const float2 v = *reinterpret_cast<const float2*>(a.var + e);
+      const float2 g = *reinterpret_cast<const float2*>(a.gamma + e);
+      const DenoiseOut o0 = one(e, g.x, make_float2(m.x, m.y), v.x, make_float2(l.x, l.y));
+      const DenoiseOut o1 = one(e + 1, g.y, make_float2(m.z, m.w), v.y, make_float2(l.z, l.w));
+      *reinterpret_cast<float4*>(a.mu + e) = make_float4(o0.mean.x, o0.mean.y, o1.mean.x, o1.mean.y);
+      *reinterpret_cast<float2*>(a.var + e) = make_float2(o0.variance, o1.variance);
+      if (a.update_prior) *reinterpret_cast<float2*>(a.gamma + e) = make_float2(o0.gamma, o1.gamma);
+      if (a.keys)
+        *reinterpret_cast<uint2*>(a.keys + e) = make_uint2(float_key(abs_sq(o0.mean) + o0.variance),
+                                                           float_key(abs_sq(o1.mean) + o1.variance));
+    }
+  } else {
+    for (long long i = first; i < n; i += stride) {
+      const long long e = scene * n + i;
+      const DenoiseOut o = one(e, a.gamma[e], a.mu[e], a.var[e], lift[e]);
+      a.mu[e] = o.mean;
+      a.var[e] = o.variance;
+      if (a.update_prior) a.gamma[e] = o.gamma;
+      if (a.keys) a.keys[e] = float_key(abs_sq(o.mean) + o.variance);
+    }
+  }
+  write_block_partial(dof, red, a.part, scene, blockIdx.x, 0 * kPartWarps);
+  write_block_partial(sv, red, a.part, scene, blockIdx.x, 1 * kPartWarps);
 }
 
 // First sweep: the lifted message is (1-d)/(dv+nv) * A^H y, the previous
@@ -427,7 +428,6 @@ cudaError_t set_dft_attributes() {
   if ((e = set_attr_both<ProMessage, EpiStoreT>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProPlain, EpiPredict>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProPlain, EpiBackprojection>()) != cudaSuccess) return e;
-  if ((e = set_attr_both<ProPlain, EpiDenoise>()) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
@@ -537,9 +537,11 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                                       c.uamp_damping},
                            EpiStoreT{u.tmp}, u.status, st));
       cur ^= 1;
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2,
+                 run_stage(c.terms, a2, ProPlain{u.tmp}, EpiStoreT{u.lift}, u.status, st));
       FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
-                 run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st));
-      src_dof = PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps};
+                 (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
+      src_dof = PartSrc{bn, 1};
     }
     FBME_TIMED(prof, FBME_GROUP_FWD_1,
                run_stage(c.terms, f1, ProPlain{u.mu}, EpiStoreT{u.tmp}, u.status, st));
@@ -560,8 +562,9 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                        EpiStoreT{u.tmp}, u.status, st));
   da.update_prior = 0;
   da.keys = reinterpret_cast<uint32_t*>(u.keys);
-  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
-             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiDenoise{da, 0.f, 0.f}, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2,
+             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiStoreT{u.lift}, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
 }
 
 }  // namespace fbme
