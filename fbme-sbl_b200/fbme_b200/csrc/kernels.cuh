@@ -111,6 +111,7 @@ struct UampBuffers {
 };
 
 cudaError_t set_dft_attributes();
+cudaError_t set_polish_attributes();
 void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
                  float2* data, float2* tmp, int* status, cudaStream_t st);
 void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,

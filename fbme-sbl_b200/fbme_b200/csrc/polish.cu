@@ -520,7 +520,24 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
   const int N1 = s.n1, N2 = s.n2;
   const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
   float2* d2 = ex_shm;
+  float2* bps = ex_shm + N2;  // [kExRows][N2]: this CTA's rows of A^H y
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
+  {
+    // A^H y rows, asynchronous copies in flight during the set-up and the
+    // MAC loop: 16-byte chunks when N2 is even (every row then starts on a
+    // 16-byte boundary), else one 8-byte element each
+    const float2* src = A.p.bp + scene * s.n() + static_cast<long long>(r0) * N2;
+    const int rows = min(kExRows, N1 - r0);
+    if ((N2 & 1) == 0) {
+      for (int c = threadIdx.x; c < rows * N2 / 2; c += blockDim.x)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(bps + 2 * c)), "l"(src + 2 * c)
+                     : "memory");
+    } else {
+      for (int c = threadIdx.x; c < rows * N2; c += blockDim.x)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(bps + c)), "l"(src + c) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   for (int i = threadIdx.x; i < N2; i += blockDim.x) d2[i] = A.p.dir2[i];
   for (int i = threadIdx.x; i < kExRows * 16; i += blockDim.x) (&excl[0][0])[i] = 0u;
   __syncthreads();
@@ -567,7 +584,8 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
       }
     }
   }
-  const float2* bp = A.p.bp + scene * s.n();
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
   uint32_t key[4 * CT];
   int gidx[4 * CT];
   bool valid[4 * CT];
@@ -582,14 +600,15 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
       gidx[i] = n1 * N2 + n2;
       key[i] = 0u;
       if (valid[i]) {
-        const float2 bv = bp[gidx[i]];
+        const float2 bv = bps[lr * N2 + n2];
         const float2 r = make_float2(bv.x - acc[ri][c].x, bv.y - acc[ri][c].y);
         const bool act = (excl[lr][n2 >> 5] >> (n2 & 31)) & 1u;
         key[i] = act ? 0u : float_key_t(abs_sq(r));
       }
     }
   const size_t off = (static_cast<size_t>(scene) * gridDim.x + blockIdx.x) * E;
-  block_topk(key, gidx, valid, E, S, cand_key + off, cand_idx + off);
+  // residual scores of one CTA crowd into few top-byte bins
+  block_topk<4 * CT, true>(key, gidx, valid, E, S, cand_key + off, cand_idx + off);
 }
 
 // Final K-space outputs, fixed-budget diagnostics, effective DOF
@@ -714,6 +733,18 @@ void launch_topk_merge(const uint32_t* cand_key, const int* cand_idx, int ncand,
 
 int exchange_blocks(const BatchShape& s) { return (s.n1 + kExRows - 1) / kExRows; }
 
+// Dynamic shared memory of the exchange kernel: D2 and the CTA's rows of
+// A^H y.
+static size_t exchange_smem_bytes(int n2) { return static_cast<size_t>(1 + kExRows) * n2 * sizeof(float2); }
+
+cudaError_t set_polish_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(exchange_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(exchange_smem_bytes(256)));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(exchange_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(exchange_smem_bytes(512)));
+}
+
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof) {
   PolishArgs A{s, c, p};
@@ -724,7 +755,7 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 0)));
   if (c.exchange > 0 && c.polish_iters > 1) {
     const int nb = exchange_blocks(s);
-    const size_t shm = s.n2 * sizeof(float2);
+    const size_t shm = exchange_smem_bytes(s.n2);
     const dim3 grid(nb, s.B);
     if (s.n2 <= 256)
       FBME_TIMED(prof, FBME_GROUP_EXCHANGE,

@@ -32,7 +32,9 @@ struct TopkShared {
 // thread.  Radix select with 8-bit digits finds the k-th largest key T;
 // keys above T are all taken; among keys equal to T the lowest indices are
 // taken.  Writes k winners, sorted (key desc, index asc), to out_key/out_idx.
-template <int KPT>
+// AGG: warp-aggregated histogram atomics (lanes whose keys share a bin add
+// once); pays where the keys crowd into few bins, costs where they spread.
+template <int KPT, bool AGG = false>
 FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], const bool (&valid)[KPT],
                          int k, TopkShared& S, uint32_t* out_key, int* out_idx) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -72,8 +74,19 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
     __syncthreads();
     const uint32_t prefix = S.prefix, mask = S.mask;
 #pragma unroll
-    for (int i = 0; i < KPT; ++i)
-      if (valid[i] && (key[i] & mask) == prefix) atomicAdd(&S.hist[(key[i] >> shift) & 255u], 1u);
+    for (int i = 0; i < KPT; ++i) {
+      const bool part = valid[i] && (key[i] & mask) == prefix;
+      if constexpr (AGG) {
+        const unsigned act = __ballot_sync(0xffffffffu, part);
+        if (part) {
+          const uint32_t bin = (key[i] >> shift) & 255u;
+          const unsigned peers = __match_any_sync(act, bin);
+          if (__ffs(peers) - 1 == lane) atomicAdd(&S.hist[bin], static_cast<uint32_t>(__popc(peers)));
+        }
+      } else if (part) {
+        atomicAdd(&S.hist[(key[i] >> shift) & 255u], 1u);
+      }
+    }
     __syncthreads();
     if (warp == 0) {
       const int hi = 256 - 8 * lane;  // lane owns bins [hi-8, hi), counted from the top
