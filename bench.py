@@ -59,6 +59,29 @@ def _scenes(n: int, seed0: int):
     return [scenes.config_scene("c2", seed0 + i) for i in range(n)]
 
 
+# ---------------------------------------------------------------- ranks
+def shard_seeds(rank: int, batch: int) -> range:
+    """Scene seeds of one rank: ranks solve disjoint scenes (weak scaling,
+    no data-path collective)."""
+    return range(rank * batch, (rank + 1) * batch)
+
+
+def max_over_ranks(v: float, dist=None, device=None) -> float:
+    """The job's time: the maximum of the ranks' device times."""
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(scenes_per_rank: int, steps: int, world: int, job_ms: float) -> float:
+    """Whole-job scenes/s: every rank's scenes over the slowest rank's time."""
+    return scenes_per_rank * steps * world / (job_ms / 1000.0)
+
+
 def learned_section(device, steps: int, batch: int = 256) -> dict:
     """Plain vs learned+batched FBME on held-out scenes of the learned
     distribution (256x256 / 128x128, K ~ U{100..400}, SNR ~ U[5, 25] dB,
@@ -392,7 +415,8 @@ def run_ours(a: argparse.Namespace) -> None:
     from torch_sbl_fastest_stable import make_fastest_plan, make_stable_plan
 
     B = a.batch
-    sc = _scenes(B, rank * B)
+    seeds = shard_seeds(rank, B)
+    sc = _scenes(len(seeds), seeds.start)
     y_np = np.stack([s.y for s in sc])
     x_true = np.stack([s.x for s in sc]).astype(np.complex64)
     y_host = torch.from_numpy(y_np).pin_memory()
@@ -405,12 +429,8 @@ def run_ours(a: argparse.Namespace) -> None:
             dist.barrier()
         torch.cuda.synchronize(device)
 
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def job_ms(v: float) -> float:
+        return max_over_ranks(v, dist, device)
 
     gpu_id = None
     try:
@@ -429,8 +449,8 @@ def run_ours(a: argparse.Namespace) -> None:
     e1.record(stream)
     barrier()
     clk = clocks.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    value = B * a.steps * world / (ms / 1000.0)
+    ms = job_ms(e0.elapsed_time(e1))
+    value = job_rate(B, a.steps, world, ms)
 
     # end to end through the public API (fbme_b200.streaming.HostPipeline):
     # every step copies its observations from pinned host memory and its
@@ -455,12 +475,12 @@ def run_ours(a: argparse.Namespace) -> None:
         pipe.join()
         e1.record(stream)
         barrier()
-        t = max_over_ranks(e0.elapsed_time(e1))
+        t = job_ms(e0.elapsed_time(e1))
         last = outs[(a.steps - 1) % 2]
         d2h = sum(getattr(last, f).numel() * getattr(last, f).element_size()
                   for f in ("noise_variance", "negative_log_evidence", "status", "active_indices",
                             "active_values", "x") if getattr(last, f) is not None)
-        return B * a.steps * world / (t / 1000.0), last, d2h
+        return job_rate(B, a.steps, world, t), last, d2h
 
     e2e, host_res, e2e_d2h = run_pipeline(False)
     e2e_dense, _, e2e_dense_d2h = run_pipeline(True)
