@@ -52,54 +52,6 @@ struct ProYPower {
   }
 };
 
-// UAMP message update fused into the adjoint's operand load
-// (triton_kernels.py:72-84).  Reads the previous message from `msg_in`,
-// writes the new one to `msg_out` (column tile 0 only) and feeds it to the
-// tensor core.
-struct ProMessage {
-  static constexpr int kBatch = 8;
-  static constexpr bool kPipelined = false;
-  struct Frag {
-    float2 y0, y1, p0, p1, m0, m1;
-  };
-  const float2 *y, *pred, *msg_in;
-  float2* msg_out;
-  const float *prec, *dvar;
-  float damping;
-  FBME_DEV void fetch(const TileCtx& t, long long e, int avail, Frag& f) const {
-    if (avail <= 0) {
-      f.y0 = f.y1 = f.p0 = f.p1 = f.m0 = f.m1 = make_float2(0.f, 0.f);
-      return;
-    }
-    const bool vec = vec_ok(*t.g);
-    load2c(y, e, avail, vec, f.y0, f.y1);
-    load2c(pred, e, avail, vec, f.p0, f.p1);
-    load2c(msg_in, e, avail, vec, f.m0, f.m1);
-  }
-  FBME_DEV float4 make(const TileCtx& t, long long e, int avail, const Frag& f) const {
-    if (avail <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
-    const float pr = prec[t.scene], dv = dvar[t.scene];
-    const float keep = damping, upd = 1.0f - damping;
-    auto step = [&](float2 yy, float2 pp, float2 mm) {
-      const float2 pseudo = make_float2(pp.x - dv * mm.x, pp.y - dv * mm.y);
-      const float2 cand = make_float2(pr * (yy.x - pseudo.x), pr * (yy.y - pseudo.y));
-      return make_float2(keep * mm.x + upd * cand.x, keep * mm.y + upd * cand.y);
-    };
-    const float2 o0 = step(f.y0, f.p0, f.m0);
-    const float2 o1 = avail >= 2 ? step(f.y1, f.p1, f.m1) : make_float2(0.f, 0.f);
-    if (t.col_tile == 0) {
-      if (avail >= 2 && vec_ok(*t.g)) {
-        *reinterpret_cast<float4*>(msg_out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
-      } else {
-        msg_out[e] = o0;
-        if (avail >= 2) msg_out[e + 1] = o1;
-      }
-    }
-    return make_float4(o0.x, o0.y, o1.x, o1.y);
-  }
-  FBME_DEV void tile_done(const TileCtx&, int, int) {}
-};
-
 // ---------------------------------------------------------------------------
 // epilogues
 // ---------------------------------------------------------------------------
@@ -313,6 +265,42 @@ __global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, Denoi
   write_block_partial(sv, red, a.part, scene, blockIdx.x, 1 * kPartWarps);
 }
 
+// UAMP message update (triton_kernels.py:72-84) for sweeps 2..T_u and the
+// final E-step: m' = d m + (1-d) prec (y - (p - dvar m)), into `msg_out`,
+// which adjoint stage 1 then reads.  Full occupancy, two samples per step
+// where y is 16-byte aligned and M even.
+__global__ void __launch_bounds__(kEwThreads)
+message_kernel(BatchShape s, const float2* y, const float2* pred, const float2* msg_in, float2* msg_out,
+               const float* prec, const float* dvar, float damping) {
+  const int scene = blockIdx.y;
+  const long long m = s.m();
+  const float pr = prec[scene], dv = dvar[scene];
+  const float keep = damping, upd = 1.0f - damping;
+  auto step = [&](float2 yy, float2 pp, float2 mm) {
+    const float2 pseudo = make_float2(pp.x - dv * mm.x, pp.y - dv * mm.y);
+    const float2 cand = make_float2(pr * (yy.x - pseudo.x), pr * (yy.y - pseudo.y));
+    return make_float2(keep * mm.x + upd * cand.x, keep * mm.y + upd * cand.y);
+  };
+  const long long first = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  if ((m & 1) == 0 && (reinterpret_cast<uintptr_t>(y) & 15u) == 0) {
+    for (long long j = first; j < m / 2; j += stride) {
+      const long long e = scene * m + 2 * j;
+      const float4 a = __ldg(reinterpret_cast<const float4*>(y + e));
+      const float4 p = __ldg(reinterpret_cast<const float4*>(pred + e));
+      const float4 q = __ldg(reinterpret_cast<const float4*>(msg_in + e));
+      const float2 o0 = step(make_float2(a.x, a.y), make_float2(p.x, p.y), make_float2(q.x, q.y));
+      const float2 o1 = step(make_float2(a.z, a.w), make_float2(p.z, p.w), make_float2(q.z, q.w));
+      *reinterpret_cast<float4*>(msg_out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
+    }
+  } else {
+    for (long long i = first; i < m; i += stride) {
+      const long long e = scene * m + i;
+      msg_out[e] = step(y[e], pred[e], msg_in[e]);
+    }
+  }
+}
+
 // First sweep: the lifted message is (1-d)/(dv+nv) * A^H y, the previous
 // mean is zero and the previous variance equals the initial prior
 // (solver.py:1160-1182, 2775-2783).  Blocks past `nblk_n` write the first
@@ -450,7 +438,6 @@ cudaError_t set_dft_attributes() {
   cudaError_t e;
   if ((e = set_attr_both<ProPlain, EpiStoreT>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProYPower, EpiStoreT>()) != cudaSuccess) return e;
-  if ((e = set_attr_both<ProMessage, EpiStoreT>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProPlain, EpiPredict>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProPlain, EpiBackprojection>()) != cudaSuccess) return e;
   return cudaSuccess;
@@ -513,7 +500,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
               cudaStream_t st, Profiler* prof) {
   const int nt = t.n_tile;
   const DftGeom f1 = stage_geom(kFwd1, s, t, nt), f2 = stage_geom(kFwd2, s, t, nt);
-  const DftGeom a1 = with_y(stage_geom(kAdj1, s, t, nt), u.y), a2 = stage_geom(kAdj2, s, t, nt);
+  const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   const long long BM = static_cast<long long>(s.B) * s.m();
   float2* msg[2] = {u.msg, u.msg + BM};
@@ -557,10 +544,10 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
       src_dof = PartSrc{bn, 1};
     } else {
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-                 run_stage(c.terms, a1,
-                           ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar,
-                                      c.uamp_damping},
-                           EpiStoreT{u.tmp}, u.status, st));
+                 (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
+                                                                      u.sc.prec, u.sc.dvar, c.uamp_damping)));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+                 run_stage(c.terms, a1, ProPlain{msg[cur ^ 1]}, EpiStoreT{u.tmp}, u.status, st));
       cur ^= 1;
       FBME_TIMED(prof, FBME_GROUP_ADJ_2,
                  run_stage(c.terms, a2, ProPlain{u.tmp}, EpiStoreT{u.lift}, u.status, st));
@@ -581,10 +568,10 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
 
   // --- final E-step (no prior update, no prediction), score keys ---
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-             run_stage(c.terms, a1,
-                       ProMessage{u.y, u.pred, msg[cur], msg[cur ^ 1], u.sc.prec, u.sc.dvar,
-                                  c.uamp_damping},
-                       EpiStoreT{u.tmp}, u.status, st));
+             (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
+                                                                  u.sc.prec, u.sc.dvar, c.uamp_damping)));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+             run_stage(c.terms, a1, ProPlain{msg[cur ^ 1]}, EpiStoreT{u.tmp}, u.status, st));
   da.update_prior = 0;
   da.keys = reinterpret_cast<uint32_t*>(u.keys);
   FBME_TIMED(prof, FBME_GROUP_ADJ_2,
