@@ -125,7 +125,12 @@ class FBMEEngine:
         for i in range(self.batch):
             shapes[i] = nat.FbmeShape(self.grid[0], self.grid[1], self.sample[0], self.sample[1])
         self._shapes = shapes
-        # the DFT stage tile width (None: the library default)
+        # the DFT stage tile width (None: chosen from the batch's tile count)
+        if n_tile is None:
+            from .autotune import default_width
+
+            n_tile = default_width(self.grid, self.sample, self.batch, int(cfg.dft_terms),
+                                   torch.cuda.get_device_properties(device).multi_processor_count)
         self.n_tile = n_tile
         self._params = nat.FbmeShapeParams(shapes[0], 0, -1.0, -1, int(n_tile or 0))
         nbytes = self.lib.fbme_plan_workspace_bytes_ex(shapes, self.batch, ctypes.byref(self.native_cfg),

@@ -88,11 +88,22 @@ class UnevenEngine:
         for i, (g, s) in enumerate(self.scenes):
             shape_arr[i] = nat.FbmeShape(g[0], g[1], s[0], s[1])
         params = (nat.FbmeShapeParams * len(distinct))()
+        # the buckets run concurrently, so the narrow-tile default applies
+        # only when all of them together leave SMs idle
+        from .autotune import candidates, default_width, stage_tiles
+
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        terms = int(cfg.dft_terms)
+        fill = sum(sum(stage_tiles(sh[0], sh[1], max(candidates(sh[0], sh[1], terms) or [256])))
+                   for sh in self.scenes)
+        self.tile_widths = {sh: int(tile_widths.get(sh) or default_width(sh[0], sh[1], 1, terms,
+                                                                         sms if fill < sms else 0))
+                            for sh in distinct}
         for i, sh in enumerate(distinct):
             r = resolved[sh]
             params[i] = nat.FbmeShapeParams(nat.FbmeShape(sh[0][0], sh[0][1], sh[1][0], sh[1][1]),
                                             r.uamp_iterations, r.uamp_damping, r.exchange_size,
-                                            int(tile_widths.get(sh, 0)))
+                                            self.tile_widths[sh])
         self._shape_arr, self._params = shape_arr, params
         nbytes = self.lib.fbme_plan_workspace_bytes_ex(shape_arr, self.batch, ctypes.byref(base), params,
                                                        len(distinct))

@@ -106,3 +106,18 @@ def test_autotuner_cache_round_trip(tmp_path):
                       device_name="test-device") == 128
     assert len(calls) == n
     assert cache_key((64, 64), (32, 32), 3, 3, "dev") == "64x64/32x32/t3/b4/dev"
+
+
+def test_default_width_follows_the_tile_count():
+    from fbme_b200.autotune import default_width, stage_tiles
+
+    g, s = (256, 256), (128, 128)
+    assert stage_tiles(g, s, 256) == [2, 1, 2, 4]  # forward 1, forward 2, adjoint 1, adjoint 2
+    # a lone scene leaves most SMs idle: the narrowest width
+    assert default_width(g, s, 1, 3, 148) == 64
+    # a batch whose tiles outnumber the SMs: the widest
+    assert default_width(g, s, 64, 3, 148) == 256
+    # the largest grid allows no narrow tile at all
+    assert default_width((1024, 512), (300, 500), 1, 3, 148) == 128
+    # six-term products have one width
+    assert default_width(g, s, 1, 6, 148) == 128
