@@ -120,6 +120,7 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
     plain = make_stable_plan(y, GRID, warmup=1)
     r_learned = rate(lambda: learned.replay(y), batch, steps)
     fallbacks = learned.fallbacks
+    r_warm = rate(lambda: learned.replay(y, fallback=False), batch, steps)
     n_learned = nmse(learned.replay(y, synchronize=True).x.cpu().numpy())
     r_plain = rate(lambda: plain.replay(y), batch, steps)
     n_plain = nmse(plain.replay(y, synchronize=True).x.cpu().numpy())
@@ -144,6 +145,7 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
         "workload": "held-out learned-distribution scenes, 256x256 / 128x128, K~U{100..400}, "
                     f"SNR~U[5,25] dB, batch {batch}",
         "learned_batched_scenes_per_s": r_learned,
+        "warm_solve_alone_scenes_per_s": r_warm,  # the same plan without its fallback check (not a result)
         "plain_batched_scenes_per_s": r_plain,
         "plain_single_scene_scenes_per_s": r_single,
         "learned_batched_vs_plain_single": r_learned / r_single,

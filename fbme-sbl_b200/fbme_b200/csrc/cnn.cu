@@ -257,7 +257,10 @@ conv3x3_kernel(const TIn* x, const __nv_bfloat16* mask, const __nv_bfloat16* wt,
 // padding 1, from CIN channels of an NHWC BF16 input (stride CSTR) to COUT
 // outputs over a 16 x 32 tile; each of the 128 threads computes 4 pixels
 // of one column, so every input value loaded from shared memory serves up
-// to 3 taps of 4 pixels and every weight vector 4 pixels.  BF16-rounded
+// to 3 taps of 4 pixels and every weight vector 4 pixels.  The tile holds
+// channel pairs, and the multiply-adds run on the paired FP32 FMA over
+// pairs of output channels (layer 1) or input channels (layer 3): the
+// kernel is bound by issued instructions, which this halves.  BF16-rounded
 // weights w[tap][ci][co], FP32 accumulation.  RELU_BF16: relu, BF16 NHWC
 // output with COUT channels; else FP32 channel 0.  With f1part (layer 1),
 // input channel 1 is not read: it is the scene constant BF16(sum of the
@@ -272,7 +275,7 @@ conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, voi
   static_assert(COUT == 8 || COUT == 1, "output channels");
   constexpr int TW = kSmallTW + 2, TH = kSmallTH + 2, NP = TW * TH, R = kSmallRows;
   constexpr int NW = 9 * CIN * COUT;
-  __shared__ float xs[CIN * NP];  // channel-major: lanes read consecutive words
+  __shared__ float2 xs2[(CIN / 2) * NP];  // channel pairs, pair-major: lanes read consecutive pairs
   __shared__ __align__(16) float ws[NW + 8];
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * kSmallTW, y0 = blockIdx.y * kSmallTH, b = blockIdx.z;
@@ -303,48 +306,56 @@ conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, voi
     if constexpr (CIN == 8) {
       const uint32_t u[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[k]));
-        xs[(2 * k) * NP + pix] = f.x;
-        xs[(2 * k + 1) * NP + pix] = f.y;
-      }
+      for (int k = 0; k < 4; ++k)
+        xs2[k * NP + pix] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[k]));
     } else {
       const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v[j]));
-      xs[pix] = f.x;
-      xs[NP + pix] = f1part ? (in[j] ? c1 : 0.f) : f.y;
+      xs2[pix] = make_float2(f.x, f1part ? (in[j] ? c1 : 0.f) : f.y);
     }
   }
   for (int i = tid; i < NW; i += kSmallThreads) ws[i] = w[i];
   if (tid < COUT) ws[NW + tid] = bias[tid];
   __syncthreads();
   const int px = tid % kSmallTW, r0 = (tid / kSmallTW) * R;
-  float acc[R][COUT];
+  // COUT == 8: acc2[p][k] holds output channels (2k, 2k+1); COUT == 1:
+  // acc2[p][0] holds the sums over the even and the odd input channels
+  constexpr int NA = COUT == 8 ? 4 : 1;
+  float2 acc2[R][NA];
 #pragma unroll
   for (int p = 0; p < R; ++p)
 #pragma unroll
-    for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
+    for (int k = 0; k < NA; ++k) acc2[p][k] = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int ci = 0; ci < CIN; ++ci) {
-    float xw[R + 2][3];
+  for (int cp = 0; cp < CIN / 2; ++cp) {
+    float2 xw[R + 2][3];
 #pragma unroll
     for (int r = 0; r < R + 2; ++r)
 #pragma unroll
-      for (int dx = 0; dx < 3; ++dx) xw[r][dx] = xs[ci * NP + (r0 + r) * TW + px + dx];
+      for (int dx = 0; dx < 3; ++dx) xw[r][dx] = xs2[cp * NP + (r0 + r) * TW + px + dx];
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
-      float wv[COUT];
       if constexpr (COUT == 8) {
-        const float4 a = *reinterpret_cast<const float4*>(ws + (tap * CIN + ci) * 8);
-        const float4 c = *reinterpret_cast<const float4*>(ws + (tap * CIN + ci) * 8 + 4);
-        wv[0] = a.x; wv[1] = a.y; wv[2] = a.z; wv[3] = a.w;
-        wv[4] = c.x; wv[5] = c.y; wv[6] = c.z; wv[7] = c.w;
+        const float4* wp = reinterpret_cast<const float4*>(ws + (tap * CIN + 2 * cp) * 8);
+        const float4 a0 = wp[0], a1 = wp[1], b0 = wp[2], b1 = wp[3];  // channels 2cp and 2cp + 1
+        const float2 wa[4] = {make_float2(a0.x, a0.y), make_float2(a0.z, a0.w), make_float2(a1.x, a1.y),
+                              make_float2(a1.z, a1.w)};
+        const float2 wb[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                              make_float2(b1.z, b1.w)};
+#pragma unroll
+        for (int p = 0; p < R; ++p) {
+          const float2 xv = xw[p + tap / 3][tap % 3];
+          const float2 xa = make_float2(xv.x, xv.x), xb = make_float2(xv.y, xv.y);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            acc2[p][k] = __ffma2_rn(xa, wa[k], acc2[p][k]);
+            acc2[p][k] = __ffma2_rn(xb, wb[k], acc2[p][k]);
+          }
+        }
       } else {
-        wv[0] = ws[tap * CIN + ci];
+        const float2 wv = *reinterpret_cast<const float2*>(ws + tap * CIN + 2 * cp);
+#pragma unroll
+        for (int p = 0; p < R; ++p) acc2[p][0] = __ffma2_rn(xw[p + tap / 3][tap % 3], wv, acc2[p][0]);
       }
-#pragma unroll
-      for (int p = 0; p < R; ++p)
-#pragma unroll
-        for (int co = 0; co < COUT; ++co) acc[p][co] += xw[p + tap / 3][tap % 3] * wv[co];
     }
   }
   const int gx = x0 + px;
@@ -359,10 +370,10 @@ conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, voi
       uint32_t o[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k)
-        o[k] = pack_bf16x2(fmaxf(acc[p][2 * k] + ws[NW + 2 * k], 0.f), fmaxf(acc[p][2 * k + 1] + ws[NW + 2 * k + 1], 0.f));
+        o[k] = pack_bf16x2(fmaxf(acc2[p][k].x + ws[NW + 2 * k], 0.f), fmaxf(acc2[p][k].y + ws[NW + 2 * k + 1], 0.f));
       *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * COUT) = make_uint4(o[0], o[1], o[2], o[3]);
     } else {
-      static_cast<float*>(out)[pix] = acc[p][0] + ws[NW];
+      static_cast<float*>(out)[pix] = (acc2[p][0].x + acc2[p][0].y) + ws[NW];
     }
   }
 }
