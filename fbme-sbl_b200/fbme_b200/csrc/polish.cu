@@ -498,36 +498,57 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
 
 // Residual exchange scoring (solver.py:4398-4412) without the M-space
 // residual: score[n] = |A^H y[n] - sum_k mu_k D1[n1-a_k] D2[n2-b_k]|^2 over
-// the grid, active atoms excluded.  A CTA covers kExRows grid rows; thread
-// (tx, ty) accumulates a 4-row x CT-column block (columns tx + 64 c), so
-// each u_k(n1) = mu_k D1[n1-a_k] and each D2 value loaded is reused 4 and
-// CT times; complex MACs use the paired FP32 FMA.  Each CTA emits its E best
+// the grid, active atoms excluded.  A CTA covers TY*RPT grid rows; thread
+// (tx, ty) accumulates RPT rows x CPT columns, the columns in pairs
+// 2tx + {0, 1} + 2*TX*c.  One paired FP32 FMA then serves two columns: with
+// RE, IM the real and imaginary accumulators of the pair,
+//   RE += ux*Dx;  IM += ux*Dy;  RE += uy*(-Dy);  IM += uy*Dx
+// (per element the rounding sequence of a complex MAC).  D2 sits in shared
+// memory split into re, im and -im, unrolled past the wrap, and twice, at
+// even and at odd offset, so that the pair at any shift is one aligned
+// 8-byte load with no index arithmetic.  Each CTA emits its E best
 // (key, index) candidates.
-constexpr int kExRows = 16;
 constexpr int kExThreads = 256;
 
-template <int CT>
-__global__ void __launch_bounds__(kExThreads)
+template <int RPT, int CPT, int TX>
+struct ExTile {
+  static constexpr int ty = kExThreads / TX;
+  static constexpr int rows = ty * RPT;     // grid rows per CTA
+  static constexpr int span = TX * CPT;     // columns of the thread grid
+  static constexpr int pairs = CPT / 2;
+  static constexpr int kpt = RPT * CPT;     // scores per thread
+  // floats per D2 table: index e + 1 <= N2 + span must be in range
+  __host__ __device__ static int table_len(int n2) { return (n2 + span + 2) & ~1; }
+  static size_t smem_bytes(int n2) {
+    return static_cast<size_t>(rows) * n2 * sizeof(float2) + 6ull * table_len(n2) * sizeof(float);
+  }
+};
+
+template <int RPT, int CPT, int TX>
+__global__ void __launch_bounds__(kExThreads, 2)
 exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
-  extern __shared__ float2 ex_shm[];
-  __shared__ TopkShared S;
-  __shared__ float4 u4[kMaxPolish][kExRows];  // {u.x, u.x, -u.y, u.y}
-  __shared__ int bk[kMaxPolish];
-  __shared__ uint32_t excl[kExRows][16];      // active-atom bitmap per row (N2 <= 512)
+  using T = ExTile<RPT, CPT, TX>;
+  extern __shared__ float4 ex_shm4[];
+  __shared__ TopkPrunedShared S;
+  __shared__ float4 u4[kMaxPolish][T::rows];  // {ux, ux, uy, uy}
+  __shared__ uint32_t excl[T::rows][16];      // active-atom bitmap per row (N2 <= 512)
+  __shared__ int atom_a[kMaxPolish], atom_b[kMaxPolish];
+  __shared__ float2 atom_mu[kMaxPolish];
   const BatchShape& s = A.s;
-  const int scene = blockIdx.y, r0 = blockIdx.x * kExRows;
+  const int scene = blockIdx.y, r0 = blockIdx.x * T::rows;
   const int K = A.c.polish_size, E = A.c.exchange;
   const int N1 = s.n1, N2 = s.n2;
-  const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
-  float2* d2 = ex_shm;
-  float2* bps = ex_shm + N2;  // [kExRows][N2]: this CTA's rows of A^H y
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  float2* bps = reinterpret_cast<float2*>(ex_shm4);  // [rows][N2]: this CTA's rows of A^H y
+  float* tab = reinterpret_cast<float*>(bps + T::rows * N2);
+  const int L = T::table_len(N2);
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
   {
     // A^H y rows, asynchronous copies in flight during the set-up and the
     // MAC loop: 16-byte chunks when N2 is even (every row then starts on a
     // 16-byte boundary), else one 8-byte element each
     const float2* src = A.p.bp + scene * s.n() + static_cast<long long>(r0) * N2;
-    const int rows = min(kExRows, N1 - r0);
+    const int rows = min(T::rows, N1 - r0);
     if ((N2 & 1) == 0) {
       for (int c = threadIdx.x; c < rows * N2 / 2; c += blockDim.x)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(bps + 2 * c)), "l"(src + 2 * c)
@@ -538,78 +559,110 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
-  for (int i = threadIdx.x; i < N2; i += blockDim.x) d2[i] = A.p.dir2[i];
-  for (int i = threadIdx.x; i < kExRows * 16; i += blockDim.x) (&excl[0][0])[i] = 0u;
-  __syncthreads();
-  for (int i = threadIdx.x; i < K * kExRows; i += blockDim.x) {
-    const int k = i / kExRows, ri = i % kExRows;
-    const int idx = ps->active[k];
+  // D2 tables: [parity][re, im, -im][L]; parity p holds D2[(e + p) mod N2] at e
+  for (int e = threadIdx.x; e < L; e += blockDim.x) {
+    const float2 v0 = __ldg(A.p.dir2 + e % N2), v1 = __ldg(A.p.dir2 + (e + 1) % N2);
+    tab[e] = v0.x;
+    tab[L + e] = v0.y;
+    tab[2 * L + e] = -v0.y;
+    tab[3 * L + e] = v1.x;
+    tab[4 * L + e] = v1.y;
+    tab[5 * L + e] = -v1.y;
+  }
+  for (int i = threadIdx.x; i < T::rows * 16; i += blockDim.x) (&excl[0][0])[i] = 0u;
+  if (threadIdx.x < K) {
+    const int idx = ps->active[threadIdx.x];
     const int a = idx / N2;
-    int dd = r0 + ri - a;
-    dd %= N1;
-    if (dd < 0) dd += N1;
-    const float2 uv = (r0 + ri < N1) ? cmul(ps->best_mean[k], A.p.dir1[dd]) : make_float2(0.f, 0.f);
-    u4[k][ri] = make_float4(uv.x, uv.x, -uv.y, uv.y);
-    if (ri == 0) {
-      bk[k] = idx % N2;
-      const int ra = a - r0;
-      if (ra >= 0 && ra < kExRows) atomicOr(&excl[ra][(idx % N2) >> 5], 1u << ((idx % N2) & 31));
-    }
+    atom_a[threadIdx.x] = a;
+    atom_b[threadIdx.x] = idx - a * N2;
+    atom_mu[threadIdx.x] = ps->best_mean[threadIdx.x];
   }
   __syncthreads();
-  float2 acc[4][CT];
+  if (threadIdx.x < K) {
+    const int ra = atom_a[threadIdx.x] - r0, b = atom_b[threadIdx.x];
+    if (ra >= 0 && ra < T::rows) atomicOr(&excl[ra][b >> 5], 1u << (b & 31));
+  }
+  for (int i = threadIdx.x; i < K * T::rows; i += blockDim.x) {
+    const int k = i / T::rows, ri = i % T::rows;
+    float2 uv = make_float2(0.f, 0.f);
+    if (r0 + ri < N1) {
+      int dd = r0 + ri - atom_a[k];
+      dd += dd < 0 ? N1 : 0;
+      uv = cmul(atom_mu[k], A.p.dir1[dd]);
+    }
+    u4[k][ri] = make_float4(uv.x, uv.x, uv.y, uv.y);
+  }
+  __syncthreads();
+  float2 re[RPT][T::pairs], im[RPT][T::pairs];
 #pragma unroll
-  for (int ri = 0; ri < 4; ++ri)
+  for (int r = 0; r < RPT; ++r)
 #pragma unroll
-    for (int c = 0; c < CT; ++c) acc[ri][c] = make_float2(0.f, 0.f);
+    for (int c = 0; c < T::pairs; ++c) {
+      re[r][c] = make_float2(0.f, 0.f);
+      im[r][c] = make_float2(0.f, 0.f);
+    }
+#pragma unroll 1
   for (int k = 0; k < K; ++k) {
-    const int b = bk[k];
-    float2 d[CT], ds[CT];
+    // pair (D2[e], D2[e+1]) at e = n2 - b + N2 >= 1; e's parity is the warp's
+    const int e0 = 2 * tx - atom_b[k] + N2;
+    const int odd = e0 & 1;
+    const float* base = tab + odd * 3 * L + (e0 - odd);
+    float2 dx[T::pairs], dy[T::pairs], ny[T::pairs];
 #pragma unroll
-    for (int c = 0; c < CT; ++c) {
-      const int n2 = tx + 64 * c;
-      int i2 = n2 - b;
-      i2 += i2 < 0 ? N2 : 0;
-      d[c] = n2 < N2 ? d2[i2] : make_float2(0.f, 0.f);
-      ds[c] = make_float2(d[c].y, d[c].x);
+    for (int c = 0; c < T::pairs; ++c) {
+      dx[c] = *reinterpret_cast<const float2*>(base + 2 * TX * c);
+      dy[c] = *reinterpret_cast<const float2*>(base + L + 2 * TX * c);
+      ny[c] = *reinterpret_cast<const float2*>(base + 2 * L + 2 * TX * c);
     }
 #pragma unroll
-    for (int ri = 0; ri < 4; ++ri) {
-      const float4 uu = u4[k][4 * ty + ri];
+    for (int r = 0; r < RPT; ++r) {
+      const float4 uu = u4[k][ty * RPT + r];
       const float2 ux = make_float2(uu.x, uu.y), uy = make_float2(uu.z, uu.w);
 #pragma unroll
-      for (int c = 0; c < CT; ++c) {
-        acc[ri][c] = __ffma2_rn(ux, d[c], acc[ri][c]);
-        acc[ri][c] = __ffma2_rn(uy, ds[c], acc[ri][c]);
+      for (int c = 0; c < T::pairs; ++c) {
+        re[r][c] = __ffma2_rn(ux, dx[c], re[r][c]);
+        im[r][c] = __ffma2_rn(ux, dy[c], im[r][c]);
+        re[r][c] = __ffma2_rn(uy, ny[c], re[r][c]);
+        im[r][c] = __ffma2_rn(uy, dx[c], im[r][c]);
       }
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
-  uint32_t key[4 * CT];
-  int gidx[4 * CT];
-  bool valid[4 * CT];
+  uint32_t key[T::kpt];
+  uint32_t valid = 0u;
 #pragma unroll
-  for (int ri = 0; ri < 4; ++ri)
+  for (int r = 0; r < RPT; ++r)
 #pragma unroll
-    for (int c = 0; c < CT; ++c) {
-      const int i = ri * CT + c;
-      const int lr = 4 * ty + ri;
-      const int n1 = r0 + lr, n2 = tx + 64 * c;
-      valid[i] = n1 < N1 && n2 < N2;
-      gidx[i] = n1 * N2 + n2;
-      key[i] = 0u;
-      if (valid[i]) {
-        const float2 bv = bps[lr * N2 + n2];
-        const float2 r = make_float2(bv.x - acc[ri][c].x, bv.y - acc[ri][c].y);
-        const bool act = (excl[lr][n2 >> 5] >> (n2 & 31)) & 1u;
-        key[i] = act ? 0u : float_key_t(abs_sq(r));
+    for (int c = 0; c < T::pairs; ++c)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int i = (r * T::pairs + c) * 2 + j;
+        const int lr = ty * RPT + r;
+        const int n2 = 2 * tx + 2 * TX * c + j;
+        key[i] = 0u;
+        if (r0 + lr < N1 && n2 < N2) {
+          valid |= 1u << i;
+          const float2 bv = bps[lr * N2 + n2];
+          const float2 acc = j ? make_float2(re[r][c].y, im[r][c].y) : make_float2(re[r][c].x, im[r][c].x);
+          const float2 d = make_float2(bv.x - acc.x, bv.y - acc.y);
+          const bool act = (excl[lr][n2 >> 5] >> (n2 & 31)) & 1u;
+          key[i] = act ? 0u : float_key_t(abs_sq(d));
+        }
       }
-    }
   const size_t off = (static_cast<size_t>(scene) * gridDim.x + blockIdx.x) * E;
-  // residual scores of one CTA crowd into few top-byte bins
-  block_topk<4 * CT, true>(key, gidx, valid, E, S, cand_key + off, cand_idx + off);
+  auto gidx = [&](int i) {
+    const int r = i / (2 * T::pairs), c = (i / 2) % T::pairs, j = i & 1;
+    return (r0 + ty * RPT + r) * N2 + 2 * tx + 2 * TX * c + j;
+  };
+  // residual scores of one CTA crowd into few top-byte bins (radix fallback)
+  block_topk_pruned<T::kpt, true>(key, valid, gidx, E, S, cand_key + off, cand_idx + off);
 }
+
+using ExSmall = ExTile<8, 2, 32>;   // N2 <= 64
+using ExMid = ExTile<8, 2, 64>;     // N2 <= 128
+using ExWide = ExTile<8, 4, 64>;    // N2 <= 256
+using ExWidest = ExTile<4, 8, 64>;  // N2 <= 512
 
 // Final K-space outputs, fixed-budget diagnostics, effective DOF
 // (solver.py:1989-2021, 2081-2092, 3408-3496, 2108-2126).
@@ -731,18 +784,34 @@ void launch_topk(const uint32_t* keys, long long n, int k, int B, uint32_t* cand
 void launch_topk_merge(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, int B,
                        int* out_idx, float* out_val, cudaStream_t st);
 
-int exchange_blocks(const BatchShape& s) { return (s.n1 + kExRows - 1) / kExRows; }
+static int exchange_rows(int n2) {
+  return n2 <= 64 ? ExSmall::rows : n2 <= 128 ? ExMid::rows : n2 <= 256 ? ExWide::rows : ExWidest::rows;
+}
 
-// Dynamic shared memory of the exchange kernel: D2 and the CTA's rows of
-// A^H y.
-static size_t exchange_smem_bytes(int n2) { return static_cast<size_t>(1 + kExRows) * n2 * sizeof(float2); }
+int exchange_blocks(const BatchShape& s) {
+  const int rows = exchange_rows(s.n2);
+  return (s.n1 + rows - 1) / rows;
+}
+
+template <int RPT, int CPT, int TX>
+static cudaError_t set_exchange_smem(int n2_max) {
+  return cudaFuncSetAttribute(exchange_kernel<RPT, CPT, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(ExTile<RPT, CPT, TX>::smem_bytes(n2_max)));
+}
 
 cudaError_t set_polish_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(exchange_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(exchange_smem_bytes(256)));
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(exchange_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(exchange_smem_bytes(512)));
+  cudaError_t e = set_exchange_smem<8, 2, 32>(64);
+  if (e == cudaSuccess) e = set_exchange_smem<8, 2, 64>(128);
+  if (e == cudaSuccess) e = set_exchange_smem<8, 4, 64>(256);
+  if (e == cudaSuccess) e = set_exchange_smem<4, 8, 64>(512);
+  return e;
+}
+
+template <int RPT, int CPT, int TX>
+static void launch_exchange(const PolishArgs& A, const PolishBuffers& p, cudaStream_t st) {
+  const dim3 grid(exchange_blocks(A.s), A.s.B);
+  exchange_kernel<RPT, CPT, TX><<<grid, kExThreads, ExTile<RPT, CPT, TX>::smem_bytes(A.s.n2), st>>>(
+      A, p.cand_key, p.cand_idx);
 }
 
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
@@ -755,14 +824,14 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 0)));
   if (c.exchange > 0 && c.polish_iters > 1) {
     const int nb = exchange_blocks(s);
-    const size_t shm = exchange_smem_bytes(s.n2);
-    const dim3 grid(nb, s.B);
-    if (s.n2 <= 256)
-      FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
-                 (exchange_kernel<4><<<grid, kExThreads, shm, st>>>(A, p.cand_key, p.cand_idx)));
+    if (s.n2 <= 64)
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<8, 2, 32>(A, p, st)));
+    else if (s.n2 <= 128)
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<8, 2, 64>(A, p, st)));
+    else if (s.n2 <= 256)
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<8, 4, 64>(A, p, st)));
     else
-      FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
-                 (exchange_kernel<8><<<grid, kExThreads, shm, st>>>(A, p.cand_key, p.cand_idx)));
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<4, 8, 64>(A, p, st)));
     FBME_TIMED(prof, FBME_GROUP_TOPK,
                launch_topk_merge(p.cand_key, p.cand_idx, nb * c.exchange, c.exchange, s.B,
                                  p.xcand_idx, p.xcand_val, st));

@@ -34,9 +34,11 @@ struct TopkShared {
 // taken.  Writes k winners, sorted (key desc, index asc), to out_key/out_idx.
 // AGG: warp-aggregated histogram atomics (lanes whose keys share a bin add
 // once); pays where the keys crowd into few bins, costs where they spread.
-template <int KPT, bool AGG = false>
-FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], const bool (&valid)[KPT],
-                         int k, TopkShared& S, uint32_t* out_key, int* out_idx) {
+// Entries are read through valid(i) and gidx(i), so callers can compute
+// them instead of holding arrays.
+template <int KPT, bool AGG, typename Valid, typename GIdx>
+FBME_DEV void block_topk_fn(const uint32_t (&key)[KPT], Valid valid, GIdx gidx, int k, TopkShared& S,
+                            uint32_t* out_key, int* out_idx) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
   if (tid == 0) {
@@ -51,7 +53,7 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
   {
     int nv = 0;
 #pragma unroll
-    for (int i = 0; i < KPT; ++i) nv += valid[i] ? 1 : 0;
+    for (int i = 0; i < KPT; ++i) nv += valid(i) ? 1 : 0;
     nv = warp_sum(nv);
     if (lane == 0 && nv) atomicAdd(&S.nvalid, nv);
   }
@@ -75,7 +77,7 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
     const uint32_t prefix = S.prefix, mask = S.mask;
 #pragma unroll
     for (int i = 0; i < KPT; ++i) {
-      const bool part = valid[i] && (key[i] & mask) == prefix;
+      const bool part = valid(i) && (key[i] & mask) == prefix;
       if constexpr (AGG) {
         const unsigned act = __ballot_sync(0xffffffffu, part);
         if (part) {
@@ -126,14 +128,14 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
   int my_eq = 0;
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
-    if (valid[i] && key[i] > T) {
+    if (valid(i) && key[i] > T) {
       const int pos = atomicAdd(&S.ngt, 1);
       if (pos < 32) {
         S.sel_key[pos] = key[i];
-        S.sel_idx[pos] = gidx[i];
+        S.sel_idx[pos] = gidx(i);
       }
     }
-    my_eq += (valid[i] && key[i] == T) ? 1 : 0;
+    my_eq += (valid(i) && key[i] == T) ? 1 : 0;
   }
   my_eq = warp_sum(my_eq);
   if (lane == 0 && my_eq) atomicAdd(&S.neq, my_eq);
@@ -143,10 +145,10 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
     // every tie is a winner
 #pragma unroll
     for (int i = 0; i < KPT; ++i) {
-      if (valid[i] && key[i] == T) {
+      if (valid(i) && key[i] == T) {
         const int pos = atomicAdd(&S.filled, 1);
         S.sel_key[base + pos] = T;
-        S.sel_idx[base + pos] = gidx[i];
+        S.sel_idx[base + pos] = gidx(i);
       }
     }
   } else {
@@ -156,7 +158,7 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
       int best = 0x7fffffff;
 #pragma unroll
       for (int i = 0; i < KPT; ++i)
-        if (valid[i] && key[i] == T && gidx[i] > taken_below && gidx[i] < best) best = gidx[i];
+        if (valid(i) && key[i] == T && gidx(i) > taken_below && gidx(i) < best) best = gidx(i);
       for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
       if (lane == 0) S.red_idx[warp] = best;
       __syncthreads();
@@ -189,6 +191,111 @@ FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], con
     if (lane < k_out) {
       out_key[lane] = lane < k ? kk : 0u;
       out_idx[lane] = lane < k ? ii : 0x7fffffff;
+    }
+  }
+  __syncthreads();
+}
+
+template <int KPT, bool AGG = false>
+FBME_DEV void block_topk(const uint32_t (&key)[KPT], const int (&gidx)[KPT], const bool (&valid)[KPT],
+                         int k, TopkShared& S, uint32_t* out_key, int* out_idx) {
+  block_topk_fn<KPT, AGG>(
+      key, [&](int i) { return valid[i]; }, [&](int i) { return gidx[i]; }, k, S, out_key, out_idx);
+}
+
+constexpr int kPrunedCap = 256;
+constexpr int kPrunedLaneMax = 256;  // warps x k lane maxima ranked for the bound
+
+struct TopkPrunedShared {
+  TopkShared radix;  // the fallback's
+  uint32_t lane_max[kPrunedLaneMax];
+  uint32_t t0;
+  int ncand;
+  uint2 cand[kPrunedCap];  // (key, index)
+};
+
+// Block-wide top-k (k <= 32) with the result of block_topk, for key sets
+// whose k best are few among many.  Every thread's largest key is a lane
+// maximum; the k-th largest lane maximum T0 is a lower bound on the
+// block's k-th key (k different threads hold a key >= T0), so the block's
+// top k are among the keys >= T0, typically little more than k of them.
+// Each warp sorts its lane maxima and offers its k largest, which contain
+// the block's k largest; T0 is found among those by counting.  The keys
+// >= T0 go on a shared list, where each finds its output place by counting
+// the entries ahead of it (key desc, index asc).  A zero bound or a list
+// longer than kPrunedCap falls back to the radix select.  valid: bit i set
+// when entry i counts; gidx(i): its index.  The block is whole warps.
+template <int KPT, bool AGG, typename GIdx>
+FBME_DEV void block_topk_pruned(const uint32_t (&key)[KPT], uint32_t valid, GIdx gidx, int k,
+                                TopkPrunedShared& P, uint32_t* out_key, int* out_idx) {
+  static_assert(KPT <= 32, "the valid mask holds 32 entries");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int offered = (blockDim.x >> 5) * k;
+  auto radix = [&]() {
+    block_topk_fn<KPT, AGG>(
+        key, [&](int i) { return ((valid >> i) & 1u) != 0u; }, gidx, k, P.radix, out_key, out_idx);
+  };
+  if (offered > kPrunedLaneMax) {
+    radix();
+    return;
+  }
+  uint32_t m = 0u;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i)
+    if ((valid >> i) & 1u) m = max(m, key[i]);
+  // bitonic sort of the warp's lane maxima, descending
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const uint32_t o = __shfl_xor_sync(0xffffffffu, m, stride);
+      const bool keep_max = ((lane & stride) == 0) == ((lane & size) == 0);
+      m = keep_max ? max(m, o) : min(m, o);
+    }
+  if (lane < k) P.lane_max[warp * k + lane] = m;
+  if (tid == 0) {
+    P.t0 = 0u;
+    P.ncand = 0;
+  }
+  __syncthreads();
+  if (tid < offered) {
+    // place among the offered maxima, ties by position: unique
+    const uint32_t me = P.lane_max[tid];
+    int rank = 0;
+    for (int j = 0; j < offered; ++j) {
+      const uint32_t o = P.lane_max[j];
+      rank += (o > me || (o == me && j < tid)) ? 1 : 0;
+    }
+    if (rank == k - 1) P.t0 = me;
+  }
+  __syncthreads();
+  const uint32_t t0 = P.t0;
+  if (t0 == 0u) {
+    radix();
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < KPT; ++i)
+    if (((valid >> i) & 1u) && key[i] >= t0) {
+      const int pos = atomicAdd(&P.ncand, 1);
+      if (pos < kPrunedCap) P.cand[pos] = make_uint2(key[i], static_cast<uint32_t>(gidx(i)));
+    }
+  __syncthreads();
+  const int n = P.ncand;  // >= k: k threads hold a valid key >= t0
+  if (n > kPrunedCap) {
+    radix();
+    return;
+  }
+  for (int c = tid; c < n; c += blockDim.x) {
+    const uint2 me = P.cand[c];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const uint2 o = P.cand[j];
+      rank += (o.x > me.x || (o.x == me.x && static_cast<int>(o.y) < static_cast<int>(me.y))) ? 1 : 0;
+    }
+    if (rank < k) {
+      out_key[rank] = me.x;
+      out_idx[rank] = static_cast<int>(me.y);
     }
   }
   __syncthreads();
