@@ -17,6 +17,18 @@
 
 namespace fbme {
 
+// SMs of the current device (persistent grids size to it).
+static inline int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+      n = 148;
+  }
+  return n;
+}
+
 // ---------------------------------------------------------------------------
 // complex helpers (interleaved complex64 as float2)
 // ---------------------------------------------------------------------------

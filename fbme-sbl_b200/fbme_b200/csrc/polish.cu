@@ -508,26 +508,29 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
 // even and at odd offset, so that the pair at any shift is one aligned
 // 8-byte load with no index arithmetic.  Each CTA emits its E best
 // (key, index) candidates.
-constexpr int kExThreads = 256;
-
-template <int RPT, int CPT, int TX>
+template <int RPT_, int CPT, int TX_, int THREADS, int N2MAX>
 struct ExTile {
-  static constexpr int ty = kExThreads / TX;
+  static constexpr int RPT = RPT_, TX = TX_, threads = THREADS, n2_max = N2MAX;
+  static constexpr int ty = THREADS / TX;
   static constexpr int rows = ty * RPT;     // grid rows per CTA
   static constexpr int span = TX * CPT;     // columns of the thread grid
   static constexpr int pairs = CPT / 2;
   static constexpr int kpt = RPT * CPT;     // scores per thread
+  static_assert(span >= N2MAX, "the thread grid spans the widest row");
   // floats per D2 table: index e + 1 <= N2 + span must be in range
-  __host__ __device__ static int table_len(int n2) { return (n2 + span + 2) & ~1; }
+  __host__ __device__ static constexpr int table_len(int n2) { return (n2 + span + 2) & ~1; }
   static size_t smem_bytes(int n2) {
     return static_cast<size_t>(rows) * n2 * sizeof(float2) + 6ull * table_len(n2) * sizeof(float);
   }
 };
 
-template <int RPT, int CPT, int TX>
-__global__ void __launch_bounds__(kExThreads, 2)
+// Two CTAs per SM (128 registers a thread): a persistent single CTA per SM
+// with double-buffered rows measured slower, its 8 warps too few to keep
+// the FMA pipes fed.
+template <typename T>
+__global__ void __launch_bounds__(T::threads, 2)
 exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
-  using T = ExTile<RPT, CPT, TX>;
+  constexpr int RPT = T::RPT, TX = T::TX;
   extern __shared__ float4 ex_shm4[];
   __shared__ TopkPrunedShared S;
   __shared__ float4 u4[kMaxPolish][T::rows];  // {ux, ux, uy, uy}
@@ -559,15 +562,24 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
-  // D2 tables: [parity][re, im, -im][L]; parity p holds D2[(e + p) mod N2] at e
-  for (int e = threadIdx.x; e < L; e += blockDim.x) {
-    const float2 v0 = __ldg(A.p.dir2 + e % N2), v1 = __ldg(A.p.dir2 + (e + 1) % N2);
-    tab[e] = v0.x;
-    tab[L + e] = v0.y;
-    tab[2 * L + e] = -v0.y;
-    tab[3 * L + e] = v1.x;
-    tab[4 * L + e] = v1.y;
-    tab[5 * L + e] = -v1.y;
+  // D2 tables: [parity][re, im, -im][L]; parity p holds D2[(e + p) mod N2] at
+  // e.  Unrolled to the widest table, so that every thread's loads are in
+  // flight together.
+  constexpr int kTabIters = (T::table_len(T::n2_max) + T::threads - 1) / T::threads;
+#pragma unroll
+  for (int it = 0; it < kTabIters; ++it) {
+    const int e = threadIdx.x + it * T::threads;
+    if (e < L) {
+      const int e0 = e % N2;
+      const int e1 = e0 + 1 == N2 ? 0 : e0 + 1;
+      const float2 v0 = __ldg(A.p.dir2 + e0), v1 = __ldg(A.p.dir2 + e1);
+      tab[e] = v0.x;
+      tab[L + e] = v0.y;
+      tab[2 * L + e] = -v0.y;
+      tab[3 * L + e] = v1.x;
+      tab[4 * L + e] = v1.y;
+      tab[5 * L + e] = -v1.y;
+    }
   }
   for (int i = threadIdx.x; i < T::rows * 16; i += blockDim.x) (&excl[0][0])[i] = 0u;
   if (threadIdx.x < K) {
@@ -582,15 +594,20 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
     const int ra = atom_a[threadIdx.x] - r0, b = atom_b[threadIdx.x];
     if (ra >= 0 && ra < T::rows) atomicOr(&excl[ra][b >> 5], 1u << (b & 31));
   }
-  for (int i = threadIdx.x; i < K * T::rows; i += blockDim.x) {
+  constexpr int kUIters = (kMaxPolish * T::rows + T::threads - 1) / T::threads;
+#pragma unroll
+  for (int it = 0; it < kUIters; ++it) {
+    const int i = threadIdx.x + it * T::threads;
     const int k = i / T::rows, ri = i % T::rows;
-    float2 uv = make_float2(0.f, 0.f);
-    if (r0 + ri < N1) {
-      int dd = r0 + ri - atom_a[k];
-      dd += dd < 0 ? N1 : 0;
-      uv = cmul(atom_mu[k], A.p.dir1[dd]);
+    if (k < K) {
+      float2 uv = make_float2(0.f, 0.f);
+      if (r0 + ri < N1) {
+        int dd = r0 + ri - atom_a[k];
+        dd += dd < 0 ? N1 : 0;
+        uv = cmul(atom_mu[k], __ldg(A.p.dir1 + dd));
+      }
+      u4[k][ri] = make_float4(uv.x, uv.x, uv.y, uv.y);
     }
-    u4[k][ri] = make_float4(uv.x, uv.x, uv.y, uv.y);
   }
   __syncthreads();
   float2 re[RPT][T::pairs], im[RPT][T::pairs];
@@ -659,10 +676,10 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
   block_topk_pruned<T::kpt, true>(key, valid, gidx, E, S, cand_key + off, cand_idx + off);
 }
 
-using ExSmall = ExTile<8, 2, 32>;   // N2 <= 64
-using ExMid = ExTile<8, 2, 64>;     // N2 <= 128
-using ExWide = ExTile<8, 4, 64>;    // N2 <= 256
-using ExWidest = ExTile<4, 8, 64>;  // N2 <= 512
+using ExSmall = ExTile<8, 2, 32, 256, 64>;
+using ExMid = ExTile<8, 2, 64, 256, 128>;
+using ExWide = ExTile<8, 4, 64, 256, 256>;
+using ExWidest = ExTile<4, 8, 64, 256, 512>;
 
 // Final K-space outputs, fixed-budget diagnostics, effective DOF
 // (solver.py:1989-2021, 2081-2092, 3408-3496, 2108-2126).
@@ -793,25 +810,24 @@ int exchange_blocks(const BatchShape& s) {
   return (s.n1 + rows - 1) / rows;
 }
 
-template <int RPT, int CPT, int TX>
-static cudaError_t set_exchange_smem(int n2_max) {
-  return cudaFuncSetAttribute(exchange_kernel<RPT, CPT, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(ExTile<RPT, CPT, TX>::smem_bytes(n2_max)));
+template <typename T>
+static cudaError_t set_exchange_smem() {
+  return cudaFuncSetAttribute(exchange_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(T::smem_bytes(T::n2_max)));
 }
 
 cudaError_t set_polish_attributes() {
-  cudaError_t e = set_exchange_smem<8, 2, 32>(64);
-  if (e == cudaSuccess) e = set_exchange_smem<8, 2, 64>(128);
-  if (e == cudaSuccess) e = set_exchange_smem<8, 4, 64>(256);
-  if (e == cudaSuccess) e = set_exchange_smem<4, 8, 64>(512);
+  cudaError_t e = set_exchange_smem<ExSmall>();
+  if (e == cudaSuccess) e = set_exchange_smem<ExMid>();
+  if (e == cudaSuccess) e = set_exchange_smem<ExWide>();
+  if (e == cudaSuccess) e = set_exchange_smem<ExWidest>();
   return e;
 }
 
-template <int RPT, int CPT, int TX>
+template <typename T>
 static void launch_exchange(const PolishArgs& A, const PolishBuffers& p, cudaStream_t st) {
   const dim3 grid(exchange_blocks(A.s), A.s.B);
-  exchange_kernel<RPT, CPT, TX><<<grid, kExThreads, ExTile<RPT, CPT, TX>::smem_bytes(A.s.n2), st>>>(
-      A, p.cand_key, p.cand_idx);
+  exchange_kernel<T><<<grid, T::threads, T::smem_bytes(A.s.n2), st>>>(A, p.cand_key, p.cand_idx);
 }
 
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
@@ -825,13 +841,13 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
   if (c.exchange > 0 && c.polish_iters > 1) {
     const int nb = exchange_blocks(s);
     if (s.n2 <= 64)
-      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<8, 2, 32>(A, p, st)));
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<ExSmall>(A, p, st)));
     else if (s.n2 <= 128)
-      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<8, 2, 64>(A, p, st)));
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<ExMid>(A, p, st)));
     else if (s.n2 <= 256)
-      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<8, 4, 64>(A, p, st)));
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<ExWide>(A, p, st)));
     else
-      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<4, 8, 64>(A, p, st)));
+      FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<ExWidest>(A, p, st)));
     FBME_TIMED(prof, FBME_GROUP_TOPK,
                launch_topk_merge(p.cand_key, p.cand_idx, nb * c.exchange, c.exchange, s.B,
                                  p.xcand_idx, p.xcand_val, st));

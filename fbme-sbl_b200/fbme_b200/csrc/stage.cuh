@@ -134,17 +134,6 @@ static inline DftGeom stage_geom(Stage st, const BatchShape& s, const DftTables&
 
 static inline int tiles(const DftGeom& g) { return g.n_scenes * g.row_tiles * g.col_tiles; }
 
-static inline int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
-      n = 148;
-  }
-  return n;
-}
-
 static inline int persistent_grid(const DftGeom& g) {
   const int t = tiles(g), s = sm_count();
   return t < s ? t : s;
