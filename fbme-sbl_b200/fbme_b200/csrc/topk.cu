@@ -19,26 +19,31 @@ constexpr int kTopkSlice = kTopkBlockThreads * kTopkKpt;  // 8192 keys per CTA
 constexpr int kMergeMax = 2048;
 
 // FROM_SCORES: `in` holds float scores (converted to keys); else keys.
+// The slice's k best lie among its keys at or above the k-th largest
+// thread maximum (radix bound), typically a few dozen of the 8192.
 template <bool FROM_SCORES>
 __global__ void __launch_bounds__(kTopkBlockThreads)
 topk_blocks_kernel(const void* in, long long n, int k, uint32_t* cand_key, int* cand_idx) {
-  __shared__ TopkShared S;
+  __shared__ TopkPrunedShared S;
   const int scene = blockIdx.y, blk = blockIdx.x;
   const uint32_t* kp = static_cast<const uint32_t*>(in) + scene * n;
   const float* sp = static_cast<const float*>(in) + scene * n;
-  const long long base = static_cast<long long>(blk) * kTopkSlice;
+  const long long base = static_cast<long long>(blk) * kTopkSlice + threadIdx.x;
   uint32_t key[kTopkKpt];
-  int gidx[kTopkKpt];
-  bool valid[kTopkKpt];
+  uint32_t valid = 0u;
 #pragma unroll
   for (int i = 0; i < kTopkKpt; ++i) {
-    const long long e = base + static_cast<long long>(i) * kTopkBlockThreads + threadIdx.x;
-    valid[i] = e < n;
-    key[i] = valid[i] ? (FROM_SCORES ? float_key_t(sp[e]) : kp[e]) : 0u;
-    gidx[i] = static_cast<int>(e);
+    const long long e = base + static_cast<long long>(i) * kTopkBlockThreads;
+    key[i] = 0u;
+    if (e < n) {
+      valid |= 1u << i;
+      key[i] = FROM_SCORES ? float_key_t(sp[e]) : kp[e];
+    }
   }
   const size_t off = (static_cast<size_t>(scene) * gridDim.x + blk) * k;
-  block_topk(key, gidx, valid, k, S, cand_key + off, cand_idx + off);
+  block_topk_pruned<kTopkKpt, false, TopkBound::kRadix>(
+      key, valid, [&](int i) { return static_cast<int>(base + static_cast<long long>(i) * kTopkBlockThreads); }, k,
+      S, cand_key + off, cand_idx + off);
 }
 
 template <typename Idx>

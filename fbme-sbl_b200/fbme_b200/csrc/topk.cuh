@@ -28,6 +28,71 @@ struct TopkShared {
   int sel_idx[32];
 };
 
+// Warp 0, after a radix pass's histogram: the digit bin that holds the
+// remaining-th largest key; narrows prefix/mask and the remaining count.
+FBME_DEV void radix_pick_bin(TopkShared& S, int shift, uint32_t prefix, uint32_t mask) {
+  const int lane = threadIdx.x & 31;
+  const int hi = 256 - 8 * lane;  // lane owns bins [hi-8, hi), counted from the top
+  uint32_t local = 0;
+#pragma unroll
+  for (int b = 1; b <= 8; ++b) local += S.hist[hi - b];
+  uint32_t incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const uint32_t excl = incl - local;
+  const int rem = S.remaining;
+  const bool here = excl < static_cast<uint32_t>(rem) && incl >= static_cast<uint32_t>(rem);
+  const unsigned ball = __ballot_sync(0xffffffffu, here);
+  const int owner = ball ? __ffs(ball) - 1 : 31;
+  if (lane == owner) {
+    uint32_t cum = excl;
+    int sel = hi - 8;
+    for (int b = hi - 1; b >= hi - 8; --b) {
+      if (cum + S.hist[b] >= static_cast<uint32_t>(rem)) {
+        sel = b;
+        break;
+      }
+      cum += S.hist[b];
+    }
+    S.remaining = rem - static_cast<int>(cum);
+    S.prefix = prefix | (static_cast<uint32_t>(sel) << shift);
+    S.mask = mask | (255u << shift);
+  }
+}
+
+// k-th largest of the valid keys held one per thread (1 <= k <= their
+// number): radix select with 8-bit digits, histogram counts aggregated per
+// warp (the keys crowd into few top-byte bins).  Ends on a barrier.
+FBME_DEV uint32_t block_kth_key(uint32_t key, bool valid, int k, TopkShared& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    S.prefix = 0;
+    S.mask = 0;
+    S.remaining = k;
+  }
+#pragma unroll 1
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+    for (int b = tid; b < 256; b += blockDim.x) S.hist[b] = 0;
+    __syncthreads();
+    const uint32_t prefix = S.prefix, mask = S.mask;
+    const bool part = valid && (key & mask) == prefix;
+    const unsigned act = __ballot_sync(0xffffffffu, part);
+    if (part) {
+      const uint32_t bin = (key >> shift) & 255u;
+      const unsigned peers = __match_any_sync(act, bin);
+      if (__ffs(peers) - 1 == lane) atomicAdd(&S.hist[bin], static_cast<uint32_t>(__popc(peers)));
+    }
+    __syncthreads();
+    if (warp == 0) radix_pick_bin(S, shift, prefix, mask);
+    __syncthreads();
+  }
+  return S.prefix;
+}
+
 // Block-wide top-k (k <= 32) of the valid (key, gidx) pairs held KPT per
 // thread.  Radix select with 8-bit digits finds the k-th largest key T;
 // keys above T are all taken; among keys equal to T the lowest indices are
@@ -90,37 +155,7 @@ FBME_DEV void block_topk_fn(const uint32_t (&key)[KPT], Valid valid, GIdx gidx, 
       }
     }
     __syncthreads();
-    if (warp == 0) {
-      const int hi = 256 - 8 * lane;  // lane owns bins [hi-8, hi), counted from the top
-      uint32_t local = 0;
-#pragma unroll
-      for (int b = 1; b <= 8; ++b) local += S.hist[hi - b];
-      uint32_t incl = local;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const uint32_t excl = incl - local;
-      const int rem = S.remaining;
-      const bool here = excl < static_cast<uint32_t>(rem) && incl >= static_cast<uint32_t>(rem);
-      const unsigned ball = __ballot_sync(0xffffffffu, here);
-      const int owner = ball ? __ffs(ball) - 1 : 31;
-      if (lane == owner) {
-        uint32_t cum = excl;
-        int sel = hi - 8;
-        for (int b = hi - 1; b >= hi - 8; --b) {
-          if (cum + S.hist[b] >= static_cast<uint32_t>(rem)) {
-            sel = b;
-            break;
-          }
-          cum += S.hist[b];
-        }
-        S.remaining = rem - static_cast<int>(cum);
-        S.prefix = prefix | (static_cast<uint32_t>(sel) << shift);
-        S.mask = mask | (255u << shift);
-      }
-    }
+    if (warp == 0) radix_pick_bin(S, shift, prefix, mask);
     __syncthreads();
   }
   const uint32_t T = S.prefix;
@@ -214,62 +249,78 @@ struct TopkPrunedShared {
   uint2 cand[kPrunedCap];  // (key, index)
 };
 
+// How block_topk_pruned finds its bound T0: kWarpSort sorts each warp's
+// lane maxima and ranks the warps' k largest by counting (few warps x small
+// k); kRadix runs a radix select over the lane maxima (large k).
+enum class TopkBound { kWarpSort, kRadix };
+
 // Block-wide top-k (k <= 32) with the result of block_topk, for key sets
 // whose k best are few among many.  Every thread's largest key is a lane
 // maximum; the k-th largest lane maximum T0 is a lower bound on the
 // block's k-th key (k different threads hold a key >= T0), so the block's
 // top k are among the keys >= T0, typically little more than k of them.
-// Each warp sorts its lane maxima and offers its k largest, which contain
-// the block's k largest; T0 is found among those by counting.  The keys
-// >= T0 go on a shared list, where each finds its output place by counting
-// the entries ahead of it (key desc, index asc).  A zero bound or a list
-// longer than kPrunedCap falls back to the radix select.  valid: bit i set
-// when entry i counts; gidx(i): its index.  The block is whole warps.
-template <int KPT, bool AGG, typename GIdx>
+// The keys >= T0 go on a shared list, where each finds its output place by
+// counting the entries ahead of it (key desc, index asc).  A zero bound,
+// fewer than k threads with a key, or a list longer than kPrunedCap falls
+// back to the radix select over all keys.  valid: bit i set when entry i
+// counts; gidx(i): its index.  The block is whole warps.
+template <int KPT, bool AGG, TopkBound BOUND = TopkBound::kWarpSort, typename GIdx>
 FBME_DEV void block_topk_pruned(const uint32_t (&key)[KPT], uint32_t valid, GIdx gidx, int k,
                                 TopkPrunedShared& P, uint32_t* out_key, int* out_idx) {
   static_assert(KPT <= 32, "the valid mask holds 32 entries");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int offered = (blockDim.x >> 5) * k;
   auto radix = [&]() {
     block_topk_fn<KPT, AGG>(
         key, [&](int i) { return ((valid >> i) & 1u) != 0u; }, gidx, k, P.radix, out_key, out_idx);
   };
-  if (offered > kPrunedLaneMax) {
-    radix();
-    return;
-  }
   uint32_t m = 0u;
 #pragma unroll
   for (int i = 0; i < KPT; ++i)
     if ((valid >> i) & 1u) m = max(m, key[i]);
-  // bitonic sort of the warp's lane maxima, descending
-#pragma unroll
-  for (int size = 2; size <= 32; size <<= 1)
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      const uint32_t o = __shfl_xor_sync(0xffffffffu, m, stride);
-      const bool keep_max = ((lane & stride) == 0) == ((lane & size) == 0);
-      m = keep_max ? max(m, o) : min(m, o);
+  uint32_t t0 = 0u;
+  if constexpr (BOUND == TopkBound::kWarpSort) {
+    // each warp offers its k largest lane maxima, which hold the block's k
+    // largest; T0 is found among them by counting
+    const int offered = (blockDim.x >> 5) * k;
+    if (offered > kPrunedLaneMax) {
+      radix();
+      return;
     }
-  if (lane < k) P.lane_max[warp * k + lane] = m;
-  if (tid == 0) {
-    P.t0 = 0u;
-    P.ncand = 0;
-  }
-  __syncthreads();
-  if (tid < offered) {
-    // place among the offered maxima, ties by position: unique
-    const uint32_t me = P.lane_max[tid];
-    int rank = 0;
-    for (int j = 0; j < offered; ++j) {
-      const uint32_t o = P.lane_max[j];
-      rank += (o > me || (o == me && j < tid)) ? 1 : 0;
+    // bitonic sort of the warp's lane maxima, descending
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const uint32_t o = __shfl_xor_sync(0xffffffffu, m, stride);
+        const bool keep_max = ((lane & stride) == 0) == ((lane & size) == 0);
+        m = keep_max ? max(m, o) : min(m, o);
+      }
+    if (lane < k) P.lane_max[warp * k + lane] = m;
+    if (tid == 0) {
+      P.t0 = 0u;
+      P.ncand = 0;
     }
-    if (rank == k - 1) P.t0 = me;
+    __syncthreads();
+    if (tid < offered) {
+      // place among the offered maxima, ties by position: unique
+      const uint32_t me = P.lane_max[tid];
+      int rank = 0;
+      for (int j = 0; j < offered; ++j) {
+        const uint32_t o = P.lane_max[j];
+        rank += (o > me || (o == me && j < tid)) ? 1 : 0;
+      }
+      if (rank == k - 1) P.t0 = me;
+    }
+    __syncthreads();
+    t0 = P.t0;
+  } else {
+    if (tid == 0) P.ncand = 0;
+    if (__syncthreads_count(valid != 0u) < k) {
+      radix();
+      return;
+    }
+    t0 = block_kth_key(m, valid != 0u, k, P.radix);
   }
-  __syncthreads();
-  const uint32_t t0 = P.t0;
   if (t0 == 0u) {
     radix();
     return;
