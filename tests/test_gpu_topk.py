@@ -55,3 +55,45 @@ def test_topk_all_ties_takes_lowest_indices():
     s = np.full((2, 20000), 1.5, np.float32)
     idx, _ = topk_native(torch.from_numpy(s).cuda(), 32)
     assert np.array_equal(idx.cpu().numpy()[0], np.arange(32))
+
+
+def _check(s: np.ndarray, k: int):
+    idx, val = topk_native(torch.from_numpy(s).cuda(), k)
+    ri, rv = reference_topk(s, k)
+    np.testing.assert_array_equal(idx.cpu().numpy(), ri)
+    np.testing.assert_array_equal(val.cpu().numpy(), rv)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [1, 2, 7, 16, 31, 32])
+def test_topk_every_k_ragged_n(k):
+    """A slice's k best are found among the keys at or above the k-th largest
+    thread maximum; the last slice is ragged."""
+    need_gpu()
+    rng = np.random.default_rng(100 + k)
+    _check((rng.standard_normal((3, 8192 * 2 + 4099)) * 3).astype(np.float32), k)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["few_levels", "one_thread_peaks", "inf_and_sparse", "tiny_n"])
+def test_topk_adversarial_keys(kind):
+    """Ties crowding the threshold (the candidate list overflows and the radix
+    select over all keys decides), the best keys all held by one thread,
+    infinities among sparse peaks, and fewer entries than threads."""
+    need_gpu()
+    rng = np.random.default_rng(7)
+    if kind == "few_levels":
+        s = rng.integers(0, 4, (2, 65536)).astype(np.float32)
+    elif kind == "one_thread_peaks":
+        s = rng.random((2, 65536)).astype(np.float32)
+        s[:, 3::256][:, :40] += 10.0  # slice 0, thread 3: 32 keys; slice 1: 8 more
+    elif kind == "inf_and_sparse":
+        s = np.zeros((2, 50000), np.float32)
+        s[:, rng.choice(50000, 9, replace=False)] = rng.random(9).astype(np.float32) + 1
+        s[0, 17] = np.inf
+        s[1, 4000:4100] = -np.inf
+        s[1, 33] = np.inf
+    else:
+        s = rng.random((4, 20)).astype(np.float32)
+        s[:, 3] = s[:, 5]
+    _check(s, min(32, s.shape[1]))
