@@ -270,10 +270,19 @@ class LearnedSBLPlan:
         flat = self.input_buffer.reshape(self.batch, *self.input_buffer.shape[-2:])
         self._fb = min(int(fallback_batch), self.batch)
         self._plain = make(flat[: self._fb].clone(), grid_shape, polish_size=polish_size, warmup=warmup)
+        # a replay usually has one or two failures: a small plan solves them
+        # at the latency of one scene instead of a 16-scene solve
+        small = min(2, self._fb)
+        self._plain_small = (make(flat[:small].clone(), grid_shape, polish_size=polish_size, warmup=warmup)
+                             if small < self._fb else self._plain)
         self.gamma_residual_max = gamma_residual_max
         self.noise_residual_max = noise_residual_max
         self.fallbacks = 0
         self.passed: Tensor | None = None
+        self._check_graph: torch.cuda.CUDAGraph | None = None
+        self._check_key: tuple | None = None
+        self._check_out: Tensor | None = None
+        self._rows: dict[int, tuple[list[Tensor], list[Tensor]]] = {}
 
     @property
     def result(self):
@@ -289,26 +298,62 @@ class LearnedSBLPlan:
             ok &= o["fixed_budget_noise_residual"] <= self.noise_residual_max
         return ok
 
+    def _captured_check(self) -> Tensor:
+        """check() as one graph launch (its inputs are the warm plan's
+        graph-owned outputs); recaptured when the thresholds change."""
+        key = (self.gamma_residual_max, self.noise_residual_max)
+        if self._check_graph is None or self._check_key != key:
+            stream = torch.cuda.Stream(self.input_buffer.device)
+            stream.wait_stream(torch.cuda.current_stream(self.input_buffer.device))
+            with torch.cuda.stream(stream):
+                self.check()  # warm-up outside the capture
+                graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(graph, stream=stream):
+                    out = self.check()
+            torch.cuda.current_stream(self.input_buffer.device).wait_stream(stream)
+            self._check_graph, self._check_key, self._check_out = graph, key, out
+        self._check_graph.replay()
+        return self._check_out
+
+    def _row_views(self, plan) -> tuple[list[Tensor], list[Tensor]]:
+        """The per-scene fields of the warm and of a fallback plan's results,
+        as (batch-leading) tensor pairs; the results are graph-owned, so the
+        pairs are found once per fallback plan."""
+        key = id(plan)
+        if key not in self._rows:
+            res, pres = self._warm.result, plan.result
+            nb = plan.input_buffer.reshape(-1, *plan.input_buffer.shape[-2:]).shape[0]
+            dst, src = [], []
+            for f in fields(res):
+                v, pv = getattr(res, f.name), getattr(pres, f.name)
+                if (isinstance(v, Tensor) and isinstance(pv, Tensor) and v.ndim >= 1
+                        and v.shape[1:] == pv.shape[1:] and v.shape[0] == self.batch and pv.shape[0] == nb):
+                    dst.append(v)
+                    src.append(pv)
+            self._rows[key] = (dst, src)
+        return self._rows[key]
+
     def replay(self, data: Tensor | None = None, *, synchronize: bool = False, fallback: bool = True):
         res = self._warm.replay(data, synchronize=False)
-        self.passed = self.check()
+        self.passed = self._captured_check()
         self.fallbacks = 0
         if fallback:
-            bad = (~self.passed).nonzero().flatten()
-            self.fallbacks = int(bad.numel())
+            bad = (~self.passed).nonzero().flatten().tolist()
+            self.fallbacks = len(bad)
             flat = self.input_buffer.reshape(self.batch, *self.input_buffer.shape[-2:])
             for c0 in range(0, self.fallbacks, self._fb):
-                # the failed scenes, in groups of the fallback plan's batch (the
+                # the failed scenes, in groups of a fallback plan's batch (the
                 # last group padded with its first scene)
                 idx = bad[c0:c0 + self._fb]
-                take = torch.cat([idx, idx[:1].expand(self._fb - idx.numel())])
-                plain = self._plain.replay(flat[take])
-                for f in fields(res):
-                    v, pv = getattr(res, f.name), getattr(plain, f.name)
-                    if (isinstance(v, Tensor) and isinstance(pv, Tensor) and v.ndim >= 1
-                            and v.shape[1:] == pv.shape[1:] and v.shape[0] == self.batch
-                            and pv.shape[0] == self._fb):
-                        v[idx] = pv[: idx.numel()]
+                plan = self._plain_small if len(idx) <= self._plain_small.input_buffer.reshape(
+                    -1, *flat.shape[-2:]).shape[0] else self._plain
+                pin = plan.input_buffer.reshape(-1, *flat.shape[-2:])
+                take = idx + idx[:1] * (pin.shape[0] - len(idx))
+                torch._foreach_copy_([pin[j] for j in range(len(take))], [flat[i] for i in take])
+                plan.replay()
+                dst, src = self._row_views(plan)
+                torch._foreach_copy_([v[i] for v in dst for i in idx],
+                                     [pv[j] for pv in src for j in range(len(idx))])
         if synchronize:
             torch.cuda.synchronize(self.input_buffer.device)
         return res

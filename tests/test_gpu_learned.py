@@ -75,6 +75,34 @@ def test_fallback_returns_the_plain_plan_result():
 
 
 @pytest.mark.gpu
+def test_one_failure_goes_through_the_small_fallback_plan():
+    """A single failed scene is re-solved by the 2-scene plain plan; its rows
+    become the plain result, every other row keeps the warm result."""
+    need_gpu()
+    from fbme_b200.learned import make_learned_plan
+    from torch_sbl_fastest_stable import make_stable_plan
+
+    y, _ = _batch(8, 2_150_000)
+    yt = torch.from_numpy(y).cuda()
+    learned = make_learned_plan(yt, GRID, warmup=1)
+    warm = learned.replay(yt, synchronize=True, fallback=False)
+    x_warm, nle_warm = warm.x.clone(), warm.negative_log_evidence.clone()
+    mask = torch.ones(8, dtype=torch.bool, device=yt.device)
+    mask[5] = False
+    learned._captured_check = lambda: mask
+    r = learned.replay(yt, synchronize=True)
+    assert learned.fallbacks == 1
+    assert learned._plain_small is not learned._plain
+    p = make_stable_plan(yt, GRID, warmup=1).replay(yt, synchronize=True)
+    assert torch.equal(r.x[5], p.x[5])
+    assert torch.equal(r.posterior_variance[5], p.posterior_variance[5])
+    assert torch.equal(r.negative_log_evidence[5], p.negative_log_evidence[5])
+    keep = [i for i in range(8) if i != 5]
+    assert torch.equal(r.x[keep], x_warm[keep])
+    assert torch.equal(r.negative_log_evidence[keep], nle_warm[keep])
+
+
+@pytest.mark.gpu
 def test_warm_started_solve_matches_oracle_from_the_network_prior():
     """The warm plan is the plain algorithm started from the network's prior:
     the oracle restatement given the same prior agrees (x within 1e-4
