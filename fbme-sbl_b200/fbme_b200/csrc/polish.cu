@@ -157,39 +157,54 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   // (q, i] -- independent updates instead of one dot-product chain per
   // entry.  Every entry receives its terms in the same order q = 0, 1, ...
   // as the dot-product form.
-  // Each lane touches only its own row inside the loop; the pivot and the
-  // column entries L[k][q] reach the other lanes by shuffles.
+  // Each lane writes only its own row inside the loop.  Every lane computes
+  // the pivot from the diagonal entry; the column entries L[k][q] reach
+  // the other lanes through shared memory.  A row's diagonal takes its last
+  // update before the row updates of the step, so the next pivot's entry
+  // is final, and is loaded, before those updates.
   int status = 0;
   __syncwarp();
+  float dnext = K > 0 ? M[0][0].x : 1.0f;
   for (int q = 0; q < K; ++q) {
-    float piv = 0.f;
-    if (lane == q) {
-      float sdiag = M[q][q].x;
-      if (!(sdiag > 0.f)) {
-        status |= isfinite(sdiag) ? FBME_STATUS_CHOLESKY : FBME_STATUS_NONFINITE;
-        sdiag = kTinyP;
-      }
-      piv = sqrtf(sdiag);
-      M[q][q] = make_float2(piv, 0.f);
+    float sdiag = dnext;
+    if (!(sdiag > 0.f)) {
+      if (lane == q) status |= isfinite(sdiag) ? FBME_STATUS_CHOLESKY : FBME_STATUS_NONFINITE;
+      sdiag = kTinyP;
     }
-    const float rq = 1.0f / __shfl_sync(0xffffffffu, piv, q);
+    const float piv = sqrtf(sdiag);
+    const float rq = 1.0f / piv;
+    if (lane == q) M[q][q] = make_float2(piv, 0.f);
     float2 a = make_float2(0.f, 0.f);
     if (on && lane > q) {
       const float2 v = M[lane][q];
       a = make_float2(v.x * rq, v.y * rq);
       M[lane][q] = a;
+      M[lane][lane].x -= abs2(a);
     }
-#pragma unroll 4
-    for (int k = q + 1; k < K; ++k) {
-      const float bx = __shfl_sync(0xffffffffu, a.x, k), by = __shfl_sync(0xffffffffu, a.y, k);
-      if (on && k < lane) {
-        float2 v = M[lane][k];
-        v.x -= a.x * bx + a.y * by;  // a * conj(b)
-        v.y -= a.y * bx - a.x * by;
-        M[lane][k] = v;
-      }
+    // column q reaches the other lanes through shared memory (X is free
+    // until the inverse factor); the row updates then go in batches of 8:
+    // all loads, then the arithmetic, then the stores, so the batch's
+    // shared-memory round trips overlap instead of running one by one
+    X[0][lane] = a;
+    __syncwarp();
+    if (q + 1 < K) dnext = M[q + 1][q + 1].x;
+    for (int k0 = q + 1; k0 < K; k0 += 8) {
+      float2 b[8], v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (on && k0 + u < lane) {
+          b[u] = X[0][k0 + u];
+          v[u] = M[lane][k0 + u];
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (on && k0 + u < lane) {
+          v[u].x -= a.x * b[u].x + a.y * b[u].y;  // a * conj(b)
+          v[u].y -= a.y * b[u].x - a.x * b[u].y;
+          M[lane][k0 + u] = v[u];
+        }
     }
-    if (on && lane > q) M[lane][lane].x -= abs2(a);
+    __syncwarp();
   }
   __syncwarp();
   status = __reduce_or_sync(0xffffffffu, status);
@@ -229,6 +244,7 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
     float2(*__restrict__ Xc)[33] = X;
     if (on)
       for (int i = 0; i < K; ++i) Xc[i][lane] = make_float2(0.f, 0.f);
+    float2 carry = make_float2(0.f, 0.f);  // Xc[q][lane], kept from step q-1
     for (int q = 0; q < K; ++q) {
       const float rlq = __shfl_sync(0xffffffffu, rl, q);
       if (on && lane <= q) {
@@ -236,18 +252,27 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
         if (lane == q) {
           xq = make_float2(rlq, 0.f);
         } else {
-          const float2 acc = Xc[q][lane];
-          xq = make_float2(-acc.x * rlq, -acc.y * rlq);
+          xq = make_float2(-carry.x * rlq, -carry.y * rlq);
         }
         Xc[q][lane] = xq;
         eqv += abs2(xq);
-#pragma unroll 4
-        for (int i = q + 1; i < K; ++i) {
-          const float2 l = L[i][q];
-          float2 acc = Xc[i][lane];
-          acc.x += l.x * xq.x - l.y * xq.y;
-          acc.y += l.x * xq.y + l.y * xq.x;
-          Xc[i][lane] = acc;
+        // batches of 8 rows: loads, arithmetic, stores (as the Cholesky)
+        for (int i0 = q + 1; i0 < K; i0 += 8) {
+          float2 l[8], acc[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (i0 + u < K) {
+              l[u] = L[i0 + u][q];
+              acc[u] = Xc[i0 + u][lane];
+            }
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (i0 + u < K) {
+              acc[u].x += l[u].x * xq.x - l[u].y * xq.y;
+              acc[u].y += l[u].x * xq.y + l[u].y * xq.x;
+              Xc[i0 + u][lane] = acc[u];
+            }
+          if (i0 == q + 1) carry = acc[0];
         }
       }
     }
