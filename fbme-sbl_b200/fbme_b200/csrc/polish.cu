@@ -780,44 +780,45 @@ __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOut
   }
 }
 
-// N-space outputs: zero mean, floor variance and 1/floor precision off the
-// active set, then the active entries.
-__global__ void output_fill_kernel(BatchShape s, Scalars sc, FbmeOutputs out) {
+// N-space outputs in one pass: zero mean, floor variance and 1/floor
+// precision off the active set, and the active entries.  Block b of a scene
+// owns the contiguous pixel range [e0, e1): it fills the range, then its
+// threads k < K write active atom k where it falls inside the range, so no
+// other block touches those pixels and one launch replaces fill + scatter.
+__global__ void __launch_bounds__(256) output_kernel(PolishArgs A, FbmeOutputs out) {
+  const BatchShape& s = A.s;
   const long long N = s.n();
   const int scene = blockIdx.y;
-  const float fl = sc.floor_[scene];
+  const int K = A.c.polish_size;
+  const float fl = A.p.sc.floor_[scene];
   const float inv = 1.0f / fl;
+  const long long chunk = (N + gridDim.x - 1) / gridDim.x;
+  const long long e0 = blockIdx.x * chunk, e1 = min(N, e0 + chunk);
   float2* x = reinterpret_cast<float2*>(out.x) + scene * N;
   float* pv = out.posterior_variance + scene * N;
   float* pr = out.precision + scene * N;
   uint8_t* mk = out.support_mask ? out.support_mask + scene * N : nullptr;
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < N;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     x[e] = make_float2(0.f, 0.f);
     pv[e] = fl;
     pr[e] = inv;
     if (mk) mk[e] = 0;
   }
-}
-
-__global__ void __launch_bounds__(32) output_scatter_kernel(PolishArgs A, FbmeOutputs out) {
-  const int lane = threadIdx.x & 31;
-  const int scene = blockIdx.x;
-  const int K = A.c.polish_size;
-  if (lane >= K) return;
-  const long long N = A.s.n();
+  __syncthreads();
+  const int k = threadIdx.x;
+  if (k >= K) return;
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
-  const int idx = ps->active[lane];
-  const float2 mu = ps->best_mean[lane];
-  const float pv = ps->best_pv[lane];
-  const long long e = scene * N + idx;
-  reinterpret_cast<float2*>(out.x)[e] = mu;
-  if (out.active_values) reinterpret_cast<float2*>(out.active_values)[scene * K + lane] = mu;
-  out.posterior_variance[e] = pv;
-  out.precision[e] = 1.0f / ps->best_gamma[lane];
-  if (out.support_mask && A.c.false_alarm > 0.f) {
+  const int idx = ps->active[k];
+  const float2 mu = ps->best_mean[k];
+  if (blockIdx.x == 0 && out.active_values) reinterpret_cast<float2*>(out.active_values)[scene * K + k] = mu;
+  if (idx < e0 || idx >= e1) return;
+  const float apv = ps->best_pv[k];
+  x[idx] = mu;
+  pv[idx] = apv;
+  pr[idx] = 1.0f / ps->best_gamma[k];
+  if (mk && A.c.false_alarm > 0.f) {
     const float thr = static_cast<float>(log(static_cast<double>(N) / A.c.false_alarm));
-    out.support_mask[e] = (abs_sq(mu) / fmaxf(pv, kTinyP)) > thr;
+    mk[idx] = (abs_sq(mu) / fmaxf(apv, kTinyP)) > thr;
   }
 }
 
@@ -880,9 +881,7 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
   }
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, dsm, st>>>(A, out)));
   const int fb = static_cast<int>((s.n() + 2047) / 2048);
-  FBME_TIMED(prof, FBME_GROUP_OUTPUT,
-             (output_fill_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(s, p.sc, out)));
-  FBME_TIMED(prof, FBME_GROUP_OUTPUT, (output_scatter_kernel<<<s.B, 32, 0, st>>>(A, out)));
+  FBME_TIMED(prof, FBME_GROUP_OUTPUT, (output_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(A, out)));
 }
 
 }  // namespace fbme
