@@ -242,3 +242,37 @@ def test_samples_at_an_8_byte_offset():
     torch.cuda.synchronize()
     assert torch.equal(eng.out["x"], x0)
     eng.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [((32, 320), (16, 100)), ((48, 63), (20, 30))],
+                         ids=["32x320_16x100", "48x63_20x30"])
+def test_exchange_tile_classes_match_oracle(shape):
+    """The residual-exchange scoring has one tile class per N2 range; rows
+    wider than 256 (the 16-row class) and odd N2 (8-byte row staging) meet
+    the parity bar against the oracle, with the Stable profile's exchange."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from oracle import fbme_oracle as O
+
+    dev = torch.device("cuda", 0)
+    g = shape[0]
+    sc = _scenes([shape] * 3, 2500)
+    y_np = np.stack([s.y for s in sc])
+    eng = FBMEEngine(3, shape[0], shape[1], _cfg(), dev)
+    eng.run(torch.from_numpy(y_np).to(dev).reshape(3, -1).contiguous())
+    torch.cuda.synchronize()
+    assert int(eng.out["status"].abs().sum()) == 0
+    x = eng.out["x"].cpu().numpy().reshape(3, -1)
+    pv = eng.out["posterior_variance"].cpu().numpy().reshape(3, -1)
+    ref = O.fbme_solve(y_np, g, "stable")
+    xr = ref["x"].reshape(3, -1)
+    pvr = ref["posterior_variance"].reshape(3, -1)
+    for i in range(3):
+        assert set(np.flatnonzero(x[i])) == set(np.flatnonzero(xr[i])), i
+        assert rel_l2(x[i], xr[i]) < X_TOL, i
+        sup = xr[i] != 0
+        assert np.max(np.abs(pv[i][sup] - pvr[i][sup]) / pvr[i][sup]) < PV_TOL, i
+    np.testing.assert_array_equal(eng.out["support_exchanges_accepted"].cpu().numpy(),
+                                  np.asarray(ref["support_exchanges_accepted"]).reshape(-1))
+    eng.close()
