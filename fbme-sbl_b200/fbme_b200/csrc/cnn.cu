@@ -288,7 +288,9 @@ conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, voi
   }
   // All of a thread's global loads are issued before any is stored.
   constexpr int IT = (NP + kSmallThreads - 1) / kSmallThreads;
-  using LoadT = typename std::conditional<CIN == 8, uint4, uint32_t>::type;
+  // CSTR == 1: channel 0 alone, one BF16 per pixel (channel 1 from f1part)
+  using LoadT = typename std::conditional<CIN == 8, uint4,
+                                          typename std::conditional<CSTR == 1, uint16_t, uint32_t>::type>::type;
   LoadT v[IT];
   bool in[IT];
 #pragma unroll
@@ -308,6 +310,9 @@ conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, voi
 #pragma unroll
       for (int k = 0; k < 4; ++k)
         xs2[k * NP + pix] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[k]));
+    } else if constexpr (CSTR == 1) {
+      const float f0 = __bfloat162float(__ushort_as_bfloat16(v[j]));
+      xs2[pix] = make_float2(f0, in[j] ? c1 : 0.f);
     } else {
       const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v[j]));
       xs2[pix] = make_float2(f.x, f1part ? (in[j] ? c1 : 0.f) : f.y);
@@ -508,8 +513,10 @@ __global__ void adam_kernel(float* p, const float* g, float* m, float* v, int n,
 // Features of the backprojection (see the header comment of the oracle
 // restatement): pass 0 sums |A^H y|^2, pass 1 writes f0 and sums it, pass 2
 // writes f1 = mean f0.  part: [B][64] FP64 block partials per pass.
+// compact (inference): pass 1 writes f0 alone, one BF16 per pixel, to the
+// start of x8 -- the network's first layer takes f1 from the partials.
 __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* bp, int B, long long N,
-                                                       __nv_bfloat16* x8, double* part) {
+                                                       __nv_bfloat16* x8, double* part, bool compact = false) {
   __shared__ double red[32];
   const int b = blockIdx.y;
   double acc = 0.0;
@@ -531,10 +538,14 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
     } else if (pass == 1) {
       const float f0 = logf(static_cast<float>(e / mean) + 1e-3f);
       acc += f0;
-      uint4 w;
-      w.x = pack_bf16x2(f0, 0.f);
-      w.y = w.z = w.w = 0u;
-      *reinterpret_cast<uint4*>(x8 + (b * N + n) * 8) = w;
+      if (compact) {
+        x8[b * N + n] = __float2bfloat16_rn(f0);
+      } else {
+        uint4 w;
+        w.x = pack_bf16x2(f0, 0.f);
+        w.y = w.z = w.w = 0u;
+        *reinterpret_cast<uint4*>(x8 + (b * N + n) * 8) = w;
+      }
     } else {
       x8[(b * N + n) * 8 + 1] = __float2bfloat16_rn(static_cast<float>(f1));
     }
@@ -653,7 +664,8 @@ int feature_parts(int H, int W) {
 }
 // Passes 0 and 1 (the energy mean, f0 and its partial sums); pass 2 stores
 // the f1 channel, which only the backward pass reads from the workspace.
-void features_passes(const float2* bp, int B, int H, int W, void* ws, int passes, cudaStream_t st) {
+void features_passes(const float2* bp, int B, int H, int W, void* ws, int passes, cudaStream_t st,
+                     bool compact = false) {
   using namespace cnn;
   const CnnLayout L = cnn_layout(B, H, W);
   uint8_t* w = static_cast<uint8_t*>(ws);
@@ -661,7 +673,7 @@ void features_passes(const float2* bp, int B, int H, int W, void* ws, int passes
   auto* fpart = reinterpret_cast<double*>(w + L.fpart);
   for (int pass = 0; pass < passes; ++pass)
     features_kernel<<<dim3(feature_parts(H, W), B), 256, 0, st>>>(pass, bp, B, static_cast<long long>(H) * W,
-                                                                  x8, fpart);
+                                                                  x8, fpart, compact);
 }
 }  // namespace
 
@@ -671,7 +683,8 @@ void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t 
 
 // Forward pass from the features in the workspace; the output [B][H][W]
 // stays in the workspace (for cnn_backward) and is copied to `out` if given.
-void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st) {
+void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st,
+                 bool compact) {
   using namespace cnn;
   const CnnLayout L = cnn_layout(B, H, W);
   uint8_t* w = static_cast<uint8_t*>(ws);
@@ -682,8 +695,12 @@ void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out,
   auto* h1 = reinterpret_cast<__nv_bfloat16*>(w + L.h1);
   auto* h2 = reinterpret_cast<__nv_bfloat16*>(w + L.h2);
   const dim3 grid_small((W + kSmallTW - 1) / kSmallTW, (H + kSmallTH - 1) / kSmallTH, B);
-  conv_small_kernel<kIn, kInP, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
-      x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
+  if (compact)
+    conv_small_kernel<kIn, 1, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
+        x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
+  else
+    conv_small_kernel<kIn, kInP, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
+        x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
   conv3x3_kernel<__nv_bfloat16, kHid, kHid, kOutReluBf16><<<grid, kConvThreads, 0, st>>>(
       h1, nullptr, P.wt2, P.b2, h2, H, W);
   float* wout = reinterpret_cast<float*>(w + L.out);  // kept for cnn_backward
@@ -745,10 +762,11 @@ void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, 
                     const float* data_power, const float* floor_, float* gamma, double* upart,
                     int nblocks, cudaStream_t st) {
   using namespace cnn;
-  features_passes(bp, B, H, W, ws, 2, st);
+  // f0 alone, one BF16 per pixel (the first layer takes f1 from the partials)
+  features_passes(bp, B, H, W, ws, 2, st, true);
   const CnnLayout L = cnn_layout(B, H, W);
   float* out = reinterpret_cast<float*>(static_cast<uint8_t*>(ws) + L.out);
-  cnn_forward(params, B, H, W, ws, out, st);
+  cnn_forward(params, B, H, W, ws, out, st, true);
   warm_prior_kernel<<<dim3(nblocks, B), 256, 0, st>>>(out, static_cast<long long>(H) * W, data_power,
                                                       floor_, gamma, upart);
 }

@@ -155,7 +155,8 @@ int cnn_param_count();
 size_t cnn_workspace_bytes(long long B, long long H, long long W);
 const char* cnn_check(long long B, long long H, long long W);
 void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t st);
-void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st);
+void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st,
+                 bool compact = false);
 void cnn_backward(const float* target, int B, int H, int W, void* ws, float* grad, double* loss_out,
                   cudaStream_t st);
 void cnn_adam(float* params, const float* grad, float* m, float* v, int step, float lr, cudaStream_t st);
