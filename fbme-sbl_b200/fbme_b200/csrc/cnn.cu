@@ -253,6 +253,90 @@ conv3x3_kernel(const TIn* x, const __nv_bfloat16* mask, const __nv_bfloat16* wt,
   }
 }
 
+// Layer 2 forward (8 -> 8 channels, relu, BF16 NHWC output) on a 16 x 16
+// pixel tile: 4 warps x 4 rows of 16 pixels.  An A fragment is one
+// ldmatrix.x4 from the halo tile -- a matrix row is one pixel's 8 channels
+// at one tap (16 bytes), so the four 8x8 matrices are pixels 0-7 / 8-15 at
+// taps 2ks and 2ks+1 -- and the weight fragments and the bias stay in
+// registers.  The MMA operands and their order are those of
+// conv3x3_kernel<bf16, 8, 8, kOutReluBf16>, so the output is the same bit
+// for bit, with a quarter of its shared-memory loads and half its halo
+// overhead per pixel.
+constexpr int kF8Rows = 16, kF8Cols = 16;
+FBME_DEV void ldmatrix_x4(uint32_t addr, uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+               : "r"(addr));
+}
+
+__global__ void __launch_bounds__(128) conv3x3_fwd8_kernel(const __nv_bfloat16* x, const __nv_bfloat16* wt,
+                                                          const float* bias, __nv_bfloat16* out, int H, int W) {
+  constexpr int KP = kpad(8);
+  constexpr int HW = kF8Rows + 2, WW = kF8Cols + 2, NP = HW * WW;
+  __shared__ uint4 xs[NP + 1];  // halo tile, one pixel (8 BF16) each, then a zero pixel for padded taps
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int x0 = blockIdx.x * kF8Cols, y0 = blockIdx.y * kF8Rows, b = blockIdx.z;
+  const long long img = static_cast<long long>(b) * H * W;
+  constexpr int IT = (NP + 127) / 128;
+  uint4 v[IT];
+#pragma unroll
+  for (int j = 0; j < IT; ++j) {
+    const int i = tid + j * 128;
+    const int gy = y0 - 1 + i / WW, gx = x0 - 1 + i % WW;
+    v[j] = make_uint4(0u, 0u, 0u, 0u);
+    if (i < NP && gy >= 0 && gy < H && gx >= 0 && gx < W)
+      v[j] = *reinterpret_cast<const uint4*>(x + (img + static_cast<long long>(gy) * W + gx) * 8);
+  }
+  const uint32_t* wt32 = reinterpret_cast<const uint32_t*>(wt);
+  uint32_t bq[KP / 16][2];
+#pragma unroll
+  for (int ks = 0; ks < KP / 16; ++ks) {
+    bq[ks][0] = wt32[(g * KP + ks * 16 + t * 2) / 2];
+    bq[ks][1] = wt32[(g * KP + ks * 16 + t * 2 + 8) / 2];
+  }
+  const float bias0 = bias[2 * t], bias1 = bias[2 * t + 1];
+#pragma unroll
+  for (int j = 0; j < IT; ++j) {
+    const int i = tid + j * 128;
+    if (i < NP) xs[i] = v[j];
+  }
+  if (tid == 0) xs[NP] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  // ldmatrix rows: lanes 8m..8m+7 address matrix m = (pixel half m&1, tap 2ks + (m>>1))
+  const int mj = lane >> 3, pr = (lane & 7) + (mj & 1) * 8;
+  float acc[4][4];
+#pragma unroll
+  for (int mf = 0; mf < 4; ++mf)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[mf][j] = 0.f;
+#pragma unroll
+  for (int ks = 0; ks < KP / 16; ++ks) {
+    const int tap = 2 * ks + (mj >> 1);
+#pragma unroll
+    for (int mf = 0; mf < 4; ++mf) {
+      const int yy = warp * 4 + mf;
+      const int pix = tap < 9 ? (yy + tap / 3) * WW + pr + tap % 3 : NP;
+      uint32_t a0, a1, a2, a3;
+      ldmatrix_x4(smem_u32(&xs[pix]), a0, a1, a2, a3);
+      mma_bf16_16816(acc[mf], a0, a1, a2, a3, bq[ks][0], bq[ks][1]);
+    }
+  }
+#pragma unroll
+  for (int mf = 0; mf < 4; ++mf) {
+    const int gy = y0 + warp * 4 + mf;
+    if (gy >= H) continue;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int gx = x0 + g + half * 8;
+      if (gx >= W) continue;
+      const long long pix = img + static_cast<long long>(gy) * W + gx;
+      const float v0 = acc[mf][half * 2] + bias0, v1 = acc[mf][half * 2 + 1] + bias1;
+      reinterpret_cast<uint32_t*>(out + pix * 8 + 2 * t)[0] = pack_bf16x2(fmaxf(v0, 0.f), fmaxf(v1, 0.f));
+    }
+  }
+}
+
 // Layers with few channels on the CUDA cores: 3x3 convolution, zero
 // padding 1, from CIN channels of an NHWC BF16 input (stride CSTR) to COUT
 // outputs over a 16 x 32 tile; each of the 128 threads computes 4 pixels
@@ -701,8 +785,9 @@ void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out,
   else
     conv_small_kernel<kIn, kInP, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
         x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
-  conv3x3_kernel<__nv_bfloat16, kHid, kHid, kOutReluBf16><<<grid, kConvThreads, 0, st>>>(
-      h1, nullptr, P.wt2, P.b2, h2, H, W);
+  static_assert(kHid == 8, "conv3x3_fwd8_kernel is the 8 -> 8 layer");
+  conv3x3_fwd8_kernel<<<dim3((W + kF8Cols - 1) / kF8Cols, (H + kF8Rows - 1) / kF8Rows, B), 128, 0, st>>>(
+      h1, P.wt2, P.b2, h2, H, W);
   float* wout = reinterpret_cast<float*>(w + L.out);  // kept for cnn_backward
   conv_small_kernel<kHid, kHid, 1, false><<<grid_small, kSmallThreads, 0, st>>>(h2, P.w3f, P.b3, wout, H, W);
   if (out && out != wout)
