@@ -3,7 +3,9 @@
 // Replaces torch.topk(score, K) at torch_sbl/solver.py:1931 (active set)
 // and 4410 (residual-exchange additions).  Two launches:
 //   topk_blocks_kernel  each CTA reduces an 8192-key slice of one scene to
-//                       its k best (radix select on register-held keys);
+//                       its k best: the keys at or above the k-th largest
+//                       thread maximum, ranked by counting (radix select
+//                       over all register-held keys as the fallback);
 //   topk_merge_kernel   one CTA per scene sorts the candidates as 64-bit
 //                       (key, ~index) words and keeps the k first, so the
 //                       result is the exact top-k, largest first, ties by

@@ -228,15 +228,15 @@ def attach_warm_start(engine: FBMEEngine, net: WarmStartNet) -> Tensor:
 class LearnedSBLPlan:
     """Warm-started FBME plan with the plain plan as fallback.
 
-    Two CUDA graphs: the warm-started solve of the whole batch (the
-    network's prior, ``sweeps`` UAMP sweeps, the profile's polish) and the
-    plain locked plan of the same profile for ``fallback_batch`` scenes.
-    ``replay`` launches the warm graph, applies the evidence / residual
-    check per scene, solves the scenes that fail it with the plain plan (in
-    groups of ``fallback_batch``) and returns the plain results for them
-    (this reads the failure count on the host, so a replay with fallback
-    synchronises the stream).  Results are graph-owned, as for the plain
-    plans.
+    CUDA graphs: the warm-started solve of the whole batch (the network's
+    prior, ``sweeps`` UAMP sweeps, the profile's polish), the per-scene
+    check, and the plain locked plans of the same profile for
+    ``fallback_batch`` scenes and for 2.  ``replay`` launches the warm graph
+    and the check, solves the scenes that fail it with a plain plan (the
+    2-scene one for one or two failures, else groups of ``fallback_batch``)
+    and returns the plain results for them (this reads the failure count on
+    the host, so a replay with fallback synchronises the stream).  Results
+    are graph-owned, as for the plain plans.
 
     Check (per scene): finite negative log evidence, status 0, monotone
     evidence trace, and fixed-point residuals of the prior and the noise no
