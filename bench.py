@@ -44,7 +44,7 @@ def _args() -> argparse.Namespace:
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--batch", type=int, default=256, help="scenes per step per GPU")
+    ap.add_argument("--batch", type=int, default=512, help="scenes per step per GPU")
     ap.add_argument("--profile", choices=("stable", "fast"), default="stable")
     ap.add_argument("--cpu-sample", type=int, default=32, help="scenes in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -515,7 +515,7 @@ def run_ours(a: argparse.Namespace) -> None:
         cpu = cpu_baseline(a.cpu_sample, a.profile)
     learned = None
     if world == 1 and not a.no_learned:
-        learned = learned_section(device, min(a.steps, 20))
+        learned = learned_section(device, min(a.steps, 20), a.batch)
     uneven = None
     if world == 1 and not a.no_uneven:
         uneven = uneven_section(device, min(a.steps, 20))
