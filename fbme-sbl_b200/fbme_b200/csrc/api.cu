@@ -541,6 +541,18 @@ ScatterArgs scatter_args(const FbmePlan* P, const FbmeOutputs& c) {
   return a;
 }
 
+// Polish and outputs of one bucket on `st` (its UAMP stage done).  The
+// status words of an uneven plan's buckets already live in the staging
+// area the outputs point at.
+void polish_bucket(const Bucket& k, const float2* y, const FbmeOutputs& out, cudaStream_t st,
+                   fbme::Profiler* prof = nullptr) {
+  fbme::PolishBuffers p = k.p;
+  p.y = y;
+  fbme::polish_run(k.s, k.dc, p, out, st, prof);
+  if (out.status != k.status)
+    cudaMemcpyAsync(out.status, k.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
+}
+
 // The whole solve of one bucket on `st`: status reset, UAMP, polish and
 // outputs.
 void run_bucket(const Bucket& k, const float2* y, const FbmeOutputs& out, cudaStream_t st,
@@ -549,10 +561,7 @@ void run_bucket(const Bucket& k, const float2* y, const FbmeOutputs& out, cudaSt
   fbme::UampBuffers u = k.u;
   u.y = y;
   fbme::uamp_run(k.s, k.tables, k.dc, u, st, prof);
-  fbme::PolishBuffers p = k.p;
-  p.y = y;
-  fbme::polish_run(k.s, k.dc, p, out, st, prof);
-  cudaMemcpyAsync(out.status, k.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  polish_bucket(k, y, out, st, prof);
 }
 
 int create_plan(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg,
@@ -582,6 +591,11 @@ int create_plan(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   for (Bucket& k : P->bk) bind_bucket(k, P->ws, st);
   if (P->uneven) {
+    // status words in the bucket-order staging: one reset for all buckets
+    for (Bucket& k : P->bk) {
+      int* sw = reinterpret_cast<int*>(P->ws + P->stg.status) + k.first;
+      k.status = k.u.status = k.p.status = sw;
+    }
     std::vector<SceneMap> m(n_scenes);
     long long csmp = 0, cpix = 0;
     for (int i = 0; i < n_scenes; ++i) {
@@ -766,15 +780,25 @@ int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_
 }
 
 namespace {
-// Gather, buckets, scatter of an uneven plan.  With prof == nullptr the
-// buckets run on their own streams (bucket 0 on `st`), forked from and
-// joined back to `st`; with a profiler they run one after another on `st`.
+// Gather, buckets, scatter of an uneven plan.  The UAMP stage of all
+// buckets runs as merged launches on `st` (one launch per step for every
+// bucket); then, with prof == nullptr, each bucket's polish runs on its own
+// stream (bucket 0 on `st`), forked from and joined back to `st`; with a
+// profiler they run one after another on `st`.
 void replay_uneven(FbmePlan* P, const float2* y, const FbmeOutputs& out, cudaStream_t st,
                    fbme::Profiler* prof) {
   float2* ybuf = reinterpret_cast<float2*>(P->ws + P->stg.y);
   const int gx = 8;
   FBME_TIMED(prof, FBME_GROUP_INIT, (gather_samples_kernel<<<dim3(gx, P->B), 256, 0, st>>>(P->map, y, ybuf)));
   const int nb = static_cast<int>(P->bk.size());
+  cudaMemsetAsync(P->ws + P->stg.status, 0, static_cast<size_t>(P->B) * sizeof(int), st);
+  std::vector<fbme::UampJob> jobs(nb);
+  for (int b = 0; b < nb; ++b) {
+    const Bucket& k = P->bk[b];
+    jobs[b] = fbme::UampJob{k.s, k.tables, k.dc, k.u};
+    jobs[b].u.y = ybuf + k.smp0;
+  }
+  fbme::uamp_run_multi(jobs.data(), nb, st, prof);
   if (!prof) {
     cudaEventRecord(P->events[0], st);
     for (int b = 1; b < nb; ++b) cudaStreamWaitEvent(P->streams[b - 1], P->events[0], 0);
@@ -782,7 +806,7 @@ void replay_uneven(FbmePlan* P, const float2* y, const FbmeOutputs& out, cudaStr
   for (int b = 0; b < nb; ++b) {
     const Bucket& k = P->bk[b];
     cudaStream_t sb = (prof || b == 0) ? st : P->streams[b - 1];
-    run_bucket(k, ybuf + k.smp0, bucket_outputs(P, k, out), sb, prof);
+    polish_bucket(k, ybuf + k.smp0, bucket_outputs(P, k, out), sb, prof);
   }
   if (!prof) {
     for (int b = 1; b < nb; ++b) {

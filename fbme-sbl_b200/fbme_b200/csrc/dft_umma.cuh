@@ -140,9 +140,43 @@ FBME_DEV TileCtx decode_tile(const DftGeom& g, int tile) {
   return t;
 }
 
-template <int A_PARTS, int N_TILE, class Pro, class Epi>
+// One stage launch: geometry, prologue and epilogue policies, status words.
+template <class Pro, class Epi>
+struct StageItem {
+  DftGeom g;
+  Pro pro;
+  Epi epi;
+  int* status;
+};
+
+// Up to NI stage launches of one kind (same policies and tile width) as one
+// persistent launch: item i owns the launch's tiles [tile0[i], tile0[i+1]).
+// Shape buckets of an uneven plan run their stages this way, one launch
+// for all buckets.
+template <class Pro, class Epi, int NI>
+struct StageSet {
+  int n;
+  int tile0[NI + 1];
+  StageItem<Pro, Epi> it[NI];
+  // Item of a tile: the last i with tile0[i] <= tile.
+  FBME_DEV int find(int tile) const {
+    if constexpr (NI == 1) {
+      return 0;
+    } else {
+      int lo = 0, hi = n - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile0[mid] <= tile) lo = mid;
+        else hi = mid - 1;
+      }
+      return lo;
+    }
+  }
+};
+
+template <int A_PARTS, int N_TILE, class Pro, class Epi, int NI>
 __global__ void __launch_bounds__(kDftPersistThreads, 1)
-dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* status) {
+dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
   using C = DftCfg<A_PARTS, N_TILE>;
   extern __shared__ uint8_t smem_dyn[];
   const uint32_t base_u32 = smem_u32(smem_dyn);
@@ -154,7 +188,7 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce_bar + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ntiles = g.n_scenes * g.row_tiles * g.col_tiles;
+  const int ntiles = set.tile0[set.n];
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -190,8 +224,11 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
     bool ok = true;
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-      const TileCtx t = decode_tile(g, tile);
-      int* const st_scene = status ? status + t.scene / g.status_div : nullptr;
+      const int ii = set.find(tile);
+      const DftGeom& g = set.it[ii].g;
+      Pro pro = set.it[ii].pro;  // per tile: accumulators start from the launch's values
+      const TileCtx t = decode_tile(g, tile - set.tile0[ii]);
+      int* const st_scene = set.it[ii].status ? set.it[ii].status + t.scene / g.status_div : nullptr;
       long long erow[kProIters];  // element offset of the row, -1 when outside
 #pragma unroll
       for (int i = 0; i < kProIters; ++i) {
@@ -308,8 +345,10 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
       bool ok = true;
       int it = 0, lt = 0;
       for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
-        const TileCtx t = decode_tile(g, tile);
-        int* const st_scene = status ? status + t.scene / g.status_div : nullptr;
+        const int ii = set.find(tile);
+        const DftGeom& g = set.it[ii].g;
+        const TileCtx t = decode_tile(g, tile - set.tile0[ii]);
+        int* const st_scene = set.it[ii].status ? set.it[ii].status + t.scene / g.status_div : nullptr;
         const int acc = lt & 1, ause = lt >> 1;
         if (lt >= 2) ok = mbar_wait(&acce_bar[acc], (ause - 1) & 1, st_scene);
         if (!ok) break;
@@ -345,8 +384,11 @@ dft_stage_kernel(const __grid_constant__ DftGeom g, Pro pro, Epi epi, int* statu
     bool ok = true;
     int lt = 0;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
-      const TileCtx t = decode_tile(g, tile);
-      int* const st_scene = status ? status + t.scene / g.status_div : nullptr;
+      const int ii = set.find(tile);
+      const DftGeom& g = set.it[ii].g;
+      Epi epi = set.it[ii].epi;
+      const TileCtx t = decode_tile(g, tile - set.tile0[ii]);
+      int* const st_scene = set.it[ii].status ? set.it[ii].status + t.scene / g.status_div : nullptr;
       const int acc = lt & 1;
       ok = mbar_wait(&accf_bar[acc], (lt >> 1) & 1, st_scene);
       tc_fence_after();

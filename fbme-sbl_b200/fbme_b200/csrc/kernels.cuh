@@ -120,6 +120,15 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
               cudaStream_t st, Profiler* prof = nullptr);
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
               cudaStream_t st, Profiler* prof = nullptr);
+// One shape bucket of uamp_run_multi.
+struct UampJob {
+  BatchShape s;
+  DftTables t;
+  DevConfig c;
+  UampBuffers u;
+};
+// uamp_run over several shape buckets with merged launches (no warm start).
+void uamp_run_multi(const UampJob* jobs, int n, cudaStream_t st, Profiler* prof = nullptr);
 
 // Active-set stage.
 struct PolishBuffers {

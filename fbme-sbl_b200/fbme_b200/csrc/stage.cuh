@@ -134,11 +134,6 @@ static inline DftGeom stage_geom(Stage st, const BatchShape& s, const DftTables&
 
 static inline int tiles(const DftGeom& g) { return g.n_scenes * g.row_tiles * g.col_tiles; }
 
-static inline int persistent_grid(const DftGeom& g) {
-  const int t = tiles(g), s = sm_count();
-  return t < s ? t : s;
-}
-
 // Default stage tile width (real output columns): 256 for 3-term
 // products, 128 for 6 (the 6-term operands fill shared memory sooner).
 // Plans may lay their tables out for 64 or 128 columns with 3 terms
@@ -156,17 +151,28 @@ static inline bool dft_n_tile_ok(int terms, int n_tile, const BatchShape& s) {
   return true;
 }
 
-template <int A_PARTS, int N_TILE, class Pro, class Epi>
+template <int A_PARTS, int N_TILE, class Pro, class Epi, int NI>
 static cudaError_t set_attr() {
-  return cudaFuncSetAttribute(dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>,
+  return cudaFuncSetAttribute(dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi, NI>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               DftCfg<A_PARTS, N_TILE>::kSmemBytes);
 }
 
+template <int A_PARTS, int N_TILE, class Pro, class Epi, int NI>
+static void launch_set(const StageSet<Pro, Epi, NI>& set, cudaStream_t st) {
+  const int t = set.tile0[set.n], s = sm_count();
+  dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi, NI>
+      <<<t < s ? t : s, kDftPersistThreads, DftCfg<A_PARTS, N_TILE>::kSmemBytes, st>>>(set);
+}
+
 template <int A_PARTS, int N_TILE, class Pro, class Epi>
 static void launch_stage(const DftGeom& g, const Pro& pro, const Epi& epi, int* status, cudaStream_t st) {
-  dft_stage_kernel<A_PARTS, N_TILE, Pro, Epi>
-      <<<persistent_grid(g), kDftPersistThreads, DftCfg<A_PARTS, N_TILE>::kSmemBytes, st>>>(g, pro, epi, status);
+  StageSet<Pro, Epi, 1> set;
+  set.n = 1;
+  set.tile0[0] = 0;
+  set.tile0[1] = tiles(g);
+  set.it[0] = StageItem<Pro, Epi>{g, pro, epi, status};
+  launch_set<A_PARTS, N_TILE>(set, st);
 }
 
 // One stage launch; the tile width is the one the geometry was built for.
@@ -184,13 +190,65 @@ static void run_stage(int terms, const DftGeom& g, const Pro& pro, const Epi& ep
   }
 }
 
+// Stage launches of several shape buckets merged into persistent launches
+// of up to kStageSetMax items, one per tile width (and term count).
+constexpr int kStageSetMax = 64;
+
 template <class Pro, class Epi>
+struct StageJob {
+  int terms;
+  StageItem<Pro, Epi> item;
+};
+
+template <int A_PARTS, int N_TILE, class Pro, class Epi>
+static void launch_jobs(const StageJob<Pro, Epi>* jobs, int n, int terms, int col_per_tile,
+                        cudaStream_t st) {
+  StageSet<Pro, Epi, kStageSetMax> set;
+  set.n = 0;
+  set.tile0[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    const StageJob<Pro, Epi>& j = jobs[i];
+    if (j.terms != terms || j.item.g.col_per_tile != col_per_tile) continue;
+    set.it[set.n] = j.item;
+    set.tile0[set.n + 1] = set.tile0[set.n] + tiles(j.item.g);
+    if (++set.n == kStageSetMax) {
+      launch_set<A_PARTS, N_TILE>(set, st);
+      set.n = 0;
+    }
+  }
+  if (set.n > 0) launch_set<A_PARTS, N_TILE>(set, st);
+}
+
+template <class Pro, class Epi>
+static void run_stage_multi(const StageJob<Pro, Epi>* jobs, int n, cudaStream_t st) {
+  bool w6 = false, w64 = false, w128 = false, w256 = false;
+  for (int i = 0; i < n; ++i) {
+    const int c = jobs[i].item.g.col_per_tile;
+    if (jobs[i].terms == 6) w6 = true;
+    else if (c == 32) w64 = true;
+    else if (c == 64) w128 = true;
+    else w256 = true;
+  }
+  if (w6) launch_jobs<3, 128>(jobs, n, 6, 64, st);
+  if (w64) launch_jobs<2, 64>(jobs, n, 3, 32, st);
+  if (w128) launch_jobs<2, 128>(jobs, n, 3, 64, st);
+  if (w256) launch_jobs<2, 256>(jobs, n, 3, 128, st);
+}
+
+template <class Pro, class Epi, bool kMulti = false>
 static cudaError_t set_attr_both() {
   cudaError_t e;
-  if ((e = set_attr<2, 256, Pro, Epi>()) != cudaSuccess) return e;
-  if ((e = set_attr<2, 128, Pro, Epi>()) != cudaSuccess) return e;
-  if ((e = set_attr<2, 64, Pro, Epi>()) != cudaSuccess) return e;
-  return set_attr<3, 128, Pro, Epi>();
+  if ((e = set_attr<2, 256, Pro, Epi, 1>()) != cudaSuccess) return e;
+  if ((e = set_attr<2, 128, Pro, Epi, 1>()) != cudaSuccess) return e;
+  if ((e = set_attr<2, 64, Pro, Epi, 1>()) != cudaSuccess) return e;
+  if ((e = set_attr<3, 128, Pro, Epi, 1>()) != cudaSuccess) return e;
+  if constexpr (kMulti) {
+    if ((e = set_attr<2, 256, Pro, Epi, kStageSetMax>()) != cudaSuccess) return e;
+    if ((e = set_attr<2, 128, Pro, Epi, kStageSetMax>()) != cudaSuccess) return e;
+    if ((e = set_attr<2, 64, Pro, Epi, kStageSetMax>()) != cudaSuccess) return e;
+    if ((e = set_attr<3, 128, Pro, Epi, kStageSetMax>()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace fbme

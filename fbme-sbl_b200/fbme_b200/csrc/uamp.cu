@@ -18,6 +18,8 @@
 // to run.
 #include <math.h>
 
+#include <vector>
+
 #include "dft_umma.cuh"
 #include "kernels.cuh"
 #include "stage.cuh"
@@ -175,13 +177,24 @@ FBME_DEV DenoiseOut denoise_math(const DenoiseArgs& a, float prior, float2 om, f
 // ---------------------------------------------------------------------------
 // elementwise kernels
 // ---------------------------------------------------------------------------
+// Block coordinates of an elementwise body: block x of gx along a scene's
+// range, scene y.  A plain launch passes blockIdx / gridDim; a launch merged
+// over shape buckets passes each bucket's own block count, so every block
+// covers the same elements (and sums them in the same order) as in the
+// bucket's own launch.
+struct Blk {
+  int x, gx, y;
+};
+FBME_DEV Blk blk_here() {
+  return Blk{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), static_cast<int>(blockIdx.y)};
+}
+// ---------------------------------------------------------------------------
 // Initial prior variances (solver.py:1063-1099): backprojection blend or
 // uniform, floored; per-block sums of the result.
-__global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevConfig c, Scalars sc,
-                                                            const float2* bp, float* gamma,
-                                                            double* part) {
+FBME_DEV void gamma0_body(Blk k, BatchShape s, DevConfig c, Scalars sc, const float2* bp, float* gamma,
+                          double* part) {
   __shared__ double red[32];
-  const int scene = blockIdx.y;
+  const int scene = k.y;
   const long long n = s.n();
   const float dp = sc.data_power[scene], fl = sc.floor_[scene];
   const float ebp = fmaxf(sc.ebp[scene], kEps);
@@ -197,8 +210,8 @@ __global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevCon
     acc += g;
     return g;
   };
-  const long long first = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long first = k.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long stride = static_cast<long long>(k.gx) * blockDim.x;
   if ((n & 1) == 0) {  // two coefficients per step, 16- and 8-byte accesses
     for (long long j = first; j < n / 2; j += stride) {
       const long long e = scene * n + 2 * j;
@@ -210,7 +223,12 @@ __global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevCon
   } else {
     for (long long i = first; i < n; i += stride) gamma[scene * n + i] = prior(bp[scene * n + i]);
   }
-  write_block_partial(acc, red, part, scene, blockIdx.x, 0 * kPartWarps);
+  write_block_partial(acc, red, part, scene, k.x, 0 * kPartWarps);
+}
+__global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevConfig c, Scalars sc,
+                                                            const float2* bp, float* gamma,
+                                                            double* part) {
+  gamma0_body(blk_here(), s, c, sc, bp, gamma, part);
 }
 
 // Denoiser of sweeps 2..T_u and of the final E-step, on the adjoint output
@@ -218,9 +236,9 @@ __global__ void __launch_bounds__(kEwThreads) gamma0_kernel(BatchShape s, DevCon
 // runs one CTA per SM, too few warps to keep the denoiser's loads in
 // flight, while this kernel runs at full occupancy.  Per-block DOF and
 // variance sums go to partial slots 0 and 1, as sweep1_kernel's.
-__global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, DenoiseArgs a, const float2* lift) {
+FBME_DEV void denoise_body(Blk k, BatchShape s, DenoiseArgs a, const float2* lift) {
   __shared__ double red[32];
-  const int scene = blockIdx.y;
+  const int scene = k.y;
   const long long n = s.n();
   const float pv = a.pv[scene], fl = a.floor_[scene];
   float dof = 0.f, sv = 0.f;
@@ -230,8 +248,8 @@ __global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, Denoi
     sv += o.variance;
     return o;
   };
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  const long long first = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long stride = static_cast<long long>(k.gx) * blockDim.x;
+  const long long first = k.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if ((n & 1) == 0) {
     // two coefficients per step: 16-byte accesses to mu and the lift, 8-byte
     // to the variances (scene offsets are even, so every access is aligned)
@@ -261,18 +279,20 @@ __global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, Denoi
       if (a.keys) a.keys[e] = float_key(abs_sq(o.mean) + o.variance);
     }
   }
-  write_block_partial(dof, red, a.part, scene, blockIdx.x, 0 * kPartWarps);
-  write_block_partial(sv, red, a.part, scene, blockIdx.x, 1 * kPartWarps);
+  write_block_partial(dof, red, a.part, scene, k.x, 0 * kPartWarps);
+  write_block_partial(sv, red, a.part, scene, k.x, 1 * kPartWarps);
+}
+__global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, DenoiseArgs a, const float2* lift) {
+  denoise_body(blk_here(), s, a, lift);
 }
 
 // UAMP message update (triton_kernels.py:72-84) for sweeps 2..T_u and the
 // final E-step: m' = d m + (1-d) prec (y - (p - dvar m)), into `msg_out`,
 // which adjoint stage 1 then reads.  Full occupancy, two samples per step
 // where y is 16-byte aligned and M even.
-__global__ void __launch_bounds__(kEwThreads)
-message_kernel(BatchShape s, const float2* y, const float2* pred, const float2* msg_in, float2* msg_out,
-               const float* prec, const float* dvar, float damping) {
-  const int scene = blockIdx.y;
+FBME_DEV void message_body(Blk k, BatchShape s, const float2* y, const float2* pred, const float2* msg_in,
+                           float2* msg_out, const float* prec, const float* dvar, float damping) {
+  const int scene = k.y;
   const long long m = s.m();
   const float pr = prec[scene], dv = dvar[scene];
   const float keep = damping, upd = 1.0f - damping;
@@ -281,8 +301,8 @@ message_kernel(BatchShape s, const float2* y, const float2* pred, const float2* 
     const float2 cand = make_float2(pr * (yy.x - pseudo.x), pr * (yy.y - pseudo.y));
     return make_float2(keep * mm.x + upd * cand.x, keep * mm.y + upd * cand.y);
   };
-  const long long first = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long first = k.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long stride = static_cast<long long>(k.gx) * blockDim.x;
   if ((m & 1) == 0 && (reinterpret_cast<uintptr_t>(y) & 15u) == 0) {
     for (long long j = first; j < m / 2; j += stride) {
       const long long e = scene * m + 2 * j;
@@ -300,23 +320,26 @@ message_kernel(BatchShape s, const float2* y, const float2* pred, const float2* 
     }
   }
 }
+__global__ void __launch_bounds__(kEwThreads)
+message_kernel(BatchShape s, const float2* y, const float2* pred, const float2* msg_in, float2* msg_out,
+               const float* prec, const float* dvar, float damping) {
+  message_body(blk_here(), s, y, pred, msg_in, msg_out, prec, dvar, damping);
+}
 
 // First sweep: the lifted message is (1-d)/(dv+nv) * A^H y, the previous
 // mean is zero and the previous variance equals the initial prior
 // (solver.py:1160-1182, 2775-2783).  Blocks past `nblk_n` write the first
 // message m1 = (1-d) * (y / (dv+nv)) instead.
-__global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevConfig c, Scalars sc,
-                                                            DenoiseArgs a, const float2* bp,
-                                                            const float2* y, float2* msg,
-                                                            int nblk_n) {
+FBME_DEV void sweep1_body(Blk k, BatchShape s, DevConfig c, Scalars sc, DenoiseArgs a, const float2* bp,
+                          const float2* y, float2* msg, int nblk_n) {
   __shared__ double red[32];
-  const int scene = blockIdx.y;
-  if (static_cast<int>(blockIdx.x) >= nblk_n) {
+  const int scene = k.y;
+  if (static_cast<int>(k.x) >= nblk_n) {
     const long long m = s.m();
     const float pr = sc.prec[scene];
     const float keep = c.uamp_damping, upd = 1.0f - c.uamp_damping;
-    for (long long i = (blockIdx.x - nblk_n) * static_cast<long long>(blockDim.x) + threadIdx.x;
-         i < m; i += static_cast<long long>(gridDim.x - nblk_n) * blockDim.x) {
+    for (long long i = (k.x - nblk_n) * static_cast<long long>(blockDim.x) + threadIdx.x;
+         i < m; i += static_cast<long long>(k.gx - nblk_n) * blockDim.x) {
       const long long e = scene * m + i;
       const float2 yy = y[e];
       msg[e] = make_float2(keep * 0.0f + upd * (pr * yy.x), keep * 0.0f + upd * (pr * yy.y));
@@ -334,7 +357,7 @@ __global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevCon
     sv += o.variance;
     return o;
   };
-  const long long first = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long first = k.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   const long long stride = static_cast<long long>(nblk_n) * blockDim.x;
   if ((n & 1) == 0) {  // two coefficients per step, 16- and 8-byte accesses
     for (long long j = first; j < n / 2; j += stride) {
@@ -356,8 +379,14 @@ __global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevCon
       if (a.update_prior) a.gamma[e] = o.gamma;
     }
   }
-  write_block_partial(dof, red, a.part, scene, blockIdx.x, 0 * kPartWarps);
-  write_block_partial(sv, red, a.part, scene, blockIdx.x, 1 * kPartWarps);
+  write_block_partial(dof, red, a.part, scene, k.x, 0 * kPartWarps);
+  write_block_partial(sv, red, a.part, scene, k.x, 1 * kPartWarps);
+}
+__global__ void __launch_bounds__(kEwThreads) sweep1_kernel(BatchShape s, DevConfig c, Scalars sc,
+                                                            DenoiseArgs a, const float2* bp,
+                                                            const float2* y, float2* msg,
+                                                            int nblk_n) {
+  sweep1_body(blk_here(), s, c, sc, a, bp, y, msg, nblk_n);
 }
 
 // Per-scene scalar updates from the per-tile sums (fixed summation order).
@@ -367,11 +396,10 @@ enum ScalarMode { kScalarInit1 = 0, kScalarInit2 = 1, kScalarSweep = 2 };
 // adds them, lane 0 applies the update.
 constexpr int kScalarScenesPerBlock = 4;
 
-__global__ void __launch_bounds__(32 * kScalarScenesPerBlock)
-scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part, PartSrc p0,
-               PartSrc p1, PartSrc p2) {
+FBME_DEV void scalars_body(Blk k, int mode, BatchShape s, DevConfig c, Scalars sc, const double* part,
+                           PartSrc p0, PartSrc p1, PartSrc p2) {
   const int lane = threadIdx.x & 31;
-  const int scene = blockIdx.x * kScalarScenesPerBlock + (threadIdx.x >> 5);
+  const int scene = k.x * kScalarScenesPerBlock + (threadIdx.x >> 5);
   if (scene >= s.B) return;
   auto sum = [&](int id, PartSrc src) {
     double v = 0.0;
@@ -430,16 +458,108 @@ scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* pa
     sc.prec[scene] = 1.0f / (dv + nv);
   }
 }
+__global__ void __launch_bounds__(32 * kScalarScenesPerBlock)
+scalars_kernel(int mode, BatchShape s, DevConfig c, Scalars sc, const double* part, PartSrc p0, PartSrc p1,
+               PartSrc p2) {
+  scalars_body(blk_here(), mode, s, c, sc, part, p0, p1, p2);
+}
+
+// ---------------------------------------------------------------------------
+// elementwise launches merged over shape buckets: blockIdx.z is the bucket;
+// blocks past a bucket's own grid return at once
+// ---------------------------------------------------------------------------
+constexpr int kEwMulti = 64;
+template <class J>
+struct EwJobs {
+  int n;
+  J j[kEwMulti];
+};
+FBME_DEV bool ew_block(int gx, int scenes, Blk& k) {
+  k = Blk{static_cast<int>(blockIdx.x), gx, static_cast<int>(blockIdx.y)};
+  return k.x < gx && k.y < scenes;
+}
+
+struct Gamma0Job {
+  int gx;
+  BatchShape s;
+  DevConfig c;
+  Scalars sc;
+  const float2* bp;
+  float* gamma;
+  double* part;
+};
+__global__ void __launch_bounds__(kEwThreads) gamma0_multi_kernel(const __grid_constant__ EwJobs<Gamma0Job> m) {
+  const Gamma0Job& j = m.j[blockIdx.z];
+  Blk k;
+  if (ew_block(j.gx, j.s.B, k)) gamma0_body(k, j.s, j.c, j.sc, j.bp, j.gamma, j.part);
+}
+
+struct DenoiseJob {
+  int gx;
+  BatchShape s;
+  DenoiseArgs a;
+  const float2* lift;
+};
+__global__ void __launch_bounds__(kEwThreads) denoise_multi_kernel(const __grid_constant__ EwJobs<DenoiseJob> m) {
+  const DenoiseJob& j = m.j[blockIdx.z];
+  Blk k;
+  if (ew_block(j.gx, j.s.B, k)) denoise_body(k, j.s, j.a, j.lift);
+}
+
+struct MessageJob {
+  int gx;
+  BatchShape s;
+  const float2 *y, *pred, *msg_in;
+  float2* msg_out;
+  const float *prec, *dvar;
+  float damping;
+};
+__global__ void __launch_bounds__(kEwThreads) message_multi_kernel(const __grid_constant__ EwJobs<MessageJob> m) {
+  const MessageJob& j = m.j[blockIdx.z];
+  Blk k;
+  if (ew_block(j.gx, j.s.B, k)) message_body(k, j.s, j.y, j.pred, j.msg_in, j.msg_out, j.prec, j.dvar, j.damping);
+}
+
+struct Sweep1Job {
+  int gx, nblk_n;
+  BatchShape s;
+  DevConfig c;
+  Scalars sc;
+  DenoiseArgs a;
+  const float2 *bp, *y;
+  float2* msg;
+};
+__global__ void __launch_bounds__(kEwThreads) sweep1_multi_kernel(const __grid_constant__ EwJobs<Sweep1Job> m) {
+  const Sweep1Job& j = m.j[blockIdx.z];
+  Blk k;
+  if (ew_block(j.gx, j.s.B, k)) sweep1_body(k, j.s, j.c, j.sc, j.a, j.bp, j.y, j.msg, j.nblk_n);
+}
+
+// Scalar updates: blockIdx.x strides the bucket's scene blocks.
+struct ScalarsJob {
+  int gx;
+  BatchShape s;
+  DevConfig c;
+  Scalars sc;
+  const double* part;
+  PartSrc p0, p1, p2;
+};
+__global__ void __launch_bounds__(32 * kScalarScenesPerBlock)
+scalars_multi_kernel(int mode, const __grid_constant__ EwJobs<ScalarsJob> m) {
+  const ScalarsJob& j = m.j[blockIdx.z];
+  if (static_cast<int>(blockIdx.x) < j.gx)
+    scalars_body(Blk{static_cast<int>(blockIdx.x), j.gx, 0}, mode, j.s, j.c, j.sc, j.part, j.p0, j.p1, j.p2);
+}
 
 // ---------------------------------------------------------------------------
 // stage geometry and launch
 // ---------------------------------------------------------------------------
 cudaError_t set_dft_attributes() {
   cudaError_t e;
-  if ((e = set_attr_both<ProPlain, EpiStoreT>()) != cudaSuccess) return e;
-  if ((e = set_attr_both<ProYPower, EpiStoreT>()) != cudaSuccess) return e;
-  if ((e = set_attr_both<ProPlain, EpiPredict>()) != cudaSuccess) return e;
-  if ((e = set_attr_both<ProPlain, EpiBackprojection>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiStoreT, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProYPower, EpiStoreT, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiPredict, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiBackprojection, true>()) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
@@ -465,6 +585,26 @@ void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float
 // Geometry of a stage whose prologue reads the caller's observations y:
 // vector (16-byte) accesses need y itself 16-byte aligned, which a caller's
 // pointer need not be (complex64 is 8-byte aligned).
+// Denoiser arguments of a sweep (prior update on, no score keys).
+static DenoiseArgs denoise_args(const DevConfig& c, const UampBuffers& u) {
+  DenoiseArgs da;
+  da.mu = u.mu;
+  da.var = u.var;
+  da.gamma = u.gamma;
+  da.pv = u.sc.pv;
+  da.floor_ = u.sc.floor_;
+  da.part = u.part;
+  da.keys = nullptr;
+  da.damping = c.uamp_damping;
+  da.prior_damping = c.damping;
+  da.prior_max = c.max_prec;
+  da.hyper_shape = c.hyper_shape;
+  da.hyper_rate = c.hyper_rate;
+  da.inv_hyper = 1.0f / (1.0f + c.hyper_shape);
+  da.update_prior = 1;
+  return da;
+}
+
 static DftGeom with_y(DftGeom g, const float2* y) {
   if (reinterpret_cast<uintptr_t>(y) & 15u) g.vec4 = 0;
   return g;
@@ -517,21 +657,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                    kScalarInit2, s, c, u.sc, u.part, PartSrc{bn, 1}, PartSrc{0, 0}, PartSrc{0, 0})));
   }
-  DenoiseArgs da;
-  da.mu = u.mu;
-  da.var = u.var;
-  da.gamma = u.gamma;
-  da.pv = u.sc.pv;
-  da.floor_ = u.sc.floor_;
-  da.part = u.part;
-  da.keys = nullptr;
-  da.damping = c.uamp_damping;
-  da.prior_damping = c.damping;
-  da.prior_max = c.max_prec;
-  da.hyper_shape = c.hyper_shape;
-  da.hyper_rate = c.hyper_rate;
-  da.inv_hyper = 1.0f / (1.0f + c.hyper_shape);
-  da.update_prior = 1;
+  DenoiseArgs da = denoise_args(c, u);
 
   // --- sweeps ---
   int cur = 0;  // msg[cur] holds the latest message
@@ -579,4 +705,164 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
 }
 
+// ---------------------------------------------------------------------------
+// several shape buckets at once
+// ---------------------------------------------------------------------------
+static_assert(sizeof(EwJobs<Sweep1Job>) < 32000, "merged launch parameters exceed the 32 KB limit");
+static_assert(sizeof(StageSet<ProYPower, EpiPredict, kStageSetMax>) < 32000,
+              "merged stage parameters exceed the 32 KB limit");
+
+// Merged elementwise launches of `jobs` in groups of kEwMulti; the grid is
+// the largest bucket's block count x scene count x buckets.
+template <class J, class F>
+static void ew_launch(const std::vector<J>& jobs, F&& launch) {
+  EwJobs<J> m;
+  for (size_t i0 = 0; i0 < jobs.size(); i0 += kEwMulti) {
+    m.n = 0;
+    int gx = 1, gy = 1;
+    for (size_t i = i0; i < jobs.size() && m.n < kEwMulti; ++i) {
+      m.j[m.n++] = jobs[i];
+      gx = jobs[i].gx > gx ? jobs[i].gx : gx;
+      gy = jobs[i].s.B > gy ? jobs[i].s.B : gy;
+    }
+    launch(m, dim3(gx, gy, m.n));
+  }
+}
+
+static void scalars_multi(int mode, const std::vector<ScalarsJob>& jobs, cudaStream_t st) {
+  ew_launch(jobs, [&](const EwJobs<ScalarsJob>& m, dim3 g) {
+    scalars_multi_kernel<<<dim3(g.x, 1, g.z), 32 * kScalarScenesPerBlock, 0, st>>>(mode, m);
+  });
+}
+
+// uamp_run for several shape buckets (no warm start): each stage and
+// elementwise step is one launch over all buckets, and bucket b takes part
+// in sweeps 1..T_u(b) only.  A bucket's blocks, tiles and summation orders
+// are those of its own uamp_run, so the results are identical.
+void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
+  std::vector<DftGeom> f1(nb), f2(nb), a1(nb), a2(nb);
+  std::vector<int> bn(nb), bm(nb), cur(nb, 0);
+  int iters = 0;
+  for (int b = 0; b < nb; ++b) {
+    const BatchShape& s = J[b].s;
+    const int nt = J[b].t.n_tile;
+    f1[b] = stage_geom(kFwd1, s, J[b].t, nt);
+    f2[b] = stage_geom(kFwd2, s, J[b].t, nt);
+    a1[b] = stage_geom(kAdj1, s, J[b].t, nt);
+    a2[b] = stage_geom(kAdj2, s, J[b].t, nt);
+    bn[b] = ew_blocks_host(s.n());
+    bm[b] = ew_blocks_host(s.m());
+    iters = J[b].c.uamp_iters > iters ? J[b].c.uamp_iters : iters;
+  }
+  auto msg = [&](int b, int which) { return J[b].u.msg + which * static_cast<long long>(J[b].s.B) * J[b].s.m(); };
+  auto sgx = [&](int b) { return ceil_div(J[b].s.B, kScalarScenesPerBlock); };
+  auto plain_stage = [&](const std::vector<int>& bs, const std::vector<DftGeom>& g, auto in, auto out) {
+    std::vector<StageJob<ProPlain, EpiStoreT>> j;
+    for (int b : bs) j.push_back({J[b].c.terms, {g[b], ProPlain{in(b)}, EpiStoreT{out(b)}, J[b].u.status}});
+    run_stage_multi(j.data(), static_cast<int>(j.size()), st);
+  };
+  std::vector<int> all(nb);
+  for (int b = 0; b < nb; ++b) all[b] = b;
+
+  // --- initialisation (sbl_init) ---
+  {
+    std::vector<StageJob<ProYPower, EpiStoreT>> jy;
+    std::vector<StageJob<ProPlain, EpiBackprojection>> jb;
+    std::vector<ScalarsJob> s1, s2;
+    std::vector<Gamma0Job> g0;
+    for (int b = 0; b < nb; ++b) {
+      const UampBuffers& u = J[b].u;
+      const DftGeom a1y = with_y(a1[b], u.y);
+      jy.push_back({J[b].c.terms, {a1y, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status}});
+      jb.push_back({J[b].c.terms, {a2[b], ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f}, u.status}});
+      s1.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{a1y.row_tiles * a1y.col_tiles, kProWarps},
+                    PartSrc{a2[b].row_tiles * a2[b].col_tiles, kPartWarps}, PartSrc{0, 0}});
+      g0.push_back({bn[b], J[b].s, J[b].c, u.sc, u.bp, u.gamma, u.part});
+      s2.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{bn[b], 1}, PartSrc{0, 0}, PartSrc{0, 0}});
+    }
+    FBME_TIMED(prof, FBME_GROUP_INIT, run_stage_multi(jy.data(), nb, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT, run_stage_multi(jb.data(), nb, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT, scalars_multi(kScalarInit1, s1, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT, ew_launch(g0, [&](const EwJobs<Gamma0Job>& m, dim3 g) {
+                 gamma0_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+               }));
+    FBME_TIMED(prof, FBME_GROUP_INIT, scalars_multi(kScalarInit2, s2, st));
+  }
+
+  // --- sweeps ---
+  for (int it = 1; it <= iters; ++it) {
+    std::vector<int> act;
+    for (int b = 0; b < nb; ++b)
+      if (J[b].c.uamp_iters >= it) act.push_back(b);
+    if (it == 1) {
+      std::vector<Sweep1Job> j;
+      for (int b : act) {
+        const UampBuffers& u = J[b].u;
+        j.push_back({bn[b] + bm[b], bn[b], J[b].s, J[b].c, u.sc, denoise_args(J[b].c, u), u.bp, u.y, msg(b, cur[b])});
+      }
+      FBME_TIMED(prof, FBME_GROUP_SWEEP1, ew_launch(j, [&](const EwJobs<Sweep1Job>& m, dim3 g) {
+                   sweep1_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+                 }));
+    } else {
+      std::vector<MessageJob> jm;
+      std::vector<DenoiseJob> jd;
+      for (int b : act) {
+        const UampBuffers& u = J[b].u;
+        jm.push_back({bm[b], J[b].s, u.y, u.pred, msg(b, cur[b]), msg(b, cur[b] ^ 1), u.sc.prec, u.sc.dvar,
+                      J[b].c.uamp_damping});
+        jd.push_back({bn[b], J[b].s, denoise_args(J[b].c, u), u.lift});
+      }
+      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
+                   message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+                 }));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+                 plain_stage(act, a1, [&](int b) { return msg(b, cur[b] ^ 1); }, [&](int b) { return J[b].u.tmp; }));
+      for (int b : act) cur[b] ^= 1;
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2,
+                 plain_stage(act, a2, [&](int b) { return J[b].u.tmp; }, [&](int b) { return J[b].u.lift; }));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
+                   denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+                 }));
+    }
+    FBME_TIMED(prof, FBME_GROUP_FWD_1,
+               plain_stage(act, f1, [&](int b) { return J[b].u.mu; }, [&](int b) { return J[b].u.tmp; }));
+    {
+      std::vector<StageJob<ProPlain, EpiPredict>> j;
+      std::vector<ScalarsJob> sj;
+      for (int b : act) {
+        const UampBuffers& u = J[b].u;
+        j.push_back({J[b].c.terms, {f2[b], ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f}, u.status}});
+        sj.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{bn[b], 1}, PartSrc{bn[b], 1},
+                      PartSrc{f2[b].row_tiles * f2[b].col_tiles, kPartWarps}});
+      }
+      FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, run_stage_multi(j.data(), static_cast<int>(j.size()), st));
+      FBME_TIMED(prof, FBME_GROUP_SCALARS, scalars_multi(kScalarSweep, sj, st));
+    }
+  }
+
+  // --- final E-step (no prior update, no prediction), score keys ---
+  std::vector<MessageJob> jm;
+  std::vector<DenoiseJob> jd;
+  for (int b = 0; b < nb; ++b) {
+    const UampBuffers& u = J[b].u;
+    jm.push_back({bm[b], J[b].s, u.y, u.pred, msg(b, cur[b]), msg(b, cur[b] ^ 1), u.sc.prec, u.sc.dvar,
+                  J[b].c.uamp_damping});
+    DenoiseArgs da = denoise_args(J[b].c, u);
+    da.update_prior = 0;
+    da.keys = reinterpret_cast<uint32_t*>(u.keys);
+    jd.push_back({bn[b], J[b].s, da, u.lift});
+  }
+  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
+               message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+             }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+             plain_stage(all, a1, [&](int b) { return msg(b, cur[b] ^ 1); }, [&](int b) { return J[b].u.tmp; }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2,
+             plain_stage(all, a2, [&](int b) { return J[b].u.tmp; }, [&](int b) { return J[b].u.lift; }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
+               denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+             }));
+}
+
 }  // namespace fbme
+
