@@ -276,3 +276,43 @@ def test_exchange_tile_classes_match_oracle(shape):
     np.testing.assert_array_equal(eng.out["support_exchanges_accepted"].cpu().numpy(),
                                   np.asarray(ref["support_exchanges_accepted"]).reshape(-1))
     eng.close()
+
+
+@pytest.mark.gpu
+def test_more_buckets_than_one_merged_launch_holds():
+    """70 distinct shapes: the merged UAMP launches take at most 64 buckets
+    each, so every step splits into two launches; every scene still equals
+    its own single-scene plan bit for bit, and the buckets stop at
+    different sweeps."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(31)
+    shapes = []
+    while len(shapes) < 70:
+        g = (int(rng.choice([32, 40, 48, 64])), int(rng.choice([32, 48, 56, 64, 80])))
+        s = (int(rng.integers(8, g[0] // 2 + 1)), int(rng.integers(8, g[1] // 2 + 1)))
+        if (g, s) not in shapes:
+            shapes.append((g, s))
+    sc = _scenes(shapes, 2100)
+    cfg = _cfg()
+    eng = UnevenEngine(shapes, cfg, dev)
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    assert len(eng.buckets()) == 70
+    assert len({b["uamp_iterations"] for b in eng.buckets()}) > 1
+    assert int(eng.out["status"].abs().sum()) == 0
+    for i in range(0, 70, 3):
+        g, s = shapes[i]
+        ref = FBMEEngine(1, g, s, cfg, dev, n_tile=eng.tile_widths[(g, s)])
+        ref.run(torch.from_numpy(sc[i].y).to(dev).reshape(1, -1).contiguous())
+        torch.cuda.synchronize()
+        p0, n = eng.pix_off[i], g[0] * g[1]
+        for f in FIELDS_PIX:
+            assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][0]), (f, i)
+        for f in FIELDS_SCENE:
+            assert torch.equal(eng.out[f][i], ref.out[f][0]), (f, i)
+        ref.close()
+    eng.close()
