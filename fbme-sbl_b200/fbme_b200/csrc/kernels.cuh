@@ -116,8 +116,10 @@ void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float
                  float2* data, float2* tmp, int* status, cudaStream_t st);
 void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
                  float2* coeff, float2* tmp, int* status, cudaStream_t st);
+// plain_prior = false stops after the data power, floors and initial noise
+// (a warm start supplies the prior).
 void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
-              cudaStream_t st, Profiler* prof = nullptr);
+              cudaStream_t st, Profiler* prof = nullptr, bool plain_prior = true);
 void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
               cudaStream_t st, Profiler* prof = nullptr);
 // One shape bucket of uamp_run_multi.

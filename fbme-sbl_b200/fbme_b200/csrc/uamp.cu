@@ -611,7 +611,7 @@ static DftGeom with_y(DftGeom g, const float2* y) {
 }
 
 void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const UampBuffers& u,
-              cudaStream_t st, Profiler* prof) {
+              cudaStream_t st, Profiler* prof, bool plain_prior) {
   const int nt = t.n_tile;
   const DftGeom a1 = with_y(stage_geom(kAdj1, s, t, nt), u.y), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
@@ -624,6 +624,7 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
              (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                  kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, kProWarps},
                  PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
+  if (!plain_prior) return;
   const int bn = ew_blocks_host(s.n());
   FBME_TIMED(prof, FBME_GROUP_INIT,
              (gamma0_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, c, u.sc, u.bp, u.gamma,
@@ -645,7 +646,9 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   const long long BM = static_cast<long long>(s.B) * s.m();
   float2* msg[2] = {u.msg, u.msg + BM};
 
-  sbl_init(s, t, c, u, st, prof);
+  // A warm start replaces the initial prior, its partial sums and the
+  // scalars computed from them, so the plain prior is not formed.
+  sbl_init(s, t, c, u, st, prof, u.warm_params == nullptr);
   const int bn = ew_blocks_host(s.n()), bm = ew_blocks_host(s.m());
   if (u.warm_params) {
     // learned warm start: the network's prior replaces the initial prior,
