@@ -5,12 +5,14 @@ The reference batches only equal shapes, through leading dimensions
 builds one plan per shape and replays them one after another.
 ``UnevenEngine`` binds one native plan over a list of scene shapes.  The
 library groups the scenes into one bucket per shape (in order of first
-appearance) and solves each bucket as an equal-shape batch.  The shape-
-dependent values -- the UAMP sweep budget T_u (solver.py:1295-1309), the
-adaptive damping (solver.py:1183-1189), the resolved exchange size and the
-tuned DFT tile width -- are set per bucket, so a scene stops after its own
-shape's T_u sweeps.  The buckets run on parallel streams; a gather and a
-scatter kernel map the packed scene-order buffers to bucket order and back.
+appearance), each with the state and tables of an equal-shape batch.  The
+shape-dependent values -- the UAMP sweep budget T_u (solver.py:1295-1309),
+the adaptive damping (solver.py:1183-1189), the resolved exchange size and
+the tuned DFT tile width -- are set per bucket, so a scene stops after its
+own shape's T_u sweeps.  Each UAMP step is one launch over all buckets (up
+to 64 per launch); each bucket's polish runs on its own stream; a gather and
+a scatter kernel map the packed scene-order buffers to bucket order and
+back.  Every scene's result equals that of an equal-shape plan bit for bit.
 
 Inputs and outputs are packed: scene i's M1*M2 samples (N1*N2 pixels)
 follow scene i-1's.  ``UnevenSBLPlan`` captures the whole uneven solve in

@@ -1,9 +1,10 @@
 """Uneven batches and tuned tile widths on the B200.
 
-An uneven plan groups its scenes into one bucket per shape and solves each
-bucket as an equal-shape batch; scenes are independent, so every scene's
-result must equal, bit for bit, the result of an equal-shape plan holding
-that shape's scenes in the same order.  Odd shapes (non-square grids,
+An uneven plan groups its scenes into one bucket per shape; its UAMP steps
+run as launches merged over the buckets and each bucket's polish as its own
+equal-shape batch.  Scenes are independent, so every scene's result must
+equal, bit for bit, the result of an equal-shape plan holding that shape's
+scenes in the same order.  Odd shapes (non-square grids,
 prefix lengths that are not multiples of the tile sizes) are checked
 against the oracle at the parity bar: identical support, x within 1e-4
 relative L2, posterior variance within 1e-3 on the support.  The tile
