@@ -317,3 +317,38 @@ def test_more_buckets_than_one_merged_launch_holds():
             assert torch.equal(eng.out[f][i], ref.out[f][0]), (f, i)
         ref.close()
     eng.close()
+
+
+@pytest.mark.gpu
+def test_buckets_with_different_tile_widths():
+    """Buckets laid out for 64-, 128- and 256-column tiles: each merged UAMP
+    step splits into one launch per width, and every scene still equals the
+    equal-shape plan of its width bit for bit."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    widths = {A: 64, B: 128, C: 256}
+    sc = _scenes(ORDER, 2600)
+    cfg = _cfg()
+    eng = UnevenEngine(ORDER, cfg, dev, tile_widths=widths)
+    assert {sh: eng.tile_widths[sh] for sh in widths} == widths
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    assert int(eng.out["status"].abs().sum()) == 0
+    for shape, w in widths.items():
+        idx = [i for i, s in enumerate(ORDER) if s == shape]
+        ref = FBMEEngine(len(idx), shape[0], shape[1], cfg, dev, n_tile=w)
+        ys = torch.stack([torch.from_numpy(sc[i].y).to(dev) for i in idx]).reshape(len(idx), -1)
+        ref.run(ys.contiguous())
+        torch.cuda.synchronize()
+        n = shape[0][0] * shape[0][1]
+        for j, i in enumerate(idx):
+            p0 = eng.pix_off[i]
+            for f in FIELDS_PIX:
+                assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][j]), (f, i, w)
+            for f in FIELDS_SCENE:
+                assert torch.equal(eng.out[f][i], ref.out[f][j]), (f, i, w)
+        ref.close()
+    eng.close()
