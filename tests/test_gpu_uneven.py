@@ -352,3 +352,38 @@ def test_buckets_with_different_tile_widths():
                 assert torch.equal(eng.out[f][i], ref.out[f][j]), (f, i, w)
         ref.close()
     eng.close()
+
+
+@pytest.mark.gpu
+def test_six_term_buckets_match_per_shape_plans():
+    """6-term DFT products (BF16 hi/mid/lo) in an uneven plan: the merged
+    steps take the 6-term stage launches, and every scene equals the
+    equal-shape 6-term plan bit for bit."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    cfg = _cfg()
+    cfg.dft_terms = 6
+    order = [A, C, A]
+    sc = _scenes(order, 2900)
+    eng = UnevenEngine(order, cfg, dev)
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    assert int(eng.out["status"].abs().sum()) == 0
+    for shape in (A, C):
+        idx = [i for i, s in enumerate(order) if s == shape]
+        ref = FBMEEngine(len(idx), shape[0], shape[1], cfg, dev, n_tile=eng.tile_widths[shape])
+        ys = torch.stack([torch.from_numpy(sc[i].y).to(dev) for i in idx]).reshape(len(idx), -1)
+        ref.run(ys.contiguous())
+        torch.cuda.synchronize()
+        n = shape[0][0] * shape[0][1]
+        for j, i in enumerate(idx):
+            p0 = eng.pix_off[i]
+            for f in FIELDS_PIX:
+                assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][j]), (f, i)
+            for f in FIELDS_SCENE:
+                assert torch.equal(eng.out[f][i], ref.out[f][j]), (f, i)
+        ref.close()
+    eng.close()
