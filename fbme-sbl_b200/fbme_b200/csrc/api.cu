@@ -120,6 +120,10 @@ int check_bucket(const fbme::BatchShape& s, const FbmeConfig* c, int nt) {
   if (!(c->uamp_damping >= 0.f && c->uamp_damping < 1.f) || !(c->damping >= 0.f && c->damping < 1.f))
     return fail(FBME_ERR_INVALID, "damping values must be in [0, 1)");
   if (N * s.B > (1LL << 40)) return fail(FBME_ERR_INVALID, "batch too large");
+  // Elementwise, top-k and polish launches put the scenes of a bucket on
+  // gridDim.y / gridDim.z, whose limit is 65535.
+  if (s.B > 65535)
+    return fail(FBME_ERR_UNSUPPORTED, "more than 65535 scenes of one shape in a plan are not built");
   if (N > 524288 || s.n2 > 512)
     return fail(FBME_ERR_UNSUPPORTED, "grids above 524288 points or N2 > 512 are not built");
   if (static_cast<long long>((s.n1 + 15) / 16) * c->exchange_size > 2048)

@@ -111,6 +111,7 @@ size_t topk_scratch_bytes(long long n, int k, int batch) {
 
 const char* topk_check(long long n, int k, int batch) {
   if (n < 1 || batch < 1) return "n and batch must be positive";
+  if (batch > 65535) return "batch above 65535 (rows run on gridDim.y)";
   if (k < 1 || k > 32) return "k must be in [1, 32]";
   if (k > n) return "k exceeds n";
   if (n > (1LL << 31) - 1) return "n above 2^31 - 1";
@@ -141,6 +142,8 @@ void topk_scores(const float* scores, long long n, int k, int batch, void* scrat
 // device pointers from another framework.  The candidate scratch lives in a
 // library-owned, file-scope device array instead of a caller workspace.
 // ---------------------------------------------------------------------------
+#include <cuda.h>
+
 #include <mutex>
 #include <string>
 
@@ -153,12 +156,45 @@ __device__ __align__(256) unsigned char g_topk_scratch[kStaticScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
+// Per device: the array's device address and the unique ID of the context
+// it was looked up in.  cudaDeviceReset destroys the context and a later
+// call runs in a new one (new ID), so the address is looked up again then.
 void* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
 thread_local std::string g_static_error;
 
-// Device address of g_topk_scratch on the current device, looked up once per
-// device (with that device current).  In host code the array's name is only
-// a host-side stand-in, never a device address.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique ID of the calling thread's current context (0 when it cannot be
+// read).  The driver functions come through the runtime's entry-point
+// query, so the library needs no link against libcuda.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
+
+// Device address of g_topk_scratch on the current device, looked up with
+// that device current: once per device, and again whenever the device's
+// context has changed since (after cudaDeviceReset).  In host code the
+// array's name is only a host-side stand-in, never a device address.
 int static_scratch(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -170,8 +206,9 @@ int static_scratch(void** out) {
     g_static_error = "device ordinal outside the static scratch table";
     return FBME_ERR_UNSUPPORTED;
   }
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_ptr[dev]) {
+  if (!g_scratch_ptr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_topk_scratch);
     if (e != cudaSuccess || !p) {
@@ -179,6 +216,7 @@ int static_scratch(void** out) {
       return FBME_ERR_CUDA;
     }
     g_scratch_ptr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return FBME_OK;
@@ -201,6 +239,14 @@ extern "C" int fbme_topk_static(const float* scores, int64_t n, int32_t k, int32
     g_static_error = "fbme_topk_static: batch * ceil(n/8192) * k * 8 bytes exceeds the " +
                      std::to_string(kStaticScratchBytes) + "-byte static scratch";
     return FBME_ERR_INVALID;
+  }
+  // An error left pending by an earlier, unrelated launch is reported as
+  // such, before anything is launched, so it is not taken for this call's.
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    g_static_error = std::string("fbme_topk_static: error pending from an earlier call: ") +
+                     cudaGetErrorString(pending);
+    return FBME_ERR_CUDA;
   }
   void* scratch = nullptr;
   const int rc = static_scratch(&scratch);

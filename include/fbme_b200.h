@@ -198,6 +198,8 @@ int fbme_plan_state(FbmePlan* plan, FbmeState* state);
 /* Top-k (k <= 32) of each of `batch` rows of `n` float scores: values
  * largest first, ties by lower index, as torch.topk(scores, k) at
  * torch_sbl/solver.py:1931 and 4410.  `indices` / `values` are [batch, k].
+ * batch <= 65535 (rows run on a grid dimension of that limit), k <= n and
+ * ceil(n/8192) * k <= 2048; other sizes return FBME_ERR_INVALID.
  * The caller provides fbme_topk_workspace_bytes(n, k, batch) bytes of
  * 16-byte aligned device workspace for the per-slice candidates. */
 size_t fbme_topk_workspace_bytes(int64_t n, int32_t k, int32_t batch);
@@ -212,12 +214,15 @@ int fbme_topk(const float* scores, int64_t n, int32_t k, int32_t batch, void* wo
  * The candidate scratch is a library-owned static device array of
  * FBME_TOPK_STATIC_SCRATCH_BYTES (1 MiB), held by every GPU that loads the
  * library until the process exits.  Requests needing more than that
- * (batch * ceil(n/8192) * k * 8 bytes) return FBME_ERR_INVALID.  The first
- * call on a device looks up the array's device address with that device
- * current: make it before any stream capture.  All calls share the array
- * (nothing in it needs to start at zero); calls that overlap on the GPU race
- * on it, so the caller must order them.  Allocates nothing.  Error text:
- * fbme_topk_static_error(). */
+ * (batch * ceil(n/8192) * k * 8 bytes) return FBME_ERR_INVALID, as do the
+ * sizes fbme_topk rejects.  The first call on a device (and the first after
+ * cudaDeviceReset, which gives the device a new context) looks up the
+ * array's device address with that device current: make it before any
+ * stream capture.  All calls share the array (nothing in it needs to start
+ * at zero); calls that overlap on the GPU race on it, so the caller must
+ * order them.  An error left pending by an earlier launch is returned as
+ * FBME_ERR_CUDA before anything is launched.  Allocates nothing.  Error
+ * text: fbme_topk_static_error(). */
 #define FBME_TOPK_STATIC_SCRATCH_BYTES (1u << 20)
 int fbme_topk_static(const float* scores, int64_t n, int32_t k, int32_t batch, int64_t* indices,
                      float* values, fbme_stream_t stream);

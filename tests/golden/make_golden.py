@@ -1,9 +1,9 @@
 """Generate golden vectors by executing the reference FBME-SBL package.
 
-Run in the build container only (it imports the reference from
-/root/reference, which does not travel to GPU machines):
+Run in a container that holds the reference source tree (it does not
+travel to GPU machines); give its root in FBME_REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py
+    FBME_REFERENCE_ROOT=<path to FBME-SBL> python tests/golden/make_golden.py
 
 For each seeded synthetic scene it runs the reference ``fast_sbl`` with the
 exact FBME-Stable / FBME-Fast plan configurations on the CPU
@@ -23,6 +23,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
+sys.path.insert(0, str(HERE))
+from make_golden_configs import reference_root  # noqa: E402
 
 CASES = [
     # (name, config, seed, profiles)
@@ -36,8 +38,8 @@ def _child(name: str, config: str, seed: int) -> None:
     import numpy as np
     import torch
 
-    sys.path.insert(0, "/root/reference")
-    sys.path.insert(0, str(REPO / "fbme-sbl_b200"))
+    sys.path.insert(0, reference_root())
+    sys.path.append(str(REPO / "fbme-sbl_b200"))
     from fbme_b200 import scenes
     from torch_sbl.solver import SBLConfig, fast_sbl  # reference package
 

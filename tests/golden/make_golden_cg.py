@@ -1,9 +1,9 @@
 """Generate mode="cg" golden vectors by executing the reference FBME-SBL package.
 
-Run in the build container only (it imports the reference from
-/root/reference, which does not travel to GPU machines):
+Run in a container that holds the reference source tree (it does not
+travel to GPU machines); give its root in FBME_REFERENCE_ROOT:
 
-    python tests/golden/make_golden_cg.py
+    FBME_REFERENCE_ROOT=<path to FBME-SBL> python tests/golden/make_golden_cg.py
 
 For each case it runs the reference ``fast_sbl`` with ``mode="cg"`` and
 ``active_set=False`` on the CPU, once with complex128 input (the
@@ -27,6 +27,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "cg"
 REPO = HERE.parents[1]
+sys.path.insert(0, str(HERE))
+from make_golden_configs import reference_root  # noqa: E402
 
 # (name, scene config, seeds stacked as a batch, max_iter)
 CASES = [
@@ -41,7 +43,7 @@ def _child(name: str, config: str, seeds: tuple[int, ...], max_iter: int) -> Non
     import torch
 
     sys.path.append(str(REPO / "fbme-sbl_b200"))
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, reference_root())
     from fbme_b200 import scenes
     from torch_sbl.solver import SBLConfig, fast_sbl  # reference package
 
@@ -88,7 +90,7 @@ def _probes() -> None:
     import numpy as np
     import torch
 
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, reference_root())
     from torch_sbl.solver import _make_probes  # reference package
 
     out = {}

@@ -1,0 +1,74 @@
+"""Loading of the reference-generated golden fixtures (tests/golden).
+
+Fixtures made by make_golden.py store the observation ``y``.  Those made by
+make_golden_configs.py store the generator call and the SHA-256 of its
+observation instead; the observation is regenerated here with the committed
+scene generator and checked against the digest, so a changed generator
+fails loudly rather than comparing against the wrong scene.
+"""
+
+from __future__ import annotations
+
+import glob
+import hashlib
+import re
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
+
+# single-scene plan fixtures (one scene, both profiles)
+PLAN_FILES = sorted(p for p in glob.glob(str(GOLDEN_DIR / "*.npz")) if not Path(p).name.startswith("c4_"))
+# batched-uneven fixtures (64 scenes each)
+UNEVEN_FILES = sorted(glob.glob(str(GOLDEN_DIR / "c4_*.npz")))
+
+
+def _digest(y) -> str:
+    return hashlib.sha256(np.ascontiguousarray(y, dtype=np.complex64).tobytes()).hexdigest()
+
+
+def plan_case(path):
+    """(y [M1, M2] complex64, grid, fixture) of a single-scene fixture."""
+    g = np.load(path)
+    grid = tuple(int(v) for v in g["grid"])
+    if "y" in g.files:
+        return g["y"], grid, g
+    from fbme_b200 import scenes
+
+    m = re.fullmatch(r"config_scene\('(\w+)', (\d+)\)", str(g["scene"]))
+    assert m, str(g["scene"])
+    y = scenes.config_scene(m.group(1), int(m.group(2))).y
+    assert _digest(y) == str(g["y_sha256"]), "scene generator changed: fixture no longer matches"
+    return y, grid, g
+
+
+def uneven_case(path):
+    """(list of scenes, fixture) of a batched-uneven fixture."""
+    from fbme_b200 import scenes
+
+    g = np.load(path)
+    m = re.fullmatch(r"uneven_batch\((\d+)\)", str(g["scene"]))
+    assert m, str(g["scene"])
+    batch = scenes.uneven_batch(int(m.group(1)))
+    assert [_digest(s.y) for s in batch] == [str(v) for v in g["y_sha256"]], "scene generator changed"
+    return batch, g
+
+
+def scene_field(g, key: str, i: int):
+    """Field ``key`` of scene i of a packed batched fixture."""
+    off = g[key + "_off"]
+    return g[key].reshape(-1)[off[i]:off[i + 1]]
+
+
+def scene_fields(g, profile: str, i: int) -> dict:
+    """Every field of scene i under ``profile`` as a single-scene fixture has them."""
+    p = profile + "_"
+    out = {}
+    for k in g.files:
+        if k.startswith(p) and not k.endswith("_off"):
+            v = scene_field(g, k, i)
+            out[k] = v if k[len(p):] in ("active", "x_active", "pv_active", "precision_active",
+                                         "pv_inactive_unique", "precision_inactive_unique",
+                                         "mask_indices", "evidence_trace") else v.reshape(())
+    return out

@@ -73,3 +73,25 @@ def test_workspace_bytes_and_validation_codes():
         nat.check(nat.FBME_ERR_UNSUPPORTED, "x")
     with pytest.raises(RuntimeError):
         nat.check(nat.FBME_ERR_CUDA, "x")
+
+
+def test_batch_limits_are_rejected_on_the_host():
+    """Launches put a plan's scenes and top-k rows on a 65535-limited grid
+    dimension; larger requests fail at validation with a clear code."""
+    lib = nat.lib()
+    c = _cfg()
+    c.exchange_size = 12
+    n = 65536
+    shapes = (nat.FbmeShape * n)(*([nat.FbmeShape(64, 64, 32, 32)] * n))
+    assert lib.fbme_plan_workspace_bytes(shapes, n, ctypes.byref(c)) == 0
+    plan = ctypes.c_void_p()
+    rc = lib.fbme_plan_create(shapes, n, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
+    assert rc == nat.FBME_ERR_UNSUPPORTED and "65535" in nat.last_error()
+    ok = lib.fbme_plan_workspace_bytes(shapes, n - 1, ctypes.byref(c))
+    assert ok > 0
+    assert lib.fbme_topk_workspace_bytes(100, 1, 65536) == 0
+    assert lib.fbme_topk_workspace_bytes(100, 1, 65535) > 0
+    # non-NULL stand-ins: the size check fails before any pointer is used
+    fake = ctypes.c_void_p(256)
+    rc = lib.fbme_topk(fake, 100, 1, 65536, fake, 0, fake, fake, None)
+    assert rc == nat.FBME_ERR_INVALID and "65535" in nat.last_error()

@@ -8,17 +8,19 @@ Bar: identical final support, x within 1e-4 relative L2, posterior variance
 within 1e-3 relative on the support, noise / evidence within 1e-4 relative.
 """
 
-import glob
 from pathlib import Path
 
 import numpy as np
 import pytest
 
+from golden_util import PLAN_FILES, UNEVEN_FILES, plan_case, scene_fields, uneven_case
 from gpu_util import PV_TOL, X_TOL, need_gpu, rel_l2
 
 torch = pytest.importorskip("torch")
 
-GOLDEN = sorted(glob.glob(str(Path(__file__).parent / "golden" / "*.npz")))
+# C3 (ill-conditioned clustered scenes): distance to the reference's FP64
+# result in units of the reference's own FP32-vs-FP64 gap.
+C3_GAP_FACTOR = 5.0
 
 
 def _plan(profile, y, grid):
@@ -28,41 +30,87 @@ def _plan(profile, y, grid):
     return make(y, grid, polish_size=32, warmup=1)
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("profile", ["stable", "fast"])
-@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: Path(p).stem)
-def test_plan_matches_reference_golden(path, profile):
-    need_gpu()
-    g = np.load(path)
-    grid = tuple(int(v) for v in g["grid"])
-    y = torch.from_numpy(g["y"]).cuda()
-    res = _plan(profile, y, grid).replay(y, synchronize=True)
+def _check_plan_fields(res, g, profile, b=None, label=""):
+    """One scene's plan result against a reference fixture's fields."""
     p = profile + "_"
-    x = res.x.cpu().numpy().reshape(-1)
+    sel = (lambda t: t.cpu().numpy().reshape(-1)) if b is None else (lambda t: t[b].cpu().numpy().reshape(-1))
+    x = sel(res.x)
     act = np.flatnonzero(x)
-    assert set(act) == set(g[p + "active"])
+    assert set(act) == set(g[p + "active"]), label
     xr = np.zeros_like(x)
     xr[g[p + "active"]] = g[p + "x_active"]
-    assert rel_l2(x, xr) < X_TOL
-    pv = res.posterior_variance.cpu().numpy().reshape(-1)
-    np.testing.assert_allclose(pv[g[p + "active"]], g[p + "pv_active"], rtol=PV_TOL)
-    np.testing.assert_allclose(res.noise_variance.cpu().numpy(), g[p + "noise_variance"], rtol=1e-4)
-    np.testing.assert_allclose(res.negative_log_evidence.cpu().numpy(), g[p + "negative_log_evidence"],
-                               rtol=1e-4)
-    np.testing.assert_allclose(res.evidence_trace.cpu().numpy(), g[p + "evidence_trace"], rtol=1e-4)
-    np.testing.assert_allclose(res.effective_dof.cpu().numpy(), g[p + "effective_dof"], rtol=1e-4)
-    assert np.array_equal(np.flatnonzero(res.support_mask.cpu().numpy().reshape(-1)), g[p + "mask_indices"])
-    assert res.iterations == int(g[p + "iterations"])
-    assert int(res.status.item()) == 0
+    assert rel_l2(x, xr) < X_TOL, (label, rel_l2(x, xr))
+    pv = sel(res.posterior_variance)
+    np.testing.assert_allclose(pv[g[p + "active"]], g[p + "pv_active"], rtol=PV_TOL, err_msg=label)
+    for f in ("noise_variance", "negative_log_evidence", "evidence_trace", "effective_dof"):
+        np.testing.assert_allclose(sel(getattr(res, f)), np.reshape(g[p + f], -1), rtol=1e-4, err_msg=label + f)
+    assert np.array_equal(np.flatnonzero(sel(res.support_mask)), g[p + "mask_indices"]), label
+    assert int(sel(res.status)[0]) == 0, label
     if profile == "stable":
-        assert int(res.support_exchanges_accepted.item()) == int(g[p + "support_exchanges_accepted"])
-        assert bool(res.fixed_budget_monotone.item()) == bool(g[p + "fixed_budget_monotone"])
-        np.testing.assert_allclose(res.fixed_budget_noise_residual.cpu().numpy(),
-                                   g[p + "fixed_budget_noise_residual"], rtol=2e-2, atol=1e-6)
-        np.testing.assert_allclose(res.fixed_budget_gamma_residual.cpu().numpy(),
-                                   g[p + "fixed_budget_gamma_residual"], rtol=2e-2, atol=1e-6)
-    else:
+        assert int(sel(res.support_exchanges_accepted)[0]) == int(g[p + "support_exchanges_accepted"]), label
+        assert bool(sel(res.fixed_budget_monotone)[0]) == bool(g[p + "fixed_budget_monotone"]), label
+        for f in ("fixed_budget_noise_residual", "fixed_budget_gamma_residual"):
+            dev, ref = float(sel(getattr(res, f))[0]), float(np.reshape(g[p + f], -1)[0])
+            print(f"{label} {f}: device {dev:.7g} reference {ref:.7g} rel {abs(dev - ref) / abs(ref):.2e}")
+            np.testing.assert_allclose(dev, ref, rtol=2e-2, atol=1e-6, err_msg=label + f)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+@pytest.mark.parametrize("path", PLAN_FILES, ids=lambda p: Path(p).stem)
+def test_plan_matches_reference_golden(path, profile):
+    need_gpu()
+    y_np, grid, g = plan_case(path)
+    y = torch.from_numpy(y_np).cuda()
+    res = _plan(profile, y, grid).replay(y, synchronize=True)
+    p = profile + "_"
+    if "cholesky" in g.files:
+        # C3: identical support; x as close to the reference's FP64 answer
+        # as a few times the reference's own FP32 error on this scene
+        x = res.x.cpu().numpy().reshape(-1)
+        act = np.flatnonzero(x)
+        assert set(act) == set(g[p + "active"]) == set(g["f64_" + p + "active"])
+        x64 = np.zeros_like(x)
+        x64[g["f64_" + p + "active"]] = g["f64_" + p + "x_active"]
+        x32 = np.zeros_like(x)
+        x32[g[p + "active"]] = g[p + "x_active"]
+        gap = float(g["gap_" + p + "x"])
+        err64, err32 = rel_l2(x, x64), rel_l2(x, x32)
+        print(f"{Path(path).stem} {profile}: x vs FP64 {err64:.2e} vs FP32 {err32:.2e} "
+              f"(reference FP32 vs FP64 {gap:.2e})")
+        assert err64 < C3_GAP_FACTOR * gap + X_TOL
+        pv = res.posterior_variance.cpu().numpy().reshape(-1)
+        a64 = g["f64_" + p + "active"]
+        pv_err = np.max(np.abs(pv[a64] - g["f64_" + p + "pv_active"]) / g["f64_" + p + "pv_active"])
+        print(f"  posterior variance vs FP64 {pv_err:.2e} (reference gap {float(g['gap_' + p + 'pv']):.2e})")
+        assert pv_err < C3_GAP_FACTOR * float(g["gap_" + p + "pv"]) + PV_TOL
+        assert res.iterations == int(g[p + "iterations"])
+        assert int(res.status.item()) == 0
+        return
+    _check_plan_fields(res, g, profile, label=Path(path).stem)
+    assert res.iterations == int(g[p + "iterations"])
+    if profile == "fast":
         assert res.fixed_budget_monotone is None and res.support_exchanges_accepted is None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+@pytest.mark.parametrize("path", UNEVEN_FILES, ids=lambda p: Path(p).stem)
+def test_uneven_plan_matches_reference_golden(path, profile):
+    """The 64-scene batched-uneven workload (four grids, prefix ratios in
+    [0.3, 0.7]) in one uneven plan against the reference's per-scene solves."""
+    need_gpu()
+    from fbme_b200.uneven import make_uneven_plan
+
+    batch, g = uneven_case(path)
+    ys = [torch.from_numpy(s.y).cuda() for s in batch]
+    plan = make_uneven_plan(ys, [s.grid for s in batch], profile=profile, polish_size=32, warmup=1)
+    results = plan.replay(ys, synchronize=True)
+    assert len(results) == len(batch)
+    for i, r in enumerate(results):
+        f = scene_fields(g, profile, i)
+        _check_plan_fields(r, f, profile, label=f"scene {i} {batch[i].grid}/{batch[i].y.shape}")
+        assert r.iterations == int(f[profile + "_iterations"])
 
 
 @pytest.mark.gpu

@@ -2,26 +2,32 @@
 
 The fixtures in tests/golden were produced by executing the reference
 FBME-SBL ``fast_sbl`` (CPU, ``uamp_backend="torch"``) with the exact
-FBME-Stable / FBME-Fast plan configurations (tests/golden/make_golden.py).
-The oracle runs with the reference's CPU Cholesky loading schedule
-(torch_sbl/solver.py:2922-2931) for this comparison.
-"""
+FBME-Stable / FBME-Fast plan configurations (tests/golden/make_golden.py,
+make_golden_configs.py).  The oracle runs with the reference's CPU
+Cholesky loading schedule (torch_sbl/solver.py:2922-2931) for this
+comparison, except on fixtures made with the reference's CUDA loading
+(C3), where it takes that one (2910-2920).
 
-import glob
+C3 (512^2 / 256x192, clustered points) is ill-conditioned: its reduced
+32-atom systems hold atoms one pixel apart, and the reference's own FP32
+result differs from its FP64 result by 8e-4 to 2.7e-2 relative L2 in x.
+There the bar is relative to that gap: the oracle's FP32 arithmetic must
+land as close to the FP64 answer as a few times the reference's own FP32
+error, with the identical support.
+"""
 
 import numpy as np
 import pytest
 
+from golden_util import PLAN_FILES, UNEVEN_FILES, plan_case, scene_fields, uneven_case
 from oracle import fbme_oracle as O
 
-FILES = sorted(glob.glob(str(__import__("pathlib").Path(__file__).parent / "golden" / "*.npz")))
+# distance to the reference's FP64 result, in units of the reference's own
+# FP32-vs-FP64 gap (C3 only; measured: up to 3.6x for the oracle)
+C3_GAP_FACTOR = 5.0
 
 
-@pytest.mark.parametrize("path", FILES, ids=lambda p: p.rsplit("/", 1)[-1][:-4])
-@pytest.mark.parametrize("profile", ["stable", "fast"])
-def test_oracle_matches_reference(path, profile):
-    g = np.load(path)
-    r = O.fbme_solve(g["y"], tuple(int(v) for v in g["grid"]), profile, chol_mode="cpu")
+def _check_fields(r, g, profile, x_tol=2e-5, pv_rtol=1e-4, scalar_rtol=1e-5):
     p = profile + "_"
     x = r["x"].reshape(-1)
     act = np.flatnonzero(x != 0)
@@ -29,23 +35,60 @@ def test_oracle_matches_reference(path, profile):
     assert np.array_equal(np.sort(act), np.sort(g[p + "active"]))
     xr = np.zeros_like(x)
     xr[g[p + "active"]] = g[p + "x_active"]
-    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 2e-5
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < x_tol
     pv = r["posterior_variance"].reshape(-1)
-    np.testing.assert_allclose(pv[g[p + "active"]], g[p + "pv_active"], rtol=1e-4)
+    np.testing.assert_allclose(pv[g[p + "active"]], g[p + "pv_active"], rtol=pv_rtol)
     inactive = np.setdiff1d(np.arange(x.size), act)
     np.testing.assert_allclose(np.unique(pv[inactive]), g[p + "pv_inactive_unique"], rtol=1e-6)
     np.testing.assert_allclose(r["precision"].reshape(-1)[g[p + "active"]],
-                               g[p + "precision_active"], rtol=1e-4)
-    np.testing.assert_allclose(r["noise_variance"], g[p + "noise_variance"], rtol=1e-5)
-    np.testing.assert_allclose(r["effective_dof"], g[p + "effective_dof"], rtol=1e-5)
-    np.testing.assert_allclose(r["negative_log_evidence"], g[p + "negative_log_evidence"], rtol=1e-5)
-    np.testing.assert_allclose(r["evidence_trace"], g[p + "evidence_trace"], rtol=1e-5)
+                               g[p + "precision_active"], rtol=pv_rtol)
+    for f in ("noise_variance", "effective_dof", "negative_log_evidence", "evidence_trace"):
+        np.testing.assert_allclose(np.reshape(r[f], -1), np.reshape(g[p + f], -1), rtol=scalar_rtol)
     assert np.array_equal(np.flatnonzero(r["support_mask"].reshape(-1)), g[p + "mask_indices"])
     assert r["iterations"] == int(g[p + "iterations"])
     if profile == "stable":
         assert int(r["support_exchanges_accepted"]) == int(g[p + "support_exchanges_accepted"])
+        assert bool(r["fixed_budget_monotone"]) == bool(g[p + "fixed_budget_monotone"])
+
+
+@pytest.mark.parametrize("path", PLAN_FILES, ids=lambda p: p.rsplit("/", 1)[-1][:-4])
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+def test_oracle_matches_reference(path, profile):
+    y, grid, g = plan_case(path)
+    if "cholesky" in g.files:  # C3: CUDA loading, FP64 answer, gap-relative bar
+        r = O.fbme_solve(y, grid, profile, chol_mode="cuda")
+        p = profile + "_"
+        x = r["x"].reshape(-1)
+        act = np.flatnonzero(x != 0)
+        assert np.array_equal(np.sort(act), np.sort(g[p + "active"]))
+        assert np.array_equal(np.sort(act), np.sort(g["f64_" + p + "active"]))
+        x64 = np.zeros_like(x)
+        x64[g["f64_" + p + "active"]] = g["f64_" + p + "x_active"]
+        err = np.linalg.norm(x - x64) / np.linalg.norm(x64)
+        assert err < C3_GAP_FACTOR * float(g["gap_" + p + "x"]) + 1e-4, (err, float(g["gap_" + p + "x"]))
+        assert r["iterations"] == int(g[p + "iterations"])
+        return
+    r = O.fbme_solve(y, grid, profile, chol_mode="cpu")
+    _check_fields(r, g, profile)
+    if profile == "stable":
+        p = profile + "_"
         np.testing.assert_allclose(r["fixed_budget_noise_residual"],
                                    g[p + "fixed_budget_noise_residual"], rtol=1e-3, atol=1e-7)
         np.testing.assert_allclose(r["fixed_budget_gamma_residual"],
                                    g[p + "fixed_budget_gamma_residual"], rtol=2e-3, atol=1e-7)
-        assert bool(r["fixed_budget_monotone"]) == bool(g[p + "fixed_budget_monotone"])
+
+
+@pytest.mark.parametrize("path", UNEVEN_FILES, ids=lambda p: p.rsplit("/", 1)[-1][:-4])
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+def test_oracle_matches_reference_on_uneven_shapes(path, profile):
+    """The first scene of each of the four grids of the batched-uneven
+    workload (prefix ratios in [0.3, 0.7], odd prefix lengths)."""
+    batch, g = uneven_case(path)
+    seen = {}
+    for i, s in enumerate(batch):
+        seen.setdefault(s.grid, i)
+    assert len(seen) == 4
+    for i in seen.values():
+        s = batch[i]
+        r = O.fbme_solve(s.y, s.grid, profile, chol_mode="cpu")
+        _check_fields(r, scene_fields(g, profile, i), profile)

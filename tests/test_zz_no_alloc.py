@@ -70,11 +70,43 @@ def test_static_scratch_topk_matches_workspace_topk_twice():
 
 
 @pytest.mark.gpu
+def test_static_scratch_ragged_rows_match_workspace_topk():
+    """A row length that is not a multiple of the 8192-score slice leaves a
+    short last slice whose unused candidate slots feed the merge."""
+    need_gpu()
+    rng = np.random.default_rng(12)
+    batch, n, k = 3, 8192 * 3 + 5, 32
+    idx = torch.empty(batch, k, dtype=torch.int64, device="cuda")
+    val = torch.empty(batch, k, dtype=torch.float32, device="cuda")
+    s = rng.random((batch, n)).astype(np.float32)
+    s[:, -5:] = 2.0  # the best scores sit in the short last slice
+    s[1, -3] = 3.0
+    scores = torch.from_numpy(s).cuda()
+    ref_idx, ref_val = _topk_workspace(scores, k)
+    rc, err = _topk_static(scores, k, idx, val)
+    assert rc == 0, err
+    torch.cuda.synchronize()
+    assert torch.equal(idx, ref_idx)
+    assert torch.equal(val, ref_val)
+
+
+@pytest.mark.gpu
 def test_static_scratch_rejects_oversize_requests():
     need_gpu()
-    batch, n, k = 64, 262144, 32  # needs 64 * 32 * 32 * 8 = 512 KiB... scale past 1 MiB
-    scores = torch.zeros(batch * 4, n, dtype=torch.float32, device="cuda")
-    idx = torch.empty(batch * 4, k, dtype=torch.int64, device="cuda")
-    val = torch.empty(batch * 4, k, dtype=torch.float32, device="cuda")
+    # 4097 rows of one slice (n <= 8192) at k = 32 need
+    # 4097 * 1 * 32 * 8 = 1,048,832 bytes of candidates: 256 bytes more than
+    # the 1 MiB static scratch.  The scores take 4 MiB.
+    batch, n, k = 4097, 256, 32
+    scores = torch.zeros(batch, n, dtype=torch.float32, device="cuda")
+    idx = torch.empty(batch, k, dtype=torch.int64, device="cuda")
+    val = torch.empty(batch, k, dtype=torch.float32, device="cuda")
     rc, err = _topk_static(scores, k, idx, val)
     assert rc == 1 and "static scratch" in err
+    # exactly 1 MiB of candidates fits; all-equal scores take the ties path
+    rc, err = _topk_static(scores[:4096], k, idx[:4096], val[:4096])
+    assert rc == 0, err
+    ref_idx, ref_val = _topk_workspace(scores[:4096], k)
+    torch.cuda.synchronize()
+    assert torch.equal(idx[:4096], ref_idx)
+    assert torch.equal(ref_idx[0], torch.arange(k, device="cuda"))
+    assert torch.equal(val[:4096], ref_val)
