@@ -46,7 +46,9 @@ def _args() -> argparse.Namespace:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--batch", type=int, default=512, help="scenes per step per GPU")
     ap.add_argument("--profile", choices=("stable", "fast"), default="stable")
-    ap.add_argument("--cpu-sample", type=int, default=32, help="scenes in the CPU baseline sample")
+    ap.add_argument("--cpu-rounds", type=int, default=2,
+                    help="rounds of one scene per host core in the CPU baseline sample")
+    ap.add_argument("--no-cg", action="store_true", help="skip the mode='cg' section")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain section")
     ap.add_argument("--no-uneven", action="store_true", help="skip the batched-uneven section")
@@ -245,6 +247,49 @@ def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
     }
 
 
+# mode="cg" workloads: sbl_2d's default cg path (active_set off) with the EM
+# loop capped at a fixed iteration count, as the reference's CPU sbl_2d is
+# timed at 256x256 (its uncapped C1 run takes 200 iterations).
+CG_CASES = (("c1", (64, 64), 20, 64), ("c2", (256, 256), 6, 8))  # (config, grid, EM iterations, GPU batch)
+
+
+def cg_section(device) -> dict:
+    """Scenes/s of the native cg solve (fbme_cg_solve through CGEngine,
+    including its host reads at the PCG and convergence checks) at C1 and
+    C2, EM iterations capped as CG_CASES states."""
+    import numpy as np
+    import torch
+
+    from fbme_b200 import scenes
+    from fbme_b200.cg import CGEngine
+    from fbme_b200.config import SBLConfig
+
+    out = {}
+    for name, grid, iters, batch in CG_CASES:
+        sc = [scenes.config_scene(name, 3_000_000 + i) for i in range(batch)]
+        y = torch.from_numpy(np.stack([s.y.reshape(-1) for s in sc])).to(device)
+        cfg = SBLConfig(mode="cg", active_set=False, max_iter=iters)
+        eng = CGEngine(batch, grid, sc[0].y.shape, cfg, device)
+        probes = eng.default_probes()
+        eng.solve(y, probes)
+        torch.cuda.synchronize(device)
+        reps = 3
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            res = eng.solve(y, probes)
+        e1.record()
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1) / reps
+        hist = res.history.get("cg_iterations") if res.history else None
+        out[name] = {"grid": list(grid), "scenes_per_solve": batch, "em_iterations": res.iterations,
+                     "ms_per_solve": ms, "scenes_per_s": batch / (ms / 1000.0),
+                     "status_nonzero": int((res.status != 0).sum().item()),
+                     "pcg_iterations": hist}
+        eng.close()
+    return out
+
+
 # ---------------------------------------------------------------- CPU side
 def _oracle_solve(args):
     y, grid, profile = args
@@ -253,20 +298,50 @@ def _oracle_solve(args):
     return O.fbme_solve(y, grid, profile)["x"]
 
 
-def cpu_baseline(n_scenes: int, profile: str) -> dict:
-    """Oracle port (numpy restatement of the reference) on one core."""
-    import numpy as np  # noqa: F401
+def _oracle_cg_solve(args):
+    y, grid, iters = args
+    import numpy as np
 
     from oracle import fbme_oracle as O
 
-    sc = _scenes(n_scenes, 1_000_000)
-    O.fbme_solve(sc[0].y, sc[0].grid, profile)  # warm
-    t0 = time.perf_counter()
-    for s in sc:
-        O.fbme_solve(s.y, s.grid, profile)
-    dt = time.perf_counter() - t0
-    return {"value": n_scenes / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{n_scenes} scenes of the same workload, numpy oracle, one process"}
+    return O.fast_sbl_cg(y[None].astype(np.complex64), grid,
+                         O.OracleConfig(mode="cg", active_set=False, max_iter=iters))["x"]
+
+
+def _pool_rate(fn, work, rounds: int) -> float:
+    """Items per second of ``fn`` over ``work`` on a spawn pool of one
+    process per host core (one thread each), after one warm-up round."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")  # the parent has a CUDA context: never fork
+    with ctx.Pool(len(work), initializer=_limit_threads) as pool:
+        pool.map(fn, work)
+        t0 = time.perf_counter()
+        for _ in range(rounds):
+            pool.map(fn, work)
+        dt = time.perf_counter() - t0
+    return len(work) * rounds / dt
+
+
+def cpu_baseline(profile: str, rounds: int = 2) -> dict:
+    """The oracle port (numpy restatement of the reference) on every host
+    core: one process per core, each solving its own scene of the plan
+    workload; plus the C1 cg-mode leg standing in for the reference's CPU
+    sbl_2d (EM loop capped, CG_CASES)."""
+    from fbme_b200 import scenes
+
+    cores = os.cpu_count() or 1
+    sc = _scenes(cores, 1_000_000)
+    value = _pool_rate(_oracle_solve, [(s.y, s.grid, profile) for s in sc], rounds)
+    _, grid, iters, _ = CG_CASES[0]
+    c1 = [scenes.config_scene("c1", 1_000_000 + i) for i in range(cores)]
+    cg_rate = _pool_rate(_oracle_cg_solve, [(s.y, s.grid, iters) for s in c1], 1)
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{cores * rounds} scenes of the same workload ({rounds} rounds of one scene per core), "
+                      "numpy oracle, one single-threaded process per host core",
+            "c1_cg": {"value": cg_rate, "unit": UNIT, "cores": cores,
+                      "sample": f"{cores} 64x64 / 32x32 scenes, oracle mode='cg' (sbl_2d's default path, "
+                                f"active_set off), {iters} EM iterations, one per core"}}
 
 
 def run_reference(a: argparse.Namespace) -> None:
@@ -353,12 +428,17 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- roofline
-def _peaks() -> tuple[float, str]:
+def _peaks() -> dict:
+    """Roofline denominators: MEASURED_PEAKS.json when the run has it, else
+    the earlier measurement on this GPU type (6650 GB/s copy, 1590 TFLOP/s
+    dense BF16 burst)."""
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return {"hbm": float(d["hbm_gbs"]), "bf16": float(d.get("bf16_tflops", 1590.0)),
+                "source": "measured: MEASURED_PEAKS.json hbm_gbs / bf16_tflops"}
+    return {"hbm": 6650.0, "bf16": 1590.0,
+            "source": "fallback: 6650 GB/s copy and 1590 TFLOP/s BF16 (MEASURED_PEAKS.json absent)"}
 
 
 def algorithmic_bytes(group: str, n: int, m: int) -> int:
@@ -366,12 +446,45 @@ def algorithmic_bytes(group: str, n: int, m: int) -> int:
     (intermediates of the two-stage DFT are not counted)."""
     table = {
         "adjoint_denoise": 32 * n,    # read gamma, mu, v; write mu', v', gamma' (or keys)
-        "adjoint_message": 24 * m,    # read y, m; write m'
+        "message": 24 * m,            # read y, m; write m'
         "forward_1": 8 * n,           # read mu
         "forward_residual": 16 * m,   # read y; write prediction
         "sweep1_denoise": 24 * n + 16 * m,
     }
     return table.get(group, 0)
+
+
+def physical_bytes(group: str, grid, prefix) -> int:
+    """Bytes one scene moves to and from HBM in one launch of a kernel group,
+    intermediates included (each array read or written once)."""
+    n1, n2 = grid
+    m1, m2 = prefix
+    n, m = n1 * n2, m1 * m2
+    t_fwd, t_adj = 8 * m2 * n1, 8 * n2 * m1  # the two-stage intermediates T, U
+    table = {
+        "adjoint_denoise": 40 * n,            # read lift 8, mu 8, gamma 4, v 4; write mu 8, v 4, gamma 4
+        "message": 32 * m,                    # read y, prediction, message; write message
+        "adjoint_1": 8 * m + t_adj,           # read message; write U
+        "adjoint_2": t_adj + 8 * n,           # read U; write lift
+        "forward_1": 8 * n + t_fwd,           # read mu; write T
+        "forward_residual": t_fwd + 16 * m,   # read T, y; write prediction
+    }
+    return table.get(group, 0)
+
+
+def stage_flops(group: str, grid, prefix, terms: int = 3, n_tile: int = 256) -> int:
+    """Tensor-core FLOPs one scene executes in one launch of a DFT stage:
+    the real GEMM [rows, 2K] x [2K, 2C] padded to the tile (128 rows, 64-wide
+    K chunks, n_tile columns), once per split-BF16 product."""
+    n1, n2 = grid
+    m1, m2 = prefix
+    rkc = {"forward_1": (n1, n2, m2), "forward_residual": (m2, n1, m1),
+           "adjoint_1": (m1, m2, n2), "adjoint_2": (n2, m1, n1)}.get(group)
+    if rkc is None:
+        return 0
+    r, k, c = rkc
+    up = lambda v, q: -(-v // q) * q  # noqa: E731
+    return 2 * up(r, 128) * up(2 * k, 64) * up(2 * c, n_tile) * terms
 
 
 def scene_bytes(n: int, m: int, t_u: int, p: int) -> int:
@@ -380,18 +493,25 @@ def scene_bytes(n: int, m: int, t_u: int, p: int) -> int:
     return (t_u + 1) * (32 * n + 24 * m) + 8 * m + 8 * n + 12 * n + p * 8 * m + 17 * n
 
 
-# DRAM bytes per scene of one launch, from one ncu capture of 128 scenes of
-# 256x256 / 128x128 (dram__bytes_read.sum + dram__bytes_write.sum, in
-# the profiles/ summary of the kernel).  Traffic grows in proportion to
-# the scenes of a launch.
-TRAFFIC_PER_SCENE = {"adjoint_denoise": (201.48e6 + 85.42e6) / 128}
-
-
-def _traffic(group: str, batch: int):
-    """Measured DRAM bytes per launch for ``group`` (per-scene figure of the
-    capture scaled by the batch), or None where no capture exists."""
-    v = TRAFFIC_PER_SCENE.get(group)
-    return None if v is None else v * batch
+def stages_table(prof: dict, batch: int, grid, prefix, peaks: dict, terms: int = 3, n_tile: int = 256) -> dict:
+    """Per kernel group of one replay: launches, time per launch, the bytes
+    it must move (physical_bytes) against HBM, and for the DFT stages the
+    executed tensor FLOPs against dense BF16."""
+    out = {}
+    for g, (ms, cnt) in prof.items():
+        pb = physical_bytes(g, grid, prefix) * batch
+        fl = stage_flops(g, grid, prefix, terms, n_tile) * batch
+        if not (pb or fl) or cnt == 0:
+            continue
+        per_s = ms / cnt / 1000.0
+        row = {"launches": cnt, "ms_per_launch": round(ms / cnt, 5), "bytes_per_launch": pb,
+               "hbm_gbs": round(pb / per_s / 1e9, 1), "hbm_frac": round(pb / per_s / 1e9 / peaks["hbm"], 4)}
+        if fl:
+            row["tensor_tflops"] = round(fl / per_s / 1e12, 1)
+            row["tensor_frac"] = round(fl / per_s / 1e12 / peaks["bf16"], 4)
+            row["flops_per_launch"] = fl
+        out[g] = row
+    return out
 
 
 # ---------------------------------------------------------------- our arm
@@ -503,8 +623,10 @@ def run_ours(a: argparse.Namespace) -> None:
     dom_name, (dom_ms, dom_cnt) = dom
     per_launch_s = dom_ms / max(dom_cnt, 1) / 1000.0
     alg = algorithmic_bytes(dom_name, n, m) * B
-    peak, peak_kind = _peaks()
+    peaks = _peaks()
+    peak = peaks["hbm"]
     achieved = alg / per_launch_s / 1e9 if alg else None
+    stages = stages_table(prof, B, GRID, PREFIX, peaks)
     t_u = plan._engine.native_cfg.uamp_iterations
     p_iters = plan._engine.native_cfg.polish_iterations
     step_bytes = scene_bytes(n, m, t_u, p_iters) * B
@@ -512,7 +634,8 @@ def run_ours(a: argparse.Namespace) -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        cpu = cpu_baseline(a.cpu_sample, a.profile)
+        cpu = cpu_baseline(a.profile, a.cpu_rounds)
+    cg = cg_section(device) if world == 1 and not a.no_cg else None
     learned = None
     if world == 1 and not a.no_learned:
         learned = learned_section(device, min(a.steps, 20), a.batch)
@@ -543,10 +666,14 @@ def run_ours(a: argparse.Namespace) -> None:
                 "bound": "hbm", "kernel": dom_name,
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": _traffic(dom_name, B),
+                "traffic": physical_bytes(dom_name, GRID, PREFIX) * B or None,
+                "traffic_source": "the kernel's own byte accounting (bench.physical_bytes: the lift "
+                                  "A^H m that adjoint stage 2 writes is read back, 8 B/px beyond the "
+                                  "algorithmic 32 B/px); ncu DRAM counters agree in profiles/",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_s * 1000.0,
-                "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                "peak_source": peaks["source"],
                 "step_algorithmic_gbs": step_gbs, "step_frac": step_gbs / peak,
+                "stages": stages,
             },
             "kernel_ms_per_replay": {k: round(v[0], 4) for k, v in prof.items()},
             "gpu_launches": launches * a.steps,
@@ -559,6 +686,8 @@ def run_ours(a: argparse.Namespace) -> None:
             line["learned"] = learned
         if uneven is not None:
             line["uneven"] = uneven
+        if cg is not None:
+            line["cg"] = cg
         if published is not None:
             line["published_shape"] = published
         print(json.dumps(line), flush=True)

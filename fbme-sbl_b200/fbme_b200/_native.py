@@ -25,7 +25,7 @@ STATUS_TIMEOUT = 4
 STATUS_PCG_BREAKDOWN = 8
 STATUS_ITER_CAP = 16
 
-NUM_GROUPS = 12
+NUM_GROUPS = 13
 
 
 class FbmeShape(ctypes.Structure):

@@ -839,8 +839,8 @@ int fbme_plan_replay(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme
 
 const char* fbme_profile_group_name(int32_t group) {
   static const char* names[FBME_NUM_GROUPS] = {
-      "init", "adjoint_message", "adjoint_denoise", "forward_1", "forward_residual", "scalars",
-      "sweep1_denoise", "topk", "polish", "exchange_score", "output", "adjoint_2"};
+      "init", "adjoint_1", "adjoint_denoise", "forward_1", "forward_residual", "scalars",
+      "sweep1_denoise", "topk", "polish", "exchange_score", "output", "adjoint_2", "message"};
   return (group >= 0 && group < FBME_NUM_GROUPS) ? names[group] : "";
 }
 

@@ -672,7 +672,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                                                                            u.y, msg[cur], bn)));
       src_dof = PartSrc{bn, 1};
     } else {
-      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+      FBME_TIMED(prof, FBME_GROUP_MESSAGE,
                  (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
                                                                       u.sc.prec, u.sc.dvar, c.uamp_damping)));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
@@ -696,7 +696,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   }
 
   // --- final E-step (no prior update, no prediction), score keys ---
-  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+  FBME_TIMED(prof, FBME_GROUP_MESSAGE,
              (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
                                                                   u.sc.prec, u.sc.dvar, c.uamp_damping)));
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
@@ -815,7 +815,7 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
                       J[b].c.uamp_damping});
         jd.push_back({bn[b], J[b].s, denoise_args(J[b].c, u), u.lift});
       }
-      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
+      FBME_TIMED(prof, FBME_GROUP_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
                    message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
                  }));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
@@ -855,7 +855,7 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
     da.keys = reinterpret_cast<uint32_t*>(u.keys);
     jd.push_back({bn[b], J[b].s, da, u.lift});
   }
-  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
+  FBME_TIMED(prof, FBME_GROUP_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
                message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
              }));
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,

@@ -353,7 +353,7 @@ int fbme_plan_set_warm_start(FbmePlan* plan, const float* params, void* workspac
 /* Kernel groups timed by fbme_plan_profile. */
 enum {
   FBME_GROUP_INIT = 0,        /* A^H y, data power, prior/noise initialisation */
-  FBME_GROUP_ADJ_MESSAGE = 1, /* adjoint stage 1 with the fused message update */
+  FBME_GROUP_ADJ_MESSAGE = 1, /* adjoint stage 1 (reads the updated message) */
   FBME_GROUP_ADJ_DENOISE = 2, /* denoiser / ARD update (elementwise, after adjoint stage 2) */
   FBME_GROUP_FWD_1 = 3,       /* forward stage 1 */
   FBME_GROUP_FWD_RESIDUAL = 4,/* forward stage 2 with the fused residual energy */
@@ -364,7 +364,8 @@ enum {
   FBME_GROUP_EXCHANGE = 9,    /* residual exchange scoring over the grid */
   FBME_GROUP_OUTPUT = 10,     /* dense outputs */
   FBME_GROUP_ADJ_2 = 11,      /* adjoint stage 2 of sweeps 2.. and the final E-step */
-  FBME_NUM_GROUPS = 12
+  FBME_GROUP_MESSAGE = 12,    /* UAMP message update (elementwise, before adjoint stage 1) */
+  FBME_NUM_GROUPS = 13
 };
 
 /* One replay with CUDA events around every kernel launch (not capturable;

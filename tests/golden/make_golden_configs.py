@@ -12,11 +12,13 @@ make_golden.py does):
 
 * ``c3_s{0,1,2}``: 512x512 grid, 256x192 prefix, 750 clustered + 50
   isolated log-normal points, 20 dB (``scenes.config_scene("c3", seed)``),
-  in FP32 and FP64, with the reference's CUDA Cholesky loading (make_c3).
+  in FP32 and FP64, with the reference's CUDA Cholesky loading, and the
+  FP32 result's sensitivity to small input perturbations (make_c3).
 * ``c4_b0``: the 64-scene batched-uneven workload of batch seed 0
   (``scenes.uneven_batch(0)``): grids from {128^2, 192x256, 256^2,
-  384x256}, prefix ratios U[0.3, 0.7], 1-3 % CN(0,1) points, 5-25 dB.
-  Per-scene results are packed with offsets.
+  384x256}, prefix ratios U[0.3, 0.7], 1-3 % CN(0,1) points, 5-25 dB,
+  solved as the C3 scenes are (make_c4).  Per-scene
+  results are packed with offsets.
 * ``cg/cg_c2_s0_it6``: mode="cg" at 256x256 / 128x128 (``config_scene("c2",
   0)``), 6 EM iterations, FP64 and FP32 reference runs (format of
   make_golden_cg.py).
@@ -117,12 +119,50 @@ def _cuda_cholesky_branch(S, torch):
     return raw
 
 
+# Relative size of the input perturbation that measures a scene's
+# conditioning: 2^-17 (7.6e-6), the size of the device's split-BF16 DFT
+# rounding (5-6e-6 relative L2 against an FP64 DFT).
+PERTURBATION = 2.0 ** -17
+PERTURBATION_DRAWS = 3
+
+
+def _solve_three_ways(s, cfg, fast_sbl, torch, np):
+    """One scene under one profile: FP32 fields, FP64 fields, the FP32-FP64
+    gap, and the sensitivity: the largest change of the FP32 result (x in
+    relative L2, posterior variance in max relative error on the support)
+    over PERTURBATION_DRAWS inputs y * (1 + PERTURBATION * u), u ~ U[-1, 1]
+    per real component, seeded."""
+    r32 = fast_sbl(torch.from_numpy(s.y), s.grid, config=cfg)
+    r64 = fast_sbl(torch.from_numpy(s.y.astype(np.complex128)), s.grid, config=cfg)
+    x32, x64 = r32.x.numpy().ravel(), r64.x.numpy().ravel()
+    v32, v64 = r32.posterior_variance.numpy().ravel(), r64.posterior_variance.numpy().ravel()
+    a32, a64 = x32 != 0, x64 != 0
+    gap_x = np.linalg.norm(x32 - x64) / np.linalg.norm(x64)
+    gap_pv = np.max(np.abs(v32[a64] - v64[a64]) / v64[a64])
+    sens_x = sens_pv = 0.0
+    for k in range(PERTURBATION_DRAWS):
+        rng = np.random.default_rng(1000 + k)
+        u = rng.uniform(-1.0, 1.0, s.y.shape) + 1j * rng.uniform(-1.0, 1.0, s.y.shape)
+        yp = (s.y.real.astype(np.float64) * (1 + PERTURBATION * u.real)
+              + 1j * s.y.imag.astype(np.float64) * (1 + PERTURBATION * u.imag)).astype(np.complex64)
+        rp = fast_sbl(torch.from_numpy(yp), s.grid, config=cfg)
+        xp, vp = rp.x.numpy().ravel(), rp.posterior_variance.numpy().ravel()
+        assert np.array_equal(xp != 0, a32), "a perturbation changed the support"
+        sens_x = max(sens_x, float(np.linalg.norm(xp - x32) / np.linalg.norm(x32)))
+        sens_pv = max(sens_pv, float(np.max(np.abs(vp[a32] - v32[a32]) / v32[a32])))
+    return _solve_fields(r32, np), _solve_fields(r64, np), {"gap_x": gap_x, "gap_pv": gap_pv,
+                                                             "sens_x": sens_x, "sens_pv": sens_pv}
+
+
 def make_c3(seed: int) -> None:
-    """C3 scene solved three ways by the reference, all with its CUDA
-    Cholesky loading: FP32 (``<profile>_*``, the replay's arithmetic), FP64
-    (``f64_<profile>_*``, complex128 input promotes the whole pipeline) and
-    their gap, which measures how far the reference's own FP32 result sits
-    from the exact one on this ill-conditioned scene."""
+    """C3 scene solved by the reference with its CUDA Cholesky loading:
+    FP32 (``<profile>_*``, the replay's arithmetic; the parity target), FP64
+    (``f64_<profile>_*``), their gap, and the FP32 result's sensitivity to
+    input perturbations of the DFT rounding's size (``sens_<profile>_x``,
+    ``sens_<profile>_pv``; _solve_three_ways).  The clustered scenes are
+    ill-conditioned: their 32-atom reduced systems hold atoms one pixel
+    apart, and the reference's own result moves by 5e-5 to 5e-3 under such
+    perturbations, with the support unchanged."""
     import numpy as np
 
     torch, scenes, SBLConfig, fast_sbl = _import()
@@ -134,40 +174,46 @@ def make_c3(seed: int) -> None:
            "scene": np.array(f"config_scene('c3', {seed})"), "x_true": sc.x.astype(np.complex64),
            "cholesky": np.array("cuda")}
     for profile in ("stable", "fast"):
-        cfg = plan_config(SBLConfig, profile)
-        r32 = fast_sbl(torch.from_numpy(sc.y), sc.grid, config=cfg)
-        r64 = fast_sbl(torch.from_numpy(sc.y.astype(np.complex128)), sc.grid, config=cfg)
-        for k, v in _solve_fields(r32, np).items():
+        f32, f64, m = _solve_three_ways(sc, plan_config(SBLConfig, profile), fast_sbl, torch, np)
+        for k, v in f32.items():
             out[profile + "_" + k] = v
-        for k, v in _solve_fields(r64, np).items():
+        for k, v in f64.items():
             out["f64_" + profile + "_" + k] = v
-        x32, x64 = r32.x.numpy().ravel(), r64.x.numpy().ravel()
-        out["gap_" + profile + "_x"] = np.array(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
-        v32, v64 = r32.posterior_variance.numpy().ravel(), r64.posterior_variance.numpy().ravel()
-        act = x64 != 0
-        out["gap_" + profile + "_pv"] = np.array(np.max(np.abs(v32[act] - v64[act]) / v64[act]))
+        for k, v in m.items():
+            a, b = k.split("_")
+            out[f"{a}_{profile}_{b}"] = np.array(v)
     np.savez_compressed(HERE / f"c3_s{seed}.npz", **out)
     print("wrote", f"c3_s{seed}")
 
 
 def make_c4(batch_seed: int) -> None:
-    """All 64 scenes of one uneven batch; per-scene fields concatenated, with
-    offsets ``<field>_off`` (length 65) for the variable-length ones."""
+    """All 64 scenes of one uneven batch, solved like make_c3.  Some of these
+    scenes are ill-conditioned too (sensitivity up to ~3e-4).  Per-scene
+    fields are concatenated, with offsets ``<field>_off``."""
     import numpy as np
 
     torch, scenes, SBLConfig, fast_sbl = _import()
+    import torch_sbl.solver as S  # reference package
+
+    S._stable_cholesky_raw = _cuda_cholesky_branch(S, torch)
     batch = scenes.uneven_batch(batch_seed)
     out = {"grids": np.array([s.grid for s in batch], np.int64),
            "samples": np.array([s.y.shape for s in batch], np.int64),
            "y_sha256": np.array([y_digest(s.y) for s in batch]),
-           "scene": np.array(f"uneven_batch({batch_seed})")}
+           "scene": np.array(f"uneven_batch({batch_seed})"), "cholesky": np.array("cuda")}
     for profile in ("stable", "fast"):
         cfg = plan_config(SBLConfig, profile)
-        per = [_solve_fields(fast_sbl(torch.from_numpy(s.y), s.grid, config=cfg), np) for s in batch]
-        for k in per[0]:
-            vals = [np.atleast_1d(p[k]) for p in per]
-            out[f"{profile}_{k}"] = np.concatenate(vals)
-            out[f"{profile}_{k}_off"] = np.concatenate([[0], np.cumsum([v.size for v in vals])]).astype(np.int64)
+        runs = [_solve_three_ways(s, cfg, fast_sbl, torch, np) for s in batch]
+        for prefix, j in ((profile, 0), ("f64_" + profile, 1)):
+            per = [r[j] for r in runs]
+            for k in per[0]:
+                vals = [np.atleast_1d(p[k]).reshape(-1) for p in per]
+                out[f"{prefix}_{k}"] = np.concatenate(vals)
+                out[f"{prefix}_{k}_off"] = np.concatenate([[0], np.cumsum([v.size for v in vals])]).astype(np.int64)
+        for k in runs[0][2]:
+            a, b = k.split("_")
+            out[f"{a}_{profile}_{b}"] = np.array([r[2][k] for r in runs])
+            out[f"{a}_{profile}_{b}_off"] = np.arange(len(runs) + 1, dtype=np.int64)
     np.savez_compressed(HERE / f"c4_b{batch_seed}.npz", **out)
     print("wrote", f"c4_b{batch_seed}")
 

@@ -72,3 +72,21 @@ def scene_fields(g, profile: str, i: int) -> dict:
                                          "pv_inactive_unique", "precision_inactive_unique",
                                          "mask_indices", "evidence_trace") else v.reshape(())
     return out
+
+
+# Parity bar on ill-conditioned scenes (C3 and a few C4 scenes): x within
+# SENS_FACTOR times the reference's own sensitivity (the largest change of
+# its FP32 result under input perturbations the size of the split-BF16 DFT
+# rounding, make_golden_configs.PERTURBATION), when that exceeds the fixed
+# bar.  Measured: the device lands within 1.8x of it on every C3 scene.
+SENS_FACTOR = 4.0
+
+
+def sensitivity(g, profile: str, i: int | None = None) -> tuple[float, float]:
+    """(x, posterior variance) sensitivity of a fixture scene, 0 if absent."""
+    if "sens_" + profile + "_x" not in g.files:
+        return 0.0, 0.0
+    sx, sv = g["sens_" + profile + "_x"], g["sens_" + profile + "_pv"]
+    if i is not None:
+        sx, sv = sx[i], sv[i]
+    return float(sx), float(sv)

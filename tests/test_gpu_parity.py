@@ -13,14 +13,11 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from golden_util import PLAN_FILES, UNEVEN_FILES, plan_case, scene_fields, uneven_case
+from golden_util import (PLAN_FILES, SENS_FACTOR, UNEVEN_FILES, plan_case, scene_fields, sensitivity,
+                         uneven_case)
 from gpu_util import PV_TOL, X_TOL, need_gpu, rel_l2
 
 torch = pytest.importorskip("torch")
-
-# C3 (ill-conditioned clustered scenes): distance to the reference's FP64
-# result in units of the reference's own FP32-vs-FP64 gap.
-C3_GAP_FACTOR = 5.0
 
 
 def _plan(profile, y, grid):
@@ -30,22 +27,30 @@ def _plan(profile, y, grid):
     return make(y, grid, polish_size=32, warmup=1)
 
 
-def _check_plan_fields(res, g, profile, b=None, label=""):
-    """One scene's plan result against a reference fixture's fields."""
+def _check_plan_fields(res, g, profile, sens=(0.0, 0.0), label=""):
+    """One scene's plan result against a reference fixture's fields.  On an
+    ill-conditioned scene (sens = the reference's own sensitivity, see
+    golden_util.SENS_FACTOR) the value bars widen to SENS_FACTOR * sens."""
     p = profile + "_"
-    sel = (lambda t: t.cpu().numpy().reshape(-1)) if b is None else (lambda t: t[b].cpu().numpy().reshape(-1))
+    sel = lambda t: t.cpu().numpy().reshape(-1)  # noqa: E731
+    x_tol, pv_tol = max(X_TOL, SENS_FACTOR * sens[0]), max(PV_TOL, SENS_FACTOR * sens[1])
+    s_tol = max(1e-4, SENS_FACTOR * sens[0])
     x = sel(res.x)
     act = np.flatnonzero(x)
     assert set(act) == set(g[p + "active"]), label
     xr = np.zeros_like(x)
     xr[g[p + "active"]] = g[p + "x_active"]
-    assert rel_l2(x, xr) < X_TOL, (label, rel_l2(x, xr))
+    err = rel_l2(x, xr)
+    if sens[0] > 0:
+        print(f"{label} {profile}: x {err:.2e} (bar {x_tol:.2e}, reference sensitivity {sens[0]:.2e})")
+    assert err < x_tol, (label, err, x_tol)
     pv = sel(res.posterior_variance)
-    np.testing.assert_allclose(pv[g[p + "active"]], g[p + "pv_active"], rtol=PV_TOL, err_msg=label)
+    np.testing.assert_allclose(pv[g[p + "active"]], g[p + "pv_active"], rtol=pv_tol, err_msg=label)
     for f in ("noise_variance", "negative_log_evidence", "evidence_trace", "effective_dof"):
-        np.testing.assert_allclose(sel(getattr(res, f)), np.reshape(g[p + f], -1), rtol=1e-4, err_msg=label + f)
+        np.testing.assert_allclose(sel(getattr(res, f)), np.reshape(g[p + f], -1), rtol=s_tol, err_msg=label + f)
     assert np.array_equal(np.flatnonzero(sel(res.support_mask)), g[p + "mask_indices"]), label
     assert int(sel(res.status)[0]) == 0, label
+    assert res.iterations == int(np.reshape(g[p + "iterations"], -1)[0]), label
     if profile == "stable":
         assert int(sel(res.support_exchanges_accepted)[0]) == int(g[p + "support_exchanges_accepted"]), label
         assert bool(sel(res.fixed_budget_monotone)[0]) == bool(g[p + "fixed_budget_monotone"]), label
@@ -53,6 +58,8 @@ def _check_plan_fields(res, g, profile, b=None, label=""):
             dev, ref = float(sel(getattr(res, f))[0]), float(np.reshape(g[p + f], -1)[0])
             print(f"{label} {f}: device {dev:.7g} reference {ref:.7g} rel {abs(dev - ref) / abs(ref):.2e}")
             np.testing.assert_allclose(dev, ref, rtol=2e-2, atol=1e-6, err_msg=label + f)
+    else:
+        assert res.fixed_budget_monotone is None and res.support_exchanges_accepted is None
 
 
 @pytest.mark.gpu
@@ -63,34 +70,7 @@ def test_plan_matches_reference_golden(path, profile):
     y_np, grid, g = plan_case(path)
     y = torch.from_numpy(y_np).cuda()
     res = _plan(profile, y, grid).replay(y, synchronize=True)
-    p = profile + "_"
-    if "cholesky" in g.files:
-        # C3: identical support; x as close to the reference's FP64 answer
-        # as a few times the reference's own FP32 error on this scene
-        x = res.x.cpu().numpy().reshape(-1)
-        act = np.flatnonzero(x)
-        assert set(act) == set(g[p + "active"]) == set(g["f64_" + p + "active"])
-        x64 = np.zeros_like(x)
-        x64[g["f64_" + p + "active"]] = g["f64_" + p + "x_active"]
-        x32 = np.zeros_like(x)
-        x32[g[p + "active"]] = g[p + "x_active"]
-        gap = float(g["gap_" + p + "x"])
-        err64, err32 = rel_l2(x, x64), rel_l2(x, x32)
-        print(f"{Path(path).stem} {profile}: x vs FP64 {err64:.2e} vs FP32 {err32:.2e} "
-              f"(reference FP32 vs FP64 {gap:.2e})")
-        assert err64 < C3_GAP_FACTOR * gap + X_TOL
-        pv = res.posterior_variance.cpu().numpy().reshape(-1)
-        a64 = g["f64_" + p + "active"]
-        pv_err = np.max(np.abs(pv[a64] - g["f64_" + p + "pv_active"]) / g["f64_" + p + "pv_active"])
-        print(f"  posterior variance vs FP64 {pv_err:.2e} (reference gap {float(g['gap_' + p + 'pv']):.2e})")
-        assert pv_err < C3_GAP_FACTOR * float(g["gap_" + p + "pv"]) + PV_TOL
-        assert res.iterations == int(g[p + "iterations"])
-        assert int(res.status.item()) == 0
-        return
-    _check_plan_fields(res, g, profile, label=Path(path).stem)
-    assert res.iterations == int(g[p + "iterations"])
-    if profile == "fast":
-        assert res.fixed_budget_monotone is None and res.support_exchanges_accepted is None
+    _check_plan_fields(res, g, profile, sensitivity(g, profile), label=Path(path).stem)
 
 
 @pytest.mark.gpu
@@ -108,9 +88,8 @@ def test_uneven_plan_matches_reference_golden(path, profile):
     results = plan.replay(ys, synchronize=True)
     assert len(results) == len(batch)
     for i, r in enumerate(results):
-        f = scene_fields(g, profile, i)
-        _check_plan_fields(r, f, profile, label=f"scene {i} {batch[i].grid}/{batch[i].y.shape}")
-        assert r.iterations == int(f[profile + "_iterations"])
+        _check_plan_fields(r, scene_fields(g, profile, i), profile, sensitivity(g, profile, i),
+                           label=f"scene {i} {batch[i].grid}/{batch[i].y.shape}")
 
 
 @pytest.mark.gpu
