@@ -184,6 +184,10 @@ SIGNATURES = {
     "fbme_uamp_run": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fbme_polish_run": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
     "fbme_plan_state": (c_int, [c_void_p, POINTER(FbmeState)]),
+    "fbme_selftest_workspace_bytes": (c_size_t, []),
+    "fbme_selftest_stage_timeout": (c_int, [c_void_p, c_size_t, c_void_p, c_int64, c_void_p]),
+    "fbme_uamp_prior_update": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int64, c_float,
+                                       c_float, c_float, c_float, c_void_p, c_void_p]),
     "fbme_plan_profile": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p,
                                   POINTER(c_float), POINTER(c_int32), c_int32]),
     "fbme_profile_group_name": (c_char_p, [c_int32]),

@@ -882,6 +882,38 @@ int fbme_plan_profile(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbm
   return rc;
 }
 
+int fbme_uamp_prior_update(const void* mean, const float* posterior_variance, const float* old_prior,
+                           const float* prior_floor, int32_t batch, int64_t n, float hyper_shape,
+                           float hyper_rate, float damping, float maximum, float* out,
+                           fbme_stream_t stream) {
+  if (!mean || !posterior_variance || !old_prior || !prior_floor || !out)
+    return fail(FBME_ERR_INVALID, "NULL argument");
+  if (batch < 1 || batch > 65535 || n < 1)
+    return fail(FBME_ERR_INVALID, "batch must be in [1, 65535] and n positive");
+  if ((n + 1023) / 1024 > 0x7fffffffLL) return fail(FBME_ERR_INVALID, "n too large");
+  if ((reinterpret_cast<uintptr_t>(mean) & 7u) != 0 || (reinterpret_cast<uintptr_t>(posterior_variance) & 3u) != 0 ||
+      (reinterpret_cast<uintptr_t>(old_prior) & 3u) != 0 || (reinterpret_cast<uintptr_t>(out) & 3u) != 0)
+    return fail(FBME_ERR_INVALID, "misaligned complex64 / float32 buffer");
+  fbme::uamp_prior_update(static_cast<const float2*>(mean), posterior_variance, old_prior, prior_floor, batch, n,
+                          hyper_shape, hyper_rate, damping, maximum, out,
+                          reinterpret_cast<cudaStream_t>(stream));
+  return check_launch("fbme_uamp_prior_update");
+}
+
+size_t fbme_selftest_workspace_bytes(void) { return fbme::stage_selftest_bytes(); }
+
+int fbme_selftest_stage_timeout(void* workspace, size_t workspace_bytes, int32_t* status, int64_t wait_cycles,
+                                fbme_stream_t stream) {
+  if (!workspace || !status) return fail(FBME_ERR_INVALID, "NULL argument");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0 || workspace_bytes < fbme::stage_selftest_bytes())
+    return fail(FBME_ERR_WORKSPACE, "workspace smaller than fbme_selftest_workspace_bytes() or not 256-byte aligned");
+  if (wait_cycles < 1000 || wait_cycles > 2000000000LL)
+    return fail(FBME_ERR_INVALID, "wait_cycles must be in [1e3, 2e9]");
+  const cudaError_t e = fbme::stage_selftest(workspace, status, wait_cycles, reinterpret_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(FBME_ERR_CUDA, std::string("fbme_selftest_stage_timeout: ") + cudaGetErrorString(e));
+  return FBME_OK;
+}
+
 size_t fbme_topk_workspace_bytes(int64_t n, int32_t k, int32_t batch) {
   if (fbme::topk_check(n, k, batch)) return 0;
   return fbme::topk_scratch_bytes(n, k, batch);

@@ -110,13 +110,14 @@ FBME_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
   return ok != 0;
 }
-// Bounded wait: ~0.5 s of SM clock at most.
+// Bounded wait: ~0.5 s of SM clock at most by default; launches may pass a
+// shorter limit.
 constexpr long long kWaitCycles = 1000000000LL;
-FBME_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
+FBME_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, long long limit = kWaitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       record_status(status, FBME_STATUS_TIMEOUT);
       return false;
     }

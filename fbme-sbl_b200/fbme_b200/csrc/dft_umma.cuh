@@ -158,6 +158,8 @@ struct StageSet {
   int n;
   int tile0[NI + 1];
   StageItem<Pro, Epi> it[NI];
+  long long wait_cycles = kWaitCycles;  // limit of every mbarrier wait
+  int hold = 0;  // nonzero: the producer issues nothing (failure-detection self-test)
   // Item of a tile: the last i with tile0[i] <= tile.
   FBME_DEV int find(int tile) const {
     if constexpr (NI == 1) {
@@ -185,7 +187,9 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
   uint64_t* empty_bar = full_bar + kStages;
   uint64_t* accf_bar = empty_bar + kStages;  // [2]
   uint64_t* acce_bar = accf_bar + 2;         // [2]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce_bar + 2);
+  uint64_t* drain_bar = acce_bar + 2;        // MMA completion before TMEM release
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
+  const long long wlim = set.wait_cycles;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = set.tile0[set.n];
@@ -199,6 +203,7 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
       mbar_init(&accf_bar[a], 1);
       mbar_init(&acce_bar[a], kEpiThreads / 32);
     }
+    mbar_init(drain_bar, 1);
     fence_mbar_init();
   }
   if (warp == kMmaWarp) tmem_alloc(tmem_slot, 2 * N_TILE);
@@ -223,7 +228,9 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
       soff[i] = sw128_offset((pw + kProWarps * i) * 2 + (lane >> 4), q * 4);
     bool ok = true;
     int it = 0;
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    // A held producer (self-test) issues no load, copy or arrive: the
+    // issuer's and the epilogue's waits run out instead.
+    for (int tile = blockIdx.x; tile < ntiles && ok && !set.hold; tile += gridDim.x) {
       const int ii = set.find(tile);
       const DftGeom& g = set.it[ii].g;
       Pro pro = set.it[ii].pro;  // per tile: accumulators start from the launch's values
@@ -251,7 +258,7 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
         auto store_all = [&](int kcc, const typename Pro::Frag(&f)[kProIters]) -> bool {
           const int s = it % kStages, use = it / kStages;
           uint8_t* st = smem + s * C::kStageBytes;
-          if (it >= kStages && !mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene)) return false;
+          if (it >= kStages && !mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene, wlim)) return false;
           if (tid == 0) {
             asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;"
                          ::"r"(smem_u32(&full_bar[s])), "r"(uint32_t(A_PARTS * C::kPartBytesB))
@@ -306,7 +313,7 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
             pro.fetch(t, er + j0, er >= 0 ? avail : 0, f[i]);
           }
           if (b0 == 0) {
-            if (it >= kStages) ok = mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene);
+            if (it >= kStages) ok = mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene, wlim);
             if (!ok) break;
             if (tid == 0) {
               asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;"
@@ -342,22 +349,25 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
   } else if (warp == kMmaWarp) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      bool ok = true;
+      bool ok = true, issued = false;
       int it = 0, lt = 0;
+      int* st_last = nullptr;
       for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++lt) {
         const int ii = set.find(tile);
         const DftGeom& g = set.it[ii].g;
         const TileCtx t = decode_tile(g, tile - set.tile0[ii]);
         int* const st_scene = set.it[ii].status ? set.it[ii].status + t.scene / g.status_div : nullptr;
+        st_last = st_scene;
         const int acc = lt & 1, ause = lt >> 1;
-        if (lt >= 2) ok = mbar_wait(&acce_bar[acc], (ause - 1) & 1, st_scene);
+        if (lt >= 2) ok = mbar_wait(&acce_bar[acc], (ause - 1) & 1, st_scene, wlim);
         if (!ok) break;
         tc_fence_after();
         const uint32_t dtm = tmem + static_cast<uint32_t>(acc * N_TILE);
         for (int kc = 0; kc < g.kchunks && ok; ++kc, ++it) {
           const int s = it % kStages, use = it / kStages;
-          ok = mbar_wait(&full_bar[s], use & 1, st_scene);
+          ok = mbar_wait(&full_bar[s], use & 1, st_scene, wlim);
           if (!ok) break;
+          issued = true;
           tc_fence_after();
           const uint32_t a0 = smem_u32(smem + s * C::kStageBytes);
           const uint32_t b0 = a0 + A_PARTS * kPartBytesA;
@@ -372,7 +382,14 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
           }
           umma_commit(&empty_bar[s]);
         }
-        umma_commit(&accf_bar[acc]);
+        if (ok) umma_commit(&accf_bar[acc]);
+      }
+      // After a timeout, MMAs issued before it may still be running: wait
+      // (bounded) until they have completed, so tensor memory is released
+      // only once nothing writes it.
+      if (!ok && issued) {
+        umma_commit(drain_bar);
+        mbar_wait(drain_bar, 0, st_last, wlim);
       }
     }
     __syncwarp();
@@ -390,7 +407,7 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
       const TileCtx t = decode_tile(g, tile - set.tile0[ii]);
       int* const st_scene = set.it[ii].status ? set.it[ii].status + t.scene / g.status_div : nullptr;
       const int acc = lt & 1;
-      ok = mbar_wait(&accf_bar[acc], (lt >> 1) & 1, st_scene);
+      ok = mbar_wait(&accf_bar[acc], (lt >> 1) & 1, st_scene, wlim);
       tc_fence_after();
       if (ok) {
         const uint32_t base = tmem + static_cast<uint32_t>(acc * N_TILE) +

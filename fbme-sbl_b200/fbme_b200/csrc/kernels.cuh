@@ -155,6 +155,13 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
 size_t polish_state_bytes();
 int topk_slices(long long n);
+// Stage-kernel wait-timeout self-test (uamp.cu).
+size_t stage_selftest_bytes();
+cudaError_t stage_selftest(void* ws, int* status, long long wait_cycles, cudaStream_t st);
+// Unfused variational ARD prior update (prior.cu).
+void uamp_prior_update(const float2* mean, const float* var, const float* old_prior, const float* floor_,
+                       int batch, long long n, float hyper_shape, float hyper_rate, float damping,
+                       float maximum, float* out, cudaStream_t st);
 size_t topk_scratch_bytes(long long n, int k, int batch);
 const char* topk_check(long long n, int k, int batch);
 void topk_scores(const float* scores, long long n, int k, int batch, void* scratch,

@@ -869,3 +869,38 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
 
 }  // namespace fbme
 
+
+// ---------------------------------------------------------------------------
+// failure-detection self-test of the stage kernel's bounded waits
+// ---------------------------------------------------------------------------
+namespace fbme {
+
+// One 128 x 128 output tile over one 64-wide K chunk: input 128 x 32
+// complex, output 128 x 128 complex, one 256-column twiddle block of two
+// parts (nothing of it is read: the producer is held).
+size_t stage_selftest_bytes() { return 128 * 32 * 8 + 128 * 128 * 8 + 2 * 256 * 128; }
+
+// Launch that stage with its producer held back and `wait_cycles` as the
+// wait limit: the issuer's wait for a full stage and the epilogue's wait
+// for the accumulator run out, record FBME_STATUS_TIMEOUT in *status, and
+// the kernel returns.
+cudaError_t stage_selftest(void* ws, int* status, long long wait_cycles, cudaStream_t st) {
+  uint8_t* p = static_cast<uint8_t*>(ws);
+  float2* in = reinterpret_cast<float2*>(p);
+  float2* out = reinterpret_cast<float2*>(p + 128 * 32 * 8);
+  const uint8_t* table = p + 128 * 32 * 8 + 128 * 128 * 8;
+  const DftGeom g = make_geom(1, 128, 32, 128, 32, 128 * 32, 128, 128 * 128, table, 1, 256);
+  StageSet<ProPlain, EpiStoreT, 1> set;
+  set.n = 1;
+  set.tile0[0] = 0;
+  set.tile0[1] = tiles(g);
+  set.it[0] = StageItem<ProPlain, EpiStoreT>{g, ProPlain{in}, EpiStoreT{out}, status};
+  set.wait_cycles = wait_cycles;
+  set.hold = 1;
+  cudaError_t e = set_attr<2, 256, ProPlain, EpiStoreT, 1>();
+  if (e != cudaSuccess) return e;
+  launch_set<2, 256>(set, st);
+  return cudaGetLastError();
+}
+
+}  // namespace fbme

@@ -321,3 +321,45 @@ class FBMEEngine:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------ stand-alone kernels
+def _tensor_contract(name: str, tensor: Tensor, *, dtype: torch.dtype, shape: tuple[int, ...],
+                     device: torch.device | None = None) -> None:
+    """The raw-pointer contract of the stand-alone kernels, with the
+    reference's messages (torch_sbl/triton_kernels.py:451-473)."""
+    if not tensor.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor.")
+    if tensor.dtype != dtype:
+        raise ValueError(f"{name} must have dtype {dtype}.")
+    if tuple(tensor.shape) != shape:
+        raise ValueError(f"{name} must have shape {shape}, got {tuple(tensor.shape)}.")
+    if not tensor.is_contiguous():
+        raise ValueError(f"{name} must be C-contiguous.")
+    if device is not None and tensor.device != device:
+        raise ValueError(f"{name} must be on {device}, got {tensor.device}.")
+
+
+def uamp_prior_update(mean: Tensor, posterior_variance: Tensor, old_prior: Tensor, prior_floor: Tensor, *,
+                      hyper_shape: float, hyper_rate: float, damping: float, maximum: float) -> Tensor:
+    """The unfused variational ARD update of one UAMP iteration, as
+    torch_sbl/triton_kernels.py:670-735 (uamp_prior_update): same arguments,
+    contract and errors; runs the library's fbme_uamp_prior_update kernel."""
+    if old_prior.ndim != 2:
+        raise ValueError("old_prior must have shape [B, N].")
+    batch_size, n_grid = old_prior.shape
+    dev = old_prior.device
+    _tensor_contract("mean", mean, dtype=torch.complex64, shape=(batch_size, n_grid), device=dev)
+    for name, t in (("posterior_variance", posterior_variance), ("old_prior", old_prior)):
+        _tensor_contract(name, t, dtype=torch.float32, shape=(batch_size, n_grid), device=dev)
+    _tensor_contract("prior_floor", prior_floor, dtype=torch.float32, shape=(batch_size,), device=dev)
+    out = torch.empty_like(old_prior)
+    lib = nat.lib()
+    with torch.cuda.device(dev):
+        rc = lib.fbme_uamp_prior_update(
+            ctypes.c_void_p(mean.data_ptr()), ctypes.c_void_p(posterior_variance.data_ptr()),
+            ctypes.c_void_p(old_prior.data_ptr()), ctypes.c_void_p(prior_floor.data_ptr()), batch_size, n_grid,
+            float(hyper_shape), float(hyper_rate), float(damping), float(maximum),
+            ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    nat.check(rc, "fbme_uamp_prior_update")
+    return out

@@ -226,23 +226,37 @@ def attach_warm_start(engine: FBMEEngine, net: WarmStartNet) -> Tensor:
 
 
 class LearnedSBLPlan:
-    """Warm-started FBME plan with the plain plan as fallback.
+    """Warm-started FBME plan with the plain plan as fallback, all on the device.
 
-    CUDA graphs: the warm-started solve of the whole batch (the network's
-    prior, ``sweeps`` UAMP sweeps, the profile's polish), the per-scene
-    check, and the plain locked plans of the same profile for
-    ``fallback_batch`` scenes and for 2.  ``replay`` launches the warm graph
-    and the check, solves the scenes that fail it with a plain plan (the
-    2-scene one for one or two failures, else groups of ``fallback_batch``)
-    and returns the plain results for them (this reads the failure count on
-    the host, so a replay with fallback synchronises the stream).  Results
-    are graph-owned, as for the plain plans.
+    One replay is two CUDA graphs on the caller's device:
+
+    * the warm-started solve of the whole batch (the network's prior,
+      ``sweeps`` UAMP sweeps, the profile's polish);
+    * the fallback, on a side stream after it: the per-scene check, the
+      compaction of the failing scenes into a fixed-capacity batch of
+      ``fallback_capacity`` (its unused slots repeat the first failing
+      scene), the plain locked solve of that batch, and the scatter of its
+      rows back over the failing scenes' results.
+
+    Nothing is read on the host.  More failures than the capacity are
+    flagged on the device (``overflow``); the host re-solves the excess with
+    the plain plan when the caller synchronises (``replay(synchronize=True)``,
+    ``synchronize()``, or reading ``fallbacks``).
+
+    ``pipelined=False`` (default): the caller's stream waits for the
+    fallback at the end of ``replay``, so results are complete in stream
+    order, as for the plain plans.  ``pipelined=True``: two warm plans take
+    turns, and replay i's fallback overlaps replay i+1's warm solve; replay
+    i's results are complete once the caller's stream has passed replay
+    i+1 (or after ``synchronize()``), and the replay after next overwrites
+    them.
 
     Check (per scene): finite negative log evidence, status 0, monotone
     evidence trace, and fixed-point residuals of the prior and the noise no
     larger than ``gamma_residual_max`` / ``noise_residual_max`` (above the
     90th percentiles of plain FBME-Stable solves, 0.63 and 0.006, on the
-    training distribution).
+    training distribution); ``force_fallback`` marks scenes to re-solve
+    regardless.
     """
 
     profile = "fbme-sbl-stable-learned-warm-start"
@@ -250,9 +264,8 @@ class LearnedSBLPlan:
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, net: WarmStartNet | None = None,
                  weights: str | Path = DEFAULT_WEIGHTS, sweeps: int = 1, polish_size: int = 32,
                  warmup: int = 3, profile: str = "stable", gamma_residual_max: float = 0.75,
-                 noise_residual_max: float = 0.05, fallback_batch: int = 16) -> None:
-        from torch_sbl_fastest_stable import make_fastest_plan, make_stable_plan
-
+                 noise_residual_max: float = 0.05, fallback_capacity: int = 16,
+                 pipelined: bool = False) -> None:
         from .plans import CUDAGraphSBLPlan
 
         if profile not in ("stable", "fast"):
@@ -261,107 +274,185 @@ class LearnedSBLPlan:
         cfg = plain_config(sweeps, profile)
         cfg.uamp_polish_size = polish_size
         self._ws: list[Tensor] = []
-        self._warm = CUDAGraphSBLPlan(
-            example_data, grid_shape, config=cfg, warmup=warmup,
-            engine_hook=lambda eng: self._ws.append(attach_warm_start(eng, self.net)))
-        make = make_stable_plan if profile == "stable" else make_fastest_plan
-        self.input_buffer = self._warm.input_buffer
-        self.batch = self._warm._engine.batch
-        flat = self.input_buffer.reshape(self.batch, *self.input_buffer.shape[-2:])
-        self._fb = min(int(fallback_batch), self.batch)
-        self._plain = make(flat[: self._fb].clone(), grid_shape, polish_size=polish_size, warmup=warmup)
-        # a replay usually has one or two failures: a small plan solves them
-        # at the latency of one scene instead of a 16-scene solve
-        small = min(2, self._fb)
-        self._plain_small = (make(flat[:small].clone(), grid_shape, polish_size=polish_size, warmup=warmup)
-                             if small < self._fb else self._plain)
+        self.pipelined = bool(pipelined)
+        self._warm = [
+            CUDAGraphSBLPlan(example_data, grid_shape, config=cfg, warmup=warmup,
+                             engine_hook=lambda eng: self._ws.append(attach_warm_start(eng, self.net)))
+            for _ in range(2 if self.pipelined else 1)]
+        w0 = self._warm[0]
+        self.device = w0.input_buffer.device
+        self.batch = w0._engine.batch
+        self.grid = w0._engine.grid
+        self.sample = w0._engine.sample
+        self.capacity = max(1, min(int(fallback_capacity), self.batch))
+        plain_cfg = plain_config(None, profile)
+        plain_cfg.uamp_polish_size = polish_size
+        self._plain = FBMEEngine(self.capacity, self.grid, self.sample, plain_cfg, self.device)
+        self._plain_in = torch.zeros(self.capacity, prod(self.sample), dtype=torch.complex64, device=self.device)
+        self._plain.run(self._plain_in)  # first launches outside any capture
         self.gamma_residual_max = gamma_residual_max
         self.noise_residual_max = noise_residual_max
-        self.fallbacks = 0
-        self.passed: Tensor | None = None
-        self._check_graph: torch.cuda.CUDAGraph | None = None
-        self._check_key: tuple | None = None
-        self._check_out: Tensor | None = None
-        self._rows: dict[int, tuple[list[Tensor], list[Tensor]]] = {}
+        self.force_fallback = torch.zeros(self.batch, dtype=torch.bool, device=self.device)
+        dev = dict(device=self.device)
+        self._arange_b = torch.arange(self.batch, **dev)
+        self._arange_f = torch.arange(self.capacity, **dev)
+        nw = len(self._warm)
+        self._idxbuf = [torch.zeros(self.capacity + 1, dtype=torch.int64, **dev) for _ in range(nw)]
+        self._passed = [torch.ones(self.batch, dtype=torch.bool, **dev) for _ in range(nw)]
+        self._count = [torch.zeros((), dtype=torch.int64, **dev) for _ in range(nw)]
+        self._side = torch.cuda.Stream(self.device)
+        self._warm_done = [torch.cuda.Event() for _ in range(nw)]
+        self._done = [torch.cuda.Event() for _ in range(nw)]
+        self._graphs: list[torch.cuda.CUDAGraph | None] = [None] * nw
+        self._graph_key: tuple | None = None
+        self._slot = nw - 1
+        self._pending = [False] * nw
 
+    # ------------------------------------------------------------ results
     @property
     def result(self):
-        return self._warm.result
+        return self._warm[self._slot].result
 
-    def check(self) -> Tensor:
-        """Per-scene pass flags of the last warm-started solve (device bool)."""
-        o = self._warm._engine.out
-        ok = torch.isfinite(o["negative_log_evidence"]) & (o["status"] == 0)
-        if self._warm._engine.native_cfg.fixed_budget_diagnostics:
+    @property
+    def input_buffer(self) -> Tensor:
+        return self._warm[(self._slot + 1) % len(self._warm)].input_buffer
+
+    @property
+    def passed(self) -> Tensor:
+        """Per-scene pass flags of the last replay (device bool)."""
+        return self._passed[self._slot]
+
+    @property
+    def overflow(self) -> Tensor:
+        """Device flag: the last replay had more failures than the capacity."""
+        return self._count[self._slot] > self.capacity
+
+    @property
+    def fallbacks(self) -> int:
+        """Scenes of the last replay solved by the plain plan (synchronises)."""
+        self.synchronize()
+        return int(self._count[self._slot].item())
+
+    # -------------------------------------------------------------- check
+    def check(self, slot: int = 0) -> Tensor:
+        """Per-scene pass flags of a warm plan's last solve (device bool)."""
+        eng = self._warm[slot]._engine
+        o = eng.out
+        ok = torch.isfinite(o["negative_log_evidence"]) & (o["status"] == 0) & ~self.force_fallback
+        if eng.native_cfg.fixed_budget_diagnostics:
             ok &= o["fixed_budget_monotone"]
             ok &= o["fixed_budget_gamma_residual"] <= self.gamma_residual_max
             ok &= o["fixed_budget_noise_residual"] <= self.noise_residual_max
         return ok
 
-    def _captured_check(self) -> Tensor:
-        """check() as one graph launch (its inputs are the warm plan's
-        graph-owned outputs); recaptured when the thresholds change."""
+    def _fallback_body(self, s: int) -> None:
+        """Check, compaction, plain re-solve and scatter of slot s (stream-ordered)."""
+        F = self.capacity
+        warm = self._warm[s]._engine
+        ok = self.check(s)
+        failed = ~ok
+        count = failed.sum()
+        pos = torch.cumsum(failed.to(torch.int64), 0) - 1
+        target = torch.where(failed & (pos < F), pos, torch.full_like(pos, F))
+        idxbuf = self._idxbuf[s]
+        idxbuf.zero_()
+        idxbuf.scatter_(0, target, self._arange_b)  # slot F collects the rest (discarded)
+        idx = torch.where(self._arange_f < count, idxbuf[:F], idxbuf[:1].expand(F))
+        flat = self._warm[s].input_buffer.reshape(self.batch, -1)
+        self._plain_in.copy_(flat.index_select(0, idx))
+        self._plain.run(self._plain_in)
+        any_failed = count > 0
+        for name, dst in warm.out.items():
+            src = self._plain.out[name]
+            rows = dst.index_select(0, idx)
+            sel = any_failed.view(*([1] * rows.ndim))
+            dst.index_copy_(0, idx, torch.where(sel, src, rows))
+        self._passed[s].copy_(ok)
+        self._count[s].copy_(count)
+
+    def _fallback_graph(self, s: int) -> torch.cuda.CUDAGraph:
         key = (self.gamma_residual_max, self.noise_residual_max)
-        if self._check_graph is None or self._check_key != key:
-            stream = torch.cuda.Stream(self.input_buffer.device)
-            stream.wait_stream(torch.cuda.current_stream(self.input_buffer.device))
-            with torch.cuda.stream(stream):
-                self.check()  # warm-up outside the capture
+        if self._graph_key != key:
+            self._graphs = [None] * len(self._warm)
+            self._graph_key = key
+        if self._graphs[s] is None:
+            torch.cuda.synchronize(self.device)
+            with torch.cuda.stream(self._side):
                 graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(graph, stream=stream):
-                    out = self.check()
-            torch.cuda.current_stream(self.input_buffer.device).wait_stream(stream)
-            self._check_graph, self._check_key, self._check_out = graph, key, out
-        self._check_graph.replay()
-        return self._check_out
+                with torch.cuda.graph(graph, stream=self._side):
+                    self._fallback_body(s)
+            torch.cuda.synchronize(self.device)
+            self._graphs[s] = graph
+        return self._graphs[s]
 
-    def _row_views(self, plan) -> tuple[list[Tensor], list[Tensor]]:
-        """The per-scene fields of the warm and of a fallback plan's results,
-        as (batch-leading) tensor pairs; the results are graph-owned, so the
-        pairs are found once per fallback plan."""
-        key = id(plan)
-        if key not in self._rows:
-            res, pres = self._warm.result, plan.result
-            nb = plan.input_buffer.reshape(-1, *plan.input_buffer.shape[-2:]).shape[0]
-            dst, src = [], []
-            for f in fields(res):
-                v, pv = getattr(res, f.name), getattr(pres, f.name)
-                if (isinstance(v, Tensor) and isinstance(pv, Tensor) and v.ndim >= 1
-                        and v.shape[1:] == pv.shape[1:] and v.shape[0] == self.batch and pv.shape[0] == nb):
-                    dst.append(v)
-                    src.append(pv)
-            self._rows[key] = (dst, src)
-        return self._rows[key]
-
+    # -------------------------------------------------------------- replay
     def replay(self, data: Tensor | None = None, *, synchronize: bool = False, fallback: bool = True):
-        res = self._warm.replay(data, synchronize=False)
-        self.passed = self._captured_check()
-        self.fallbacks = 0
-        if fallback:
-            bad = (~self.passed).nonzero().flatten().tolist()
-            self.fallbacks = len(bad)
-            flat = self.input_buffer.reshape(self.batch, *self.input_buffer.shape[-2:])
-            for c0 in range(0, self.fallbacks, self._fb):
-                # the failed scenes, in groups of a fallback plan's batch (the
-                # last group padded with its first scene)
-                idx = bad[c0:c0 + self._fb]
-                plan = self._plain_small if len(idx) <= self._plain_small.input_buffer.reshape(
-                    -1, *flat.shape[-2:]).shape[0] else self._plain
-                pin = plan.input_buffer.reshape(-1, *flat.shape[-2:])
-                take = idx + idx[:1] * (pin.shape[0] - len(idx))
-                torch._foreach_copy_([pin[j] for j in range(len(take))], [flat[i] for i in take])
-                plan.replay()
-                dst, src = self._row_views(plan)
-                torch._foreach_copy_([v[i] for v in dst for i in idx],
-                                     [pv[j] for pv in src for j in range(len(idx))])
+        nw = len(self._warm)
+        s = (self._slot + 1) % nw
+        main = torch.cuda.current_stream(self.device)
+        graph = self._fallback_graph(s) if fallback else None
+        if self._pending[s]:
+            main.wait_event(self._done[s])  # the replay before last still fills this slot
+        res = self._warm[s].replay(data, synchronize=False)
+        self._slot = s
+        if graph is None:
+            self._pending[s] = False
+            self._count[s].zero_()
+            self._passed[s].copy_(self.check(s))
+        else:
+            self._warm_done[s].record(main)
+            self._side.wait_event(self._warm_done[s])
+            with torch.cuda.stream(self._side):
+                graph.replay()
+            self._done[s].record(self._side)
+            self._pending[s] = True
+            if not self.pipelined:
+                main.wait_event(self._done[s])
         if synchronize:
-            torch.cuda.synchronize(self.input_buffer.device)
+            self.synchronize()
         return res
+
+    def join(self) -> None:
+        """Make the caller's stream wait for every pending fallback (no host
+        synchronisation; failures beyond the capacity stay flagged)."""
+        main = torch.cuda.current_stream(self.device)
+        for s in range(len(self._warm)):
+            if self._pending[s]:
+                main.wait_event(self._done[s])
+
+    def synchronize(self) -> None:
+        """Wait for every replay's fallback; re-solve on the host the
+        failures beyond the device capacity."""
+        for s in range(len(self._warm)):
+            if self._pending[s]:
+                self._done[s].synchronize()
+                self._pending[s] = False
+                self._host_overflow(s)
+        torch.cuda.synchronize(self.device)
+
+    def _host_overflow(self, s: int) -> None:
+        n = int(self._count[s].item())
+        if n <= self.capacity:
+            return
+        bad = (~self._passed[s]).nonzero().flatten().tolist()[self.capacity:]
+        warm = self._warm[s]._engine
+        flat = self._warm[s].input_buffer.reshape(self.batch, -1)
+        F = self.capacity
+        for c0 in range(0, len(bad), F):
+            grp = bad[c0:c0 + F]
+            take = grp + grp[:1] * (F - len(grp))
+            self._plain_in.copy_(flat[take])
+            self._plain.run(self._plain_in)
+            sel = torch.tensor(grp, device=self.device)
+            for name, dst in warm.out.items():
+                dst.index_copy_(0, sel, self._plain.out[name][: len(grp)])
 
 
 def make_learned_plan(example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
                       warmup: int = 3, sweeps: int = 1, weights: str | Path = DEFAULT_WEIGHTS,
-                      profile: str = "stable") -> LearnedSBLPlan:
+                      profile: str = "stable", pipelined: bool = False,
+                      fallback_capacity: int = 16) -> LearnedSBLPlan:
     """Build the warm-started plan (same call shape as make_stable_plan)."""
     return LearnedSBLPlan(example_data, grid_shape, weights=weights, sweeps=sweeps, polish_size=polish_size,
-                          warmup=warmup, profile=profile)
+                          warmup=warmup, profile=profile, pipelined=pipelined,
+                          fallback_capacity=fallback_capacity)

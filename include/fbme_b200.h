@@ -195,6 +195,21 @@ int fbme_uamp_run(FbmePlan* plan, const void* y, fbme_stream_t stream);
 int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream);
 int fbme_plan_state(FbmePlan* plan, FbmeState* state);
 
+/* Unfused variational ARD prior update, replacing uamp_prior_update /
+ * _uamp_prior_kernel (torch_sbl/triton_kernels.py:670-735, 196-235; taken
+ * at torch_sbl/solver.py:1605-1625 when the UAMP posterior has not already
+ * damped the prior).  For `batch` scenes of `n` coefficients:
+ *   cand  = clamp((|mean|^2 + posterior_variance + hyper_rate)
+ *                 / (1 + hyper_shape), prior_floor[b], maximum)
+ *   out   = max(damping * old_prior + (1 - damping) * cand, prior_floor[b])
+ * with |mean|^2 = re^2 + im^2 and every float32 operation rounded on its
+ * own.  mean is complex64 [batch, n]; posterior_variance, old_prior, out
+ * float32 [batch, n]; prior_floor float32 [batch].  batch <= 65535. */
+int fbme_uamp_prior_update(const void* mean, const float* posterior_variance, const float* old_prior,
+                           const float* prior_floor, int32_t batch, int64_t n, float hyper_shape,
+                           float hyper_rate, float damping, float maximum, float* out,
+                           fbme_stream_t stream);
+
 /* Top-k (k <= 32) of each of `batch` rows of `n` float scores: values
  * largest first, ties by lower index, as torch.topk(scores, k) at
  * torch_sbl/solver.py:1931 and 4410.  `indices` / `values` are [batch, k].
@@ -374,6 +389,19 @@ enum {
 int fbme_plan_profile(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream,
                       float* group_ms, int32_t* group_launches, int32_t n_groups);
 const char* fbme_profile_group_name(int32_t group);
+
+/* Failure-detection self-test of the bounded device waits (no counterpart
+ * in the reference, which has no device-side waits).  Launches one DFT
+ * stage tile with its operand producer held back, so the tensor-core
+ * issuer's wait for a full operand stage and the epilogue's wait for the
+ * accumulator both run out after `wait_cycles` SM cycles (in [1e3, 2e9];
+ * plans use 1e9).  The kernel then ORs FBME_STATUS_TIMEOUT into *status,
+ * releases its tensor memory and returns, leaving the context usable.
+ * `workspace` (fbme_selftest_workspace_bytes(), 256-byte aligned) holds
+ * the tile's operands and output; nothing in it is read or written. */
+size_t fbme_selftest_workspace_bytes(void);
+int fbme_selftest_stage_timeout(void* workspace, size_t workspace_bytes, int32_t* status, int64_t wait_cycles,
+                                fbme_stream_t stream);
 
 /* Thread-local description of the last failure ("" if none). */
 const char* fbme_last_error(void);

@@ -95,3 +95,14 @@ def test_batch_limits_are_rejected_on_the_host():
     fake = ctypes.c_void_p(256)
     rc = lib.fbme_topk(fake, 100, 1, 65536, fake, 0, fake, fake, None)
     assert rc == nat.FBME_ERR_INVALID and "65535" in nat.last_error()
+
+
+def test_selftest_arguments_are_checked_on_the_host():
+    lib = nat.lib()
+    n = lib.fbme_selftest_workspace_bytes()
+    assert n > 0
+    fake = ctypes.c_void_p(256)
+    assert lib.fbme_selftest_stage_timeout(fake, n, fake, 10, None) == nat.FBME_ERR_INVALID
+    assert lib.fbme_selftest_stage_timeout(ctypes.c_void_p(257), n, fake, 10**6, None) == nat.FBME_ERR_WORKSPACE
+    assert lib.fbme_selftest_stage_timeout(fake, n - 1, fake, 10**6, None) == nat.FBME_ERR_WORKSPACE
+    assert lib.fbme_selftest_stage_timeout(None, n, fake, 10**6, None) == nat.FBME_ERR_INVALID

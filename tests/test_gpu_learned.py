@@ -75,31 +75,84 @@ def test_fallback_returns_the_plain_plan_result():
 
 
 @pytest.mark.gpu
-def test_one_failure_goes_through_the_small_fallback_plan():
-    """A single failed scene is re-solved by the 2-scene plain plan; its rows
-    become the plain result, every other row keeps the warm result."""
+def test_one_forced_failure_is_resolved_on_the_device():
+    """A single failed scene is re-solved by the plain plan inside the
+    fallback graph; its rows become the plain result, every other row keeps
+    the warm result."""
     need_gpu()
     from fbme_b200.learned import make_learned_plan
     from torch_sbl_fastest_stable import make_stable_plan
 
     y, _ = _batch(8, 2_150_000)
     yt = torch.from_numpy(y).cuda()
-    learned = make_learned_plan(yt, GRID, warmup=1)
+    learned = make_learned_plan(yt, GRID, warmup=1, fallback_capacity=4)
     warm = learned.replay(yt, synchronize=True, fallback=False)
     x_warm, nle_warm = warm.x.clone(), warm.negative_log_evidence.clone()
-    mask = torch.ones(8, dtype=torch.bool, device=yt.device)
-    mask[5] = False
-    learned._captured_check = lambda: mask
-    r = learned.replay(yt, synchronize=True)
-    assert learned.fallbacks == 1
-    assert learned._plain_small is not learned._plain
+    passed_warm = learned.passed.clone()
+    learned.force_fallback[5] = True
+    r = learned.replay(yt)
+    torch.cuda.current_stream().synchronize()  # stream order alone completes the results
+    assert not bool(learned.passed[5]) and not bool(learned.overflow)
     p = make_stable_plan(yt, GRID, warmup=1).replay(yt, synchronize=True)
     assert torch.equal(r.x[5], p.x[5])
     assert torch.equal(r.posterior_variance[5], p.posterior_variance[5])
     assert torch.equal(r.negative_log_evidence[5], p.negative_log_evidence[5])
-    keep = [i for i in range(8) if i != 5]
+    keep = [i for i in range(8) if i != 5 and bool(passed_warm[i])]
+    assert keep, "every warm scene failed its check"
     assert torch.equal(r.x[keep], x_warm[keep])
     assert torch.equal(r.negative_log_evidence[keep], nle_warm[keep])
+    assert learned.fallbacks == 1 + int((~passed_warm).sum()) - int(not bool(passed_warm[5]))
+
+
+@pytest.mark.gpu
+def test_failures_beyond_the_capacity_are_resolved_on_synchronize():
+    need_gpu()
+    from fbme_b200.learned import make_learned_plan
+    from torch_sbl_fastest_stable import make_stable_plan
+
+    y, _ = _batch(8, 2_100_000)
+    yt = torch.from_numpy(y).cuda()
+    learned = make_learned_plan(yt, GRID, warmup=1, fallback_capacity=3)
+    learned.force_fallback.fill_(True)
+    learned.replay(yt)
+    assert bool(learned.overflow)
+    r = learned.replay(yt, synchronize=True)
+    assert learned.fallbacks == 8
+    p = make_stable_plan(yt, GRID, warmup=1).replay(yt, synchronize=True)
+    assert torch.equal(r.x, p.x)
+    assert torch.equal(r.noise_variance, p.noise_variance)
+
+
+def _tensors(res):
+    from dataclasses import fields
+
+    return {f.name: getattr(res, f.name).clone() for f in fields(res)
+            if isinstance(getattr(res, f.name), torch.Tensor)}
+
+
+@pytest.mark.gpu
+def test_pipelined_replays_equal_stream_ordered_replays():
+    """Two warm plans take turns and each replay's fallback overlaps the next
+    replay's warm solve; after synchronize() every replay's results equal
+    the stream-ordered plan's."""
+    need_gpu()
+    from fbme_b200.learned import make_learned_plan
+
+    ya, _ = _batch(8, 2_300_000)
+    yb, _ = _batch(8, 2_300_100)
+    ta, tb = torch.from_numpy(ya).cuda(), torch.from_numpy(yb).cuda()
+    plain = make_learned_plan(ta, GRID, warmup=1)
+    plain.force_fallback[[1, 6]] = True
+    ra, rb = _tensors(plain.replay(ta, synchronize=True)), _tensors(plain.replay(tb, synchronize=True))
+    pipe = make_learned_plan(ta, GRID, warmup=1, pipelined=True)
+    pipe.force_fallback[[1, 6]] = True
+    r1 = pipe.replay(ta)
+    r2 = pipe.replay(tb)
+    pipe.synchronize()
+    assert r1 is not r2
+    for ref, got in ((ra, r1), (rb, r2)):
+        for k, v in ref.items():
+            assert torch.equal(getattr(got, k), v), k
 
 
 @pytest.mark.gpu
