@@ -126,7 +126,7 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
     plain = make_stable_plan(y, GRID, warmup=1)
     r_learned = rate(lambda: learned.replay(y), batch, steps, learned.join)
     fallbacks = learned.fallbacks
-    overflow = bool(learned.overflow)
+    overflow = int(learned.overflows.item())  # replays (warm-up included) beyond the device capacity
     ordered = make_learned_plan(y, GRID, warmup=1)
     r_ordered = rate(lambda: ordered.replay(y), batch, steps)
     r_warm = rate(lambda: ordered.replay(y, fallback=False), batch, steps)
@@ -156,9 +156,9 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
                     f"SNR~U[5,25] dB, batch {batch}",
         "learned_batched_scenes_per_s": r_learned,
         "learned_batched_stream_ordered_scenes_per_s": r_ordered,
-        "fallback": "device graph: check, compaction into 16 slots, plain re-solve, scatter; "
-                    "pipelined with the next replay's warm solve",
-        "fallback_overflow": overflow,
+        "fallback": f"device graph: check, compaction into {learned.capacity} slots, plain re-solve, "
+                    "scatter; pipelined with the next replay's warm solve on a high-priority stream",
+        "fallback_overflow_replays": overflow,
         "warm_solve_alone_scenes_per_s": r_warm,  # the same plan without its fallback check (not a result)
         "plain_batched_scenes_per_s": r_plain,
         "plain_single_scene_scenes_per_s": r_single,

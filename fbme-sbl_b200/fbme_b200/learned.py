@@ -264,7 +264,7 @@ class LearnedSBLPlan:
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, net: WarmStartNet | None = None,
                  weights: str | Path = DEFAULT_WEIGHTS, sweeps: int = 1, polish_size: int = 32,
                  warmup: int = 3, profile: str = "stable", gamma_residual_max: float = 0.75,
-                 noise_residual_max: float = 0.05, fallback_capacity: int = 16,
+                 noise_residual_max: float = 0.05, fallback_capacity: int = 8,
                  pipelined: bool = False) -> None:
         from .plans import CUDAGraphSBLPlan
 
@@ -300,7 +300,11 @@ class LearnedSBLPlan:
         self._idxbuf = [torch.zeros(self.capacity + 1, dtype=torch.int64, **dev) for _ in range(nw)]
         self._passed = [torch.ones(self.batch, dtype=torch.bool, **dev) for _ in range(nw)]
         self._count = [torch.zeros((), dtype=torch.int64, **dev) for _ in range(nw)]
-        self._side = torch.cuda.Stream(self.device)
+        # replays whose failures exceeded the capacity (device counter)
+        self.overflows = torch.zeros((), dtype=torch.int64, **dev)
+        # the fallback's short, latency-bound launches take priority over the
+        # warm solve's wide grids, so they interleave instead of queueing
+        self._side = torch.cuda.Stream(self.device, priority=-1)
         self._warm_done = [torch.cuda.Event() for _ in range(nw)]
         self._done = [torch.cuda.Event() for _ in range(nw)]
         self._graphs: list[torch.cuda.CUDAGraph | None] = [None] * nw
@@ -369,6 +373,7 @@ class LearnedSBLPlan:
             dst.index_copy_(0, idx, torch.where(sel, src, rows))
         self._passed[s].copy_(ok)
         self._count[s].copy_(count)
+        self.overflows.add_((count > F).to(torch.int64))
 
     def _fallback_graph(self, s: int) -> torch.cuda.CUDAGraph:
         key = (self.gamma_residual_max, self.noise_residual_max)
@@ -451,7 +456,7 @@ class LearnedSBLPlan:
 def make_learned_plan(example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
                       warmup: int = 3, sweeps: int = 1, weights: str | Path = DEFAULT_WEIGHTS,
                       profile: str = "stable", pipelined: bool = False,
-                      fallback_capacity: int = 16) -> LearnedSBLPlan:
+                      fallback_capacity: int = 8) -> LearnedSBLPlan:
     """Build the warm-started plan (same call shape as make_stable_plan)."""
     return LearnedSBLPlan(example_data, grid_shape, weights=weights, sweeps=sweeps, polish_size=polish_size,
                           warmup=warmup, profile=profile, pipelined=pipelined,

@@ -52,7 +52,8 @@ def test_prior_update_matches_float32_reference_bitwise(batch, n, offset, dampin
     assert bool((got >= floor[:, None]).all())
     # the rounding-free value agrees to float32 resolution
     m64 = mean.to(torch.complex128)
-    cand = ((m64.abs() ** 2 + pv.double() + 1e-8) / (1 + 1e-8)).clamp(min=floor.double()[:, None], max=50.0)
+    cand = torch.maximum(((m64.abs() ** 2 + pv.double() + 1e-8) / (1 + 1e-8)).clamp(max=50.0),
+                         floor.double()[:, None])
     exact = torch.maximum(damping * old.double() + (1 - damping) * cand, floor.double()[:, None])
     np.testing.assert_allclose(got.double().cpu().numpy(), exact.cpu().numpy(), rtol=3e-7)
 
