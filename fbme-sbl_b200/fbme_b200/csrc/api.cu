@@ -66,8 +66,15 @@ Layout make_layout(const fbme::BatchShape& s, const FbmeConfig& c, int nt) {
   L.gamma = take(B * N * sizeof(float));
   L.msg = take(2 * B * M * sizeof(float2));
   L.pred = take(B * M * sizeof(float2));
-  const size_t tmp1 = static_cast<size_t>(s.m2) * s.n1, tmp2 = static_cast<size_t>(s.n2) * s.m1;
-  L.tmp = take(B * (tmp1 > tmp2 ? tmp1 : tmp2) * sizeof(float2));
+  // the two-stage intermediates: FP32 complex, or (3-term products) the
+  // second stage's pre-split operand, whose rows and K are tile-padded
+  size_t tmp1 = static_cast<size_t>(s.m2) * s.n1 * sizeof(float2);
+  size_t tmp2 = static_cast<size_t>(s.n2) * s.m1 * sizeof(float2);
+  if (c.dft_terms == 3) {
+    tmp1 = static_cast<size_t>(fbme::split_unit_bytes(s.m2, s.n1));
+    tmp2 = static_cast<size_t>(fbme::split_unit_bytes(s.n2, s.m1));
+  }
+  L.tmp = take(B * (tmp1 > tmp2 ? tmp1 : tmp2));
   L.lift = take(B * N * sizeof(float2));
   L.keys = take(B * N * sizeof(uint32_t));
   L.part = take(B * fbme::kMaxTilesPerScene * fbme::kPartSlots * sizeof(double));
@@ -380,6 +387,7 @@ void bind_bucket(Bucket& k, uint8_t* ws, cudaStream_t st) {
   u.msg = reinterpret_cast<float2*>(w + L.msg);
   u.pred = reinterpret_cast<float2*>(w + L.pred);
   u.tmp = reinterpret_cast<float2*>(w + L.tmp);
+  u.split = k.cfg.dft_terms == 3;
   u.lift = reinterpret_cast<float2*>(w + L.lift);
   u.var = reinterpret_cast<float*>(w + L.var);
   u.gamma = reinterpret_cast<float*>(w + L.gamma);

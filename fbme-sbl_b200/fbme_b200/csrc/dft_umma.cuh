@@ -30,9 +30,18 @@
 // axis, so a warp's 32 lanes write 32 consecutive elements.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace fbme {
+
+// A prologue policy with `static constexpr bool kBulk = true` supplies its
+// operand already split and swizzled: the producer only bulk-copies it.
+template <class P, class = void>
+struct ProBulk : std::false_type {};
+template <class P>
+struct ProBulk<P, std::void_t<decltype(P::kBulk)>> : std::bool_constant<P::kBulk> {};
 
 constexpr int kTileRows = 128;  // UMMA M
 constexpr int kKChunk = 64;     // real K per pipeline stage (one 128-byte row)
@@ -196,7 +205,7 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full_bar[s], kProThreads);
+      mbar_init(&full_bar[s], ProBulk<Pro>::value ? 1 : kProThreads);
       mbar_init(&empty_bar[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -212,7 +221,46 @@ dft_stage_kernel(const __grid_constant__ StageSet<Pro, Epi, NI> set) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp < kEpiWarp0 && warp != kMmaWarp) {
+  if (ProBulk<Pro>::value && warp < kEpiWarp0 && warp != kMmaWarp) {
+    // ---------------- bulk producer ----------------
+    // The operand is stored pre-split and pre-swizzled by the previous
+    // stage's epilogue: [unit][row tile][K chunk][part][128 rows x 128 B].
+    // Thread 0 copies a chunk's A parts (one contiguous block) and its
+    // twiddle blocks, completing on the stage's full barrier; no register
+    // work, so the stage runs at the copy engine's and the tensor core's pace.
+    if constexpr (ProBulk<Pro>::value) {
+      if (threadIdx.x == 0) {
+        bool ok = true;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles && ok && !set.hold; tile += gridDim.x) {
+          const int ii = set.find(tile);
+          const DftGeom& g = set.it[ii].g;
+          const Pro& pro = set.it[ii].pro;
+          const TileCtx t = decode_tile(g, tile - set.tile0[ii]);
+          int* const st_scene = set.it[ii].status ? set.it[ii].status + t.scene / g.status_div : nullptr;
+          constexpr uint32_t kABytes = A_PARTS * kPartBytesA;
+          const uint8_t* a_src = pro.in + static_cast<size_t>(t.scene) * pro.unit_bytes +
+                                 static_cast<size_t>(t.row_tile) * g.kchunks * kABytes;
+          const uint8_t* b_src =
+              g.table + static_cast<size_t>(t.col_tile) * g.table_kchunks * A_PARTS * C::kPartBytesB;
+          for (int kc = 0; kc < g.kchunks && ok; ++kc, ++it) {
+            const int s = it % kStages, use = it / kStages;
+            uint8_t* st = smem + s * C::kStageBytes;
+            if (it >= kStages) {
+              ok = mbar_wait(&empty_bar[s], (use - 1) & 1, st_scene, wlim);
+              if (!ok) break;
+            }
+            mbar_arrive_expect_tx(&full_bar[s], kABytes + A_PARTS * C::kPartBytesB);
+            bulk_g2s(st, a_src + static_cast<size_t>(kc) * kABytes, kABytes, &full_bar[s]);
+            for (int p = 0; p < A_PARTS; ++p)
+              bulk_g2s(st + kABytes + p * C::kPartBytesB,
+                       b_src + (static_cast<size_t>(kc) * A_PARTS + p) * C::kPartBytesB, C::kPartBytesB,
+                       &full_bar[s]);
+          }
+        }
+      }
+    }
+  } else if (warp < kEpiWarp0 && warp != kMmaWarp) {
     // ---------------- producer ----------------
     // Producer warp pw stages row pairs p = pw + kProWarps * i (tile rows 2p
     // and 2p + 1); lane l covers complex columns 2(l%16), 2(l%16)+1 of the
@@ -511,5 +559,67 @@ struct EpiStoreT {
   }
   FBME_DEV void tile_done(const TileCtx&, int, int) {}
 };
+
+// Intermediate of a two-stage transform stored as the next stage's operand:
+// element (r, c) of this stage's output is row c, complex column r of the
+// next stage's A, written as its two BF16 parts (hi = bf16(x), lo = bf16(x -
+// hi), the split the producer would otherwise do) straight into the
+// K-major 128-byte-swizzled layout
+//   [unit][c / 128][r / 32][part][c % 128 rows x 128 B].
+// A warp's 32 lanes hold 32 consecutive r, one 128-byte operand row per
+// column and part: fully coalesced stores.  Rows r past this stage's rows
+// carry exact zeros (their inputs read as zero), which is the next stage's
+// K padding; columns past `cols` are never written, and the next stage's
+// rows that read them are discarded by its epilogue.
+struct EpiSplitT {
+  using Pre = NoPre;
+  uint8_t* out;
+  long long unit_bytes;  // row_tiles2 * kchunks2 * 2 * 16 KiB
+  int kchunks2;          // K chunks of the next stage (32 complex each)
+  FBME_DEV void prefetch(const TileCtx&, int, int, Pre&) const {}
+  FBME_DEV void consume(const TileCtx& t, int row, int c0, const float* v, const Pre&) const {
+    const DftGeom& g = *t.g;
+    const int r = t.row0() + row;
+    if (r >= kchunks2 * 32) return;
+    const int kc = r >> 5, w = r & 31;
+    uint8_t* base = out + t.scene * unit_bytes + static_cast<size_t>(kc) * 2 * kPartBytesA;
+    const int jb = t.col0() + (c0 >> 1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int c = jb + i;
+      if (c >= g.cols) continue;
+      const float2 x = make_float2(v[2 * i], v[2 * i + 1]);
+      const __nv_bfloat162 hi = __float22bfloat162_rn(x);
+      const float2 h = __bfloat1622float2(hi);
+      const __nv_bfloat162 lo = __float22bfloat162_rn(make_float2(x.x - h.x, x.y - h.y));
+      const int cr = c & 127;
+      uint8_t* blk = base + static_cast<size_t>(c >> 7) * kchunks2 * 2 * kPartBytesA;
+      const uint32_t off = cr * 128u + ((((w >> 2) ^ (cr & 7)) & 7) << 4) + (w & 3) * 4u;
+      *reinterpret_cast<__nv_bfloat162*>(blk + off) = hi;
+      *reinterpret_cast<__nv_bfloat162*>(blk + kPartBytesA + off) = lo;
+    }
+  }
+  FBME_DEV void tile_done(const TileCtx&, int, int) {}
+};
+
+// Prologue of a stage whose A operand EpiSplitT wrote (3-term products).
+struct ProSplit {
+  static constexpr bool kBulk = true;
+  // unused register-producer interface (the bulk producer copies instead)
+  static constexpr int kBatch = 1;
+  static constexpr bool kPipelined = false;
+  using Frag = float4;
+  const uint8_t* in;
+  long long unit_bytes;
+  FBME_DEV void fetch(const TileCtx&, long long, int, Frag& f) const { f = make_float4(0.f, 0.f, 0.f, 0.f); }
+  FBME_DEV float4 make(const TileCtx&, long long, int, const Frag& f) const { return f; }
+  FBME_DEV void tile_done(const TileCtx&, int, int) {}
+};
+
+// Bytes per unit of the split operand of a stage with `rows` rows and a
+// contracted length of `kcplx` complex values.
+__host__ __device__ inline long long split_unit_bytes(int rows, int kcplx) {
+  return static_cast<long long>((rows + kTileRows - 1) / kTileRows) * ((kcplx + 31) / 32) * 2 * kPartBytesA;
+}
 
 }  // namespace fbme

@@ -105,6 +105,9 @@ struct UampBuffers {
   uint32_t* keys;  // [B][N] order-preserving score keys (final E-step)
   Scalars sc;
   int* status;   // launch status word
+  // nonzero: tmp holds the two-stage intermediates as the second stage's
+  // pre-split operand (split_unit_bytes per scene; 3-term products only)
+  int split;
   // learned warm start (optional): FP32 network parameters and its workspace
   const float* warm_params;
   void* warm_ws;

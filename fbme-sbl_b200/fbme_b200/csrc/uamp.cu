@@ -560,23 +560,59 @@ cudaError_t set_dft_attributes() {
   if ((e = set_attr_both<ProYPower, EpiStoreT, true>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProPlain, EpiPredict, true>()) != cudaSuccess) return e;
   if ((e = set_attr_both<ProPlain, EpiBackprojection, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProPlain, EpiSplitT, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProYPower, EpiSplitT, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProSplit, EpiStoreT, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProSplit, EpiPredict, true>()) != cudaSuccess) return e;
+  if ((e = set_attr_both<ProSplit, EpiBackprojection, true>()) != cudaSuccess) return e;
   return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// the intermediate of a two-stage transform
+// ---------------------------------------------------------------------------
+// Stage 1 stores it in `tmp` and stage 2 reads it.  With `split` (plans of
+// 3-term products) it is stage 2's A operand already split into BF16 parts
+// and swizzled (EpiSplitT), which stage 2 bulk-copies (ProSplit); otherwise
+// FP32 complex (EpiStoreT / ProPlain) that stage 2's producer splits.  The
+// same FP32 values are split the same way in both, so results are identical.
+static EpiSplitT split_epi(float2* tmp, const DftGeom& g2) {
+  return EpiSplitT{reinterpret_cast<uint8_t*>(tmp), split_unit_bytes(g2.rows, g2.kcplx), g2.kchunks};
+}
+static ProSplit split_pro(const float2* tmp, const DftGeom& g2) {
+  return ProSplit{reinterpret_cast<const uint8_t*>(tmp), split_unit_bytes(g2.rows, g2.kcplx)};
+}
+template <class Pro1>
+static void stage1(int terms, bool split, const DftGeom& g1, const DftGeom& g2, const Pro1& p1, float2* tmp,
+                   int* status, cudaStream_t st) {
+  if (split)
+    run_stage(terms, g1, p1, split_epi(tmp, g2), status, st);
+  else
+    run_stage(terms, g1, p1, EpiStoreT{tmp}, status, st);
+}
+template <class Epi2>
+static void stage2(int terms, bool split, const DftGeom& g2, const float2* tmp, const Epi2& e2, int* status,
+                   cudaStream_t st) {
+  if (split)
+    run_stage(terms, g2, split_pro(tmp, g2), e2, status, st);
+  else
+    run_stage(terms, g2, ProPlain{tmp}, e2, status, st);
 }
 
 void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
                  float2* data, float2* tmp, int* status, cudaStream_t st) {
   const int nt = t.n_tile;
   const DftGeom g1 = stage_geom(kFwd1, s, t, nt), g2 = stage_geom(kFwd2, s, t, nt);
-  run_stage(terms, g1, ProPlain{coeff}, EpiStoreT{tmp}, status, st);
-  run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{data}, status, st);
+  stage1(terms, terms == 3, g1, g2, ProPlain{coeff}, tmp, status, st);
+  stage2(terms, terms == 3, g2, tmp, EpiStoreT{data}, status, st);
 }
 
 void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float2* data,
                  float2* coeff, float2* tmp, int* status, cudaStream_t st) {
   const int nt = t.n_tile;
   const DftGeom g1 = stage_geom(kAdj1, s, t, nt), g2 = stage_geom(kAdj2, s, t, nt);
-  run_stage(terms, g1, ProPlain{data}, EpiStoreT{tmp}, status, st);
-  run_stage(terms, g2, ProPlain{tmp}, EpiStoreT{coeff}, status, st);
+  stage1(terms, terms == 3, g1, g2, ProPlain{data}, tmp, status, st);
+  stage2(terms, terms == 3, g2, tmp, EpiStoreT{coeff}, status, st);
 }
 
 // Initialisation shared by the UAMP and PCG paths (solver.py:1063-1159):
@@ -615,11 +651,11 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   const int nt = t.n_tile;
   const DftGeom a1 = with_y(stage_geom(kAdj1, s, t, nt), u.y), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
+  const bool split = u.split && c.terms == 3;
   FBME_TIMED(prof, FBME_GROUP_INIT,
-             run_stage(c.terms, a1, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status, st));
+             stage1(c.terms, split, a1, a2, ProYPower{u.y, u.part, 0.f}, u.tmp, u.status, st));
   FBME_TIMED(prof, FBME_GROUP_INIT,
-             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f},
-                       u.status, st));
+             stage2(c.terms, split, a2, u.tmp, EpiBackprojection{u.bp, u.part, 0.f}, u.status, st));
   FBME_TIMED(prof, FBME_GROUP_INIT,
              (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                  kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, kProWarps},
@@ -644,6 +680,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   const DftGeom a1 = stage_geom(kAdj1, s, t, nt), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   const long long BM = static_cast<long long>(s.B) * s.m();
+  const bool split = u.split && c.terms == 3;
   float2* msg[2] = {u.msg, u.msg + BM};
 
   // A warm start replaces the initial prior, its partial sums and the
@@ -676,19 +713,16 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                  (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
                                                                       u.sc.prec, u.sc.dvar, c.uamp_damping)));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-                 run_stage(c.terms, a1, ProPlain{msg[cur ^ 1]}, EpiStoreT{u.tmp}, u.status, st));
+                 stage1(c.terms, split, a1, a2, ProPlain{msg[cur ^ 1]}, u.tmp, u.status, st));
       cur ^= 1;
-      FBME_TIMED(prof, FBME_GROUP_ADJ_2,
-                 run_stage(c.terms, a2, ProPlain{u.tmp}, EpiStoreT{u.lift}, u.status, st));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2(c.terms, split, a2, u.tmp, EpiStoreT{u.lift}, u.status, st));
       FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
                  (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
       src_dof = PartSrc{bn, 1};
     }
-    FBME_TIMED(prof, FBME_GROUP_FWD_1,
-               run_stage(c.terms, f1, ProPlain{u.mu}, EpiStoreT{u.tmp}, u.status, st));
+    FBME_TIMED(prof, FBME_GROUP_FWD_1, stage1(c.terms, split, f1, f2, ProPlain{u.mu}, u.tmp, u.status, st));
     FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL,
-               run_stage(c.terms, f2, ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f},
-                         u.status, st));
+               stage2(c.terms, split, f2, u.tmp, EpiPredict{u.pred, u.y, u.part, 0.f}, u.status, st));
     FBME_TIMED(prof, FBME_GROUP_SCALARS,
                (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                    kScalarSweep, s, c, u.sc, u.part, src_dof, src_dof,
@@ -700,11 +734,10 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
              (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
                                                                   u.sc.prec, u.sc.dvar, c.uamp_damping)));
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-             run_stage(c.terms, a1, ProPlain{msg[cur ^ 1]}, EpiStoreT{u.tmp}, u.status, st));
+             stage1(c.terms, split, a1, a2, ProPlain{msg[cur ^ 1]}, u.tmp, u.status, st));
   da.update_prior = 0;
   da.keys = reinterpret_cast<uint32_t*>(u.keys);
-  FBME_TIMED(prof, FBME_GROUP_ADJ_2,
-             run_stage(c.terms, a2, ProPlain{u.tmp}, EpiStoreT{u.lift}, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2(c.terms, split, a2, u.tmp, EpiStoreT{u.lift}, u.status, st));
   FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
 }
 
@@ -759,32 +792,60 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
   }
   auto msg = [&](int b, int which) { return J[b].u.msg + which * static_cast<long long>(J[b].s.B) * J[b].s.m(); };
   auto sgx = [&](int b) { return ceil_div(J[b].s.B, kScalarScenesPerBlock); };
-  auto plain_stage = [&](const std::vector<int>& bs, const std::vector<DftGeom>& g, auto in, auto out) {
-    std::vector<StageJob<ProPlain, EpiStoreT>> j;
-    for (int b : bs) j.push_back({J[b].c.terms, {g[b], ProPlain{in(b)}, EpiStoreT{out(b)}, J[b].u.status}});
-    run_stage_multi(j.data(), static_cast<int>(j.size()), st);
+  // Stage 1 / stage 2 of the buckets `bs` through their intermediates (the
+  // pre-split form for 3-term buckets, FP32 for the others: two launches
+  // when a step holds both kinds).
+  auto split_of = [&](int b) { return J[b].u.split && J[b].c.terms == 3; };
+  auto stage1_m = [&](const std::vector<int>& bs, const std::vector<DftGeom>& g1, const std::vector<DftGeom>& g2,
+                      auto pro) {
+    using P = decltype(pro(0));
+    std::vector<StageJob<P, EpiSplitT>> js;
+    std::vector<StageJob<P, EpiStoreT>> jp;
+    for (int b : bs) {
+      if (split_of(b))
+        js.push_back({J[b].c.terms, {g1[b], pro(b), split_epi(J[b].u.tmp, g2[b]), J[b].u.status}});
+      else
+        jp.push_back({J[b].c.terms, {g1[b], pro(b), EpiStoreT{J[b].u.tmp}, J[b].u.status}});
+    }
+    if (!js.empty()) run_stage_multi(js.data(), static_cast<int>(js.size()), st);
+    if (!jp.empty()) run_stage_multi(jp.data(), static_cast<int>(jp.size()), st);
+  };
+  auto stage2_m = [&](const std::vector<int>& bs, const std::vector<DftGeom>& g2, auto epi) {
+    using E = decltype(epi(0));
+    std::vector<StageJob<ProSplit, E>> js;
+    std::vector<StageJob<ProPlain, E>> jp;
+    for (int b : bs) {
+      if (split_of(b))
+        js.push_back({J[b].c.terms, {g2[b], split_pro(J[b].u.tmp, g2[b]), epi(b), J[b].u.status}});
+      else
+        jp.push_back({J[b].c.terms, {g2[b], ProPlain{J[b].u.tmp}, epi(b), J[b].u.status}});
+    }
+    if (!js.empty()) run_stage_multi(js.data(), static_cast<int>(js.size()), st);
+    if (!jp.empty()) run_stage_multi(jp.data(), static_cast<int>(jp.size()), st);
   };
   std::vector<int> all(nb);
   for (int b = 0; b < nb; ++b) all[b] = b;
 
   // --- initialisation (sbl_init) ---
   {
-    std::vector<StageJob<ProYPower, EpiStoreT>> jy;
-    std::vector<StageJob<ProPlain, EpiBackprojection>> jb;
+    std::vector<DftGeom> a1ys(nb);
     std::vector<ScalarsJob> s1, s2;
     std::vector<Gamma0Job> g0;
     for (int b = 0; b < nb; ++b) {
       const UampBuffers& u = J[b].u;
       const DftGeom a1y = with_y(a1[b], u.y);
-      jy.push_back({J[b].c.terms, {a1y, ProYPower{u.y, u.part, 0.f}, EpiStoreT{u.tmp}, u.status}});
-      jb.push_back({J[b].c.terms, {a2[b], ProPlain{u.tmp}, EpiBackprojection{u.bp, u.part, 0.f}, u.status}});
+      a1ys[b] = a1y;
       s1.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{a1y.row_tiles * a1y.col_tiles, kProWarps},
                     PartSrc{a2[b].row_tiles * a2[b].col_tiles, kPartWarps}, PartSrc{0, 0}});
       g0.push_back({bn[b], J[b].s, J[b].c, u.sc, u.bp, u.gamma, u.part});
       s2.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{bn[b], 1}, PartSrc{0, 0}, PartSrc{0, 0}});
     }
-    FBME_TIMED(prof, FBME_GROUP_INIT, run_stage_multi(jy.data(), nb, st));
-    FBME_TIMED(prof, FBME_GROUP_INIT, run_stage_multi(jb.data(), nb, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT, stage1_m(all, a1ys, a2, [&](int b) {
+                 return ProYPower{J[b].u.y, J[b].u.part, 0.f};
+               }));
+    FBME_TIMED(prof, FBME_GROUP_INIT, stage2_m(all, a2, [&](int b) {
+                 return EpiBackprojection{J[b].u.bp, J[b].u.part, 0.f};
+               }));
     FBME_TIMED(prof, FBME_GROUP_INIT, scalars_multi(kScalarInit1, s1, st));
     FBME_TIMED(prof, FBME_GROUP_INIT, ew_launch(g0, [&](const EwJobs<Gamma0Job>& m, dim3 g) {
                  gamma0_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
@@ -819,26 +880,24 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
                    message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
                  }));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-                 plain_stage(act, a1, [&](int b) { return msg(b, cur[b] ^ 1); }, [&](int b) { return J[b].u.tmp; }));
+                 stage1_m(act, a1, a2, [&](int b) { return ProPlain{msg(b, cur[b] ^ 1)}; }));
       for (int b : act) cur[b] ^= 1;
-      FBME_TIMED(prof, FBME_GROUP_ADJ_2,
-                 plain_stage(act, a2, [&](int b) { return J[b].u.tmp; }, [&](int b) { return J[b].u.lift; }));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2_m(act, a2, [&](int b) { return EpiStoreT{J[b].u.lift}; }));
       FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
                    denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
                  }));
     }
-    FBME_TIMED(prof, FBME_GROUP_FWD_1,
-               plain_stage(act, f1, [&](int b) { return J[b].u.mu; }, [&](int b) { return J[b].u.tmp; }));
+    FBME_TIMED(prof, FBME_GROUP_FWD_1, stage1_m(act, f1, f2, [&](int b) { return ProPlain{J[b].u.mu}; }));
     {
-      std::vector<StageJob<ProPlain, EpiPredict>> j;
       std::vector<ScalarsJob> sj;
       for (int b : act) {
         const UampBuffers& u = J[b].u;
-        j.push_back({J[b].c.terms, {f2[b], ProPlain{u.tmp}, EpiPredict{u.pred, u.y, u.part, 0.f}, u.status}});
         sj.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{bn[b], 1}, PartSrc{bn[b], 1},
                       PartSrc{f2[b].row_tiles * f2[b].col_tiles, kPartWarps}});
       }
-      FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, run_stage_multi(j.data(), static_cast<int>(j.size()), st));
+      FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, stage2_m(act, f2, [&](int b) {
+                   return EpiPredict{J[b].u.pred, J[b].u.y, J[b].u.part, 0.f};
+                 }));
       FBME_TIMED(prof, FBME_GROUP_SCALARS, scalars_multi(kScalarSweep, sj, st));
     }
   }
@@ -859,9 +918,8 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
                message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
              }));
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-             plain_stage(all, a1, [&](int b) { return msg(b, cur[b] ^ 1); }, [&](int b) { return J[b].u.tmp; }));
-  FBME_TIMED(prof, FBME_GROUP_ADJ_2,
-             plain_stage(all, a2, [&](int b) { return J[b].u.tmp; }, [&](int b) { return J[b].u.lift; }));
+             stage1_m(all, a1, a2, [&](int b) { return ProPlain{msg(b, cur[b] ^ 1)}; }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2_m(all, a2, [&](int b) { return EpiStoreT{J[b].u.lift}; }));
   FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
                denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
              }));
