@@ -35,6 +35,7 @@ struct Layout {
   size_t tab_f2, tab_f1, tab_a2, tab_a1, dir1, dir2;
   size_t mu, bp, var, gamma, msg, pred, tmp, lift, keys, part, scal;
   size_t active, score, pstate, xval, xidx, status, ckey, cidx;
+  size_t mask, ymask, gram, gscr;  // observation mask (fbme_plan_set_observation_mask)
   size_t total;
 };
 
@@ -90,6 +91,10 @@ Layout make_layout(const fbme::BatchShape& s, const FbmeConfig& c, int nt) {
   const size_t nc = c1 > c2 ? c1 : c2;
   L.ckey = take(B * nc * sizeof(uint32_t));
   L.cidx = take(B * nc * sizeof(int));
+  L.mask = take(M);
+  L.ymask = take(B * M * sizeof(float2));
+  L.gram = take(N * sizeof(float2));
+  L.gscr = take(fbme::mask_gram_scratch_bytes(s));
   L.total = off;
   return L;
 }
@@ -142,7 +147,7 @@ int check_bucket(const fbme::BatchShape& s, const FbmeConfig* c, int nt) {
 }
 
 fbme::DevConfig dev_config(const FbmeConfig& c) {
-  fbme::DevConfig d;
+  fbme::DevConfig d{};
   d.uamp_damping = c.uamp_damping;
   d.damping = c.damping;
   d.blend = c.initialization_blend;
@@ -194,6 +199,7 @@ struct Bucket {
   int first;       // first scene in bucket order
   long long pix0;  // first pixel in bucket order
   long long smp0;  // first sample in bucket order
+  float2* ymask;   // masked copy of the observations (under an observation mask)
 };
 
 // Where scene i (caller order) lives: samples and pixels in the caller's
@@ -389,6 +395,8 @@ void bind_bucket(Bucket& k, uint8_t* ws, cudaStream_t st) {
   u.tmp = reinterpret_cast<float2*>(w + L.tmp);
   u.split = k.cfg.dft_terms == 3;
   u.lift = reinterpret_cast<float2*>(w + L.lift);
+  u.mask = nullptr;
+  k.ymask = reinterpret_cast<float2*>(w + L.ymask);
   u.var = reinterpret_cast<float*>(w + L.var);
   u.gamma = reinterpret_cast<float*>(w + L.gamma);
   u.part = reinterpret_cast<double*>(w + L.part);
@@ -571,6 +579,10 @@ void run_bucket(const Bucket& k, const float2* y, const FbmeOutputs& out, cudaSt
                 fbme::Profiler* prof = nullptr) {
   cudaMemsetAsync(k.status, 0, k.s.B * sizeof(int), st);
   fbme::UampBuffers u = k.u;
+  if (k.u.mask) {  // the solve reads the masked copy of the observations
+    fbme::mask_data(k.s, y, k.u.mask, k.ymask, st);
+    y = k.ymask;
+  }
   u.y = y;
   fbme::uamp_run(k.s, k.tables, k.dc, u, st, prof);
   polish_bucket(k, y, out, st, prof);
@@ -773,6 +785,10 @@ int fbme_uamp_run(FbmePlan* plan, const void* y, fbme_stream_t stream) {
   cudaMemsetAsync(k.status, 0, k.s.B * sizeof(int), st);
   fbme::UampBuffers u = k.u;
   u.y = static_cast<const float2*>(y);
+  if (k.u.mask) {
+    fbme::mask_data(k.s, u.y, k.u.mask, k.ymask, st);
+    u.y = k.ymask;
+  }
   fbme::uamp_run(k.s, k.tables, k.dc, u, st);
   return check_launch("uamp_run");
 }
@@ -786,6 +802,10 @@ int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   fbme::PolishBuffers p = k.p;
   p.y = static_cast<const float2*>(y);
+  if (k.u.mask) {
+    fbme::mask_data(k.s, p.y, k.u.mask, k.ymask, st);
+    p.y = k.ymask;
+  }
   fbme::polish_run(k.s, k.dc, p, *out, st);
   cudaMemcpyAsync(out->status, k.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
   return check_launch("polish_run");
@@ -937,6 +957,31 @@ int fbme_topk(const float* scores, int64_t n, int32_t k, int32_t batch, void* wo
   fbme::topk_scores(scores, n, k, batch, workspace, indices, values,
                     reinterpret_cast<cudaStream_t>(stream));
   return check_launch("fbme_topk");
+}
+
+int fbme_plan_set_observation_mask(FbmePlan* plan, const uint8_t* mask, fbme_stream_t stream) {
+  int rc = single_bucket(plan);
+  if (rc != FBME_OK) return rc;
+  Bucket& k = plan->bk[0];
+  uint8_t* w = plan->ws + k.base;
+  if (!mask) {  // back to the whole M1 x M2 block
+    k.u.mask = nullptr;
+    k.p.gram2d = nullptr;
+    k.dc.m_obs = 0.f;
+    return FBME_OK;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  uint8_t* dmask = w + k.L.mask;
+  float2* gram = reinterpret_cast<float2*>(w + k.L.gram);
+  long long observed = 0;
+  const cudaError_t e = fbme::mask_setup(k.s, mask, dmask, gram, w + k.L.gscr, &observed, st);
+  if (e != cudaSuccess)
+    return fail(FBME_ERR_CUDA, std::string("fbme_plan_set_observation_mask: ") + cudaGetErrorString(e));
+  if (observed == 0) return fail(FBME_ERR_INVALID, "observation_mask must retain at least one sample.");
+  k.u.mask = dmask;
+  k.p.gram2d = gram;
+  k.dc.m_obs = static_cast<float>(observed);
+  return FBME_OK;
 }
 
 int fbme_plan_state(FbmePlan* plan, FbmeState* st) {

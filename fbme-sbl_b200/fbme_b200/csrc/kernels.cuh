@@ -56,7 +56,15 @@ struct DevConfig {
   float false_alarm;
   int terms;
   int uamp_iters;
+  // observed samples per scene under an observation mask (0: the whole
+  // M1 x M2 block is observed)
+  float m_obs;
 };
+
+// Samples a scene's data terms count: the observed ones under a mask.
+__host__ __device__ inline double observed_samples(const BatchShape& s, const DevConfig& c) {
+  return c.m_obs > 0.f ? static_cast<double>(c.m_obs) : static_cast<double>(s.m());
+}
 
 // Optional per-launch event timing (fbme_plan_profile); nullptr otherwise.
 struct Profiler {
@@ -105,6 +113,9 @@ struct UampBuffers {
   uint32_t* keys;  // [B][N] order-preserving score keys (final E-step)
   Scalars sc;
   int* status;   // launch status word
+  // observation mask [M1*M2] (nullptr: all observed); y is then the masked
+  // copy of the caller's data
+  const uint8_t* mask;
   // nonzero: tmp holds the two-stage intermediates as the second stage's
   // pre-split operand (split_unit_bytes per scene; 3-term products only)
   int split;
@@ -140,6 +151,9 @@ struct PolishBuffers {
   const float2* y;
   const float2* bp;
   const float2 *mu, *dir1, *dir2;
+  // under an observation mask: the Gram table G(d) = sum over observed
+  // samples m of exp(2 pi i m.d / N), [N1][N2] (replaces dir1 x dir2)
+  const float2* gram2d;
   const float *var, *gamma;
   Scalars sc;
   // per-scene state
@@ -158,6 +172,12 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
 size_t polish_state_bytes();
 int topk_slices(long long n);
+// Observation masks (mask.cu): set-up (normalised mask, observed count,
+// 2-D Gram table; synchronises `st`) and the masked copy of the data.
+size_t mask_gram_scratch_bytes(const BatchShape& s);
+cudaError_t mask_setup(const BatchShape& s, const uint8_t* mask_in, uint8_t* mask, float2* gram, void* scratch,
+                       long long* observed, cudaStream_t st);
+void mask_data(const BatchShape& s, const float2* y, const uint8_t* mask, float2* out, cudaStream_t st);
 // Stage-kernel wait-timeout self-test (uamp.cu).
 size_t stage_selftest_bytes();
 cudaError_t stage_selftest(void* ws, int* status, long long wait_cycles, cudaStream_t st);

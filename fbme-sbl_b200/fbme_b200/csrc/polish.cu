@@ -64,6 +64,20 @@ FBME_DEV float2 dirichlet2(const float2* d1, const float2* d2, int n1, int n2, i
   return cmul(d1[i1], d2[i2]);
 }
 
+// Gram entry G[i][j] of atoms (a1, a2) and (b1, b2): the separable
+// Dirichlet product for the full prefix block, or the 2-D table of an
+// observation mask (global memory, L2-resident).
+FBME_DEV float2 gram_at(const PolishArgs& A, const float2* d1, const float2* d2, int a1, int a2, int b1,
+                        int b2) {
+  if (A.p.gram2d) {
+    int i1 = a1 - b1, i2 = a2 - b2;
+    if (i1 < 0) i1 += A.s.n1;
+    if (i2 < 0) i2 += A.s.n2;
+    return __ldg(A.p.gram2d + static_cast<long long>(i1) * A.s.n2 + i2);
+  }
+  return dirichlet2(d1, d2, A.s.n1, A.s.n2, a1, a2, b1, b2);
+}
+
 // Copy the Dirichlet tables of a scene shape into shared memory.
 FBME_DEV void load_dirichlet(const PolishArgs& A, float2* d1, float2* d2) {
   for (int i = threadIdx.x; i < A.s.n1; i += blockDim.x) d1[i] = __ldg(A.p.dir1 + i);
@@ -96,7 +110,7 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   for (int j = 0; j < kMaxPolish; ++j) {
     const int n1j = __shfl_sync(0xffffffffu, n1i, j), n2j = __shfl_sync(0xffffffffu, n2i, j);
     if (on && j < K) {
-      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, n1j, n2j);
+      const float2 g = gram_at(A, d1, d2, n1i, n2i, n1j, n2j);
       float2 a = make_float2(g.x * inv_nu, g.y * inv_nu);
       if (j == lane) a.x += inv_g;
       M[lane][j] = a;
@@ -290,7 +304,7 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
   ld = warp_sum(ld);
   lg = warp_sum(lg);
   qd = warp_sum(qd);
-  const double logdet = static_cast<double>(s.m()) * log(static_cast<double>(nu)) + lg + 2.0 * ld;
+  const double logdet = observed_samples(s, A.c) * log(static_cast<double>(nu)) + lg + 2.0 * ld;
   double quad = static_cast<double>(data_energy) / nu - qd;
   if (quad < 0.0) quad = 0.0;
   o.nle = logdet + quad;
@@ -313,7 +327,7 @@ FBME_DEV double residual_energy(const PolishArgs& A, const float2* d1, const flo
       const int n1j = __shfl_sync(__activemask(), n1i, j), n2j = __shfl_sync(__activemask(), n2i, j);
       const float mjx = __shfl_sync(__activemask(), my_mu.x, j);
       const float mjy = __shfl_sync(__activemask(), my_mu.y, j);
-      const float2 g = dirichlet2(d1, d2, s.n1, s.n2, n1i, n2i, n1j, n2j);
+      const float2 g = gram_at(A, d1, d2, n1i, n2i, n1j, n2j);
       gr += static_cast<double>(g.x) * mjx - static_cast<double>(g.y) * mjy;
       gi += static_cast<double>(g.x) * mjy + static_cast<double>(g.y) * mjx;
     }
@@ -372,7 +386,7 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
   PolishScene* ps = reinterpret_cast<PolishScene*>(A.p.pstate) + scene;
   const float fl = A.p.sc.floor_[scene];
   const float data_energy = A.p.sc.data_energy[scene];
-  const float Mf = static_cast<float>(s.m());
+  const float Mf = static_cast<float>(observed_samples(s, c));
   const long long N = s.n();
   const float2* bp = A.p.bp + scene * N;
   float2(*M)[33] = Msm[threadIdx.x >> 5];
@@ -719,7 +733,7 @@ __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOut
   const bool on = lane < K;
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
   const float fl = A.p.sc.floor_[scene];
-  const float Mf = static_cast<float>(s.m());
+  const float Mf = static_cast<float>(observed_samples(s, c));
   const long long N = s.n();
   float2* d1 = dtab;
   float2* d2 = dtab + s.n1;
@@ -733,7 +747,7 @@ __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOut
   // effective DOF with relevance projection
   float rel = on ? fminf(fmaxf(g * dd, 0.f), 1.f) : 0.f;
   const float raw = warp_sum(rel);
-  const float max_dof = static_cast<float>(static_cast<double>(s.m()) * (1.0 - 10.0 * kEpsP));
+  const float max_dof = static_cast<float>(observed_samples(s, c) * (1.0 - 10.0 * kEpsP));
   const float sc = fminf(1.0f, max_dof / fmaxf(raw, kEpsP));
   const float dof = warp_sum(rel * sc);
   if (lane == 0) {
@@ -850,6 +864,43 @@ cudaError_t set_polish_attributes() {
   return e;
 }
 
+// Residual exchange scoring under an observation mask (solver.py:4398-4412
+// with the masked operator): score[n] = |A^H y[n] - sum_k mu_k G(n - a_k)|^2
+// with the mask's 2-D Gram table G, written as order-preserving keys for a
+// top-E selection; active atoms get key 0 (the reference's -inf).  One
+// thread per grid point; the table lookups hit L2.
+__global__ void __launch_bounds__(256) exchange_masked_kernel(PolishArgs A) {
+  __shared__ int atom1[kMaxPolish], atom2[kMaxPolish], atom[kMaxPolish];
+  __shared__ float2 amu[kMaxPolish];
+  const int scene = blockIdx.y;
+  const BatchShape& s = A.s;
+  const int K = A.c.polish_size;
+  const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
+  if (threadIdx.x < K) {
+    const int a = ps->active[threadIdx.x];
+    atom[threadIdx.x] = a;
+    atom1[threadIdx.x] = a / s.n2;
+    atom2[threadIdx.x] = a % s.n2;
+    amu[threadIdx.x] = ps->best_mean[threadIdx.x];
+  }
+  __syncthreads();
+  const long long N = s.n();
+  const float2* bp = A.p.bp + scene * N;
+  uint32_t* keys = A.p.keys + scene * N;
+  for (long long n = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; n < N;
+       n += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int n1 = static_cast<int>(n / s.n2), n2 = static_cast<int>(n % s.n2);
+    float2 r = __ldg(bp + n);
+    bool act = false;
+    for (int k = 0; k < K; ++k) {
+      act |= atom[k] == n;
+      const float2 t = cmul(amu[k], gram_at(A, nullptr, nullptr, n1, n2, atom1[k], atom2[k]));
+      r = make_float2(r.x - t.x, r.y - t.y);
+    }
+    keys[n] = act ? 0u : float_key_t(abs_sq(r));
+  }
+}
+
 template <typename T>
 static void launch_exchange(const PolishArgs& A, const PolishBuffers& p, cudaStream_t st) {
   const dim3 grid(exchange_blocks(A.s), A.s.B);
@@ -864,7 +915,14 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
              launch_topk(p.keys, s.n(), K, s.B, p.cand_key, p.cand_idx, p.active, p.score, st));
   const size_t dsm = (s.n1 + s.n2) * sizeof(float2);
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 0)));
-  if (c.exchange > 0 && c.polish_iters > 1) {
+  if (c.exchange > 0 && c.polish_iters > 1 && p.gram2d) {
+    const long long nblk = (s.n() + 255) / 256;
+    FBME_TIMED(prof, FBME_GROUP_EXCHANGE,
+               (exchange_masked_kernel<<<dim3(static_cast<unsigned>(nblk < 1024 ? nblk : 1024), s.B), 256, 0, st>>>(A)));
+    FBME_TIMED(prof, FBME_GROUP_TOPK,
+               launch_topk(p.keys, s.n(), c.exchange, s.B, p.cand_key, p.cand_idx, p.xcand_idx, p.xcand_val, st));
+    FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 1)));
+  } else if (c.exchange > 0 && c.polish_iters > 1) {
     const int nb = exchange_blocks(s);
     if (s.n2 <= 64)
       FBME_TIMED(prof, FBME_GROUP_EXCHANGE, (launch_exchange<ExSmall>(A, p, st)));

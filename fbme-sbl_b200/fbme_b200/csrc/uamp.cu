@@ -67,6 +67,7 @@ struct EpiPredict {
   const float2* y;
   double* part;
   float acc;
+  const uint8_t* mask;  // observation mask: the residual sums observed samples only
   FBME_DEV void prefetch(const TileCtx& t, int row, int c0, Pre& p) const {
     const DftGeom& g = *t.g;
     const int r = t.row0() + row;
@@ -89,7 +90,7 @@ struct EpiPredict {
         const float2 p = make_float2(v[2 * i], v[2 * i + 1]);
         ps[(jb + i) * g.out_ld + r] = p;
         const float dr = pre.y[i].x - p.x, di = pre.y[i].y - p.y;
-        acc += dr * dr + di * di;
+        if (!mask || mask[(jb + i) * g.out_ld + r]) acc += dr * dr + di * di;
       }
     }
   }
@@ -290,8 +291,12 @@ __global__ void __launch_bounds__(kEwThreads) denoise_kernel(BatchShape s, Denoi
 // final E-step: m' = d m + (1-d) prec (y - (p - dvar m)), into `msg_out`,
 // which adjoint stage 1 then reads.  Full occupancy, two samples per step
 // where y is 16-byte aligned and M even.
+// Under an observation mask the message of an unobserved sample is zero: the
+// masked operator's rows stop at the observed samples, and A^H of the
+// zero-filled message is the masked adjoint (operators.py:255-280, 484-496).
 FBME_DEV void message_body(Blk k, BatchShape s, const float2* y, const float2* pred, const float2* msg_in,
-                           float2* msg_out, const float* prec, const float* dvar, float damping) {
+                           float2* msg_out, const float* prec, const float* dvar, float damping,
+                           const uint8_t* mask = nullptr) {
   const int scene = k.y;
   const long long m = s.m();
   const float pr = prec[scene], dv = dvar[scene];
@@ -309,21 +314,25 @@ FBME_DEV void message_body(Blk k, BatchShape s, const float2* y, const float2* p
       const float4 a = __ldg(reinterpret_cast<const float4*>(y + e));
       const float4 p = __ldg(reinterpret_cast<const float4*>(pred + e));
       const float4 q = __ldg(reinterpret_cast<const float4*>(msg_in + e));
-      const float2 o0 = step(make_float2(a.x, a.y), make_float2(p.x, p.y), make_float2(q.x, q.y));
-      const float2 o1 = step(make_float2(a.z, a.w), make_float2(p.z, p.w), make_float2(q.z, q.w));
+      float2 o0 = step(make_float2(a.x, a.y), make_float2(p.x, p.y), make_float2(q.x, q.y));
+      float2 o1 = step(make_float2(a.z, a.w), make_float2(p.z, p.w), make_float2(q.z, q.w));
+      if (mask) {
+        if (!mask[2 * j]) o0 = make_float2(0.f, 0.f);
+        if (!mask[2 * j + 1]) o1 = make_float2(0.f, 0.f);
+      }
       *reinterpret_cast<float4*>(msg_out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
     }
   } else {
     for (long long i = first; i < m; i += stride) {
       const long long e = scene * m + i;
-      msg_out[e] = step(y[e], pred[e], msg_in[e]);
+      msg_out[e] = (mask && !mask[i]) ? make_float2(0.f, 0.f) : step(y[e], pred[e], msg_in[e]);
     }
   }
 }
 __global__ void __launch_bounds__(kEwThreads)
 message_kernel(BatchShape s, const float2* y, const float2* pred, const float2* msg_in, float2* msg_out,
-               const float* prec, const float* dvar, float damping) {
-  message_body(blk_here(), s, y, pred, msg_in, msg_out, prec, dvar, damping);
+               const float* prec, const float* dvar, float damping, const uint8_t* mask) {
+  message_body(blk_here(), s, y, pred, msg_in, msg_out, prec, dvar, damping, mask);
 }
 
 // First sweep: the lifted message is (1-d)/(dv+nv) * A^H y, the previous
@@ -411,7 +420,8 @@ FBME_DEV void scalars_body(Blk k, int mode, BatchShape s, DevConfig c, Scalars s
     }
     return warp_sum(v);
   };
-  const float M = static_cast<float>(s.m());
+  const double Md = observed_samples(s, c);
+  const float M = static_cast<float>(Md);
   // all reductions first (collective over the warp), then lane 0 alone
   const double r0 = mode == kScalarInit1 ? sum(3, p0) : sum(0, p0);
   const double r1 = mode == kScalarInit2 ? 0.0 : sum(1, p1);
@@ -419,7 +429,7 @@ FBME_DEV void scalars_body(Blk k, int mode, BatchShape s, DevConfig c, Scalars s
   if (lane != 0) return;
   if (mode == kScalarInit1) {
     const double ysum = r0;
-    const float dp = fmaxf(static_cast<float>(ysum / static_cast<double>(s.m())), kEps);
+    const float dp = fmaxf(static_cast<float>(ysum / Md), kEps);
     const float fl = fmaxf(dp * c.min_var, kTiny);
     sc.data_power[scene] = dp;
     sc.floor_[scene] = fl;
@@ -433,7 +443,7 @@ FBME_DEV void scalars_body(Blk k, int mode, BatchShape s, DevConfig c, Scalars s
     sc.pv[scene] = fmaxf((dv + nv) / M, kTiny);
     sc.prec[scene] = 1.0f / (dv + nv);
   } else {
-    const float max_dof = static_cast<float>(static_cast<double>(s.m()) * (1.0 - 10.0 * kEps));
+    const float max_dof = static_cast<float>(Md * (1.0 - 10.0 * kEps));
     const float dof = fminf(static_cast<float>(r0), max_dof);
     const float sv = static_cast<float>(r1);
     const float energy = static_cast<float>(r2);
@@ -711,7 +721,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
     } else {
       FBME_TIMED(prof, FBME_GROUP_MESSAGE,
                  (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
-                                                                      u.sc.prec, u.sc.dvar, c.uamp_damping)));
+                                                                      u.sc.prec, u.sc.dvar, c.uamp_damping, u.mask)));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
                  stage1(c.terms, split, a1, a2, ProPlain{msg[cur ^ 1]}, u.tmp, u.status, st));
       cur ^= 1;
@@ -722,7 +732,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
     }
     FBME_TIMED(prof, FBME_GROUP_FWD_1, stage1(c.terms, split, f1, f2, ProPlain{u.mu}, u.tmp, u.status, st));
     FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL,
-               stage2(c.terms, split, f2, u.tmp, EpiPredict{u.pred, u.y, u.part, 0.f}, u.status, st));
+               stage2(c.terms, split, f2, u.tmp, EpiPredict{u.pred, u.y, u.part, 0.f, u.mask}, u.status, st));
     FBME_TIMED(prof, FBME_GROUP_SCALARS,
                (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                    kScalarSweep, s, c, u.sc, u.part, src_dof, src_dof,
@@ -732,7 +742,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   // --- final E-step (no prior update, no prediction), score keys ---
   FBME_TIMED(prof, FBME_GROUP_MESSAGE,
              (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
-                                                                  u.sc.prec, u.sc.dvar, c.uamp_damping)));
+                                                                  u.sc.prec, u.sc.dvar, c.uamp_damping, u.mask)));
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
              stage1(c.terms, split, a1, a2, ProPlain{msg[cur ^ 1]}, u.tmp, u.status, st));
   da.update_prior = 0;

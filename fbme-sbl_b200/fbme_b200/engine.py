@@ -37,9 +37,13 @@ def uamp_iteration_limit(cfg: SBLConfig, n_grid: int, n_samples: int) -> int:
     return limit
 
 
-def resolve_native_config(cfg: SBLConfig, grid: Sequence[int], sample: Sequence[int]) -> nat.FbmeConfig:
-    """Map the hot-path fields of ``cfg`` to ``FbmeConfig``."""
-    n_grid, n_samples = prod(grid), prod(sample)
+def resolve_native_config(cfg: SBLConfig, grid: Sequence[int], sample: Sequence[int],
+                          n_observed: int | None = None) -> nat.FbmeConfig:
+    """Map the hot-path fields of ``cfg`` to ``FbmeConfig``.  Under an
+    observation mask the sample count is the observed one
+    (operator.n_samples in solver.py)."""
+    n_grid = prod(grid)
+    n_samples = prod(sample) if n_observed is None else int(n_observed)
     damping = cfg.uamp_damping
     if cfg.uamp_adaptive_damping:  # solver.py:1183-1189
         damping = max(damping, min(cfg.uamp_max_damping, 0.02 * n_grid / n_samples))
@@ -108,7 +112,7 @@ class FBMEEngine:
 
     def __init__(self, batch: int, grid: Sequence[int], sample: Sequence[int], cfg: SBLConfig,
                  device: torch.device, stream: torch.cuda.Stream | None = None,
-                 n_tile: int | None = None) -> None:
+                 n_tile: int | None = None, observation_mask: Tensor | None = None) -> None:
         self.lib = nat.lib()
         if device.type != "cuda":
             raise RuntimeError("the FBME B200 engine needs a CUDA device")
@@ -120,7 +124,19 @@ class FBMEEngine:
         self.sample = tuple(int(v) for v in sample)
         self.cfg = cfg
         self.n_grid, self.n_samples = prod(self.grid), prod(self.sample)
-        self.native_cfg = resolve_native_config(cfg, self.grid, self.sample)
+        # observation mask (operators.py:57-75): [M1, M2] bool, shared by the batch
+        self.mask = None
+        n_observed = None
+        if observation_mask is not None:
+            m = torch.as_tensor(observation_mask, device=device, dtype=torch.bool)
+            if tuple(m.shape) != self.sample:
+                raise ValueError(f"observation_mask must have shape {self.sample}, got {tuple(m.shape)}.")
+            n_observed = int(m.sum())
+            if n_observed == 0:
+                raise ValueError("observation_mask must retain at least one sample.")
+            self.mask = m.to(torch.uint8).contiguous()
+        self.n_observed = self.n_samples if n_observed is None else n_observed
+        self.native_cfg = resolve_native_config(cfg, self.grid, self.sample, n_observed)
         shapes = (nat.FbmeShape * self.batch)()
         for i in range(self.batch):
             shapes[i] = nat.FbmeShape(self.grid[0], self.grid[1], self.sample[0], self.sample[1])
@@ -174,6 +190,11 @@ class FBMEEngine:
                                               ctypes.c_size_t(nbytes), ctypes.c_void_p(st.cuda_stream),
                                               ctypes.byref(self._plan))
         nat.check(rc, "fbme_plan_create")
+        if self.mask is not None:
+            with torch.cuda.device(device):
+                rc = self.lib.fbme_plan_set_observation_mask(self._plan, ctypes.c_void_p(self.mask.data_ptr()),
+                                                             ctypes.c_void_p(st.cuda_stream))
+            nat.check(rc, "fbme_plan_set_observation_mask")
         # constant result fields of the zero-tail polish (solver.py:4052-4068, 4639-4653)
         self._false = torch.zeros(B, dtype=torch.bool, device=device)
         self._true = torch.ones(B, dtype=torch.bool, device=device)

@@ -31,7 +31,8 @@ class CUDAGraphSBLPlan:
     """
 
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, config: SBLConfig,
-                 warmup: int = 3, engine_hook: Callable[[FBMEEngine], None] | None = None) -> None:
+                 warmup: int = 3, engine_hook: Callable[[FBMEEngine], None] | None = None,
+                 observation_mask: Any | None = None) -> None:
         if not torch.cuda.is_available():
             raise RuntimeError("CUDA Graph execution requires CUDA.")
         if not isinstance(example_data, Tensor) or not example_data.is_cuda:
@@ -73,7 +74,10 @@ class CUDAGraphSBLPlan:
         batch = prod(self._batch_shape) if self._batch_shape else 1
         self.input_buffer = torch.empty(self.shape, dtype=self.dtype, device=self.device)
         self.input_buffer.copy_(example_data)
-        self._engine = FBMEEngine(batch, self.grid_shape, sample, self.config, self.device)
+        # observation mask (an extension of the reference's plans, which take
+        # the full block; sbl_2d's masked operator, operators.py:57-75)
+        self._engine = FBMEEngine(batch, self.grid_shape, sample, self.config, self.device,
+                                  observation_mask=observation_mask)
         if engine_hook is not None:  # e.g. the learned warm start, before warm-up and capture
             engine_hook(self._engine)
         flat = self.input_buffer.view(batch, -1)
@@ -128,13 +132,15 @@ class RealtimeSBLPlan(CUDAGraphSBLPlan):
     certificate_scope = "fixed-budget-monotone-type2"
 
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
-                 warmup: int = 3, config_overrides: dict[str, Any] | None = None) -> None:
+                 warmup: int = 3, config_overrides: dict[str, Any] | None = None,
+                 observation_mask: Any | None = None) -> None:
         overrides: dict[str, Any] = {"device": example_data.device, "uamp_polish_size": polish_size}
         if config_overrides is not None:
             overrides.update(config_overrides)
         config = SBLConfig.realtime_hybrid_uamp(**overrides)
         self._validate_realtime_config(config)
-        super().__init__(example_data, grid_shape, config=config, warmup=warmup)
+        super().__init__(example_data, grid_shape, config=config, warmup=warmup,
+                         observation_mask=observation_mask)
 
     @staticmethod
     def _validate_realtime_config(config: SBLConfig) -> None:

@@ -91,11 +91,18 @@ def fast_sbl(data: Any, grid_shape: Sequence[int], *, config: SBLConfig | None =
     device = _resolve_device(cfg.device, tensor)
     if device.type != "cuda":
         raise RuntimeError("the FBME B200 path runs on CUDA devices only")
-    if observation_mask is not None:
-        raise NotImplementedError("observation masks are not built on the B200 path yet")
+    mask = None
+    if observation_mask is not None:  # solver.py:986-1000
+        mask = torch.as_tensor(observation_mask, device=device, dtype=torch.bool)
+        if tuple(mask.shape) != sample:
+            raise ValueError("observation_mask must match the trailing data dimensions.")
+        if not bool(mask.any()):
+            raise ValueError("observation_mask must retain at least one sample.")
+        if cfg.offgrid_refinement:
+            raise ValueError("Run off-grid refinement after masked reconstruction.")
     if tensor.dtype in (torch.complex128, torch.float64) or cfg.uamp_polish_high_precision:
         raise NotImplementedError("the B200 path computes in complex64; pass complex64 data")
-    n_samples = prod(sample)
+    n_samples = prod(sample) if mask is None else int(mask.sum())
     threshold = cfg.dense_threshold if device.type == "cuda" else min(cfg.dense_threshold, 512)
     mode = ("dense" if cfg.mode == "auto" and n_samples <= threshold
             else "cg" if cfg.mode == "auto" else cfg.mode)
@@ -104,6 +111,9 @@ def fast_sbl(data: Any, grid_shape: Sequence[int], *, config: SBLConfig | None =
             "dense exact mode (M x M Cholesky) is not built on the B200 path; use mode='uamp' "
             "or mode='cg'")
     if mode == "cg":
+        if mask is not None:
+            raise NotImplementedError(
+                "observation masks run on the B200 uamp path (mode='uamp'); cg mode takes the full block")
         from .cg import cg_sbl  # noqa: PLC0415  (PCG + Hutchinson device path)
         return cg_sbl(tensor, grid, sample, batch_shape, cfg, device)
     check_supported(cfg)
@@ -111,7 +121,10 @@ def fast_sbl(data: Any, grid_shape: Sequence[int], *, config: SBLConfig | None =
     sample2 = sample if len(sample) == 2 else (1, sample[0])
     batch = prod(batch_shape) if batch_shape else 1
     y = tensor.to(device=device, dtype=torch.complex64).reshape(batch, -1).contiguous()
-    eng = _engine(batch, grid2, sample2, cfg, device)
+    if mask is None:
+        eng = _engine(batch, grid2, sample2, cfg, device)
+    else:  # a masked plan is built per call (its Gram table depends on the mask)
+        eng = FBMEEngine(batch, grid2, sample2, cfg, device, observation_mask=mask.reshape(sample2))
     eng.run(y)
     res = eng.result(batch_shape)
     # eager calls return fresh tensors (the engine's buffers are reused)

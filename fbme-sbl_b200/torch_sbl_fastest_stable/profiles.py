@@ -11,7 +11,7 @@ profiles share one numerical core and differ in the active-set budget:
 
 from __future__ import annotations
 
-from typing import Sequence
+from typing import Any, Sequence
 
 import torch
 from torch import Tensor
@@ -38,7 +38,7 @@ class FastestSBLPlan(CUDAGraphSBLPlan):
     )
 
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
-                 warmup: int = 3) -> None:
+                 warmup: int = 3, observation_mask: Any | None = None) -> None:
         _require_frozen_core()
         if example_data.dtype != torch.complex64:
             raise ValueError("FastestSBLPlan is locked to CUDA complex64 arithmetic.")
@@ -52,7 +52,8 @@ class FastestSBLPlan(CUDAGraphSBLPlan):
         )
         if config.uamp_backend != "triton":
             raise RuntimeError("The fastest profile requires the fused device path.")
-        super().__init__(example_data, grid_shape, config=config, warmup=warmup)
+        super().__init__(example_data, grid_shape, config=config, warmup=warmup,
+                         observation_mask=observation_mask)
 
 
 class StableSBLPlan(RealtimeSBLPlan):
@@ -62,12 +63,13 @@ class StableSBLPlan(RealtimeSBLPlan):
     certificate_scope = "fixed-budget-monotone-type2"
 
     def __init__(self, example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
-                 warmup: int = 3) -> None:
+                 warmup: int = 3, observation_mask: Any | None = None) -> None:
         _require_frozen_core()
         if example_data.dtype != torch.complex64:
             raise ValueError("StableSBLPlan is locked to CUDA complex64 arithmetic.")
         super().__init__(
             example_data, grid_shape, polish_size=polish_size, warmup=warmup,
+            observation_mask=observation_mask,
             config_overrides={
                 "uamp_polish_iterations": 3,
                 "uamp_polish_residual_exchange_size": 12,
@@ -78,12 +80,16 @@ class StableSBLPlan(RealtimeSBLPlan):
 
 
 def make_fastest_plan(example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
-                      warmup: int = 3) -> FastestSBLPlan:
-    """Build the locked fastest plan."""
-    return FastestSBLPlan(example_data, grid_shape, polish_size=polish_size, warmup=warmup)
+                      warmup: int = 3, observation_mask: Any | None = None) -> FastestSBLPlan:
+    """Build the locked fastest plan (``observation_mask``: B200 extension,
+    an [M1, M2] bool mask of observed samples shared by the batch)."""
+    return FastestSBLPlan(example_data, grid_shape, polish_size=polish_size, warmup=warmup,
+                          observation_mask=observation_mask)
 
 
 def make_stable_plan(example_data: Tensor, grid_shape: Sequence[int], *, polish_size: int = 32,
-                     warmup: int = 3) -> StableSBLPlan:
-    """Build the locked stable plan."""
-    return StableSBLPlan(example_data, grid_shape, polish_size=polish_size, warmup=warmup)
+                     warmup: int = 3, observation_mask: Any | None = None) -> StableSBLPlan:
+    """Build the locked stable plan (``observation_mask`` as for
+    make_fastest_plan)."""
+    return StableSBLPlan(example_data, grid_shape, polish_size=polish_size, warmup=warmup,
+                         observation_mask=observation_mask)

@@ -195,6 +195,19 @@ int fbme_uamp_run(FbmePlan* plan, const void* y, fbme_stream_t stream);
 int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_stream_t stream);
 int fbme_plan_state(FbmePlan* plan, FbmeState* state);
 
+/* Observation mask (non-rectangular sampling), replacing the
+ * observation_mask of PrefixFourierOperator (torch_sbl/operators.py:57-75,
+ * 473-496) and of sbl_2d (torch_sbl/solver.py:986-1021) on the plan path.
+ * `mask` is a device array of M1*M2 bytes (nonzero = observed), shared by
+ * every scene of an equal-shape plan; NULL restores the full block.  The
+ * observations keep the M1 x M2 layout; unobserved samples are ignored.
+ * Builds the masked Gram table and reads the observed count back, so it
+ * synchronises `stream`: call it after fbme_plan_create and before replays
+ * are captured.  The caller resolves the config's sweep budget from the
+ * observed count (as solver.py does from operator.n_samples).  An uneven
+ * plan returns FBME_ERR_UNSUPPORTED; an all-zero mask FBME_ERR_INVALID. */
+int fbme_plan_set_observation_mask(FbmePlan* plan, const uint8_t* mask, fbme_stream_t stream);
+
 /* Unfused variational ARD prior update, replacing uamp_prior_update /
  * _uamp_prior_kernel (torch_sbl/triton_kernels.py:670-735, 196-235; taken
  * at torch_sbl/solver.py:1605-1625 when the UAMP posterior has not already

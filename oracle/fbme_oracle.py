@@ -179,7 +179,7 @@ class PrefixOperator:
     Coefficients are ``[B, N1*N2]`` (row-major), data ``[B, M1*M2]``.
     """
 
-    def __init__(self, grid, sample, cdtype=np.complex64):
+    def __init__(self, grid, sample, cdtype=np.complex64, observation_mask=None):
         self.grid = tuple(int(v) for v in grid)
         self.sample = tuple(int(v) for v in sample)
         if len(self.grid) != 2 or len(self.sample) != 2:
@@ -189,7 +189,17 @@ class PrefixOperator:
         self.cdtype = np.dtype(cdtype)
         self.rdtype = np.float64 if self.cdtype == np.complex128 else np.float32
         self.n_grid = prod(self.grid)
-        self.n_samples = prod(self.sample)
+        self.full_n_samples = prod(self.sample)
+        # observed samples (operators.py:57-75): data hold only those
+        self.observed = None
+        if observation_mask is not None:
+            mask = np.asarray(observation_mask, bool)
+            if mask.shape != self.sample:
+                raise ValueError(f"observation_mask must have shape {self.sample}, got {mask.shape}.")
+            self.observed = np.flatnonzero(mask.reshape(-1))
+            if self.observed.size == 0:
+                raise ValueError("observation_mask must retain at least one sample.")
+        self.n_samples = self.full_n_samples if self.observed is None else int(self.observed.size)
         # operators.py:103-147 embedding for the BTTB (Toeplitz) matvec
         self.embedding = tuple(_next_smooth_length(2 * m - 1) for m in self.sample)
         pos, lag = [], []
@@ -204,18 +214,33 @@ class PrefixOperator:
         ).reshape(-1)
         a0, a1 = np.meshgrid(np.arange(self.sample[0]), np.arange(self.sample[1]), indexing="ij")
         self.sample_coordinates = np.stack([a0.reshape(-1), a1.reshape(-1)], 1)
+        if self.observed is not None:
+            self.sample_coordinates = self.sample_coordinates[self.observed]
+
+    def restrict(self, full: np.ndarray) -> np.ndarray:
+        """operators.py:473-482: observed entries of [B, M1*M2, ...] data."""
+        return full if self.observed is None else full[:, self.observed]
+
+    def expand(self, data: np.ndarray) -> np.ndarray:
+        """operators.py:484-496: observed entries scattered into a zero block."""
+        if self.observed is None:
+            return data
+        full = np.zeros((data.shape[0], self.full_n_samples, *data.shape[2:]), data.dtype)
+        full[:, self.observed] = data
+        return full
 
     def forward_flat(self, coefficients: np.ndarray) -> np.ndarray:
-        """operators.py:237-253: fft2 then crop."""
+        """operators.py:237-253: fft2 then crop (and restrict)."""
         b = coefficients.shape[0]
         field = coefficients.reshape(b, *self.grid)
         spec = np.fft.fft2(field, axes=(1, 2))
-        return spec[:, : self.sample[0], : self.sample[1]].reshape(b, self.n_samples).astype(self.cdtype)
+        full = spec[:, : self.sample[0], : self.sample[1]].reshape(b, self.full_n_samples)
+        return self.restrict(full).astype(self.cdtype)
 
     def adjoint_flat(self, data: np.ndarray) -> np.ndarray:
         """operators.py:255-280: N * ifft2 with end zero padding."""
         b = data.shape[0]
-        field = data.reshape(b, *self.sample)
+        field = self.expand(data).reshape(b, *self.sample)
         coeff = np.fft.ifft2(field, s=self.grid, axes=(1, 2)).astype(self.cdtype)
         return (coeff * self.rdtype(self.n_grid)).reshape(b, self.n_grid)
 
@@ -459,7 +484,8 @@ def _uamp_iteration_limit(cfg: OracleConfig, n_grid: int, n_samples: int) -> int
 
 
 def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str = "cuda",
-                  stop_after_uamp: bool = False, initial_prior: np.ndarray | None = None):
+                  stop_after_uamp: bool = False, initial_prior: np.ndarray | None = None,
+                  observation_mask: np.ndarray | None = None):
     """Restatement of ``fast_sbl`` for ``mode="uamp"`` with the polish.
 
     ``data`` is ``[M1, M2]`` or ``[B, M1, M2]``.  Returns a dict of the
@@ -474,10 +500,10 @@ def fast_sbl_uamp(data: np.ndarray, grid, cfg: OracleConfig, *, chol_mode: str =
     y3 = data[None] if single else data
     b = y3.shape[0]
     sample = y3.shape[1:]
-    op = PrefixOperator(grid, sample, cdtype)
+    op = PrefixOperator(grid, sample, cdtype, observation_mask)
     rd = op.rdtype
     eps, tiny = _finfo(rd)
-    y = y3.reshape(b, op.n_samples).astype(cdtype)
+    y = op.restrict(y3.reshape(b, op.full_n_samples)).astype(cdtype)  # solver.py:1022-1024
     n, m = op.n_grid, op.n_samples
     if cfg.uamp_support_false_alarm_budget is not None and cfg.uamp_support_false_alarm_budget >= n:
         raise ValueError("uamp_support_false_alarm_budget must be smaller than the grid size.")
@@ -755,10 +781,11 @@ def fixed_budget_em_residuals(y, mean, pv, prior, noise, active, prior_floor, op
 
 
 def fbme_solve(data, grid, profile: str = "stable", *, polish_size: int = 32,
-               chol_mode: str = "cuda"):
-    """The FBME-Fast / FBME-Stable plan replay (profiles.py:35-148)."""
+               chol_mode: str = "cuda", observation_mask=None):
+    """The FBME-Fast / FBME-Stable plan replay (profiles.py:35-148),
+    optionally under an observation mask (sbl_2d, solver.py:986-1024)."""
     cfg = OracleConfig.stable(polish_size) if profile == "stable" else OracleConfig.fastest(polish_size)
-    return fast_sbl_uamp(data, grid, cfg, chol_mode=chol_mode)
+    return fast_sbl_uamp(data, grid, cfg, chol_mode=chol_mode, observation_mask=observation_mask)
 
 
 # ---------------------------------------------------------------------------

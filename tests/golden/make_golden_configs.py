@@ -218,6 +218,65 @@ def make_c4(batch_seed: int) -> None:
     print("wrote", f"c4_b{batch_seed}")
 
 
+def observation_mask(kind: str, sample, seed: int):
+    """The masks of the masked fixtures: "random" keeps each sample with
+    probability 0.7 (seeded); "ellipse" keeps the samples inside the
+    ellipse inscribed in the M1 x M2 block (a non-rectangular aperture)."""
+    import numpy as np
+
+    m1, m2 = sample
+    if kind == "random":
+        return np.random.default_rng(50_000 + seed).random((m1, m2)) < 0.7
+    a = (np.arange(m1)[:, None] + 0.5) / m1 - 0.5
+    b = (np.arange(m2)[None, :] + 0.5) / m2 - 0.5
+    return (a / 0.5) ** 2 + (b / 0.5) ** 2 <= 1.0
+
+
+def make_masked(config: str, seed: int, kind: str) -> None:
+    """A scene solved through the reference's sbl_2d with an observation
+    mask (solver.py:986-1021, the masked PrefixFourierOperator) under the
+    FBME plan configurations, CUDA Cholesky loading, with the FP32 result's
+    sensitivity (the perturbation of _solve_three_ways, observed samples
+    only)."""
+    import numpy as np
+
+    torch, scenes, SBLConfig, fast_sbl = _import()
+    import torch_sbl.solver as S  # reference package
+
+    S._stable_cholesky_raw = _cuda_cholesky_branch(S, torch)
+    sc = scenes.config_scene(config, seed)
+    mask = observation_mask(kind, sc.y.shape, seed)
+    tm = torch.from_numpy(mask)
+    out = {"grid": np.array(sc.grid), "sample": np.array(sc.y.shape), "y_sha256": np.array(y_digest(sc.y)),
+           "scene": np.array(f"config_scene('{config}', {seed})"), "mask": mask, "mask_kind": np.array(kind),
+           "cholesky": np.array("cuda")}
+    for profile in ("stable", "fast"):
+        cfg = plan_config(SBLConfig, profile)
+        r = S.sbl_2d(torch.from_numpy(sc.y), sc.grid, config=cfg, observation_mask=tm)
+        f = _solve_fields(r, np)
+        x0, v0 = r.x.numpy().ravel(), r.posterior_variance.numpy().ravel()
+        a0 = x0 != 0
+        sens_x = sens_pv = 0.0
+        for k in range(PERTURBATION_DRAWS):
+            rng = np.random.default_rng(1000 + k)
+            u = rng.uniform(-1.0, 1.0, sc.y.shape) + 1j * rng.uniform(-1.0, 1.0, sc.y.shape)
+            yp = (sc.y.real.astype(np.float64) * (1 + PERTURBATION * u.real)
+                  + 1j * sc.y.imag.astype(np.float64) * (1 + PERTURBATION * u.imag)).astype(np.complex64)
+            rp = S.sbl_2d(torch.from_numpy(yp), sc.grid, config=cfg, observation_mask=tm)
+            xp, vp = rp.x.numpy().ravel(), rp.posterior_variance.numpy().ravel()
+            assert np.array_equal(xp != 0, a0), "a perturbation changed the support"
+            sens_x = max(sens_x, float(np.linalg.norm(xp - x0) / np.linalg.norm(x0)))
+            sens_pv = max(sens_pv, float(np.max(np.abs(vp[a0] - v0[a0]) / v0[a0])))
+        for k, v in f.items():
+            out[profile + "_" + k] = v
+        out[f"sens_{profile}_x"] = np.array(sens_x)
+        out[f"sens_{profile}_pv"] = np.array(sens_pv)
+        out[f"{profile}_mode"] = np.array(r.mode)
+    name = f"masked_{config}_{kind}_s{seed}"
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print("wrote", name)
+
+
 def make_cg_c2(seed: int, max_iter: int) -> None:
     import numpy as np
 
@@ -256,11 +315,16 @@ def make_cg_c2(seed: int, max_iter: int) -> None:
     print("wrote", name)
 
 
-JOBS = [("c3", "0"), ("c3", "1"), ("c3", "2"), ("c4", "0"), ("cg_c2", "0", "6")]
+JOBS = [("c3", "0"), ("c3", "1"), ("c3", "2"), ("c4", "0"), ("cg_c2", "0", "6"),
+        ("masked", "c1", "0", "random"), ("masked", "c1", "1", "ellipse"), ("masked", "c2", "0", "random"),
+        ("masked", "c2", "1", "ellipse")]
 
 
 def main() -> None:
     if len(sys.argv) > 1:
+        if sys.argv[1] == "masked":
+            make_masked(sys.argv[2], int(sys.argv[3]), sys.argv[4])
+            return
         kind, args = sys.argv[1], [int(v) for v in sys.argv[2:]]
         {"c3": make_c3, "c4": make_c4, "cg_c2": make_cg_c2}[kind](*args)
         return

@@ -19,7 +19,10 @@ import numpy as np
 GOLDEN_DIR = Path(__file__).resolve().parent / "golden"
 
 # single-scene plan fixtures (one scene, both profiles)
-PLAN_FILES = sorted(p for p in glob.glob(str(GOLDEN_DIR / "*.npz")) if not Path(p).name.startswith("c4_"))
+PLAN_FILES = sorted(p for p in glob.glob(str(GOLDEN_DIR / "*.npz"))
+                    if not Path(p).name.startswith(("c4_", "masked_")))
+# single-scene fixtures solved under an observation mask (key "mask")
+MASKED_FILES = sorted(glob.glob(str(GOLDEN_DIR / "masked_*.npz")))
 # batched-uneven fixtures (64 scenes each)
 UNEVEN_FILES = sorted(glob.glob(str(GOLDEN_DIR / "c4_*.npz")))
 

@@ -19,7 +19,8 @@ error, with the identical support.
 import numpy as np
 import pytest
 
-from golden_util import PLAN_FILES, SENS_FACTOR, UNEVEN_FILES, plan_case, scene_fields, sensitivity, uneven_case
+from golden_util import (MASKED_FILES, PLAN_FILES, SENS_FACTOR, UNEVEN_FILES, plan_case, scene_fields, sensitivity,
+                         uneven_case)
 from oracle import fbme_oracle as O
 
 # distance to the reference's FP64 result, in units of the reference's own
@@ -93,3 +94,15 @@ def test_oracle_matches_reference_on_uneven_shapes(path, profile):
         r = O.fbme_solve(s.y, s.grid, profile, chol_mode="cuda")  # the fixture's loading
         _check_fields(r, scene_fields(g, profile, i), profile,
                       x_tol=max(2e-5, SENS_FACTOR * sensitivity(g, profile, i)[0]))
+
+
+@pytest.mark.parametrize("path", MASKED_FILES, ids=lambda p: p.rsplit("/", 1)[-1][:-4])
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+def test_oracle_matches_reference_under_observation_masks(path, profile):
+    """sbl_2d with an observation mask (random 70 % and an elliptical
+    aperture) under the FBME plan configurations."""
+    y, grid, g = plan_case(path)
+    r = O.fbme_solve(y, grid, profile, chol_mode="cuda", observation_mask=g["mask"])
+    sx, sv = sensitivity(g, profile)
+    _check_fields(r, g, profile, x_tol=max(2e-5, SENS_FACTOR * sx), pv_rtol=max(1e-4, SENS_FACTOR * sv),
+                  scalar_rtol=max(1e-5, SENS_FACTOR * sx))
