@@ -185,6 +185,7 @@ SIGNATURES = {
     "fbme_polish_run": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
     "fbme_plan_state": (c_int, [c_void_p, POINTER(FbmeState)]),
     "fbme_plan_set_observation_mask": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "fbme_plan_set_warm_prior_map": (c_int, [c_void_p, c_void_p]),
     "fbme_selftest_workspace_bytes": (c_size_t, []),
     "fbme_selftest_stage_timeout": (c_int, [c_void_p, c_size_t, c_void_p, c_int64, c_void_p]),
     "fbme_uamp_prior_update": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int64, c_float,

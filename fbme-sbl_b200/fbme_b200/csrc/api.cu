@@ -741,6 +741,20 @@ int fbme_plan_set_warm_start(FbmePlan* plan, const float* params, void* workspac
                                     "or not 256-byte aligned");
   k.u.warm_params = params;
   k.u.warm_ws = workspace;
+  k.u.warm_map = nullptr;
+  return FBME_OK;
+}
+
+int fbme_plan_set_warm_prior_map(FbmePlan* plan, const float* map) {
+  int rc = single_bucket(plan);
+  if (rc != FBME_OK) return rc;
+  if (map && (reinterpret_cast<uintptr_t>(map) & 3u) != 0) return fail(FBME_ERR_INVALID, "misaligned map");
+  Bucket& k = plan->bk[0];
+  k.u.warm_map = map;
+  if (map) {
+    k.u.warm_params = nullptr;
+    k.u.warm_ws = nullptr;
+  }
   return FBME_OK;
 }
 

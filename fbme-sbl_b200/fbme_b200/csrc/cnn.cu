@@ -856,6 +856,12 @@ void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, 
                                                       floor_, gamma, upart);
 }
 
+void warm_prior_from_map(const float* map, int B, long long N, const float* data_power, const float* floor_,
+                         float* gamma, double* upart, int nblocks, cudaStream_t st) {
+  using namespace cnn;
+  warm_prior_kernel<<<dim3(nblocks, B), 256, 0, st>>>(map, N, data_power, floor_, gamma, upart);
+}
+
 }  // namespace fbme
 
 // ---------------------------------------------------------------------------

@@ -122,6 +122,8 @@ struct UampBuffers {
   // learned warm start (optional): FP32 network parameters and its workspace
   const float* warm_params;
   void* warm_ws;
+  // caller-supplied warm start (optional): [B][N] log(prior / (P/N)) map
+  const float* warm_map;
 };
 
 cudaError_t set_dft_attributes();
@@ -204,6 +206,9 @@ void cnn_adam(float* params, const float* grad, float* m, float* v, int step, fl
 void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, void* ws,
                     const float* data_power, const float* floor_, float* gamma, double* upart,
                     int nblocks, cudaStream_t st);
+// The same initial prior from a caller-supplied [B][N] log(prior / (P/N)) map.
+void warm_prior_from_map(const float* map, int B, long long N, const float* data_power, const float* floor_,
+                         float* gamma, double* upart, int nblocks, cudaStream_t st);
 
 // Shared by the C ABI translation units.
 int api_fail(int code, const std::string& msg);

@@ -695,14 +695,20 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
 
   // A warm start replaces the initial prior, its partial sums and the
   // scalars computed from them, so the plain prior is not formed.
-  sbl_init(s, t, c, u, st, prof, u.warm_params == nullptr);
+  const bool warm = u.warm_params != nullptr || u.warm_map != nullptr;
+  sbl_init(s, t, c, u, st, prof, !warm);
   const int bn = ew_blocks_host(s.n()), bm = ew_blocks_host(s.m());
-  if (u.warm_params) {
-    // learned warm start: the network's prior replaces the initial prior,
-    // then the scalar initialisation is redone from its sums
-    FBME_TIMED(prof, FBME_GROUP_INIT,
-               cnn_warm_prior(u.warm_params, u.bp, s.B, s.n1, s.n2, u.warm_ws, u.sc.data_power,
-                              u.sc.floor_, u.gamma, u.part, bn, st));
+  if (warm) {
+    // learned warm start: the network's prior (or a caller's map) replaces
+    // the initial prior, then the scalar initialisation is redone from its sums
+    if (u.warm_params)
+      FBME_TIMED(prof, FBME_GROUP_INIT,
+                 cnn_warm_prior(u.warm_params, u.bp, s.B, s.n1, s.n2, u.warm_ws, u.sc.data_power,
+                                u.sc.floor_, u.gamma, u.part, bn, st));
+    else
+      FBME_TIMED(prof, FBME_GROUP_INIT,
+                 warm_prior_from_map(u.warm_map, s.B, s.n(), u.sc.data_power, u.sc.floor_, u.gamma, u.part, bn,
+                                     st));
     FBME_TIMED(prof, FBME_GROUP_INIT,
                (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
                    kScalarInit2, s, c, u.sc, u.part, PartSrc{bn, 1}, PartSrc{0, 0}, PartSrc{0, 0})));

@@ -461,3 +461,17 @@ def make_learned_plan(example_data: Tensor, grid_shape: Sequence[int], *, polish
     return LearnedSBLPlan(example_data, grid_shape, weights=weights, sweeps=sweeps, polish_size=polish_size,
                           warmup=warmup, profile=profile, pipelined=pipelined,
                           fallback_capacity=fallback_capacity)
+
+
+def attach_warm_prior_map(engine: FBMEEngine, prior_map: Tensor | None) -> None:
+    """Warm-start a native plan from the caller's own predictor: ``prior_map``
+    ([B, N] float32 on the plan's device, log(prior / (P/N)) as the network
+    outputs) is read at every replay until detached with None; the caller
+    keeps it alive and fills it before each replay."""
+    if prior_map is not None:
+        if prior_map.dtype != torch.float32 or not prior_map.is_cuda or not prior_map.is_contiguous():
+            raise ValueError("prior_map must be a contiguous float32 CUDA tensor")
+        if tuple(prior_map.shape) != (engine.batch, engine.n_grid):
+            raise ValueError(f"prior_map must have shape {(engine.batch, engine.n_grid)}")
+    nat.check(engine.lib.fbme_plan_set_warm_prior_map(engine._plan, _ptr(prior_map)),
+              "fbme_plan_set_warm_prior_map")

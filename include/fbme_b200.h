@@ -377,6 +377,13 @@ int fbme_cnn_adam(float* params, const float* grad, float* m, float* v, int32_t 
  * must outlive the replays; params == NULL turns the warm start off. */
 size_t fbme_plan_warm_workspace_bytes(const FbmeShape* shapes, int32_t n_scenes);
 int fbme_plan_set_warm_start(FbmePlan* plan, const float* params, void* workspace, size_t workspace_bytes);
+/* Warm start from the caller's own predictor: from the next replay on, the
+ * initial prior is max(P/N * exp(map), floor), map a device float array
+ * [B, N1*N2] of log(prior / (P/N)) that the caller fills before each replay
+ * (for example from A^H y, fbme_dft_adjoint).  Caller-owned, read at every
+ * replay; NULL turns it off.  Replaces a network set by
+ * fbme_plan_set_warm_start (and is replaced by it).  Any grid. */
+int fbme_plan_set_warm_prior_map(FbmePlan* plan, const float* map);
 
 /* Kernel groups timed by fbme_plan_profile. */
 enum {

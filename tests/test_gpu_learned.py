@@ -189,3 +189,35 @@ def test_warm_started_solve_matches_oracle_from_the_network_prior():
         assert set(np.flatnonzero(x[b])) == set(np.flatnonzero(xo[b]))
     assert rel_l2(x, xo) < X_TOL
     del ws
+
+
+@pytest.mark.gpu
+def test_warm_prior_map_equals_the_attached_network():
+    """A caller-supplied log-prior map (here: the shipped network's output
+    for A^H y) warm-starts the plan exactly as the attached network does."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.learned import (DEFAULT_WEIGHTS, WarmStartNet, attach_warm_prior_map, attach_warm_start,
+                                   plain_config)
+
+    y, _ = _batch(4, 2_400_000)
+    dev = torch.device("cuda", 0)
+    yt = torch.from_numpy(y).cuda().view(4, -1)
+    net = WarmStartNet.load(DEFAULT_WEIGHTS, dev)
+    a = FBMEEngine(4, GRID, PREFIX, plain_config(1), dev)
+    ws = attach_warm_start(a, net)
+    a.run(yt)
+    b = FBMEEngine(4, GRID, PREFIX, plain_config(1), dev)
+    prior_map = net.predict(b.dft_adjoint(yt), *GRID).contiguous()
+    attach_warm_prior_map(b, prior_map)
+    b.run(yt)
+    torch.cuda.synchronize()
+    for f in ("x", "posterior_variance", "negative_log_evidence", "noise_variance"):
+        assert torch.equal(a.out[f], b.out[f]), f
+    attach_warm_prior_map(b, None)  # back to the plain initialisation
+    b.run(yt)
+    c = FBMEEngine(4, GRID, PREFIX, plain_config(1), dev)
+    c.run(yt)
+    torch.cuda.synchronize()
+    assert torch.equal(b.out["x"], c.out["x"])
+    del ws
