@@ -52,6 +52,7 @@ def _args() -> argparse.Namespace:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain section")
     ap.add_argument("--no-uneven", action="store_true", help="skip the batched-uneven section")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision-workload section")
     return ap.parse_args()
 
 
@@ -100,13 +101,22 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
     from fbme_b200.learned import make_learned_plan
     from torch_sbl_fastest_stable import make_stable_plan
 
-    sc = [scenes.learned_scene(2_000_000 + i) for i in range(batch)]
-    y = torch.from_numpy(np.stack([s.y for s in sc])).to(device)
-    x_true = np.stack([s.x.reshape(-1) for s in sc])
+    # 1024 held-out seeds (the evaluation set of the learned workload), in
+    # batches of `batch`; rates are timed on the first batch
+    n_eval = max(1024, batch)
+    sc = [scenes.learned_scene(2_000_000 + i) for i in range(n_eval)]
+    ys = [torch.from_numpy(np.stack([s.y for s in sc[k:k + batch]])).to(device)
+          for k in range(0, n_eval - batch + 1, batch)]
+    xts = [np.stack([s.x.reshape(-1) for s in sc[k:k + batch]]) for k in range(0, n_eval - batch + 1, batch)]
+    y = ys[0]
 
-    def nmse(xh):
-        xh = xh.reshape(len(sc), -1)
-        return float(np.mean(10 * np.log10(np.sum(np.abs(xh - x_true) ** 2, 1) / np.sum(np.abs(x_true) ** 2, 1))))
+    def nmse_of(plan, **kw):
+        """Mean raw NMSE (dB) of `plan` over every evaluation batch."""
+        vals = []
+        for yb, xt in zip(ys, xts):
+            xh = plan.replay(yb, synchronize=True, **kw).x.cpu().numpy().reshape(len(xt), -1)
+            vals.append(10 * np.log10(np.sum(np.abs(xh - xt) ** 2, 1) / np.sum(np.abs(xt) ** 2, 1)))
+        return float(np.mean(np.concatenate(vals)))
 
     def rate(fn, n_scenes, reps, join=None):
         for _ in range(3):
@@ -131,9 +141,13 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
     r_ordered = rate(lambda: ordered.replay(y), batch, steps)
     r_warm = rate(lambda: ordered.replay(y, fallback=False), batch, steps)
     del ordered
-    n_learned = nmse(learned.replay(y, synchronize=True).x.cpu().numpy())
+    n_learned = nmse_of(learned)
+    fallbacks_eval = 0
+    for yb in ys:  # fallbacks over the evaluation set (each read synchronises)
+        learned.replay(yb)
+        fallbacks_eval += learned.fallbacks
     r_plain = rate(lambda: plain.replay(y), batch, steps)
-    n_plain = nmse(plain.replay(y, synchronize=True).x.cpu().numpy())
+    n_plain = nmse_of(plain)
     single = make_stable_plan(y[:1], GRID, warmup=1)
     r_single = rate(lambda: single.replay(y[:1]), 1, max(steps, 50))
     # plain FBME at larger sweep budgets: the cheapest one that reaches the
@@ -145,7 +159,7 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
     equal = None
     for sweeps in (6, 8, 12, 16):
         p = CUDAGraphSBLPlan(y, GRID, config=plain_config(sweeps), warmup=1)
-        n_p = nmse(p.replay(y, synchronize=True).x.cpu().numpy())
+        n_p = nmse_of(p)
         r_p = rate(lambda: p.replay(y), batch, steps)
         budgets[str(sweeps)] = {"scenes_per_s": r_p, "nmse_db": n_p}
         if equal is None and n_p <= n_learned:
@@ -153,7 +167,7 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
         del p
     return {
         "workload": "held-out learned-distribution scenes, 256x256 / 128x128, K~U{100..400}, "
-                    f"SNR~U[5,25] dB, batch {batch}",
+                    f"SNR~U[5,25] dB, batch {batch}; NMSE and fallbacks over {n_eval} held-out seeds",
         "learned_batched_scenes_per_s": r_learned,
         "learned_batched_stream_ordered_scenes_per_s": r_ordered,
         "fallback": f"device graph: check, compaction into {learned.capacity} slots, plain re-solve, "
@@ -166,6 +180,7 @@ def learned_section(device, steps: int, batch: int = 256) -> dict:
         "learned_vs_plain_batched": r_learned / r_plain,
         "nmse_db": {"plain": n_plain, "learned": n_learned},
         "fallbacks_per_replay": fallbacks,
+        "fallbacks_on_eval_set": fallbacks_eval,
         "learned_sweeps": 1, "plain_sweeps": 4,
         "plain_budgets": budgets,
         "equal_nmse": equal if equal is not None else
@@ -257,6 +272,86 @@ def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
         "single_scene_plans_scenes_per_s": r_single,
         "uneven_vs_single_scene_plans": r_uneven / r_single,
     }
+
+
+def precision_section(device, steps: int, y_main=None, batch: int = 32) -> dict:
+    """The precision workload (512x512 grid, 256x192 prefix, clustered
+    log-normal scatterers, 20 dB) under the three operator modes: 3- and
+    6-term split-BF16 tensor-core products and FP32 FFTs (dft_terms 0).
+    Per mode: scenes/s of one captured FBME-Stable plan over `batch` scenes,
+    its NMSE against the ground truth, and the relative L2 error of A x and
+    A^H y against an FP64 FFT on one random complex input.  With `y_main`
+    (the headline batch), the headline workload is also replayed with the
+    3-term products and with FP32 FFTs, with the per-stage table of each."""
+    import numpy as np
+    import torch
+
+    from fbme_b200 import scenes
+    from fbme_b200.config import SBLConfig, fbme_profile_config
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.plans import CUDAGraphSBLPlan
+
+    grid, prefix = (512, 512), (256, 192)
+    sc = [scenes.config_scene("c3", 4_000_000 + i) for i in range(batch)]
+    y = torch.from_numpy(np.stack([s.y for s in sc])).to(device)
+    truth = np.stack([s.x for s in sc])
+    rng = np.random.default_rng(11)
+    xr = (rng.standard_normal(grid) + 1j * rng.standard_normal(grid)).astype(np.complex64)
+    yr = (rng.standard_normal(prefix) + 1j * rng.standard_normal(prefix)).astype(np.complex64)
+    ref_f = np.fft.fft2(xr.astype(np.complex128))[:prefix[0], :prefix[1]]
+    ref_a = np.fft.ifft2(yr.astype(np.complex128), s=grid) * (grid[0] * grid[1])
+
+    def rel(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    out = {"workload": f"{batch} precision-workload scenes per replay, 512x512 grid / 256x192 prefix, "
+                       "800 clustered + 50 isolated log-normal scatterers, 20 dB; FBME-Stable"}
+    for name, terms in (("bf16x3", 3), ("bf16x6", 6), ("fp32_fft", 0)):
+        eng = FBMEEngine(1, grid, prefix, SBLConfig.paper_hybrid_uamp(uamp_polish_size=32, dft_terms=terms),
+                         device)
+        fx = eng.dft_forward(torch.from_numpy(xr.reshape(1, -1)).to(device)).cpu().numpy().reshape(prefix)
+        ay = eng.dft_adjoint(torch.from_numpy(yr.reshape(1, -1)).to(device)).cpu().numpy().reshape(grid)
+        cfg = fbme_profile_config("stable")
+        cfg.dft_terms = terms
+        plan = CUDAGraphSBLPlan(y, grid, config=cfg, warmup=1)
+        for _ in range(3):
+            plan.replay(y)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            res = plan.replay(y)
+        e1.record()
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1) / steps
+        x_hat = res.x.cpu().numpy()
+        out[name] = {"dft_terms": terms, "scenes_per_s": batch / (ms / 1000.0), "ms_per_replay": ms,
+                     "nmse_db": float(np.mean([scenes.nmse_db(x_hat[i], truth[i]) for i in range(batch)])),
+                     "forward_rel_l2_vs_fp64": rel(fx, ref_f), "adjoint_rel_l2_vs_fp64": rel(ay, ref_a)}
+        del plan, eng
+    if y_main is not None:
+        B = y_main.shape[0]
+        main = {"workload": WORKLOAD + f", batch {B}"}
+        for name, terms in (("bf16x3", 3), ("fp32_fft", 0)):
+            cfg = fbme_profile_config("stable")
+            cfg.dft_terms = terms
+            plan = CUDAGraphSBLPlan(y_main, GRID, config=cfg, warmup=1)
+            for _ in range(3):
+                plan.replay(y_main)
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                plan.replay(y_main)
+            e1.record()
+            torch.cuda.synchronize(device)
+            ms = e0.elapsed_time(e1) / steps
+            prof = plan._engine.profile(plan.input_buffer.view(B, -1))
+            main[name] = {"scenes_per_s": B / (ms / 1000.0), "ms_per_replay": ms,
+                          "stages": stages_table(prof, B, GRID, PREFIX, _peaks(), terms)}
+            del plan
+        out["headline_workload"] = main
+    return out
 
 
 # mode="cg" workloads: sbl_2d's default cg path (active_set off) with the EM
@@ -655,6 +750,9 @@ def run_ours(a: argparse.Namespace) -> None:
     if world == 1 and not a.no_uneven:
         uneven = uneven_section(device, min(a.steps, 20))
     published = published_shape_section(device) if world == 1 and not a.no_uneven else None
+    precision = None
+    if world == 1 and not a.no_precision:
+        precision = precision_section(device, min(a.steps, 20), y_dev)
 
     if rank == 0:
         line = {
@@ -702,6 +800,8 @@ def run_ours(a: argparse.Namespace) -> None:
             line["cg"] = cg
         if published is not None:
             line["published_shape"] = published
+        if precision is not None:
+            line["precision"] = precision
         print(json.dumps(line), flush=True)
     del plan
     if dist is not None:

@@ -26,6 +26,7 @@ int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b
 // Bytes of one split-BF16 twiddle table for axis length L laid out for
 // stage tiles of nt real columns.
 size_t table_bytes(int L, int terms, int nt) {
+  if (terms == 0) return 0;  // the FP32 FFT mode has no tensor-core tables
   const int parts = terms == 6 ? 3 : 2;
   return static_cast<size_t>(ceil_div(2LL * L, nt)) * ceil_div(2LL * L, 64) * parts * nt * 128;
 }
@@ -36,6 +37,7 @@ struct Layout {
   size_t mu, bp, var, gamma, msg, pred, tmp, lift, keys, part, scal;
   size_t active, score, pstate, xval, xidx, status, ckey, cidx;
   size_t mask, ymask, gram, gscr;  // observation mask (fbme_plan_set_observation_mask)
+  size_t fft1, fft2;               // FP32 FFT twiddles (dft_terms 0)
   size_t total;
 };
 
@@ -95,6 +97,8 @@ Layout make_layout(const fbme::BatchShape& s, const FbmeConfig& c, int nt) {
   L.ymask = take(B * M * sizeof(float2));
   L.gram = take(N * sizeof(float2));
   L.gscr = take(fbme::mask_gram_scratch_bytes(s));
+  L.fft1 = take(c.dft_terms == 0 ? s.n1 * sizeof(float2) : 0);
+  L.fft2 = take(c.dft_terms == 0 ? s.n2 * sizeof(float2) : 0);
   L.total = off;
   return L;
 }
@@ -108,8 +112,10 @@ int check_shape(const FbmeShape& s) {
 // Checks of one bucket: its shape s (s.B scenes) under its resolved config.
 int check_bucket(const fbme::BatchShape& s, const FbmeConfig* c, int nt) {
   const long long N = s.n();
-  if (c->dft_terms != 3 && c->dft_terms != 6)
-    return fail(FBME_ERR_INVALID, "dft_terms must be 3 or 6");
+  if (c->dft_terms != 0 && c->dft_terms != 3 && c->dft_terms != 6)
+    return fail(FBME_ERR_INVALID, "dft_terms must be 0 (FP32 FFT), 3 or 6");
+  if (c->dft_terms == 0 && (!fbme::fft_length_ok(s.n1) || !fbme::fft_length_ok(s.n2)))
+    return fail(FBME_ERR_UNSUPPORTED, "the FP32 FFT mode needs N1 and N2 of the form 2^a or 3 * 2^a, at most 512");
   if (c->uamp_iterations < 1) return fail(FBME_ERR_INVALID, "uamp_iterations must be positive");
   if (c->polish_size < 1 || !c->polish_prune_tail)
     return fail(FBME_ERR_UNSUPPORTED,
@@ -140,7 +146,7 @@ int check_bucket(const fbme::BatchShape& s, const FbmeConfig* c, int nt) {
     return fail(FBME_ERR_UNSUPPORTED, "grids above 524288 points or N2 > 512 are not built");
   if (static_cast<long long>((s.n1 + 15) / 16) * c->exchange_size > 2048)
     return fail(FBME_ERR_UNSUPPORTED, "exchange candidate count above 2048");
-  if (!fbme::dft_n_tile_ok(c->dft_terms, nt, s))
+  if (c->dft_terms != 0 && !fbme::dft_n_tile_ok(c->dft_terms, nt, s))
     return fail(FBME_ERR_INVALID, "dft_n_tile must be 64, 128 or 256 with 3 terms (128 with 6) and give at "
                                   "most 64 tiles per scene in every stage");
   return FBME_OK;
@@ -310,6 +316,8 @@ int plan_spec(const FbmeShape* shapes, int n, const FbmeConfig* c, const FbmeSha
     if (rc != FBME_OK) return rc;
     if (nb > 1 && (k.cfg.polish_size != c->polish_size || k.cfg.polish_iterations != c->polish_iterations))
       return fail(FBME_ERR_INVALID, "an uneven plan needs one polish size and iteration count");
+    if (nb > 1 && k.cfg.dft_terms == 0)
+      return fail(FBME_ERR_UNSUPPORTED, "the FP32 FFT mode (dft_terms 0) is built for equal-shape plans");
     k.tables.n_tile = nt;
     k.L = make_layout(k.s, k.cfg, nt);
     k.base = off;
@@ -367,6 +375,7 @@ void bind_bucket(Bucket& k, uint8_t* ws, cudaStream_t st) {
   k.dc = dev_config(k.cfg);
   const int nt = k.tables.n_tile, parts = k.cfg.dft_terms == 6 ? 3 : 2;
   auto build_table = [&](size_t off, int Lx, int sign) {
+    if (k.cfg.dft_terms == 0) return;
     fbme::launch_twiddle_table(w + off, Lx, sign, nt, ceil_div(2LL * Lx, nt), ceil_div(2LL * Lx, 64), parts, st);
   };
   build_table(L.tab_f2, s.n2, -1);
@@ -381,6 +390,15 @@ void bind_bucket(Bucket& k, uint8_t* ws, cudaStream_t st) {
   k.tables.adj_n1 = w + L.tab_a1;
   k.tables.kchunks_n1 = ceil_div(2LL * s.n1, 64);
   k.tables.kchunks_n2 = ceil_div(2LL * s.n2, 64);
+  k.tables.fft_n1 = k.tables.fft_n2 = nullptr;
+  if (k.cfg.dft_terms == 0) {
+    float2* f1 = reinterpret_cast<float2*>(w + L.fft1);
+    float2* f2 = reinterpret_cast<float2*>(w + L.fft2);
+    fbme::launch_fft_twiddles(f1, s.n1, st);
+    fbme::launch_fft_twiddles(f2, s.n2, st);
+    k.tables.fft_n1 = f1;
+    k.tables.fft_n2 = f2;
+  }
   float2* dir1 = reinterpret_cast<float2*>(w + L.dir1);
   float2* dir2 = reinterpret_cast<float2*>(w + L.dir2);
   fbme::launch_dirichlet(dir1, s.m1, s.n1, st);
@@ -602,6 +620,7 @@ int create_plan(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg
     return fail(FBME_ERR_WORKSPACE, "workspace smaller than fbme_plan_workspace_bytes()");
   cudaError_t e = fbme::set_dft_attributes();
   if (e == cudaSuccess) e = fbme::set_polish_attributes();
+  if (e == cudaSuccess) e = fbme::set_fft_attributes();
   if (e != cudaSuccess) return fail(FBME_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 
   FbmePlan* P = new (std::nothrow) FbmePlan();

@@ -101,7 +101,17 @@ struct DftTables {
   const uint8_t* adj_n1;  // L = N1, sign +1
   int kchunks_n1, kchunks_n2;
   int n_tile;  // real output columns per stage tile the tables are laid out for
+  // FP32 FFT mode (dft_terms = 0): exp(-2 pi i k / L), k < L, for L = N1, N2
+  const float2* fft_n1;
+  const float2* fft_n2;
 };
+
+// FP32 FFT stages (fft.cu).  mode 0 store, 1 store + sum |out|^2 (slot 1),
+// 2 store + masked sum |y - out|^2 (slot 2); ysum: sum |in|^2 (slot 3).
+int fft_length_ok(int L);
+int fft_stage_tiles(int rows, int L);
+cudaError_t set_fft_attributes();
+void launch_fft_twiddles(float2* dst, int L, cudaStream_t st);
 
 // Buffers of the UAMP stage.
 struct UampBuffers {

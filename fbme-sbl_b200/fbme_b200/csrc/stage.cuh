@@ -252,3 +252,11 @@ static cudaError_t set_attr_both() {
 }
 
 }  // namespace fbme
+
+namespace fbme {
+// One FP32 FFT stage (fft.cu) with the geometry of the GEMM stage `g`: a
+// length-L transform of sign `sign` per row, input zero-padded from g.kcplx,
+// output truncated to g.cols.
+void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2* in, float2* out,
+               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st);
+}  // namespace fbme

@@ -609,10 +609,30 @@ static void stage2(int terms, bool split, const DftGeom& g2, const float2* tmp, 
     run_stage(terms, g2, ProPlain{tmp}, e2, status, st);
 }
 
+// FP32 FFT form of stage `which` (dft_terms = 0), fft.cu: stages 1 contract
+// the N2 axis, stages 2 the N1 axis; forward stages take the minus sign.
+static void fft_of(Stage which, const BatchShape& s, const DftTables& t, const DftGeom& g, const float2* in,
+                   float2* out, const float2* y, const uint8_t* mask, double* part, int mode, int ysum,
+                   cudaStream_t st) {
+  const bool ax2 = which == kFwd1 || which == kAdj1;
+  fft_stage(g, ax2 ? s.n2 : s.n1, (which == kFwd1 || which == kFwd2) ? -1 : 1, ax2 ? t.fft_n2 : t.fft_n1, in,
+            out, y, mask, part, mode, ysum, st);
+}
+// Partial-sum source of an FFT stage: its row tiles x 8 warps.
+static PartSrc fft_src(Stage which, const BatchShape& s, const DftGeom& g) {
+  const bool ax2 = which == kFwd1 || which == kAdj1;
+  return PartSrc{fft_stage_tiles(g.rows, ax2 ? s.n2 : s.n1), kPartWarps};
+}
+
 void dft_forward(const BatchShape& s, const DftTables& t, int terms, const float2* coeff,
                  float2* data, float2* tmp, int* status, cudaStream_t st) {
   const int nt = t.n_tile;
   const DftGeom g1 = stage_geom(kFwd1, s, t, nt), g2 = stage_geom(kFwd2, s, t, nt);
+  if (terms == 0) {
+    fft_of(kFwd1, s, t, g1, coeff, tmp, nullptr, nullptr, nullptr, 0, 0, st);
+    fft_of(kFwd2, s, t, g2, tmp, data, nullptr, nullptr, nullptr, 0, 0, st);
+    return;
+  }
   stage1(terms, terms == 3, g1, g2, ProPlain{coeff}, tmp, status, st);
   stage2(terms, terms == 3, g2, tmp, EpiStoreT{data}, status, st);
 }
@@ -621,6 +641,11 @@ void dft_adjoint(const BatchShape& s, const DftTables& t, int terms, const float
                  float2* coeff, float2* tmp, int* status, cudaStream_t st) {
   const int nt = t.n_tile;
   const DftGeom g1 = stage_geom(kAdj1, s, t, nt), g2 = stage_geom(kAdj2, s, t, nt);
+  if (terms == 0) {
+    fft_of(kAdj1, s, t, g1, data, tmp, nullptr, nullptr, nullptr, 0, 0, st);
+    fft_of(kAdj2, s, t, g2, tmp, coeff, nullptr, nullptr, nullptr, 0, 0, st);
+    return;
+  }
   stage1(terms, terms == 3, g1, g2, ProPlain{data}, tmp, status, st);
   stage2(terms, terms == 3, g2, tmp, EpiStoreT{coeff}, status, st);
 }
@@ -662,14 +687,21 @@ void sbl_init(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   const DftGeom a1 = with_y(stage_geom(kAdj1, s, t, nt), u.y), a2 = stage_geom(kAdj2, s, t, nt);
   const int sc_blocks = ceil_div(s.B, kScalarScenesPerBlock);
   const bool split = u.split && c.terms == 3;
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             stage1(c.terms, split, a1, a2, ProYPower{u.y, u.part, 0.f}, u.tmp, u.status, st));
-  FBME_TIMED(prof, FBME_GROUP_INIT,
-             stage2(c.terms, split, a2, u.tmp, EpiBackprojection{u.bp, u.part, 0.f}, u.status, st));
+  PartSrc src_y{a1.row_tiles * a1.col_tiles, kProWarps}, src_bp{a2.row_tiles * a2.col_tiles, kPartWarps};
+  if (c.terms == 0) {  // FP32 FFT mode
+    FBME_TIMED(prof, FBME_GROUP_INIT, fft_of(kAdj1, s, t, a1, u.y, u.tmp, nullptr, nullptr, u.part, 0, 1, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT, fft_of(kAdj2, s, t, a2, u.tmp, u.bp, nullptr, nullptr, u.part, 1, 0, st));
+    src_y = fft_src(kAdj1, s, a1);
+    src_bp = fft_src(kAdj2, s, a2);
+  } else {
+    FBME_TIMED(prof, FBME_GROUP_INIT,
+               stage1(c.terms, split, a1, a2, ProYPower{u.y, u.part, 0.f}, u.tmp, u.status, st));
+    FBME_TIMED(prof, FBME_GROUP_INIT,
+               stage2(c.terms, split, a2, u.tmp, EpiBackprojection{u.bp, u.part, 0.f}, u.status, st));
+  }
   FBME_TIMED(prof, FBME_GROUP_INIT,
              (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
-                 kScalarInit1, s, c, u.sc, u.part, PartSrc{a1.row_tiles * a1.col_tiles, kProWarps},
-                 PartSrc{a2.row_tiles * a2.col_tiles, kPartWarps}, PartSrc{0, 0})));
+                 kScalarInit1, s, c, u.sc, u.part, src_y, src_bp, PartSrc{0, 0})));
   if (!plain_prior) return;
   const int bn = ew_blocks_host(s.n());
   FBME_TIMED(prof, FBME_GROUP_INIT,
@@ -715,6 +747,26 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   }
   DenoiseArgs da = denoise_args(c, u);
 
+  // the four stages: tensor-core split-BF16 products, or FP32 FFTs (dft_terms = 0)
+  const bool fft = c.terms == 0;
+  auto adj1 = [&](const float2* m) {
+    if (fft) fft_of(kAdj1, s, t, a1, m, u.tmp, nullptr, nullptr, nullptr, 0, 0, st);
+    else stage1(c.terms, split, a1, a2, ProPlain{m}, u.tmp, u.status, st);
+  };
+  auto adj2 = [&]() {
+    if (fft) fft_of(kAdj2, s, t, a2, u.tmp, u.lift, nullptr, nullptr, nullptr, 0, 0, st);
+    else stage2(c.terms, split, a2, u.tmp, EpiStoreT{u.lift}, u.status, st);
+  };
+  auto fwd1 = [&]() {
+    if (fft) fft_of(kFwd1, s, t, f1, u.mu, u.tmp, nullptr, nullptr, nullptr, 0, 0, st);
+    else stage1(c.terms, split, f1, f2, ProPlain{u.mu}, u.tmp, u.status, st);
+  };
+  auto fwd2 = [&]() {
+    if (fft) fft_of(kFwd2, s, t, f2, u.tmp, u.pred, u.y, u.mask, u.part, 2, 0, st);
+    else stage2(c.terms, split, f2, u.tmp, EpiPredict{u.pred, u.y, u.part, 0.f, u.mask}, u.status, st);
+  };
+  const PartSrc src_res = fft ? fft_src(kFwd2, s, f2) : PartSrc{f2.row_tiles * f2.col_tiles, kPartWarps};
+
   // --- sweeps ---
   int cur = 0;  // msg[cur] holds the latest message
   for (int it = 1; it <= c.uamp_iters; ++it) {
@@ -728,32 +780,28 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
       FBME_TIMED(prof, FBME_GROUP_MESSAGE,
                  (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
                                                                       u.sc.prec, u.sc.dvar, c.uamp_damping, u.mask)));
-      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-                 stage1(c.terms, split, a1, a2, ProPlain{msg[cur ^ 1]}, u.tmp, u.status, st));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, adj1(msg[cur ^ 1]));
       cur ^= 1;
-      FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2(c.terms, split, a2, u.tmp, EpiStoreT{u.lift}, u.status, st));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2, adj2());
       FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
                  (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
       src_dof = PartSrc{bn, 1};
     }
-    FBME_TIMED(prof, FBME_GROUP_FWD_1, stage1(c.terms, split, f1, f2, ProPlain{u.mu}, u.tmp, u.status, st));
-    FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL,
-               stage2(c.terms, split, f2, u.tmp, EpiPredict{u.pred, u.y, u.part, 0.f, u.mask}, u.status, st));
+    FBME_TIMED(prof, FBME_GROUP_FWD_1, fwd1());
+    FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, fwd2());
     FBME_TIMED(prof, FBME_GROUP_SCALARS,
                (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(
-                   kScalarSweep, s, c, u.sc, u.part, src_dof, src_dof,
-                   PartSrc{f2.row_tiles * f2.col_tiles, kPartWarps})));
+                   kScalarSweep, s, c, u.sc, u.part, src_dof, src_dof, src_res)));
   }
 
   // --- final E-step (no prior update, no prediction), score keys ---
   FBME_TIMED(prof, FBME_GROUP_MESSAGE,
              (message_kernel<<<dim3(bm, s.B), kEwThreads, 0, st>>>(s, u.y, u.pred, msg[cur], msg[cur ^ 1],
                                                                   u.sc.prec, u.sc.dvar, c.uamp_damping, u.mask)));
-  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-             stage1(c.terms, split, a1, a2, ProPlain{msg[cur ^ 1]}, u.tmp, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, adj1(msg[cur ^ 1]));
   da.update_prior = 0;
   da.keys = reinterpret_cast<uint32_t*>(u.keys);
-  FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2(c.terms, split, a2, u.tmp, EpiStoreT{u.lift}, u.status, st));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2, adj2());
   FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
 }
 

@@ -71,3 +71,37 @@ def test_delta_gives_dft_row_and_adjointness():
     lhs = np.vdot(yr.astype(np.complex128), ax.astype(np.complex128))
     rhs = np.vdot(ahy.astype(np.complex128), xr.astype(np.complex128))
     assert abs(lhs - rhs) / abs(lhs) < 2e-5
+
+
+FFT_SHAPES = [
+    (512, 512, 256, 192, 1),  # the precision workload's shape
+    (256, 256, 128, 128, 2),
+    (192, 256, 77, 101, 1),
+    (384, 256, 171, 165, 1),
+    (64, 64, 32, 32, 3),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", FFT_SHAPES, ids=lambda s: "x".join(map(str, s)))
+def test_fp32_fft_mode_error_is_that_of_an_fp32_fft(shape):
+    """dft_terms=0 runs the operator as FP32 FFTs: its error against an FP64
+    DFT is at most twice that of cuFFT in FP32 on the same input."""
+    need_gpu()
+    n1, n2, m1, m2, b = shape
+    eng = _engine(shape, 0)
+    rng = np.random.default_rng(8)
+    x = (rng.standard_normal((b, n1 * n2)) + 1j * rng.standard_normal((b, n1 * n2))).astype(np.complex64)
+    y = (rng.standard_normal((b, m1 * m2)) + 1j * rng.standard_normal((b, m1 * m2))).astype(np.complex64)
+    xt, yt = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    fx = eng.dft_forward(xt).cpu().numpy()
+    ay = eng.dft_adjoint(yt).cpu().numpy()
+    ref_f = np.fft.fft2(x.astype(np.complex128).reshape(b, n1, n2))[:, :m1, :m2].reshape(b, -1)
+    ref_a = (np.fft.ifft2(y.astype(np.complex128).reshape(b, m1, m2), s=(n1, n2)) * n1 * n2).reshape(b, -1)
+    cu_f = torch.fft.fft2(xt.view(b, n1, n2))[:, :m1, :m2].reshape(b, -1).cpu().numpy()
+    cu_a = (torch.fft.ifft2(yt.view(b, m1, m2), s=(n1, n2)) * (n1 * n2)).reshape(b, -1).cpu().numpy()
+    ef, ea = rel_l2(fx, ref_f), rel_l2(ay, ref_a)
+    cf, ca = rel_l2(cu_f, ref_f), rel_l2(cu_a, ref_a)
+    print(f"{shape}: forward {ef:.2e} (cuFFT FP32 {cf:.2e}), adjoint {ea:.2e} (cuFFT FP32 {ca:.2e})")
+    assert ef <= 2 * cf and ea <= 2 * ca
+    assert ef < 2e-7 and ea < 2e-7

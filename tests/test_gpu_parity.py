@@ -149,3 +149,21 @@ def test_replays_are_bit_reproducible_and_graph_owned():
     assert not torch.equal(r1.x, a)
     r2 = plan.replay(y0, synchronize=True)
     assert torch.equal(r2.x, a)  # deterministic reductions
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+@pytest.mark.parametrize("path", [p for p in PLAN_FILES if "rtx_" not in p], ids=lambda p: Path(p).stem)
+def test_fp32_fft_mode_plan_matches_reference_golden(path, profile):
+    """The plans with the operator as FP32 FFTs (dft_terms=0) meet the same
+    bar against the reference."""
+    need_gpu()
+    from fbme_b200.config import fbme_profile_config
+    from fbme_b200.plans import CUDAGraphSBLPlan
+
+    y_np, grid, g = plan_case(path)
+    y = torch.from_numpy(y_np).cuda()
+    cfg = fbme_profile_config(profile)
+    cfg.dft_terms = 0
+    res = CUDAGraphSBLPlan(y, grid, config=cfg, warmup=1).replay(y, synchronize=True)
+    _check_plan_fields(res, g, profile, sensitivity(g, profile), label=Path(path).stem + " fft")
