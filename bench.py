@@ -34,6 +34,9 @@ for _p in (str(REPO), str(REPO / "fbme-sbl_b200")):
 METRIC = "scenes/s at equal NMSE: plain vs learned+batched FBME on 1 B200; % roofline"
 UNIT = "scenes/s"
 GRID, PREFIX = (256, 256), (128, 128)
+DFT_FORMS = {0: "FP32 FFT stages (two-pass register FFT, cp.async double-buffered)",
+             3: "tcgen05 split-BF16 3-term, FP32 accumulation",
+             6: "tcgen05 split-BF16 6-term, FP32 accumulation"}
 WORKLOAD = ("FBME-Stable replay, 256x256 grid / 128x128 prefix, 200 Rayleigh points, 15 dB, "
             "polish_size=32")
 
@@ -733,7 +736,7 @@ def run_ours(a: argparse.Namespace) -> None:
     peaks = _peaks()
     peak = peaks["hbm"]
     achieved = alg / per_launch_s / 1e9 if alg else None
-    stages = stages_table(prof, B, GRID, PREFIX, peaks)
+    stages = stages_table(prof, B, GRID, PREFIX, peaks, int(plan._engine.native_cfg.dft_terms))
     t_u = plan._engine.native_cfg.uamp_iterations
     p_iters = plan._engine.native_cfg.polish_iterations
     step_bytes = scene_bytes(n, m, t_u, p_iters) * B
@@ -763,7 +766,7 @@ def run_ours(a: argparse.Namespace) -> None:
                 "workload": WORKLOAD, "profile": a.profile, "scenes_per_step_per_gpu": B,
                 "parallelism": f"scene-sharded x{world}", "l2": "inputs larger than L2 "
                 f"(resident state {step_bytes / 1e6:.0f} MB algorithmic traffic per step)",
-                "dft": "tcgen05 split-BF16 3-term, FP32 accumulation",
+                "dft": DFT_FORMS[int(plan._engine.native_cfg.dft_terms)],
                 "nmse_db": nmse_db, "scenes_with_status": status_bad,
             },
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(y_host.numel() * 8),

@@ -121,8 +121,12 @@ def measure(grid: Sequence[int], sample: Sequence[int], cfg, device, batch: int,
     stage tiles `n_tile` wide (CUDA events, after two warm-up solves)."""
     import torch
 
-    from .engine import FBMEEngine
+    import dataclasses
 
+    from .engine import FBMEEngine, resolve_dft_terms
+
+    # timed as the uneven plans run it: the tensor-core stages
+    cfg = dataclasses.replace(cfg, dft_terms=resolve_dft_terms(int(cfg.dft_terms), grid, uneven=True))
     eng = FBMEEngine(batch, grid, sample, cfg, device, n_tile=n_tile)
     try:
         g = torch.Generator(device=device).manual_seed(1234)
@@ -146,7 +150,12 @@ def tune_shape(grid: Sequence[int], sample: Sequence[int], cfg, device, batch: i
                device_name: str | None = None) -> int:
     """The fastest tile width for this shape and batch class, from the cache
     or measured (and then stored)."""
-    terms = int(getattr(cfg, "dft_terms", 3))
+    from .engine import resolve_dft_terms
+
+    # the tile width of the tensor-core stages, which uneven plans run
+    terms = resolve_dft_terms(int(getattr(cfg, "dft_terms", 3)), grid, uneven=True)
+    if terms == 0:
+        return 256  # the FP32 FFT stages have no tile width to choose
     if device_name is None:
         import torch
 

@@ -159,13 +159,14 @@ class SBLConfig:
     device: str | torch.device = "auto"
     return_history: bool = True
     verbose: bool = False
-    # B200 extension: split-BF16 products of the tensor-core DFT (3 or 6)
-    # for mode="uamp" and mode="cg".  Both stay within 1e-5 relative of the
-    # exact operator (FP32 tensor-core accumulation bounds the error).
-    # dft_terms=0 (mode="uamp", equal-shape plans, N1 and N2 of the form
-    # 2^a or 3 * 2^a up to 512) runs the operator as FP32 FFTs instead: the
-    # error of an FP32 FFT (~5e-8).
-    dft_terms: int = 3
+    # B200 extension: how the prefix DFT stages run for mode="uamp".
+    # 3 or 6: split-BF16 products on the tensor cores (within 1e-5 relative
+    # of the exact operator; FP32 tensor-core accumulation bounds the error).
+    # 0: FP32 FFT stages (equal-shape plans, N1 and N2 of the form 2^a or
+    # 3 * 2^a up to 512), with the error of an FP32 FFT (~1.5e-7).
+    # -1 (default): 0 where that applies, else 3.  cg_dft_terms is the
+    # same choice for mode="cg" (3 or 6).
+    dft_terms: int = -1
     cg_dft_terms: int = 3
 
     # ------------------------------------------------------------------ presets
@@ -398,7 +399,7 @@ def _rules(c: SBLConfig):
     yield ("Off-grid refinement settings are invalid.",
            c.offgrid_max_iter < 1 or c.offgrid_tolerance <= 0.0 or c.offgrid_max_step <= 0.0
            or c.offgrid_damping <= 0.0 or c.offgrid_ridge < 0.0)
-    yield "dft_terms must be 0 (FP32 FFT), 3 or 6.", c.dft_terms not in (0, 3, 6)
+    yield "dft_terms must be -1 (automatic), 0 (FP32 FFT), 3 or 6.", c.dft_terms not in (-1, 0, 3, 6)
     yield "cg_dft_terms must be 3 or 6.", c.cg_dft_terms not in (3, 6)
 
 

@@ -459,34 +459,65 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
         }
       }
     }
-    __syncthreads();
 
     // outputs c < C, row on the contiguous axis: thread (c0, row) stores
-    // columns c0, c0 + P, ... of row r0 + row (ROWS consecutive rows)
+    // columns c0 + P i (i < L / P) of row r0 + row (ROWS consecutive rows).
+    // The residual's observations (and mask bits) are loaded a chunk of
+    // CH columns ahead, the first chunk before the barrier, so that their
+    // latency overlaps it.
+    constexpr int NC = L / P;
+    constexpr int CH = NC <= 16 ? NC : (NC % 16 == 0 ? 16 : 8);
     const int row = threadIdx.x % ROWS, c0 = threadIdx.x / ROWS;
     const int rr = r0 + row;
-    float acc = 0.f;
-    if (rr < st.rows) {
-      const long long base = unit * st.out_stride;
-      const long long step = static_cast<long long>(P) * st.out_ld;
-      long long o = static_cast<long long>(c0) * st.out_ld + rr;
-      const float2* sp = buf + row * A + row;
-      if (io.mode == 0) {
-        for (int c = c0; c < st.cols; c += P, o += step) io.out[base + o] = sp[c];
-      } else if (io.mode == 1) {
-        for (int c = c0; c < st.cols; c += P, o += step) {
-          const float2 x = sp[c];
-          io.out[base + o] = x;
-          acc += abs_sq(x);
+    const bool live_out = rr < st.rows;
+    const long long base = unit * st.out_stride;
+    const long long o0 = static_cast<long long>(c0) * st.out_ld + rr;
+    const long long step = static_cast<long long>(P) * st.out_ld;
+    float2 yv[CH];
+    uint32_t obs = 0;
+    auto load_chunk = [&](int g) {
+      obs = 0;
+      if (io.mode == 2 && live_out) {
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          const int ii = g * CH + i;
+          const long long o = o0 + ii * step;
+          if (c0 + P * ii < st.cols && (!io.mask || io.mask[o])) {
+            yv[i] = __ldg(io.y + base + o);
+            obs |= 1u << i;
+          }
         }
-      } else {
+      }
+    };
+    load_chunk(0);
+    __syncthreads();
+
+    float acc = 0.f;
+    const float2* sp = buf + row * A + row;
+    if (io.mode != 2) {
+      if (live_out) {
+        long long o = base + o0;
         for (int c = c0; c < st.cols; c += P, o += step) {
           const float2 x = sp[c];
-          io.out[base + o] = x;
-          if (!io.mask || io.mask[o]) {
-            const float2 yy = __ldg(io.y + base + o);
-            const float dr = yy.x - x.x, di = yy.y - x.y;
-            acc += dr * dr + di * di;
+          io.out[o] = x;
+          if (io.mode == 1) acc += abs_sq(x);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int g = 0; g < NC / CH; ++g) {
+        if (g > 0) load_chunk(g);
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          const int ii = g * CH + i;
+          const int c = c0 + P * ii;
+          if (live_out && c < st.cols) {
+            const float2 x = sp[c];
+            io.out[base + o0 + ii * step] = x;
+            if (obs >> i & 1u) {
+              const float dr = yv[i].x - x.x, di = yv[i].y - x.y;
+              acc += dr * dr + di * di;
+            }
           }
         }
       }

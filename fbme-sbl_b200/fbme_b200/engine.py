@@ -37,8 +37,28 @@ def uamp_iteration_limit(cfg: SBLConfig, n_grid: int, n_samples: int) -> int:
     return limit
 
 
+def fft_length_ok(n: int) -> bool:
+    """Grid lengths the FP32 FFT stages take: 2^a or 3 * 2^a, 2 <= n <= 512."""
+    n = int(n)
+    if n < 2 or n > 512:
+        return False
+    if n % 3 == 0:
+        n //= 3
+    return n & (n - 1) == 0
+
+
+def resolve_dft_terms(requested: int, grid: Sequence[int], uneven: bool = False) -> int:
+    """The DFT stage form a plan runs: ``requested`` unless it is -1
+    (automatic), which picks the FP32 FFT stages (0) for equal-shape plans
+    whose grid lengths allow them and the 3-term tensor-core products
+    otherwise."""
+    if requested != -1:
+        return int(requested)
+    return 0 if not uneven and fft_length_ok(grid[0]) and fft_length_ok(grid[1]) else 3
+
+
 def resolve_native_config(cfg: SBLConfig, grid: Sequence[int], sample: Sequence[int],
-                          n_observed: int | None = None) -> nat.FbmeConfig:
+                          n_observed: int | None = None, uneven: bool = False) -> nat.FbmeConfig:
     """Map the hot-path fields of ``cfg`` to ``FbmeConfig``.  Under an
     observation mask the sample count is the observed one
     (operator.n_samples in solver.py)."""
@@ -75,7 +95,7 @@ def resolve_native_config(cfg: SBLConfig, grid: Sequence[int], sample: Sequence[
     c.cholesky_jitter_multiplier = cfg.cuda_cholesky_jitter_multiplier
     c.support_false_alarm_budget = (cfg.uamp_support_false_alarm_budget
                                     if cfg.uamp_support_false_alarm_budget is not None else 0.0)
-    c.dft_terms = cfg.dft_terms
+    c.dft_terms = resolve_dft_terms(cfg.dft_terms, grid, uneven)
     return c
 
 
@@ -145,7 +165,7 @@ class FBMEEngine:
         if n_tile is None:
             from .autotune import default_width
 
-            n_tile = default_width(self.grid, self.sample, self.batch, int(cfg.dft_terms),
+            n_tile = default_width(self.grid, self.sample, self.batch, int(self.native_cfg.dft_terms),
                                    torch.cuda.get_device_properties(device).multi_processor_count)
         self.n_tile = n_tile
         self._params = nat.FbmeShapeParams(shapes[0], 0, -1.0, -1, int(n_tile or 0))

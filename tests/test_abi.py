@@ -56,10 +56,15 @@ def test_workspace_bytes_and_validation_codes():
     rc = lib.fbme_plan_create(bad, 1, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
     assert rc == nat.FBME_ERR_INVALID and "0 < M <= N" in nat.last_error()
     # scenes of different shapes make an uneven plan: sized, then refused
-    # here only for the missing workspace
+    # here only for the missing workspace.  Uneven plans run the tensor-core
+    # stages; the FP32 FFT stages (what the 256x256 config resolves to) are
+    # refused for them.
+    assert c.dft_terms == 0
     uneven = (nat.FbmeShape * 2)(nat.FbmeShape(64, 64, 32, 32), nat.FbmeShape(128, 64, 32, 32))
-    assert lib.fbme_plan_workspace_bytes(uneven, 2, ctypes.byref(c)) > 0
-    rc = lib.fbme_plan_create(uneven, 2, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
+    assert lib.fbme_plan_workspace_bytes(uneven, 2, ctypes.byref(c)) == 0
+    c3 = _cfg(dft_terms=3)
+    assert lib.fbme_plan_workspace_bytes(uneven, 2, ctypes.byref(c3)) > 0
+    rc = lib.fbme_plan_create(uneven, 2, ctypes.byref(c3), None, 0, None, ctypes.byref(plan))
     assert rc == nat.FBME_ERR_WORKSPACE
     rc = lib.fbme_plan_create(shapes, 2, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
     assert rc == nat.FBME_ERR_WORKSPACE

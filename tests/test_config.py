@@ -56,7 +56,16 @@ def test_uamp_budget_and_native_mapping():
     n = resolve_native_config(stable, (256, 256), (128, 128))
     assert n.uamp_iterations == 4 and n.polish_size == 32 and n.exchange_size == 12
     assert abs(n.uamp_damping - 0.05) < 1e-7 and n.fixed_budget_diagnostics == 1
-    assert abs(n.support_false_alarm_budget - 0.5) < 1e-7 and n.dft_terms == 3
+    assert abs(n.support_false_alarm_budget - 0.5) < 1e-7
+    # automatic DFT form: FP32 FFT stages where both grid lengths are 2^a or
+    # 3 * 2^a (<= 512) in an equal-shape plan, else the 3-term products
+    assert n.dft_terms == 0
+    assert resolve_native_config(stable, (40, 32), (20, 16)).dft_terms == 3
+    assert resolve_native_config(stable, (384, 192), (100, 90)).dft_terms == 0
+    assert resolve_native_config(stable, (1024, 256), (512, 128)).dft_terms == 3
+    assert resolve_native_config(stable, (256, 256), (128, 128), uneven=True).dft_terms == 3
+    assert resolve_native_config(SBLConfig.paper_hybrid_uamp(uamp_polish_size=32, dft_terms=6),
+                                 (256, 256), (128, 128)).dft_terms == 6
     hybrid = SBLConfig.fast_hybrid_uamp()
     h = resolve_native_config(hybrid, (256, 256), (128, 128))
     # adaptive damping: max(0.1, min(0.8, 0.02 * N / M)) = 0.1

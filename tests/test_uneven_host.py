@@ -25,7 +25,8 @@ SHAPES = [((64, 64), (32, 32)), ((128, 64), (48, 40)), ((96, 128), (40, 64)),
 def _sizes(shapes, params=None, cfg=None):
     lib = nat.lib()
     cfg = cfg or fbme_profile_config("stable")
-    c = resolve_native_config(cfg, shapes[0][0], shapes[0][1])
+    # the tensor-core stages, whose tile widths these tests probe
+    c = resolve_native_config(cfg, shapes[0][0], shapes[0][1], uneven=True)
     arr = (nat.FbmeShape * len(shapes))(*[nat.FbmeShape(g[0], g[1], s[0], s[1]) for g, s in shapes])
     if params is None:
         return lib.fbme_plan_workspace_bytes_ex(arr, len(shapes), ctypes.byref(c), None, 0)
