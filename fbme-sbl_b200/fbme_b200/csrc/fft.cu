@@ -40,7 +40,7 @@ struct FftPlan {
   int radix[kFftMaxPasses];    // radices in pass order
   int rows_per_cta;            // RT
   float sign;                  // -1 forward, +1 adjoint
-  const float2* tw;            // exp(-2 pi i k / L), k < L (FP64-evaluated)
+  const float2* tw;            // FP64-evaluated roots of unity (fft_twiddle_kernel's layout)
 };
 
 // One stage over `units` transforms: geometry of the GEMM stage it replaces.
@@ -340,14 +340,16 @@ __host__ __device__ constexpr int fast_threads_per_row(int L) {
   return L == 512 || L == 384 || L == 256 ? 16 : L == 192 || L == 128 || L == 96 || L == 64 ? 8
                                                  : L == 48 || L == 32 ? 4 : 0;
 }
-// Complex values of one row's area: at least Q (P + 1) for the exchange
-// and L + ROWS for the output staging (row lr stages its outputs at offset
-// lr, so that the ROWS rows read in one pass fall on distinct banks), and
-// = P mod 16 so that the 16 / P rows served in one shared-memory phase of
-// the exchange fall on disjoint banks.
+// Complex values of one row's area: at least Q (P + 2) for the exchange
+// (column k1 at k1 (P + 2): 16-byte aligned for the pass-2 vector reads,
+// whose 8-lane phases then fall on distinct banks) and L + ROWS for the
+// output staging (row lr stages its outputs at offset lr, so that the ROWS
+// rows read in one pass fall on distinct banks), and = P mod 16 so that the
+// 16 / P rows served in one 64-bit shared-memory phase of the exchange fall
+// on disjoint banks.
 __host__ __device__ constexpr int fast_row_area(int L) {
   const int P = fast_threads_per_row(L), Q = L / P, ROWS = kFftThreads / P;
-  int a = Q * (P + 1) > L + ROWS ? Q * (P + 1) : L + ROWS;
+  int a = Q * (P + 2) > L + ROWS ? Q * (P + 2) : L + ROWS;
   while (a % 16 != P % 16) ++a;
   return a;
 }
@@ -427,11 +429,11 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
 #pragma unroll
     for (int k1 = 0; k1 < Q; ++k1) {
       float2 y = v[k1];
-      if (k1 > 0) {  // w_L^(p k1), p k1 < L
-        const float2 w = __ldg(st.p.tw + p * k1);
+      if (k1 > 0) {  // w_L^(p k1), stored at k1 P + p
+        const float2 w = __ldg(st.p.tw + k1 * P + p);
         y = cmul(y, S < 0 ? w : make_float2(w.x, -w.y));
       }
-      ya[k1 * (P + 1) + p] = y;
+      ya[k1 * (P + 2) + p] = y;
     }
     __syncwarp();
 
@@ -441,8 +443,13 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
     for (int j = 0; j < J; ++j) {
       const int k1 = p + j * P;
       if (Q % P == 0 || k1 < Q) {
+        const float4* col = reinterpret_cast<const float4*>(ya + k1 * (P + 2));
 #pragma unroll
-        for (int pp = 0; pp < P; ++pp) u[j][pp] = ya[k1 * (P + 1) + pp];
+        for (int pp = 0; pp < P / 2; ++pp) {
+          const float4 t = col[pp];
+          u[j][2 * pp] = make_float2(t.x, t.y);
+          u[j][2 * pp + 1] = make_float2(t.z, t.w);
+        }
         RegDft<P, S>::run(u[j]);
       }
     }
@@ -654,17 +661,22 @@ void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2
 int fft_stage_tiles(int rows, int L) { return ceil_div(rows, fft_rows_per_cta(L)); }
 
 namespace {
-__global__ void fft_twiddle_kernel(float2* dst, int L) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= L) return;
+// The twiddles of one transform length, FP64-evaluated: for the two-pass
+// kernel (P threads per row) entry k1 P + p is w_L^(p k1), so that the P
+// threads of a row read one contiguous run per k1; for the Stockham kernel
+// entry k is w_L^k.
+__global__ void fft_twiddle_kernel(float2* dst, int L, int P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L) return;
+  const int e = P ? ((i % P) * (i / P)) % L : i;
   double s, c;
-  sincospi(-2.0 * static_cast<double>(k) / static_cast<double>(L), &s, &c);
-  dst[k] = make_float2(static_cast<float>(c), static_cast<float>(s));
+  sincospi(-2.0 * static_cast<double>(e) / static_cast<double>(L), &s, &c);
+  dst[i] = make_float2(static_cast<float>(c), static_cast<float>(s));
 }
 }  // namespace
 
 void launch_fft_twiddles(float2* dst, int L, cudaStream_t st) {
-  fft_twiddle_kernel<<<(L + 255) / 256, 256, 0, st>>>(dst, L);
+  fft_twiddle_kernel<<<(L + 255) / 256, 256, 0, st>>>(dst, L, fast_threads_per_row(L));
 }
 
 }  // namespace fbme

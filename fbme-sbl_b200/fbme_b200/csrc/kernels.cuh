@@ -101,7 +101,8 @@ struct DftTables {
   const uint8_t* adj_n1;  // L = N1, sign +1
   int kchunks_n1, kchunks_n2;
   int n_tile;  // real output columns per stage tile the tables are laid out for
-  // FP32 FFT mode (dft_terms = 0): exp(-2 pi i k / L), k < L, for L = N1, N2
+  // FP32 FFT mode (dft_terms = 0): the FP64-evaluated twiddles of lengths
+  // N1 and N2, in the layout of fft.cu (fft_twiddle_kernel)
   const float2* fft_n1;
   const float2* fft_n2;
 };
