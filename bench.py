@@ -564,15 +564,18 @@ def algorithmic_bytes(group: str, n: int, m: int) -> int:
     return table.get(group, 0)
 
 
-def physical_bytes(group: str, grid, prefix) -> int:
+def physical_bytes(group: str, grid, prefix, fused_denoise: bool = False) -> int:
     """Bytes one scene moves to and from HBM in one launch of a kernel group,
-    intermediates included (each array read or written once)."""
+    intermediates included (each array read or written once).  With
+    `fused_denoise` (the FP32 FFT stages) adjoint stage 2 runs the denoiser
+    in its epilogue: the group reads U instead of the lift A^H m."""
     n1, n2 = grid
     m1, m2 = prefix
     n, m = n1 * n2, m1 * m2
     t_fwd, t_adj = 8 * m2 * n1, 8 * n2 * m1  # the two-stage intermediates T, U
     table = {
-        "adjoint_denoise": 40 * n,            # read lift 8, mu 8, gamma 4, v 4; write mu 8, v 4, gamma 4
+        # read lift 8 (fused: U), mu 8, gamma 4, v 4; write mu 8, v 4, gamma 4
+        "adjoint_denoise": (t_adj + 32 * n) if fused_denoise else 40 * n,
         "message": 32 * m,                    # read y, prediction, message; write message
         "adjoint_1": 8 * m + t_adj,           # read message; write U
         "adjoint_2": t_adj + 8 * n,           # read U; write lift
@@ -609,7 +612,7 @@ def stages_table(prof: dict, batch: int, grid, prefix, peaks: dict, terms: int =
     executed tensor FLOPs against dense BF16."""
     out = {}
     for g, (ms, cnt) in prof.items():
-        pb = physical_bytes(g, grid, prefix) * batch
+        pb = physical_bytes(g, grid, prefix, terms == 0) * batch
         fl = stage_flops(g, grid, prefix, terms, n_tile) * batch
         if not (pb or fl) or cnt == 0:
             continue
@@ -736,6 +739,7 @@ def run_ours(a: argparse.Namespace) -> None:
     peaks = _peaks()
     peak = peaks["hbm"]
     achieved = alg / per_launch_s / 1e9 if alg else None
+    fft_stages = int(plan._engine.native_cfg.dft_terms) == 0
     stages = stages_table(prof, B, GRID, PREFIX, peaks, int(plan._engine.native_cfg.dft_terms))
     t_u = plan._engine.native_cfg.uamp_iterations
     p_iters = plan._engine.native_cfg.polish_iterations
@@ -779,10 +783,13 @@ def run_ours(a: argparse.Namespace) -> None:
                 "bound": "hbm", "kernel": dom_name,
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": physical_bytes(dom_name, GRID, PREFIX) * B or None,
-                "traffic_source": "the kernel's own byte accounting (bench.physical_bytes: the lift "
-                                  "A^H m that adjoint stage 2 writes is read back, 8 B/px beyond the "
-                                  "algorithmic 32 B/px); ncu DRAM counters agree in profiles/",
+                "traffic": physical_bytes(dom_name, GRID, PREFIX, fft_stages) * B or None,
+                "traffic_source": ("the kernel's own byte accounting (bench.physical_bytes: adjoint "
+                                   "stage 2 with the denoiser in its epilogue reads the intermediate U, "
+                                   "8 N2 M1 B per scene beyond the algorithmic 32 B/px)" if fft_stages else
+                                   "the kernel's own byte accounting (bench.physical_bytes: the lift "
+                                   "A^H m that adjoint stage 2 writes is read back, 8 B/px beyond the "
+                                   "algorithmic 32 B/px)") + "; ncu DRAM counters agree in profiles/",
                 "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_s * 1000.0,
                 "peak_source": peaks["source"],
                 "step_algorithmic_gbs": step_gbs, "step_frac": step_gbs / peak,

@@ -24,6 +24,7 @@
 #include <utility>
 
 #include "common.cuh"
+#include "denoise.cuh"
 #include "kernels.cuh"
 #include "stage.cuh"
 
@@ -132,6 +133,10 @@ FBME_DEV float2* fft_rows(const FftPlan& p, int rt, int pitch, float2* a, float2
 //   mode 1  store A^H y, sum |A^H y|^2  (EpiBackprojection, slot 1)
 //   mode 2  store p, sum |y - p|^2      (EpiPredict, slot 2; masked)
 // and `ysum`: sum |In|^2 of the input rows (ProYPower, slot 3).
+//   mode 3  the UAMP denoiser on A^H m in place of storing it (two-pass
+//           kernel only): mean, variance, prior and score keys updated as
+//           denoise_kernel does, per-tile sums of relevance (slot 0) and
+//           variance (slot 1)
 struct FftIo {
   const float2* in;
   float2* out;
@@ -140,6 +145,7 @@ struct FftIo {
   double* part;
   int mode;
   int ysum;
+  DenoiseArgs dn;         // mode 3
 };
 
 __global__ void __launch_bounds__(kFftThreads) fft_stage_kernel(const FftStage S, const FftIo io) {
@@ -389,7 +395,8 @@ FBME_DEV void fast_issue(const FftStage& st, const FftIo& io, int t, float2* buf
 // Persistent: CTA b takes tiles b, b + gridDim.x, ... (tile t = unit x
 // tiles + row tile); the copy of its next tile is in flight while the
 // current one is transformed.
-template <int L, int S>
+// EPI: 0 store (modes 0 and 1), 1 residual (mode 2), 2 denoiser (mode 3)
+template <int L, int S, int EPI>
 __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage st, const FftIo io) {
   constexpr int P = fast_threads_per_row(L), Q = L / P, ROWS = kFftThreads / P;
   constexpr int J = (Q + P - 1) / P;     // output columns k1 per thread in pass 2
@@ -467,9 +474,10 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
       }
     }
 
-    // outputs c < C, row on the contiguous axis: thread (c0, row) stores
+    // outputs c < C, row on the contiguous axis: thread (c0, row) handles
     // columns c0 + P i (i < L / P) of row r0 + row (ROWS consecutive rows).
-    // The residual's observations (and mask bits) are loaded a chunk of
+    // The epilogue's other operands (the residual's observations and mask
+    // bits, the denoiser's prior, mean and variance) are loaded a chunk of
     // CH columns ahead, the first chunk before the barrier, so that their
     // latency overlaps it.
     constexpr int NC = L / P;
@@ -480,28 +488,10 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
     const long long base = unit * st.out_stride;
     const long long o0 = static_cast<long long>(c0) * st.out_ld + rr;
     const long long step = static_cast<long long>(P) * st.out_ld;
-    float2 yv[CH];
-    uint32_t obs = 0;
-    auto load_chunk = [&](int g) {
-      obs = 0;
-      if (io.mode == 2 && live_out) {
-#pragma unroll
-        for (int i = 0; i < CH; ++i) {
-          const int ii = g * CH + i;
-          const long long o = o0 + ii * step;
-          if (c0 + P * ii < st.cols && (!io.mask || io.mask[o])) {
-            yv[i] = __ldg(io.y + base + o);
-            obs |= 1u << i;
-          }
-        }
-      }
-    };
-    load_chunk(0);
-    __syncthreads();
-
-    float acc = 0.f;
     const float2* sp = buf + row * A + row;
-    if (io.mode != 2) {
+    if constexpr (EPI == 0) {
+      __syncthreads();
+      float acc = 0.f;
       if (live_out) {
         long long o = base + o0;
         for (int c = c0; c < st.cols; c += P, o += step) {
@@ -510,7 +500,30 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
           if (io.mode == 1) acc += abs_sq(x);
         }
       }
-    } else {
+      if (io.mode == 1) {
+        const double w = warp_sum(static_cast<double>(acc));
+        if ((threadIdx.x & 31) == 0) *part_slot(io.part, unit, tile, 1 * kPartWarps + (threadIdx.x >> 5)) = w;
+      }
+    } else if constexpr (EPI == 1) {
+      float2 yv[CH];
+      uint32_t obs = 0;
+      auto load_chunk = [&](int g) {
+        obs = 0;
+        if (live_out) {
+#pragma unroll
+          for (int i = 0; i < CH; ++i) {
+            const int ii = g * CH + i;
+            const long long o = o0 + ii * step;
+            if (c0 + P * ii < st.cols && (!io.mask || io.mask[o])) {
+              yv[i] = __ldg(io.y + base + o);
+              obs |= 1u << i;
+            }
+          }
+        }
+      };
+      load_chunk(0);
+      __syncthreads();
+      float acc = 0.f;
 #pragma unroll
       for (int g = 0; g < NC / CH; ++g) {
         if (g > 0) load_chunk(g);
@@ -528,38 +541,101 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
           }
         }
       }
-    }
-    if (io.mode != 0) {
       const double w = warp_sum(static_cast<double>(acc));
-      if ((threadIdx.x & 31) == 0)
-        *part_slot(io.part, unit, tile, (io.mode == 1 ? 1 : 2) * kPartWarps + (threadIdx.x >> 5)) = w;
+      if ((threadIdx.x & 31) == 0) *part_slot(io.part, unit, tile, 2 * kPartWarps + (threadIdx.x >> 5)) = w;
+    } else {
+      // four registers a column: chunks of at most 8 columns
+      constexpr int CD = NC % 8 == 0 ? 8 : (NC % 4 == 0 ? 4 : NC);
+      const DenoiseArgs& dn = io.dn;
+      float gv[CD], vv[CD];
+      float2 mv[CD];
+      auto load_chunk = [&](int g) {
+        if (live_out) {
+#pragma unroll
+          for (int i = 0; i < CD; ++i) {
+            const int ii = g * CD + i;
+            if (c0 + P * ii < st.cols) {
+              const long long o = base + o0 + ii * step;
+              gv[i] = dn.gamma[o];
+              mv[i] = dn.mu[o];
+              vv[i] = dn.var[o];
+            }
+          }
+        }
+      };
+      load_chunk(0);
+      __syncthreads();
+      const float pv = dn.pv[unit], fl = dn.floor_[unit];
+      float dof = 0.f, sv = 0.f;
+#pragma unroll
+      for (int g = 0; g < NC / CD; ++g) {
+        if (g > 0) load_chunk(g);
+#pragma unroll
+        for (int i = 0; i < CD; ++i) {
+          const int ii = g * CD + i;
+          const int c = c0 + P * ii;
+          if (live_out && c < st.cols) {
+            const DenoiseOut r = denoise_math(dn, gv[i], mv[i], vv[i], sp[c], pv, fl);
+            const long long o = base + o0 + ii * step;
+            dn.mu[o] = r.mean;
+            dn.var[o] = r.variance;
+            if (dn.update_prior) dn.gamma[o] = r.gamma;
+            if (dn.keys) dn.keys[o] = float_key(abs_sq(r.mean) + r.variance);
+            dof += r.rel;
+            sv += r.variance;
+          }
+        }
+      }
+      const double w0 = warp_sum(static_cast<double>(dof));
+      const double w1 = warp_sum(static_cast<double>(sv));
+      if ((threadIdx.x & 31) == 0) {
+        *part_slot(io.part, unit, tile, 0 * kPartWarps + (threadIdx.x >> 5)) = w0;
+        *part_slot(io.part, unit, tile, 1 * kPartWarps + (threadIdx.x >> 5)) = w1;
+      }
     }
     __syncthreads();  // this buffer takes the copy issued at the top of the next tile
   }
   cp_async_wait<0>();
 }
 
-template <int L>
-void launch_fast(const FftStage& S, const FftIo& io, int sign, cudaStream_t st) {
-  void (*kern)(const FftStage, const FftIo) = sign < 0 ? fft_fast_kernel<L, -1> : fft_fast_kernel<L, 1>;
+template <int L, int S, int EPI>
+void launch_fast_as(const FftStage& S_, const FftIo& io, cudaStream_t st) {
+  auto kern = fft_fast_kernel<L, S, EPI>;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFftThreads, fast_smem_bytes(L)) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  const long long total = static_cast<long long>(S.tiles) * S.units;
+  const long long total = static_cast<long long>(S_.tiles) * S_.units;
   const long long cap = static_cast<long long>(sm_count()) * per_sm;
   const int grid = static_cast<int>(total < cap ? total : cap);
-  if (grid > 0) kern<<<grid, kFftThreads, fast_smem_bytes(L), st>>>(S, io);
+  if (grid > 0) kern<<<grid, kFftThreads, fast_smem_bytes(L), st>>>(S_, io);
+}
+
+// Forward stages store or take the residual; adjoint stages store or run
+// the denoiser (the combinations the UAMP sweeps use).
+template <int L>
+void launch_fast(const FftStage& S, const FftIo& io, int sign, cudaStream_t st) {
+  if (sign < 0) {
+    if (io.mode == 2) launch_fast_as<L, -1, 1>(S, io, st);
+    else launch_fast_as<L, -1, 0>(S, io, st);
+  } else {
+    if (io.mode == 3) launch_fast_as<L, 1, 2>(S, io, st);
+    else launch_fast_as<L, 1, 0>(S, io, st);
+  }
 }
 
 template <int L>
 cudaError_t set_fast_attr() {
-  cudaError_t e = cudaFuncSetAttribute(fft_fast_kernel<L, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(fast_smem_bytes(L)));
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(fft_fast_kernel<L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(fast_smem_bytes(L)));
+  const int bytes = static_cast<int>(fast_smem_bytes(L));
+  cudaError_t e = cudaFuncSetAttribute(fft_fast_kernel<L, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fft_fast_kernel<L, -1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fft_fast_kernel<L, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fft_fast_kernel<L, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
 }
 
 }  // namespace
@@ -629,8 +705,14 @@ cudaError_t set_fft_attributes() {
 
 // One FFT stage of `units` transforms (the geometry of the GEMM stage `g`,
 // whose contracted length K is padded to the transform length L).
+// The fused denoiser epilogue pays where two CTAs fit on an SM; at L = 512
+// (one CTA of 147 KB) its loads find too few warps, and the elementwise
+// denoiser at full occupancy is faster.
+int fft_denoise_fused(int L) { return fast_threads_per_row(L) != 0 && L < 512; }
+
 void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2* in, float2* out,
-               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st) {
+               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st,
+               const DenoiseArgs* dn) {
   FftStage S;
   S.p = make_plan(L, sign, tw);
   S.rows = g.rows;
@@ -643,6 +725,7 @@ void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2
   S.tiles = ceil_div(g.rows, fft_rows_per_cta(L));
   S.units = g.n_scenes;
   FftIo io{in, out, y, mask, part, mode, ysum};
+  if (dn) io.dn = *dn;
   switch (L) {
     case 512: launch_fast<512>(S, io, sign, st); return;
     case 384: launch_fast<384>(S, io, sign, st); return;

@@ -254,9 +254,14 @@ static cudaError_t set_attr_both() {
 }  // namespace fbme
 
 namespace fbme {
+struct DenoiseArgs;
 // One FP32 FFT stage (fft.cu) with the geometry of the GEMM stage `g`: a
 // length-L transform of sign `sign` per row, input zero-padded from g.kcplx,
-// output truncated to g.cols.
+// output truncated to g.cols.  Mode 3 (with `dn`) runs the UAMP denoiser on
+// the outputs instead of storing them; fft_denoise_fused(L) says whether
+// that is built for the length.
 void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2* in, float2* out,
-               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st);
+               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st,
+               const DenoiseArgs* dn = nullptr);
+int fft_denoise_fused(int L);
 }  // namespace fbme

@@ -20,6 +20,7 @@
 
 #include <vector>
 
+#include "denoise.cuh"
 #include "dft_umma.cuh"
 #include "kernels.cuh"
 #include "stage.cuh"
@@ -127,53 +128,6 @@ struct EpiBackprojection {
     acc = 0.f;
   }
 };
-
-// Gaussian denoiser with damping and the fused ARD prior update
-// (triton_kernels.py:140-192; solver.py:2832-2850, 1600-1607).
-struct DenoiseArgs {
-  float2* mu;
-  float* var;
-  float* gamma;
-  const float* pv;
-  const float* floor_;
-  double* part;
-  uint32_t* keys;  // optional: score key of |mu|^2 + v for the top-K
-  float damping, prior_damping, prior_max, hyper_shape, hyper_rate;
-  float inv_hyper;  // 1 / (1 + hyper_shape)
-  int update_prior;
-};
-
-FBME_DEV uint32_t float_key(float f) {
-  const uint32_t b = __float_as_uint(f);
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
-// One coefficient of the denoiser (triton_kernels.py:140-184): new mean,
-// variance, relevance and (optionally) prior variance.  Divisions use the
-// fast reciprocal path (<= 2 ulp), as the fused Triton kernel's `/` does.
-struct DenoiseOut {
-  float2 mean;
-  float variance, rel, gamma;
-};
-
-FBME_DEV DenoiseOut denoise_math(const DenoiseArgs& a, float prior, float2 om, float ov_raw,
-                                 float2 L, float pv, float fl) {
-  DenoiseOut o;
-  const float ov = fmaxf(ov_raw, kTiny);
-  const float den = fmaxf(prior + pv, kTiny);
-  const float gain = __fdividef(prior, den);
-  const float2 pm = make_float2(om.x + pv * L.x, om.y + pv * L.y);
-  const float keep = a.damping, upd = 1.0f - a.damping;
-  o.mean = make_float2(keep * om.x + upd * (gain * pm.x), keep * om.y + upd * (gain * pm.y));
-  const float cv = __fdividef(prior * pv, den);
-  o.variance = fmaxf(keep * ov + upd * cv, kTiny);
-  o.rel = fmaxf(0.0f, fminf(1.0f, 1.0f - __fdividef(o.variance, fmaxf(prior, kTiny))));
-  const float second = o.mean.x * o.mean.x + o.mean.y * o.mean.y + o.variance;
-  float cand = (second + a.hyper_rate) * a.inv_hyper;
-  cand = fmaxf(fl, fminf(a.prior_max, cand));
-  o.gamma = fmaxf(a.prior_damping * prior + (1.0f - a.prior_damping) * cand, fl);
-  return o;
-}
 
 // ---------------------------------------------------------------------------
 // elementwise kernels
@@ -613,10 +567,10 @@ static void stage2(int terms, bool split, const DftGeom& g2, const float2* tmp, 
 // the N2 axis, stages 2 the N1 axis; forward stages take the minus sign.
 static void fft_of(Stage which, const BatchShape& s, const DftTables& t, const DftGeom& g, const float2* in,
                    float2* out, const float2* y, const uint8_t* mask, double* part, int mode, int ysum,
-                   cudaStream_t st) {
+                   cudaStream_t st, const DenoiseArgs* dn = nullptr) {
   const bool ax2 = which == kFwd1 || which == kAdj1;
   fft_stage(g, ax2 ? s.n2 : s.n1, (which == kFwd1 || which == kFwd2) ? -1 : 1, ax2 ? t.fft_n2 : t.fft_n1, in,
-            out, y, mask, part, mode, ysum, st);
+            out, y, mask, part, mode, ysum, st, dn);
 }
 // Partial-sum source of an FFT stage: its row tiles x 8 warps.
 static PartSrc fft_src(Stage which, const BatchShape& s, const DftGeom& g) {
@@ -757,6 +711,10 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
     if (fft) fft_of(kAdj2, s, t, a2, u.tmp, u.lift, nullptr, nullptr, nullptr, 0, 0, st);
     else stage2(c.terms, split, a2, u.tmp, EpiStoreT{u.lift}, u.status, st);
   };
+  // FP32 FFT mode: adjoint stage 2 runs the denoiser in its epilogue, so
+  // A^H m never goes to memory
+  const bool fused_denoise = fft && fft_denoise_fused(s.n1);
+  auto adj2_denoise = [&]() { fft_of(kAdj2, s, t, a2, u.tmp, nullptr, nullptr, nullptr, u.part, 3, 0, st, &da); };
   auto fwd1 = [&]() {
     if (fft) fft_of(kFwd1, s, t, f1, u.mu, u.tmp, nullptr, nullptr, nullptr, 0, 0, st);
     else stage1(c.terms, split, f1, f2, ProPlain{u.mu}, u.tmp, u.status, st);
@@ -782,10 +740,15 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                                                                       u.sc.prec, u.sc.dvar, c.uamp_damping, u.mask)));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, adj1(msg[cur ^ 1]));
       cur ^= 1;
-      FBME_TIMED(prof, FBME_GROUP_ADJ_2, adj2());
-      FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
-                 (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
-      src_dof = PartSrc{bn, 1};
+      if (fused_denoise) {
+        FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, adj2_denoise());
+        src_dof = fft_src(kAdj2, s, a2);
+      } else {
+        FBME_TIMED(prof, FBME_GROUP_ADJ_2, adj2());
+        FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
+                   (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
+        src_dof = PartSrc{bn, 1};
+      }
     }
     FBME_TIMED(prof, FBME_GROUP_FWD_1, fwd1());
     FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, fwd2());
@@ -801,8 +764,13 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE, adj1(msg[cur ^ 1]));
   da.update_prior = 0;
   da.keys = reinterpret_cast<uint32_t*>(u.keys);
-  FBME_TIMED(prof, FBME_GROUP_ADJ_2, adj2());
-  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
+  if (fused_denoise) {
+    FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, adj2_denoise());
+  } else {
+    FBME_TIMED(prof, FBME_GROUP_ADJ_2, adj2());
+    FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE,
+               (denoise_kernel<<<dim3(bn, s.B), kEwThreads, 0, st>>>(s, da, u.lift)));
+  }
 }
 
 // ---------------------------------------------------------------------------
