@@ -348,9 +348,13 @@ def _stable_cholesky(matrix: np.ndarray, tiny, eps, *, mode: str, multiplier: fl
 
 
 def active_posterior_with_evidence(y, prior, noise, op: PrefixOperator, active, *, columns,
-                                   gram, column_data, data_energy, chol_mode, chol_multiplier):
-    """solver.py:3591-3779 with tail_loading=0 and no global certificate.
+                                   gram, column_data, data_energy, chol_mode, chol_multiplier,
+                                   tail_loading=0.0):
+    """solver.py:3591-3779 without the global certificate.
 
+    ``tail_loading``: 0 (the exact zero-tail model of the polish) or None,
+    the omitted prior variance sum(prior) - sum(prior[active]) as an
+    isotropic loading (solver.py:3632-3639, the cg active-set posterior).
     Returns (mean[B,N], posterior_variance[B,N], data_diagonal[B,N], nle[B]).
     """
     rd = op.rdtype
@@ -358,7 +362,11 @@ def active_posterior_with_evidence(y, prior, noise, op: PrefixOperator, active, 
     b, k = active.shape
     rows = np.arange(b)[:, None]
     gamma = prior[rows, active]
-    eff_noise = noise + rd(0.0)
+    if tail_loading is None:
+        omitted = np.maximum(prior.sum(axis=1, dtype=rd) - gamma.sum(axis=1, dtype=rd), rd(0.0))
+    else:
+        omitted = rd(tail_loading)
+    eff_noise = (noise + omitted).astype(rd)
     system = np.zeros((b, k, k), y.dtype)
     system[:, np.arange(k), np.arange(k)] = (rd(1.0) / gamma).astype(y.dtype)
     system = system + gram / eff_noise[:, None, None]
@@ -944,6 +952,25 @@ def pcg(rhs, prior, noise, op: PrefixOperator, cfg: OracleConfig, *, initial, to
     return out.astype(op.cdtype), it
 
 
+def select_active_indices(prior, minimum_size, maximum_size, tail_fraction):
+    """solver.py:3184-3216: the ARD active set of a single scene once at
+    most ``maximum_size`` coefficients hold 1 - tail_fraction of the prior
+    variance (largest first, ties by index), else None."""
+    if prior.shape[0] != 1 or not np.isfinite(prior).all():
+        return None
+    rd = prior.dtype.type
+    maximum = min(maximum_size, prior.shape[1])
+    order = np.argsort(-prior[0], kind="stable")[:maximum]
+    values = prior[0, order]
+    target = rd(1.0 - tail_fraction) * prior.sum(axis=1, dtype=rd)[0]
+    if values.sum(dtype=rd) < target:
+        return None
+    cumulative = np.cumsum(values, dtype=rd)
+    required = min(int(np.searchsorted(cumulative, target, side="left")), maximum - 1) + 1
+    size = min(maximum, max(minimum_size, required))
+    return order[None, :size]
+
+
 def project_relevance(prior, dd, n_samples, eps):
     """solver.py:3156-3181."""
     rel = np.clip(prior * dd, 0, 1)
@@ -953,8 +980,10 @@ def project_relevance(prior, dd, n_samples, eps):
 
 
 def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda"):
-    """``fast_sbl`` with ``mode="cg"`` and ``active_set=False`` (or batch >
-    1, where the reference never switches).  ``probes``: [B, M, Pmax]
+    """``fast_sbl`` with ``mode="cg"``.  A single scene with ``active_set``
+    switches to the exact reduced posterior on the selected ARD set once the
+    variance tail is small (solver.py:1316-1341, 3184-3216), after which the
+    omitted prior variances stay fixed (1684-1693).  ``probes``: [B, M, Pmax]
     (default: the reference's CPU Rademacher stream)."""
     data = np.asarray(data)
     cdtype = np.complex128 if data.dtype in (np.complex128, np.float64) else np.complex64
@@ -993,31 +1022,61 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
     solution = None
     streak = 0
     converged = False
-    hist = {"relative_change": [], "noise_variance": [], "effective_dof": [], "cg_iterations": []}
+    hist = {"relative_change": [], "noise_variance": [], "effective_dof": [], "cg_iterations": [],
+            "active_set_size": []}
+    active = None
+    columns = gram = None
+
+    def reduced():
+        """solver.py:3897-3920: the reduced posterior with the omitted
+        variance as an isotropic loading."""
+        cd = np.conj(np.swapaxes(columns, 1, 2)) @ y[:, :, None]
+        mean_a, pv_a, dd_a, _ = active_posterior_with_evidence(
+            y, prior, noise, op, active, columns=columns, gram=gram, column_data=cd,
+            data_energy=_abs2(y).sum(axis=1, dtype=rd), chol_mode=chol_mode,
+            chol_multiplier=cfg.cuda_cholesky_jitter_multiplier, tail_loading=None)
+        return mean_a.astype(cdtype), pv_a.astype(rd), dd_a.astype(rd)
+
     it = 0
     for it in range(1, limit + 1):
+        if (cfg.active_set and b == 1 and active is None and it >= cfg.active_set_start
+                and (it - cfg.active_set_start) % cfg.active_set_check_interval == 0):
+            active = select_active_indices(prior, cfg.active_set_min_size, cfg.active_set_max_size,
+                                           cfg.active_set_tail_fraction)
+            if active is not None:
+                columns = op.fourier_columns(active).astype(cdtype)
+                gram = np.conj(np.swapaxes(columns, 1, 2)) @ columns
+                solution = None
         count, tol_cg = cg_schedule(it, cfg, pmax)
         tol_cg = max(tol_cg, 3.0 * float(eps) ** 0.5)
+        if active is not None:
+            mean, pv, dd = reduced()
+            cg_it = 0
         rhs = np.concatenate([y[:, :, None], probes[:, :, :count]], axis=2)
-        if cfg.cg_warm_start and solution is not None and solution.shape[2] != 1 + count:
-            rs = np.zeros((b, m, 1 + count), cdtype)
-            sh = min(1 + count, solution.shape[2])
-            rs[:, :, :sh] = solution[:, :, :sh]
-            solution = rs
-        sol, cg_it = pcg(rhs, prior, noise, op, cfg, initial=solution if cfg.cg_warm_start else None,
-                         tolerance=tol_cg, chol_mode=chol_mode, matvec_mode=cfg.cg_matvec)
-        lifted = op.adjoint(sol)
-        dd = np.maximum(np.real(lifted[:, :, 1:] * np.conj(lifted_probes[:, :, :count])).mean(axis=2),
-                        0.0).astype(rd)
-        mean = (prior * lifted[:, :, 0]).astype(cdtype)
-        pv = np.maximum(prior - np.square(prior) * dd, 0.0).astype(rd)
-        solution = sol if cfg.cg_warm_start else None
+        if active is None:
+            if cfg.cg_warm_start and solution is not None and solution.shape[2] != 1 + count:
+                rs = np.zeros((b, m, 1 + count), cdtype)
+                sh = min(1 + count, solution.shape[2])
+                rs[:, :, :sh] = solution[:, :, :sh]
+                solution = rs
+            sol, cg_it = pcg(rhs, prior, noise, op, cfg, initial=solution if cfg.cg_warm_start else None,
+                             tolerance=tol_cg, chol_mode=chol_mode, matvec_mode=cfg.cg_matvec)
+            lifted = op.adjoint(sol)
+            dd = np.maximum(np.real(lifted[:, :, 1:] * np.conj(lifted_probes[:, :, :count])).mean(axis=2),
+                            0.0).astype(rd)
+            mean = (prior * lifted[:, :, 0]).astype(cdtype)
+            pv = np.maximum(prior - np.square(prior) * dd, 0.0).astype(rd)
+            solution = sol if cfg.cg_warm_start else None
         rel = project_relevance(prior, dd, m, eps).astype(rd)
         dof = rel.sum(axis=1, dtype=rd)
         # MacKay precision update (solver.py:1669-1677)
         prec = (rel + rd(cfg.hyper_shape)) / (_abs2(mean) + rd(cfg.hyper_rate))
         prec = np.clip(prec, rd(1.0 / cfg.max_precision), rd(cfg.max_precision))
         new_prior = (rd(1.0) / prec).astype(rd)
+        if active is not None:  # ARD deletion is permanent (solver.py:1684-1693)
+            keep_mask = np.zeros((b, n), bool)
+            keep_mask[0, active[0]] = True
+            new_prior = np.where(keep_mask, new_prior, prior).astype(rd)
         # noise update (solver.py:1737-1768)
         residual = y - op.forward_flat(mean)
         energy = _abs2(residual).sum(axis=1, dtype=rd)
@@ -1040,31 +1099,38 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
         hist["noise_variance"].append(float(noise.mean()))
         hist["effective_dof"].append(float(dof.mean()))
         hist["cg_iterations"].append(cg_it)
+        hist["active_set_size"].append(0 if active is None else int(active.shape[1]))
         if should_check:
             streak = streak + 1 if change <= cfg.tol else 0
             if streak >= cfg.convergence_patience:
                 converged = True
                 break
-    # final posterior with all probes (solver.py:2023-2080)
-    rhs = np.concatenate([y[:, :, None], probes], axis=2)
-    if cfg.cg_warm_start and solution is not None and solution.shape[2] != rhs.shape[2]:
-        rs = np.zeros_like(rhs)
-        sh = min(rhs.shape[2], solution.shape[2])
-        rs[:, :, :sh] = solution[:, :, :sh]
-        solution = rs
-    sol, _ = pcg(rhs, prior, noise, op, cfg, initial=solution if cfg.cg_warm_start else None,
-                 tolerance=max(cfg.cg_tolerance, 3.0 * float(eps) ** 0.5), chol_mode=chol_mode,
-                 matvec_mode=cfg.cg_matvec)
-    lifted = op.adjoint(sol)
-    dd = np.maximum(np.real(lifted[:, :, 1:] * np.conj(lifted_probes)).mean(axis=2), 0.0).astype(rd)
-    mean = (prior * lifted[:, :, 0]).astype(cdtype)
-    pv = np.maximum(prior - np.square(prior) * dd, 0.0).astype(rd)
+    # final posterior: all probes, or the reduced posterior after a switch
+    # (solver.py:2023-2080)
+    if active is not None:
+        mean, pv, dd = reduced()
+    else:
+        rhs = np.concatenate([y[:, :, None], probes], axis=2)
+        if cfg.cg_warm_start and solution is not None and solution.shape[2] != rhs.shape[2]:
+            rs = np.zeros_like(rhs)
+            sh = min(rhs.shape[2], solution.shape[2])
+            rs[:, :, :sh] = solution[:, :, :sh]
+            solution = rs
+        sol, _ = pcg(rhs, prior, noise, op, cfg, initial=solution if cfg.cg_warm_start else None,
+                     tolerance=max(cfg.cg_tolerance, 3.0 * float(eps) ** 0.5), chol_mode=chol_mode,
+                     matvec_mode=cfg.cg_matvec)
+        lifted = op.adjoint(sol)
+        dd = np.maximum(np.real(lifted[:, :, 1:] * np.conj(lifted_probes)).mean(axis=2), 0.0).astype(rd)
+        mean = (prior * lifted[:, :, 0]).astype(cdtype)
+        pv = np.maximum(prior - np.square(prior) * dd, 0.0).astype(rd)
     dof = project_relevance(prior, dd, m, eps).sum(axis=1, dtype=rd)
     shape = tuple(grid)
     out = dict(x=mean.reshape((b,) + shape), posterior_variance=pv.reshape((b,) + shape),
                precision=(rd(1.0) / prior).reshape((b,) + shape), noise_variance=noise,
                effective_dof=dof.astype(rd), iterations=it, converged=converged, mode="cg",
-               history=hist, relative_change=hist["relative_change"][-1])
+               history=hist, relative_change=hist["relative_change"][-1],
+               active_set_size=0 if active is None else int(active.shape[1]),
+               active_indices=None if active is None else active[0])
     if single:
         for key in ("x", "posterior_variance", "precision", "noise_variance", "effective_dof"):
             out[key] = out[key][0]

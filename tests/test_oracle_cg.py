@@ -15,7 +15,9 @@ import pytest
 
 from oracle import fbme_oracle as O
 
-CG = sorted(glob.glob(str(Path(__file__).parent / "golden" / "cg" / "cg_*.npz")))
+CG = sorted(p for p in glob.glob(str(Path(__file__).parent / "golden" / "cg" / "cg_*.npz"))
+            if not Path(p).name.startswith("cg_active_"))
+ACTIVE = sorted(glob.glob(str(Path(__file__).parent / "golden" / "cg" / "cg_active_*.npz")))
 
 
 def _rel(a, b):
@@ -41,6 +43,45 @@ def test_cg_oracle_matches_reference_fp64(path):
     np.testing.assert_array_equal(r["history"]["cg_iterations"], g["f64_history_cg_iterations"])
     np.testing.assert_allclose(r["history"]["relative_change"], g["f64_history_relative_change"],
                                rtol=1e-9)
+
+
+@pytest.mark.parametrize("path", ACTIVE, ids=lambda p: Path(p).stem)
+def test_cg_active_set_switch_matches_reference(path):
+    """A single scene switches to the exact reduced posterior on the same
+    ARD set at the same iteration as the reference (sbl_2d, mode="cg",
+    default active-set parameters, CUDA Cholesky loading), and the FP64
+    restatement reproduces the reference's FP64 run."""
+    g = np.load(path)
+    grid = tuple(int(v) for v in g["grid"])
+    cfg = O.OracleConfig(mode="cg", max_iter=int(g["max_iter"]), tol=0.0)
+    for tag, dtype, bar in (("f64", np.complex128, 1e-6), ("f32", np.complex64, 4.0 * float(g["gap_x"]))):
+        r = O.fast_sbl_cg(g["y"][0].astype(dtype), grid, cfg)
+        np.testing.assert_array_equal(r["history"]["active_set_size"], g[tag + "_history_active_set_size"])
+        assert r["active_set_size"] == int(g[tag + "_active_set_size"])
+        assert _rel(r["x"], g[tag + "_x"]) < bar
+        assert _rel(r["posterior_variance"], g[tag + "_posterior_variance"]) < 1e2 * bar
+        np.testing.assert_allclose(r["noise_variance"], g[tag + "_noise_variance"][0], rtol=1e2 * bar)
+        np.testing.assert_allclose(r["effective_dof"], g[tag + "_effective_dof"][0], rtol=1e2 * bar)
+
+
+def test_active_set_selection_rule():
+    """solver.py:3184-3216 on hand-made priors: no switch while the tail
+    holds more than the fraction, the smallest prefix reaching 1 - tail
+    otherwise, clamped to [minimum, maximum]; batches never switch."""
+    p = np.full((1, 100), 1e-3, np.float32)
+    p[0, [5, 17, 42]] = [10.0, 5.0, 1.0]
+    # total 16.097: 95 % needs the three large values, 90 % two of them
+    np.testing.assert_array_equal(O.select_active_indices(p, 2, 10, 0.05), [[5, 17, 42]])
+    np.testing.assert_array_equal(O.select_active_indices(p, 1, 10, 0.1), [[5, 17]])
+    assert O.select_active_indices(p, 4, 10, 0.1).shape == (1, 4)
+    # the 10 largest hold 16.007 < 99.9 % of the total: no switch
+    assert O.select_active_indices(p, 1, 10, 0.001) is None
+    flat = np.ones((1, 100), np.float32)
+    assert O.select_active_indices(flat, 2, 10, 0.05) is None
+    assert O.select_active_indices(np.concatenate([p, p]), 2, 10, 0.05) is None
+    bad = p.copy()
+    bad[0, 3] = np.nan
+    assert O.select_active_indices(bad, 2, 10, 0.05) is None
 
 
 def _dense_q(op, prior, noise):
