@@ -136,6 +136,11 @@ class FbmeCgConfig(ctypes.Structure):
         ("warm_start", c_int32),
         ("jitter_multiplier", c_float),
         ("dft_terms", c_int32),
+        ("active_set_start", c_int32),
+        ("active_set_check_interval", c_int32),
+        ("active_set_min_size", c_int32),
+        ("active_set_max_size", c_int32),
+        ("active_set_tail_fraction", c_float),
     ]
 
 
@@ -159,6 +164,8 @@ class FbmeCgInfo(ctypes.Structure):
         ("relative_change", c_float),
         ("last_cg_iterations", c_int32),
         ("history", POINTER(c_float)),
+        ("active_set_size", c_int32),
+        ("active_set_iteration", c_int32),
     ]
 
 

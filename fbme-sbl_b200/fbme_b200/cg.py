@@ -9,10 +9,13 @@ noise initialisation, the PCG solves with the low-rank preconditioner, the
 Hutchinson diagonal, the MacKay and noise updates, the convergence test and
 the final posterior.
 
+A single scene with ``active_set`` switches to the exact reduced posterior
+on its ARD set once the variance tail is small (solver.py:1316-1341): the
+native plan selects the set on the device and reads only its size.
+
 Not built here (``NotImplementedError``): joint sparsity, spatial coupling,
-the circulant / Nystrom / no preconditioner, off-grid refinement, and the
-active-set switch that single-scene runs make at ``active_set_start``
-(solver.py:1316-1341); pass ``active_set=False`` or a batch of scenes.
+the circulant / Nystrom / no preconditioner, off-grid refinement, and active
+sets above 1024 coefficients (``active_set_max_size``).
 """
 
 from __future__ import annotations
@@ -97,15 +100,15 @@ def check_cg_supported(cfg: SBLConfig, batch: int) -> None:
     bad = [k for k, v in unsupported.items() if v]
     if bad:
         raise NotImplementedError("the B200 cg path does not implement: " + ", ".join(bad))
-    if cfg.active_set and batch == 1 and cfg.max_iter >= cfg.active_set_start:
-        raise NotImplementedError(
-            "the active-set switch of single-scene cg runs (solver.py:1316-1341) is not built "
-            "on the B200 path; pass active_set=False or solve a batch")
+    if cfg.active_set and batch == 1 and cfg.active_set_max_size > 1024:
+        raise NotImplementedError("active_set_max_size above 1024 is not built on the B200 cg path")
     if cfg.cg_preconditioner_rank > 32:
         raise NotImplementedError("cg_preconditioner_rank above 32 is not built")
 
 
-def resolve_cg_config(cfg: SBLConfig, n_grid: int, n_samples: int) -> nat.FbmeCgConfig:
+def resolve_cg_config(cfg: SBLConfig, n_grid: int, n_samples: int, batch: int = 1) -> nat.FbmeCgConfig:
+    """Map ``cfg`` to ``FbmeCgConfig``; the active-set switch applies to a
+    single scene only (solver.py:1316-1323)."""
     c = nat.FbmeCgConfig()
     c.max_iter = cfg.max_iter
     c.min_iter = cfg.min_iter
@@ -139,6 +142,12 @@ def resolve_cg_config(cfg: SBLConfig, n_grid: int, n_samples: int) -> nat.FbmeCg
     c.warm_start = int(cfg.cg_warm_start)
     c.jitter_multiplier = cfg.cuda_cholesky_jitter_multiplier
     c.dft_terms = cfg.cg_dft_terms
+    switch = cfg.active_set and batch == 1 and not cfg.joint_sparsity
+    c.active_set_start = cfg.active_set_start if switch else 0
+    c.active_set_check_interval = cfg.active_set_check_interval
+    c.active_set_min_size = cfg.active_set_min_size
+    c.active_set_max_size = cfg.active_set_max_size
+    c.active_set_tail_fraction = cfg.active_set_tail_fraction
     return c
 
 
@@ -158,7 +167,7 @@ class CGEngine:
         self.sample = tuple(int(v) for v in sample)
         self.cfg = cfg
         self.n_grid, self.n_samples = prod(self.grid), prod(self.sample)
-        self.native_cfg = resolve_cg_config(cfg, self.n_grid, self.n_samples)
+        self.native_cfg = resolve_cg_config(cfg, self.n_grid, self.n_samples, self.batch)
         self.probes = int(self.native_cfg.probes)
         self._shape = nat.FbmeShape(self.grid[0], self.grid[1], self.sample[0], self.sample[1])
         nbytes = self.lib.fbme_cg_workspace_bytes(ctypes.byref(self._shape), self.batch,
@@ -241,7 +250,8 @@ class CGEngine:
             rows = hist[: it * 6].reshape(it, 6).astype(np.float64)
             for j, key in enumerate(nat.CG_HISTORY_COLUMNS):
                 history[key] = rows[:, j].tolist()
-            history["active_set_size"] = [0.0] * it
+            size, at = int(info.active_set_size), int(info.active_set_iteration)
+            history["active_set_size"] = [float(size) if size and i + 1 >= at else 0.0 for i in range(it)]
             history["spatial_vertical_coupling"] = [float(cfg.spatial_coupling)] * it
             history["spatial_horizontal_coupling"] = [float(cfg.spatial_coupling)] * it
         report = cfg.return_history or cfg.eager_change_tracking or cfg.tol > 0.0 or cfg.verbose
@@ -249,7 +259,8 @@ class CGEngine:
             x=x, posterior_variance=pv, precision=prec, noise_variance=noise, effective_dof=dof,
             iterations=it, converged=bool(info.converged),
             relative_change=float(info.relative_change) if report else float("nan"),
-            mode="cg", arithmetic_dtype="complex64", uamp_backend_used=None, active_set_size=0,
+            mode="cg", arithmetic_dtype="complex64", uamp_backend_used=None,
+            active_set_size=int(info.active_set_size),
             support_mask=mask,
             support_score_threshold=(torch.full((B,), threshold, **f32) if budget is not None
                                      else None),

@@ -752,6 +752,9 @@ struct CgEmArgs {
   float* gamma;
   const float* floor_;
   float keep, hyper_shape, hyper_rate, max_prec;
+  // after an active-set switch: 1 on the active set; the prior variances
+  // elsewhere keep their value (ARD deletion is permanent, solver.py:1684-1693)
+  const uint8_t* amask;
 };
 
 FBME_DEV float relevance_scale(const double* part, int b, int nb, long long M) {
@@ -780,8 +783,9 @@ __global__ void __launch_bounds__(kEwThreads) cg_em_kernel(const __grid_constant
     const float am = abs_sq(mu);
     float prec = (rel + A.hyper_shape) / (am + A.hyper_rate);
     prec = fminf(fmaxf(prec, lo), A.max_prec);
-    const float gnew = 1.0f / prec;
-    const float g = fmaxf(A.keep * A.gamma[e] + (1.0f - A.keep) * gnew, fl);
+    const float gold = A.gamma[e];
+    const float gnew = (A.amask && !A.amask[e]) ? gold : 1.0f / prec;
+    const float g = fmaxf(A.keep * gold + (1.0f - A.keep) * gnew, fl);
     A.gamma[e] = g;
     gs += g;
     const float2 pm = A.prev[e];
@@ -1333,8 +1337,10 @@ struct FbmeCgPlan {
   fbme::DftTables tables;
   float2 *dir1, *dir2;
   fbme::CgBuffers buf;
+  fbme::ActiveBufs act{};  // active-set switch (single-scene plans with active_set_start > 0)
+  int act_kmax = 0;        // 0: the switch is off
   fbme::CgEngine* eng = nullptr;
-  int* host = nullptr;  // pinned: [0] restart flag
+  int* host = nullptr;  // pinned: [0] restart flag, [4] change, [8] active-set size
   ~FbmeCgPlan() {
     delete eng;
     if (host) cudaFreeHost(host);
@@ -1348,8 +1354,14 @@ using fbme::api_fail;
 size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
 struct CgLayout {
-  size_t tab_f2, tab_a2, tab_f1, tab_a1, dir1, dir2, buffers, total;
+  size_t tab_f2, tab_a2, tab_f1, tab_a1, dir1, dir2, buffers, active, total;
 };
+
+// Size of the active set the switch may select (0: the switch is off).
+int active_kmax(const fbme::BatchShape& s, const FbmeCgConfig& c) {
+  if (c.active_set_start <= 0 || s.B != 1) return 0;
+  return static_cast<int>(std::min<long long>(c.active_set_max_size, s.n()));
+}
 
 CgLayout cg_layout(const fbme::BatchShape& s, const FbmeCgConfig& c) {
   CgLayout L{};
@@ -1373,6 +1385,8 @@ CgLayout cg_layout(const fbme::BatchShape& s, const FbmeCgConfig& c) {
   size_t offs[fbme::CgBuffers::kSlots];
   const int rank = std::min<long long>(c.preconditioner_rank, std::min(s.m(), s.n()));
   L.buffers = take(fbme::CgBuffers::layout(s, c.probes, rank, c.max_iter, offs));
+  const int kmax = active_kmax(s, c);
+  L.active = kmax > 0 ? take(fbme::cg_active_bytes(s.n(), kmax)) : 0;
   L.total = off;
   return L;
 }
@@ -1394,6 +1408,15 @@ int cg_validate(const FbmeShape* shape, int n, const FbmeCgConfig* c, fbme::Batc
     return api_fail(FBME_ERR_INVALID, "cg_max_iter and cg_check_interval must be positive");
   if (!(c->damping >= 0.f && c->damping < 1.f) || !(c->cg_damping >= 0.f && c->cg_damping < 1.f))
     return api_fail(FBME_ERR_INVALID, "damping values must be in [0, 1)");
+  if (c->active_set_start > 0) {
+    if (c->active_set_check_interval < 1 || c->active_set_min_size < 1 ||
+        c->active_set_max_size < c->active_set_min_size ||
+        !(c->active_set_tail_fraction > 0.f && c->active_set_tail_fraction < 1.f))
+      return api_fail(FBME_ERR_INVALID,
+                      "active set: check interval >= 1, 1 <= min_size <= max_size, tail fraction in (0, 1)");
+    if (c->active_set_max_size > fbme::kActiveMax)
+      return api_fail(FBME_ERR_UNSUPPORTED, "active_set_max_size above 1024 is not built");
+  }
   if (N > 524288 || s.n2 > 512)
     return api_fail(FBME_ERR_UNSUPPORTED, "grids above 524288 points or N2 > 512 are not built");
   if (N * n * (1LL + c->probes) > (1LL << 36)) return api_fail(FBME_ERR_INVALID, "batch too large");
@@ -1490,6 +1513,29 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
   int R_cur = 0;
   bool warm = false;
   int streak = 0, converged = 0, it = 0, last_cg = 0;
+  // active-set switch (single-scene plans): size and iteration once switched
+  int act_size = 0, act_iter = 0;
+  ActiveArgs aa{};
+  if (P->act_kmax > 0) {
+    aa.N = N;
+    aa.n1 = s.n1;
+    aa.n2 = s.n2;
+    aa.nb = nb;
+    aa.idx = P->act.idx;
+    aa.gamma = bf.gamma;
+    aa.bp = bf.bp;
+    aa.noise = bf.scal.noise;
+    aa.d1 = P->dir1;
+    aa.d2 = P->dir2;
+    aa.jitter = c.jitter_multiplier;
+    aa.E = P->act.E;
+    aa.X = P->act.X;
+    aa.mean = bf.mean;
+    aa.relc = bf.relc;
+    aa.pv_out = nullptr;
+    aa.part = bf.part;
+    aa.status = bf.status;
+  }
   std::vector<float> hchange(B);
   auto ensure_rhs = [&](int R) {
     if (R == R_cur) return;
@@ -1501,16 +1547,38 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     R_cur = R;
   };
   for (it = 1; it <= limit; ++it) {
+    if (P->act_kmax > 0 && act_size == 0 && it >= c.active_set_start &&
+        (it - c.active_set_start) % c.active_set_check_interval == 0) {
+      // _select_active_indices on the current prior (solver.py:1316-1341);
+      // the host reads the outcome, as the reference does
+      cg_active_select(bf.gamma, N, P->act_kmax, c.active_set_min_size, c.active_set_tail_fraction, P->act, st);
+      cudaMemcpyAsync(P->host + 8, P->act.sel, sizeof(int), cudaMemcpyDeviceToHost, st);
+      cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return api_fail(FBME_ERR_CUDA, std::string("cg_solve: ") + cudaGetErrorString(e));
+      if (P->host[8] > 0) {
+        act_size = P->host[8];
+        act_iter = it;
+        aa.K = act_size;
+        cg_active_mask(P->act, N, P->act_kmax, st);
+      }
+    }
     int count = pmax;
     float tolcg = c.cg_tolerance;
     cg_schedule(c, it, &count, &tolcg);
     tolcg = std::max(tolcg, floor_tol);
-    ensure_rhs(1 + count);
-    const int R = R_cur;
-    E.precond_build(st);
-    last_cg = E.pcg(R, tolcg, warm, st);
-    warm = c.warm_start != 0;
-    lift_and_hutch(P, R, count, nullptr, st);
+    if (act_size > 0) {
+      // exact reduced posterior on the active set: no PCG, no probes
+      cg_active_posterior(aa, st);
+      last_cg = 0;
+      count = 0;
+    } else {
+      ensure_rhs(1 + count);
+      const int R = R_cur;
+      E.precond_build(st);
+      last_cg = E.pcg(R, tolcg, warm, st);
+      warm = c.warm_start != 0;
+      lift_and_hutch(P, R, count, nullptr, st);
+    }
     run_stage(c.dft_terms, f1b, ProPlain{bf.mean}, EpiStoreT{bf.t2}, bf.status, st);
     run_stage(c.dft_terms, f2b, ProPlain{bf.t2}, EpiEnergy{y, bf.part, 0.0}, bf.status, st);
     CgEmArgs em;
@@ -1527,6 +1595,7 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     em.hyper_shape = c.hyper_shape;
     em.hyper_rate = c.hyper_rate;
     em.max_prec = c.max_precision;
+    em.amask = act_size > 0 ? P->act.mask : nullptr;
     CgScalarArgs sa;
     sa.s = s;
     sa.nb = nb;
@@ -1567,11 +1636,17 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     }
   }
   const int iterations = it > limit ? limit : it;
-  // final posterior with every probe (solver.py:2023-2080)
-  ensure_rhs(1 + pmax);
-  E.precond_build(st);
-  E.pcg(R_cur, std::max(c.cg_tolerance, floor_tol), warm, st);
-  lift_and_hutch(P, R_cur, pmax, out->posterior_variance, st);
+  // final posterior: every probe, or the reduced posterior after a switch
+  // (solver.py:2023-2080)
+  if (act_size > 0) {
+    aa.pv_out = out->posterior_variance;
+    cg_active_posterior(aa, st);
+  } else {
+    ensure_rhs(1 + pmax);
+    E.precond_build(st);
+    E.pcg(R_cur, std::max(c.cg_tolerance, floor_tol), warm, st);
+    lift_and_hutch(P, R_cur, pmax, out->posterior_variance, st);
+  }
   {
     CgScalarArgs sa{};
     sa.s = s;
@@ -1605,6 +1680,8 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     info->converged = converged;
     info->relative_change = hist[static_cast<size_t>(iterations - 1) * 6];
     info->last_cg_iterations = last_cg;
+    info->active_set_size = act_size;
+    info->active_set_iteration = act_iter;
     if (info->history) std::memcpy(info->history, hist.data(), hist.size() * sizeof(float));
   }
   return check_launch("cg_solve");
@@ -1673,6 +1750,8 @@ int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig*
   fbme::launch_dirichlet(P->dir2, s.m2, s.n2, st);
   const int rank = static_cast<int>(std::min<long long>(cfg->preconditioner_rank, std::min(s.m(), s.n())));
   P->buf.bind(s, cfg->probes, rank, cfg->max_iter, w + L.buffers);
+  P->act_kmax = active_kmax(s, *cfg);
+  if (P->act_kmax > 0) P->act = fbme::cg_active_bind(w + L.active, s.n(), P->act_kmax);
   fbme::CgSettings cs;
   cs.terms = terms;
   cs.rank = rank;

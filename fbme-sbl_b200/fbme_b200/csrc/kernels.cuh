@@ -221,6 +221,40 @@ void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, 
 void warm_prior_from_map(const float* map, int B, long long N, const float* data_power, const float* floor_,
                          float* gamma, double* upart, int nblocks, cudaStream_t st);
 
+// Active-set switch of single-scene cg runs (cg_active.cu).
+struct ActiveBufs {
+  int* sel;        // [0] selected size (0: no switch), [1] non-finite flag
+  int* idx;        // [kmax] selected grid indices, largest prior first
+  uint8_t* mask;   // [N] 1 on the active set
+  float2* E;       // [kmax * kmax] equilibrated system / Cholesky factor (column-major)
+  float2* X;       // [kmax * kmax] L^-1 (column-major, lower)
+};
+struct ActiveArgs {
+  long long N;
+  int n1, n2;      // grid
+  int K;           // active-set size
+  int nb;          // tiles of the EM kernels' relevance partials
+  const int* idx;
+  const float* gamma;
+  const float2* bp;    // A^H y
+  const float* noise;  // [1]
+  const float2 *d1, *d2;  // Dirichlet tables of the prefix
+  float jitter;        // Cholesky loading multiplier
+  float2 *E, *X;
+  float2* mean;        // [N] out
+  float* relc;         // [N] out: clipped relevance
+  float* pv_out;       // [N] out (optional): posterior variance
+  double* part;        // partial slots of scene 0
+  int* status;
+};
+constexpr int kActiveMax = 1024;  // largest active_set_max_size built
+size_t cg_active_bytes(long long N, int kmax);
+ActiveBufs cg_active_bind(uint8_t* w, long long N, int kmax);
+void cg_active_select(const float* gamma, long long N, int kmax, int min_size, float tail, const ActiveBufs& ab,
+                      cudaStream_t st);
+void cg_active_mask(const ActiveBufs& ab, long long N, int kmax, cudaStream_t st);
+void cg_active_posterior(const ActiveArgs& a, cudaStream_t st);
+
 // Shared by the C ABI translation units.
 int api_fail(int code, const std::string& msg);
 size_t dft_table_bytes(int L, int terms);

@@ -270,8 +270,13 @@ const char* fbme_topk_static_error(void);
  *                         low-rank preconditioner 5786-5848
  *   fbme_cg_matvec    <-> torch_sbl/operators.py:299-371 (Q = noise I +
  *                         A diag(prior) A^H; toeplitz_matvec / matvec)
- * The active-set switch of single-scene runs (solver.py:1316-1341) is not
- * part of this entry point: the host runs it with active_set off.
+ * A single-scene plan with active_set_start > 0 also runs the active-set
+ * switch (solver.py:1316-1341): from that EM iteration, every
+ * active_set_check_interval iterations until it switches, the ARD set is
+ * selected (_select_active_indices, 3184-3216) and, once selected, the
+ * remaining iterations and the final posterior use the exact reduced
+ * posterior on it (_active_posterior, 3897-3920) with the omitted prior
+ * variances fixed (1684-1693).
  * ---------------------------------------------------------------------- */
 typedef struct {
   int32_t max_iter, min_iter;           /* outer EM iterations */
@@ -293,6 +298,11 @@ typedef struct {
   int32_t adaptive_cg, adaptive_probes, warm_start;
   float jitter_multiplier;              /* Cholesky loading: max(10, m) * eps * mean|diag| */
   int32_t dft_terms;                    /* 3 or 6 split-BF16 products */
+  /* active-set switch (one scene only; 0 = off) */
+  int32_t active_set_start;             /* first EM iteration that may switch */
+  int32_t active_set_check_interval;
+  int32_t active_set_min_size, active_set_max_size;  /* max <= 1024 */
+  float active_set_tail_fraction;       /* in (0, 1) */
 } FbmeCgConfig;
 
 /* Device outputs of fbme_cg_solve (shapes [B][N1][N2] / [B]). */
@@ -316,6 +326,8 @@ typedef struct {
   float relative_change;
   int32_t last_cg_iterations;
   float* history;
+  int32_t active_set_size;       /* size of the switched-to active set (0: none) */
+  int32_t active_set_iteration;  /* EM iteration of the switch (0: none) */
 } FbmeCgInfo;
 
 typedef struct FbmeCgPlan FbmeCgPlan;
@@ -326,8 +338,8 @@ int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig*
                    FbmeCgPlan** plan);
 /* y: complex64 [B][M1][M2]; probes: float32 +-1 [B][P][M1][M2] (probe p of
  * scene b over the observed samples, the reference's probes[b, :, p]).
- * Synchronises `stream` at PCG restart checks and convergence checks, as
- * the reference reads those flags on the host. */
+ * Synchronises `stream` at PCG restart checks, convergence checks and
+ * active-set checks, as the reference reads those flags on the host. */
 int fbme_cg_solve(FbmeCgPlan* plan, const void* y, const float* probes, const FbmeCgOutputs* out,
                   FbmeCgInfo* info, fbme_stream_t stream);
 int fbme_cg_destroy(FbmeCgPlan* plan);

@@ -75,8 +75,10 @@ def test_resolve_cg_config_fields():
 
 
 def test_unsupported_cg_features_raise():
-    with pytest.raises(NotImplementedError, match="active-set"):
-        check_cg_supported(SBLConfig(), batch=1)
+    check_cg_supported(SBLConfig(), batch=1)  # the single-scene active-set switch is built
+    with pytest.raises(NotImplementedError, match="active_set_max_size"):
+        check_cg_supported(SBLConfig(active_set_max_size=2048), batch=1)
+    check_cg_supported(SBLConfig(active_set_max_size=2048), batch=2)  # batches never switch
     check_cg_supported(SBLConfig(), batch=2)
     check_cg_supported(SBLConfig(active_set=False), batch=1)
     with pytest.raises(NotImplementedError, match="circulant"):

@@ -29,7 +29,9 @@ torch = pytest.importorskip("torch")
 
 from oracle import fbme_oracle as O  # noqa: E402
 
-CG = sorted(glob.glob(str(Path(__file__).parent / "golden" / "cg" / "cg_*.npz")))
+CG = sorted(p for p in glob.glob(str(Path(__file__).parent / "golden" / "cg" / "cg_*.npz"))
+            if not Path(p).name.startswith("cg_active_"))
+ACTIVE = sorted(glob.glob(str(Path(__file__).parent / "golden" / "cg" / "cg_active_*.npz")))
 PCG_FLOOR_F32 = 3.0 * float(np.finfo(np.float32).eps) ** 0.5  # solver.py:1349-1352
 
 
@@ -178,6 +180,46 @@ def test_cg_solve_matches_reference_golden(path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", ACTIVE, ids=lambda p: Path(p).stem)
+def test_cg_active_set_switch_matches_reference_golden(path):
+    """One scene with the default active-set switch (sbl_2d's defaults,
+    tol=0, the reference's CPU probes): the switch comes at the reference's
+    iteration with the reference's set size, and the result meets the bar
+    of the cg fixtures against the reference's FP64 run."""
+    need_gpu()
+    from fbme_b200.cg import CGEngine
+    from fbme_b200.config import SBLConfig
+
+    g = np.load(path)
+    grid = tuple(int(v) for v in g["grid"])
+    y = g["y"]
+    M = y.shape[1] * y.shape[2]
+    cfg = SBLConfig(mode="cg", max_iter=int(g["max_iter"]), tol=0.0)
+    eng = CGEngine(1, grid, y.shape[1:], cfg, torch.device("cuda"))
+    probes = O.rademacher_probes(1, M, eng.probes, 0)
+    z = torch.from_numpy(np.ascontiguousarray(np.swapaxes(probes, 1, 2)).astype(np.float32)).cuda()
+    res = eng.solve(torch.from_numpy(y.reshape(1, M)).cuda(), z)
+    eng.close()
+    assert res.active_set_size == int(g["f64_active_set_size"])
+    np.testing.assert_array_equal(res.history["active_set_size"], g["f64_history_active_set_size"])
+    x = res.x.cpu().numpy().reshape(1, -1)
+    ex = rel_l2(x, g["f64_x"].reshape(1, -1))
+    epv = rel_l2(res.posterior_variance.cpu().numpy(), g["f64_posterior_variance"])
+    epr = rel_l2(res.precision.cpu().numpy(), g["f64_precision"])
+    print(f"{Path(path).stem}: x {ex:.2e} (ref gap {float(g['gap_x']):.2e}) pv {epv:.2e} "
+          f"(ref gap {float(g['gap_posterior_variance']):.2e}) precision {epr:.2e}")
+    assert ex < 3 * float(g["gap_x"]) + 2e-5
+    assert epv < 3 * float(g["gap_posterior_variance"]) + 2e-5
+    assert epr < 3 * float(g["gap_precision"]) + 2e-5
+    np.testing.assert_allclose(res.noise_variance.cpu().numpy().reshape(-1), g["f64_noise_variance"],
+                               rtol=1e-3)
+    np.testing.assert_allclose(res.effective_dof.cpu().numpy().reshape(-1), g["f64_effective_dof"],
+                               rtol=1e-3)
+    assert res.iterations == int(g["f64_iterations"])
+    assert int(res.status.abs().sum()) == 0
+
+
+@pytest.mark.gpu
 def test_cg_batch_equals_single_scene_solves():
     need_gpu()
     g = np.load([p for p in CG if "_b2_" in p][0])
@@ -205,8 +247,10 @@ def test_sbl_2d_cg_public_api():
     # the reference's CUDA probe stream: same seed -> same result
     res2 = sbl_2d(yt, grid, config=SBLConfig(mode="cg", active_set=False, max_iter=6))
     assert torch.equal(res.x, res2.x)
-    with pytest.raises(NotImplementedError):
-        sbl_2d(yt, grid, config=SBLConfig(mode="cg"))
+    # the default single-scene call switches to the reduced posterior
+    rd = sbl_2d(yt, grid, config=SBLConfig(mode="cg", max_iter=40))
+    assert rd.active_set_size > 0 and rd.history["active_set_size"][-1] == rd.active_set_size
+    assert rd.history["cg_iterations"][-1] == 0 and rd.history["hutchinson_probes"][-1] == 0
     batch = torch.stack([yt, yt])
     rb = sbl_2d(batch, grid, config=SBLConfig(mode="cg", max_iter=4,
                                                uamp_support_false_alarm_budget=0.5))
