@@ -141,6 +141,7 @@ class FbmeCgConfig(ctypes.Structure):
         ("active_set_min_size", c_int32),
         ("active_set_max_size", c_int32),
         ("active_set_tail_fraction", c_float),
+        ("dense", c_int32),
     ]
 
 

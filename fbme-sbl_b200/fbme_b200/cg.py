@@ -90,11 +90,11 @@ def make_probes(batch: int, n_samples: int, count: int, *, device: torch.device,
     return signs.index_select(2, owner).to(torch.float32) * hadamard.unsqueeze(0)
 
 
-def check_cg_supported(cfg: SBLConfig, batch: int) -> None:
+def check_cg_supported(cfg: SBLConfig, batch: int, dense: bool = False) -> None:
     unsupported = {
         "joint_sparsity": cfg.joint_sparsity,
         "spatial_coupling": cfg.spatial_coupling > 0.0 or cfg.learn_spatial_coupling,
-        f"cg_preconditioner={cfg.cg_preconditioner!r}": cfg.cg_preconditioner != "low_rank",
+        f"cg_preconditioner={cfg.cg_preconditioner!r}": cfg.cg_preconditioner != "low_rank" and not dense,
         "offgrid_refinement": cfg.offgrid_refinement,
     }
     bad = [k for k, v in unsupported.items() if v]
@@ -106,9 +106,11 @@ def check_cg_supported(cfg: SBLConfig, batch: int) -> None:
         raise NotImplementedError("cg_preconditioner_rank above 32 is not built")
 
 
-def resolve_cg_config(cfg: SBLConfig, n_grid: int, n_samples: int, batch: int = 1) -> nat.FbmeCgConfig:
+def resolve_cg_config(cfg: SBLConfig, n_grid: int, n_samples: int, batch: int = 1,
+                      dense: bool = False) -> nat.FbmeCgConfig:
     """Map ``cfg`` to ``FbmeCgConfig``; the active-set switch applies to a
-    single scene only (solver.py:1316-1323)."""
+    single scene only (solver.py:1316-1323).  ``dense``: mode="dense", the
+    exact posterior through the data covariance (no probes)."""
     c = nat.FbmeCgConfig()
     c.max_iter = cfg.max_iter
     c.min_iter = cfg.min_iter
@@ -142,12 +144,15 @@ def resolve_cg_config(cfg: SBLConfig, n_grid: int, n_samples: int, batch: int = 
     c.warm_start = int(cfg.cg_warm_start)
     c.jitter_multiplier = cfg.cuda_cholesky_jitter_multiplier
     c.dft_terms = cfg.cg_dft_terms
-    switch = cfg.active_set and batch == 1 and not cfg.joint_sparsity
+    switch = cfg.active_set and batch == 1 and not cfg.joint_sparsity and not dense
     c.active_set_start = cfg.active_set_start if switch else 0
     c.active_set_check_interval = cfg.active_set_check_interval
     c.active_set_min_size = cfg.active_set_min_size
     c.active_set_max_size = cfg.active_set_max_size
     c.active_set_tail_fraction = cfg.active_set_tail_fraction
+    c.dense = int(dense)
+    if dense:
+        c.probes = 0
     return c
 
 
@@ -155,10 +160,11 @@ class CGEngine:
     """A native cg plan for ``batch`` scenes of one shape and configuration."""
 
     def __init__(self, batch: int, grid: Sequence[int], sample: Sequence[int], cfg: SBLConfig,
-                 device: torch.device) -> None:
+                 device: torch.device, dense: bool = False) -> None:
         self.lib = nat.lib()
         if device.type != "cuda":
             raise RuntimeError("the B200 cg path needs a CUDA device")
+        self.dense = bool(dense)
         if device.index is None:
             device = torch.device("cuda", torch.cuda.current_device())
         self.device = device
@@ -167,7 +173,7 @@ class CGEngine:
         self.sample = tuple(int(v) for v in sample)
         self.cfg = cfg
         self.n_grid, self.n_samples = prod(self.grid), prod(self.sample)
-        self.native_cfg = resolve_cg_config(cfg, self.n_grid, self.n_samples, self.batch)
+        self.native_cfg = resolve_cg_config(cfg, self.n_grid, self.n_samples, self.batch, self.dense)
         self.probes = int(self.native_cfg.probes)
         self._shape = nat.FbmeShape(self.grid[0], self.grid[1], self.sample[0], self.sample[1])
         nbytes = self.lib.fbme_cg_workspace_bytes(ctypes.byref(self._shape), self.batch,
@@ -214,11 +220,14 @@ class CGEngine:
         the reference's generator stream)."""
         B, N, M = self.batch, self.n_grid, self.n_samples
         y = y.to(device=self.device, dtype=torch.complex64).reshape(B, M).contiguous()
-        if probes is None:
-            probes = self.default_probes()
-        probes = probes.to(device=self.device, dtype=torch.float32).contiguous()
-        if tuple(probes.shape) != (B, self.probes, M):
-            raise ValueError(f"probes must have shape {(B, self.probes, M)}")
+        if self.dense:  # no probes: a placeholder pointer for the C ABI
+            probes = torch.zeros(1, dtype=torch.float32, device=self.device)
+        else:
+            if probes is None:
+                probes = self.default_probes()
+            probes = probes.to(device=self.device, dtype=torch.float32).contiguous()
+            if tuple(probes.shape) != (B, self.probes, M):
+                raise ValueError(f"probes must have shape {(B, self.probes, M)}")
         f32 = dict(dtype=torch.float32, device=self.device)
         x = torch.empty(B, N, dtype=torch.complex64, device=self.device)
         pv = torch.empty(B, N, **f32)
@@ -259,7 +268,7 @@ class CGEngine:
             x=x, posterior_variance=pv, precision=prec, noise_variance=noise, effective_dof=dof,
             iterations=it, converged=bool(info.converged),
             relative_change=float(info.relative_change) if report else float("nan"),
-            mode="cg", arithmetic_dtype="complex64", uamp_backend_used=None,
+            mode="dense" if self.dense else "cg", arithmetic_dtype="complex64", uamp_backend_used=None,
             active_set_size=int(info.active_set_size),
             support_mask=mask,
             support_score_threshold=(torch.full((B,), threshold, **f32) if budget is not None
@@ -304,13 +313,14 @@ class CGEngine:
 
 
 def cg_sbl(tensor: Tensor, grid: Sequence[int], sample: Sequence[int], batch_shape: Sequence[int],
-           cfg: SBLConfig, device: torch.device) -> SBLResult:
-    """``fast_sbl`` with ``mode="cg"`` for ``tensor`` ``[*batch, *sample]``."""
+           cfg: SBLConfig, device: torch.device, dense: bool = False) -> SBLResult:
+    """``fast_sbl`` with ``mode="cg"`` (or ``mode="dense"``) for ``tensor``
+    ``[*batch, *sample]``."""
     batch = prod(batch_shape) if batch_shape else 1
-    check_cg_supported(cfg, batch)
+    check_cg_supported(cfg, batch, dense)
     grid2 = tuple(grid) if len(grid) == 2 else (1, grid[0])
     sample2 = tuple(sample) if len(sample) == 2 else (1, sample[0])
-    eng = CGEngine(batch, grid2, sample2, cfg, device)
+    eng = CGEngine(batch, grid2, sample2, cfg, device, dense=dense)
     try:
         y = tensor.to(device=device, dtype=torch.complex64).reshape(batch, -1)
         res = eng.solve(y)

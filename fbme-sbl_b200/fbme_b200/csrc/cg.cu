@@ -1337,6 +1337,7 @@ struct FbmeCgPlan {
   fbme::DftTables tables;
   float2 *dir1, *dir2;
   fbme::CgBuffers buf;
+  fbme::DenseBufs dense{};  // mode="dense" buffers (cfg.dense)
   fbme::ActiveBufs act{};  // active-set switch (single-scene plans with active_set_start > 0)
   int act_kmax = 0;        // 0: the switch is off
   fbme::CgEngine* eng = nullptr;
@@ -1354,12 +1355,12 @@ using fbme::api_fail;
 size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
 struct CgLayout {
-  size_t tab_f2, tab_a2, tab_f1, tab_a1, dir1, dir2, buffers, active, total;
+  size_t tab_f2, tab_a2, tab_f1, tab_a1, dir1, dir2, buffers, active, dense, total;
 };
 
 // Size of the active set the switch may select (0: the switch is off).
 int active_kmax(const fbme::BatchShape& s, const FbmeCgConfig& c) {
-  if (c.active_set_start <= 0 || s.B != 1) return 0;
+  if (c.dense || c.active_set_start <= 0 || s.B != 1) return 0;
   return static_cast<int>(std::min<long long>(c.active_set_max_size, s.n()));
 }
 
@@ -1387,6 +1388,7 @@ CgLayout cg_layout(const fbme::BatchShape& s, const FbmeCgConfig& c) {
   L.buffers = take(fbme::CgBuffers::layout(s, c.probes, rank, c.max_iter, offs));
   const int kmax = active_kmax(s, c);
   L.active = kmax > 0 ? take(fbme::cg_active_bytes(s.n(), kmax)) : 0;
+  L.dense = c.dense ? take(fbme::dense_bytes(s)) : 0;
   L.total = off;
   return L;
 }
@@ -1399,7 +1401,9 @@ int cg_validate(const FbmeShape* shape, int n, const FbmeCgConfig* c, fbme::Batc
   const long long N = 1LL * s.n1 * s.n2;
   if (c->dft_terms != 3 && c->dft_terms != 6) return api_fail(FBME_ERR_INVALID, "dft_terms must be 3 or 6");
   if (c->max_iter < 1 || c->min_iter < 0) return api_fail(FBME_ERR_INVALID, "max_iter must be positive");
-  if (c->probes < 1) return api_fail(FBME_ERR_INVALID, "CG mode requires Hutchinson probes");
+  if (c->dense && 1LL * s.m1 * s.m2 > 4096)
+    return api_fail(FBME_ERR_UNSUPPORTED, "dense mode above 4096 samples is not built");
+  if (c->probes < 1 && !c->dense) return api_fail(FBME_ERR_INVALID, "CG mode requires Hutchinson probes");
   if (c->probes > 128) return api_fail(FBME_ERR_UNSUPPORTED, "more than 128 Hutchinson probes");
   if (c->initial_probes < 1) return api_fail(FBME_ERR_INVALID, "initial_probes must be positive");
   if (c->preconditioner_rank < 0 || c->preconditioner_rank > 32)
@@ -1495,17 +1499,21 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
   u.status = bf.status;
   sbl_init(s, P->tables, P->dc, u, st);
   cudaMemcpyAsync(bf.gsum, bf.scal.dvar, B * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  const bool dense = c.dense != 0;
   // probes and their lift A^H z (solver.py:1209-1221)
-  cg_probe_kernel<<<grid_for(1LL * B * pmax * M), 256, 0, st>>>(1LL * B * pmax * M, probes, bf.pz);
-  adjoint_units(P, B * pmax, pmax, bf.pz, bf.lp, st);
+  if (!dense) {
+    cg_probe_kernel<<<grid_for(1LL * B * pmax * M), 256, 0, st>>>(1LL * B * pmax * M, probes, bf.pz);
+    adjoint_units(P, B * pmax, pmax, bf.pz, bf.lp, st);
+  }
   cudaMemsetAsync(bf.prev, 0, B * N * sizeof(float2), st);
   E.prior = bf.gamma;
   E.noise = bf.scal.noise;
   E.dcur = 0;
-  const int minimum = std::max(c.min_iter, c.cg_min_iter);
+  // mode="dense": damping alone and min_iter as the minimum (solver.py:1287-1293, 1483-1487)
+  const int minimum = dense ? c.min_iter : std::max(c.min_iter, c.cg_min_iter);
   const int limit = c.max_iter;
   const bool conv = c.tol > 0.f && minimum < limit;
-  const float keep = std::max(c.damping, c.cg_damping);
+  const float keep = dense ? c.damping : std::max(c.damping, c.cg_damping);
   const float floor_tol = 3.0f * std::sqrt(1.1920929e-07f);
   const int nb = ew_blocks_host(N);
   const DftGeom f1b = stage_geom_units(kFwd1, s, P->tables, nt, B, 1);
@@ -1566,7 +1574,12 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     float tolcg = c.cg_tolerance;
     cg_schedule(c, it, &count, &tolcg);
     tolcg = std::max(tolcg, floor_tol);
-    if (act_size > 0) {
+    if (dense) {
+      dense_posterior(s, P->dense, bf.gamma, bf.scal.noise, y, c.jitter_multiplier, bf.mean, bf.relc, nullptr,
+                      bf.part, nb, bf.status, st);
+      last_cg = 0;
+      count = 0;
+    } else if (act_size > 0) {
       // exact reduced posterior on the active set: no PCG, no probes
       cg_active_posterior(aa, st);
       last_cg = 0;
@@ -1579,8 +1592,10 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
       warm = c.warm_start != 0;
       lift_and_hutch(P, R, count, nullptr, st);
     }
-    run_stage(c.dft_terms, f1b, ProPlain{bf.mean}, EpiStoreT{bf.t2}, bf.status, st);
-    run_stage(c.dft_terms, f2b, ProPlain{bf.t2}, EpiEnergy{y, bf.part, 0.0}, bf.status, st);
+    if (!dense) {  // residual energy (dense mode: from Q^-1 y, in dense_posterior)
+      run_stage(c.dft_terms, f1b, ProPlain{bf.mean}, EpiStoreT{bf.t2}, bf.status, st);
+      run_stage(c.dft_terms, f2b, ProPlain{bf.t2}, EpiEnergy{y, bf.part, 0.0}, bf.status, st);
+    }
     CgEmArgs em;
     em.s = s;
     em.nb = nb;
@@ -1599,7 +1614,7 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     CgScalarArgs sa;
     sa.s = s;
     sa.nb = nb;
-    sa.etiles = f2b.row_tiles * f2b.col_tiles;
+    sa.etiles = dense ? 1 : f2b.row_tiles * f2b.col_tiles;
     sa.part = bf.part;
     sa.part2 = bf.part2;
     sa.noise = bf.scal.noise;
@@ -1638,7 +1653,10 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
   const int iterations = it > limit ? limit : it;
   // final posterior: every probe, or the reduced posterior after a switch
   // (solver.py:2023-2080)
-  if (act_size > 0) {
+  if (dense) {
+    dense_posterior(s, P->dense, bf.gamma, bf.scal.noise, y, c.jitter_multiplier, bf.mean, bf.relc,
+                    out->posterior_variance, bf.part, nb, bf.status, st);
+  } else if (act_size > 0) {
     aa.pv_out = out->posterior_variance;
     cg_active_posterior(aa, st);
   } else {
@@ -1750,6 +1768,7 @@ int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig*
   fbme::launch_dirichlet(P->dir2, s.m2, s.n2, st);
   const int rank = static_cast<int>(std::min<long long>(cfg->preconditioner_rank, std::min(s.m(), s.n())));
   P->buf.bind(s, cfg->probes, rank, cfg->max_iter, w + L.buffers);
+  if (cfg->dense) P->dense = fbme::dense_bind(w + L.dense, s, st);
   P->act_kmax = active_kmax(s, *cfg);
   if (P->act_kmax > 0) P->act = fbme::cg_active_bind(w + L.active, s.n(), P->act_kmax);
   fbme::CgSettings cs;

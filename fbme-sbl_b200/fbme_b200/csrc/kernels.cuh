@@ -255,6 +255,23 @@ void cg_active_select(const float* gamma, long long N, int kmax, int min_size, f
 void cg_active_mask(const ActiveBufs& ab, long long N, int kmax, cudaStream_t st);
 void cg_active_posterior(const ActiveArgs& a, cudaStream_t st);
 
+// mode="dense": the exact posterior through the M x M data covariance in
+// FP64 (dense.cu).
+struct DenseBufs {
+  double2 *Q, *X;      // [B][M][M] Cholesky factor, then Q^-1 / L^-1 (column-major)
+  double2 *lag, *lsum; // [B][2M1-1][2M2-1] lags of the prior, lag sums of Q^-1
+  double2* pass;       // separable-transform pass buffer
+  double2* z;          // [B][M] Q^-1 y
+  double2* lift;       // [B][N] A^H Q^-1 y
+  double* dd;          // [B][N] diag(A^H Q^-1 A)
+  double2 *tw1, *tw2;  // FP64 twiddles of N1, N2
+};
+size_t dense_bytes(const BatchShape& s);
+DenseBufs dense_bind(uint8_t* w, const BatchShape& s, cudaStream_t st);
+void dense_posterior(const BatchShape& s, const DenseBufs& d, const float* gamma, const float* noise,
+                     const float2* y, float jitter, float2* mean, float* relc, float* pv_out, double* part, int nb,
+                     int* status, cudaStream_t st);
+
 // Shared by the C ABI translation units.
 int api_fail(int code, const std::string& msg);
 size_t dft_table_bytes(int L, int terms);

@@ -107,9 +107,13 @@ def fast_sbl(data: Any, grid_shape: Sequence[int], *, config: SBLConfig | None =
     mode = ("dense" if cfg.mode == "auto" and n_samples <= threshold
             else "cg" if cfg.mode == "auto" else cfg.mode)
     if mode == "dense":
-        raise NotImplementedError(
-            "dense exact mode (M x M Cholesky) is not built on the B200 path; use mode='uamp' "
-            "or mode='cg'")
+        if mask is not None:
+            raise NotImplementedError(
+                "observation masks run on the B200 uamp path (mode='uamp'); dense mode takes the full block")
+        if prod(sample) > 4096:
+            raise NotImplementedError("dense mode above 4096 samples is not built on the B200 path")
+        from .cg import cg_sbl  # noqa: PLC0415  (the EM loop of the cg plan, exact posterior)
+        return cg_sbl(tensor, grid, sample, batch_shape, cfg, device, dense=True)
     if mode == "cg":
         if mask is not None:
             raise NotImplementedError(

@@ -257,7 +257,8 @@ int fbme_topk_static(const float* scores, int64_t n, int32_t k, int32_t batch, i
 const char* fbme_topk_static_error(void);
 
 /* ------------------------------------------------------------------------
- * mode="cg": PCG + Hutchinson SBL for a batch of equally shaped scenes.
+ * mode="cg": PCG + Hutchinson SBL for a batch of equally shaped scenes
+ * (and mode="dense" with `dense` set: the same EM loop, exact posterior).
  *
  * Replaces (FBME-SBL v1.1):
  *   fbme_cg_solve     <-> torch_sbl/solver.py:925-2393 (fast_sbl) with
@@ -303,6 +304,10 @@ typedef struct {
   int32_t active_set_check_interval;
   int32_t active_set_min_size, active_set_max_size;  /* max <= 1024 */
   float active_set_tail_fraction;       /* in (0, 1) */
+  /* 1: mode="dense" (solver.py:2962-2990): the exact posterior through the
+   * M x M data covariance, in FP64, instead of PCG + Hutchinson (probes,
+   * cg_* and the active set unused); M <= 4096 */
+  int32_t dense;
 } FbmeCgConfig;
 
 /* Device outputs of fbme_cg_solve (shapes [B][N1][N2] / [B]). */

@@ -979,12 +979,60 @@ def project_relevance(prior, dd, n_samples, eps):
     return rel * scale[:, None]
 
 
-def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda"):
+def lag_index(op: PrefixOperator) -> np.ndarray:
+    """operators.py:191-205: flat grid index of the lag m - m' (mod N) of
+    every sample pair, [M, M]."""
+    c = op.sample_coordinates
+    lag = np.remainder(c[:, None, :] - c[None, :, :], np.array(op.grid))
+    return lag[..., 0] * op.grid[1] + lag[..., 1]
+
+
+def dense_posterior(y, prior, noise, op: PrefixOperator, *, chol_mode, chol_multiplier):
+    """solver.py:2962-2990 with 3025-3035: the exact posterior through the
+    data covariance Q = noise I + A diag(prior) A^H (operators.py:282-297,
+    built from the FFT of the prior at the sample lags), its Cholesky
+    factor, Q^-1 y and the data diagonal diag(A^H Q^-1 A) from the lag sums
+    of Q^-1 (operators.py:418-442).  Returns (mean, posterior variance,
+    data diagonal)."""
+    rd = op.rdtype
+    eps, tiny = _finfo(rd)
+    b, n, m = prior.shape[0], op.n_grid, op.n_samples
+    li = lag_index(op)
+    lags = np.fft.fft2(prior.reshape(b, *op.grid).astype(op.cdtype), axes=(1, 2)).reshape(b, n)
+    q = lags[:, li] + noise[:, None, None].astype(op.cdtype) * np.eye(m, dtype=op.cdtype)
+    chol = _stable_cholesky(q, tiny, eps, mode=chol_mode, multiplier=chol_multiplier,
+                            fallback=(1.0, 10.0, 100.0, 1000.0))
+    if chol is None:
+        raise RuntimeError("Data covariance is not numerically positive definite.")
+    eye = np.broadcast_to(np.eye(m, dtype=op.cdtype), (b, m, m))
+    rhs = np.concatenate([y[:, :, None], eye], axis=2)
+    fwd = _tri_solve(chol, rhs)
+    solved = _tri_solve(np.conj(np.swapaxes(chol, 1, 2)), fwd, upper=True)
+    q_inv_y, q_inv = solved[:, :, 0], solved[:, :, 1:]
+    lag_sums = np.zeros((b, n), op.cdtype)
+    for i in range(b):
+        np.add.at(lag_sums[i], li.reshape(-1), q_inv[i].reshape(-1))
+    dd = (rd(n) * np.fft.ifft2(lag_sums.reshape(b, *op.grid), axes=(1, 2))).real.reshape(b, n).astype(rd)
+    lifted = op.adjoint_flat(q_inv_y.astype(op.cdtype))
+    mean = (prior * lifted).astype(op.cdtype)
+    pv = np.maximum(prior - np.square(prior) * dd, rd(0.0)).astype(rd)
+    return mean, pv, dd
+
+
+def fast_sbl_dense(data, grid, cfg: OracleConfig, *, chol_mode="cuda"):
+    """``fast_sbl`` with ``mode="dense"`` (solver.py:925-2393, posterior
+    2962-2990): the cg EM loop with the exact posterior, ``damping`` alone
+    and ``min_iter`` as the minimum."""
+    return fast_sbl_cg(data, grid, cfg, chol_mode=chol_mode, dense=True)
+
+
+def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda", dense=False):
     """``fast_sbl`` with ``mode="cg"``.  A single scene with ``active_set``
     switches to the exact reduced posterior on the selected ARD set once the
     variance tail is small (solver.py:1316-1341, 3184-3216), after which the
     omitted prior variances stay fixed (1684-1693).  ``probes``: [B, M, Pmax]
-    (default: the reference's CPU Rademacher stream)."""
+    (default: the reference's CPU Rademacher stream).  ``dense``: mode="dense"
+    (fast_sbl_dense)."""
     data = np.asarray(data)
     cdtype = np.complex128 if data.dtype in (np.complex128, np.float64) else np.complex64
     single = data.ndim == 2
@@ -1009,15 +1057,16 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
     prior = np.maximum(prior, floor[:, None]).astype(rd)
     noise = (np.full(b, cfg.fixed_noise_variance, rd) if cfg.fixed_noise_variance is not None
              else np.maximum(rd(cfg.initial_noise_fraction) * dp, floor).astype(rd))
-    pmax = cg_probe_count(cfg, n, m)
-    if probes is None:
-        probes = rademacher_probes(b, m, pmax, cfg.seed)
-    probes = np.asarray(probes).astype(cdtype)
-    lifted_probes = op.adjoint(probes)
-    minimum = max(cfg.min_iter, cfg.cg_min_iter)
+    pmax = 0 if dense else cg_probe_count(cfg, n, m)
+    if not dense:
+        if probes is None:
+            probes = rademacher_probes(b, m, pmax, cfg.seed)
+        probes = np.asarray(probes).astype(cdtype)
+        lifted_probes = op.adjoint(probes)
+    minimum = cfg.min_iter if dense else max(cfg.min_iter, cfg.cg_min_iter)
     limit = cfg.max_iter
     conv = cfg.tol > 0.0 and minimum < limit
-    keep = rd(max(cfg.damping, cfg.cg_damping))
+    keep = rd(cfg.damping if dense else max(cfg.damping, cfg.cg_damping))
     prev_mean = np.zeros((b, n), cdtype)
     solution = None
     streak = 0
@@ -1039,7 +1088,7 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
 
     it = 0
     for it in range(1, limit + 1):
-        if (cfg.active_set and b == 1 and active is None and it >= cfg.active_set_start
+        if (not dense and cfg.active_set and b == 1 and active is None and it >= cfg.active_set_start
                 and (it - cfg.active_set_start) % cfg.active_set_check_interval == 0):
             active = select_active_indices(prior, cfg.active_set_min_size, cfg.active_set_max_size,
                                            cfg.active_set_tail_fraction)
@@ -1047,13 +1096,18 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
                 columns = op.fourier_columns(active).astype(cdtype)
                 gram = np.conj(np.swapaxes(columns, 1, 2)) @ columns
                 solution = None
-        count, tol_cg = cg_schedule(it, cfg, pmax)
-        tol_cg = max(tol_cg, 3.0 * float(eps) ** 0.5)
+        if dense:
+            mean, pv, dd = dense_posterior(y, prior, noise, op, chol_mode=chol_mode,
+                                           chol_multiplier=cfg.cuda_cholesky_jitter_multiplier)
+            cg_it = 0
+        else:
+            count, tol_cg = cg_schedule(it, cfg, pmax)
+            tol_cg = max(tol_cg, 3.0 * float(eps) ** 0.5)
         if active is not None:
             mean, pv, dd = reduced()
             cg_it = 0
-        rhs = np.concatenate([y[:, :, None], probes[:, :, :count]], axis=2)
-        if active is None:
+        if active is None and not dense:
+            rhs = np.concatenate([y[:, :, None], probes[:, :, :count]], axis=2)
             if cfg.cg_warm_start and solution is not None and solution.shape[2] != 1 + count:
                 rs = np.zeros((b, m, 1 + count), cdtype)
                 sh = min(1 + count, solution.shape[2])
@@ -1107,7 +1161,10 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
                 break
     # final posterior: all probes, or the reduced posterior after a switch
     # (solver.py:2023-2080)
-    if active is not None:
+    if dense:
+        mean, pv, dd = dense_posterior(y, prior, noise, op, chol_mode=chol_mode,
+                                       chol_multiplier=cfg.cuda_cholesky_jitter_multiplier)
+    elif active is not None:
         mean, pv, dd = reduced()
     else:
         rhs = np.concatenate([y[:, :, None], probes], axis=2)
@@ -1127,7 +1184,8 @@ def fast_sbl_cg(data, grid, cfg: OracleConfig, *, probes=None, chol_mode="cuda")
     shape = tuple(grid)
     out = dict(x=mean.reshape((b,) + shape), posterior_variance=pv.reshape((b,) + shape),
                precision=(rd(1.0) / prior).reshape((b,) + shape), noise_variance=noise,
-               effective_dof=dof.astype(rd), iterations=it, converged=converged, mode="cg",
+               effective_dof=dof.astype(rd), iterations=it, converged=converged,
+               mode="dense" if dense else "cg",
                history=hist, relative_change=hist["relative_change"][-1],
                active_set_size=0 if active is None else int(active.shape[1]),
                active_indices=None if active is None else active[0])

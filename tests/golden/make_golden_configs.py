@@ -24,6 +24,8 @@ make_golden.py does):
   make_golden_cg.py).
 * ``cg/cg_active_c1_s0_it44``: one C1 scene through sbl_2d with mode="cg"
   and the default active-set switch, 44 iterations (make_cg_active).
+* ``dense/dense_c1_s{0,1}_it30``: C1 scenes through sbl_2d with
+  mode="dense", 30 iterations (make_dense).
 
 The observations are not stored: the tests regenerate them with the
 committed scene generator (numpy PCG64 streams, the same on every machine)
@@ -317,6 +319,48 @@ def make_cg_c2(seed: int, max_iter: int) -> None:
     print("wrote", name)
 
 
+def make_dense(config: str, seed: int, max_iter: int) -> None:
+    """A single scene through the reference's ``sbl_2d`` with
+    ``mode="dense"`` (the exact posterior through the M x M data covariance,
+    solver.py:2962-2990; what ``mode="auto"`` picks for M <= 2048), ``tol=0``,
+    CUDA Cholesky loading; FP64 and FP32 runs in the cg fixture format."""
+    import numpy as np
+
+    torch, scenes, SBLConfig, fast_sbl = _import()
+    import torch_sbl.solver as S  # reference package
+
+    S._stable_cholesky_raw = _cuda_cholesky_branch(S, torch)
+    sc = scenes.config_scene(config, seed)
+    out = {"y": sc.y[None], "grid": np.array(sc.grid), "seeds": np.array([seed]),
+           "max_iter": np.array(max_iter), "x_true": sc.x[None].astype(np.complex64),
+           "cholesky": np.array("cuda"), "mode": np.array("dense")}
+    runs = {}
+    for tag, dtype in (("f64", np.complex128), ("f32", np.complex64)):
+        cfg = SBLConfig(mode="dense", max_iter=max_iter, tol=0.0, device="cpu", return_history=True)
+        r = S.sbl_2d(torch.from_numpy(sc.y.astype(dtype)), sc.grid, config=cfg)
+        assert r.mode == "dense"
+        runs[tag] = r
+        out[tag + "_x"] = r.x.numpy().astype(np.complex64)[None]
+        out[tag + "_posterior_variance"] = r.posterior_variance.numpy().astype(np.float32)[None]
+        out[tag + "_precision"] = r.precision.numpy().astype(np.float32)[None]
+        out[tag + "_noise_variance"] = np.atleast_1d(r.noise_variance.numpy())
+        out[tag + "_effective_dof"] = np.atleast_1d(r.effective_dof.numpy())
+        out[tag + "_iterations"] = np.array(r.iterations)
+        for key in ("relative_change", "noise_variance", "effective_dof"):
+            out[tag + "_history_" + key] = np.array(r.history[key])
+
+    def gap(a, b):
+        a, b = np.asarray(a, np.complex128).ravel(), np.asarray(b, np.complex128).ravel()
+        return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+    for f in ("x", "posterior_variance", "precision"):
+        out["gap_" + f] = np.array(gap(getattr(runs["f32"], f).numpy(), getattr(runs["f64"], f).numpy()))
+    (HERE / "dense").mkdir(exist_ok=True)
+    name = f"dense_{config}_s{seed}_it{max_iter}"
+    np.savez_compressed(HERE / "dense" / f"{name}.npz", **out)
+    print("wrote", name, "gaps", out["gap_x"], out["gap_posterior_variance"])
+
+
 def make_cg_active(config: str, seed: int, max_iter: int) -> None:
     """A single scene through the reference's ``sbl_2d`` with ``mode="cg"``
     and its default active-set switch (solver.py:1316-1341: from iteration
@@ -365,7 +409,8 @@ def make_cg_active(config: str, seed: int, max_iter: int) -> None:
 
 JOBS = [("c3", "0"), ("c3", "1"), ("c3", "2"), ("c4", "0"), ("cg_c2", "0", "6"),
         ("masked", "c1", "0", "random"), ("masked", "c1", "1", "ellipse"), ("masked", "c2", "0", "random"),
-        ("masked", "c2", "1", "ellipse"), ("cg_active", "c1", "0", "44")]
+        ("masked", "c2", "1", "ellipse"), ("cg_active", "c1", "0", "44"),
+        ("dense", "c1", "0", "30"), ("dense", "c1", "1", "30")]
 
 
 def main() -> None:
@@ -373,8 +418,9 @@ def main() -> None:
         if sys.argv[1] == "masked":
             make_masked(sys.argv[2], int(sys.argv[3]), sys.argv[4])
             return
-        if sys.argv[1] == "cg_active":
-            make_cg_active(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]))
+        if sys.argv[1] in ("cg_active", "dense"):
+            {"cg_active": make_cg_active, "dense": make_dense}[sys.argv[1]](
+                sys.argv[2], int(sys.argv[3]), int(sys.argv[4]))
             return
         kind, args = sys.argv[1], [int(v) for v in sys.argv[2:]]
         {"c3": make_c3, "c4": make_c4, "cg_c2": make_cg_c2}[kind](*args)

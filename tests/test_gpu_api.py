@@ -90,6 +90,7 @@ def test_unbuilt_modes_raise():
     need_gpu()
     from torch_sbl import SBLConfig, sbl_2d
 
-    y = torch.zeros(32, 32, dtype=torch.complex64, device="cuda")
+    # dense mode is built up to 4096 samples
+    y = torch.zeros(128, 64, dtype=torch.complex64, device="cuda")
     with pytest.raises(NotImplementedError):
-        sbl_2d(y, (64, 64), config=SBLConfig(mode="dense", device="cuda"))
+        sbl_2d(y, (256, 256), config=SBLConfig(mode="dense", device="cuda"))

@@ -219,6 +219,44 @@ def test_cg_active_set_switch_matches_reference_golden(path):
     assert int(res.status.abs().sum()) == 0
 
 
+DENSE = sorted(glob.glob(str(Path(__file__).parent / "golden" / "dense" / "dense_*.npz")))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", DENSE, ids=lambda p: Path(p).stem)
+def test_dense_mode_matches_reference_golden(path):
+    """mode="dense" through sbl_2d against the reference's FP64 run: the
+    device solves the data covariance in FP64 with the FP64 loading (the
+    prior and the EM updates stay FP32 between iterations), so x, the
+    precision, noise and DOF stay within a tenth of the reference's own
+    FP32-FP64 gap, and the posterior variance, which the reference's FP32
+    run loses to cancellation, matches its FP64 run."""
+    need_gpu()
+    from torch_sbl import SBLConfig, sbl_2d
+
+    g = np.load(path)
+    grid = tuple(int(v) for v in g["grid"])
+    y = torch.from_numpy(g["y"][0]).cuda()
+    res = sbl_2d(y, grid, config=SBLConfig(mode="dense", max_iter=int(g["max_iter"]), tol=0.0))
+    assert res.mode == "dense" and res.iterations == int(g["f64_iterations"])
+    ex = rel_l2(res.x.cpu().numpy(), g["f64_x"][0])
+    epr = rel_l2(res.precision.cpu().numpy(), g["f64_precision"][0])
+    epv = rel_l2(res.posterior_variance.cpu().numpy(), g["f64_posterior_variance"][0])
+    print(f"{Path(path).stem}: x {ex:.2e} (ref FP32 gap {float(g['gap_x']):.2e}) precision {epr:.2e} "
+          f"(gap {float(g['gap_precision']):.2e}) pv {epv:.2e} (gap {float(g['gap_posterior_variance']):.2e})")
+    # the prior and the EM updates are FP32 between iterations: a tenth of
+    # the reference's own FP32-FP64 gap
+    assert ex < 0.1 * float(g["gap_x"])
+    assert epr < 0.1 * float(g["gap_precision"])
+    assert epv < 1e-3
+    for f in ("noise_variance", "effective_dof"):
+        ref64, ref32 = float(g["f64_" + f][0]), float(g["f32_" + f][0])
+        got = float(getattr(res, f))
+        print(f"  {f}: {got:.9g} (FP64 {ref64:.9g}, FP32 {ref32:.9g})")
+        assert abs(got - ref64) <= 0.1 * abs(ref32 - ref64) + 1e-6 * abs(ref64)
+    assert int(res.status.abs().sum()) == 0
+
+
 @pytest.mark.gpu
 def test_cg_batch_equals_single_scene_solves():
     need_gpu()

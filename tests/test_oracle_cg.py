@@ -64,6 +64,26 @@ def test_cg_active_set_switch_matches_reference(path):
         np.testing.assert_allclose(r["effective_dof"], g[tag + "_effective_dof"][0], rtol=1e2 * bar)
 
 
+DENSE = sorted(glob.glob(str(Path(__file__).parent / "golden" / "dense" / "dense_*.npz")))
+
+
+@pytest.mark.parametrize("path", DENSE, ids=lambda p: Path(p).stem)
+def test_dense_oracle_matches_reference_fp64(path):
+    """mode="dense" (the exact posterior through the M x M data covariance)
+    restated in FP64 reproduces the reference's FP64 run."""
+    g = np.load(path)
+    grid = tuple(int(v) for v in g["grid"])
+    cfg = O.OracleConfig(mode="dense", max_iter=int(g["max_iter"]), tol=0.0)
+    r = O.fast_sbl_dense(g["y"][0].astype(np.complex128), grid, cfg)
+    assert r["mode"] == "dense"
+    assert _rel(r["x"], g["f64_x"]) < 1e-6
+    assert _rel(r["precision"], g["f64_precision"]) < 1e-6
+    assert _rel(r["posterior_variance"], g["f64_posterior_variance"]) < 1e-5
+    np.testing.assert_allclose(r["noise_variance"], g["f64_noise_variance"][0], rtol=1e-7)
+    np.testing.assert_allclose(r["effective_dof"], g["f64_effective_dof"][0], rtol=1e-7)
+    np.testing.assert_allclose(r["history"]["relative_change"], g["f64_history_relative_change"], rtol=1e-5)
+
+
 def test_active_set_selection_rule():
     """solver.py:3184-3216 on hand-made priors: no switch while the tail
     holds more than the fraction, the smallest prefix reaching 1 - tail
