@@ -130,39 +130,86 @@ __global__ void dense_build_q_kernel(const double2* lag, int B, int m1, int m2, 
   }
 }
 
-// Factor columns [k, k + kPanel) of Q (rows k..M-1), whose trailing part
-// is up to date.  One CTA per scene.  status: FBME_STATUS_CHOLESKY on a
-// non-positive pivot (replaced by the smallest normal double).
-__global__ void __launch_bounds__(256) dense_panel_chol_kernel(double2* Q, int M, int k, int* status) {
-  __shared__ double s_piv;
+
+// The diagonal block [k, k + 32) of the Cholesky factor, in shared memory:
+// one warp per scene, lane i owning row i of the block.
+__global__ void __launch_bounds__(32) dense_diag_chol_kernel(double2* Q, int M, int k, int* status) {
+  __shared__ double2 D[kPanel][kPanel + 1];
   double2* A = Q + static_cast<long long>(blockIdx.x) * M * M;
-  const int end = k + kPanel < M ? k + kPanel : M;
-  for (int c = k; c < end; ++c) {
-    if (threadIdx.x == 0) {
-      double d = A[static_cast<long long>(c) * M + c].x;
-      if (!(d > 0.0)) {
-        if (status) atomicOr(status + blockIdx.x, isfinite(d) ? FBME_STATUS_CHOLESKY : FBME_STATUS_NONFINITE);
-        d = 2.2250738585072014e-308;
-      }
-      s_piv = sqrt(d);
-      A[static_cast<long long>(c) * M + c] = make_double2(s_piv, 0.0);
+  const int nb = M - k < kPanel ? M - k : kPanel, lane = threadIdx.x;
+  for (int c = 0; c < nb; ++c)
+    if (lane < nb && lane >= c) D[lane][c] = A[static_cast<long long>(k + c) * M + k + lane];
+  __syncwarp();
+  for (int c = 0; c < nb; ++c) {
+    double d = D[c][c].x;
+    if (!(d > 0.0)) {
+      if (lane == 0 && status)
+        atomicOr(status + blockIdx.x, isfinite(d) ? FBME_STATUS_CHOLESKY : FBME_STATUS_NONFINITE);
+      d = 2.2250738585072014e-308;
     }
-    __syncthreads();
-    const double piv = s_piv;
-    double2* col = A + static_cast<long long>(c) * M;
-    for (int i = c + 1 + threadIdx.x; i < M; i += blockDim.x) col[i] = make_double2(col[i].x / piv, col[i].y / piv);
-    __syncthreads();
-    // the rest of the panel: A[i][c'] -= A[i][c] conj(A[c'][c]), i >= c'
-    for (int cp = c + 1; cp < end; ++cp) {
-      const double2 bc = col[cp];
-      double2* dst = A + static_cast<long long>(cp) * M;
-      for (int i = cp + threadIdx.x; i < M; i += blockDim.x) {
-        const double2 v = zmulc(col[i], bc);
-        dst[i] = make_double2(dst[i].x - v.x, dst[i].y - v.y);
+    const double piv = sqrt(d);
+    __syncwarp();
+    if (lane > c && lane < nb) D[lane][c] = make_double2(D[lane][c].x / piv, D[lane][c].y / piv);
+    if (lane == c) D[c][c] = make_double2(piv, 0.0);
+    __syncwarp();
+    if (lane > c && lane < nb) {
+      const double2 li = D[lane][c];
+      for (int j = c + 1; j <= lane; ++j) {
+        const double2 v = zmulc(li, D[j][c]);
+        D[lane][j] = make_double2(D[lane][j].x - v.x, D[lane][j].y - v.y);
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
+  for (int c = 0; c < nb; ++c)
+    if (lane < nb && lane >= c) A[static_cast<long long>(k + c) * M + k + lane] = D[lane][c];
+}
+
+// The panel below the diagonal block: L21 = A21 L11^-H, one warp per row r
+// (lane c holding column k + c), forward over the block's columns.
+__global__ void __launch_bounds__(256) dense_panel_trsm_kernel(double2* Q, int M, int k) {
+  double2* A = Q + static_cast<long long>(blockIdx.y) * M * M;
+  const int r = k + kPanel + blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (r >= M) return;  // whole warps: r is uniform in a warp
+  double2 a = A[static_cast<long long>(k + lane) * M + r];
+  for (int c = 0; c < kPanel; ++c) {
+    if (lane == c) {
+      const double piv = A[static_cast<long long>(k + c) * M + k + c].x;
+      a = make_double2(a.x / piv, a.y / piv);
+    }
+    const double2 x = make_double2(__shfl_sync(0xffffffffu, a.x, c), __shfl_sync(0xffffffffu, a.y, c));
+    if (lane > c) {
+      const double2 v = zmulc(x, A[static_cast<long long>(k + c) * M + k + lane]);  // x conj(L11[lane][c])
+      a = make_double2(a.x - v.x, a.y - v.y);
+    }
+  }
+  A[static_cast<long long>(k + lane) * M + r] = a;
+}
+
+// Rows [k, k + 32) of X = L^-1, forward substitution within the diagonal
+// block: one warp per column j < k + 32, lane i holding row k + i.
+__global__ void __launch_bounds__(256) dense_inv_panel_kernel(const double2* L, double2* X, int M, int k) {
+  const long long MM = static_cast<long long>(M) * M;
+  const double2* Lb = L + blockIdx.y * MM;
+  double2* Xb = X + blockIdx.y * MM;
+  const int nb = M - k < kPanel ? M - k : kPanel;
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (j >= k + nb) return;
+  const int row = k + lane;
+  const bool own = lane < nb && row >= j;  // X is lower triangular
+  double2 v = own ? Xb[static_cast<long long>(j) * M + row] : make_double2(0.0, 0.0);
+  for (int c = 0; c < nb; ++c) {
+    if (lane == c) {
+      const double piv = Lb[static_cast<long long>(k + c) * M + k + c].x;
+      v = make_double2(v.x / piv, v.y / piv);
+    }
+    const double2 x = make_double2(__shfl_sync(0xffffffffu, v.x, c), __shfl_sync(0xffffffffu, v.y, c));
+    if (lane > c && lane < nb) {
+      const double2 p = zmul(Lb[static_cast<long long>(k + c) * M + row], x);
+      v = make_double2(v.x - p.x, v.y - p.y);
+    }
+  }
+  if (own) Xb[static_cast<long long>(j) * M + row] = v;
 }
 
 // Tile updates over 64 x 64 output tiles (grid: tiles x scenes), depth in
@@ -173,7 +220,7 @@ __global__ void __launch_bounds__(256) dense_panel_chol_kernel(double2* Q, int M
 //           Q[i][j] -= sum_{c in [k0, k1)} Q[i][c] conj(Q[j][c])
 //   MODE 1  inverse update, rows [k1, M) x columns [0, k1):
 //           X[i][j] -= sum_{c in [k0, k1)} L[i][c] X[c][j]
-//   MODE 2  R = X^H X, lower tiles of [0, M):
+//   MODE 2  R = X^H X, lower tiles of [0, M), stored in both triangles:
 //           R[i][j] = sum_{r >= i0} conj(X[r][i]) X[r][j]
 template <int MODE>
 __global__ void __launch_bounds__(256) dense_tile_kernel(double2* C, const double2* A, const double2* Xm, int M,
@@ -275,8 +322,9 @@ __global__ void __launch_bounds__(256) dense_tile_kernel(double2* C, const doubl
       const int i = i0 + ri + 16 * a;
       if (i >= M || (MODE != 1 && i < j)) continue;
       double2* dst = C + static_cast<long long>(j) * M + i;
-      if (MODE == 2) {
+      if (MODE == 2) {  // R is stored in full (both triangles)
         *dst = acc[a][b];
+        if (i != j) C[static_cast<long long>(i) * M + j] = make_double2(acc[a][b].x, -acc[a][b].y);
       } else {
         *dst = make_double2(dst->x - acc[a][b].x, dst->y - acc[a][b].y);
       }
@@ -295,71 +343,60 @@ __global__ void dense_identity_kernel(double2* X, int B, int M) {
   }
 }
 
-// Rows [k, k + kPanel) of X = L^-1: forward substitution within the
-// diagonal block, for every column j < k + kPanel (the rows' earlier terms
-// came from the tile updates).  One CTA per scene, a thread per column.
-__global__ void __launch_bounds__(256) dense_panel_inv_kernel(const double2* L, double2* X, int M, int k) {
-  const long long MM = static_cast<long long>(M) * M;
-  const double2* Lb = L + blockIdx.x * MM;
-  double2* Xb = X + blockIdx.x * MM;
-  const int end = k + kPanel < M ? k + kPanel : M;
-  for (int j = threadIdx.x; j < end; j += blockDim.x) {
-    double2* col = Xb + static_cast<long long>(j) * M;
-    const int r0 = j > k ? j : k;
-    for (int r = r0; r < end; ++r) {
-      double2 v = col[r];
-      for (int c = r0; c < r; ++c) {
-        const double2 p = zmul(Lb[static_cast<long long>(c) * M + r], col[c]);
-        v = make_double2(v.x - p.x, v.y - p.y);
-      }
-      const double piv = Lb[static_cast<long long>(r) * M + r].x;
-      col[r] = make_double2(v.x / piv, v.y / piv);
-    }
-  }
+
+__device__ __forceinline__ double2 warp_sum2(double2 v) {
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  return v;
 }
 
-// R (Hermitian, lower part stored) entry (i, j)
-__device__ __forceinline__ double2 herm_at(const double2* R, int M, int i, int j) {
-  if (i >= j) return R[static_cast<long long>(j) * M + i];
-  const double2 v = R[static_cast<long long>(i) * M + j];
-  return make_double2(v.x, -v.y);
-}
-
-// z = Q^-1 y (y complex64 [B][M])
-__global__ void dense_qinv_y_kernel(const double2* R, const float2* y, int B, int M, double2* z) {
+// z = Q^-1 y (y complex64 [B][M]): one warp per row i, over column i of the
+// Hermitian R (z_i = sum_j conj(R[j][i]) y_j), coalesced.
+__global__ void __launch_bounds__(256) dense_qinv_y_kernel(const double2* R, const float2* y, int B, int M,
+                                                            double2* z) {
   const int b = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (i >= M) return;
-  const double2* Rb = R + static_cast<long long>(b) * M * M;
+  const double2* col = R + static_cast<long long>(b) * M * M + static_cast<long long>(i) * M;
   const float2* yb = y + static_cast<long long>(b) * M;
   double2 acc = make_double2(0.0, 0.0);
-  for (int j = 0; j < M; ++j) {
+  for (int j = lane; j < M; j += 32) {
+    const double2 r = col[j];
     const float2 v = yb[j];
-    acc = zadd(acc, zmul(herm_at(Rb, M, i, j), make_double2(v.x, v.y)));
+    acc.x += r.x * v.x + r.y * v.y;  // conj(r) * v
+    acc.y += r.x * v.y - r.y * v.x;
   }
-  z[static_cast<long long>(b) * M + i] = acc;
+  acc = warp_sum2(acc);
+  if (lane == 0) z[static_cast<long long>(b) * M + i] = acc;
 }
 
 // Lag sums of Q^-1 (operators.py:427-435): S[e1][e2] = sum of R[i][j] over
-// the sample pairs with m_i - m_j = (e1 - (M1-1), e2 - (M2-1)).
-__global__ void dense_lag_sum_kernel(const double2* R, int B, int m1, int m2, double2* S) {
+// the sample pairs with m_i - m_j = (e1 - (M1-1), e2 - (M2-1)); one warp
+// per lag, lanes over the pairs in a fixed order.
+__global__ void __launch_bounds__(256) dense_lag_sum_kernel(const double2* R, int B, int m1, int m2,
+                                                             double2* S) {
   const int M = m1 * m2, W1 = 2 * m1 - 1, W2 = 2 * m2 - 1;
   const long long total = static_cast<long long>(B) * W1 * W2;
-  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
-       t += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int e2 = static_cast<int>(t % W2);
-    const long long r = t / W2;
-    const int e1 = static_cast<int>(r % W1), b = static_cast<int>(r / W1);
-    const int d1 = e1 - (m1 - 1), d2 = e2 - (m2 - 1);
-    const double2* Rb = R + static_cast<long long>(b) * M * M;
-    double2 acc = make_double2(0.0, 0.0);
-    const int a1lo = d1 > 0 ? d1 : 0, a1hi = d1 < 0 ? m1 + d1 : m1;
-    const int a2lo = d2 > 0 ? d2 : 0, a2hi = d2 < 0 ? m2 + d2 : m2;
-    for (int a1 = a1lo; a1 < a1hi; ++a1)
-      for (int a2 = a2lo; a2 < a2hi; ++a2)
-        acc = zadd(acc, herm_at(Rb, M, a1 * m2 + a2, (a1 - d1) * m2 + (a2 - d2)));
-    S[t] = acc;
+  const long long t = blockIdx.x * 8LL + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= total) return;
+  const int e2 = static_cast<int>(t % W2);
+  const long long r = t / W2;
+  const int e1 = static_cast<int>(r % W1), b = static_cast<int>(r / W1);
+  const int d1 = e1 - (m1 - 1), d2 = e2 - (m2 - 1);
+  const double2* Rb = R + static_cast<long long>(b) * M * M;
+  const int a1lo = d1 > 0 ? d1 : 0, a1hi = d1 < 0 ? m1 + d1 : m1;
+  const int a2lo = d2 > 0 ? d2 : 0, a2hi = d2 < 0 ? m2 + d2 : m2;
+  const int w = a2hi - a2lo, cnt = (a1hi - a1lo) * w;
+  const int shift = d1 * m2 + d2;  // j = i - shift
+  double2 acc = make_double2(0.0, 0.0);
+  for (int u = lane; u < cnt; u += 32) {
+    const int a1 = a1lo + u / w, a2 = a2lo + u % w;
+    const int i = a1 * m2 + a2;
+    acc = zadd(acc, Rb[static_cast<long long>(i - shift) * M + i]);
   }
+  acc = warp_sum2(acc);
+  if (lane == 0) S[t] = acc;
 }
 
 // Inverse-sign separable transform of a W1 x W2 rectangle of frequencies
@@ -512,9 +549,10 @@ void dense_posterior(const BatchShape& s, const DenseBufs& d, const float* gamma
   dense_build_q_kernel<<<grid_of(1LL * B * M * M), 256, 0, st>>>(d.lag, B, m1, m2, noise, jitter, d.Q);
   // Cholesky
   for (int k = 0; k < M; k += kPanel) {
-    dense_panel_chol_kernel<<<B, 256, 0, st>>>(d.Q, M, k, status);
+    dense_diag_chol_kernel<<<B, 32, 0, st>>>(d.Q, M, k, status);
     const int k1 = k + kPanel;
     if (k1 < M) {
+      dense_panel_trsm_kernel<<<dim3((M - k1 + 7) / 8, B), 256, 0, st>>>(d.Q, M, k);
       const int T = (M - k1 + kTile - 1) / kTile;
       dense_tile_kernel<0><<<dim3(T * (T + 1) / 2, B), 256, 0, st>>>(d.Q, d.Q, nullptr, M, k, k1);
     }
@@ -522,7 +560,7 @@ void dense_posterior(const BatchShape& s, const DenseBufs& d, const float* gamma
   // X = L^-1
   dense_identity_kernel<<<grid_of(1LL * B * M * M), 256, 0, st>>>(d.X, B, M);
   for (int k = 0; k < M; k += kPanel) {
-    dense_panel_inv_kernel<<<B, 256, 0, st>>>(d.Q, d.X, M, k);
+    dense_inv_panel_kernel<<<dim3((std::min(k + kPanel, M) + 7) / 8, B), 256, 0, st>>>(d.Q, d.X, M, k);
     const int k1 = k + kPanel;
     if (k1 < M) {
       const int TI = (M - k1 + kTile - 1) / kTile, TJ = (k1 + kTile - 1) / kTile;
@@ -534,10 +572,10 @@ void dense_posterior(const BatchShape& s, const DenseBufs& d, const float* gamma
     const int T = (M + kTile - 1) / kTile;
     dense_tile_kernel<2><<<dim3(T * (T + 1) / 2, B), 256, 0, st>>>(d.Q, d.Q, d.X, M, 0, 0);
   }
-  dense_qinv_y_kernel<<<dim3((M + 255) / 256, B), 256, 0, st>>>(d.Q, y, B, M, d.z);
+  dense_qinv_y_kernel<<<dim3((M + 7) / 8, B), 256, 0, st>>>(d.Q, y, B, M, d.z);
   dense_energy_kernel<<<B, 256, 0, st>>>(d.z, d.lag, noise, jitter, m1, m2, part);
   // data diagonal: Re N ifft2 of the lag sums
-  dense_lag_sum_kernel<<<grid_of(1LL * B * W1 * W2), 256, 0, st>>>(d.Q, B, m1, m2, d.lsum);
+  dense_lag_sum_kernel<<<static_cast<int>((1LL * B * W1 * W2 + 7) / 8), 256, 0, st>>>(d.Q, B, m1, m2, d.lsum);
   dense_inv1_kernel<<<grid_of(1LL * B * W1 * n2), 256, 0, st>>>(d.lsum, B, W1, W2, -(m2 - 1), n2, d.tw2, d.pass);
   dense_inv2_kernel<true><<<grid_of(1LL * B * n1 * n2), 256, 0, st>>>(d.pass, B, W1, -(m1 - 1), n1, n2, d.tw1,
                                                                          nullptr, d.dd);
