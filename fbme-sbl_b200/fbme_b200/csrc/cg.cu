@@ -42,6 +42,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "dft_umma.cuh"
@@ -90,6 +91,7 @@ struct CgArgs {
   float* best_rel;
   int* any_active;
   float tol;
+  const float* tol_dev;  // the tolerance in device memory (graph-resident loops), else nullptr
   int fixed;
 };
 
@@ -535,12 +537,13 @@ __global__ void __launch_bounds__(256) cg_finish_kernel(const __grid_constant__ 
   bb = warp_sum(bb);
   if (lane != 0) return;
   const double tiny = static_cast<double>(kTiny);
+  const float tol = A.tol_dev ? *A.tol_dev : A.tol;
   if (mode == kFinishInit) {
     // solver.py:5620-5639
     const float inorm = fmaxf(static_cast<float>(sqrt(bb)), kEps);
     A.init_norm[unit] = inorm;
     const float rn = static_cast<float>(sqrt(rr));
-    const int act = rn > A.tol * inorm ? 1 : 0;
+    const int act = rn > tol * inorm ? 1 : 0;
     A.active[unit] = act;
     A.dmask[unit] = act;
     A.beta[unit] = 0.f;
@@ -559,7 +562,7 @@ __global__ void __launch_bounds__(256) cg_finish_kernel(const __grid_constant__ 
     // solver.py:5667-5707
     const float rl = static_cast<float>(sqrt(rr)) / A.init_norm[unit];
     A.rel[unit] = rl;
-    int act = (isfinite(rl) && rl > A.tol) ? 1 : 0;
+    int act = (isfinite(rl) && rl > tol) ? 1 : 0;
     if (A.fixed) {
       act = act && A.valid[unit];
       const int imp = rl < A.best_rel[unit];
@@ -814,6 +817,7 @@ struct CgScalarArgs {
   float keep, fixed_noise, noise_shape, noise_rate;
   int evidence;
   int cg_iters, probes;
+  const int* cg_iters_dev;  // PCG iterations counted on the device (graph-resident loop), else nullptr
   float cg_tol;
   int update;        // 0: final pass (DOF only)
 };
@@ -881,7 +885,7 @@ __global__ void __launch_bounds__(256) cg_scalars_kernel(const __grid_constant__
     A.hist[0] = static_cast<float>(cmax);
     A.hist[1] = static_cast<float>(ns / A.s.B);
     A.hist[2] = static_cast<float>(ds / A.s.B);
-    A.hist[3] = static_cast<float>(A.cg_iters);
+    A.hist[3] = static_cast<float>(A.cg_iters_dev ? *A.cg_iters_dev : A.cg_iters);
     A.hist[4] = static_cast<float>(A.probes);
     A.hist[5] = A.cg_tol;
   }
@@ -1013,10 +1017,22 @@ class CgEngine {
   void precondition(const CgArgs& A, cudaStream_t st);
   dim3 vec_grid(int R) const;
   int pcg(int R, float tol, bool warm, cudaStream_t st);
+  ~CgEngine();
   // operator inputs of the next matvec / PCG solve
   const float* prior = nullptr;
   const float* noise = nullptr;
   int* host_flag = nullptr;  // pinned int for the restart test
+  // Graph-resident PCG loop: the restart test runs on the device and a
+  // graph WHILE node repeats chunks of check_interval iterations while any
+  // right-hand side is active (an IF node runs the rest up to max_cg_iter);
+  // pcg() then returns -1 and the iteration count stays in it_dev.
+  bool graph_loop = false;
+  float* tol_dev = nullptr;
+  int* it_dev = nullptr;
+  void pcg_iteration(int R, float tol, bool check, cudaStream_t st);
+  cudaGraphExec_t loop_graph(int R);
+  std::map<int, cudaGraphExec_t> loops;
+  bool dev_tol = false;  // args() hands the kernels tol_dev
   BatchShape s;
   CgSettings c;
   DftTables t;
@@ -1179,6 +1195,7 @@ CgArgs CgEngine::args(int R, float tol) const {
   A.best_rel = buf.best_rel;
   A.any_active = buf.any_active;
   A.tol = tol;
+  A.tol_dev = dev_tol ? tol_dev : nullptr;
   A.fixed = c.fixed_iterations > 0;
   return A;
 }
@@ -1234,8 +1251,148 @@ void CgEngine::precondition(const CgArgs& A, cudaStream_t st) {
 
 static const int kVecSmem = (kCgSlice * kFsLd + kCgChunk * kCgSlice) * static_cast<int>(sizeof(float2));
 
+// Device side of the graph-resident PCG loop.
+__global__ void cg_loop_init_kernel(float* tol_dev, float tol, int* it_dev) {
+  *tol_dev = tol;
+  *it_dev = 0;
+}
+// End of a chunk of `chunk` iterations (the last one a restart check):
+// repeat while a right-hand side is active and a whole chunk still fits.
+__global__ void cg_loop_cond_kernel(cudaGraphConditionalHandle h, const int* any_active, int* it_dev, int chunk,
+                                    int limit) {
+  const int it = *it_dev + chunk;
+  *it_dev = it;
+  cudaGraphSetConditional(h, (*any_active && it + chunk <= limit) ? 1u : 0u);
+}
+// After the chunks: the rest up to the limit, if still active.
+__global__ void cg_tail_cond_kernel(cudaGraphConditionalHandle h, const int* any_active, const int* it_dev,
+                                    int limit) {
+  cudaGraphSetConditional(h, (*any_active && *it_dev < limit) ? 1u : 0u);
+}
+__global__ void cg_add_kernel(int* it_dev, int n) { *it_dev += n; }
+
+// One PCG iteration (solver.py:5641-5721): the matvec along the direction,
+// then either the plain step or, with `check`, the update, the residual
+// recomputation and the restart test (any_active set by the finish kernel).
+void CgEngine::pcg_iteration(int R, float tol, bool check, cudaStream_t st) {
+  const int units = s.B * R;
+  const int fin_blocks = (units + 7) / 8;
+  matvec(R, nullptr, true, buf.q, false, st);
+  CgArgs A = args(R, tol);
+  if (!check) {
+    cg_vector_kernel<true, true, false><<<vec_grid(R), kCgThreads, kVecSmem, st>>>(A);
+    precondition(A, st);
+    cg_finish_kernel<<<fin_blocks, 256, 0, st>>>(A, kFinishStep);
+    return;
+  }
+  cg_vector_kernel<true, false, false><<<vec_grid(R), kCgThreads, 0, st>>>(A);
+  matvec(R, buf.x, false, nullptr, true, st);
+  A = args(R, tol);
+  cudaMemsetAsync(buf.any_active, 0, sizeof(int), st);
+  cg_vector_kernel<false, true, true><<<vec_grid(R), kCgThreads, kVecSmem, st>>>(A);
+  precondition(A, st);
+  cg_finish_kernel<<<fin_blocks, 256, 0, st>>>(A, kFinishRestart);
+  if (c.fixed_iterations > 0) {
+    const long long UM = static_cast<long long>(s.B) * R * s.m();
+    cg_best_kernel<<<grid_for(UM), 256, 0, st>>>(s, R, buf.improved, buf.x, buf.best);
+  }
+}
+
+// The loop of pcg() as a CUDA graph, for R right-hand sides: a WHILE node
+// over chunks of check_interval iterations whose last kernel sets the
+// condition from the device's restart test, then an IF node with the
+// remaining max_cg_iter % check_interval iterations.  The tolerance is read
+// from tol_dev, the count left in it_dev.  Chunks of an even length end on
+// the direction buffer they started on.  nullptr if the graph cannot be
+// built (the host loop runs instead).
+cudaGraphExec_t CgEngine::loop_graph(int R) {
+  auto found = loops.find(R);
+  if (found != loops.end()) return found->second;
+  const int interval = c.check_interval, limit = c.max_cg_iter, tail = limit % interval;
+  cudaGraph_t g = nullptr;
+  cudaStream_t cs = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const int saved = dcur;
+  const bool saved_dev = dev_tol;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
+  cudaGraphConditionalHandle hw{};
+  cudaGraphNodeParams wp{};
+  cudaGraphNode_t wn{};
+  if (ok) {
+    ok = cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    ok = ok && cudaGraphAddNode(&wn, g, nullptr, 0, &wp) == cudaSuccess;
+  }
+  dev_tol = true;
+  if (ok) {
+    ok = cudaStreamBeginCaptureToGraph(cs, wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed) == cudaSuccess;
+    if (ok) {
+      dcur = 0;
+      for (int j = 1; j <= interval; ++j) pcg_iteration(R, 0.f, j == interval, cs);
+      cg_loop_cond_kernel<<<1, 1, 0, cs>>>(hw, buf.any_active, it_dev, interval, limit);
+      cudaGraph_t body = nullptr;
+      ok = cudaStreamEndCapture(cs, &body) == cudaSuccess;
+    }
+  }
+  if (ok && tail > 0) {
+    cudaGraphConditionalHandle hi{};
+    ok = cudaGraphConditionalHandleCreate(&hi, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+    const int* aa = buf.any_active;
+    const int* itp = it_dev;
+    int lim = limit;
+    void* kargs[] = {&hi, &aa, &itp, &lim};
+    cudaKernelNodeParams kp{};
+    kp.func = reinterpret_cast<void*>(cg_tail_cond_kernel);
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = kargs;
+    cudaGraphNode_t kn{};
+    ok = ok && cudaGraphAddKernelNode(&kn, g, &wn, 1, &kp) == cudaSuccess;
+    cudaGraphNodeParams ip{};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hi;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t in{};
+    ok = ok && cudaGraphAddNode(&in, g, &kn, 1, &ip) == cudaSuccess;
+    ok = ok && cudaStreamBeginCaptureToGraph(cs, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeRelaxed) == cudaSuccess;
+    if (ok) {
+      dcur = 0;
+      for (int j = 1; j <= tail; ++j) pcg_iteration(R, 0.f, j == tail, cs);
+      cg_add_kernel<<<1, 1, 0, cs>>>(it_dev, tail);
+      cudaGraph_t body = nullptr;
+      ok = cudaStreamEndCapture(cs, &body) == cudaSuccess;
+    }
+  }
+  dcur = saved;
+  dev_tol = saved_dev;
+  if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (cs) cudaStreamDestroy(cs);
+  if (!ok) {
+    cudaGetLastError();  // the host loop runs instead
+    graph_loop = false;
+    return nullptr;
+  }
+  loops[R] = exec;
+  return exec;
+}
+
+CgEngine::~CgEngine() {
+  for (auto& kv : loops)
+    if (kv.second) cudaGraphExecDestroy(kv.second);
+}
+
 // One PCG solve over the R right-hand sides in buf.rhs (solver.py:5582-5723).
-// Returns the iteration count of the loop.
+// Returns the iteration count of the loop, or -1 when the loop ran as the
+// graph-resident loop (the count is then in it_dev).
 int CgEngine::pcg(int R, float tol, bool warm, cudaStream_t st) {
   const long long UM = static_cast<long long>(s.B) * R * s.m();
   const int units = s.B * R;
@@ -1257,27 +1414,21 @@ int CgEngine::pcg(int R, float tol, bool warm, cudaStream_t st) {
   if (fixed)
     cudaMemcpyAsync(buf.best, buf.x, UM * sizeof(float2), cudaMemcpyDeviceToDevice, st);
   const int limit = fixed ? c.fixed_iterations : c.max_cg_iter;
+  if (graph_loop && !fixed && c.check_interval % 2 == 0 && limit >= c.check_interval) {
+    cudaGraphExec_t exec = loop_graph(R);
+    if (exec) {
+      cg_loop_init_kernel<<<1, 1, 0, st>>>(tol_dev, tol, it_dev);
+      dcur = 0;
+      cudaGraphLaunch(exec, st);
+      dcur = 0;  // a finished loop's direction buffer is never read (beta = 0 at the next start)
+      return -1;
+    }
+  }
   int it = 0;
   for (it = 1; it <= limit; ++it) {
-    matvec(R, nullptr, true, buf.q, false, st);
-    A = args(R, tol);
     const bool check = (it % c.check_interval == 0) || it == limit;
-    if (!check) {
-      cg_vector_kernel<true, true, false><<<vec_grid(R), kCgThreads, kVecSmem, st>>>(A);
-      precondition(A, st);
-      cg_finish_kernel<<<fin_blocks, 256, 0, st>>>(A, kFinishStep);
-      continue;
-    }
-    cg_vector_kernel<true, false, false><<<vec_grid(R), kCgThreads, 0, st>>>(A);
-    matvec(R, buf.x, false, nullptr, true, st);
-    A = args(R, tol);
-    cudaMemsetAsync(buf.any_active, 0, sizeof(int), st);
-    cg_vector_kernel<false, true, true><<<vec_grid(R), kCgThreads, kVecSmem, st>>>(A);
-    precondition(A, st);
-    cg_finish_kernel<<<fin_blocks, 256, 0, st>>>(A, kFinishRestart);
-    if (fixed) {
-      cg_best_kernel<<<grid_for(UM), 256, 0, st>>>(s, R, buf.improved, buf.x, buf.best);
-    } else {
+    pcg_iteration(R, tol, check, st);
+    if (check && !fixed) {
       cudaMemcpyAsync(host_flag, buf.any_active, sizeof(int), cudaMemcpyDeviceToHost, st);
       cudaStreamSynchronize(st);
       if (!*host_flag) break;
@@ -1509,6 +1660,9 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
   E.prior = bf.gamma;
   E.noise = bf.scal.noise;
   E.dcur = 0;
+  // the PCG restart test runs on the device (graph-resident loop) where the
+  // schedule allows: no fixed-iteration checkpointing, an even check interval
+  E.graph_loop = c.cg_fixed_iterations == 0 && c.cg_check_interval % 2 == 0 && c.cg_max_iter >= c.cg_check_interval;
   // mode="dense": damping alone and min_iter as the minimum (solver.py:1287-1293, 1483-1487)
   const int minimum = dense ? c.min_iter : std::max(c.min_iter, c.cg_min_iter);
   const int limit = c.max_iter;
@@ -1628,7 +1782,8 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     sa.noise_shape = c.noise_shape;
     sa.noise_rate = c.noise_rate;
     sa.evidence = c.noise_update;
-    sa.cg_iters = last_cg;
+    sa.cg_iters = last_cg > 0 ? last_cg : 0;
+    sa.cg_iters_dev = last_cg < 0 ? E.it_dev : nullptr;
     sa.probes = count;
     sa.cg_tol = tolcg;
     sa.update = 1;
@@ -1697,7 +1852,7 @@ int cg_solve(FbmeCgPlan* P, const float2* y, const float* probes, const FbmeCgOu
     info->iterations = iterations;
     info->converged = converged;
     info->relative_change = hist[static_cast<size_t>(iterations - 1) * 6];
-    info->last_cg_iterations = last_cg;
+    info->last_cg_iterations = last_cg >= 0 ? last_cg : static_cast<int>(hist[static_cast<size_t>(iterations - 1) * 6 + 3]);
     info->active_set_size = act_size;
     info->active_set_iteration = act_iter;
     if (info->history) std::memcpy(info->history, hist.data(), hist.size() * sizeof(float));
@@ -1784,6 +1939,8 @@ int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig*
     return api_fail(FBME_ERR_INVALID, "out of host memory");
   }
   P->eng->host_flag = P->host;
+  P->eng->it_dev = P->buf.any_active + 1;
+  P->eng->tol_dev = reinterpret_cast<float*>(P->buf.any_active + 2);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     delete P;
@@ -1839,7 +1996,10 @@ int fbme_pcg_solve(FbmeCgPlan* plan, const float* prior, const float* noise, con
   E.dcur = 0;
   fbme::cg_gsum_kernel<<<s.B, 256, 0, st>>>(s.n(), prior, bf.gsum);
   E.precond_build(st);
+  const bool graph = E.graph_loop;
+  E.graph_loop = false;  // this entry reports the iteration count on the host
   const int it = E.pcg(rhs_count, tolerance, initial != nullptr, st);
+  E.graph_loop = graph;
   cudaMemcpyAsync(solution, bf.x, bytes, cudaMemcpyDeviceToDevice, st);
   const cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return api_fail(FBME_ERR_CUDA, std::string("fbme_pcg_solve: ") + cudaGetErrorString(e));

@@ -343,8 +343,11 @@ int fbme_cg_create(const FbmeShape* shape, int32_t n_scenes, const FbmeCgConfig*
                    FbmeCgPlan** plan);
 /* y: complex64 [B][M1][M2]; probes: float32 +-1 [B][P][M1][M2] (probe p of
  * scene b over the observed samples, the reference's probes[b, :, p]).
- * Synchronises `stream` at PCG restart checks, convergence checks and
- * active-set checks, as the reference reads those flags on the host. */
+ * The PCG restart test runs on the device (a CUDA graph WHILE node repeats
+ * chunks of cg_check_interval iterations while a right-hand side is active;
+ * with cg_fixed_iterations or an odd check interval the host reads it).
+ * Synchronises `stream` at the EM convergence checks and active-set checks,
+ * as the reference reads those on the host. */
 int fbme_cg_solve(FbmeCgPlan* plan, const void* y, const float* probes, const FbmeCgOutputs* out,
                   FbmeCgInfo* info, fbme_stream_t stream);
 int fbme_cg_destroy(FbmeCgPlan* plan);
