@@ -748,14 +748,22 @@ int feature_parts(int H, int W) {
 }
 // Passes 0 and 1 (the energy mean, f0 and its partial sums); pass 2 stores
 // the f1 channel, which only the backward pass reads from the workspace.
+// The feature statistics' first pass from a known sum |bp|^2 per scene (the
+// initialisation's sum of the backprojection power): partial 0 holds it,
+// the other partials of the pass zero.
+__global__ void seed_feature_sum_kernel(const float* ebp, int B, int parts, double* part) {
+  const int b = blockIdx.x, k = threadIdx.x;
+  if (b < B && k < parts) part[b * 128 + k] = k == 0 ? static_cast<double>(ebp[b]) : 0.0;
+}
+
 void features_passes(const float2* bp, int B, int H, int W, void* ws, int passes, cudaStream_t st,
-                     bool compact = false) {
+                     bool compact = false, int first = 0) {
   using namespace cnn;
   const CnnLayout L = cnn_layout(B, H, W);
   uint8_t* w = static_cast<uint8_t*>(ws);
   auto* x8 = reinterpret_cast<__nv_bfloat16*>(w + L.x8);
   auto* fpart = reinterpret_cast<double*>(w + L.fpart);
-  for (int pass = 0; pass < passes; ++pass)
+  for (int pass = first; pass < passes; ++pass)
     features_kernel<<<dim3(feature_parts(H, W), B), 256, 0, st>>>(pass, bp, B, static_cast<long long>(H) * W,
                                                                   x8, fpart, compact);
 }
@@ -845,10 +853,18 @@ void cnn_adam(float* params, const float* grad, float* m, float* v, int step, fl
 // block sums; the caller then re-runs the scalar initialisation.
 void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, void* ws,
                     const float* data_power, const float* floor_, float* gamma, double* upart,
-                    int nblocks, cudaStream_t st) {
+                    int nblocks, cudaStream_t st, const float* ebp) {
   using namespace cnn;
-  // f0 alone, one BF16 per pixel (the first layer takes f1 from the partials)
-  features_passes(bp, B, H, W, ws, 2, st, true);
+  // f0 alone, one BF16 per pixel (the first layer takes f1 from the partials);
+  // with the backprojection power `ebp` the statistics pass is not repeated
+  if (ebp) {
+    const CnnLayout L = cnn_layout(B, H, W);
+    seed_feature_sum_kernel<<<B, 64, 0, st>>>(ebp, B, feature_parts(H, W),
+                                             reinterpret_cast<double*>(static_cast<uint8_t*>(ws) + L.fpart));
+    features_passes(bp, B, H, W, ws, 2, st, true, 1);
+  } else {
+    features_passes(bp, B, H, W, ws, 2, st, true);
+  }
   const CnnLayout L = cnn_layout(B, H, W);
   float* out = reinterpret_cast<float*>(static_cast<uint8_t*>(ws) + L.out);
   cnn_forward(params, B, H, W, ws, out, st, true);

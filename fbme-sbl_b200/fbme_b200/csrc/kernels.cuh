@@ -214,9 +214,10 @@ void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out,
 void cnn_backward(const float* target, int B, int H, int W, void* ws, float* grad, double* loss_out,
                   cudaStream_t st);
 void cnn_adam(float* params, const float* grad, float* m, float* v, int step, float lr, cudaStream_t st);
+// ebp (optional): sum |bp|^2 per scene, from the initialisation
 void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, void* ws,
                     const float* data_power, const float* floor_, float* gamma, double* upart,
-                    int nblocks, cudaStream_t st);
+                    int nblocks, cudaStream_t st, const float* ebp = nullptr);
 // The same initial prior from a caller-supplied [B][N] log(prior / (P/N)) map.
 void warm_prior_from_map(const float* map, int B, long long N, const float* data_power, const float* floor_,
                          float* gamma, double* upart, int nblocks, cudaStream_t st);

@@ -690,7 +690,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
     if (u.warm_params)
       FBME_TIMED(prof, FBME_GROUP_INIT,
                  cnn_warm_prior(u.warm_params, u.bp, s.B, s.n1, s.n2, u.warm_ws, u.sc.data_power,
-                                u.sc.floor_, u.gamma, u.part, bn, st));
+                                u.sc.floor_, u.gamma, u.part, bn, st, u.sc.ebp));
     else
       FBME_TIMED(prof, FBME_GROUP_INIT,
                  warm_prior_from_map(u.warm_map, s.B, s.n(), u.sc.data_power, u.sc.floor_, u.gamma, u.part, bn,
