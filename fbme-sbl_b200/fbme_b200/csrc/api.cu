@@ -621,6 +621,7 @@ int create_plan(const FbmeShape* shapes, int32_t n_scenes, const FbmeConfig* cfg
   cudaError_t e = fbme::set_dft_attributes();
   if (e == cudaSuccess) e = fbme::set_polish_attributes();
   if (e == cudaSuccess) e = fbme::set_fft_attributes();
+  if (e == cudaSuccess) e = fbme::set_cnn_attributes();
   if (e != cudaSuccess) return fail(FBME_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 
   FbmePlan* P = new (std::nothrow) FbmePlan();

@@ -9,17 +9,16 @@
 //   out = conv(h2, W3) + b3                     [B][H][W]     FP32
 //   prior0 = max(data_power / N * exp(out), floor)
 //
-// The 8-to-8-channel convolutions (layer 2 forward, the input gradients)
-// run as implicit GEMMs on the tensor cores (mma.sync m16n8k16, BF16
-// operands, FP32 accumulation): M = 16 pixels of one tile row, N = 8 output
-// channels, K = (tap, input channel) with the channel fastest, so an operand
-// pair is one 32-bit load from the NHWC tile in shared memory.  Layers 1
-// (2 inputs) and 3 (1 output) run on the CUDA cores: padded to MMA shapes
-// they would waste most of the work.  The gradient with respect to a layer input is the same
-// convolution with flipped, transposed weights; the weight gradient is a
-// reduction over pixels on the CUDA cores with fixed-order block partials.
-// Parameters are an FP32 master vector; every use packs them into the BF16
-// matrices the kernels read.
+// The forward pass (training and inference) is one kernel per 32 x 32
+// output tile with all three layers on the tensor cores (mma.sync, BF16
+// operands, FP32 accumulation; net_tile_kernel below).  The backward pass's
+// input gradients are the same convolutions with flipped, transposed
+// weights, as implicit GEMMs on the tensor cores (M = 16 pixels of one tile
+// row, N = 8 output channels, K = (tap, input channel) with the channel
+// fastest, so an operand pair is one 32-bit load from the NHWC tile in
+// shared memory); the weight gradient is a reduction over pixels on the
+// CUDA cores with fixed-order block partials.  Parameters are an FP32
+// master vector; the kernels round them to BF16 where they read them.
 #include <cuda_bf16.h>
 #include <type_traits>
 #include <math.h>
@@ -49,53 +48,37 @@ constexpr int kOffW3 = kOffB2 + kHid;
 constexpr int kOffB3 = kOffW3 + 9 * kHid;
 constexpr int kNParams = kOffB3 + 1;
 
-constexpr int kK1 = kpad(kInP);   // 80
-constexpr int kK2 = kpad(kHid);   // 144
+constexpr int kK2 = kpad(kHid);   // 80: (tap, channel) of an 8-channel input, padded
 constexpr int kKb3 = kpad(8);     // 80: layer-3 backward, input = 8 padded gradient channels
 
-// BF16 operand matrices [Cout][K] and padded biases.
+// BF16 operand matrices [Cout][K] of the backward pass's input gradients.
 struct Packed {
-  __nv_bfloat16* wt1;  // [16][80]
-  __nv_bfloat16* wt2;  // [16][144]
-  __nv_bfloat16* wt3;  // [8][144]
-  __nv_bfloat16* wb3;  // [16][80]   d h2 = conv(d out, W3 flipped)
-  __nv_bfloat16* wb2;  // [16][144]  d h1 = conv(d a2, W2 flipped)
-  float *b1, *b2, *b3;  // [kHid], [kHid], [8]
-  float* w1f;  // [9][2][kHid]  layer 1, BF16-rounded, for the CUDA-core forward
-  float* w3f;  // [9][kHid]     layer 3, BF16-rounded
+  __nv_bfloat16* wb3;  // [8][80]  d h2 = conv(d out, W3 flipped)
+  __nv_bfloat16* wb2;  // [8][80]  d h1 = conv(d a2, W2 flipped)
 };
 
 __global__ void pack_kernel(const float* p, Packed P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  // forward layer 1: k = tap * 8 + ci
-  if (i < kHid * kK1) {
-    const int co = i / kK1, k = i % kK1, tap = k / kInP, ci = k % kInP;
-    const float v = (k < 9 * kInP && ci < kIn) ? p[kOffW1 + (tap * kIn + ci) * kHid + co] : 0.f;
-    P.wt1[i] = __float2bfloat16_rn(v);
-  }
   if (i < kHid * kK2) {
-    const int co = i / kK2, k = i % kK2, tap = k / kHid, ci = k % kHid;
-    P.wt2[i] = __float2bfloat16_rn(p[kOffW2 + (tap * kHid + ci) * kHid + co]);
-    // backward of layer 2: out channel = ci of W2, in channel = co of W2, taps flipped
-    const int cin2 = co, cout2 = ci;  // rename: row = input channel of the forward layer
-    P.wb2[i] = __float2bfloat16_rn(p[kOffW2 + ((8 - tap) * kHid + cin2) * kHid + cout2]);
-  }
-  if (i < 8 * kK2) {
-    const int co = i / kK2, k = i % kK2, tap = k / kHid, ci = k % kHid;
-    P.wt3[i] = __float2bfloat16_rn(co == 0 ? p[kOffW3 + tap * kHid + ci] : 0.f);
+    // row = input channel of the forward layer 2, column k = (flipped tap, its output channel)
+    const int cin2 = i / kK2, k = i % kK2, tap = k / kHid, cout2 = k % kHid;
+    const float v = k < 9 * kHid ? p[kOffW2 + ((8 - tap) * kHid + cin2) * kHid + cout2] : 0.f;
+    P.wb2[i] = __float2bfloat16_rn(v);
   }
   if (i < kHid * kKb3) {
     const int ci = i / kKb3, k = i % kKb3, tap = k / 8, co = k % 8;
     const float v = (k < 72 && co == 0) ? p[kOffW3 + (8 - tap) * kHid + ci] : 0.f;
     P.wb3[i] = __float2bfloat16_rn(v);
   }
-  if (i < kHid) {
-    P.b1[i] = p[kOffB1 + i];
-    P.b2[i] = p[kOffB2 + i];
-  }
-  if (i < 9 * kIn * kHid) P.w1f[i] = __bfloat162float(__float2bfloat16_rn(p[kOffW1 + i]));
-  if (i < 9 * kHid) P.w3f[i] = __bfloat162float(__float2bfloat16_rn(p[kOffW3 + i]));
-  if (i < 8) P.b3[i] = i == 0 ? p[kOffB3] : 0.f;
+}
+
+// Sum of a scene's n <= 64 FP64 feature partials p[0..n) in one fixed
+// order (two per lane, then the warp butterfly); every lane of the calling
+// warp returns the same value, so all kernels that read the partials agree.
+FBME_DEV double parts_sum(const double* p, int n) {
+  const int lane = threadIdx.x & 31;
+  const double v = (lane < n ? p[lane] : 0.0) + (lane + 32 < n ? p[lane + 32] : 0.0);
+  return warp_sum(v);
 }
 
 FBME_DEV uint32_t pack_bf16x2(float lo, float hi) {
@@ -253,219 +236,13 @@ conv3x3_kernel(const TIn* x, const __nv_bfloat16* mask, const __nv_bfloat16* wt,
   }
 }
 
-// Layer 2 forward (8 -> 8 channels, relu, BF16 NHWC output) on a 16 x 16
-// pixel tile: 4 warps x 4 rows of 16 pixels.  An A fragment is one
-// ldmatrix.x4 from the halo tile -- a matrix row is one pixel's 8 channels
-// at one tap (16 bytes), so the four 8x8 matrices are pixels 0-7 / 8-15 at
-// taps 2ks and 2ks+1 -- and the weight fragments and the bias stay in
-// registers.  The MMA operands and their order are those of
-// conv3x3_kernel<bf16, 8, 8, kOutReluBf16>, so the output is the same bit
-// for bit, with a quarter of its shared-memory loads and half its halo
-// overhead per pixel.
-constexpr int kF8Rows = 16, kF8Cols = 16;
 FBME_DEV void ldmatrix_x4(uint32_t addr, uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3) {
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
                : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
                : "r"(addr));
 }
 
-__global__ void __launch_bounds__(128) conv3x3_fwd8_kernel(const __nv_bfloat16* x, const __nv_bfloat16* wt,
-                                                          const float* bias, __nv_bfloat16* out, int H, int W) {
-  constexpr int KP = kpad(8);
-  constexpr int HW = kF8Rows + 2, WW = kF8Cols + 2, NP = HW * WW;
-  __shared__ uint4 xs[NP + 1];  // halo tile, one pixel (8 BF16) each, then a zero pixel for padded taps
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int x0 = blockIdx.x * kF8Cols, y0 = blockIdx.y * kF8Rows, b = blockIdx.z;
-  const long long img = static_cast<long long>(b) * H * W;
-  constexpr int IT = (NP + 127) / 128;
-  uint4 v[IT];
-#pragma unroll
-  for (int j = 0; j < IT; ++j) {
-    const int i = tid + j * 128;
-    const int gy = y0 - 1 + i / WW, gx = x0 - 1 + i % WW;
-    v[j] = make_uint4(0u, 0u, 0u, 0u);
-    if (i < NP && gy >= 0 && gy < H && gx >= 0 && gx < W)
-      v[j] = *reinterpret_cast<const uint4*>(x + (img + static_cast<long long>(gy) * W + gx) * 8);
-  }
-  const uint32_t* wt32 = reinterpret_cast<const uint32_t*>(wt);
-  uint32_t bq[KP / 16][2];
-#pragma unroll
-  for (int ks = 0; ks < KP / 16; ++ks) {
-    bq[ks][0] = wt32[(g * KP + ks * 16 + t * 2) / 2];
-    bq[ks][1] = wt32[(g * KP + ks * 16 + t * 2 + 8) / 2];
-  }
-  const float bias0 = bias[2 * t], bias1 = bias[2 * t + 1];
-#pragma unroll
-  for (int j = 0; j < IT; ++j) {
-    const int i = tid + j * 128;
-    if (i < NP) xs[i] = v[j];
-  }
-  if (tid == 0) xs[NP] = make_uint4(0u, 0u, 0u, 0u);
-  __syncthreads();
-  // ldmatrix rows: lanes 8m..8m+7 address matrix m = (pixel half m&1, tap 2ks + (m>>1))
-  const int mj = lane >> 3, pr = (lane & 7) + (mj & 1) * 8;
-  float acc[4][4];
-#pragma unroll
-  for (int mf = 0; mf < 4; ++mf)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[mf][j] = 0.f;
-#pragma unroll
-  for (int ks = 0; ks < KP / 16; ++ks) {
-    const int tap = 2 * ks + (mj >> 1);
-#pragma unroll
-    for (int mf = 0; mf < 4; ++mf) {
-      const int yy = warp * 4 + mf;
-      const int pix = tap < 9 ? (yy + tap / 3) * WW + pr + tap % 3 : NP;
-      uint32_t a0, a1, a2, a3;
-      ldmatrix_x4(smem_u32(&xs[pix]), a0, a1, a2, a3);
-      mma_bf16_16816(acc[mf], a0, a1, a2, a3, bq[ks][0], bq[ks][1]);
-    }
-  }
-#pragma unroll
-  for (int mf = 0; mf < 4; ++mf) {
-    const int gy = y0 + warp * 4 + mf;
-    if (gy >= H) continue;
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int gx = x0 + g + half * 8;
-      if (gx >= W) continue;
-      const long long pix = img + static_cast<long long>(gy) * W + gx;
-      const float v0 = acc[mf][half * 2] + bias0, v1 = acc[mf][half * 2 + 1] + bias1;
-      reinterpret_cast<uint32_t*>(out + pix * 8 + 2 * t)[0] = pack_bf16x2(fmaxf(v0, 0.f), fmaxf(v1, 0.f));
-    }
-  }
-}
 
-// Layers with few channels on the CUDA cores: 3x3 convolution, zero
-// padding 1, from CIN channels of an NHWC BF16 input (stride CSTR) to COUT
-// outputs over a 16 x 32 tile; each of the 128 threads computes 4 pixels
-// of one column, so every input value loaded from shared memory serves up
-// to 3 taps of 4 pixels and every weight vector 4 pixels.  The tile holds
-// channel pairs, and the multiply-adds run on the paired FP32 FMA over
-// pairs of output channels (layer 1) or input channels (layer 3): the
-// kernel is bound by issued instructions, which this halves.  BF16-rounded
-// weights w[tap][ci][co], FP32 accumulation.  RELU_BF16: relu, BF16 NHWC
-// output with COUT channels; else FP32 channel 0.  With f1part (layer 1),
-// input channel 1 is not read: it is the scene constant BF16(sum of the
-// nparts feature partials f1part[b * 128 + 64 + k] / N), the value the
-// third feature pass stores.
-constexpr int kSmallTW = 16, kSmallTH = 32, kSmallThreads = 128, kSmallRows = 4;
-template <int CIN, int CSTR, int COUT, bool RELU_BF16>
-__global__ void __launch_bounds__(kSmallThreads)
-conv_small_kernel(const __nv_bfloat16* x, const float* w, const float* bias, void* out, int H, int W,
-                  const double* f1part = nullptr, int nparts = 0) {
-  static_assert(CIN == 2 || CIN == 8, "input channels: one 32-bit or 128-bit load");
-  static_assert(COUT == 8 || COUT == 1, "output channels");
-  constexpr int TW = kSmallTW + 2, TH = kSmallTH + 2, NP = TW * TH, R = kSmallRows;
-  constexpr int NW = 9 * CIN * COUT;
-  __shared__ float2 xs2[(CIN / 2) * NP];  // channel pairs, pair-major: lanes read consecutive pairs
-  __shared__ __align__(16) float ws[NW + 8];
-  const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * kSmallTW, y0 = blockIdx.y * kSmallTH, b = blockIdx.z;
-  const long long img = static_cast<long long>(b) * H * W;
-  float c1 = 0.f;
-  if (CIN == 2 && f1part) {
-    double f1 = 0.0;
-    for (int k = 0; k < nparts; ++k) f1 += f1part[b * 128 + 64 + k];
-    c1 = __bfloat162float(__float2bfloat16_rn(static_cast<float>(f1 / (static_cast<double>(H) * W))));
-  }
-  // All of a thread's global loads are issued before any is stored.
-  constexpr int IT = (NP + kSmallThreads - 1) / kSmallThreads;
-  // CSTR == 1: channel 0 alone, one BF16 per pixel (channel 1 from f1part)
-  using LoadT = typename std::conditional<CIN == 8, uint4,
-                                          typename std::conditional<CSTR == 1, uint16_t, uint32_t>::type>::type;
-  LoadT v[IT];
-  bool in[IT];
-#pragma unroll
-  for (int j = 0; j < IT; ++j) {
-    const int pix = tid + j * kSmallThreads;
-    const int gy = y0 - 1 + pix / TW, gx = x0 - 1 + pix % TW;
-    in[j] = pix < NP && gy >= 0 && gy < H && gx >= 0 && gx < W;
-    v[j] = LoadT{};
-    if (in[j]) v[j] = *reinterpret_cast<const LoadT*>(x + (img + static_cast<long long>(gy) * W + gx) * CSTR);
-  }
-#pragma unroll
-  for (int j = 0; j < IT; ++j) {
-    const int pix = tid + j * kSmallThreads;
-    if (pix >= NP) break;
-    if constexpr (CIN == 8) {
-      const uint32_t u[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        xs2[k * NP + pix] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u[k]));
-    } else if constexpr (CSTR == 1) {
-      const float f0 = __bfloat162float(__ushort_as_bfloat16(v[j]));
-      xs2[pix] = make_float2(f0, in[j] ? c1 : 0.f);
-    } else {
-      const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v[j]));
-      xs2[pix] = make_float2(f.x, f1part ? (in[j] ? c1 : 0.f) : f.y);
-    }
-  }
-  for (int i = tid; i < NW; i += kSmallThreads) ws[i] = w[i];
-  if (tid < COUT) ws[NW + tid] = bias[tid];
-  __syncthreads();
-  const int px = tid % kSmallTW, r0 = (tid / kSmallTW) * R;
-  // COUT == 8: acc2[p][k] holds output channels (2k, 2k+1); COUT == 1:
-  // acc2[p][0] holds the sums over the even and the odd input channels
-  constexpr int NA = COUT == 8 ? 4 : 1;
-  float2 acc2[R][NA];
-#pragma unroll
-  for (int p = 0; p < R; ++p)
-#pragma unroll
-    for (int k = 0; k < NA; ++k) acc2[p][k] = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int cp = 0; cp < CIN / 2; ++cp) {
-    float2 xw[R + 2][3];
-#pragma unroll
-    for (int r = 0; r < R + 2; ++r)
-#pragma unroll
-      for (int dx = 0; dx < 3; ++dx) xw[r][dx] = xs2[cp * NP + (r0 + r) * TW + px + dx];
-#pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-      if constexpr (COUT == 8) {
-        const float4* wp = reinterpret_cast<const float4*>(ws + (tap * CIN + 2 * cp) * 8);
-        const float4 a0 = wp[0], a1 = wp[1], b0 = wp[2], b1 = wp[3];  // channels 2cp and 2cp + 1
-        const float2 wa[4] = {make_float2(a0.x, a0.y), make_float2(a0.z, a0.w), make_float2(a1.x, a1.y),
-                              make_float2(a1.z, a1.w)};
-        const float2 wb[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
-                              make_float2(b1.z, b1.w)};
-#pragma unroll
-        for (int p = 0; p < R; ++p) {
-          const float2 xv = xw[p + tap / 3][tap % 3];
-          const float2 xa = make_float2(xv.x, xv.x), xb = make_float2(xv.y, xv.y);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            acc2[p][k] = __ffma2_rn(xa, wa[k], acc2[p][k]);
-            acc2[p][k] = __ffma2_rn(xb, wb[k], acc2[p][k]);
-          }
-        }
-      } else {
-        const float2 wv = *reinterpret_cast<const float2*>(ws + tap * CIN + 2 * cp);
-#pragma unroll
-        for (int p = 0; p < R; ++p) acc2[p][0] = __ffma2_rn(xw[p + tap / 3][tap % 3], wv, acc2[p][0]);
-      }
-    }
-  }
-  const int gx = x0 + px;
-  if (gx >= W) return;
-#pragma unroll
-  for (int p = 0; p < R; ++p) {
-    const int gy = y0 + r0 + p;
-    if (gy >= H) break;
-    const long long pix = img + static_cast<long long>(gy) * W + gx;
-    if constexpr (RELU_BF16) {
-      static_assert(!RELU_BF16 || COUT == 8, "one 128-bit store per pixel");
-      uint32_t o[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        o[k] = pack_bf16x2(fmaxf(acc2[p][k].x + ws[NW + 2 * k], 0.f), fmaxf(acc2[p][k].y + ws[NW + 2 * k + 1], 0.f));
-      *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * COUT) = make_uint4(o[0], o[1], o[2], o[3]);
-    } else {
-      static_cast<float*>(out)[pix] = (acc2[p][0].x + acc2[p][0].y) + ws[NW];
-    }
-  }
-}
 
 // Weight gradient of one layer: dW[tap][ci][co] = sum_p x[p + shift(tap)][ci]
 // * g[p][co] (g masked by mask > 0 when a mask is given) and db[co] =
@@ -605,14 +382,8 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
   const int b = blockIdx.y;
   double acc = 0.0;
   double mean = 0.0, f1 = 0.0;
-  if (pass >= 1) {
-    for (int k = 0; k < gridDim.x; ++k) mean += part[b * 128 + k];
-    mean = fmax(mean / static_cast<double>(N), 1e-30);
-  }
-  if (pass == 2) {
-    for (int k = 0; k < gridDim.x; ++k) f1 += part[b * 128 + 64 + k];
-    f1 /= static_cast<double>(N);
-  }
+  if (pass >= 1) mean = fmax(parts_sum(part + b * 128, gridDim.x) / static_cast<double>(N), 1e-30);
+  if (pass == 2) f1 = parts_sum(part + b * 128 + 64, gridDim.x) / static_cast<double>(N);
   if (pass == 1 && compact && (N & 3) == 0) {
     // four pixels a step: two 16-byte loads, one 8-byte store of BF16 f0
     const float4* src = reinterpret_cast<const float4*>(bp + b * N);
@@ -661,27 +432,305 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
   }
 }
 
-// prior0 = max(data_power / N * exp(out), floor) and its per-block sums
-// (slot 0 of the UAMP partial array, as the plain initialisation writes).
-__global__ void __launch_bounds__(256) warm_prior_kernel(const float* out, long long N,
-                                                         const float* data_power, const float* floor_,
-                                                         float* gamma, double* upart) {
+// ---------------------------------------------------------------------------
+// The whole network on 32 x 32 output tiles, all three layers on the
+// tensor cores (mma.sync, BF16 operands, FP32 accumulation), every
+// intermediate in shared memory.  Per tile:
+//   x  : the f0 halo, 38 x 38 pixels of (f0, f1) BF16 pairs (f1 = the
+//        scene constant), zero outside the image;
+//   h1 : layer 1 on the 36 x 36 region, 16-pixel fragments in raster
+//        order, K = (tap, channel) = 18 plus the bias (below), padded to 32;
+//   h2 : layer 2 on the 34 x 34 region, A fragments by ldmatrix from h1
+//        (as conv3x3_kernel), K = 72 plus the bias, padded to 80;
+//   z  : the accumulator fragment of layer 2, relu'd and rounded to BF16,
+//        is the A fragment of an m16n8k8 product with W3 (K = 8 channels,
+//        N = 9 taps): z[tap][q] = sum_c W3[tap][c] h2[q][c];
+//   out: b3 + sum over the 9 taps of z[tap][q + shift(tap)].
+// Biases ride in the products: an input slot of ones (x: pair slot 9;
+// h1: channels 0-1 of a constant pixel) meets the bias split into BF16
+// hi + lo parts (hi + lo = the FP32 bias to 2^-16 relative).  Region
+// pixels outside the image are zero, as the convolution's zero padding
+// reads them.  Inference writes prior0 = max(data_power / N * exp(out),
+// floor) and its partial sums; training writes h1, h2 (NHWC BF16) and out
+// (FP32) for the backward pass.  Traffic: 2 bytes of f0 read and 4 bytes
+// of prior written per pixel.
+// ---------------------------------------------------------------------------
+constexpr int kFT = 32, kFThreads = 256, kFStrip = 4;   // the gather: 4-row strips per thread
+constexpr int kFXW = kFT + 6, kFXN = kFXW * kFXW;       // x halo
+constexpr int kF1W = kFT + 4, kF1N = kF1W * kF1W;       // h1 region
+constexpr int kF2W = kFT + 2, kF2N = kF2W * kF2W;       // h2 / z region
+constexpr int kFFrag1 = (kF1N + 15) / 16, kFFrag2 = (kF2N + 15) / 16;
+// dynamic shared memory: z [9][kF2N] FP32 (the x halo [kFXN + 2] BF16
+// pairs, then a pair of ones and a zero pair, lie under it until layer 1
+// is done), then h1 [kF1N + 1] NHWC BF16 pixels, the last one (1, 1, 0, ...)
+constexpr size_t kFSmemA = sizeof(float) * 9 * kF2N;
+constexpr size_t kFSmemB = sizeof(uint4) * (kF1N + 1);
+constexpr size_t kFSmem = kFSmemA + kFSmemB;
+static_assert(kFSmemA >= sizeof(uint32_t) * (kFXN + 2), "the x halo fits under z");
+static_assert(kFSmemA % 16 == 0, "16-byte aligned h1");
+static_assert(kFThreads == kFT * (kFT / kFStrip), "the gather: one strip per thread");
+constexpr uint32_t kOnesBf16x2 = 0x3F803F80u;  // (1.0, 1.0) in BF16
+
+// Prior of the strip (gy0 + p, gx), p < kFStrip, from the network outputs
+// o[p]: stores gamma and adds the priors to acc in pixel order (both
+// warm-prior tile kernels use it, so their partial sums agree bit for bit).
+FBME_DEV void prior_strip(const float (&o)[kFStrip], float base, float fl, float* gamma_img, int H, int W,
+                          int gy0, int gx, double& acc) {
+  if (gx >= W) return;
+#pragma unroll
+  for (int p = 0; p < kFStrip; ++p) {
+    const int gy = gy0 + p;
+    if (gy >= H) break;
+    const float gm = fmaxf(base * expf(fminf(fmaxf(o[p], -40.f), 40.f)), fl);
+    gamma_img[static_cast<long long>(gy) * W + gx] = gm;
+    acc += gm;
+  }
+}
+
+// The same prior from a caller's [B][H][W] map, over the same tiles, strips
+// and partial-sum slots as warm_net_kernel.
+__global__ void __launch_bounds__(kFThreads) warm_map_kernel(const float* map, int H, int W,
+                                                            const float* data_power, const float* floor_,
+                                                            float* gamma, double* upart) {
   __shared__ double red[32];
   const int b = blockIdx.y;
-  const float base = data_power[b] / static_cast<float>(N), fl = floor_[b];
+  const long long img = static_cast<long long>(b) * H * W;
+  const float base = data_power[b] / static_cast<float>(static_cast<long long>(H) * W), fl = floor_[b];
+  const int tx_n = (W + kFT - 1) / kFT, ntiles = tx_n * ((H + kFT - 1) / kFT);
+  const int col = threadIdx.x % kFT, r0 = (threadIdx.x / kFT) * kFStrip;
   double acc = 0.0;
-  for (long long n = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; n < N;
-       n += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const float o = fminf(fmaxf(out[b * N + n], -40.f), 40.f);
-    const float gm = fmaxf(base * expf(o), fl);
-    gamma[b * N + n] = gm;
-    acc += gm;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int y0 = (tile / tx_n) * kFT, x0 = (tile % tx_n) * kFT;
+    const int gx = x0 + col;
+    float o[kFStrip];
+#pragma unroll
+    for (int p = 0; p < kFStrip; ++p) {
+      const int gy = y0 + r0 + p;
+      o[p] = (gy < H && gx < W) ? map[img + static_cast<long long>(gy) * W + gx] : 0.f;
+    }
+    prior_strip(o, base, fl, gamma + img, H, W, y0 + r0, gx, acc);
   }
   const double s = block_sum(acc, red);
   if (threadIdx.x == 0)
     upart[(static_cast<long long>(b) * kMaxTilesPerScene + blockIdx.x) * kPartSlots] = s;
 }
 
+FBME_DEV void mma_bf16_1688(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0));
+}
+
+// An FP32 value as a BF16 pair (hi, lo) with hi + lo equal to it to 2^-16.
+FBME_DEV uint32_t bf16_hi_lo(float v) {
+  const float hi = __bfloat162float(__float2bfloat16_rn(v));
+  return pack_bf16x2(hi, v - hi);
+}
+
+// relu(BF16(a)), relu(BF16(b)) as a BF16 pair.
+FBME_DEV uint32_t relu_bf16x2(float a, float b) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  v = __hmax2(v, __float2bfloat162_rn(0.f));
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+FBME_DEV bool in_image(int y, int x, int H, int W) {
+  return static_cast<unsigned>(y) < static_cast<unsigned>(H) && static_cast<unsigned>(x) < static_cast<unsigned>(W);
+}
+
+struct NetArgs {
+  const __nv_bfloat16* x;  // f0 at x[pixel * CSTR]
+  const double* fpart;     // feature partials [B][128]; f1 = the pass-1 sum / N
+  int nparts;
+  const float* params;     // FP32 master parameters
+  int H, W;
+  // inference: the prior and its partial sums
+  const float* data_power;
+  const float* floor_;
+  float* gamma;
+  double* upart;
+  // training: the activations for the backward pass
+  __nv_bfloat16* h1;
+  __nv_bfloat16* h2;
+  float* out;
+};
+
+static_assert(kF1N % 16 == 0, "layer 1: every fragment row is a region pixel");
+
+template <bool TRAIN, int CSTR>
+__global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
+  extern __shared__ __align__(16) uint8_t fsm[];
+  __shared__ double red[32];
+  float* z = reinterpret_cast<float*>(fsm);         // [9][kF2N]
+  uint32_t* xs = reinterpret_cast<uint32_t*>(fsm);  // [kFXN] (f0, f1), then ones, zero
+  uint4* h1 = reinterpret_cast<uint4*>(fsm + kFSmemA);
+  uint32_t* h1w = reinterpret_cast<uint32_t*>(h1);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int b = blockIdx.y, H = a.H, W = a.W;
+  const long long N = static_cast<long long>(H) * W, img = static_cast<long long>(b) * N;
+  const float* p = a.params;
+  const uint32_t c1hi = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(
+                            static_cast<float>(parts_sum(a.fpart + b * 128 + 64, a.nparts) / static_cast<double>(N)))))
+                        << 16;
+  // B fragments (lane: n = g, k = 2 t4 (+1), + 8 for the second register)
+  const uint32_t l1b0 = pack_bf16x2(p[kOffW1 + (t4 * kIn) * kHid + g], p[kOffW1 + (t4 * kIn + 1) * kHid + g]);
+  const uint32_t l1b1 =
+      pack_bf16x2(p[kOffW1 + ((t4 + 4) * kIn) * kHid + g], p[kOffW1 + ((t4 + 4) * kIn + 1) * kHid + g]);
+  const uint32_t l1b2 = t4 == 0   ? pack_bf16x2(p[kOffW1 + (8 * kIn) * kHid + g], p[kOffW1 + (8 * kIn + 1) * kHid + g])
+                        : t4 == 1 ? bf16_hi_lo(p[kOffB1 + g])
+                                  : 0u;
+  constexpr int KP2 = kpad(kHid);
+  uint32_t bq[KP2 / 16][2];
+#pragma unroll
+  for (int ks = 0; ks < KP2 / 16; ++ks)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = ks * 16 + 2 * t4 + 8 * h;  // k = tap * 8 + channel; 72: the bias
+      bq[ks][h] = k < 9 * kHid ? pack_bf16x2(p[kOffW2 + k * kHid + g], p[kOffW2 + (k + 1) * kHid + g])
+                  : k == 9 * kHid ? bf16_hi_lo(p[kOffB2 + g])
+                                  : 0u;
+    }
+  const uint32_t bz0 = pack_bf16x2(p[kOffW3 + g * kHid + 2 * t4], p[kOffW3 + g * kHid + 2 * t4 + 1]);
+  const uint32_t bz1 =
+      g == 0 ? pack_bf16x2(p[kOffW3 + 8 * kHid + 2 * t4], p[kOffW3 + 8 * kHid + 2 * t4 + 1]) : 0u;
+  const float b3 = p[kOffB3];
+  float base = 0.f, fl = 0.f;
+  if constexpr (!TRAIN) {
+    base = a.data_power[b] / static_cast<float>(N);
+    fl = a.floor_[b];
+  }
+  // layer-1 tap offsets in the x halo; layer-2 ldmatrix row of this lane
+  const int o1a = (t4 / 3) * kFXW + t4 % 3, o1b = ((t4 + 4) / 3) * kFXW + (t4 + 4) % 3;
+  constexpr int o8 = 2 * kFXW + 2;
+  const int mj = lane >> 3, pr = (lane & 7) + (mj & 1) * 8;
+  if (tid == 0) h1[kF1N] = make_uint4(kOnesBf16x2, 0u, 0u, 0u);
+
+  const int tx_n = (W + kFT - 1) / kFT, ntiles = tx_n * ((H + kFT - 1) / kFT);
+  double acc = 0.0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int y0 = (tile / tx_n) * kFT, x0 = (tile % tx_n) * kFT;
+    // the whole halo lies inside the image: no region pixel is padding
+    const bool inner = y0 >= 3 && x0 >= 3 && y0 + kFT + 3 <= H && x0 + kFT + 3 <= W;
+    __syncthreads();  // the previous tile's z is read
+    {  // x halo: all of a thread's loads issued before any is stored
+      constexpr int IT = (kFXN + kFThreads - 1) / kFThreads;
+      const uint16_t* x16 = reinterpret_cast<const uint16_t*>(a.x);
+      uint32_t v[IT];
+#pragma unroll
+      for (int j = 0; j < IT; ++j) {
+        const int i = tid + j * kFThreads, iy = i / kFXW;
+        const int gy = y0 - 3 + iy, gx = x0 - 3 + (i - iy * kFXW);
+        v[j] = 0u;
+        if (i < kFXN && in_image(gy, gx, H, W))
+          v[j] = c1hi | x16[(img + static_cast<long long>(gy) * W + gx) * CSTR];
+      }
+#pragma unroll
+      for (int j = 0; j < IT; ++j) {
+        const int i = tid + j * kFThreads;
+        if (i < kFXN) xs[i] = v[j];
+      }
+      if (tid == 0) {
+        xs[kFXN] = kOnesBf16x2;
+        xs[kFXN + 1] = 0u;
+      }
+    }
+    __syncthreads();
+    // layer 1: rows g, g + 8 of fragment f are region pixels p0, p1; the
+    // second k step holds tap 8 (t4 = 0) and the bias (t4 = 1)
+    for (int f = warp; f < kFFrag1; f += kFThreads / 32) {
+      const int p0 = f * 16 + g, p1 = p0 + 8;
+      const int ry0 = p0 / kF1W, rx0 = p0 - ry0 * kF1W, ry1 = p1 / kF1W, rx1 = p1 - ry1 * kF1W;
+      const int q0 = ry0 * kFXW + rx0, q1 = ry1 * kFXW + rx1;
+      const int i0 = t4 == 0 ? q0 + o8 : kFXN + (t4 > 1), i1 = t4 == 0 ? q1 + o8 : kFXN + (t4 > 1);
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+      mma_bf16_16816(c, xs[q0 + o1a], xs[q1 + o1a], xs[q0 + o1b], xs[q1 + o1b], l1b0, l1b1);
+      mma_bf16_16816(c, xs[i0], xs[i1], 0u, 0u, l1b2, 0u);
+      const int gy0 = y0 - 2 + ry0, gx0 = x0 - 2 + rx0, gy1 = y0 - 2 + ry1, gx1 = x0 - 2 + rx1;
+      const bool in0 = inner || in_image(gy0, gx0, H, W), in1 = inner || in_image(gy1, gx1, H, W);
+      const uint32_t w0 = in0 ? relu_bf16x2(c[0], c[1]) : 0u, w1 = in1 ? relu_bf16x2(c[2], c[3]) : 0u;
+      h1w[p0 * 4 + t4] = w0;
+      h1w[p1 * 4 + t4] = w1;
+      if constexpr (TRAIN) {  // the tile's own 32 x 32 pixels
+        if (in0 && ry0 >= 2 && ry0 < kFT + 2 && rx0 >= 2 && rx0 < kFT + 2)
+          reinterpret_cast<uint32_t*>(a.h1 + (img + static_cast<long long>(gy0) * W + gx0) * kHid)[t4] = w0;
+        if (in1 && ry1 >= 2 && ry1 < kFT + 2 && rx1 >= 2 && rx1 < kFT + 2)
+          reinterpret_cast<uint32_t*>(a.h1 + (img + static_cast<long long>(gy1) * W + gx1) * kHid)[t4] = w1;
+      }
+    }
+    __syncthreads();
+    // layer 2 and the per-pixel tap products of layer 3
+    for (int f = warp; f < kFFrag2; f += kFThreads / 32) {
+      const int pa = min(f * 16 + pr, kF2N - 1);
+      const int ay = pa / kF2W;
+      const int abase = ay * kF1W + (pa - ay * kF2W);
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int ks = 0; ks < KP2 / 16; ++ks) {
+        const int tap = 2 * ks + (mj >> 1);
+        const int pix = tap < 9 ? abase + (tap / 3) * kF1W + tap % 3 : kF1N;
+        uint32_t a0, a1, a2, a3;
+        ldmatrix_x4(smem_u32(&h1[pix]), a0, a1, a2, a3);
+        mma_bf16_16816(c, a0, a1, a2, a3, bq[ks][0], bq[ks][1]);
+      }
+      const int q0 = f * 16 + g, q1 = q0 + 8;
+      const int sy0 = q0 / kF2W, sx0 = q0 - sy0 * kF2W, sy1 = q1 / kF2W, sx1 = q1 - sy1 * kF2W;
+      const int gy0 = y0 - 1 + sy0, gx0 = x0 - 1 + sx0, gy1 = y0 - 1 + sy1, gx1 = x0 - 1 + sx1;
+      const bool in0 = q0 < kF2N && (inner || in_image(gy0, gx0, H, W));
+      const bool in1 = q1 < kF2N && (inner || in_image(gy1, gx1, H, W));
+      const uint32_t u0 = in0 ? relu_bf16x2(c[0], c[1]) : 0u, u1 = in1 ? relu_bf16x2(c[2], c[3]) : 0u;
+      if constexpr (TRAIN) {
+        if (in0 && sy0 >= 1 && sy0 <= kFT && sx0 >= 1 && sx0 <= kFT)
+          reinterpret_cast<uint32_t*>(a.h2 + (img + static_cast<long long>(gy0) * W + gx0) * kHid)[t4] = u0;
+        if (in1 && sy1 >= 1 && sy1 <= kFT && sx1 >= 1 && sx1 <= kFT)
+          reinterpret_cast<uint32_t*>(a.h2 + (img + static_cast<long long>(gy1) * W + gx1) * kHid)[t4] = u1;
+      }
+      // the accumulator fragment (rows g, g + 8; channels 2 t4, 2 t4 + 1) is
+      // the A fragment of m16n8k8: z for taps 0-7, then tap 8
+      float za[4] = {0.f, 0.f, 0.f, 0.f}, zb[4] = {0.f, 0.f, 0.f, 0.f};
+      mma_bf16_1688(za, u0, u1, bz0);
+      mma_bf16_1688(zb, u0, u1, bz1);
+      if (q0 < kF2N) {
+        z[(2 * t4) * kF2N + q0] = za[0];
+        z[(2 * t4 + 1) * kF2N + q0] = za[1];
+        if (t4 == 0) z[8 * kF2N + q0] = zb[0];
+      }
+      if (q1 < kF2N) {
+        z[(2 * t4) * kF2N + q1] = za[2];
+        z[(2 * t4 + 1) * kF2N + q1] = za[3];
+        if (t4 == 0) z[8 * kF2N + q1] = zb[2];
+      }
+    }
+    __syncthreads();
+    {  // layer 3: out = sum over the taps (in order) + b3
+      const int col = tid % kFT, r0 = (tid / kFT) * kFStrip;
+      float o[kFStrip];
+#pragma unroll
+      for (int pp = 0; pp < kFStrip; ++pp) {
+        const int qb = (r0 + pp) * kF2W + col;
+        float sacc = z[qb];
+#pragma unroll
+        for (int tap = 1; tap < 9; ++tap) sacc += z[tap * kF2N + qb + (tap / 3) * kF2W + tap % 3];
+        o[pp] = sacc + b3;
+      }
+      if constexpr (TRAIN) {
+        const int gx = x0 + col;
+#pragma unroll
+        for (int pp = 0; pp < kFStrip; ++pp) {
+          const int gy = y0 + r0 + pp;
+          if (gy < H && gx < W) a.out[img + static_cast<long long>(gy) * W + gx] = o[pp];
+        }
+      } else {
+        prior_strip(o, base, fl, a.gamma + img, H, W, y0 + r0, x0 + col, acc);
+      }
+    }
+  }
+  if constexpr (!TRAIN) {
+    const double sum = block_sum(acc, red);
+    if (tid == 0) a.upart[(static_cast<long long>(b) * kMaxTilesPerScene + blockIdx.x) * kPartSlots] = sum;
+  }
+}
 }  // namespace cnn
 }  // namespace fbme
 
@@ -735,16 +784,8 @@ cnn::Packed packed_at(uint8_t* w) {
     p += a256(bytes);
     return r;
   };
-  P.wt1 = reinterpret_cast<__nv_bfloat16*>(take(kHid * kK1 * 2));
-  P.wt2 = reinterpret_cast<__nv_bfloat16*>(take(kHid * kK2 * 2));
-  P.wt3 = reinterpret_cast<__nv_bfloat16*>(take(8 * kK2 * 2));
   P.wb3 = reinterpret_cast<__nv_bfloat16*>(take(kHid * kKb3 * 2));
   P.wb2 = reinterpret_cast<__nv_bfloat16*>(take(kHid * kK2 * 2));
-  P.b1 = reinterpret_cast<float*>(take(kHid * 4));
-  P.b2 = reinterpret_cast<float*>(take(kHid * 4));
-  P.b3 = reinterpret_cast<float*>(take(8 * 4));
-  P.w1f = reinterpret_cast<float*>(take(9 * kIn * kHid * 4));
-  P.w3f = reinterpret_cast<float*>(take(9 * kHid * 4));
   return P;
 }
 
@@ -796,29 +837,25 @@ void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t 
 
 // Forward pass from the features in the workspace; the output [B][H][W]
 // stays in the workspace (for cnn_backward) and is copied to `out` if given.
-void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st,
-                 bool compact) {
+void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st) {
   using namespace cnn;
   const CnnLayout L = cnn_layout(B, H, W);
   uint8_t* w = static_cast<uint8_t*>(ws);
-  const Packed P = packed_at(w + L.packed);
+  const Packed P = packed_at(w + L.packed);  // the backward pass's operand matrices
   pack_kernel<<<(kHid * kK2 + 255) / 256, 256, 0, st>>>(params, P);
-  const dim3 grid(W / kTileW, H / kTileH, B);
-  auto* x8 = reinterpret_cast<const __nv_bfloat16*>(w + L.x8);
-  auto* h1 = reinterpret_cast<__nv_bfloat16*>(w + L.h1);
-  auto* h2 = reinterpret_cast<__nv_bfloat16*>(w + L.h2);
-  const dim3 grid_small((W + kSmallTW - 1) / kSmallTW, (H + kSmallTH - 1) / kSmallTH, B);
-  if (compact)
-    conv_small_kernel<kIn, 1, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
-        x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
-  else
-    conv_small_kernel<kIn, kInP, kHid, true><<<grid_small, kSmallThreads, 0, st>>>(
-        x8, P.w1f, P.b1, h1, H, W, reinterpret_cast<const double*>(w + L.fpart), feature_parts(H, W));
-  static_assert(kHid == 8, "conv3x3_fwd8_kernel is the 8 -> 8 layer");
-  conv3x3_fwd8_kernel<<<dim3((W + kF8Cols - 1) / kF8Cols, (H + kF8Rows - 1) / kF8Rows, B), 128, 0, st>>>(
-      h1, P.wt2, P.b2, h2, H, W);
   float* wout = reinterpret_cast<float*>(w + L.out);  // kept for cnn_backward
-  conv_small_kernel<kHid, kHid, 1, false><<<grid_small, kSmallThreads, 0, st>>>(h2, P.w3f, P.b3, wout, H, W);
+  NetArgs na{};
+  na.x = reinterpret_cast<const __nv_bfloat16*>(w + L.x8);
+  na.fpart = reinterpret_cast<const double*>(w + L.fpart);
+  na.nparts = feature_parts(H, W);
+  na.params = params;
+  na.H = H;
+  na.W = W;
+  na.h1 = reinterpret_cast<__nv_bfloat16*>(w + L.h1);
+  na.h2 = reinterpret_cast<__nv_bfloat16*>(w + L.h2);
+  na.out = wout;
+  const int ntiles = ((H + kFT - 1) / kFT) * ((W + kFT - 1) / kFT);
+  net_tile_kernel<true, kInP><<<dim3(ntiles, B), kFThreads, kFSmem, st>>>(na);
   if (out && out != wout)
     cudaMemcpyAsync(out, wout, static_cast<size_t>(B) * H * W * sizeof(float), cudaMemcpyDeviceToDevice, st);
 }
@@ -870,33 +907,51 @@ void cnn_adam(float* params, const float* grad, float* m, float* v, int step, fl
                                                                  1e-8f, c1, c2);
 }
 
-// Warm start inside a plan: features of A^H y, forward, prior0 and its
-// block sums; the caller then re-runs the scalar initialisation.
+// Warm start inside a plan: features of A^H y, then the fused network +
+// prior (prior0 and its partial sums in `nblocks` slots per scene); the
+// caller then re-runs the scalar initialisation.
 void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, void* ws,
                     const float* data_power, const float* floor_, float* gamma, double* upart,
                     int nblocks, cudaStream_t st, const float* ebp) {
   using namespace cnn;
-  // f0 alone, one BF16 per pixel (the first layer takes f1 from the partials);
+  const CnnLayout L = cnn_layout(B, H, W);
+  uint8_t* w = static_cast<uint8_t*>(ws);
+  auto* fpart = reinterpret_cast<double*>(w + L.fpart);
+  // f0 alone, one BF16 per pixel (the network takes f1 from the partials);
   // with the backprojection power `ebp` the statistics pass is not repeated
   if (ebp) {
-    const CnnLayout L = cnn_layout(B, H, W);
-    seed_feature_sum_kernel<<<B, 64, 0, st>>>(ebp, B, feature_parts(H, W),
-                                             reinterpret_cast<double*>(static_cast<uint8_t*>(ws) + L.fpart));
+    seed_feature_sum_kernel<<<B, 64, 0, st>>>(ebp, B, feature_parts(H, W), fpart);
     features_passes(bp, B, H, W, ws, 2, st, true, 1);
   } else {
     features_passes(bp, B, H, W, ws, 2, st, true);
   }
-  const CnnLayout L = cnn_layout(B, H, W);
-  float* out = reinterpret_cast<float*>(static_cast<uint8_t*>(ws) + L.out);
-  cnn_forward(params, B, H, W, ws, out, st, true);
-  warm_prior_kernel<<<dim3(nblocks, B), 256, 0, st>>>(out, static_cast<long long>(H) * W, data_power,
-                                                      floor_, gamma, upart);
+  NetArgs na{};
+  na.x = reinterpret_cast<const __nv_bfloat16*>(w + L.x8);
+  na.fpart = fpart;
+  na.nparts = feature_parts(H, W);
+  na.params = params;
+  na.H = H;
+  na.W = W;
+  na.data_power = data_power;
+  na.floor_ = floor_;
+  na.gamma = gamma;
+  na.upart = upart;
+  net_tile_kernel<false, 1><<<dim3(nblocks, B), kFThreads, kFSmem, st>>>(na);
 }
 
-void warm_prior_from_map(const float* map, int B, long long N, const float* data_power, const float* floor_,
+void warm_prior_from_map(const float* map, int B, int H, int W, const float* data_power, const float* floor_,
                          float* gamma, double* upart, int nblocks, cudaStream_t st) {
   using namespace cnn;
-  warm_prior_kernel<<<dim3(nblocks, B), 256, 0, st>>>(map, N, data_power, floor_, gamma, upart);
+  warm_map_kernel<<<dim3(nblocks, B), kFThreads, 0, st>>>(map, H, W, data_power, floor_, gamma, upart);
+}
+
+cudaError_t set_cnn_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(cnn::net_tile_kernel<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(cnn::kFSmem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cnn::net_tile_kernel<true, cnn::kInP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(cnn::kFSmem));
+  return e;
 }
 
 }  // namespace fbme

@@ -209,8 +209,7 @@ int cnn_param_count();
 size_t cnn_workspace_bytes(long long B, long long H, long long W);
 const char* cnn_check(long long B, long long H, long long W);
 void cnn_features(const float2* bp, int B, int H, int W, void* ws, cudaStream_t st);
-void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st,
-                 bool compact = false);
+void cnn_forward(const float* params, int B, int H, int W, void* ws, float* out, cudaStream_t st);
 void cnn_backward(const float* target, int B, int H, int W, void* ws, float* grad, double* loss_out,
                   cudaStream_t st);
 void cnn_adam(float* params, const float* grad, float* m, float* v, int step, float lr, cudaStream_t st);
@@ -219,8 +218,9 @@ void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, 
                     const float* data_power, const float* floor_, float* gamma, double* upart,
                     int nblocks, cudaStream_t st, const float* ebp = nullptr);
 // The same initial prior from a caller-supplied [B][N] log(prior / (P/N)) map.
-void warm_prior_from_map(const float* map, int B, long long N, const float* data_power, const float* floor_,
+void warm_prior_from_map(const float* map, int B, int H, int W, const float* data_power, const float* floor_,
                          float* gamma, double* upart, int nblocks, cudaStream_t st);
+cudaError_t set_cnn_attributes();
 
 // Active-set switch of single-scene cg runs (cg_active.cu).
 struct ActiveBufs {

@@ -693,7 +693,7 @@ void uamp_run(const BatchShape& s, const DftTables& t, const DevConfig& c, const
                                 u.sc.floor_, u.gamma, u.part, bn, st, u.sc.ebp));
     else
       FBME_TIMED(prof, FBME_GROUP_INIT,
-                 warm_prior_from_map(u.warm_map, s.B, s.n(), u.sc.data_power, u.sc.floor_, u.gamma, u.part, bn,
+                 warm_prior_from_map(u.warm_map, s.B, s.n1, s.n2, u.sc.data_power, u.sc.floor_, u.gamma, u.part, bn,
                                      st));
     FBME_TIMED(prof, FBME_GROUP_INIT,
                (scalars_kernel<<<sc_blocks, 32 * kScalarScenesPerBlock, 0, st>>>(

@@ -192,23 +192,31 @@ def test_warm_started_solve_matches_oracle_from_the_network_prior():
 
 
 @pytest.mark.gpu
-def test_warm_prior_map_equals_the_attached_network():
+@pytest.mark.parametrize("grid,prefix", [(GRID, PREFIX), ((40, 48), (24, 32))])
+def test_warm_prior_map_equals_the_attached_network(grid, prefix):
     """A caller-supplied log-prior map (here: the shipped network's output
-    for A^H y) warm-starts the plan exactly as the attached network does."""
+    for A^H y, through the unfused layer kernels) warm-starts the plan
+    exactly as the attached network (the fused network + prior kernel)
+    does; the 40 x 48 grid has tiles cut by the image edge."""
     need_gpu()
     from fbme_b200.engine import FBMEEngine
     from fbme_b200.learned import (DEFAULT_WEIGHTS, WarmStartNet, attach_warm_prior_map, attach_warm_start,
                                    plain_config)
 
-    y, _ = _batch(4, 2_400_000)
+    if grid == GRID:
+        y, _ = _batch(4, 2_400_000)
+    else:
+        rng = np.random.default_rng(11)
+        m = prefix[0] * prefix[1]
+        y = (rng.normal(size=(4, m)) + 1j * rng.normal(size=(4, m))).astype(np.complex64)
     dev = torch.device("cuda", 0)
     yt = torch.from_numpy(y).cuda().view(4, -1)
     net = WarmStartNet.load(DEFAULT_WEIGHTS, dev)
-    a = FBMEEngine(4, GRID, PREFIX, plain_config(1), dev)
+    a = FBMEEngine(4, grid, prefix, plain_config(1), dev)
     ws = attach_warm_start(a, net)
     a.run(yt)
-    b = FBMEEngine(4, GRID, PREFIX, plain_config(1), dev)
-    prior_map = net.predict(b.dft_adjoint(yt), *GRID).contiguous()
+    b = FBMEEngine(4, grid, prefix, plain_config(1), dev)
+    prior_map = net.predict(b.dft_adjoint(yt), *grid).contiguous()
     attach_warm_prior_map(b, prior_map)
     b.run(yt)
     torch.cuda.synchronize()
@@ -216,7 +224,7 @@ def test_warm_prior_map_equals_the_attached_network():
         assert torch.equal(a.out[f], b.out[f]), f
     attach_warm_prior_map(b, None)  # back to the plain initialisation
     b.run(yt)
-    c = FBMEEngine(4, GRID, PREFIX, plain_config(1), dev)
+    c = FBMEEngine(4, grid, prefix, plain_config(1), dev)
     c.run(yt)
     torch.cuda.synchronize()
     assert torch.equal(b.out["x"], c.out["x"])
