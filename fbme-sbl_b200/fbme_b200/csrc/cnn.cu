@@ -88,7 +88,7 @@ FBME_DEV uint32_t pack_bf16x2(float lo, float hi) {
 
 FBME_DEV void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                              uint32_t b0, uint32_t b1) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
       "{%8,%9}, {%0,%1,%2,%3};"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -456,17 +456,23 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
 // of prior written per pixel.
 // ---------------------------------------------------------------------------
 constexpr int kFT = 32, kFThreads = 256, kFStrip = 4;   // the gather: 4-row strips per thread
-constexpr int kFXW = kFT + 6, kFXN = kFXW * kFXW;       // x halo
+constexpr int kFXH = kFT + 6, kFXP = kFT + 8;           // x halo: 38 rows of 40 (columns x0 - 4 ...)
+constexpr int kFXN = kFXH * kFXP, kFXChunks = kFXH * (kFXP / 4);  // 4-pixel chunks
 constexpr int kF1W = kFT + 4, kF1N = kF1W * kF1W;       // h1 region
 constexpr int kF2W = kFT + 2, kF2N = kF2W * kF2W;       // h2 / z region
 constexpr int kFFrag1 = (kF1N + 15) / 16, kFFrag2 = (kF2N + 15) / 16;
-// dynamic shared memory: z [9][kF2N] FP32 (the x halo [kFXN + 2] BF16
-// pairs, then a pair of ones and a zero pair, lie under it until layer 1
-// is done), then h1 [kF1N + 1] NHWC BF16 pixels, the last one (1, 1, 0, ...)
+// dynamic shared memory: z [9][kF2N] FP32 (the x halo [kFXN] BF16 pairs
+// lies under it until layer 1 is done; its rows are 16-byte aligned), h1 [kF1N + 1] NHWC BF16 pixels (the
+// last one (1, 1, 0, ...)), then two address tables built once per CTA:
+// layer 1, per fragment and row g < 8, the halo indices of its pixels g and
+// g + 8 (16 bits each); layer 2, per fragment and row, the h1 index of the
+// pixel's first tap (16 bits).
+constexpr int kFTab1 = kFFrag1 * 8, kFTab2 = kFFrag2 * 16;
 constexpr size_t kFSmemA = sizeof(float) * 9 * kF2N;
 constexpr size_t kFSmemB = sizeof(uint4) * (kF1N + 1);
-constexpr size_t kFSmem = kFSmemA + kFSmemB;
-static_assert(kFSmemA >= sizeof(uint32_t) * (kFXN + 2), "the x halo fits under z");
+constexpr size_t kFSmem = kFSmemA + kFSmemB + sizeof(uint32_t) * kFTab1 + sizeof(uint16_t) * kFTab2;
+static_assert(kFSmemA >= sizeof(uint32_t) * kFXN, "the x halo fits under z");
+static_assert(kFXChunks <= 2 * kFThreads, "the x halo: two chunks per thread at most");
 static_assert(kFSmemA % 16 == 0, "16-byte aligned h1");
 static_assert(kFThreads == kFT * (kFT / kFStrip), "the gather: one strip per thread");
 constexpr uint32_t kOnesBf16x2 = 0x3F803F80u;  // (1.0, 1.0) in BF16
@@ -491,7 +497,7 @@ FBME_DEV void prior_strip(const float (&o)[kFStrip], float base, float fl, float
 // and partial-sum slots as warm_net_kernel.
 __global__ void __launch_bounds__(kFThreads) warm_map_kernel(const float* map, int H, int W,
                                                             const float* data_power, const float* floor_,
-                                                            float* gamma, double* upart) {
+                                                            float* gamma, double* upart, int nslots) {
   __shared__ double red[32];
   const int b = blockIdx.y;
   const long long img = static_cast<long long>(b) * H * W;
@@ -512,11 +518,20 @@ __global__ void __launch_bounds__(kFThreads) warm_map_kernel(const float* map, i
   }
   const double s = block_sum(acc, red);
   if (threadIdx.x == 0)
-    upart[(static_cast<long long>(b) * kMaxTilesPerScene + blockIdx.x) * kPartSlots] = s;
+    for (int k = blockIdx.x; k < nslots; k += gridDim.x)
+      upart[(static_cast<long long>(b) * kMaxTilesPerScene + k) * kPartSlots] = k == blockIdx.x ? s : 0.0;
+}
+
+// CTAs per scene of the two warm-prior tile kernels: about four tiles each
+// (amortising the per-CTA setup and prefetching the next tile's halo), at
+// most the `nslots` partial-sum slots the initialisation reads.
+inline int warm_ctas(int H, int W, int nslots) {
+  const int ntiles = ((H + kFT - 1) / kFT) * ((W + kFT - 1) / kFT);
+  return std::max(1, std::min(nslots, (ntiles + 3) / 4));
 }
 
 FBME_DEV void mma_bf16_1688(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a0), "r"(a1), "r"(b0));
@@ -550,6 +565,7 @@ struct NetArgs {
   const float* floor_;
   float* gamma;
   double* upart;
+  int nslots;  // partial-sum slots per scene (>= gridDim.x; the rest are zeroed)
   // training: the activations for the backward pass
   __nv_bfloat16* h1;
   __nv_bfloat16* h2;
@@ -563,7 +579,7 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
   extern __shared__ __align__(16) uint8_t fsm[];
   __shared__ double red[32];
   float* z = reinterpret_cast<float*>(fsm);         // [9][kF2N]
-  uint32_t* xs = reinterpret_cast<uint32_t*>(fsm);  // [kFXN] (f0, f1), then ones, zero
+  uint32_t* xs = reinterpret_cast<uint32_t*>(fsm);  // [kFXN] (f0, f1) pairs
   uint4* h1 = reinterpret_cast<uint4*>(fsm + kFSmemA);
   uint32_t* h1w = reinterpret_cast<uint32_t*>(h1);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -601,108 +617,180 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
     base = a.data_power[b] / static_cast<float>(N);
     fl = a.floor_[b];
   }
-  // layer-1 tap offsets in the x halo; layer-2 ldmatrix row of this lane
-  const int o1a = (t4 / 3) * kFXW + t4 % 3, o1b = ((t4 + 4) / 3) * kFXW + (t4 + 4) % 3;
-  constexpr int o8 = 2 * kFXW + 2;
-  const int mj = lane >> 3, pr = (lane & 7) + (mj & 1) * 8;
+  // per-lane constants: layer-1 tap offsets in the x halo and the second k
+  // step's operand where it is not tap 8 (t4 = 1: the bias's ones, t4 > 1:
+  // zero); layer-2 ldmatrix row and tap offsets in h1 (the fifth k step's
+  // odd half reads the ones pixel)
+  const int o1a = (t4 / 3) * kFXP + t4 % 3, o1b = ((t4 + 4) / 3) * kFXP + (t4 + 4) % 3;
+  constexpr int o8 = 2 * kFXP + 2;
+  const uint32_t k1w = t4 == 1 ? kOnesBf16x2 : 0u;
+  const int mj = lane >> 3, pr = (lane & 7) + (mj & 1) * 8, odd = mj >> 1;
+  int o2[KP2 / 16];
+#pragma unroll
+  for (int ks = 0; ks < KP2 / 16; ++ks) {
+    const int tap = 2 * ks + odd;
+    o2[ks] = tap < 9 ? (tap / 3) * kF1W + tap % 3 : 0;
+  }
+  uint32_t* tab1 = reinterpret_cast<uint32_t*>(fsm + kFSmemA + kFSmemB);
+  uint16_t* tab2 = reinterpret_cast<uint16_t*>(tab1 + kFTab1);
+  for (int i = tid; i < kFTab1; i += kFThreads) {
+    const int p0 = (i / 8) * 16 + i % 8, p1 = p0 + 8;
+    // region pixel (ry, rx) reads the halo from (ry, rx + 1): the halo starts a column earlier
+    tab1[i] = static_cast<uint32_t>(p0 / kF1W * kFXP + p0 % kF1W + 1) |
+              (static_cast<uint32_t>(p1 / kF1W * kFXP + p1 % kF1W + 1) << 16);
+  }
+  for (int i = tid; i < kFTab2; i += kFThreads) {
+    const int pa = min(i, kF2N - 1);
+    tab2[i] = static_cast<uint16_t>(pa / kF2W * kF1W + pa % kF2W);
+  }
   if (tid == 0) h1[kF1N] = make_uint4(kOnesBf16x2, 0u, 0u, 0u);
 
   const int tx_n = (W + kFT - 1) / kFT, ntiles = tx_n * ((H + kFT - 1) / kFT);
+  // x halo chunks (4 pixels of one row, 8 bytes of compact f0): a thread
+  // fetches chunks tid and tid + kFThreads of a tile into registers one tile
+  // ahead, so the loads fly while the previous tile computes.  W % 16 == 0,
+  // so a chunk lies wholly inside or wholly outside the image.
+  uint2 hv[2];
+  bool hin[2];
+  auto fetch = [&](int t) {
+    const int fy0 = (t / tx_n) * kFT, fx0 = (t % tx_n) * kFT;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int ch = tid + j * kFThreads, row = ch / (kFXP / 4), k = ch - row * (kFXP / 4);
+      const int gy = fy0 - 3 + row, gx = fx0 - 4 + 4 * k;
+      hin[j] = ch < kFXChunks && in_image(gy, gx, H, W);
+      hv[j] = make_uint2(0u, 0u);
+      if (hin[j]) {
+        const long long e = img + static_cast<long long>(gy) * W + gx;
+        if constexpr (CSTR == 1) {
+          hv[j] = *reinterpret_cast<const uint2*>(a.x + e);
+        } else {
+          const uint16_t* x16 = reinterpret_cast<const uint16_t*>(a.x);
+          hv[j] = make_uint2(x16[e * CSTR] | (static_cast<uint32_t>(x16[(e + 1) * CSTR]) << 16),
+                             x16[(e + 2) * CSTR] | (static_cast<uint32_t>(x16[(e + 3) * CSTR]) << 16));
+        }
+      }
+    }
+  };
   double acc = 0.0;
+  if (blockIdx.x < ntiles) fetch(blockIdx.x);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int y0 = (tile / tx_n) * kFT, x0 = (tile % tx_n) * kFT;
     // the whole halo lies inside the image: no region pixel is padding
     const bool inner = y0 >= 3 && x0 >= 3 && y0 + kFT + 3 <= H && x0 + kFT + 3 <= W;
-    __syncthreads();  // the previous tile's z is read
-    {  // x halo: all of a thread's loads issued before any is stored
-      constexpr int IT = (kFXN + kFThreads - 1) / kFThreads;
-      const uint16_t* x16 = reinterpret_cast<const uint16_t*>(a.x);
-      uint32_t v[IT];
+    __syncthreads();  // the tables are built; the previous tile's z is read
 #pragma unroll
-      for (int j = 0; j < IT; ++j) {
-        const int i = tid + j * kFThreads, iy = i / kFXW;
-        const int gy = y0 - 3 + iy, gx = x0 - 3 + (i - iy * kFXW);
-        v[j] = 0u;
-        if (i < kFXN && in_image(gy, gx, H, W))
-          v[j] = c1hi | x16[(img + static_cast<long long>(gy) * W + gx) * CSTR];
+    for (int j = 0; j < 2; ++j) {  // (f0, f1) pairs, zero outside the image
+      const int ch = tid + j * kFThreads;
+      if (ch < kFXChunks) {
+        const uint32_t m = hin[j] ? c1hi : 0u;
+        reinterpret_cast<uint4*>(xs)[ch] =
+            make_uint4(m | (hv[j].x & 0xFFFFu), m | (hv[j].x >> 16), m | (hv[j].y & 0xFFFFu), m | (hv[j].y >> 16));
       }
+    }
+    if (tile + gridDim.x < ntiles) fetch(tile + gridDim.x);
+    __syncthreads();
+    // layer 1: rows g, g + 8 of fragment f are region pixels f * 16 + g (+ 8);
+    // a warp takes fragments f and f + 8 together (two independent chains)
+    for (int f = warp; f < kFFrag1; f += 2 * (kFThreads / 32)) {
+      const int fb = min(f + kFThreads / 32, kFFrag1 - 1);
+      const uint32_t qa = tab1[f * 8 + g], qb = tab1[fb * 8 + g];
+      const uint32_t *xa0 = xs + (qa & 0xFFFFu), *xa1 = xs + (qa >> 16);
+      const uint32_t *xb0 = xs + (qb & 0xFFFFu), *xb1 = xs + (qb >> 16);
+      float ca[4] = {0.f, 0.f, 0.f, 0.f}, cb[4] = {0.f, 0.f, 0.f, 0.f};
+      mma_bf16_16816(ca, xa0[o1a], xa1[o1a], xa0[o1b], xa1[o1b], l1b0, l1b1);
+      mma_bf16_16816(cb, xb0[o1a], xb1[o1a], xb0[o1b], xb1[o1b], l1b0, l1b1);
+      mma_bf16_16816(ca, t4 == 0 ? xa0[o8] : k1w, t4 == 0 ? xa1[o8] : k1w, 0u, 0u, l1b2, 0u);
+      mma_bf16_16816(cb, t4 == 0 ? xb0[o8] : k1w, t4 == 0 ? xb1[o8] : k1w, 0u, 0u, l1b2, 0u);
+      const int nf = f + kFThreads / 32 < kFFrag1 ? 2 : 1;
 #pragma unroll
-      for (int j = 0; j < IT; ++j) {
-        const int i = tid + j * kFThreads;
-        if (i < kFXN) xs[i] = v[j];
+      for (int u = 0; u < 2; ++u) {
+        if (u >= nf) break;
+        const float* cc = u ? cb : ca;
+        const uint32_t w0 = relu_bf16x2(cc[0], cc[1]), w1 = relu_bf16x2(cc[2], cc[3]);
+        const int p0 = (u ? fb : f) * 16 + g;
+        h1w[p0 * 4 + t4] = w0;
+        h1w[(p0 + 8) * 4 + t4] = w1;
+        if constexpr (TRAIN) {  // the tile's own 32 x 32 pixels
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int pp = p0 + 8 * h, ry = pp / kF1W, rx = pp - ry * kF1W;
+            const int gy = y0 - 2 + ry, gx = x0 - 2 + rx;
+            if (ry >= 2 && ry < kFT + 2 && rx >= 2 && rx < kFT + 2 && in_image(gy, gx, H, W))
+              reinterpret_cast<uint32_t*>(a.h1 + (img + static_cast<long long>(gy) * W + gx) * kHid)[t4] =
+                  h ? w1 : w0;
+          }
+        }
       }
-      if (tid == 0) {
-        xs[kFXN] = kOnesBf16x2;
-        xs[kFXN + 1] = 0u;
+    }
+    if (!inner) {  // region pixels outside the image are the zero padding
+      __syncthreads();
+      for (int i = tid; i < kF1N; i += kFThreads) {
+        const int ry = i / kF1W;
+        if (!in_image(y0 - 2 + ry, x0 - 2 + (i - ry * kF1W), H, W)) h1[i] = make_uint4(0u, 0u, 0u, 0u);
       }
     }
     __syncthreads();
-    // layer 1: rows g, g + 8 of fragment f are region pixels p0, p1; the
-    // second k step holds tap 8 (t4 = 0) and the bias (t4 = 1)
-    for (int f = warp; f < kFFrag1; f += kFThreads / 32) {
-      const int p0 = f * 16 + g, p1 = p0 + 8;
-      const int ry0 = p0 / kF1W, rx0 = p0 - ry0 * kF1W, ry1 = p1 / kF1W, rx1 = p1 - ry1 * kF1W;
-      const int q0 = ry0 * kFXW + rx0, q1 = ry1 * kFXW + rx1;
-      const int i0 = t4 == 0 ? q0 + o8 : kFXN + (t4 > 1), i1 = t4 == 0 ? q1 + o8 : kFXN + (t4 > 1);
-      float c[4] = {0.f, 0.f, 0.f, 0.f};
-      mma_bf16_16816(c, xs[q0 + o1a], xs[q1 + o1a], xs[q0 + o1b], xs[q1 + o1b], l1b0, l1b1);
-      mma_bf16_16816(c, xs[i0], xs[i1], 0u, 0u, l1b2, 0u);
-      const int gy0 = y0 - 2 + ry0, gx0 = x0 - 2 + rx0, gy1 = y0 - 2 + ry1, gx1 = x0 - 2 + rx1;
-      const bool in0 = inner || in_image(gy0, gx0, H, W), in1 = inner || in_image(gy1, gx1, H, W);
-      const uint32_t w0 = in0 ? relu_bf16x2(c[0], c[1]) : 0u, w1 = in1 ? relu_bf16x2(c[2], c[3]) : 0u;
-      h1w[p0 * 4 + t4] = w0;
-      h1w[p1 * 4 + t4] = w1;
-      if constexpr (TRAIN) {  // the tile's own 32 x 32 pixels
-        if (in0 && ry0 >= 2 && ry0 < kFT + 2 && rx0 >= 2 && rx0 < kFT + 2)
-          reinterpret_cast<uint32_t*>(a.h1 + (img + static_cast<long long>(gy0) * W + gx0) * kHid)[t4] = w0;
-        if (in1 && ry1 >= 2 && ry1 < kFT + 2 && rx1 >= 2 && rx1 < kFT + 2)
-          reinterpret_cast<uint32_t*>(a.h1 + (img + static_cast<long long>(gy1) * W + gx1) * kHid)[t4] = w1;
-      }
-    }
-    __syncthreads();
-    // layer 2 and the per-pixel tap products of layer 3
-    for (int f = warp; f < kFFrag2; f += kFThreads / 32) {
-      const int pa = min(f * 16 + pr, kF2N - 1);
-      const int ay = pa / kF2W;
-      const int abase = ay * kF1W + (pa - ay * kF2W);
-      float c[4] = {0.f, 0.f, 0.f, 0.f};
+    // layer 2 and the per-pixel tap products of layer 3, fragments f and
+    // f + 8 together
+    for (int f = warp; f < kFFrag2; f += 2 * (kFThreads / 32)) {
+      const int fb = min(f + kFThreads / 32, kFFrag2 - 1);
+      const uint4* ha = h1 + tab2[f * 16 + pr];
+      const uint4* hb = h1 + tab2[fb * 16 + pr];
+      float ca[4] = {0.f, 0.f, 0.f, 0.f}, cb[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int ks = 0; ks < KP2 / 16; ++ks) {
-        const int tap = 2 * ks + (mj >> 1);
-        const int pix = tap < 9 ? abase + (tap / 3) * kF1W + tap % 3 : kF1N;
-        uint32_t a0, a1, a2, a3;
-        ldmatrix_x4(smem_u32(&h1[pix]), a0, a1, a2, a3);
-        mma_bf16_16816(c, a0, a1, a2, a3, bq[ks][0], bq[ks][1]);
+        const bool ones = ks == KP2 / 16 - 1 && odd;
+        uint32_t a0, a1, a2, a3, b0, b1, b2, b3v;
+        ldmatrix_x4(smem_u32(ones ? h1 + kF1N : ha + o2[ks]), a0, a1, a2, a3);
+        ldmatrix_x4(smem_u32(ones ? h1 + kF1N : hb + o2[ks]), b0, b1, b2, b3v);
+        mma_bf16_16816(ca, a0, a1, a2, a3, bq[ks][0], bq[ks][1]);
+        mma_bf16_16816(cb, b0, b1, b2, b3v, bq[ks][0], bq[ks][1]);
       }
-      const int q0 = f * 16 + g, q1 = q0 + 8;
-      const int sy0 = q0 / kF2W, sx0 = q0 - sy0 * kF2W, sy1 = q1 / kF2W, sx1 = q1 - sy1 * kF2W;
-      const int gy0 = y0 - 1 + sy0, gx0 = x0 - 1 + sx0, gy1 = y0 - 1 + sy1, gx1 = x0 - 1 + sx1;
-      const bool in0 = q0 < kF2N && (inner || in_image(gy0, gx0, H, W));
-      const bool in1 = q1 < kF2N && (inner || in_image(gy1, gx1, H, W));
-      const uint32_t u0 = in0 ? relu_bf16x2(c[0], c[1]) : 0u, u1 = in1 ? relu_bf16x2(c[2], c[3]) : 0u;
-      if constexpr (TRAIN) {
-        if (in0 && sy0 >= 1 && sy0 <= kFT && sx0 >= 1 && sx0 <= kFT)
-          reinterpret_cast<uint32_t*>(a.h2 + (img + static_cast<long long>(gy0) * W + gx0) * kHid)[t4] = u0;
-        if (in1 && sy1 >= 1 && sy1 <= kFT && sx1 >= 1 && sx1 <= kFT)
-          reinterpret_cast<uint32_t*>(a.h2 + (img + static_cast<long long>(gy1) * W + gx1) * kHid)[t4] = u1;
-      }
-      // the accumulator fragment (rows g, g + 8; channels 2 t4, 2 t4 + 1) is
-      // the A fragment of m16n8k8: z for taps 0-7, then tap 8
-      float za[4] = {0.f, 0.f, 0.f, 0.f}, zb[4] = {0.f, 0.f, 0.f, 0.f};
-      mma_bf16_1688(za, u0, u1, bz0);
-      mma_bf16_1688(zb, u0, u1, bz1);
-      if (q0 < kF2N) {
-        z[(2 * t4) * kF2N + q0] = za[0];
-        z[(2 * t4 + 1) * kF2N + q0] = za[1];
-        if (t4 == 0) z[8 * kF2N + q0] = zb[0];
-      }
-      if (q1 < kF2N) {
-        z[(2 * t4) * kF2N + q1] = za[2];
-        z[(2 * t4 + 1) * kF2N + q1] = za[3];
-        if (t4 == 0) z[8 * kF2N + q1] = zb[2];
+      const int nf = f + kFThreads / 32 < kFFrag2 ? 2 : 1;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        if (u >= nf) break;
+        const float* cc = u ? cb : ca;
+        const uint32_t u0 = relu_bf16x2(cc[0], cc[1]), u1 = relu_bf16x2(cc[2], cc[3]);
+        const int q0 = (u ? fb : f) * 16 + g;
+        if constexpr (TRAIN) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int q = q0 + 8 * h, sy = q / kF2W, sx = q - sy * kF2W;
+            const int gy = y0 - 1 + sy, gx = x0 - 1 + sx;
+            if (q < kF2N && sy >= 1 && sy <= kFT && sx >= 1 && sx <= kFT && in_image(gy, gx, H, W))
+              reinterpret_cast<uint32_t*>(a.h2 + (img + static_cast<long long>(gy) * W + gx) * kHid)[t4] =
+                  h ? u1 : u0;
+          }
+        }
+        // the accumulator fragment (rows g, g + 8; channels 2 t4, 2 t4 + 1)
+        // is the A fragment of m16n8k8: z for taps 0-7, then tap 8
+        float za[4] = {0.f, 0.f, 0.f, 0.f}, zb[4] = {0.f, 0.f, 0.f, 0.f};
+        mma_bf16_1688(za, u0, u1, bz0);
+        mma_bf16_1688(zb, u0, u1, bz1);
+        if (q0 < kF2N) {
+          z[(2 * t4) * kF2N + q0] = za[0];
+          z[(2 * t4 + 1) * kF2N + q0] = za[1];
+          if (t4 == 0) z[8 * kF2N + q0] = zb[0];
+        }
+        if (q0 + 8 < kF2N) {
+          z[(2 * t4) * kF2N + q0 + 8] = za[2];
+          z[(2 * t4 + 1) * kF2N + q0 + 8] = za[3];
+          if (t4 == 0) z[8 * kF2N + q0 + 8] = zb[2];
+        }
       }
     }
     __syncthreads();
+    if (!inner) {  // h2 outside the image is zero padding: so are its tap products
+      for (int i = tid; i < kF2N; i += kFThreads) {
+        const int sy = i / kF2W;
+        if (!in_image(y0 - 1 + sy, x0 - 1 + (i - sy * kF2W), H, W))
+#pragma unroll
+          for (int tap = 0; tap < 9; ++tap) z[tap * kF2N + i] = 0.f;
+      }
+      __syncthreads();
+    }
     {  // layer 3: out = sum over the taps (in order) + b3
       const int col = tid % kFT, r0 = (tid / kFT) * kFStrip;
       float o[kFStrip];
@@ -728,9 +816,12 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
   }
   if constexpr (!TRAIN) {
     const double sum = block_sum(acc, red);
-    if (tid == 0) a.upart[(static_cast<long long>(b) * kMaxTilesPerScene + blockIdx.x) * kPartSlots] = sum;
+    if (tid == 0)
+      for (int k = blockIdx.x; k < a.nslots; k += gridDim.x)
+        a.upart[(static_cast<long long>(b) * kMaxTilesPerScene + k) * kPartSlots] = k == blockIdx.x ? sum : 0.0;
   }
 }
+
 }  // namespace cnn
 }  // namespace fbme
 
@@ -936,13 +1027,15 @@ void cnn_warm_prior(const float* params, const float2* bp, int B, int H, int W, 
   na.floor_ = floor_;
   na.gamma = gamma;
   na.upart = upart;
-  net_tile_kernel<false, 1><<<dim3(nblocks, B), kFThreads, kFSmem, st>>>(na);
+  na.nslots = nblocks;
+  net_tile_kernel<false, 1><<<dim3(warm_ctas(H, W, nblocks), B), kFThreads, kFSmem, st>>>(na);
 }
 
 void warm_prior_from_map(const float* map, int B, int H, int W, const float* data_power, const float* floor_,
                          float* gamma, double* upart, int nblocks, cudaStream_t st) {
   using namespace cnn;
-  warm_map_kernel<<<dim3(nblocks, B), kFThreads, 0, st>>>(map, H, W, data_power, floor_, gamma, upart);
+  warm_map_kernel<<<dim3(warm_ctas(H, W, nblocks), B), kFThreads, 0, st>>>(map, H, W, data_power, floor_, gamma,
+                                                                          upart, nblocks);
 }
 
 cudaError_t set_cnn_attributes() {
