@@ -241,6 +241,9 @@ FBME_DEV void ldmatrix_x4(uint32_t addr, uint32_t& a0, uint32_t& a1, uint32_t& a
                : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
                : "r"(addr));
 }
+FBME_DEV void ldmatrix_x2(uint32_t addr, uint32_t& a0, uint32_t& a1) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(a0), "=r"(a1) : "r"(addr));
+}
 
 
 
@@ -439,43 +442,42 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
 //   x  : the f0 halo, 38 x 38 pixels of (f0, f1) BF16 pairs (f1 = the
 //        scene constant), zero outside the image;
 //   h1 : layer 1 on the 36 x 36 region, 16-pixel fragments in raster
-//        order, K = (tap, channel) = 18 plus the bias (below), padded to 32;
+//        order, K = (tap, channel) = 18, padded to 32;
 //   h2 : layer 2 on the 34 x 34 region, A fragments by ldmatrix from h1
-//        (as conv3x3_kernel), K = 72 plus the bias, padded to 80;
+//        (as conv3x3_kernel), K = 72 (four m16n8k16 steps and an m16n8k8);
 //   z  : the accumulator fragment of layer 2, relu'd and rounded to BF16,
 //        is the A fragment of an m16n8k8 product with W3 (K = 8 channels,
 //        N = 9 taps): z[tap][q] = sum_c W3[tap][c] h2[q][c];
 //   out: b3 + sum over the 9 taps of z[tap][q + shift(tap)].
-// Biases ride in the products: an input slot of ones (x: pair slot 9;
-// h1: channels 0-1 of a constant pixel) meets the bias split into BF16
-// hi + lo parts (hi + lo = the FP32 bias to 2^-16 relative).  Region
-// pixels outside the image are zero, as the convolution's zero padding
+// Biases are the accumulators' initial values (FP32).  Region pixels
+// outside the image are zero, as the convolution's zero padding
 // reads them.  Inference writes prior0 = max(data_power / N * exp(out),
 // floor) and its partial sums; training writes h1, h2 (NHWC BF16) and out
 // (FP32) for the backward pass.  Traffic: 2 bytes of f0 read and 4 bytes
 // of prior written per pixel.
 // ---------------------------------------------------------------------------
 constexpr int kFT = 32, kFThreads = 256, kFStrip = 4;   // the gather: 4-row strips per thread
-constexpr int kFXH = kFT + 6, kFXP = kFT + 8;           // x halo: 38 rows of 40 (columns x0 - 4 ...)
-constexpr int kFXN = kFXH * kFXP, kFXChunks = kFXH * (kFXP / 4);  // 4-pixel chunks
+// x halo: 38 rows of 40 pixels (columns x0 - 4 ...), in rows of 48 words
+// (48 = 16 mod 32 banks: layer 1's taps of 8 pixels fall on distinct banks)
+constexpr int kFXH = kFT + 6, kFXC = kFT + 8, kFXP = 48;
+constexpr int kFXN = kFXH * kFXP, kFXChunks = kFXH * (kFXC / 4);  // 4-pixel chunks
 constexpr int kF1W = kFT + 4, kF1N = kF1W * kF1W;       // h1 region
 constexpr int kF2W = kFT + 2, kF2N = kF2W * kF2W;       // h2 / z region
 constexpr int kFFrag1 = (kF1N + 15) / 16, kFFrag2 = (kF2N + 15) / 16;
 // dynamic shared memory: z [9][kF2N] FP32 (the x halo [kFXN] BF16 pairs
-// lies under it until layer 1 is done; its rows are 16-byte aligned), h1 [kF1N + 1] NHWC BF16 pixels (the
-// last one (1, 1, 0, ...)), then two address tables built once per CTA:
+// lies under it until layer 1 is done; its rows are 16-byte aligned), h1
+// [kF1N] NHWC BF16 pixels, then two address tables built once per CTA:
 // layer 1, per fragment and row g < 8, the halo indices of its pixels g and
 // g + 8 (16 bits each); layer 2, per fragment and row, the h1 index of the
 // pixel's first tap (16 bits).
 constexpr int kFTab1 = kFFrag1 * 8, kFTab2 = kFFrag2 * 16;
 constexpr size_t kFSmemA = sizeof(float) * 9 * kF2N;
-constexpr size_t kFSmemB = sizeof(uint4) * (kF1N + 1);
+constexpr size_t kFSmemB = sizeof(uint4) * kF1N;
 constexpr size_t kFSmem = kFSmemA + kFSmemB + sizeof(uint32_t) * kFTab1 + sizeof(uint16_t) * kFTab2;
 static_assert(kFSmemA >= sizeof(uint32_t) * kFXN, "the x halo fits under z");
 static_assert(kFXChunks <= 2 * kFThreads, "the x halo: two chunks per thread at most");
 static_assert(kFSmemA % 16 == 0, "16-byte aligned h1");
 static_assert(kFThreads == kFT * (kFT / kFStrip), "the gather: one strip per thread");
-constexpr uint32_t kOnesBf16x2 = 0x3F803F80u;  // (1.0, 1.0) in BF16
 
 // Prior of the strip (gy0 + p, gx), p < kFStrip, from the network outputs
 // o[p]: stores gamma and adds the priors to acc in pixel order (both
@@ -537,12 +539,6 @@ FBME_DEV void mma_bf16_1688(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0
       : "r"(a0), "r"(a1), "r"(b0));
 }
 
-// An FP32 value as a BF16 pair (hi, lo) with hi + lo equal to it to 2^-16.
-FBME_DEV uint32_t bf16_hi_lo(float v) {
-  const float hi = __bfloat162float(__float2bfloat16_rn(v));
-  return pack_bf16x2(hi, v - hi);
-}
-
 // relu(BF16(a)), relu(BF16(b)) as a BF16 pair.
 FBME_DEV uint32_t relu_bf16x2(float a, float b) {
   __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
@@ -594,42 +590,40 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
   const uint32_t l1b0 = pack_bf16x2(p[kOffW1 + (t4 * kIn) * kHid + g], p[kOffW1 + (t4 * kIn + 1) * kHid + g]);
   const uint32_t l1b1 =
       pack_bf16x2(p[kOffW1 + ((t4 + 4) * kIn) * kHid + g], p[kOffW1 + ((t4 + 4) * kIn + 1) * kHid + g]);
-  const uint32_t l1b2 = t4 == 0   ? pack_bf16x2(p[kOffW1 + (8 * kIn) * kHid + g], p[kOffW1 + (8 * kIn + 1) * kHid + g])
-                        : t4 == 1 ? bf16_hi_lo(p[kOffB1 + g])
-                                  : 0u;
+  const uint32_t l1b2 =
+      t4 == 0 ? pack_bf16x2(p[kOffW1 + (8 * kIn) * kHid + g], p[kOffW1 + (8 * kIn + 1) * kHid + g]) : 0u;
   constexpr int KP2 = kpad(kHid);
   uint32_t bq[KP2 / 16][2];
 #pragma unroll
   for (int ks = 0; ks < KP2 / 16; ++ks)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int k = ks * 16 + 2 * t4 + 8 * h;  // k = tap * 8 + channel; 72: the bias
-      bq[ks][h] = k < 9 * kHid ? pack_bf16x2(p[kOffW2 + k * kHid + g], p[kOffW2 + (k + 1) * kHid + g])
-                  : k == 9 * kHid ? bf16_hi_lo(p[kOffB2 + g])
-                                  : 0u;
+      const int k = ks * 16 + 2 * t4 + 8 * h;  // k = tap * 8 + channel
+      bq[ks][h] = k < 9 * kHid ? pack_bf16x2(p[kOffW2 + k * kHid + g], p[kOffW2 + (k + 1) * kHid + g]) : 0u;
     }
   const uint32_t bz0 = pack_bf16x2(p[kOffW3 + g * kHid + 2 * t4], p[kOffW3 + g * kHid + 2 * t4 + 1]);
   const uint32_t bz1 =
       g == 0 ? pack_bf16x2(p[kOffW3 + 8 * kHid + 2 * t4], p[kOffW3 + 8 * kHid + 2 * t4 + 1]) : 0u;
   const float b3 = p[kOffB3];
+  // biases of this lane's accumulator columns (channels 2 t4, 2 t4 + 1)
+  const float b1a = p[kOffB1 + 2 * t4], b1b = p[kOffB1 + 2 * t4 + 1];
+  const float b2a = p[kOffB2 + 2 * t4], b2b = p[kOffB2 + 2 * t4 + 1];
   float base = 0.f, fl = 0.f;
   if constexpr (!TRAIN) {
     base = a.data_power[b] / static_cast<float>(N);
     fl = a.floor_[b];
   }
-  // per-lane constants: layer-1 tap offsets in the x halo and the second k
-  // step's operand where it is not tap 8 (t4 = 1: the bias's ones, t4 > 1:
-  // zero); layer-2 ldmatrix row and tap offsets in h1 (the fifth k step's
-  // odd half reads the ones pixel)
+  // per-lane constants: layer-1 tap offsets in the x halo (the second k
+  // step holds tap 8 in lanes t4 = 0, zero elsewhere); layer-2 ldmatrix row
+  // and tap offsets in h1 (the fifth k step is tap 8 alone)
   const int o1a = (t4 / 3) * kFXP + t4 % 3, o1b = ((t4 + 4) / 3) * kFXP + (t4 + 4) % 3;
   constexpr int o8 = 2 * kFXP + 2;
-  const uint32_t k1w = t4 == 1 ? kOnesBf16x2 : 0u;
   const int mj = lane >> 3, pr = (lane & 7) + (mj & 1) * 8, odd = mj >> 1;
   int o2[KP2 / 16];
 #pragma unroll
   for (int ks = 0; ks < KP2 / 16; ++ks) {
     const int tap = 2 * ks + odd;
-    o2[ks] = tap < 9 ? (tap / 3) * kF1W + tap % 3 : 0;
+    o2[ks] = tap < 9 ? (tap / 3) * kF1W + tap % 3 : 2 * kF1W + 2;  // x2 load: upper lanes unused
   }
   uint32_t* tab1 = reinterpret_cast<uint32_t*>(fsm + kFSmemA + kFSmemB);
   uint16_t* tab2 = reinterpret_cast<uint16_t*>(tab1 + kFTab1);
@@ -643,7 +637,6 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
     const int pa = min(i, kF2N - 1);
     tab2[i] = static_cast<uint16_t>(pa / kF2W * kF1W + pa % kF2W);
   }
-  if (tid == 0) h1[kF1N] = make_uint4(kOnesBf16x2, 0u, 0u, 0u);
 
   const int tx_n = (W + kFT - 1) / kFT, ntiles = tx_n * ((H + kFT - 1) / kFT);
   // x halo chunks (4 pixels of one row, 8 bytes of compact f0): a thread
@@ -656,7 +649,7 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
     const int fy0 = (t / tx_n) * kFT, fx0 = (t % tx_n) * kFT;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const int ch = tid + j * kFThreads, row = ch / (kFXP / 4), k = ch - row * (kFXP / 4);
+      const int ch = tid + j * kFThreads, row = ch / (kFXC / 4), k = ch - row * (kFXC / 4);
       const int gy = fy0 - 3 + row, gx = fx0 - 4 + 4 * k;
       hin[j] = ch < kFXChunks && in_image(gy, gx, H, W);
       hv[j] = make_uint2(0u, 0u);
@@ -681,10 +674,10 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
     __syncthreads();  // the tables are built; the previous tile's z is read
 #pragma unroll
     for (int j = 0; j < 2; ++j) {  // (f0, f1) pairs, zero outside the image
-      const int ch = tid + j * kFThreads;
+      const int ch = tid + j * kFThreads, row = ch / (kFXC / 4);
       if (ch < kFXChunks) {
         const uint32_t m = hin[j] ? c1hi : 0u;
-        reinterpret_cast<uint4*>(xs)[ch] =
+        reinterpret_cast<uint4*>(xs + row * kFXP)[ch - row * (kFXC / 4)] =
             make_uint4(m | (hv[j].x & 0xFFFFu), m | (hv[j].x >> 16), m | (hv[j].y & 0xFFFFu), m | (hv[j].y >> 16));
       }
     }
@@ -697,11 +690,11 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
       const uint32_t qa = tab1[f * 8 + g], qb = tab1[fb * 8 + g];
       const uint32_t *xa0 = xs + (qa & 0xFFFFu), *xa1 = xs + (qa >> 16);
       const uint32_t *xb0 = xs + (qb & 0xFFFFu), *xb1 = xs + (qb >> 16);
-      float ca[4] = {0.f, 0.f, 0.f, 0.f}, cb[4] = {0.f, 0.f, 0.f, 0.f};
+      float ca[4] = {b1a, b1b, b1a, b1b}, cb[4] = {b1a, b1b, b1a, b1b};
       mma_bf16_16816(ca, xa0[o1a], xa1[o1a], xa0[o1b], xa1[o1b], l1b0, l1b1);
       mma_bf16_16816(cb, xb0[o1a], xb1[o1a], xb0[o1b], xb1[o1b], l1b0, l1b1);
-      mma_bf16_16816(ca, t4 == 0 ? xa0[o8] : k1w, t4 == 0 ? xa1[o8] : k1w, 0u, 0u, l1b2, 0u);
-      mma_bf16_16816(cb, t4 == 0 ? xb0[o8] : k1w, t4 == 0 ? xb1[o8] : k1w, 0u, 0u, l1b2, 0u);
+      mma_bf16_16816(ca, t4 == 0 ? xa0[o8] : 0u, t4 == 0 ? xa1[o8] : 0u, 0u, 0u, l1b2, 0u);
+      mma_bf16_16816(cb, t4 == 0 ? xb0[o8] : 0u, t4 == 0 ? xb1[o8] : 0u, 0u, 0u, l1b2, 0u);
       const int nf = f + kFThreads / 32 < kFFrag1 ? 2 : 1;
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
@@ -737,15 +730,21 @@ __global__ void __launch_bounds__(kFThreads, 3) net_tile_kernel(NetArgs a) {
       const int fb = min(f + kFThreads / 32, kFFrag2 - 1);
       const uint4* ha = h1 + tab2[f * 16 + pr];
       const uint4* hb = h1 + tab2[fb * 16 + pr];
-      float ca[4] = {0.f, 0.f, 0.f, 0.f}, cb[4] = {0.f, 0.f, 0.f, 0.f};
+      float ca[4] = {b2a, b2b, b2a, b2b}, cb[4] = {b2a, b2b, b2a, b2b};
 #pragma unroll
-      for (int ks = 0; ks < KP2 / 16; ++ks) {
-        const bool ones = ks == KP2 / 16 - 1 && odd;
+      for (int ks = 0; ks < KP2 / 16 - 1; ++ks) {
         uint32_t a0, a1, a2, a3, b0, b1, b2, b3v;
-        ldmatrix_x4(smem_u32(ones ? h1 + kF1N : ha + o2[ks]), a0, a1, a2, a3);
-        ldmatrix_x4(smem_u32(ones ? h1 + kF1N : hb + o2[ks]), b0, b1, b2, b3v);
+        ldmatrix_x4(smem_u32(ha + o2[ks]), a0, a1, a2, a3);
+        ldmatrix_x4(smem_u32(hb + o2[ks]), b0, b1, b2, b3v);
         mma_bf16_16816(ca, a0, a1, a2, a3, bq[ks][0], bq[ks][1]);
         mma_bf16_16816(cb, b0, b1, b2, b3v, bq[ks][0], bq[ks][1]);
+      }
+      {  // tap 8 (k 64-71): pixels 0-7 and 8-15 of the fragment
+        uint32_t a0, a1, b0, b1;
+        ldmatrix_x2(smem_u32(ha + o2[KP2 / 16 - 1]), a0, a1);
+        ldmatrix_x2(smem_u32(hb + o2[KP2 / 16 - 1]), b0, b1);
+        mma_bf16_1688(ca, a0, a1, bq[KP2 / 16 - 1][0]);
+        mma_bf16_1688(cb, b0, b1, bq[KP2 / 16 - 1][0]);
       }
       const int nf = f + kFThreads / 32 < kFFrag2 ? 2 : 1;
 #pragma unroll
