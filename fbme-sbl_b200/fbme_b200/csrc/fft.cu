@@ -369,6 +369,7 @@ FBME_DEV void cp_async8(float2* dst, const float2* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 FBME_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+FBME_DEV void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 template <int N>
 FBME_DEV void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -413,6 +414,26 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
       fast_issue<L>(st, io, t + gridDim.x, fsm + ((it + 1) & 1) * BUF, lr, p);
     else
       cp_async_commit();  // empty group: the wait below counts the same
+    if constexpr (EPI != 0) {
+      // the next tile's epilogue operands (observations; prior, mean and
+      // variance) into L2, one line per output column and array, so their
+      // DRAM reads overlap this tile's transform
+      const int tn = t + gridDim.x;
+      if (tn < total) {
+        const int un = tn / st.tiles;
+        const long long bn = un * st.out_stride + static_cast<long long>(tn - un * st.tiles) * ROWS;
+        for (int c = threadIdx.x; c < st.cols; c += kFftThreads) {
+          const long long o = bn + static_cast<long long>(c) * st.out_ld;
+          if constexpr (EPI == 1) {
+            prefetch_l2(io.y + o);
+          } else {
+            prefetch_l2(io.dn.gamma + o);
+            prefetch_l2(io.dn.mu + o);
+            prefetch_l2(io.dn.var + o);
+          }
+        }
+      }
+    }
     cp_async_wait<1>();   // this thread's copies of tile t (it reads only its own)
     const int unit = t / st.tiles, tile = t - unit * st.tiles;
     const int r0 = tile * ROWS;
