@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
     // four pixels a step: two 16-byte loads, one 8-byte store of BF16 f0
     const float4* src = reinterpret_cast<const float4*>(bp + b * N);
     uint2* dst = reinterpret_cast<uint2*>(x8 + b * N);
+#pragma unroll 4
     for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < N / 4;
          q += static_cast<long long>(gridDim.x) * blockDim.x) {
       const float4 u = src[2 * q], w = src[2 * q + 1];
@@ -408,6 +409,7 @@ __global__ void __launch_bounds__(256) features_kernel(int pass, const float2* b
     if (threadIdx.x == 0) part[b * 128 + pass * 64 + blockIdx.x] = sum;
     return;
   }
+#pragma unroll 4
   for (long long n = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; n < N;
        n += static_cast<long long>(gridDim.x) * blockDim.x) {
     const float2 v = bp[b * N + n];
@@ -895,8 +897,10 @@ const char* cnn_check(long long B, long long H, long long W) {
 }
 
 namespace {
+// Blocks (and FP64 partials) per scene of a feature pass: a block takes
+// 4096 pixels or more, 16 a thread, so its loads overlap.
 int feature_parts(int H, int W) {
-  return static_cast<int>(std::min<long long>(64, (static_cast<long long>(H) * W + 255) / 256));
+  return static_cast<int>(std::min<long long>(16, (static_cast<long long>(H) * W + 4095) / 4096));
 }
 // Passes 0 and 1 (the energy mean, f0 and its partial sums); pass 2 stores
 // the f1 channel, which only the backward pass reads from the workspace.
