@@ -235,7 +235,9 @@ def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
     sparsity 1-3 %, SNR U[5, 25] dB (every scene its own shape).  Scenes/s
     of one captured uneven plan, and of one single-scene plan per scene
     replayed in turn (the only way to solve such a batch with equal-shape
-    plans); the two give bit-identical results."""
+    plans); the two give bit-identical results.  For scale, the rate of
+    one equal-shape plan of 64 scenes of the headline shape."""
+    import numpy as np
     import torch
 
     from fbme_b200 import scenes
@@ -267,6 +269,12 @@ def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
             q.replay()
 
     r_single = rate(one_by_one, max(2, steps // 10))
+    # for scale: one equal-shape plan of 64 scenes of the headline shape
+    # (256x256 / 128x128)
+    eq = [scenes.config_scene("c2", 5_000_000 + i) for i in range(n_scenes)]
+    y_eq = torch.from_numpy(np.stack([s.y for s in eq])).to(device)
+    eq_plan = make_stable_plan(y_eq, GRID, warmup=1)
+    r_equal = rate(lambda: eq_plan.replay(y_eq), steps)
     return {
         "workload": f"{n_scenes} uneven scenes, grids from {{128x128, 192x256, 256x256, 384x256}}, "
                     "prefix ratio U[0.3,0.7] per axis, 1-3 % CN(0,1) points, SNR U[5,25] dB",
@@ -274,6 +282,11 @@ def uneven_section(device, steps: int, n_scenes: int = 64) -> dict:
         "uneven_plan_scenes_per_s": r_uneven,
         "single_scene_plans_scenes_per_s": r_single,
         "uneven_vs_single_scene_plans": r_uneven / r_single,
+        "equal_shape_plan_scenes_per_s": r_equal,
+        "equal_shape_workload": f"{n_scenes} scenes of 256x256 / 128x128 in one equal-shape plan",
+        "uneven_vs_equal_shape": r_uneven / r_equal,
+        "dft_form": "FP32 FFT stages" if int(plan.engine.native_cfg.dft_terms) == 0
+                    else "split-BF16 tensor-core stages",
     }
 
 

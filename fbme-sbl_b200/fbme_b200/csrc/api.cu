@@ -316,8 +316,6 @@ int plan_spec(const FbmeShape* shapes, int n, const FbmeConfig* c, const FbmeSha
     if (rc != FBME_OK) return rc;
     if (nb > 1 && (k.cfg.polish_size != c->polish_size || k.cfg.polish_iterations != c->polish_iterations))
       return fail(FBME_ERR_INVALID, "an uneven plan needs one polish size and iteration count");
-    if (nb > 1 && k.cfg.dft_terms == 0)
-      return fail(FBME_ERR_UNSUPPORTED, "the FP32 FFT mode (dft_terms 0) is built for equal-shape plans");
     k.tables.n_tile = nt;
     k.L = make_layout(k.s, k.cfg, nt);
     k.base = off;
@@ -864,7 +862,8 @@ void replay_uneven(FbmePlan* P, const float2* y, const FbmeOutputs& out, cudaStr
     jobs[b] = fbme::UampJob{k.s, k.tables, k.dc, k.u};
     jobs[b].u.y = ybuf + k.smp0;
   }
-  fbme::uamp_run_multi(jobs.data(), nb, st, prof);
+  fbme::uamp_run_multi(jobs.data(), nb, st, prof, P->streams.data(), P->events.data(),
+                       static_cast<int>(P->streams.size()));
   if (!prof) {
     cudaEventRecord(P->events[0], st);
     for (int b = 1; b < nb; ++b) cudaStreamWaitEvent(P->streams[b - 1], P->events[0], 0);

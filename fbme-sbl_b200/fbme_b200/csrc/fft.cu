@@ -148,6 +148,34 @@ struct FftIo {
   DenoiseArgs dn;         // mode 3
 };
 
+// The stages of one launch of the two-pass kernel: item i owns the launch's
+// tiles [tile0[i], tile0[i + 1]) (one item: a single stage; several: the
+// same-length stages of an uneven plan's shape buckets, each computed
+// exactly as its own launch computes it).
+constexpr int kFftSetMax = 64;
+template <int NMAX>
+struct FftSet {
+  int n;
+  int tile0[NMAX + 1];
+  FftStage st[NMAX];
+  FftIo io[NMAX];
+};
+
+template <int NMAX>
+FBME_DEV int fft_set_item(const FftSet<NMAX>& set, int t) {
+  if constexpr (NMAX == 1) {
+    return 0;
+  } else {
+    int lo = 0, hi = set.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (set.tile0[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+}
+
 __global__ void __launch_bounds__(kFftThreads) fft_stage_kernel(const FftStage S, const FftIo io) {
   extern __shared__ float2 fsm[];
   const int unit = blockIdx.y, tile = blockIdx.x;
@@ -379,7 +407,7 @@ FBME_DEV void cp_async_wait() {
 // x[p + P q] of row lr with p + P q < K (the rest of the row is zero and is
 // never copied); one commit group.
 template <int L>
-FBME_DEV void fast_issue(const FftStage& st, const FftIo& io, int t, float2* buf, int lr, int p) {
+FBME_DEV void fast_issue(const FftStage& st, const FftIo& io, int t, float2* buf, int lr, int p) {  // t: the item's tile
   constexpr int P = fast_threads_per_row(L), Q = L / P, ROWS = kFftThreads / P, A = fast_row_area(L);
   const int unit = t / st.tiles, tile = t - unit * st.tiles;
   const int r = tile * ROWS + lr;
@@ -619,6 +647,242 @@ __global__ void __launch_bounds__(kFftThreads, 2) fft_fast_kernel(const FftStage
   cp_async_wait<0>();
 }
 
+// The same kernel over a set of same-length stages (uneven plans' shape
+// buckets): tile t belongs to the item whose tile range holds it, and is
+// computed exactly as that item's own launch computes it.  A separate
+// kernel, so that the single-stage kernel keeps its code.
+template <int L, int S, int EPI, int NMAX>
+__global__ void __launch_bounds__(kFftThreads, 2) fft_fast_set_kernel(const FftSet<NMAX> set) {
+  constexpr int P = fast_threads_per_row(L), Q = L / P, ROWS = kFftThreads / P;
+  constexpr int J = (Q + P - 1) / P;     // output columns k1 per thread in pass 2
+  constexpr int A = fast_row_area(L);    // row stride of a buffer
+  constexpr int BUF = ROWS * A;
+  extern __shared__ float2 fsm[];
+  const int lr = threadIdx.x / P, p = threadIdx.x % P;
+  const int total = set.tile0[set.n];
+  int t = blockIdx.x;
+  if (t < total) {
+    const int i = fft_set_item(set, t);
+    fast_issue<L>(set.st[i], set.io[i], t - set.tile0[i], fsm, lr, p);
+  }
+  for (int it = 0; t < total; ++it, t += gridDim.x) {
+    const int item = fft_set_item(set, t);
+    const FftStage& st = set.st[item];
+    const FftIo& io = set.io[item];
+    float2* buf = fsm + (it & 1) * BUF;
+    const int tn = t + gridDim.x;
+    if (tn < total) {
+      const int in_ = fft_set_item(set, tn);
+      const FftStage& sn = set.st[in_];
+      const int tl = tn - set.tile0[in_];
+      fast_issue<L>(sn, set.io[in_], tl, fsm + ((it + 1) & 1) * BUF, lr, p);
+      if constexpr (EPI != 0) {
+        // the next tile's epilogue operands (observations; prior, mean and
+        // variance) into L2, one line per output column and array, so their
+        // DRAM reads overlap this tile's transform
+        const FftIo& ion = set.io[in_];
+        const int un = tl / sn.tiles;
+        const long long bn = un * sn.out_stride + static_cast<long long>(tl - un * sn.tiles) * ROWS;
+        for (int c = threadIdx.x; c < sn.cols; c += kFftThreads) {
+          const long long o = bn + static_cast<long long>(c) * sn.out_ld;
+          if constexpr (EPI == 1) {
+            prefetch_l2(ion.y + o);
+          } else {
+            prefetch_l2(ion.dn.gamma + o);
+            prefetch_l2(ion.dn.mu + o);
+            prefetch_l2(ion.dn.var + o);
+          }
+        }
+      }
+    } else {
+      cp_async_commit();  // empty group: the wait below counts the same
+    }
+    cp_async_wait<1>();   // this thread's copies of tile t (it reads only its own)
+    const int tloc = t - set.tile0[item];
+    const int unit = tloc / st.tiles, tile = tloc - unit * st.tiles;
+    const int r0 = tile * ROWS;
+    const bool live = r0 + lr < st.rows;
+    float2* ya = buf + lr * A;
+
+    // pass 1: DFT-Q of x[p + P q] in registers
+    float2 v[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      v[q] = (live && p + P * q < st.kin) ? ya[p + P * q] : make_float2(0.f, 0.f);
+    if (io.ysum) {
+      float acc = 0.f;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) acc += abs_sq(v[q]);
+      const double w = warp_sum(static_cast<double>(acc));
+      if ((threadIdx.x & 31) == 0) *part_slot(io.part, unit, tile, 3 * kPartWarps + (threadIdx.x >> 5)) = w;
+    }
+    __syncwarp();  // the row's inputs are read before the exchange overwrites them
+    RegDft<Q, S>::run(v);
+#pragma unroll
+    for (int k1 = 0; k1 < Q; ++k1) {
+      float2 y = v[k1];
+      if (k1 > 0) {  // w_L^(p k1), stored at k1 P + p
+        const float2 w = __ldg(st.p.tw + k1 * P + p);
+        y = cmul(y, S < 0 ? w : make_float2(w.x, -w.y));
+      }
+      ya[k1 * (P + 2) + p] = y;
+    }
+    __syncwarp();
+
+    // pass 2: DFT-P over p for the columns k1 = p + j P
+    float2 u[J][P];
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int k1 = p + j * P;
+      if (Q % P == 0 || k1 < Q) {
+        const float4* col = reinterpret_cast<const float4*>(ya + k1 * (P + 2));
+#pragma unroll
+        for (int pp = 0; pp < P / 2; ++pp) {
+          const float4 t = col[pp];
+          u[j][2 * pp] = make_float2(t.x, t.y);
+          u[j][2 * pp + 1] = make_float2(t.z, t.w);
+        }
+        RegDft<P, S>::run(u[j]);
+      }
+    }
+    __syncwarp();  // the row's exchange values are read before its staging overwrites them
+    float2* xo = ya + lr;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int k1 = p + j * P;
+      if (Q % P == 0 || k1 < Q) {
+#pragma unroll
+        for (int k2 = 0; k2 < P; ++k2) {
+          const int c = k1 + Q * k2;
+          if (c < st.cols) xo[c] = u[j][k2];
+        }
+      }
+    }
+
+    // outputs c < C, row on the contiguous axis: thread (c0, row) handles
+    // columns c0 + P i (i < L / P) of row r0 + row (ROWS consecutive rows).
+    // The epilogue's other operands (the residual's observations and mask
+    // bits, the denoiser's prior, mean and variance) are loaded a chunk of
+    // CH columns ahead, the first chunk before the barrier, so that their
+    // latency overlaps it.
+    constexpr int NC = L / P;
+    constexpr int CH = NC <= 16 ? NC : (NC % 16 == 0 ? 16 : 8);
+    const int row = threadIdx.x % ROWS, c0 = threadIdx.x / ROWS;
+    const int rr = r0 + row;
+    const bool live_out = rr < st.rows;
+    const long long base = unit * st.out_stride;
+    const long long o0 = static_cast<long long>(c0) * st.out_ld + rr;
+    const long long step = static_cast<long long>(P) * st.out_ld;
+    const float2* sp = buf + row * A + row;
+    if constexpr (EPI == 0) {
+      __syncthreads();
+      float acc = 0.f;
+      if (live_out) {
+        long long o = base + o0;
+        for (int c = c0; c < st.cols; c += P, o += step) {
+          const float2 x = sp[c];
+          io.out[o] = x;
+          if (io.mode == 1) acc += abs_sq(x);
+        }
+      }
+      if (io.mode == 1) {
+        const double w = warp_sum(static_cast<double>(acc));
+        if ((threadIdx.x & 31) == 0) *part_slot(io.part, unit, tile, 1 * kPartWarps + (threadIdx.x >> 5)) = w;
+      }
+    } else if constexpr (EPI == 1) {
+      float2 yv[CH];
+      uint32_t obs = 0;
+      auto load_chunk = [&](int g) {
+        obs = 0;
+        if (live_out) {
+#pragma unroll
+          for (int i = 0; i < CH; ++i) {
+            const int ii = g * CH + i;
+            const long long o = o0 + ii * step;
+            if (c0 + P * ii < st.cols && (!io.mask || io.mask[o])) {
+              yv[i] = __ldg(io.y + base + o);
+              obs |= 1u << i;
+            }
+          }
+        }
+      };
+      load_chunk(0);
+      __syncthreads();
+      float acc = 0.f;
+#pragma unroll
+      for (int g = 0; g < NC / CH; ++g) {
+        if (g > 0) load_chunk(g);
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+          const int ii = g * CH + i;
+          const int c = c0 + P * ii;
+          if (live_out && c < st.cols) {
+            const float2 x = sp[c];
+            io.out[base + o0 + ii * step] = x;
+            if (obs >> i & 1u) {
+              const float dr = yv[i].x - x.x, di = yv[i].y - x.y;
+              acc += dr * dr + di * di;
+            }
+          }
+        }
+      }
+      const double w = warp_sum(static_cast<double>(acc));
+      if ((threadIdx.x & 31) == 0) *part_slot(io.part, unit, tile, 2 * kPartWarps + (threadIdx.x >> 5)) = w;
+    } else {
+      // four registers a column: chunks of at most 8 columns
+      constexpr int CD = NC % 8 == 0 ? 8 : (NC % 4 == 0 ? 4 : NC);
+      const DenoiseArgs& dn = io.dn;
+      float gv[CD], vv[CD];
+      float2 mv[CD];
+      auto load_chunk = [&](int g) {
+        if (live_out) {
+#pragma unroll
+          for (int i = 0; i < CD; ++i) {
+            const int ii = g * CD + i;
+            if (c0 + P * ii < st.cols) {
+              const long long o = base + o0 + ii * step;
+              gv[i] = dn.gamma[o];
+              mv[i] = dn.mu[o];
+              vv[i] = dn.var[o];
+            }
+          }
+        }
+      };
+      load_chunk(0);
+      __syncthreads();
+      const float pv = dn.pv[unit], fl = dn.floor_[unit];
+      float dof = 0.f, sv = 0.f;
+#pragma unroll
+      for (int g = 0; g < NC / CD; ++g) {
+        if (g > 0) load_chunk(g);
+#pragma unroll
+        for (int i = 0; i < CD; ++i) {
+          const int ii = g * CD + i;
+          const int c = c0 + P * ii;
+          if (live_out && c < st.cols) {
+            const DenoiseOut r = denoise_math(dn, gv[i], mv[i], vv[i], sp[c], pv, fl);
+            const long long o = base + o0 + ii * step;
+            dn.mu[o] = r.mean;
+            dn.var[o] = r.variance;
+            if (dn.update_prior) dn.gamma[o] = r.gamma;
+            if (dn.keys) dn.keys[o] = float_key(abs_sq(r.mean) + r.variance);
+            dof += r.rel;
+            sv += r.variance;
+          }
+        }
+      }
+      const double w0 = warp_sum(static_cast<double>(dof));
+      const double w1 = warp_sum(static_cast<double>(sv));
+      if ((threadIdx.x & 31) == 0) {
+        *part_slot(io.part, unit, tile, 0 * kPartWarps + (threadIdx.x >> 5)) = w0;
+        *part_slot(io.part, unit, tile, 1 * kPartWarps + (threadIdx.x >> 5)) = w1;
+      }
+    }
+    __syncthreads();  // this buffer takes the copy issued at the top of the next tile
+  }
+  cp_async_wait<0>();
+}
+
 template <int L, int S, int EPI>
 void launch_fast_as(const FftStage& S_, const FftIo& io, cudaStream_t st) {
   auto kern = fft_fast_kernel<L, S, EPI>;
@@ -633,6 +897,20 @@ void launch_fast_as(const FftStage& S_, const FftIo& io, cudaStream_t st) {
   if (grid > 0) kern<<<grid, kFftThreads, fast_smem_bytes(L), st>>>(S_, io);
 }
 
+template <int L, int S, int EPI>
+void launch_fast_set_as(const FftSet<kFftSetMax>& set, cudaStream_t st) {
+  auto kern = fft_fast_set_kernel<L, S, EPI, kFftSetMax>;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFftThreads, fast_smem_bytes(L)) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long long total = set.tile0[set.n];
+  const long long cap = static_cast<long long>(sm_count()) * per_sm;
+  const int grid = static_cast<int>(total < cap ? total : cap);
+  if (grid > 0) kern<<<grid, kFftThreads, fast_smem_bytes(L), st>>>(set);
+}
+
 // Forward stages store or take the residual; adjoint stages store or run
 // the denoiser (the combinations the UAMP sweeps use).
 template <int L>
@@ -645,17 +923,32 @@ void launch_fast(const FftStage& S, const FftIo& io, int sign, cudaStream_t st) 
     else launch_fast_as<L, 1, 0>(S, io, st);
   }
 }
+template <int L>
+void launch_fast_set(const FftSet<kFftSetMax>& set, int sign, int mode, cudaStream_t st) {
+  if (sign < 0) {
+    if (mode == 2) launch_fast_set_as<L, -1, 1>(set, st);
+    else launch_fast_set_as<L, -1, 0>(set, st);
+  } else {
+    if (mode == 3) launch_fast_set_as<L, 1, 2>(set, st);
+    else launch_fast_set_as<L, 1, 0>(set, st);
+  }
+}
 
+template <typename K>
+cudaError_t smem_attr(K kern, int bytes) {
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
 template <int L>
 cudaError_t set_fast_attr() {
   const int bytes = static_cast<int>(fast_smem_bytes(L));
-  cudaError_t e = cudaFuncSetAttribute(fft_fast_kernel<L, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fft_fast_kernel<L, -1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fft_fast_kernel<L, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fft_fast_kernel<L, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = smem_attr(fft_fast_kernel<L, -1, 0>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_kernel<L, -1, 1>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_kernel<L, 1, 0>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_kernel<L, 1, 2>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_set_kernel<L, -1, 0, kFftSetMax>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_set_kernel<L, -1, 1, kFftSetMax>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_set_kernel<L, 1, 0, kFftSetMax>, bytes);
+  if (e == cudaSuccess) e = smem_attr(fft_fast_set_kernel<L, 1, 2, kFftSetMax>, bytes);
   return e;
 }
 
@@ -731,9 +1024,7 @@ cudaError_t set_fft_attributes() {
 // denoiser at full occupancy is faster.
 int fft_denoise_fused(int L) { return fast_threads_per_row(L) != 0 && L < 512; }
 
-void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2* in, float2* out,
-               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st,
-               const DenoiseArgs* dn) {
+static FftStage fft_stage_of(const DftGeom& g, int L, int sign, const float2* tw) {
   FftStage S;
   S.p = make_plan(L, sign, tw);
   S.rows = g.rows;
@@ -745,6 +1036,28 @@ void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2
   S.out_stride = g.out_stride;
   S.tiles = ceil_div(g.rows, fft_rows_per_cta(L));
   S.units = g.n_scenes;
+  return S;
+}
+
+static void launch_fast_set_len(const FftSet<kFftSetMax>& set, int L, int sign, int mode, cudaStream_t st) {
+  switch (L) {
+    case 512: launch_fast_set<512>(set, sign, mode, st); return;
+    case 384: launch_fast_set<384>(set, sign, mode, st); return;
+    case 256: launch_fast_set<256>(set, sign, mode, st); return;
+    case 192: launch_fast_set<192>(set, sign, mode, st); return;
+    case 128: launch_fast_set<128>(set, sign, mode, st); return;
+    case 96: launch_fast_set<96>(set, sign, mode, st); return;
+    case 64: launch_fast_set<64>(set, sign, mode, st); return;
+    case 48: launch_fast_set<48>(set, sign, mode, st); return;
+    case 32: launch_fast_set<32>(set, sign, mode, st); return;
+    default: return;
+  }
+}
+
+void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2* in, float2* out,
+               const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st,
+               const DenoiseArgs* dn) {
+  const FftStage S = fft_stage_of(g, L, sign, tw);
   FftIo io{in, out, y, mask, part, mode, ysum};
   if (dn) io.dn = *dn;
   switch (L) {
@@ -760,6 +1073,28 @@ void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2
     default: break;
   }
   fft_stage_kernel<<<dim3(S.tiles, g.n_scenes), kFftThreads, fft_smem_bytes(L), st>>>(S, io);
+}
+
+// The same-length stages of several shape buckets in one launch of the
+// two-pass kernel (L must have one: fft_set_length_ok).  Each item is
+// computed as fft_stage computes it alone.
+int fft_set_length_ok(int L) { return fast_threads_per_row(L) != 0; }
+
+void fft_stage_set(const FftSetJob* jobs, int n, int L, int sign, int mode, cudaStream_t st) {
+  for (int j0 = 0; j0 < n; j0 += kFftSetMax) {
+    const int cnt = n - j0 < kFftSetMax ? n - j0 : kFftSetMax;
+    FftSet<kFftSetMax> set;
+    set.n = cnt;
+    set.tile0[0] = 0;
+    for (int i = 0; i < cnt; ++i) {
+      const FftSetJob& j = jobs[j0 + i];
+      set.st[i] = fft_stage_of(j.g, L, sign, j.tw);
+      set.io[i] = FftIo{j.in, j.out, j.y, j.mask, j.part, mode, j.ysum};
+      if (mode == 3) set.io[i].dn = *j.dn;
+      set.tile0[i + 1] = set.tile0[i] + set.st[i].tiles * set.st[i].units;
+    }
+    launch_fast_set_len(set, L, sign, mode, st);
+  }
 }
 
 int fft_stage_tiles(int rows, int L) { return ceil_div(rows, fft_rows_per_cta(L)); }

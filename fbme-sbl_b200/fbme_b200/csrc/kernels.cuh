@@ -157,7 +157,11 @@ struct UampJob {
   UampBuffers u;
 };
 // uamp_run over several shape buckets with merged launches (no warm start).
-void uamp_run_multi(const UampJob* jobs, int n, cudaStream_t st, Profiler* prof = nullptr);
+// FP32 FFT buckets of different transform lengths run their per-length
+// launches of a step on `st` and the `naux` side streams, forked and joined
+// through `ev` (naux + 1 events), when no profiler is given.
+void uamp_run_multi(const UampJob* jobs, int n, cudaStream_t st, Profiler* prof = nullptr,
+                    const cudaStream_t* aux = nullptr, const cudaEvent_t* ev = nullptr, int naux = 0);
 
 // Active-set stage.
 struct PolishBuffers {

@@ -264,4 +264,23 @@ void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2
                const float2* y, const uint8_t* mask, double* part, int mode, int ysum, cudaStream_t st,
                const DenoiseArgs* dn = nullptr);
 int fft_denoise_fused(int L);
+
+// One shape bucket's stage in a merged FFT launch (fft_stage_set): the
+// arguments fft_stage takes, per bucket.
+struct FftSetJob {
+  DftGeom g;
+  const float2* tw;
+  const float2* in;
+  float2* out;
+  const float2* y;
+  const uint8_t* mask;
+  double* part;
+  int ysum;
+  const DenoiseArgs* dn;  // mode 3
+};
+// The stages `jobs[0..n)` of one transform length L (fft_set_length_ok),
+// sign and mode in as few launches as fit (64 buckets each); every bucket's
+// results and partial sums are those of its own fft_stage launch.
+void fft_stage_set(const FftSetJob* jobs, int n, int L, int sign, int mode, cudaStream_t st);
+int fft_set_length_ok(int L);
 }  // namespace fbme

@@ -18,6 +18,7 @@
 // to run.
 #include <math.h>
 
+#include <map>
 #include <vector>
 
 #include "denoise.cuh"
@@ -807,7 +808,8 @@ static void scalars_multi(int mode, const std::vector<ScalarsJob>& jobs, cudaStr
 // elementwise step is one launch over all buckets, and bucket b takes part
 // in sweeps 1..T_u(b) only.  A bucket's blocks, tiles and summation orders
 // are those of its own uamp_run, so the results are identical.
-void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
+void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof, const cudaStream_t* aux,
+                    const cudaEvent_t* ev, int naux) {
   std::vector<DftGeom> f1(nb), f2(nb), a1(nb), a2(nb);
   std::vector<int> bn(nb), bm(nb), cur(nb, 0);
   int iters = 0;
@@ -855,6 +857,61 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
     if (!js.empty()) run_stage_multi(js.data(), static_cast<int>(js.size()), st);
     if (!jp.empty()) run_stage_multi(jp.data(), static_cast<int>(jp.size()), st);
   };
+  // FP32 FFT buckets (dft_terms 0): each stage step is one two-pass kernel
+  // launch per transform length, over the buckets of that length
+  auto is_fft = [&](int b) { return J[b].c.terms == 0; };
+  auto tens_of = [&](const std::vector<int>& bs) {
+    std::vector<int> r;
+    for (int b : bs)
+      if (!is_fft(b)) r.push_back(b);
+    return r;
+  };
+  auto fft_m = [&](Stage which, const std::vector<int>& bs, const std::vector<DftGeom>& g, int mode,
+                   auto make) {
+    const bool ax2 = which == kFwd1 || which == kAdj1;
+    const int sign = (which == kFwd1 || which == kFwd2) ? -1 : 1;
+    std::map<int, std::vector<FftSetJob>> by_len;
+    for (int b : bs) {
+      if (!is_fft(b)) continue;
+      FftSetJob j = make(b);
+      j.g = g[b];
+      j.tw = ax2 ? J[b].t.fft_n2 : J[b].t.fft_n1;
+      by_len[ax2 ? J[b].s.n2 : J[b].s.n1].push_back(j);
+    }
+    // lengths 1.. on side streams, forked from and joined back to `st`, so
+    // the launches of one step overlap instead of queueing
+    const int nl = static_cast<int>(by_len.size());
+    const bool fork = !prof && nl > 1 && aux && ev && naux >= nl - 1;
+    if (fork) {
+      cudaEventRecord(ev[0], st);
+      for (int k = 1; k < nl; ++k) cudaStreamWaitEvent(aux[k - 1], ev[0], 0);
+    }
+    int k = 0;
+    for (auto& kv : by_len) {
+      const cudaStream_t sk = fork && k > 0 ? aux[k - 1] : st;
+      fft_stage_set(kv.second.data(), static_cast<int>(kv.second.size()), kv.first, sign, mode, sk);
+      ++k;
+    }
+    if (fork)
+      for (int j = 1; j < nl; ++j) {
+        cudaEventRecord(ev[j], aux[j - 1]);
+        cudaStreamWaitEvent(st, ev[j], 0);
+      }
+  };
+  auto job = [](const float2* in, float2* out, double* part = nullptr) {
+    FftSetJob j{};
+    j.in = in;
+    j.out = out;
+    j.part = part;
+    return j;
+  };
+  auto fft_part = [&](Stage which, int b, const DftGeom& g) {
+    const bool ax2 = which == kFwd1 || which == kAdj1;
+    return PartSrc{fft_stage_tiles(g.rows, ax2 ? J[b].s.n2 : J[b].s.n1), kPartWarps};
+  };
+  // FFT buckets whose adjoint stage 2 runs the denoiser in its epilogue
+  auto fused = [&](int b) { return is_fft(b) && fft_denoise_fused(J[b].s.n1); };
+  std::vector<DenoiseArgs> das(nb);
   std::vector<int> all(nb);
   for (int b = 0; b < nb; ++b) all[b] = b;
 
@@ -867,16 +924,29 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
       const UampBuffers& u = J[b].u;
       const DftGeom a1y = with_y(a1[b], u.y);
       a1ys[b] = a1y;
-      s1.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{a1y.row_tiles * a1y.col_tiles, kProWarps},
-                    PartSrc{a2[b].row_tiles * a2[b].col_tiles, kPartWarps}, PartSrc{0, 0}});
+      if (is_fft(b))
+        s1.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, fft_part(kAdj1, b, a1y), fft_part(kAdj2, b, a2[b]),
+                      PartSrc{0, 0}});
+      else
+        s1.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{a1y.row_tiles * a1y.col_tiles, kProWarps},
+                      PartSrc{a2[b].row_tiles * a2[b].col_tiles, kPartWarps}, PartSrc{0, 0}});
       g0.push_back({bn[b], J[b].s, J[b].c, u.sc, u.bp, u.gamma, u.part});
       s2.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{bn[b], 1}, PartSrc{0, 0}, PartSrc{0, 0}});
     }
-    FBME_TIMED(prof, FBME_GROUP_INIT, stage1_m(all, a1ys, a2, [&](int b) {
+    const std::vector<int> tens = tens_of(all);
+    FBME_TIMED(prof, FBME_GROUP_INIT, stage1_m(tens, a1ys, a2, [&](int b) {
                  return ProYPower{J[b].u.y, J[b].u.part, 0.f};
                }));
-    FBME_TIMED(prof, FBME_GROUP_INIT, stage2_m(all, a2, [&](int b) {
+    FBME_TIMED(prof, FBME_GROUP_INIT, fft_m(kAdj1, all, a1ys, 0, [&](int b) {
+                 FftSetJob j = job(J[b].u.y, J[b].u.tmp, J[b].u.part);
+                 j.ysum = 1;
+                 return j;
+               }));
+    FBME_TIMED(prof, FBME_GROUP_INIT, stage2_m(tens, a2, [&](int b) {
                  return EpiBackprojection{J[b].u.bp, J[b].u.part, 0.f};
+               }));
+    FBME_TIMED(prof, FBME_GROUP_INIT, fft_m(kAdj2, all, a2, 1, [&](int b) {
+                 return job(J[b].u.tmp, J[b].u.bp, J[b].u.part);
                }));
     FBME_TIMED(prof, FBME_GROUP_INIT, scalars_multi(kScalarInit1, s1, st));
     FBME_TIMED(prof, FBME_GROUP_INIT, ew_launch(g0, [&](const EwJobs<Gamma0Job>& m, dim3 g) {
@@ -902,33 +972,61 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
     } else {
       std::vector<MessageJob> jm;
       std::vector<DenoiseJob> jd;
+      std::vector<int> lifted, fusing;
       for (int b : act) {
         const UampBuffers& u = J[b].u;
         jm.push_back({bm[b], J[b].s, u.y, u.pred, msg(b, cur[b]), msg(b, cur[b] ^ 1), u.sc.prec, u.sc.dvar,
                       J[b].c.uamp_damping});
-        jd.push_back({bn[b], J[b].s, denoise_args(J[b].c, u), u.lift});
+        das[b] = denoise_args(J[b].c, u);
+        if (fused(b)) {
+          fusing.push_back(b);
+        } else {
+          lifted.push_back(b);
+          jd.push_back({bn[b], J[b].s, das[b], u.lift});
+        }
       }
       FBME_TIMED(prof, FBME_GROUP_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
                    message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
                  }));
       FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-                 stage1_m(act, a1, a2, [&](int b) { return ProPlain{msg(b, cur[b] ^ 1)}; }));
+                 stage1_m(tens_of(act), a1, a2, [&](int b) { return ProPlain{msg(b, cur[b] ^ 1)}; }));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+                 fft_m(kAdj1, act, a1, 0, [&](int b) { return job(msg(b, cur[b] ^ 1), J[b].u.tmp); }));
       for (int b : act) cur[b] ^= 1;
-      FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2_m(act, a2, [&](int b) { return EpiStoreT{J[b].u.lift}; }));
-      FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
-                   denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2,
+                 stage2_m(tens_of(lifted), a2, [&](int b) { return EpiStoreT{J[b].u.lift}; }));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_2,
+                 fft_m(kAdj2, lifted, a2, 0, [&](int b) { return job(J[b].u.tmp, J[b].u.lift); }));
+      FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, fft_m(kAdj2, fusing, a2, 3, [&](int b) {
+                   FftSetJob j = job(J[b].u.tmp, nullptr, J[b].u.part);
+                   j.dn = &das[b];
+                   return j;
                  }));
+      if (!jd.empty())
+        FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
+                     denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+                   }));
     }
-    FBME_TIMED(prof, FBME_GROUP_FWD_1, stage1_m(act, f1, f2, [&](int b) { return ProPlain{J[b].u.mu}; }));
+    FBME_TIMED(prof, FBME_GROUP_FWD_1,
+               stage1_m(tens_of(act), f1, f2, [&](int b) { return ProPlain{J[b].u.mu}; }));
+    FBME_TIMED(prof, FBME_GROUP_FWD_1, fft_m(kFwd1, act, f1, 0, [&](int b) { return job(J[b].u.mu, J[b].u.tmp); }));
     {
       std::vector<ScalarsJob> sj;
       for (int b : act) {
         const UampBuffers& u = J[b].u;
-        sj.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, PartSrc{bn[b], 1}, PartSrc{bn[b], 1},
-                      PartSrc{f2[b].row_tiles * f2[b].col_tiles, kPartWarps}});
+        const PartSrc dof = it > 1 && fused(b) ? fft_part(kAdj2, b, a2[b]) : PartSrc{bn[b], 1};
+        const PartSrc res =
+            is_fft(b) ? fft_part(kFwd2, b, f2[b]) : PartSrc{f2[b].row_tiles * f2[b].col_tiles, kPartWarps};
+        sj.push_back({sgx(b), J[b].s, J[b].c, u.sc, u.part, dof, dof, res});
       }
-      FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, stage2_m(act, f2, [&](int b) {
+      FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, stage2_m(tens_of(act), f2, [&](int b) {
                    return EpiPredict{J[b].u.pred, J[b].u.y, J[b].u.part, 0.f};
+                 }));
+      FBME_TIMED(prof, FBME_GROUP_FWD_RESIDUAL, fft_m(kFwd2, act, f2, 2, [&](int b) {
+                   FftSetJob j = job(J[b].u.tmp, J[b].u.pred, J[b].u.part);
+                   j.y = J[b].u.y;
+                   j.mask = J[b].u.mask;
+                   return j;
                  }));
       FBME_TIMED(prof, FBME_GROUP_SCALARS, scalars_multi(kScalarSweep, sj, st));
     }
@@ -937,24 +1035,39 @@ void uamp_run_multi(const UampJob* J, int nb, cudaStream_t st, Profiler* prof) {
   // --- final E-step (no prior update, no prediction), score keys ---
   std::vector<MessageJob> jm;
   std::vector<DenoiseJob> jd;
+  std::vector<int> lifted, fusing;
   for (int b = 0; b < nb; ++b) {
     const UampBuffers& u = J[b].u;
     jm.push_back({bm[b], J[b].s, u.y, u.pred, msg(b, cur[b]), msg(b, cur[b] ^ 1), u.sc.prec, u.sc.dvar,
                   J[b].c.uamp_damping});
-    DenoiseArgs da = denoise_args(J[b].c, u);
-    da.update_prior = 0;
-    da.keys = reinterpret_cast<uint32_t*>(u.keys);
-    jd.push_back({bn[b], J[b].s, da, u.lift});
+    das[b] = denoise_args(J[b].c, u);
+    das[b].update_prior = 0;
+    das[b].keys = reinterpret_cast<uint32_t*>(u.keys);
+    if (fused(b)) {
+      fusing.push_back(b);
+    } else {
+      lifted.push_back(b);
+      jd.push_back({bn[b], J[b].s, das[b], u.lift});
+    }
   }
   FBME_TIMED(prof, FBME_GROUP_MESSAGE, ew_launch(jm, [&](const EwJobs<MessageJob>& m, dim3 g) {
                message_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
              }));
   FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
-             stage1_m(all, a1, a2, [&](int b) { return ProPlain{msg(b, cur[b] ^ 1)}; }));
-  FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2_m(all, a2, [&](int b) { return EpiStoreT{J[b].u.lift}; }));
-  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
-               denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+             stage1_m(tens_of(all), a1, a2, [&](int b) { return ProPlain{msg(b, cur[b] ^ 1)}; }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_MESSAGE,
+             fft_m(kAdj1, all, a1, 0, [&](int b) { return job(msg(b, cur[b] ^ 1), J[b].u.tmp); }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2, stage2_m(tens_of(lifted), a2, [&](int b) { return EpiStoreT{J[b].u.lift}; }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_2, fft_m(kAdj2, lifted, a2, 0, [&](int b) { return job(J[b].u.tmp, J[b].u.lift); }));
+  FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, fft_m(kAdj2, fusing, a2, 3, [&](int b) {
+               FftSetJob j = job(J[b].u.tmp, nullptr, J[b].u.part);
+               j.dn = &das[b];
+               return j;
              }));
+  if (!jd.empty())
+    FBME_TIMED(prof, FBME_GROUP_ADJ_DENOISE, ew_launch(jd, [&](const EwJobs<DenoiseJob>& m, dim3 g) {
+                 denoise_multi_kernel<<<g, kEwThreads, 0, st>>>(m);
+               }));
 }
 
 }  // namespace fbme

@@ -51,10 +51,19 @@ def resolve_dft_terms(requested: int, grid: Sequence[int], uneven: bool = False)
     """The DFT stage form a plan runs: ``requested`` unless it is -1
     (automatic), which picks the FP32 FFT stages (0) for equal-shape plans
     whose grid lengths allow them and the 3-term tensor-core products
-    otherwise."""
+    otherwise (uneven plans: ``resolve_uneven_dft_terms``)."""
     if requested != -1:
         return int(requested)
     return 0 if not uneven and fft_length_ok(grid[0]) and fft_length_ok(grid[1]) else 3
+
+
+def resolve_uneven_dft_terms(requested: int, grids: Sequence[Sequence[int]]) -> int:
+    """The stage form of an uneven plan (one for all its buckets): the FP32
+    FFT stages when every grid's lengths allow them, else the 3-term
+    tensor-core products; an explicit ``requested`` wins."""
+    if requested != -1:
+        return int(requested)
+    return 0 if all(fft_length_ok(g[0]) and fft_length_ok(g[1]) for g in grids) else 3
 
 
 def resolve_native_config(cfg: SBLConfig, grid: Sequence[int], sample: Sequence[int],

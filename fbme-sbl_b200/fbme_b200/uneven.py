@@ -23,6 +23,7 @@ graph-owned results, overwritten by the next replay.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from math import prod
 from typing import Sequence
 
@@ -31,7 +32,7 @@ from torch import Tensor
 
 from . import _native as nat
 from .config import SBLConfig, fbme_profile_config
-from .engine import BACKEND_NAME, check_supported, resolve_dft_terms, resolve_native_config
+from .engine import BACKEND_NAME, check_supported, resolve_native_config, resolve_uneven_dft_terms
 from .result import SBLResult
 
 Shape = tuple[tuple[int, int], tuple[int, int]]
@@ -80,7 +81,9 @@ class UnevenEngine:
         for sh in self.scenes:
             if sh not in distinct:
                 distinct.append(sh)
-        resolved = {sh: resolve_native_config(cfg, sh[0], sh[1], uneven=True) for sh in distinct}
+        terms = resolve_uneven_dft_terms(int(cfg.dft_terms), [sh[0] for sh in distinct])
+        cfg_t = dataclasses.replace(cfg, dft_terms=terms)
+        resolved = {sh: resolve_native_config(cfg_t, sh[0], sh[1], uneven=True) for sh in distinct}
         base = resolved[self.scenes[0]]
         if len({(r.polish_size, r.polish_iterations) for r in resolved.values()}) != 1:
             raise ValueError("every scene of an uneven plan needs N1*N2 >= polish_size")
@@ -95,7 +98,6 @@ class UnevenEngine:
         from .autotune import candidates, default_width, stage_tiles
 
         sms = torch.cuda.get_device_properties(device).multi_processor_count
-        terms = resolve_dft_terms(int(cfg.dft_terms), (0, 0), uneven=True)
         fill = sum(sum(stage_tiles(sh[0], sh[1], max(candidates(sh[0], sh[1], terms) or [256])))
                    for sh in self.scenes)
         self.tile_widths = {sh: int(tile_widths.get(sh) or default_width(sh[0], sh[1], 1, terms,

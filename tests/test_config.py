@@ -64,6 +64,13 @@ def test_uamp_budget_and_native_mapping():
     assert resolve_native_config(stable, (384, 192), (100, 90)).dft_terms == 0
     assert resolve_native_config(stable, (1024, 256), (512, 128)).dft_terms == 3
     assert resolve_native_config(stable, (256, 256), (128, 128), uneven=True).dft_terms == 3
+    # an uneven plan runs one form for all its buckets: the FFT stages when
+    # every grid allows them
+    from fbme_b200.engine import resolve_uneven_dft_terms
+
+    assert resolve_uneven_dft_terms(-1, [(256, 256), (192, 256), (384, 256), (128, 128)]) == 0
+    assert resolve_uneven_dft_terms(-1, [(256, 256), (40, 32)]) == 3
+    assert resolve_uneven_dft_terms(3, [(256, 256)]) == 3
     assert resolve_native_config(SBLConfig.paper_hybrid_uamp(uamp_polish_size=32, dft_terms=6),
                                  (256, 256), (128, 128)).dft_terms == 6
     hybrid = SBLConfig.fast_hybrid_uamp()

@@ -391,3 +391,93 @@ def test_six_term_buckets_match_per_shape_plans():
                 assert torch.equal(eng.out[f][i], ref.out[f][j]), (f, i)
         ref.close()
     eng.close()
+
+
+# FP32 FFT stages in uneven plans: every stage step is one merged two-pass
+# FFT launch per transform length over the buckets of that length
+FA = ((64, 64), (32, 32))
+FB = ((128, 64), (48, 40))
+FC = ((96, 128), (24, 64))
+FD = ((512, 32), (200, 16))  # N1 = 512: adjoint stage 2 stores A^H m, the elementwise denoiser follows
+F_ORDER = [FA, FB, FA, FC, FD, FB, FA]
+
+
+def _fft_cfg(profile="stable"):
+    from fbme_b200.config import fbme_profile_config
+
+    cfg = fbme_profile_config(profile)
+    cfg.dft_terms = -1  # automatic: every grid above allows the FFT stages
+    return cfg
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("profile", ["stable", "fast"])
+def test_fft_uneven_plan_equals_per_shape_plans(profile):
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    cfg = _fft_cfg(profile)
+    sc = _scenes(F_ORDER, 900)
+    eng = UnevenEngine(F_ORDER, cfg, dev)
+    assert int(eng.native_cfg.dft_terms) == 0
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    assert len({b["uamp_iterations"] for b in eng.buckets()}) > 1
+    for shape in (FA, FB, FC, FD):
+        idx = [i for i, s in enumerate(F_ORDER) if s == shape]
+        ref = FBMEEngine(len(idx), shape[0], shape[1], cfg, dev)
+        assert int(ref.native_cfg.dft_terms) == 0
+        ys = torch.stack([torch.from_numpy(sc[i].y).to(dev) for i in idx]).reshape(len(idx), -1)
+        ref.run(ys.contiguous())
+        torch.cuda.synchronize()
+        n = shape[0][0] * shape[0][1]
+        for j, i in enumerate(idx):
+            p0 = eng.pix_off[i]
+            for f in FIELDS_PIX:
+                assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][j]), (f, i)
+            for f in FIELDS_SCENE:
+                assert torch.equal(eng.out[f][i], ref.out[f][j]), (f, i)
+        ref.close()
+    assert int(eng.out["status"].abs().sum()) == 0
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_fft_buckets_beyond_one_merged_launch():
+    """70 shapes sharing N2 = 64: the N2-axis FFT steps hold 70 buckets of
+    one length and split into two launches; every checked scene equals its
+    single-scene FFT plan bit for bit."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(47)
+    shapes = []
+    while len(shapes) < 70:
+        g = (int(rng.choice([32, 48, 64, 96])), 64)
+        s = (int(rng.integers(8, g[0] // 2 + 1)), int(rng.integers(8, 33)))
+        if (g, s) not in shapes:
+            shapes.append((g, s))
+    sc = _scenes(shapes, 3100)
+    cfg = _fft_cfg()
+    eng = UnevenEngine(shapes, cfg, dev)
+    assert int(eng.native_cfg.dft_terms) == 0
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    assert len(eng.buckets()) == 70
+    assert int(eng.out["status"].abs().sum()) == 0
+    for i in range(0, 70, 3):
+        g, s = shapes[i]
+        ref = FBMEEngine(1, g, s, cfg, dev)
+        ref.run(torch.from_numpy(sc[i].y).to(dev).reshape(1, -1).contiguous())
+        torch.cuda.synchronize()
+        p0, n = eng.pix_off[i], g[0] * g[1]
+        for f in FIELDS_PIX:
+            assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][0]), (f, i)
+        for f in FIELDS_SCENE:
+            assert torch.equal(eng.out[f][i], ref.out[f][0]), (f, i)
+        ref.close()
+    eng.close()
