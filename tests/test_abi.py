@@ -56,12 +56,16 @@ def test_workspace_bytes_and_validation_codes():
     rc = lib.fbme_plan_create(bad, 1, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
     assert rc == nat.FBME_ERR_INVALID and "0 < M <= N" in nat.last_error()
     # scenes of different shapes make an uneven plan: sized, then refused
-    # here only for the missing workspace.  Uneven plans run the tensor-core
-    # stages; the FP32 FFT stages (what the 256x256 config resolves to) are
-    # refused for them.
+    # here only for the missing workspace, with the FP32 FFT stages (what
+    # the 256x256 config resolves to) or the tensor-core stages; the FFT
+    # stages need every grid length to allow them
     assert c.dft_terms == 0
     uneven = (nat.FbmeShape * 2)(nat.FbmeShape(64, 64, 32, 32), nat.FbmeShape(128, 64, 32, 32))
-    assert lib.fbme_plan_workspace_bytes(uneven, 2, ctypes.byref(c)) == 0
+    assert lib.fbme_plan_workspace_bytes(uneven, 2, ctypes.byref(c)) > 0
+    rc = lib.fbme_plan_create(uneven, 2, ctypes.byref(c), None, 0, None, ctypes.byref(plan))
+    assert rc == nat.FBME_ERR_WORKSPACE
+    odd = (nat.FbmeShape * 2)(nat.FbmeShape(64, 64, 32, 32), nat.FbmeShape(40, 64, 32, 32))
+    assert lib.fbme_plan_workspace_bytes(odd, 2, ctypes.byref(c)) == 0
     c3 = _cfg(dft_terms=3)
     assert lib.fbme_plan_workspace_bytes(uneven, 2, ctypes.byref(c3)) > 0
     rc = lib.fbme_plan_create(uneven, 2, ctypes.byref(c3), None, 0, None, ctypes.byref(plan))
