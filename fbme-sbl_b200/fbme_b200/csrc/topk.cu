@@ -91,12 +91,16 @@ topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int 
 
 int topk_slices(long long n) { return static_cast<int>((n + kTopkSlice - 1) / kTopkSlice); }
 
+void launch_topk_blocks(const uint32_t* keys, long long n, int k, int B, uint32_t* cand_key, int* cand_idx,
+                        cudaStream_t st) {
+  topk_blocks_kernel<false>
+      <<<dim3(topk_slices(n), B), kTopkBlockThreads, 0, st>>>(keys, n, k, cand_key, cand_idx);
+}
+
 void launch_topk(const uint32_t* keys, long long n, int k, int B, uint32_t* cand_key, int* cand_idx,
                  int* out_idx, float* out_val, cudaStream_t st) {
-  const int nblk = topk_slices(n);
-  topk_blocks_kernel<false>
-      <<<dim3(nblk, B), kTopkBlockThreads, 0, st>>>(keys, n, k, cand_key, cand_idx);
-  topk_merge_kernel<int><<<B, 1024, 0, st>>>(cand_key, cand_idx, nblk * k, k, out_idx, out_val);
+  launch_topk_blocks(keys, n, k, B, cand_key, cand_idx, st);
+  topk_merge_kernel<int><<<B, 1024, 0, st>>>(cand_key, cand_idx, topk_slices(n) * k, k, out_idx, out_val);
 }
 
 void launch_topk_merge(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, int B,
