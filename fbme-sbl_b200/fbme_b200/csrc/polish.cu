@@ -323,10 +323,14 @@ FBME_DEV double residual_energy(const PolishArgs& A, const float2* d1, const flo
     cross = static_cast<double>(my_c.x) * my_mu.x + static_cast<double>(my_c.y) * my_mu.y;
     const int n1i = my_idx / s.n2, n2i = my_idx % s.n2;
     double gr = 0.0, gi = 0.0;  // (G mu)_i
+    // unrolled: the shuffles and Gram entries of later j issue ahead of the
+    // FP64 sums, which still run in the order j = 0, 1, ...
+    const unsigned am = __activemask();
+#pragma unroll 8
     for (int j = 0; j < K; ++j) {
-      const int n1j = __shfl_sync(__activemask(), n1i, j), n2j = __shfl_sync(__activemask(), n2i, j);
-      const float mjx = __shfl_sync(__activemask(), my_mu.x, j);
-      const float mjy = __shfl_sync(__activemask(), my_mu.y, j);
+      const int n1j = __shfl_sync(am, n1i, j), n2j = __shfl_sync(am, n2i, j);
+      const float mjx = __shfl_sync(am, my_mu.x, j);
+      const float mjy = __shfl_sync(am, my_mu.y, j);
       const float2 g = gram_at(A, d1, d2, n1i, n2i, n1j, n2j);
       gr += static_cast<double>(g.x) * mjx - static_cast<double>(g.y) * mjy;
       gi += static_cast<double>(g.x) * mjy + static_cast<double>(g.y) * mjx;
