@@ -15,8 +15,8 @@
 
 namespace fbme {
 
-constexpr int kTopkBlockThreads = 256;
-constexpr int kTopkKpt = 32;
+constexpr int kTopkBlockThreads = 512;
+constexpr int kTopkKpt = 16;
 constexpr int kTopkSlice = kTopkBlockThreads * kTopkKpt;  // 8192 keys per CTA
 constexpr int kMergeMax = 2048;
 
@@ -24,7 +24,7 @@ constexpr int kMergeMax = 2048;
 // The slice's k best lie among its keys at or above the k-th largest
 // thread maximum (radix bound), typically a few dozen of the 8192.
 template <bool FROM_SCORES>
-__global__ void __launch_bounds__(kTopkBlockThreads)
+__global__ void __launch_bounds__(kTopkBlockThreads, 2)
 topk_blocks_kernel(const void* in, long long n, int k, uint32_t* cand_key, int* cand_idx) {
   __shared__ TopkPrunedShared S;
   const int scene = blockIdx.y, blk = blockIdx.x;
