@@ -498,7 +498,7 @@ FBME_DEV void prior_strip(const float (&o)[kFStrip], float base, float fl, float
 }
 
 // The same prior from a caller's [B][H][W] map, over the same tiles, strips
-// and partial-sum slots as warm_net_kernel.
+// and partial-sum slots as net_tile_kernel<false, 1>.
 __global__ void __launch_bounds__(kFThreads) warm_map_kernel(const float* map, int H, int W,
                                                             const float* data_power, const float* floor_,
                                                             float* gamma, double* upart, int nslots) {
