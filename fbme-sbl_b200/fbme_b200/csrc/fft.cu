@@ -1076,11 +1076,20 @@ void fft_stage(const DftGeom& g, int L, int sign, const float2* tw, const float2
 }
 
 // The same-length stages of several shape buckets in one launch of the
-// two-pass kernel (L must have one: fft_set_length_ok).  Each item is
+// two-pass kernel where L has it (fft_set_length_ok).  Each item is
 // computed as fft_stage computes it alone.
 int fft_set_length_ok(int L) { return fast_threads_per_row(L) != 0; }
 
 void fft_stage_set(const FftSetJob* jobs, int n, int L, int sign, int mode, cudaStream_t st) {
+  if (!fft_set_length_ok(L)) {
+    // lengths without the two-pass kernel (below 32): one Stockham launch
+    // per bucket, as fft_stage runs it
+    for (int i = 0; i < n; ++i) {
+      const FftSetJob& j = jobs[i];
+      fft_stage(j.g, L, sign, j.tw, j.in, j.out, j.y, j.mask, j.part, mode, j.ysum, st, j.dn);
+    }
+    return;
+  }
   for (int j0 = 0; j0 < n; j0 += kFftSetMax) {
     const int cnt = n - j0 < kFftSetMax ? n - j0 : kFftSetMax;
     FftSet<kFftSetMax> set;

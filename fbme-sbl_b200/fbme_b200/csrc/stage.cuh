@@ -278,9 +278,10 @@ struct FftSetJob {
   int ysum;
   const DenoiseArgs* dn;  // mode 3
 };
-// The stages `jobs[0..n)` of one transform length L (fft_set_length_ok),
-// sign and mode in as few launches as fit (64 buckets each); every bucket's
-// results and partial sums are those of its own fft_stage launch.
+// The stages `jobs[0..n)` of one transform length L, sign and mode: in as
+// few launches of the two-pass kernel as fit (64 buckets each) where L has
+// it (fft_set_length_ok), else one fft_stage launch per bucket; every
+// bucket's results and partial sums are those of its own fft_stage launch.
 void fft_stage_set(const FftSetJob* jobs, int n, int L, int sign, int mode, cudaStream_t st);
 int fft_set_length_ok(int L);
 }  // namespace fbme

@@ -481,3 +481,37 @@ def test_fft_buckets_beyond_one_merged_launch():
             assert torch.equal(eng.out[f][i], ref.out[f][0]), (f, i)
         ref.close()
     eng.close()
+
+
+@pytest.mark.gpu
+def test_fft_uneven_plan_with_short_transform_lengths():
+    """Grids with 16- and 24-point axes take the FFT stages too (every length
+    is 2^a or 3 * 2^a); lengths below the two-pass kernel's run one Stockham
+    launch per bucket.  Every scene equals its equal-shape FFT plan bit for
+    bit."""
+    need_gpu()
+    from fbme_b200.engine import FBMEEngine
+    from fbme_b200.uneven import UnevenEngine
+
+    shapes = [((16, 32), (8, 16)), ((24, 48), (12, 20)), ((64, 16), (30, 8)), ((16, 32), (8, 16))]
+    dev = torch.device("cuda", 0)
+    cfg = _fft_cfg()
+    cfg.uamp_polish_size = 32
+    sc = _scenes(shapes, 4100)
+    eng = UnevenEngine(shapes, cfg, dev)
+    assert int(eng.native_cfg.dft_terms) == 0
+    eng.run(eng.pack([torch.from_numpy(s.y).to(dev) for s in sc]))
+    torch.cuda.synchronize()
+    assert int(eng.out["status"].abs().sum()) == 0
+    for i, (g, smp) in enumerate(shapes):
+        ref = FBMEEngine(1, g, smp, cfg, dev)
+        assert int(ref.native_cfg.dft_terms) == 0
+        ref.run(torch.from_numpy(sc[i].y).to(dev).reshape(1, -1).contiguous())
+        torch.cuda.synchronize()
+        p0, n = eng.pix_off[i], g[0] * g[1]
+        for f in FIELDS_PIX:
+            assert torch.equal(eng.out[f][p0:p0 + n], ref.out[f][0]), (f, i)
+        for f in FIELDS_SCENE:
+            assert torch.equal(eng.out[f][i], ref.out[f][0]), (f, i)
+        ref.close()
+    eng.close()
