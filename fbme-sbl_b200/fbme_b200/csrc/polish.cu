@@ -78,10 +78,16 @@ FBME_DEV float2 gram_at(const PolishArgs& A, const float2* d1, const float2* d2,
   return dirichlet2(d1, d2, A.s.n1, A.s.n2, a1, a2, b1, b2);
 }
 
-// Copy the Dirichlet tables of a scene shape into shared memory.
+// Copy the Dirichlet tables of a scene shape into shared memory: 8-byte
+// asynchronous copies, all in flight before the one wait (a warp copying
+// one element per lane at a time waited on every round trip).
 FBME_DEV void load_dirichlet(const PolishArgs& A, float2* d1, float2* d2) {
-  for (int i = threadIdx.x; i < A.s.n1; i += blockDim.x) d1[i] = __ldg(A.p.dir1 + i);
-  for (int i = threadIdx.x; i < A.s.n2; i += blockDim.x) d2[i] = __ldg(A.p.dir2 + i);
+  for (int i = threadIdx.x; i < A.s.n1; i += blockDim.x)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(d1 + i)), "l"(A.p.dir1 + i) : "memory");
+  for (int i = threadIdx.x; i < A.s.n2; i += blockDim.x)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(d2 + i)), "l"(A.p.dir2 + i) : "memory");
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncwarp();
 }
 
