@@ -846,9 +846,9 @@ int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_
 namespace {
 // Gather, buckets, scatter of an uneven plan.  The UAMP stage of all
 // buckets runs as merged launches on `st` (one launch per step for every
-// bucket); then, with prof == nullptr, each bucket's polish runs on its own
-// stream (bucket 0 on `st`), forked from and joined back to `st`; with a
-// profiler they run one after another on `st`.
+// bucket); then, with prof == nullptr, every polish step is one launch over
+// all buckets (polish_run_multi); with a profiler the buckets' polishes run
+// one after another on `st`.
 void replay_uneven(FbmePlan* P, const float2* y, const FbmeOutputs& out, cudaStream_t st,
                    fbme::Profiler* prof) {
   float2* ybuf = reinterpret_cast<float2*>(P->ws + P->stg.y);
@@ -865,18 +865,21 @@ void replay_uneven(FbmePlan* P, const float2* y, const FbmeOutputs& out, cudaStr
   fbme::uamp_run_multi(jobs.data(), nb, st, prof, P->streams.data(), P->events.data(),
                        static_cast<int>(P->streams.size()));
   if (!prof) {
-    cudaEventRecord(P->events[0], st);
-    for (int b = 1; b < nb; ++b) cudaStreamWaitEvent(P->streams[b - 1], P->events[0], 0);
-  }
-  for (int b = 0; b < nb; ++b) {
-    const Bucket& k = P->bk[b];
-    cudaStream_t sb = (prof || b == 0) ? st : P->streams[b - 1];
-    polish_bucket(k, ybuf + k.smp0, bucket_outputs(P, k, out), sb, prof);
-  }
-  if (!prof) {
-    for (int b = 1; b < nb; ++b) {
-      cudaEventRecord(P->events[b], P->streams[b - 1]);
-      cudaStreamWaitEvent(st, P->events[b], 0);
+    // every polish step is one launch over all buckets
+    std::vector<fbme::PolishBucket> pb(nb);
+    for (int b = 0; b < nb; ++b) {
+      const Bucket& k = P->bk[b];
+      pb[b].s = k.s;
+      pb[b].c = k.dc;
+      pb[b].p = k.p;
+      pb[b].p.y = ybuf + k.smp0;
+      pb[b].out = bucket_outputs(P, k, out);
+    }
+    fbme::polish_run_multi(pb.data(), nb, st);
+  } else {
+    for (int b = 0; b < nb; ++b) {
+      const Bucket& k = P->bk[b];
+      polish_bucket(k, ybuf + k.smp0, bucket_outputs(P, k, out), st, prof);
     }
   }
   const ScatterArgs a = scatter_args(P, out);

@@ -189,6 +189,43 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
 size_t polish_state_bytes();
 int topk_slices(long long n);
+
+// Several shape buckets' top-k in one launch each (uneven plans): bucket i
+// is blockIdx.z = i, its scenes and slices in blockIdx.y / x.
+constexpr int kBucketSetMax = 64;
+struct TopkJob {
+  const uint32_t* keys;  // [B][n]
+  long long n;
+  int k, B;
+  uint32_t* cand_key;
+  int* cand_idx;
+};
+struct TopkJobs {
+  int n;
+  TopkJob j[kBucketSetMax];
+};
+struct TopkMergeJob {
+  const uint32_t* cand_key;
+  const int* cand_idx;
+  int ncand, k, B;
+  int* out_idx;
+  float* out_val;
+};
+struct TopkMergeJobs {
+  int n;
+  TopkMergeJob j[kBucketSetMax];
+};
+void launch_topk_blocks_multi(const TopkJobs& J, int max_slices, int max_b, cudaStream_t st);
+void launch_topk_merge_multi(const TopkMergeJobs& J, int max_b, cudaStream_t st);
+// The polish of several equal-config shape buckets (an uneven plan's) as
+// one launch per step: results equal polish_run per bucket.
+struct PolishBucket {
+  BatchShape s;
+  DevConfig c;
+  PolishBuffers p;
+  FbmeOutputs out;
+};
+void polish_run_multi(const PolishBucket* b, int n, cudaStream_t st);
 // Observation masks (mask.cu): set-up (normalised mask, observed count,
 // 2-D Gram table; synchronises `st`) and the masked copy of the data.
 size_t mask_gram_scratch_bytes(const BatchShape& s);

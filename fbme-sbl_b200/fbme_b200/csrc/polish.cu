@@ -20,6 +20,9 @@
 // The evidence (log-determinant + quadratic form) is accumulated in FP64.
 #include <math.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "topk.cuh"
@@ -382,12 +385,11 @@ constexpr int kPolishWarps = 1;
 // Evaluations p in [state.evals, P) until done or an exchange is needed.
 // phase 0: initialise from the top-K; phase 1: apply the exchange whose
 // candidates are in p.xcand_*, then continue.
-__global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A, int phase) {
+FBME_DEV void polish_body(const PolishArgs& A, int phase, int scene) {
   __shared__ float2 Msm[kPolishWarps][32][33];
   __shared__ float2 Xsm[kPolishWarps][32][33];
   extern __shared__ float2 dtab[];  // D1 (n1) then D2 (n2)
   const int lane = threadIdx.x & 31;
-  const int scene = blockIdx.x * kPolishWarps + (threadIdx.x >> 5);
   if (scene >= A.s.B) return;
   const BatchShape& s = A.s;
   const DevConfig& c = A.c;
@@ -544,6 +546,9 @@ __global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A,
   }
   if (status && lane == 0) atomicOr(&A.p.status[scene], status);
 }
+__global__ void __launch_bounds__(32 * kPolishWarps) polish_kernel(PolishArgs A, int phase) {
+  polish_body(A, phase, blockIdx.x * kPolishWarps + (threadIdx.x >> 5));
+}
 
 // Residual exchange scoring (solver.py:4398-4412) without the M-space
 // residual: score[n] = |A^H y[n] - sum_k mu_k D1[n1-a_k] D2[n2-b_k]|^2 over
@@ -577,8 +582,7 @@ struct ExTile {
 // with double-buffered rows measured slower, its 8 warps too few to keep
 // the FMA pipes fed.
 template <typename T>
-__global__ void __launch_bounds__(T::threads, 2)
-exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
+FBME_DEV void exchange_body(const PolishArgs& A, uint32_t* cand_key, int* cand_idx, int scene, int bx, int nbx) {
   constexpr int RPT = T::RPT, TX = T::TX;
   extern __shared__ float4 ex_shm4[];
   __shared__ TopkPrunedShared S;
@@ -587,7 +591,7 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
   __shared__ int atom_a[kMaxPolish], atom_b[kMaxPolish];
   __shared__ float2 atom_mu[kMaxPolish];
   const BatchShape& s = A.s;
-  const int scene = blockIdx.y, r0 = blockIdx.x * T::rows;
+  const int r0 = bx * T::rows;
   const int K = A.c.polish_size, E = A.c.exchange;
   const int N1 = s.n1, N2 = s.n2;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
@@ -716,13 +720,19 @@ exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
           key[i] = act ? 0u : float_key_t(abs_sq(d));
         }
       }
-  const size_t off = (static_cast<size_t>(scene) * gridDim.x + blockIdx.x) * E;
+  const size_t off = (static_cast<size_t>(scene) * nbx + bx) * E;
   auto gidx = [&](int i) {
     const int r = i / (2 * T::pairs), c = (i / 2) % T::pairs, j = i & 1;
     return (r0 + ty * RPT + r) * N2 + 2 * tx + 2 * TX * c + j;
   };
   // residual scores of one CTA crowd into few top-byte bins (radix fallback)
   block_topk_pruned<T::kpt, true>(key, valid, gidx, E, S, cand_key + off, cand_idx + off);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(T::threads, 2)
+exchange_kernel(PolishArgs A, uint32_t* cand_key, int* cand_idx) {
+  exchange_body<T>(A, cand_key, cand_idx, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 using ExSmall = ExTile<8, 2, 32, 256, 64>;
@@ -732,10 +742,9 @@ using ExWidest = ExTile<4, 8, 64, 256, 512>;
 
 // Final K-space outputs, fixed-budget diagnostics, effective DOF
 // (solver.py:1989-2021, 2081-2092, 3408-3496, 2108-2126).
-__global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOutputs out) {
+FBME_DEV void polish_finish_body(const PolishArgs& A, const FbmeOutputs& out, int scene) {
   extern __shared__ float2 dtab[];
   const int lane = threadIdx.x & 31;
-  const int scene = blockIdx.x;
   if (scene >= A.s.B) return;
   const BatchShape& s = A.s;
   const DevConfig& c = A.c;
@@ -803,21 +812,23 @@ __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOut
     }
   }
 }
+__global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOutputs out) {
+  polish_finish_body(A, out, blockIdx.x);
+}
 
 // N-space outputs in one pass: zero mean, floor variance and 1/floor
 // precision off the active set, and the active entries.  Block b of a scene
 // owns the contiguous pixel range [e0, e1): it fills the range, then its
 // threads k < K write active atom k where it falls inside the range, so no
 // other block touches those pixels and one launch replaces fill + scatter.
-__global__ void __launch_bounds__(256) output_kernel(PolishArgs A, FbmeOutputs out) {
+FBME_DEV void output_body(const PolishArgs& A, const FbmeOutputs& out, int scene, int bx, int nbx) {
   const BatchShape& s = A.s;
   const long long N = s.n();
-  const int scene = blockIdx.y;
   const int K = A.c.polish_size;
   const float fl = A.p.sc.floor_[scene];
   const float inv = 1.0f / fl;
-  const long long chunk = (N + gridDim.x - 1) / gridDim.x;
-  const long long e0 = blockIdx.x * chunk, e1 = min(N, e0 + chunk);
+  const long long chunk = (N + nbx - 1) / nbx;
+  const long long e0 = bx * chunk, e1 = min(N, e0 + chunk);
   float2* x = reinterpret_cast<float2*>(out.x) + scene * N;
   float* pv = out.posterior_variance + scene * N;
   float* pr = out.precision + scene * N;
@@ -834,7 +845,7 @@ __global__ void __launch_bounds__(256) output_kernel(PolishArgs A, FbmeOutputs o
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
   const int idx = ps->active[k];
   const float2 mu = ps->best_mean[k];
-  if (blockIdx.x == 0 && out.active_values) reinterpret_cast<float2*>(out.active_values)[scene * K + k] = mu;
+  if (bx == 0 && out.active_values) reinterpret_cast<float2*>(out.active_values)[scene * K + k] = mu;
   if (idx < e0 || idx >= e1) return;
   const float apv = ps->best_pv[k];
   x[idx] = mu;
@@ -845,11 +856,52 @@ __global__ void __launch_bounds__(256) output_kernel(PolishArgs A, FbmeOutputs o
     mk[idx] = (abs_sq(mu) / fmaxf(apv, kTinyP)) > thr;
   }
 }
+__global__ void __launch_bounds__(256) output_kernel(PolishArgs A, FbmeOutputs out) {
+  output_body(A, out, blockIdx.y, blockIdx.x, gridDim.x);
+}
 
 void launch_topk_blocks(const uint32_t* keys, long long n, int k, int B, uint32_t* cand_key, int* cand_idx,
                         cudaStream_t st);
 void launch_topk_merge(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, int B,
                        int* out_idx, float* out_val, cudaStream_t st);
+
+// The polish steps of several shape buckets (an uneven plan's), one launch
+// each: bucket i is blockIdx.z = i with its own arguments; blocks past its
+// scenes or blocks return, and every scene runs the single-bucket code.
+struct PolishSet {
+  int n;
+  PolishArgs a[kBucketSetMax];
+  FbmeOutputs out[kBucketSetMax];
+  int ex_blocks[kBucketSetMax];   // exchange row blocks per scene
+  int out_blocks[kBucketSetMax];  // output blocks per scene
+};
+static_assert(sizeof(PolishSet) <= 32764, "kernel parameter limit");
+
+FBME_DEV bool has_exchange(const DevConfig& c) { return c.exchange > 0 && c.polish_iters > 1; }
+
+__global__ void __launch_bounds__(32 * kPolishWarps) polish_set_kernel(const PolishSet S, int phase) {
+  const PolishArgs& A = S.a[blockIdx.z];
+  if (phase == 1 && !has_exchange(A.c)) return;
+  polish_body(A, phase, blockIdx.x * kPolishWarps + (threadIdx.x >> 5));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(T::threads, 2) exchange_set_kernel(const PolishSet S) {
+  const PolishArgs& A = S.a[blockIdx.z];
+  const int nbx = S.ex_blocks[blockIdx.z];
+  if (static_cast<int>(blockIdx.x) >= nbx || static_cast<int>(blockIdx.y) >= A.s.B) return;
+  exchange_body<T>(A, A.p.cand_key, A.p.cand_idx, blockIdx.y, blockIdx.x, nbx);
+}
+
+__global__ void __launch_bounds__(32) polish_finish_set_kernel(const PolishSet S) {
+  polish_finish_body(S.a[blockIdx.z], S.out[blockIdx.z], blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) output_set_kernel(const PolishSet S) {
+  const int nbx = S.out_blocks[blockIdx.z];
+  if (static_cast<int>(blockIdx.x) >= nbx || static_cast<int>(blockIdx.y) >= S.a[blockIdx.z].s.B) return;
+  output_body(S.a[blockIdx.z], S.out[blockIdx.z], blockIdx.y, blockIdx.x, nbx);
+}
 
 static int exchange_rows(int n2) {
   return n2 <= 64 ? ExSmall::rows : n2 <= 128 ? ExMid::rows : n2 <= 256 ? ExWide::rows : ExWidest::rows;
@@ -862,8 +914,12 @@ int exchange_blocks(const BatchShape& s) {
 
 template <typename T>
 static cudaError_t set_exchange_smem() {
-  return cudaFuncSetAttribute(exchange_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(T::smem_bytes(T::n2_max)));
+  cudaError_t e = cudaFuncSetAttribute(exchange_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(T::smem_bytes(T::n2_max)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(exchange_set_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(T::smem_bytes(T::n2_max)));
+  return e;
 }
 
 cudaError_t set_polish_attributes() {
@@ -955,6 +1011,106 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, dsm, st>>>(A, out)));
   const int fb = static_cast<int>((s.n() + 2047) / 2048);
   FBME_TIMED(prof, FBME_GROUP_OUTPUT, (output_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(A, out)));
+}
+
+// The polish of an uneven plan's buckets, one launch per step over all of
+// them (at most kBucketSetMax per launch), in polish_run's order.  Buckets
+// under an observation mask take polish_run.
+static int exchange_class(int n2) { return n2 <= 64 ? 0 : n2 <= 128 ? 1 : n2 <= 256 ? 2 : 3; }
+
+template <typename T>
+static void launch_exchange_set(const PolishSet& S, int max_blocks, int max_b, int max_n2, cudaStream_t st) {
+  exchange_set_kernel<T><<<dim3(max_blocks, max_b, S.n), T::threads, T::smem_bytes(max_n2), st>>>(S);
+}
+
+void polish_run_multi(const PolishBucket* b, int n, cudaStream_t st) {
+  for (int c0 = 0; c0 < n; c0 += kBucketSetMax) {
+    const int cnt = n - c0 < kBucketSetMax ? n - c0 : kBucketSetMax;
+    std::vector<int> plain;  // set members (masked buckets run on their own)
+    for (int i = 0; i < cnt; ++i) {
+      const PolishBucket& k = b[c0 + i];
+      if (k.p.gram2d) {
+        polish_run(k.s, k.c, k.p, k.out, st);
+        if (k.out.status && k.out.status != k.p.status)
+          cudaMemcpyAsync(k.out.status, k.p.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
+      } else {
+        plain.push_back(c0 + i);
+      }
+    }
+    if (plain.empty()) continue;
+    const int m = static_cast<int>(plain.size());
+    auto* S = new PolishSet();  // ~31 KB: not on the stack
+    TopkJobs tj{};
+    TopkMergeJobs tm{}, tx{};
+    S->n = m;
+    tj.n = tm.n = m;
+    int max_b = 1, max_slices = 1, max_out = 1;
+    size_t dsm = 0;
+    for (int i = 0; i < m; ++i) {
+      const PolishBucket& k = b[plain[i]];
+      const int K = k.c.polish_size, sl = topk_slices(k.s.n());
+      S->a[i] = PolishArgs{k.s, k.c, k.p};
+      S->out[i] = k.out;
+      S->ex_blocks[i] = exchange_blocks(k.s);
+      const int fb = static_cast<int>((k.s.n() + 2047) / 2048);
+      S->out_blocks[i] = fb < 64 ? fb : 64;
+      tj.j[i] = TopkJob{k.p.keys, k.s.n(), K, k.s.B, k.p.cand_key, k.p.cand_idx};
+      tm.j[i] = TopkMergeJob{k.p.cand_key, k.p.cand_idx, sl * K, K, k.s.B, k.p.active, k.p.score};
+      max_b = std::max(max_b, k.s.B);
+      max_slices = std::max(max_slices, sl);
+      max_out = std::max(max_out, S->out_blocks[i]);
+      dsm = std::max(dsm, static_cast<size_t>(k.s.n1 + k.s.n2) * sizeof(float2));
+    }
+    launch_topk_blocks_multi(tj, max_slices, max_b, st);
+    launch_topk_merge_multi(tm, max_b, st);
+    const int pb = (max_b + kPolishWarps - 1) / kPolishWarps;
+    polish_set_kernel<<<dim3(pb, 1, m), 32 * kPolishWarps, dsm, st>>>(*S, 0);
+    // the exchange, one launch per row-tile class, then its candidates' merge
+    bool any = false;
+    for (int cls = 0; cls < 4; ++cls) {
+      auto* X = new PolishSet();
+      int xb = 1, xbl = 1, xn2 = 1;
+      X->n = 0;
+      for (int i = 0; i < m; ++i) {
+        const PolishArgs& A = S->a[i];
+        if (!(A.c.exchange > 0 && A.c.polish_iters > 1) || exchange_class(A.s.n2) != cls) continue;
+        X->a[X->n] = A;
+        X->ex_blocks[X->n] = S->ex_blocks[i];
+        xb = std::max(xb, A.s.B);
+        xbl = std::max(xbl, S->ex_blocks[i]);
+        xn2 = std::max(xn2, A.s.n2);
+        ++X->n;
+      }
+      if (X->n > 0) {
+        any = true;
+        if (cls == 0) launch_exchange_set<ExSmall>(*X, xbl, xb, xn2, st);
+        else if (cls == 1) launch_exchange_set<ExMid>(*X, xbl, xb, xn2, st);
+        else if (cls == 2) launch_exchange_set<ExWide>(*X, xbl, xb, xn2, st);
+        else launch_exchange_set<ExWidest>(*X, xbl, xb, xn2, st);
+      }
+      delete X;
+    }
+    if (any) {
+      tx.n = 0;
+      for (int i = 0; i < m; ++i) {
+        const PolishArgs& A = S->a[i];
+        if (!(A.c.exchange > 0 && A.c.polish_iters > 1)) continue;
+        const int E = A.c.exchange;
+        tx.j[tx.n++] = TopkMergeJob{A.p.cand_key, A.p.cand_idx, S->ex_blocks[i] * E, E, A.s.B, A.p.xcand_idx,
+                                    A.p.xcand_val};
+      }
+      launch_topk_merge_multi(tx, max_b, st);
+      polish_set_kernel<<<dim3(pb, 1, m), 32 * kPolishWarps, dsm, st>>>(*S, 1);
+    }
+    polish_finish_set_kernel<<<dim3(max_b, 1, m), 32, dsm, st>>>(*S);
+    output_set_kernel<<<dim3(max_out, max_b, m), 256, 0, st>>>(*S);
+    for (int i = 0; i < m; ++i) {
+      const PolishBucket& k = b[plain[i]];
+      if (k.out.status && k.out.status != k.p.status)
+        cudaMemcpyAsync(k.out.status, k.p.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    }
+    delete S;
+  }
 }
 
 }  // namespace fbme

@@ -19,15 +19,15 @@ constexpr int kTopkBlockThreads = 512;
 constexpr int kTopkKpt = 16;
 constexpr int kTopkSlice = kTopkBlockThreads * kTopkKpt;  // 8192 keys per CTA
 constexpr int kMergeMax = 2048;
+FBME_DEV int topk_slices_dev(long long n) { return static_cast<int>((n + kTopkSlice - 1) / kTopkSlice); }
 
 // FROM_SCORES: `in` holds float scores (converted to keys); else keys.
 // The slice's k best lie among its keys at or above the k-th largest
 // thread maximum (radix bound), typically a few dozen of the 8192.
 template <bool FROM_SCORES>
-__global__ void __launch_bounds__(kTopkBlockThreads, 2)
-topk_blocks_kernel(const void* in, long long n, int k, uint32_t* cand_key, int* cand_idx) {
+FBME_DEV void topk_blocks_body(const void* in, long long n, int k, uint32_t* cand_key, int* cand_idx, int scene,
+                               int blk, int nblk) {
   __shared__ TopkPrunedShared S;
-  const int scene = blockIdx.y, blk = blockIdx.x;
   const uint32_t* kp = static_cast<const uint32_t*>(in) + scene * n;
   const float* sp = static_cast<const float*>(in) + scene * n;
   const long long base = static_cast<long long>(blk) * kTopkSlice + threadIdx.x;
@@ -42,18 +42,31 @@ topk_blocks_kernel(const void* in, long long n, int k, uint32_t* cand_key, int* 
       key[i] = FROM_SCORES ? float_key_t(sp[e]) : kp[e];
     }
   }
-  const size_t off = (static_cast<size_t>(scene) * gridDim.x + blk) * k;
+  const size_t off = (static_cast<size_t>(scene) * nblk + blk) * k;
   block_topk_pruned<kTopkKpt, false, TopkBound::kRadix>(
       key, valid, [&](int i) { return static_cast<int>(base + static_cast<long long>(i) * kTopkBlockThreads); }, k,
       S, cand_key + off, cand_idx + off);
 }
 
+template <bool FROM_SCORES>
+__global__ void __launch_bounds__(kTopkBlockThreads, 2)
+topk_blocks_kernel(const void* in, long long n, int k, uint32_t* cand_key, int* cand_idx) {
+  topk_blocks_body<FROM_SCORES>(in, n, k, cand_key, cand_idx, blockIdx.y, blockIdx.x, gridDim.x);
+}
+
+// Several shape buckets' slices in one launch (blockIdx.z: the bucket;
+// blocks past a bucket's own slices or scenes return).
+__global__ void __launch_bounds__(kTopkBlockThreads, 2) topk_blocks_multi_kernel(const TopkJobs J) {
+  const TopkJob& j = J.j[blockIdx.z];
+  const int nblk = topk_slices_dev(j.n);
+  if (static_cast<int>(blockIdx.x) >= nblk || static_cast<int>(blockIdx.y) >= j.B) return;
+  topk_blocks_body<false>(j.keys, j.n, j.k, j.cand_key, j.cand_idx, blockIdx.y, blockIdx.x, nblk);
+}
+
 template <typename Idx>
-__global__ void __launch_bounds__(1024)
-topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, Idx* out_idx,
-                  float* out_val) {
+FBME_DEV void topk_merge_body(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, Idx* out_idx,
+                              float* out_val, int scene) {
   __shared__ unsigned long long s[kMergeMax];
-  const int scene = blockIdx.x;
   int np = 1;
   while (np < ncand) np <<= 1;
   for (int i = threadIdx.x; i < np; i += blockDim.x) {
@@ -89,7 +102,27 @@ topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int 
   }
 }
 
+template <typename Idx>
+__global__ void __launch_bounds__(1024)
+topk_merge_kernel(const uint32_t* cand_key, const int* cand_idx, int ncand, int k, Idx* out_idx,
+                  float* out_val) {
+  topk_merge_body<Idx>(cand_key, cand_idx, ncand, k, out_idx, out_val, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(1024) topk_merge_multi_kernel(const TopkMergeJobs J) {
+  const TopkMergeJob& j = J.j[blockIdx.z];
+  if (static_cast<int>(blockIdx.x) >= j.B) return;
+  topk_merge_body<int>(j.cand_key, j.cand_idx, j.ncand, j.k, j.out_idx, j.out_val, blockIdx.x);
+}
+
 int topk_slices(long long n) { return static_cast<int>((n + kTopkSlice - 1) / kTopkSlice); }
+
+void launch_topk_blocks_multi(const TopkJobs& J, int max_slices, int max_b, cudaStream_t st) {
+  topk_blocks_multi_kernel<<<dim3(max_slices, max_b, J.n), kTopkBlockThreads, 0, st>>>(J);
+}
+void launch_topk_merge_multi(const TopkMergeJobs& J, int max_b, cudaStream_t st) {
+  topk_merge_multi_kernel<<<dim3(max_b, 1, J.n), 1024, 0, st>>>(J);
+}
 
 void launch_topk_blocks(const uint32_t* keys, long long n, int k, int B, uint32_t* cand_key, int* cand_idx,
                         cudaStream_t st) {
