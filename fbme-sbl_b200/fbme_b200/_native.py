@@ -90,6 +90,27 @@ class FbmeOutputs(ctypes.Structure):
     ]
 
 
+class FbmeCertificate(ctypes.Structure):
+    _fields_ = [
+        ("support_repairs", c_int32),
+        ("coordinate_tolerance", c_float),
+        ("familywise_ratio_threshold", c_float),
+        ("inactive_max_evidence_ratio", c_void_p),
+        ("inactive_best_index", c_void_p),
+        ("inactive_evidence_gain", c_void_p),
+        ("inactive_optimal_variance", c_void_p),
+        ("support_repairs_accepted", c_void_p),
+        ("active_max_evidence_gain", c_void_p),
+        ("active_best_index", c_void_p),
+        ("active_optimal_variance", c_void_p),
+        ("active_max_deletion_gain", c_void_p),
+        ("active_penalized_evidence_gain", c_void_p),
+        ("coordinate_stationary", c_void_p),
+        ("type2_map_coordinate_stationary", c_void_p),
+        ("familywise_no_discovery", c_void_p),
+    ]
+
+
 class FbmeState(ctypes.Structure):
     _fields_ = [
         ("mean", c_void_p),
@@ -193,6 +214,7 @@ SIGNATURES = {
     "fbme_polish_run": (c_int, [c_void_p, c_void_p, POINTER(FbmeOutputs), c_void_p]),
     "fbme_plan_state": (c_int, [c_void_p, POINTER(FbmeState)]),
     "fbme_plan_set_observation_mask": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "fbme_plan_set_certificate": (c_int, [c_void_p, POINTER(FbmeCertificate)]),
     "fbme_plan_set_warm_prior_map": (c_int, [c_void_p, c_void_p]),
     "fbme_selftest_workspace_bytes": (c_size_t, []),
     "fbme_selftest_stage_timeout": (c_int, [c_void_p, c_size_t, c_void_p, c_int64, c_void_p]),

@@ -206,6 +206,8 @@ struct Bucket {
   long long pix0;  // first pixel in bucket order
   long long smp0;  // first sample in bucket order
   float2* ymask;   // masked copy of the observations (under an observation mask)
+  bool certify = false;  // global certificate + support repairs after the polish
+  FbmeCertificate cert{};
 };
 
 // Where scene i (caller order) lives: samples and pixels in the caller's
@@ -584,7 +586,7 @@ void polish_bucket(const Bucket& k, const float2* y, const FbmeOutputs& out, cud
                    fbme::Profiler* prof = nullptr) {
   fbme::PolishBuffers p = k.p;
   p.y = y;
-  fbme::polish_run(k.s, k.dc, p, out, st, prof);
+  fbme::polish_run(k.s, k.dc, p, out, st, prof, k.certify ? &k.cert : nullptr);
   if (out.status != k.status)
     cudaMemcpyAsync(out.status, k.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
 }
@@ -838,7 +840,7 @@ int fbme_polish_run(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme_
     fbme::mask_data(k.s, p.y, k.u.mask, k.ymask, st);
     p.y = k.ymask;
   }
-  fbme::polish_run(k.s, k.dc, p, *out, st);
+  fbme::polish_run(k.s, k.dc, p, *out, st, nullptr, k.certify ? &k.cert : nullptr);
   cudaMemcpyAsync(out->status, k.status, k.s.B * sizeof(int), cudaMemcpyDeviceToDevice, st);
   return check_launch("polish_run");
 }
@@ -1017,6 +1019,34 @@ int fbme_plan_set_observation_mask(FbmePlan* plan, const uint8_t* mask, fbme_str
   k.u.mask = dmask;
   k.p.gram2d = gram;
   k.dc.m_obs = static_cast<float>(observed);
+  return FBME_OK;
+}
+
+int fbme_plan_set_certificate(FbmePlan* plan, const FbmeCertificate* cert) {
+  int rc = single_bucket(plan);
+  if (rc != FBME_OK) return rc;
+  Bucket& k = plan->bk[0];
+  if (!cert) {
+    k.certify = false;
+    k.dc.repairs = 0;
+    return FBME_OK;
+  }
+  if (k.cfg.polish_size < 1)
+    return fail(FBME_ERR_UNSUPPORTED, "the global certificate needs the active-set polish (polish_size >= 1)");
+  if (cert->support_repairs < 0 || cert->support_repairs > 4)
+    return fail(FBME_ERR_INVALID, "uamp_polish_support_repairs must be between 0 and 4.");
+  if (k.cfg.polish_iterations + cert->support_repairs > 8)
+    return fail(FBME_ERR_UNSUPPORTED, "polish iterations + support repairs above 8");
+  if (!cert->inactive_max_evidence_ratio || !cert->inactive_best_index || !cert->inactive_evidence_gain ||
+      !cert->inactive_optimal_variance || !cert->support_repairs_accepted || !cert->active_max_evidence_gain ||
+      !cert->active_best_index || !cert->active_optimal_variance || !cert->active_max_deletion_gain ||
+      !cert->active_penalized_evidence_gain || !cert->coordinate_stationary ||
+      !cert->type2_map_coordinate_stationary ||
+      (cert->familywise_ratio_threshold > 0.f && !cert->familywise_no_discovery))
+    return fail(FBME_ERR_INVALID, "NULL certificate output");
+  k.cert = *cert;
+  k.certify = true;
+  k.dc.repairs = cert->support_repairs;
   return FBME_OK;
 }
 

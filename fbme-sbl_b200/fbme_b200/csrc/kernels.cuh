@@ -59,6 +59,9 @@ struct DevConfig {
   // observed samples per scene under an observation mask (0: the whole
   // M1 x M2 block is observed)
   float m_obs;
+  // support repairs after the polish (global certificate on), whose
+  // evidence extends the trace
+  int repairs;
 };
 
 // Samples a scene's data terms count: the observed ones under a mask.
@@ -185,8 +188,11 @@ struct PolishBuffers {
   int* cand_idx;      // [B][max candidates] their grid indices
   int* status;        // [B] per-scene status
 };
+// `cert` (host copy; null: off) adds the global certificate and support
+// repairs between the polish and its outputs.
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
-                const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr);
+                const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr,
+                const FbmeCertificate* cert = nullptr);
 size_t polish_state_bytes();
 int topk_slices(long long n);
 

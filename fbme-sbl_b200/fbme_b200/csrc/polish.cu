@@ -101,6 +101,7 @@ struct EvalOut {
   float pv, dd;
   double nle;
   int status;
+  float dscale;  // equilibration scale sqrt(S_kk) of lane k's row
 };
 
 FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33], const float2* d1,
@@ -255,6 +256,7 @@ FBME_DEV EvalOut evaluate(const PolishArgs& A, float2 (*M)[33], float2 (*X)[33],
     }
   }
   EvalOut o;
+  o.dscale = dscale;
   o.mean = make_float2(w.x * inv_d, w.y * inv_d);
   // inverse factor column `lane`: X = L^{-1}, eq_var = sum_i |X[i][lane]|^2.
   // Right-looking: when X[q][lane] is final, its contribution L[i][q] X[q]
@@ -749,6 +751,7 @@ FBME_DEV void polish_finish_body(const PolishArgs& A, const FbmeOutputs& out, in
   const BatchShape& s = A.s;
   const DevConfig& c = A.c;
   const int K = c.polish_size, P = c.polish_iters;
+  const int R = c.repairs;
   const bool on = lane < K;
   const PolishScene* ps = reinterpret_cast<const PolishScene*>(A.p.pstate) + scene;
   const float fl = A.p.sc.floor_[scene];
@@ -773,8 +776,10 @@ FBME_DEV void polish_finish_body(const PolishArgs& A, const FbmeOutputs& out, in
     out.noise_variance[scene] = nu;
     out.effective_dof[scene] = dof;
     out.negative_log_evidence[scene] = static_cast<float>(ps->best_nle);
-    for (int p = 0; p < P; ++p) out.evidence_trace[scene * P + p] = ps->trace[p];
+    for (int p = 0; p < P; ++p) out.evidence_trace[scene * (P + R) + p] = ps->trace[p];
     if (out.support_exchanges_accepted) out.support_exchanges_accepted[scene] = ps->exch_acc;
+    // the support repairs append their evidence after the polish's
+    for (int r = 0; r < R; ++r) out.evidence_trace[scene * (P + R) + P + r] = ps->trace[P + r];
     if (out.support_score_threshold && c.false_alarm > 0.f)
       out.support_score_threshold[scene] =
           static_cast<float>(log(static_cast<double>(N) / static_cast<double>(c.false_alarm)));
@@ -814,6 +819,281 @@ FBME_DEV void polish_finish_body(const PolishArgs& A, const FbmeOutputs& out, in
 }
 __global__ void __launch_bounds__(32) polish_finish_kernel(PolishArgs A, FbmeOutputs out) {
   polish_finish_body(A, out, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Global certificate and support repairs (solver.py:3522-3588 inactive
+// certificate, 3219-3317 active certificate, 4511-4628 repairs, 4851-4870
+// and 5388-5460 final diagnostics).  One CTA per scene: warp 0 runs the
+// K-dimensional algebra (evaluate(), as in the polish), every thread scores
+// grid atoms.  For atom j, with g_i = a_j^H a_i from the Dirichlet tables,
+//   q_j   = (A^H y)[j] - sum_i g_i mu_i             (nu a_j^H C^-1 y)
+//   v     = L^-1 D^-1 conj(g)                       (forward substitution)
+//   s_j   = M / nu - ||v||^2 / nu^2                 (a_j^H C^-1 a_j)
+//   rho_j = |q_j / nu|^2 / s_j, and 0 on the active set,
+// where L is the Cholesky factor of the equilibrated reduced system
+// D^-1 (Gamma^-1 + A_S^H A_S / nu) D^-1: the reference obtains the same
+// quantities from K adjoint transforms of the active columns and a
+// K-right-hand-side triangular solve over the grid.
+constexpr int kCertThreads = 256;
+
+struct CertBest {
+  float ratio, prec;
+  int index;
+};
+
+FBME_DEV void cert_pick(CertBest& b, float ratio, float prec, int index) {
+  if (ratio > b.ratio || (ratio == b.ratio && index < b.index)) b = CertBest{ratio, prec, index};
+}
+
+FBME_DEV CertBest cert_warp_best(CertBest b) {
+  for (int off = 16; off > 0; off >>= 1) {
+    const float r = __shfl_xor_sync(0xffffffffu, b.ratio, off);
+    const float p = __shfl_xor_sync(0xffffffffu, b.prec, off);
+    const int i = __shfl_xor_sync(0xffffffffu, b.index, off);
+    cert_pick(b, r, p, i);
+  }
+  return b;
+}
+
+// The active set of one evaluation, staged for the grid scan.
+struct CertModel {
+  int a1[kMaxPolish], a2[kMaxPolish], idx[kMaxPolish];
+  float2 mu[kMaxPolish];
+  float inv_d[kMaxPolish], inv_l[kMaxPolish];
+};
+
+// Largest one-coordinate ratio over the grid (first index on ties, as
+// torch's max), with its atom precision s_j.
+FBME_DEV CertBest cert_scan(const PolishArgs& A, const float2 (*L)[33], const CertModel& m, int K, float nu,
+                            const float2* bp, const float2* d1, const float2* d2, CertBest* red) {
+  const BatchShape& s = A.s;
+  const long long N = s.n();
+  const float Mf = static_cast<float>(observed_samples(s, A.c));
+  const float nu2 = nu * nu;
+  CertBest b{-1.f, 1.f, 0x7fffffff};
+  for (long long j = threadIdx.x; j < N; j += blockDim.x) {
+    const int j1 = static_cast<int>(j / s.n2);
+    const int j2 = static_cast<int>(j - static_cast<long long>(j1) * s.n2);
+    float2 q = __ldg(bp + j);
+    bool act = false;
+    float2 v[kMaxPolish];
+    float red2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < kMaxPolish; ++i) {
+      if (i < K) {
+        act |= m.idx[i] == j;
+        const float2 g = gram_at(A, d1, d2, j1, j2, m.a1[i], m.a2[i]);
+        const float2 mu = m.mu[i];
+        q.x -= g.x * mu.x - g.y * mu.y;
+        q.y -= g.x * mu.y + g.y * mu.x;
+        float2 c = make_float2(g.x * m.inv_d[i], -g.y * m.inv_d[i]);
+#pragma unroll
+        for (int k = 0; k < i; ++k) {
+          const float2 l = L[i][k];
+          c.x -= l.x * v[k].x - l.y * v[k].y;
+          c.y -= l.x * v[k].y + l.y * v[k].x;
+        }
+        v[i] = make_float2(c.x * m.inv_l[i], c.y * m.inv_l[i]);
+        red2 += abs_sq(v[i]);
+      }
+    }
+    const float prec = fmaxf(Mf / nu - red2 / nu2, kTinyP);
+    const float2 qn = make_float2(q.x / nu, q.y / nu);
+    cert_pick(b, act ? 0.f : abs_sq(qn) / prec, prec, static_cast<int>(j));
+  }
+  b = cert_warp_best(b);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[w] = b;
+  __syncthreads();
+  if (w == 0) {
+    b = lane < static_cast<int>(blockDim.x >> 5) ? red[lane] : CertBest{-1.f, 1.f, 0x7fffffff};
+    b = cert_warp_best(b);
+    __syncwarp();
+    if (lane == 0) red[0] = b;
+  }
+  __syncthreads();
+  b = red[0];
+  __syncthreads();
+  return b;
+}
+
+// Inactive certificate of the best atom (solver.py:3568-3588).
+struct CertState {
+  float ratio, gain, optvar;
+  int index;
+};
+
+FBME_DEV CertState cert_state(const CertBest& b) {
+  const bool up = b.ratio > 1.0f;
+  return CertState{b.ratio, up ? b.ratio - 1.0f - logf(fmaxf(b.ratio, kTinyP)) : 0.f,
+                   up ? (b.ratio - 1.0f) / b.prec : 0.f, b.index};
+}
+
+// Lane k's exact one-coordinate terms (solver.py:3244-3290): the current
+// deletion delta, the gain of the optimal variance and that variance.
+struct ActiveTerms {
+  float current, gain, optvar;
+};
+
+FBME_DEV ActiveTerms active_terms(float2 mean, float pv, float gamma) {
+  const float g = fmaxf(gamma, kTinyP);
+  const float2 q = make_float2(mean.x / g, mean.y / g);
+  const float sc = fmaxf((g - pv) / (g * g), kTinyP);
+  const float down = fminf(fmaxf(pv / g, kTinyP), 1.0f);
+  const float loo = fmaxf(sc / down, kTinyP);
+  const float ratio = abs_sq(q) / fmaxf(sc * down, kTinyP);
+  ActiveTerms t;
+  t.optvar = ratio > 1.0f ? (ratio - 1.0f) / loo : 0.f;
+  t.current = -logf(down) - g * abs_sq(q) / down;
+  const float opt = ratio > 1.0f ? logf(fmaxf(ratio, kTinyP)) - ratio + 1.0f : 0.f;
+  t.gain = fmaxf(t.current - opt, 0.f);
+  return t;
+}
+
+// Warp argmax of (value, lane), the first lane on ties.
+FBME_DEV int warp_argmax(float v, float* best) {
+  int pos = threadIdx.x & 31;
+  for (int off = 16; off > 0; off >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int op = __shfl_xor_sync(0xffffffffu, pos, off);
+    if (ov > v || (ov == v && op < pos)) {
+      v = ov;
+      pos = op;
+    }
+  }
+  *best = v;
+  return pos;
+}
+
+__global__ void __launch_bounds__(kCertThreads) certify_kernel(PolishArgs A, FbmeCertificate C) {
+  __shared__ float2 M[32][33];
+  __shared__ float2 X[32][33];
+  __shared__ CertModel model;
+  __shared__ CertBest red[kCertThreads / 32];
+  __shared__ int keep;
+  extern __shared__ float2 dtab[];
+  const int scene = blockIdx.x;
+  if (scene >= A.s.B) return;
+  const BatchShape& s = A.s;
+  const DevConfig& c = A.c;
+  const int K = c.polish_size, P = c.polish_iters, R = c.repairs;
+  const int lane = threadIdx.x & 31;
+  const bool w0 = threadIdx.x < 32, on = lane < K;
+  PolishScene* ps = reinterpret_cast<PolishScene*>(A.p.pstate) + scene;
+  const long long N = s.n();
+  const float2* bp = A.p.bp + scene * N;
+  const float fl = A.p.sc.floor_[scene];
+  const float data_energy = A.p.sc.data_energy[scene];
+  float2* d1 = dtab;
+  float2* d2 = dtab + s.n1;
+  load_dirichlet(A, d1, d2);
+  __syncthreads();
+  const float nu = ps->best_noise;
+  int status = 0;
+  auto stage = [&](int idx, const EvalOut& o) {
+    if (on) {
+      model.idx[lane] = idx;
+      model.a1[lane] = idx / s.n2;
+      model.a2[lane] = idx % s.n2;
+      model.mu[lane] = o.mean;
+      model.inv_d[lane] = 1.0f / o.dscale;
+      model.inv_l[lane] = 1.0f / M[lane][lane].x;
+    }
+  };
+  // the model the polish kept: its factor, then its certificate
+  if (w0) {
+    const int idx = on ? ps->active[lane] : 0;
+    const float gam = on ? ps->best_gamma[lane] : 1.0f;
+    const EvalOut o = evaluate(A, M, X, d1, d2, K, idx, gam, nu, on ? bp[idx] : make_float2(0.f, 0.f),
+                               data_energy);
+    status |= o.status;
+    stage(idx, o);
+  }
+  __syncthreads();
+  CertState cur = cert_state(cert_scan(A, M, model, K, nu, bp, d1, d2, red));
+  // support repairs (solver.py:4511-4628): the best inactive atom replaces
+  // the active atom of largest deletion delta, with variance
+  // max(optimal, floor); kept when the exact evidence does not rise
+  for (int r = 0; r < R; ++r) {
+    EvalOut o{};
+    int idx = 0;
+    float gam = 1.0f;
+    if (w0) {
+      const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+      const float pv = on ? ps->best_pv[lane] : 0.f;
+      gam = on ? ps->best_gamma[lane] : 1.0f;
+      idx = on ? ps->active[lane] : 0;
+      float dmax;
+      const int pos = warp_argmax(on ? deletion_gain(mu, pv, gam) : -INFINITY, &dmax);
+      if (lane == pos) {
+        idx = cur.index;
+        gam = fmaxf(cur.optvar, fl);
+      }
+      o = evaluate(A, M, X, d1, d2, K, idx, gam, nu, on ? bp[idx] : make_float2(0.f, 0.f), data_energy);
+      status |= o.status;
+      stage(idx, o);
+    }
+    __syncthreads();
+    const CertState next = cert_state(cert_scan(A, M, model, K, nu, bp, d1, d2, red));
+    if (w0) {
+      const bool accept = cur.ratio > 1.0f && isfinite(o.nle) &&
+                          static_cast<float>(o.nle) <= static_cast<float>(ps->best_nle);
+      __syncwarp();
+      if (accept) {
+        if (on) {
+          ps->active[lane] = idx;
+          ps->best_mean[lane] = o.mean;
+          ps->best_pv[lane] = o.pv;
+          ps->best_dd[lane] = o.dd;
+          ps->best_gamma[lane] = gam;
+        }
+        if (lane == 0) {
+          ps->best_nle = o.nle;
+          ps->exch_acc += 1;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        ps->trace[P + r] = static_cast<float>(ps->best_nle);
+        keep = accept;
+      }
+    }
+    __syncthreads();
+    if (keep) cur = next;
+  }
+  if (!w0) return;
+  // final certificate (solver.py:4851-4870, 5388-5460)
+  const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+  const float pv = on ? ps->best_pv[lane] : 0.f;
+  const float g = on ? ps->best_gamma[lane] : 1.0f;
+  const int idx = on ? ps->active[lane] : 0;
+  const ActiveTerms t = active_terms(mu, pv, g);
+  float max_gain, max_nondel, max_del;
+  const int gp = warp_argmax(on ? t.gain : -INFINITY, &max_gain);
+  warp_argmax(on ? (t.optvar > 0.f ? t.gain : 0.f) : -INFINITY, &max_nondel);
+  warp_argmax(on ? t.current : -INFINITY, &max_del);
+  const int best_idx = __shfl_sync(0xffffffffu, idx, gp);
+  const float best_var = __shfl_sync(0xffffffffu, t.optvar, gp);
+  status = __reduce_or_sync(0xffffffffu, status);
+  if (lane != 0) return;
+  if (status) atomicOr(&A.p.status[scene], status);
+  const float tol = C.coordinate_tolerance;
+  const float pen = fmaxf(max_nondel, fmaxf(max_del, 0.f));
+  C.inactive_max_evidence_ratio[scene] = cur.ratio;
+  C.inactive_best_index[scene] = cur.index;
+  C.inactive_evidence_gain[scene] = cur.gain;
+  C.inactive_optimal_variance[scene] = cur.optvar;
+  C.support_repairs_accepted[scene] = ps->exch_acc;
+  C.active_max_evidence_gain[scene] = max_gain;
+  C.active_best_index[scene] = best_idx;
+  C.active_optimal_variance[scene] = best_var;
+  C.active_max_deletion_gain[scene] = max_del;
+  C.active_penalized_evidence_gain[scene] = pen;
+  C.coordinate_stationary[scene] = cur.gain <= tol && max_gain <= tol;
+  C.type2_map_coordinate_stationary[scene] = fmaxf(cur.gain, 0.f) <= tol && pen <= tol;
+  if (C.familywise_ratio_threshold > 0.f)
+    C.familywise_no_discovery[scene] = cur.ratio <= C.familywise_ratio_threshold;
 }
 
 // N-space outputs in one pass: zero mean, floor variance and 1/floor
@@ -974,7 +1254,7 @@ static void launch_exchange(const PolishArgs& A, const PolishBuffers& p, cudaStr
 }
 
 void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
-                const FbmeOutputs& out, cudaStream_t st, Profiler* prof) {
+                const FbmeOutputs& out, cudaStream_t st, Profiler* prof, const FbmeCertificate* cert) {
   PolishArgs A{s, c, p};
   const int K = c.polish_size;
   // each launch timed on its own, so the profile counts launches
@@ -1008,6 +1288,8 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                                  p.xcand_idx, p.xcand_val, st));
     FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 1)));
   }
+  if (cert)
+    FBME_TIMED(prof, FBME_GROUP_POLISH, (certify_kernel<<<s.B, kCertThreads, dsm, st>>>(A, *cert)));
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, dsm, st>>>(A, out)));
   const int fb = static_cast<int>((s.n() + 2047) / 2048);
   FBME_TIMED(prof, FBME_GROUP_OUTPUT, (output_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(A, out)));

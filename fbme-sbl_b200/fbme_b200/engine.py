@@ -113,8 +113,7 @@ def check_supported(cfg: SBLConfig) -> None:
     unsupported = {
         "joint_sparsity": cfg.joint_sparsity,
         "spatial_coupling": cfg.spatial_coupling > 0.0 or cfg.learn_spatial_coupling,
-        "uamp_polish_global_certificate": cfg.uamp_polish_global_certificate,
-        "uamp_polish_support_repairs": cfg.uamp_polish_support_repairs != 0,
+        "uamp_polish_support_prior": cfg.uamp_polish_support_prior,
         "uamp_polish_support_growth_steps": cfg.uamp_polish_support_growth_steps != 0,
         "uamp_polish_support_shrink_steps": cfg.uamp_polish_support_shrink_steps != 0,
         "uamp_polish_coordinate_steps": cfg.uamp_polish_coordinate_steps != 0,
@@ -130,10 +129,33 @@ def check_supported(cfg: SBLConfig) -> None:
         raise NotImplementedError(
             "mode='uamp' runs the fixed UAMP budget on the device; set tol=0 "
             "(every UAMP preset does)")
+    if cfg.uamp_polish_global_certificate and (
+            cfg.uamp_polish_iterations + cfg.uamp_polish_support_repairs > 8):
+        raise NotImplementedError(
+            "the device certificate keeps at most 8 evidence values: "
+            "uamp_polish_iterations + uamp_polish_support_repairs <= 8")
     if cfg.uamp_polish_size < 1 or not cfg.uamp_polish_prune_tail:
         raise NotImplementedError(
             "the device UAMP path implements the zero-tail active-set polish "
             "(uamp_polish_size >= 1 and uamp_polish_prune_tail=True, as in the FBME presets)")
+
+
+def ratio_threshold_for_evidence_tolerance(tolerance: float) -> float:
+    """The rho >= 1 with rho - 1 - log(rho) = tolerance, the inactive-ratio
+    form of the stationarity tolerance (torch_sbl/solver.py:3499-3519): an
+    upper bound by doubling, then 64 bisection steps."""
+    if tolerance <= 0.0:
+        return 1.0
+    lo, hi = 1.0, 2.0
+    while hi - 1.0 - log(hi) < tolerance:
+        hi *= 2.0
+    for _ in range(64):
+        mid = 0.5 * (lo + hi)
+        if mid - 1.0 - log(mid) < tolerance:
+            lo = mid
+        else:
+            hi = mid
+    return hi
 
 
 class FBMEEngine:
@@ -187,6 +209,8 @@ class FBMEEngine:
         self._ws_ptr = (base + 255) & ~255
         B, N, K = self.batch, self.n_grid, self.native_cfg.polish_size
         P = self.native_cfg.polish_iterations
+        self.certify = bool(cfg.uamp_polish_global_certificate)
+        R = int(cfg.uamp_polish_support_repairs) if self.certify else 0
         f32 = dict(dtype=torch.float32, device=device)
         self.out = {
             "x": torch.zeros(B, N, dtype=torch.complex64, device=device),
@@ -196,7 +220,7 @@ class FBMEEngine:
             "noise_variance": torch.zeros(B, **f32),
             "effective_dof": torch.zeros(B, **f32),
             "negative_log_evidence": torch.zeros(B, **f32),
-            "evidence_trace": torch.zeros(B, P, **f32),
+            "evidence_trace": torch.zeros(B, P + R, **f32),
             "support_exchanges_accepted": torch.zeros(B, dtype=torch.int64, device=device),
             "fixed_budget_gamma_residual": torch.zeros(B, **f32),
             "fixed_budget_noise_residual": torch.zeros(B, **f32),
@@ -224,10 +248,38 @@ class FBMEEngine:
                 rc = self.lib.fbme_plan_set_observation_mask(self._plan, ctypes.c_void_p(self.mask.data_ptr()),
                                                              ctypes.c_void_p(st.cuda_stream))
             nat.check(rc, "fbme_plan_set_observation_mask")
+        if self.certify:
+            self._set_certificate(R)
         # constant result fields of the zero-tail polish (solver.py:4052-4068, 4639-4653)
         self._false = torch.zeros(B, dtype=torch.bool, device=device)
         self._true = torch.ones(B, dtype=torch.bool, device=device)
         self._zero = torch.zeros(B, **f32)
+
+    def _set_certificate(self, repairs: int) -> None:
+        """Device outputs of the global certificate and support repairs
+        (solver.py:4511-4628, 4851-4870, 5388-5460), registered with the plan."""
+        cfg, B, dev = self.cfg, self.batch, self.device
+        fwer = cfg.uamp_polish_familywise_error_rate
+        inactive = max(self.n_grid - int(self.native_cfg.polish_size), 1)
+        self.fw_threshold = log(inactive / fwer) if fwer is not None else None
+        self.stationarity_threshold = ratio_threshold_for_evidence_tolerance(
+            cfg.uamp_polish_coordinate_tolerance)
+        floats = ("inactive_max_evidence_ratio", "inactive_evidence_gain", "inactive_optimal_variance",
+                  "active_max_evidence_gain", "active_optimal_variance", "active_max_deletion_gain",
+                  "active_penalized_evidence_gain")
+        ints = ("inactive_best_index", "support_repairs_accepted", "active_best_index")
+        flags = ("coordinate_stationary", "type2_map_coordinate_stationary", "familywise_no_discovery")
+        self.cert = {k: torch.zeros(B, dtype=torch.float32, device=dev) for k in floats}
+        self.cert.update({k: torch.zeros(B, dtype=torch.int64, device=dev) for k in ints})
+        self.cert.update({k: torch.zeros(B, dtype=torch.bool, device=dev) for k in flags})
+        c = nat.FbmeCertificate()
+        c.support_repairs = repairs
+        c.coordinate_tolerance = cfg.uamp_polish_coordinate_tolerance
+        c.familywise_ratio_threshold = self.fw_threshold if self.fw_threshold is not None else 0.0
+        for name, _ in nat.FbmeCertificate._fields_[3:]:
+            setattr(c, name, self.cert[name].data_ptr())
+        self._certificate = c
+        nat.check(self.lib.fbme_plan_set_certificate(self._plan, ctypes.byref(c)), "fbme_plan_set_certificate")
 
     # ------------------------------------------------------------------ runs
     def _stream(self) -> int:
@@ -327,7 +379,11 @@ class FBMEEngine:
         fb = bool(self.native_cfg.fixed_budget_diagnostics)
         has_mask = cfg.uamp_support_false_alarm_budget is not None
         nle = o["negative_log_evidence"].reshape(batch_shape)
+        extra = self._certificate_fields(batch_shape) if self.certify else {}
+        if self.certify:  # residual exchanges and repairs share one counter
+            exch = extra.pop("support_repairs_accepted")
         return SBLResult(
+            **extra,
             x=o["x"].reshape(out_shape),
             posterior_variance=o["posterior_variance"].reshape(out_shape),
             precision=o["precision"].reshape(out_shape),
@@ -360,6 +416,36 @@ class FBMEEngine:
                                      if has_mask else None),
             status=o["status"].reshape(batch_shape),
         )
+
+    def _certificate_fields(self, batch_shape: tuple[int, ...]) -> dict:
+        """The certificate's result fields (solver.py:2196-2330), with the
+        support log-odds penalty zero (no support prior)."""
+        c = {k: v.reshape(batch_shape) for k, v in self.cert.items()}
+        thr = torch.full(batch_shape, self.stationarity_threshold, dtype=torch.float32, device=self.device)
+        f = dict(
+            inactive_max_evidence_ratio=c["inactive_max_evidence_ratio"],
+            inactive_best_index=c["inactive_best_index"],
+            inactive_evidence_gain=c["inactive_evidence_gain"],
+            inactive_optimal_variance=c["inactive_optimal_variance"],
+            support_repairs_accepted=c["support_repairs_accepted"],
+            active_max_evidence_gain=c["active_max_evidence_gain"],
+            active_best_index=c["active_best_index"],
+            active_optimal_variance=c["active_optimal_variance"],
+            active_max_deletion_gain=c["active_max_deletion_gain"],
+            coordinate_stationary=c["coordinate_stationary"],
+            type2_coordinate_stationary=c["coordinate_stationary"],
+            inactive_ratio_threshold=thr,
+            stationarity_ratio_threshold=thr,
+            inactive_penalized_evidence_gain=c["inactive_evidence_gain"],
+            active_penalized_evidence_gain=c["active_penalized_evidence_gain"],
+            type2_map_coordinate_stationary=c["type2_map_coordinate_stationary"],
+        )
+        if self.fw_threshold is not None:
+            f.update(familywise_ratio_threshold=torch.full(batch_shape, self.fw_threshold, dtype=torch.float32,
+                                                           device=self.device),
+                     familywise_no_discovery=c["familywise_no_discovery"],
+                     familywise_support_certified=c["familywise_no_discovery"])
+        return f
 
     def close(self) -> None:
         if getattr(self, "_plan", None) is not None and self._plan.value:

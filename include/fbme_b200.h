@@ -208,6 +208,41 @@ int fbme_plan_state(FbmePlan* plan, FbmeState* state);
  * plan returns FBME_ERR_UNSUPPORTED; an all-zero mask FBME_ERR_INVALID. */
 int fbme_plan_set_observation_mask(FbmePlan* plan, const uint8_t* mask, fbme_stream_t stream);
 
+/* Global certificate and support repairs of the active-set polish
+ * (uamp_polish_global_certificate / uamp_polish_support_repairs, the
+ * certified_hybrid_uamp configuration), replacing _inactive_evidence_certificate
+ * (torch_sbl/solver.py:3522-3588), _active_evidence_certificate (3219-3317),
+ * the repair loop (4511-4628) and the final coordinate diagnostics
+ * (4851-4870, 5388-5460) of _uamp_active_em_polish.  After the polish the
+ * plan scores every grid atom j by its one-coordinate Type-II ratio
+ * |a_j^H C^-1 y|^2 / a_j^H C^-1 a_j, lets the best inactive atom replace the
+ * active atom of largest deletion gain up to `support_repairs` times (kept
+ * when the exact evidence does not rise), and writes the certificate of the
+ * final model.  Every output is a device array of B entries; the evidence
+ * trace of FbmeOutputs then holds P + support_repairs entries per scene.
+ * The tolerance-to-ratio threshold is computed by the caller.  Call before
+ * replays are captured; NULL switches the certificate off.  An uneven plan
+ * returns FBME_ERR_UNSUPPORTED. */
+typedef struct {
+  int32_t support_repairs;                  /* R in [0, 4], P + R <= 8 */
+  float coordinate_tolerance;               /* gains <= tolerance are stationary */
+  float familywise_ratio_threshold;         /* > 0: familywise_no_discovery is written */
+  float* inactive_max_evidence_ratio;
+  int64_t* inactive_best_index;
+  float* inactive_evidence_gain;
+  float* inactive_optimal_variance;
+  int64_t* support_repairs_accepted;        /* residual exchanges + repairs kept */
+  float* active_max_evidence_gain;
+  int64_t* active_best_index;
+  float* active_optimal_variance;
+  float* active_max_deletion_gain;
+  float* active_penalized_evidence_gain;
+  uint8_t* coordinate_stationary;
+  uint8_t* type2_map_coordinate_stationary;
+  uint8_t* familywise_no_discovery;         /* required when the threshold > 0 */
+} FbmeCertificate;
+int fbme_plan_set_certificate(FbmePlan* plan, const FbmeCertificate* cert);
+
 /* Unfused variational ARD prior update, replacing uamp_prior_update /
  * _uamp_prior_kernel (torch_sbl/triton_kernels.py:670-735, 196-235; taken
  * at torch_sbl/solver.py:1605-1625 when the UAMP posterior has not already

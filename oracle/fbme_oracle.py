@@ -95,6 +95,10 @@ class OracleConfig:
     uamp_polish_evidence_margin_factor: float = 0.0
     uamp_polish_residual_exchange_size: int = 0
     uamp_polish_fixed_budget_diagnostics: bool = False
+    uamp_polish_global_certificate: bool = False
+    uamp_polish_support_repairs: int = 0
+    uamp_polish_coordinate_tolerance: float = 1e-6
+    uamp_polish_familywise_error_rate: float | None = None
     uamp_support_false_alarm_budget: float | None = None
     active_set: bool = True
     active_set_start: int = 30
@@ -118,6 +122,14 @@ class OracleConfig:
         )
         s.update(overrides)
         return cls(**s)
+
+    @classmethod
+    def certified_hybrid_uamp(cls, **overrides: Any) -> "OracleConfig":
+        """torch_sbl/solver.py:300-316."""
+        s: dict[str, Any] = dict(uamp_polish_global_certificate=True, uamp_polish_iterations=4,
+                                 uamp_polish_support_repairs=1)
+        s.update(overrides)
+        return cls.fast_hybrid_uamp(**s)
 
     @classmethod
     def paper_hybrid_uamp(cls, **overrides: Any) -> "OracleConfig":
@@ -349,8 +361,9 @@ def _stable_cholesky(matrix: np.ndarray, tiny, eps, *, mode: str, multiplier: fl
 
 def active_posterior_with_evidence(y, prior, noise, op: PrefixOperator, active, *, columns,
                                    gram, column_data, data_energy, chol_mode, chol_multiplier,
-                                   tail_loading=0.0):
-    """solver.py:3591-3779 without the global certificate.
+                                   tail_loading=0.0, certificate=False):
+    """solver.py:3591-3779; with ``certificate`` the inactive-atom
+    certificate of the result (3757-3770) is returned as a fifth value.
 
     ``tail_loading``: 0 (the exact zero-tail model of the polish) or None,
     the omitted prior variance sum(prior) - sum(prior[active]) as an
@@ -401,7 +414,82 @@ def active_posterior_with_evidence(y, prior, noise, op: PrefixOperator, active, 
     mean[rows, active] = a_mean
     pv[rows, active] = a_var
     dd[rows, active] = a_dd
+    if certificate:
+        cert = inactive_evidence_certificate(y, columns, a_mean, eff_noise, dscale, chol, op, active)
+        return mean, pv, dd, nle, cert
     return mean, pv, dd, nle
+
+
+def ratio_threshold_for_evidence_tolerance(tolerance: float) -> float:
+    """solver.py:3499-3519: the rho >= 1 with rho - 1 - log(rho) = tolerance,
+    by doubling an upper bound and 64 bisection steps."""
+    if tolerance <= 0.0:
+        return 1.0
+    lo, hi = 1.0, 2.0
+    while hi - 1.0 - log(hi) < tolerance:
+        hi *= 2.0
+    for _ in range(64):
+        mid = 0.5 * (lo + hi)
+        if mid - 1.0 - log(mid) < tolerance:
+            lo = mid
+        else:
+            hi = mid
+    return hi
+
+
+def inactive_evidence_certificate(y, columns, a_mean, eff_noise, dscale, chol, op: PrefixOperator, active):
+    """solver.py:3522-3588: for every atom j, q_j = a_j^H C^-1 y (one adjoint
+    transform of the residual / noise) and s_j = a_j^H C^-1 a_j = M / nu -
+    ||L^-1 D^-1 A_S^H a_j||^2 / nu^2; the best inactive ratio |q_j|^2 / s_j
+    with its one-coordinate evidence gain and optimal variance."""
+    rd = op.rdtype
+    _, tiny = _finfo(rd)
+    b, k = active.shape
+    rows = np.arange(b)[:, None]
+    residual = y - (columns @ a_mean[:, :, None])[:, :, 0]
+    q = op.adjoint_flat(residual / eff_noise[:, None])
+    m = columns.shape[1]
+    cross = np.conj(op.adjoint_flat(np.swapaxes(columns, 1, 2).reshape(b * k, m))).reshape(b, k, -1)
+    solved = _tri_solve(chol, cross / dscale[:, :, None])
+    reduction = _abs2(solved).sum(axis=1, dtype=rd)
+    precision = np.maximum(rd(op.n_samples) / eff_noise[:, None] - reduction / np.square(eff_noise)[:, None],
+                           tiny).astype(rd)
+    ratio = (_abs2(q) / precision).astype(rd)
+    ratio[rows, active] = 0
+    best = np.argmax(ratio, axis=1)
+    max_ratio = ratio[np.arange(b), best]
+    best_prec = precision[np.arange(b), best]
+    up = max_ratio > 1.0
+    gain = np.where(up, max_ratio - rd(1.0) - np.log(np.maximum(max_ratio, tiny)), rd(0.0)).astype(rd)
+    optvar = np.where(up, (max_ratio - rd(1.0)) / best_prec, rd(0.0)).astype(rd)
+    return dict(max_ratio=max_ratio, best_index=best.astype(np.int64), evidence_gain=gain,
+                optimal_variance=optvar)
+
+
+def active_evidence_certificate(a_mean, a_pv, a_gamma, active):
+    """solver.py:3219-3317: the best exact one-coordinate update among the
+    active atoms (leave-one-out statistics by Sherman-Morrison)."""
+    rd = a_pv.dtype.type
+    _, tiny = _finfo(rd)
+    b = a_pv.shape[0]
+    r = np.arange(b)
+    g = np.maximum(a_gamma, tiny)
+    q = a_mean / g
+    s = np.maximum((g - a_pv) / np.square(g), tiny)
+    down = np.clip(a_pv / g, tiny, rd(1.0))
+    loo = np.maximum(s / down, tiny)
+    ratio = _abs2(q) / np.maximum(s * down, tiny)
+    optvar = np.where(ratio > 1.0, (ratio - rd(1.0)) / loo, rd(0.0)).astype(rd)
+    current = (-np.log(down) - g * _abs2(q) / down).astype(rd)
+    optimal = np.where(ratio > 1.0, np.log(np.maximum(ratio, tiny)) - ratio + rd(1.0), rd(0.0))
+    gain = np.maximum(current - optimal, rd(0.0)).astype(rd)
+    pos = np.argmax(gain, axis=1)
+    nondel = np.where(optvar > 0.0, gain, rd(0.0))
+    npos = np.argmax(nondel, axis=1)
+    dpos = np.argmax(current, axis=1)
+    return dict(max_gain=gain[r, pos], best_position=pos, best_index=active[r, pos].astype(np.int64),
+                optimal_variance=optvar[r, pos], max_nondeletion_gain=nondel[r, npos],
+                max_deletion_gain=current[r, dpos], best_deletion_position=dpos)
 
 
 def active_evidence_deletion_gain(a_mean, a_pv, a_gamma):
@@ -660,13 +748,17 @@ def uamp_active_em_polish(y, uamp_mean, uamp_var, prior, noise, op, active, prio
     exch_acc = np.zeros(b, np.int64) if cfg.uamp_polish_residual_exchange_size > 0 else None
     mean = uamp_mean
     pv = uamp_var
+    gcert = cfg.uamp_polish_global_certificate
     for p in range(cfg.uamp_polish_iterations):
-        c_mean, c_pv, c_dd, c_nle = active_posterior_with_evidence(
+        ev = active_posterior_with_evidence(
             y, working, active_noise, op, active, columns=columns, gram=gram,
             column_data=column_data, data_energy=data_energy, chol_mode=chol_mode,
-            chol_multiplier=cfg.cuda_cholesky_jitter_multiplier)
+            chol_multiplier=cfg.cuda_cholesky_jitter_multiplier, certificate=gcert)
+        c_mean, c_pv, c_dd, c_nle = ev[:4]
         cand = dict(mean=c_mean, pv=c_pv, dd=c_dd, prior=working, noise=active_noise, nle=c_nle,
                     active=active, columns=columns, gram=gram, column_data=column_data)
+        if gcert:  # the certificate follows its candidate through the gate (4165-4260)
+            cand.update({"cert_" + kk: v for kk, v in ev[4].items()})
         if cfg.uamp_polish_evidence_gate:
             if best is None:
                 best = {kk: (v.copy() if isinstance(v, np.ndarray) else v) for kk, v in cand.items()}
@@ -743,19 +835,76 @@ def uamp_active_em_polish(y, uamp_mean, uamp_var, prior, noise, op, active, prio
             pending = xmask.any(axis=1)
             out_ex = dict(add_idx=add_idx, rem_pos=rem_pos, xmask=xmask)
     fin = best if cfg.uamp_polish_evidence_gate else cand
+    dd = cur["dd"]
+    f_prior, f_noise, f_active, f_nle = fin["prior"], fin["noise"], fin["active"], fin["nle"]
+    cert = {kk[5:]: v for kk, v in fin.items() if kk.startswith("cert_")} if gcert else None
+    # support repairs (4511-4628): the best inactive atom replaces the active
+    # atom of largest deletion gain; kept when the exact evidence does not rise
+    if cfg.uamp_polish_support_repairs > 0 and exch_acc is None:
+        exch_acc = np.zeros(b, np.int64)
+    for _ in range(cfg.uamp_polish_support_repairs):
+        acert = active_evidence_certificate(mean[rows, f_active], pv[rows, f_active],
+                                            f_prior[rows, f_active], f_active)
+        r = np.arange(b)
+        rep_idx = cert["best_index"]
+        pos = acert["best_deletion_position"]
+        replaced = f_active[r, pos]
+        rep_active = f_active.copy()
+        rep_active[r, pos] = rep_idx
+        rep_prior = f_prior.copy()
+        rep_prior[r, replaced] = prior_floor
+        rep_prior[r, rep_idx] = np.maximum(cert["optimal_variance"], prior_floor)
+        cols = op.fourier_columns(rep_active)
+        ch = np.conj(np.swapaxes(cols, 1, 2))
+        r_mean, r_pv, r_dd, r_nle, r_cert = active_posterior_with_evidence(
+            y, rep_prior, f_noise, op, rep_active, columns=cols, gram=ch @ cols,
+            column_data=ch @ y[:, :, None], data_energy=data_energy, chol_mode=chol_mode,
+            chol_multiplier=cfg.cuda_cholesky_jitter_multiplier, certificate=True)
+        acc = (cert["max_ratio"] > 1.0) & np.isfinite(r_nle) & (r_nle <= f_nle)
+        exch_acc = exch_acc + acc.astype(np.int64)
+        m2 = acc[:, None]
+        mean, pv, dd = np.where(m2, r_mean, mean), np.where(m2, r_pv, pv), np.where(m2, r_dd, dd)
+        f_prior = np.where(m2, rep_prior, f_prior)
+        f_active = np.where(m2, rep_active, f_active)
+        f_nle = np.where(acc, r_nle, f_nle).astype(rd)
+        accepted.append(f_nle.copy())
+        cert = {kk: np.where(acc, r_cert[kk], v) for kk, v in cert.items()}
     trace = np.stack(accepted, axis=1)
     res = dict(
-        mean=mean, pv=pv, dd=cur["dd"], prior=fin["prior"], noise=fin["noise"],
-        negative_log_evidence=fin["nle"], evidence_trace=trace,
-        penalized_negative_log_evidence=fin["nle"].copy(), penalized_evidence_trace=trace.copy(),
+        mean=mean, pv=pv, dd=dd, prior=f_prior, noise=f_noise,
+        negative_log_evidence=f_nle, evidence_trace=trace,
+        penalized_negative_log_evidence=f_nle.copy(), penalized_evidence_trace=trace.copy(),
         support_log_odds_penalty=np.zeros(b, rd), hard_pruning_accepted=np.zeros(b, bool),
         truncation_certified=np.zeros(b, bool),
         active_model_selected=np.full(b, bool(cfg.uamp_polish_prune_tail)),
-        active_indices=fin["active"],
+        active_indices=f_active,
     )
     if exch_acc is not None:
         res["support_repairs_accepted"] = exch_acc
         res["support_exchanges_accepted"] = exch_acc.copy()
+    if gcert:  # final diagnostics (4851-4870, 5388-5460)
+        tol = rd(cfg.uamp_polish_coordinate_tolerance)
+        thr = np.full(b, ratio_threshold_for_evidence_tolerance(cfg.uamp_polish_coordinate_tolerance), rd)
+        acert = active_evidence_certificate(mean[rows, f_active], pv[rows, f_active],
+                                            f_prior[rows, f_active], f_active)
+        stationary = (cert["evidence_gain"] <= tol) & (acert["max_gain"] <= tol)
+        in_pen = np.maximum(cert["evidence_gain"], rd(0.0))
+        act_pen = np.maximum(acert["max_nondeletion_gain"], np.maximum(acert["max_deletion_gain"], rd(0.0)))
+        res.update(
+            inactive_max_evidence_ratio=cert["max_ratio"], inactive_best_index=cert["best_index"],
+            inactive_evidence_gain=cert["evidence_gain"], inactive_optimal_variance=cert["optimal_variance"],
+            active_max_evidence_gain=acert["max_gain"], active_best_index=acert["best_index"],
+            active_optimal_variance=acert["optimal_variance"],
+            active_max_deletion_gain=acert["max_deletion_gain"],
+            coordinate_stationary=stationary, type2_coordinate_stationary=stationary.copy(),
+            inactive_ratio_threshold=thr, stationarity_ratio_threshold=thr.copy(),
+            inactive_penalized_evidence_gain=in_pen, active_penalized_evidence_gain=act_pen,
+            type2_map_coordinate_stationary=(in_pen <= tol) & (act_pen <= tol))
+        if cfg.uamp_polish_familywise_error_rate is not None:
+            fw = np.full(b, log(max(op.n_grid - k, 1) / cfg.uamp_polish_familywise_error_rate), rd)
+            nd = cert["max_ratio"] <= fw
+            res.update(familywise_ratio_threshold=fw, familywise_no_discovery=nd,
+                       familywise_support_certified=nd.copy())
     return res
 
 

@@ -407,16 +407,66 @@ def make_cg_active(config: str, seed: int, max_iter: int) -> None:
     print("wrote", name, "active set", out["f32_active_set_size"], out["f64_active_set_size"])
 
 
+CERT_FIELDS = ("inactive_max_evidence_ratio", "inactive_best_index", "inactive_evidence_gain",
+               "inactive_optimal_variance", "support_repairs_accepted", "support_exchanges_accepted",
+               "active_max_evidence_gain", "active_best_index", "active_optimal_variance",
+               "active_max_deletion_gain", "coordinate_stationary", "inactive_ratio_threshold",
+               "type2_coordinate_stationary", "stationarity_ratio_threshold", "familywise_ratio_threshold",
+               "familywise_no_discovery", "familywise_support_certified", "inactive_penalized_evidence_gain",
+               "active_penalized_evidence_gain", "type2_map_coordinate_stationary", "noise_variance",
+               "effective_dof", "negative_log_evidence", "evidence_trace", "penalized_negative_log_evidence")
+
+
+def make_certified(config: str, seed: int, repairs: int, fwer: float) -> None:
+    """A scene solved by the reference's sbl_2d under certified_hybrid_uamp
+    (global certificate, support repairs; solver.py:300-316), CUDA Cholesky
+    loading; fwer > 0 adds the familywise screening threshold."""
+    import numpy as np
+
+    torch, scenes, SBLConfig, fast_sbl = _import()
+    import torch_sbl.solver as S  # reference package
+
+    S._stable_cholesky_raw = _cuda_cholesky_branch(S, torch)
+    sc = scenes.config_scene(config, seed)
+    over = dict(device="cpu", uamp_backend="torch", uamp_polish_compute_truncation_diagnostic=False,
+                uamp_polish_support_repairs=repairs)
+    if fwer > 0:
+        over["uamp_polish_familywise_error_rate"] = fwer
+    r = S.sbl_2d(torch.from_numpy(sc.y), sc.grid, config=SBLConfig.certified_hybrid_uamp(**over))
+    x = r.x.numpy().reshape(-1)
+    act = np.flatnonzero(x != 0)
+    inactive = np.ones(x.size, bool)
+    inactive[act] = False
+    pv, prec = r.posterior_variance.numpy().reshape(-1), r.precision.numpy().reshape(-1)
+    out = {"grid": np.array(sc.grid), "sample": np.array(sc.y.shape), "y_sha256": np.array(y_digest(sc.y)),
+           "scene": np.array(f"config_scene('{config}', {seed})"), "repairs": np.array(repairs),
+           "fwer": np.array(fwer), "cholesky": np.array("cuda"), "active": act.astype(np.int64),
+           "x_active": x[act], "pv_active": pv[act], "precision_active": prec[act],
+           "pv_inactive_unique": np.unique(pv[inactive]), "precision_inactive_unique": np.unique(prec[inactive])}
+    for f in CERT_FIELDS:
+        v = getattr(r, f)
+        if v is not None:
+            out[f] = np.asarray(v.numpy())
+    name = f"cert_{config}_s{seed}_r{repairs}" + ("_fw" if fwer > 0 else "")
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print("wrote", name, "repairs kept", int(r.support_repairs_accepted))
+
+
 JOBS = [("c3", "0"), ("c3", "1"), ("c3", "2"), ("c4", "0"), ("cg_c2", "0", "6"),
         ("masked", "c1", "0", "random"), ("masked", "c1", "1", "ellipse"), ("masked", "c2", "0", "random"),
         ("masked", "c2", "1", "ellipse"), ("cg_active", "c1", "0", "44"),
-        ("dense", "c1", "0", "30"), ("dense", "c1", "1", "30")]
+        ("dense", "c1", "0", "30"), ("dense", "c1", "1", "30"),
+        ("certified", "c1", "0", "1", "0"), ("certified", "c2", "0", "1", "0"),
+        ("certified", "c1", "1", "3", "0.05"), ("certified", "c2", "1", "2", "0")]
 
 
 def main() -> None:
     if len(sys.argv) > 1:
         if sys.argv[1] == "masked":
             make_masked(sys.argv[2], int(sys.argv[3]), sys.argv[4])
+            return
+        if sys.argv[1] == "certified":
+            make_certified(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), float(sys.argv[5]))
             return
         if sys.argv[1] in ("cg_active", "dense"):
             {"cg_active": make_cg_active, "dense": make_dense}[sys.argv[1]](
