@@ -53,6 +53,7 @@ def _args() -> argparse.Namespace:
                     help="rounds of one scene per host core in the CPU baseline sample")
     ap.add_argument("--no-cg", action="store_true", help="skip the mode='cg' section")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-certificate", action="store_true", help="skip the global-certificate section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain section")
     ap.add_argument("--no-uneven", action="store_true", help="skip the batched-uneven section")
     ap.add_argument("--no-precision", action="store_true", help="skip the precision-workload section")
@@ -413,6 +414,60 @@ def cg_section(device) -> dict:
     return out
 
 
+def certificate_flops_per_atom(k: int) -> int:
+    """FP32 FLOPs of one grid atom in the certificate scan: K complex
+    multiply-adds for q_j and K(K-1)/2 for the forward substitution (8 each),
+    K complex scalings and squared norms (6 each), the ratio (about 8)."""
+    return 8 * (k + k * (k - 1) // 2) + 6 * k + 8
+
+
+def certificate_section(device, steps: int, batch: int = 64) -> dict:
+    """certified_hybrid_uamp (global certificate, one support repair) against
+    the same solve without it (fast_hybrid_uamp with 4 polish iterations) on
+    256^2/128^2 scenes: scenes/s of each, and the certificate kernel's time
+    and FP32 rate (1 + repairs grid scans per replay) against the nominal
+    FP32 FMA peak (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz)."""
+    import numpy as np
+    import torch
+
+    from fbme_b200 import scenes
+    from fbme_b200.config import SBLConfig
+    from fbme_b200.engine import FBMEEngine
+
+    sc = [scenes.config_scene("c2", 6_000_000 + i) for i in range(batch)]
+    y = torch.from_numpy(np.stack([v.y.reshape(-1) for v in sc])).to(device)
+    grid, sample = sc[0].grid, sc[0].y.shape
+    out = {"grid": list(grid), "scenes": batch}
+    for name, cfg in (("certified", SBLConfig.certified_hybrid_uamp(device="cuda")),
+                      ("uncertified", SBLConfig.fast_hybrid_uamp(device="cuda", uamp_polish_iterations=4))):
+        eng = FBMEEngine(batch, grid, sample, cfg, device)
+        for _ in range(3):
+            eng.run(y)
+        torch.cuda.synchronize(device)
+        reps = max(steps, 5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            eng.run(y)
+        e1.record()
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms_per_replay": ms, "scenes_per_s": batch / (ms / 1000.0)}
+        if name == "certified":
+            prof = eng.profile(y)
+            cms = prof.get("certificate", (0.0, 0))[0]
+            scans = 1 + cfg.uamp_polish_support_repairs
+            flops = scans * batch * grid[0] * grid[1] * certificate_flops_per_atom(cfg.uamp_polish_size)
+            peak = 148 * 128 * 2 * 1.965e9
+            out[name].update(certificate_kernel_ms=cms, grid_scans=scans,
+                             fp32_tflops=flops / (cms * 1e-3) / 1e12 if cms else None,
+                             fp32_frac_of_nominal=flops / (cms * 1e-3) / peak if cms else None,
+                             repairs_kept=int(eng.cert["support_repairs_accepted"].sum()))
+        eng.close()
+    out["certified_vs_uncertified"] = out["certified"]["scenes_per_s"] / out["uncertified"]["scenes_per_s"]
+    return out
+
+
 # ---------------------------------------------------------------- CPU side
 def _oracle_solve(args):
     y, grid, profile = args
@@ -763,6 +818,7 @@ def run_ours(a: argparse.Namespace) -> None:
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_baseline(a.profile, a.cpu_rounds)
     cg = cg_section(device) if world == 1 and not a.no_cg else None
+    certificate = certificate_section(device, a.steps) if world == 1 and not a.no_certificate else None
     learned = None
     if world == 1 and not a.no_learned:
         learned = learned_section(device, min(a.steps, 20), a.batch)
@@ -821,6 +877,8 @@ def run_ours(a: argparse.Namespace) -> None:
             line["uneven"] = uneven
         if cg is not None:
             line["cg"] = cg
+        if certificate is not None:
+            line["certificate"] = certificate
         if published is not None:
             line["published_shape"] = published
         if precision is not None:

@@ -25,7 +25,7 @@ STATUS_TIMEOUT = 4
 STATUS_PCG_BREAKDOWN = 8
 STATUS_ITER_CAP = 16
 
-NUM_GROUPS = 13
+NUM_GROUPS = 14
 
 
 class FbmeShape(ctypes.Structure):
@@ -108,6 +108,8 @@ class FbmeCertificate(ctypes.Structure):
         ("coordinate_stationary", c_void_p),
         ("type2_map_coordinate_stationary", c_void_p),
         ("familywise_no_discovery", c_void_p),
+        ("workspace", c_void_p),
+        ("workspace_bytes", c_size_t),
     ]
 
 
@@ -215,6 +217,7 @@ SIGNATURES = {
     "fbme_plan_state": (c_int, [c_void_p, POINTER(FbmeState)]),
     "fbme_plan_set_observation_mask": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fbme_plan_set_certificate": (c_int, [c_void_p, POINTER(FbmeCertificate)]),
+    "fbme_plan_certificate_workspace_bytes": (c_size_t, [c_void_p]),
     "fbme_plan_set_warm_prior_map": (c_int, [c_void_p, c_void_p]),
     "fbme_selftest_workspace_bytes": (c_size_t, []),
     "fbme_selftest_stage_timeout": (c_int, [c_void_p, c_size_t, c_void_p, c_int64, c_void_p]),

@@ -906,7 +906,7 @@ int fbme_plan_replay(FbmePlan* plan, const void* y, const FbmeOutputs* out, fbme
 const char* fbme_profile_group_name(int32_t group) {
   static const char* names[FBME_NUM_GROUPS] = {
       "init", "adjoint_1", "adjoint_denoise", "forward_1", "forward_residual", "scalars",
-      "sweep1_denoise", "topk", "polish", "exchange_score", "output", "adjoint_2", "message"};
+      "sweep1_denoise", "topk", "polish", "exchange_score", "output", "adjoint_2", "message", "certificate"};
   return (group >= 0 && group < FBME_NUM_GROUPS) ? names[group] : "";
 }
 
@@ -1022,6 +1022,11 @@ int fbme_plan_set_observation_mask(FbmePlan* plan, const uint8_t* mask, fbme_str
   return FBME_OK;
 }
 
+size_t fbme_plan_certificate_workspace_bytes(const FbmePlan* plan) {
+  if (!plan || plan->uneven || plan->bk.empty()) return 0;
+  return fbme::cert_scratch_bytes(plan->bk[0].s);
+}
+
 int fbme_plan_set_certificate(FbmePlan* plan, const FbmeCertificate* cert) {
   int rc = single_bucket(plan);
   if (rc != FBME_OK) return rc;
@@ -1044,6 +1049,10 @@ int fbme_plan_set_certificate(FbmePlan* plan, const FbmeCertificate* cert) {
       !cert->type2_map_coordinate_stationary ||
       (cert->familywise_ratio_threshold > 0.f && !cert->familywise_no_discovery))
     return fail(FBME_ERR_INVALID, "NULL certificate output");
+  if (!cert->workspace || (reinterpret_cast<uintptr_t>(cert->workspace) & 255u) != 0 ||
+      cert->workspace_bytes < fbme::cert_scratch_bytes(k.s))
+    return fail(FBME_ERR_WORKSPACE,
+                "certificate workspace smaller than fbme_plan_certificate_workspace_bytes() or not 256-byte aligned");
   k.cert = *cert;
   k.certify = true;
   k.dc.repairs = cert->support_repairs;

@@ -194,6 +194,7 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                 const FbmeOutputs& out, cudaStream_t st, Profiler* prof = nullptr,
                 const FbmeCertificate* cert = nullptr);
 size_t polish_state_bytes();
+size_t cert_scratch_bytes(const BatchShape& s);
 int topk_slices(long long n);
 
 // Several shape buckets' top-k in one launch each (uneven plans): bucket i

@@ -863,18 +863,19 @@ struct CertModel {
   float inv_d[kMaxPolish], inv_l[kMaxPolish];
 };
 
-// Largest one-coordinate ratio over the grid (first index on ties, as
-// torch's max), with its atom precision s_j.
+// Largest one-coordinate ratio over the atoms [j0, j1) of the grid (first
+// index on ties, as torch's max), with its atom precision s_j; the block's
+// best, in every thread.
 FBME_DEV CertBest cert_scan(const PolishArgs& A, const float2 (*L)[33], const CertModel& m, int K, float nu,
-                            const float2* bp, const float2* d1, const float2* d2, CertBest* red) {
+                            const float2* bp, const float2* d1, const float2* d2, long long j0, long long j1,
+                            CertBest* red) {
   const BatchShape& s = A.s;
-  const long long N = s.n();
   const float Mf = static_cast<float>(observed_samples(s, A.c));
   const float nu2 = nu * nu;
   CertBest b{-1.f, 1.f, 0x7fffffff};
-  for (long long j = threadIdx.x; j < N; j += blockDim.x) {
-    const int j1 = static_cast<int>(j / s.n2);
-    const int j2 = static_cast<int>(j - static_cast<long long>(j1) * s.n2);
+  for (long long j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    const int j1i = static_cast<int>(j / s.n2);
+    const int j2i = static_cast<int>(j - static_cast<long long>(j1i) * s.n2);
     float2 q = __ldg(bp + j);
     bool act = false;
     float2 v[kMaxPolish];
@@ -883,7 +884,7 @@ FBME_DEV CertBest cert_scan(const PolishArgs& A, const float2 (*L)[33], const Ce
     for (int i = 0; i < kMaxPolish; ++i) {
       if (i < K) {
         act |= m.idx[i] == j;
-        const float2 g = gram_at(A, d1, d2, j1, j2, m.a1[i], m.a2[i]);
+        const float2 g = gram_at(A, d1, d2, j1i, j2i, m.a1[i], m.a2[i]);
         const float2 mu = m.mu[i];
         q.x -= g.x * mu.x - g.y * mu.y;
         q.y -= g.x * mu.y + g.y * mu.x;
@@ -966,12 +967,93 @@ FBME_DEV int warp_argmax(float v, float* best) {
   return pos;
 }
 
-__global__ void __launch_bounds__(kCertThreads) certify_kernel(PolishArgs A, FbmeCertificate C) {
+// Per-scene scratch of the certificate steps (caller workspace): the
+// factor and staged active set of the model whose certificate the next
+// scan computes, the pending repair, the current inactive certificate and
+// the scan's per-block partial results.
+struct CertScratch {
+  float2 L[kMaxPolish][kMaxPolish];
+  CertModel m;
+  int nu_bits;  // the model's noise variance
+  int pending;  // the scanned model is a repair proposal
+  int p_idx[kMaxPolish];
+  float p_gam[kMaxPolish];
+  float2 p_mean[kMaxPolish];
+  float p_pv[kMaxPolish], p_dd[kMaxPolish];
+  double p_nle;
+  CertState cur;
+};
+
+// Scan blocks per scene: enough CTAs to cover the SMs a few times, at least
+// 1024 atoms per block, at most kCertMaxBlocks.
+constexpr int kCertMaxBlocks = 256;
+int cert_blocks(const BatchShape& s) {
+  static const int sms = [] {
+    int dev = 0, v = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v;
+  }();
+  const long long want = (4LL * sms + s.B - 1) / s.B;
+  const long long most = std::max(1LL, (s.n() + 1023) / 1024);
+  return static_cast<int>(std::max(1LL, std::min({want, most, static_cast<long long>(kCertMaxBlocks)})));
+}
+
+size_t cert_scratch_bytes(const BatchShape& s) {
+  return static_cast<size_t>(s.B) * (sizeof(CertScratch) + sizeof(CertBest) * kCertMaxBlocks);
+}
+
+FBME_DEV CertScratch* cert_scene(void* ws, int scene) {
+  return reinterpret_cast<CertScratch*>(ws) + scene;
+}
+FBME_DEV CertBest* cert_parts(void* ws, int B, int scene) {
+  return reinterpret_cast<CertBest*>(reinterpret_cast<CertScratch*>(ws) + B) + static_cast<long long>(scene) *
+         kCertMaxBlocks;
+}
+
+// Warp 0 of a step: evaluate the work set (idx, gam) and stage its factor
+// and active set for the scan.
+FBME_DEV EvalOut cert_model(const PolishArgs& A, CertScratch* cs, float2 (*M)[33], float2 (*X)[33],
+                            const float2* d1, const float2* d2, int idx, float gam, float nu, const float2* bp,
+                            float data_energy) {
+  const int lane = threadIdx.x & 31;
+  const int K = A.c.polish_size;
+  const bool on = lane < K;
+  const EvalOut o = evaluate(A, M, X, d1, d2, K, idx, gam, nu, on ? bp[idx] : make_float2(0.f, 0.f), data_energy);
+  if (on) {
+    for (int k = 0; k < lane; ++k) cs->L[lane][k] = M[lane][k];
+    cs->m.idx[lane] = idx;
+    cs->m.a1[lane] = idx / A.s.n2;
+    cs->m.a2[lane] = idx % A.s.n2;
+    cs->m.mu[lane] = o.mean;
+    cs->m.inv_d[lane] = 1.0f / o.dscale;
+    cs->m.inv_l[lane] = 1.0f / M[lane][lane].x;
+  }
+  if (lane == 0) cs->nu_bits = __float_as_int(nu);
+  return o;
+}
+
+// The scan's result: the block partials merged (first index on ties).
+FBME_DEV CertBest cert_merge(void* ws, int B, int scene, int nblk) {
+  const int lane = threadIdx.x & 31;
+  const CertBest* part = cert_parts(ws, B, scene);
+  CertBest b{-1.f, 1.f, 0x7fffffff};
+  for (int i = lane; i < nblk; i += 32) cert_pick(b, part[i].ratio, part[i].prec, part[i].index);
+  return cert_warp_best(b);
+}
+
+// One certificate step of one scene (one warp).  Step 0 stages the model
+// the polish kept.  Step t in [1, R] merges the previous scan (the kept
+// model's certificate at t = 1; otherwise repair t-1's certificate and its
+// decision: kept when the inactive ratio that proposed it exceeds 1 and
+// the exact evidence does not rise) and stages repair t: the best inactive
+// atom replaces the active atom of largest deletion delta, with variance
+// max(optimal, floor).  Step R + 1 merges the last scan and writes the
+// final certificate (solver.py:4851-4870, 5388-5460).
+__global__ void __launch_bounds__(32) cert_step_kernel(PolishArgs A, FbmeCertificate C, void* ws, int nblk,
+                                                       int t) {
   __shared__ float2 M[32][33];
   __shared__ float2 X[32][33];
-  __shared__ CertModel model;
-  __shared__ CertBest red[kCertThreads / 32];
-  __shared__ int keep;
   extern __shared__ float2 dtab[];
   const int scene = blockIdx.x;
   if (scene >= A.s.B) return;
@@ -979,121 +1061,145 @@ __global__ void __launch_bounds__(kCertThreads) certify_kernel(PolishArgs A, Fbm
   const DevConfig& c = A.c;
   const int K = c.polish_size, P = c.polish_iters, R = c.repairs;
   const int lane = threadIdx.x & 31;
-  const bool w0 = threadIdx.x < 32, on = lane < K;
+  const bool on = lane < K;
   PolishScene* ps = reinterpret_cast<PolishScene*>(A.p.pstate) + scene;
+  CertScratch* cs = cert_scene(ws, scene);
   const long long N = s.n();
   const float2* bp = A.p.bp + scene * N;
   const float fl = A.p.sc.floor_[scene];
   const float data_energy = A.p.sc.data_energy[scene];
-  float2* d1 = dtab;
-  float2* d2 = dtab + s.n1;
-  load_dirichlet(A, d1, d2);
-  __syncthreads();
   const float nu = ps->best_noise;
   int status = 0;
-  auto stage = [&](int idx, const EvalOut& o) {
-    if (on) {
-      model.idx[lane] = idx;
-      model.a1[lane] = idx / s.n2;
-      model.a2[lane] = idx % s.n2;
-      model.mu[lane] = o.mean;
-      model.inv_d[lane] = 1.0f / o.dscale;
-      model.inv_l[lane] = 1.0f / M[lane][lane].x;
-    }
-  };
-  // the model the polish kept: its factor, then its certificate
-  if (w0) {
-    const int idx = on ? ps->active[lane] : 0;
-    const float gam = on ? ps->best_gamma[lane] : 1.0f;
-    const EvalOut o = evaluate(A, M, X, d1, d2, K, idx, gam, nu, on ? bp[idx] : make_float2(0.f, 0.f),
-                               data_energy);
-    status |= o.status;
-    stage(idx, o);
-  }
-  __syncthreads();
-  CertState cur = cert_state(cert_scan(A, M, model, K, nu, bp, d1, d2, red));
-  // support repairs (solver.py:4511-4628): the best inactive atom replaces
-  // the active atom of largest deletion delta, with variance
-  // max(optimal, floor); kept when the exact evidence does not rise
-  for (int r = 0; r < R; ++r) {
-    EvalOut o{};
-    int idx = 0;
-    float gam = 1.0f;
-    if (w0) {
-      const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
-      const float pv = on ? ps->best_pv[lane] : 0.f;
-      gam = on ? ps->best_gamma[lane] : 1.0f;
-      idx = on ? ps->active[lane] : 0;
-      float dmax;
-      const int pos = warp_argmax(on ? deletion_gain(mu, pv, gam) : -INFINITY, &dmax);
-      if (lane == pos) {
-        idx = cur.index;
-        gam = fmaxf(cur.optvar, fl);
-      }
-      o = evaluate(A, M, X, d1, d2, K, idx, gam, nu, on ? bp[idx] : make_float2(0.f, 0.f), data_energy);
-      status |= o.status;
-      stage(idx, o);
-    }
-    __syncthreads();
-    const CertState next = cert_state(cert_scan(A, M, model, K, nu, bp, d1, d2, red));
-    if (w0) {
-      const bool accept = cur.ratio > 1.0f && isfinite(o.nle) &&
-                          static_cast<float>(o.nle) <= static_cast<float>(ps->best_nle);
+  if (t > 0) {
+    const CertState next = cert_state(cert_merge(ws, s.B, scene, nblk));
+    bool keep = true;
+    if (cs->pending) {  // decide the repair the scan certified
+      const CertState prop = cs->cur;
+      const double nle = cs->p_nle;
+      keep = prop.ratio > 1.0f && isfinite(nle) && static_cast<float>(nle) <= static_cast<float>(ps->best_nle);
       __syncwarp();
-      if (accept) {
+      if (keep) {
         if (on) {
-          ps->active[lane] = idx;
-          ps->best_mean[lane] = o.mean;
-          ps->best_pv[lane] = o.pv;
-          ps->best_dd[lane] = o.dd;
-          ps->best_gamma[lane] = gam;
+          ps->active[lane] = cs->p_idx[lane];
+          ps->best_mean[lane] = cs->p_mean[lane];
+          ps->best_pv[lane] = cs->p_pv[lane];
+          ps->best_dd[lane] = cs->p_dd[lane];
+          ps->best_gamma[lane] = cs->p_gam[lane];
         }
         if (lane == 0) {
-          ps->best_nle = o.nle;
+          ps->best_nle = nle;
           ps->exch_acc += 1;
         }
       }
       __syncwarp();
-      if (lane == 0) {
-        ps->trace[P + r] = static_cast<float>(ps->best_nle);
-        keep = accept;
+      if (lane == 0) ps->trace[P + t - 2] = static_cast<float>(ps->best_nle);
+    }
+    __syncwarp();
+    if (lane == 0 && keep) cs->cur = next;
+    __syncwarp();
+  }
+  if (t <= R) {
+    float2* d1 = dtab;
+    float2* d2 = dtab + s.n1;
+    load_dirichlet(A, d1, d2);
+    int idx = on ? ps->active[lane] : 0;
+    float gam = on ? ps->best_gamma[lane] : 1.0f;
+    if (t > 0) {
+      const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+      const float pv = on ? ps->best_pv[lane] : 0.f;
+      float dmax;
+      const int pos = warp_argmax(on ? deletion_gain(mu, pv, gam) : -INFINITY, &dmax);
+      const CertState cur = cs->cur;
+      if (lane == pos) {
+        idx = cur.index;
+        gam = fmaxf(cur.optvar, fl);
       }
     }
-    __syncthreads();
-    if (keep) cur = next;
+    const EvalOut o = cert_model(A, cs, M, X, d1, d2, idx, gam, nu, bp, data_energy);
+    status |= o.status;
+    if (on) {
+      cs->p_idx[lane] = idx;
+      cs->p_gam[lane] = gam;
+      cs->p_mean[lane] = o.mean;
+      cs->p_pv[lane] = o.pv;
+      cs->p_dd[lane] = o.dd;
+    }
+    if (lane == 0) {
+      cs->p_nle = o.nle;
+      cs->pending = t > 0;
+    }
+  } else {
+    // final certificate of the kept model
+    const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
+    const float pv = on ? ps->best_pv[lane] : 0.f;
+    const float g = on ? ps->best_gamma[lane] : 1.0f;
+    const int idx = on ? ps->active[lane] : 0;
+    const ActiveTerms at = active_terms(mu, pv, g);
+    float max_gain, max_nondel, max_del;
+    const int gp = warp_argmax(on ? at.gain : -INFINITY, &max_gain);
+    warp_argmax(on ? (at.optvar > 0.f ? at.gain : 0.f) : -INFINITY, &max_nondel);
+    warp_argmax(on ? at.current : -INFINITY, &max_del);
+    const int best_idx = __shfl_sync(0xffffffffu, idx, gp);
+    const float best_var = __shfl_sync(0xffffffffu, at.optvar, gp);
+    if (lane == 0) {
+      const CertState cur = cs->cur;
+      const float tol = C.coordinate_tolerance;
+      const float pen = fmaxf(max_nondel, fmaxf(max_del, 0.f));
+      C.inactive_max_evidence_ratio[scene] = cur.ratio;
+      C.inactive_best_index[scene] = cur.index;
+      C.inactive_evidence_gain[scene] = cur.gain;
+      C.inactive_optimal_variance[scene] = cur.optvar;
+      C.support_repairs_accepted[scene] = ps->exch_acc;
+      C.active_max_evidence_gain[scene] = max_gain;
+      C.active_best_index[scene] = best_idx;
+      C.active_optimal_variance[scene] = best_var;
+      C.active_max_deletion_gain[scene] = max_del;
+      C.active_penalized_evidence_gain[scene] = pen;
+      C.coordinate_stationary[scene] = cur.gain <= tol && max_gain <= tol;
+      C.type2_map_coordinate_stationary[scene] = fmaxf(cur.gain, 0.f) <= tol && pen <= tol;
+      if (C.familywise_ratio_threshold > 0.f)
+        C.familywise_no_discovery[scene] = cur.ratio <= C.familywise_ratio_threshold;
+    }
   }
-  if (!w0) return;
-  // final certificate (solver.py:4851-4870, 5388-5460)
-  const float2 mu = on ? ps->best_mean[lane] : make_float2(0.f, 0.f);
-  const float pv = on ? ps->best_pv[lane] : 0.f;
-  const float g = on ? ps->best_gamma[lane] : 1.0f;
-  const int idx = on ? ps->active[lane] : 0;
-  const ActiveTerms t = active_terms(mu, pv, g);
-  float max_gain, max_nondel, max_del;
-  const int gp = warp_argmax(on ? t.gain : -INFINITY, &max_gain);
-  warp_argmax(on ? (t.optvar > 0.f ? t.gain : 0.f) : -INFINITY, &max_nondel);
-  warp_argmax(on ? t.current : -INFINITY, &max_del);
-  const int best_idx = __shfl_sync(0xffffffffu, idx, gp);
-  const float best_var = __shfl_sync(0xffffffffu, t.optvar, gp);
   status = __reduce_or_sync(0xffffffffu, status);
-  if (lane != 0) return;
-  if (status) atomicOr(&A.p.status[scene], status);
-  const float tol = C.coordinate_tolerance;
-  const float pen = fmaxf(max_nondel, fmaxf(max_del, 0.f));
-  C.inactive_max_evidence_ratio[scene] = cur.ratio;
-  C.inactive_best_index[scene] = cur.index;
-  C.inactive_evidence_gain[scene] = cur.gain;
-  C.inactive_optimal_variance[scene] = cur.optvar;
-  C.support_repairs_accepted[scene] = ps->exch_acc;
-  C.active_max_evidence_gain[scene] = max_gain;
-  C.active_best_index[scene] = best_idx;
-  C.active_optimal_variance[scene] = best_var;
-  C.active_max_deletion_gain[scene] = max_del;
-  C.active_penalized_evidence_gain[scene] = pen;
-  C.coordinate_stationary[scene] = cur.gain <= tol && max_gain <= tol;
-  C.type2_map_coordinate_stationary[scene] = fmaxf(cur.gain, 0.f) <= tol && pen <= tol;
-  if (C.familywise_ratio_threshold > 0.f)
-    C.familywise_no_discovery[scene] = cur.ratio <= C.familywise_ratio_threshold;
+  if (status && lane == 0) atomicOr(&A.p.status[scene], status);
+}
+
+// Block (bx, scene) scores atoms [bx chunk, (bx + 1) chunk) against the
+// staged model and writes its best to the scene's partials.
+__global__ void __launch_bounds__(kCertThreads) cert_scan_kernel(PolishArgs A, void* ws) {
+  __shared__ float2 M[32][33];
+  __shared__ CertModel model;
+  __shared__ CertBest red[kCertThreads / 32];
+  extern __shared__ float2 dtab[];
+  const int scene = blockIdx.y;
+  if (scene >= A.s.B) return;
+  const BatchShape& s = A.s;
+  const int K = A.c.polish_size;
+  const CertScratch* cs = cert_scene(ws, scene);
+  float2* d1 = dtab;
+  float2* d2 = dtab + s.n1;
+  load_dirichlet(A, d1, d2);
+  for (int e = threadIdx.x; e < K * K; e += blockDim.x) {
+    const int i = e / K, k = e - i * K;
+    if (k < i) M[i][k] = cs->L[i][k];
+  }
+  if (threadIdx.x < K) {
+    const int i = threadIdx.x;
+    model.idx[i] = cs->m.idx[i];
+    model.a1[i] = cs->m.a1[i];
+    model.a2[i] = cs->m.a2[i];
+    model.mu[i] = cs->m.mu[i];
+    model.inv_d[i] = cs->m.inv_d[i];
+    model.inv_l[i] = cs->m.inv_l[i];
+  }
+  __syncthreads();
+  const float nu = __int_as_float(cs->nu_bits);
+  const long long N = s.n();
+  const long long chunk = (N + gridDim.x - 1) / gridDim.x;
+  const long long j0 = blockIdx.x * chunk, j1 = min(N, j0 + chunk);
+  const CertBest b = cert_scan(A, M, model, K, nu, A.p.bp + scene * N, d1, d2, j0, j1, red);
+  if (threadIdx.x == 0) cert_parts(ws, s.B, scene)[blockIdx.x] = b;
 }
 
 // N-space outputs in one pass: zero mean, floor variance and 1/floor
@@ -1288,8 +1394,16 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
                                  p.xcand_idx, p.xcand_val, st));
     FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 1)));
   }
-  if (cert)
-    FBME_TIMED(prof, FBME_GROUP_POLISH, (certify_kernel<<<s.B, kCertThreads, dsm, st>>>(A, *cert)));
+  if (cert) {  // model, scan, (decide + model, scan) per repair, final
+    const int nblk = cert_blocks(s);
+    for (int t = 0; t <= c.repairs + 1; ++t) {
+      FBME_TIMED(prof, FBME_GROUP_CERTIFICATE,
+                 (cert_step_kernel<<<s.B, 32, dsm, st>>>(A, *cert, cert->workspace, nblk, t)));
+      if (t <= c.repairs)
+        FBME_TIMED(prof, FBME_GROUP_CERTIFICATE,
+                   (cert_scan_kernel<<<dim3(nblk, s.B), kCertThreads, dsm, st>>>(A, cert->workspace)));
+    }
+  }
   FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_finish_kernel<<<s.B, 32, dsm, st>>>(A, out)));
   const int fb = static_cast<int>((s.n() + 2047) / 2048);
   FBME_TIMED(prof, FBME_GROUP_OUTPUT, (output_kernel<<<dim3(fb < 64 ? fb : 64, s.B), 256, 0, st>>>(A, out)));

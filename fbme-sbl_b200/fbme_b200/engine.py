@@ -276,8 +276,12 @@ class FBMEEngine:
         c.support_repairs = repairs
         c.coordinate_tolerance = cfg.uamp_polish_coordinate_tolerance
         c.familywise_ratio_threshold = self.fw_threshold if self.fw_threshold is not None else 0.0
-        for name, _ in nat.FbmeCertificate._fields_[3:]:
+        for name, _ in nat.FbmeCertificate._fields_[3:-2]:
             setattr(c, name, self.cert[name].data_ptr())
+        nbytes = int(self.lib.fbme_plan_certificate_workspace_bytes(self._plan))
+        self._cert_ws = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+        c.workspace = (self._cert_ws.data_ptr() + 255) & ~255
+        c.workspace_bytes = nbytes
         self._certificate = c
         nat.check(self.lib.fbme_plan_set_certificate(self._plan, ctypes.byref(c)), "fbme_plan_set_certificate")
 

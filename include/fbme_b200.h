@@ -240,7 +240,10 @@ typedef struct {
   uint8_t* coordinate_stationary;
   uint8_t* type2_map_coordinate_stationary;
   uint8_t* familywise_no_discovery;         /* required when the threshold > 0 */
+  void* workspace;                          /* device scratch, 256-byte aligned */
+  size_t workspace_bytes;                   /* >= fbme_plan_certificate_workspace_bytes() */
 } FbmeCertificate;
+size_t fbme_plan_certificate_workspace_bytes(const FbmePlan* plan);
 int fbme_plan_set_certificate(FbmePlan* plan, const FbmeCertificate* cert);
 
 /* Unfused variational ARD prior update, replacing uamp_prior_update /
@@ -455,7 +458,8 @@ enum {
   FBME_GROUP_OUTPUT = 10,     /* dense outputs */
   FBME_GROUP_ADJ_2 = 11,      /* adjoint stage 2 of sweeps 2.. and the final E-step */
   FBME_GROUP_MESSAGE = 12,    /* UAMP message update (elementwise, before adjoint stage 1) */
-  FBME_NUM_GROUPS = 13
+  FBME_GROUP_CERTIFICATE = 13,/* global certificate and support repairs (fbme_plan_set_certificate) */
+  FBME_NUM_GROUPS = 14
 };
 
 /* One replay with CUDA events around every kernel launch (not capturable;
