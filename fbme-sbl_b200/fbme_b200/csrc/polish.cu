@@ -985,18 +985,34 @@ struct CertScratch {
 };
 
 // Scan blocks per scene: enough CTAs to cover the SMs a few times, at least
-// 1024 atoms per block, at most kCertMaxBlocks.
+// 1024 atoms per block, at most kCertMaxBlocks.  Within that range the
+// count is raised (up to 4x) until the B * nblk CTAs fill their last wave of
+// `resident` CTAs per SM to 97 %, or to the best fill seen: a last wave that
+// is mostly empty leaves the scan's slowest blocks running alone.  The
+// result does not depend on the count (first index on ties).
 constexpr int kCertMaxBlocks = 256;
-int cert_blocks(const BatchShape& s) {
+int cert_blocks(const BatchShape& s, int resident) {
   static const int sms = [] {
     int dev = 0, v = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
     return v;
   }();
-  const long long want = (4LL * sms + s.B - 1) / s.B;
-  const long long most = std::max(1LL, (s.n() + 1023) / 1024);
-  return static_cast<int>(std::max(1LL, std::min({want, most, static_cast<long long>(kCertMaxBlocks)})));
+  const long long most = std::min(std::max(1LL, (s.n() + 1023) / 1024), static_cast<long long>(kCertMaxBlocks));
+  const long long lo = std::max(1LL, std::min((4LL * sms + s.B - 1) / s.B, most));
+  const long long slots = static_cast<long long>(sms) * std::max(1, resident);
+  long long best = lo;
+  double best_fill = 0.0;
+  for (long long n = lo; n <= std::min(most, 4 * lo); ++n) {
+    const long long ctas = n * s.B;
+    const double fill = static_cast<double>(ctas) / static_cast<double>(((ctas + slots - 1) / slots) * slots);
+    if (fill > best_fill + 1e-9) {
+      best_fill = fill;
+      best = n;
+    }
+    if (fill >= 0.97) break;
+  }
+  return static_cast<int>(best);
 }
 
 size_t cert_scratch_bytes(const BatchShape& s) {
@@ -1167,7 +1183,7 @@ __global__ void __launch_bounds__(32) cert_step_kernel(PolishArgs A, FbmeCertifi
 
 // Block (bx, scene) scores atoms [bx chunk, (bx + 1) chunk) against the
 // staged model and writes its best to the scene's partials.
-__global__ void __launch_bounds__(kCertThreads) cert_scan_kernel(PolishArgs A, void* ws) {
+__global__ void __launch_bounds__(kCertThreads, 3) cert_scan_kernel(PolishArgs A, void* ws) {
   __shared__ float2 M[32][33];
   __shared__ CertModel model;
   __shared__ CertBest red[kCertThreads / 32];
@@ -1395,7 +1411,11 @@ void polish_run(const BatchShape& s, const DevConfig& c, const PolishBuffers& p,
     FBME_TIMED(prof, FBME_GROUP_POLISH, (polish_kernel<<<s.B, 32, dsm, st>>>(A, 1)));
   }
   if (cert) {  // model, scan, (decide + model, scan) per repair, final
-    const int nblk = cert_blocks(s);
+    int resident = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, cert_scan_kernel, kCertThreads, dsm) !=
+        cudaSuccess)
+      resident = 1;
+    const int nblk = cert_blocks(s, resident);
     for (int t = 0; t <= c.repairs + 1; ++t) {
       FBME_TIMED(prof, FBME_GROUP_CERTIFICATE,
                  (cert_step_kernel<<<s.B, 32, dsm, st>>>(A, *cert, cert->workspace, nblk, t)));
