@@ -866,7 +866,7 @@ struct CertModel {
 // Largest one-coordinate ratio over the atoms [j0, j1) of the grid (first
 // index on ties, as torch's max), with its atom precision s_j; the block's
 // best, in every thread.
-FBME_DEV CertBest cert_scan(const PolishArgs& A, const float2 (*L)[33], const CertModel& m, int K, float nu,
+FBME_DEV CertBest cert_scan(const PolishArgs& A, const float2 (*L)[34], const CertModel& m, int K, float nu,
                             const float2* bp, const float2* d1, const float2* d2, long long j0, long long j1,
                             CertBest* red) {
   const BatchShape& s = A.s;
@@ -889,11 +889,20 @@ FBME_DEV CertBest cert_scan(const PolishArgs& A, const float2 (*L)[33], const Ce
         q.x -= g.x * mu.x - g.y * mu.y;
         q.y -= g.x * mu.y + g.y * mu.x;
         float2 c = make_float2(g.x * m.inv_d[i], -g.y * m.inv_d[i]);
+        // Row i of L in 16-byte pairs (rows start 16-byte aligned), same
+        // order of the multiply-adds as one entry at a time.
 #pragma unroll
-        for (int k = 0; k < i; ++k) {
-          const float2 l = L[i][k];
-          c.x -= l.x * v[k].x - l.y * v[k].y;
-          c.y -= l.x * v[k].y + l.y * v[k].x;
+        for (int k = 0; k + 1 < i; k += 2) {
+          const float4 l2 = *reinterpret_cast<const float4*>(&L[i][k]);
+          c.x -= l2.x * v[k].x - l2.y * v[k].y;
+          c.y -= l2.x * v[k].y + l2.y * v[k].x;
+          c.x -= l2.z * v[k + 1].x - l2.w * v[k + 1].y;
+          c.y -= l2.z * v[k + 1].y + l2.w * v[k + 1].x;
+        }
+        if (i & 1) {
+          const float2 l = L[i][i - 1];
+          c.x -= l.x * v[i - 1].x - l.y * v[i - 1].y;
+          c.y -= l.x * v[i - 1].y + l.y * v[i - 1].x;
         }
         v[i] = make_float2(c.x * m.inv_l[i], c.y * m.inv_l[i]);
         red2 += abs_sq(v[i]);
@@ -1184,7 +1193,7 @@ __global__ void __launch_bounds__(32) cert_step_kernel(PolishArgs A, FbmeCertifi
 // Block (bx, scene) scores atoms [bx chunk, (bx + 1) chunk) against the
 // staged model and writes its best to the scene's partials.
 __global__ void __launch_bounds__(kCertThreads, 3) cert_scan_kernel(PolishArgs A, void* ws) {
-  __shared__ float2 M[32][33];
+  __shared__ __align__(16) float2 M[32][34];
   __shared__ CertModel model;
   __shared__ CertBest red[kCertThreads / 32];
   extern __shared__ float2 dtab[];
